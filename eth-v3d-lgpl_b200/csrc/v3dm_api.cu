@@ -1,0 +1,596 @@
+// v3dm_api.cu -- host side of the C ABI (include/v3dm.h) for the matcher.
+//
+// Mirrors V3D_CUDA::SIFT_Matching (V3D/CUDA/v3d_cudamatching.h:15-67,
+// v3d_cudamatching.cu:437-696): the handle keeps device buffers sized at allocate(), the
+// current left/right descriptors, and the guided gates applied since the last putative
+// call.  The reference recomputes nothing in runGuidedMatching: it masks the score
+// matrix that the last findPutativeMatches left behind (.cu:597), so gates of successive
+// guided calls compound.  Here no score matrix exists; a guided call re-runs the fused
+// kernel with every gate recorded since the last putative call, which yields the same
+// masked matrix and therefore the same matches.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "v3dm_internal.h"
+
+using namespace v3dm;
+
+struct v3dm_matcher {
+  int device = 0;
+  unsigned kernel = V3DM_KERNEL_TCGEN05;
+  cudaStream_t stream = nullptr;
+  bool allocated = false;
+  bool guidedAlloc = false;
+  int nMaxL = 0, nMaxR = 0;
+  int nL = 0, nR = 0;
+  uint8_t* dL = nullptr;
+  uint8_t* dR = nullptr;
+  float* dStage = nullptr;        // float upload staging, max(nMaxL, nMaxR) x 128
+  unsigned long long* dLBest = nullptr;  // per left: best key
+  unsigned int* dLSec = nullptr;         // per left: second value + 1
+  unsigned long long* dRBest = nullptr;  // per right: best key
+  unsigned int* dRSec = nullptr;         // per right: second value + 1
+  unsigned long long* dCand = nullptr;   // candidate list: nSeg x segCap
+  int* dSegCount = nullptr;              // nSeg counts
+  long long segCap = 0;
+  int nSeg = 0;
+  int32_t* dScratch = nullptr;    // nMaxR + nMaxL ints of finalize scratch
+  int32_t* dPairs = nullptr;      // 2 * min(nMaxL, nMaxR)
+  int32_t* dInfo = nullptr;       // kInfoWords: pair count, error flags, largest segment
+  int32_t* hInfo = nullptr;       // pinned mirror of dInfo
+  bool pendingCheck = false;      // a device-only call whose info block was not read yet
+  float* dLPos = nullptr;         // positions upload (interleaved x, y)
+  float* dRPos = nullptr;
+  float4* dGateL = nullptr;       // V3DM_MAX_GATES x nMaxL
+  float4* dGateR = nullptr;       // V3DM_MAX_GATES x nMaxR
+  int nGates = 0;
+  GateParams gates[V3DM_MAX_GATES];
+  TcPlan* tc = nullptr;
+  bool tcBound = false;
+  int lastLaunches = 0;
+};
+
+namespace {
+
+#define V3DM_CUDA_TRY(expr)                      \
+  do {                                           \
+    cudaError_t e_ = (expr);                     \
+    if (e_ != cudaSuccess) return V3DM_ERR_CUDA; \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void free_buffers(v3dm_matcher* h) {
+  dfree(h->dL);
+  dfree(h->dR);
+  dfree(h->dStage);
+  dfree(h->dLBest);
+  dfree(h->dLSec);
+  dfree(h->dRBest);
+  dfree(h->dRSec);
+  dfree(h->dCand);
+  dfree(h->dSegCount);
+  dfree(h->dScratch);
+  dfree(h->dPairs);
+  dfree(h->dInfo);
+  dfree(h->dLPos);
+  dfree(h->dRPos);
+  dfree(h->dGateL);
+  dfree(h->dGateR);
+  if (h->hInfo) cudaFreeHost(h->hInfo);
+  h->hInfo = nullptr;
+  h->allocated = false;
+  h->tcBound = false;
+  h->nL = h->nR = 0;
+  h->nGates = 0;
+  h->segCap = 0;
+  h->nSeg = 0;
+  h->pendingCheck = false;
+}
+
+// (Re)allocates the candidate list for nSeg segments of segCap entries each.
+cudaError_t alloc_candidates(v3dm_matcher* h, int nSeg, long long segCap) {
+  dfree(h->dCand);
+  dfree(h->dSegCount);
+  h->segCap = 0;
+  h->nSeg = 0;
+  cudaError_t e = dalloc(&h->dCand, (size_t)nSeg * (size_t)segCap);
+  if (e == cudaSuccess) e = dalloc(&h->dSegCount, (size_t)nSeg);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dSegCount, 0, (size_t)nSeg * sizeof(int), h->stream);
+  if (e != cudaSuccess) return e;
+  h->segCap = segCap;
+  h->nSeg = nSeg;
+  return cudaSuccess;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// ---- candidate threshold ------------------------------------------------------------
+// The decision of one side is accept(s1, s2) with s1 the best and s2 the second best score
+// of that side.  For fixed s1 it is monotone in s2: nextDist = max(0.001, 2 - 2*s2) is
+// non-increasing in s2 (each rounding is monotone) and bestDist / nextDist is monotone in
+// nextDist with the sign of bestDist.  Hence, if accept(s1, hi) == accept(s1, -1e30f) for
+// the largest value hi below T, every value below T gives the same decision.  For
+// s1 > 1 (S1 > 2^18) bestDist < 0 and ratio < 0 for every s2: the decision is the same
+// for all s2 whenever minRatio >= 0, so only S1 in [Smin, 2^18] needs checking.
+
+bool invariant_below(int32_t T, int32_t Smin, float minScore, float minRatio, bool gated) {
+  float hi = T > 0 ? score_of(T - 1) : (gated ? kMasked : kNone);
+  int32_t top = kMaxScore < (1 << 18) ? kMaxScore : (1 << 18);
+  for (int32_t S1 = Smin; S1 <= top; ++S1) {
+    float s1 = score_of(S1);
+    if (accept_scores(s1, hi, minScore, minRatio) != accept_scores(s1, kNone, minScore, minRatio)) return false;
+  }
+  return true;
+}
+
+struct ThrKey {
+  uint32_t ms, mr;
+  bool gated;
+  bool operator==(const ThrKey& o) const { return ms == o.ms && mr == o.mr && gated == o.gated; }
+};
+
+std::mutex g_thrMutex;
+ThrKey g_thrKeys[16];
+int32_t g_thrVals[16];
+int g_thrN = 0, g_thrNext = 0;
+
+int compute_threshold(float minScore, float minRatio, bool gated, int32_t* Tout) {
+  // Smin: smallest S with score(S) > minScore (kMaxScore + 1 when none).
+  int32_t Smin;
+  if (!(minScore == minScore)) {
+    Smin = kMaxScore + 1;  // NaN: 's1 > minScore' is never true
+  } else if (minScore < 0.0f) {
+    Smin = 0;
+  } else {
+    double g = std::floor((double)minScore * 262144.0);
+    Smin = g > (double)kMaxScore ? kMaxScore + 1 : (int32_t)g;
+    while (Smin > 0 && score_of(Smin - 1) > minScore) --Smin;
+    while (Smin <= kMaxScore && !(score_of(Smin) > minScore)) ++Smin;
+  }
+  if (Smin > kMaxScore || minRatio < 0.0f || !(minRatio == minRatio)) {
+    // Nothing can pass, or no ratio test, or a NaN ratio (never accepted): only the best
+    // value matters and it cannot pass below Smin.
+    *Tout = Smin;
+    return V3DM_OK;
+  }
+  if (!invariant_below(0, Smin, minScore, minRatio, gated)) return V3DM_ERR_UNSUPPORTED;
+  // Largest valid T in [0, Smin]; validity is monotone (a smaller T is valid when T is).
+  // Start from the analytic cut-off c = 1 - (1 - minScore)/minRatio of s2, then gallop up.
+  int32_t lo = 0;
+  if (minRatio > 0.0f) {
+    double c = 1.0 - (1.0 - (double)minScore) / (double)minRatio;
+    double gS = std::floor(c * 262144.0) - 4.0;
+    if (gS > 0) {
+      int32_t g = gS < (double)Smin ? (int32_t)gS : Smin;
+      while (g > 0 && !invariant_below(g, Smin, minScore, minRatio, gated)) g /= 2;
+      lo = g;
+    }
+  }
+  int32_t step = 1;
+  while (lo + step <= Smin && invariant_below(lo + step, Smin, minScore, minRatio, gated)) {
+    lo += step;
+    step *= 2;
+  }
+  int32_t hi = lo + step - 1 < Smin ? lo + step - 1 : Smin;  // lo valid; lo + step invalid or > Smin
+  while (lo < hi) {
+    int32_t mid = lo + (hi - lo + 1) / 2;
+    if (invariant_below(mid, Smin, minScore, minRatio, gated)) lo = mid;
+    else hi = mid - 1;
+  }
+  *Tout = lo;
+  return V3DM_OK;
+}
+
+}  // namespace
+
+int v3dm::host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T) {
+  ThrKey k;
+  std::memcpy(&k.ms, &minScore, 4);
+  std::memcpy(&k.mr, &minRatio, 4);
+  k.gated = gated;
+  {
+    std::lock_guard<std::mutex> lock(g_thrMutex);
+    for (int i = 0; i < g_thrN; ++i)
+      if (g_thrKeys[i] == k) {
+        *T = g_thrVals[i];
+        return V3DM_OK;
+      }
+  }
+  int32_t t = 0;
+  int st = compute_threshold(minScore, minRatio, gated, &t);
+  if (st != V3DM_OK) return st;
+  std::lock_guard<std::mutex> lock(g_thrMutex);
+  g_thrKeys[g_thrNext] = k;
+  g_thrVals[g_thrNext] = t;
+  g_thrNext = (g_thrNext + 1) % 16;
+  if (g_thrN < 16) ++g_thrN;
+  *T = t;
+  return V3DM_OK;
+}
+
+extern "C" {
+
+const char* v3dm_status_string(int s) {
+  switch (s) {
+    case V3DM_OK: return "ok";
+    case V3DM_ERR_ARG: return "invalid argument";
+    case V3DM_ERR_CUDA: return "CUDA error";
+    case V3DM_ERR_NOT_ALLOCATED: return "not allocated";
+    case V3DM_ERR_SIZE: return "feature count above the allocated maximum";
+    case V3DM_ERR_CAPACITY: return "output buffer too small";
+    case V3DM_ERR_NOT_U8: return "float descriptor is not u/512 with u in 0..255";
+    case V3DM_ERR_UNSUPPORTED: return "parameters outside the exact domain";
+    case V3DM_ERR_TIMEOUT: return "device wait timed out";
+    case V3DM_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case V3DM_ERR_CANDIDATES: return "candidate list overflow (list grown; repeat the call)";
+    default: return "unknown status";
+  }
+}
+
+int v3dm_candidate_threshold(float minScore, float minRatio, int gated, int32_t* T) {
+  if (!T) return V3DM_ERR_ARG;
+  return host_candidate_threshold(minScore, minRatio, gated != 0, T);
+}
+
+int v3dm_matcher_create(v3dm_matcher** out, int device, unsigned kernel) {
+  if (!out || kernel > V3DM_KERNEL_SIMT) return V3DM_ERR_ARG;
+  *out = nullptr;
+  int nDev = 0;
+  if (cudaGetDeviceCount(&nDev) != cudaSuccess || device < 0 || device >= nDev) return V3DM_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return V3DM_ERR_CUDA;
+  if (prop.major != 10) return V3DM_ERR_NO_DEVICE;
+  v3dm_matcher* h = new (std::nothrow) v3dm_matcher();
+  if (!h) return V3DM_ERR_ARG;
+  h->device = device;
+  h->kernel = kernel;
+  DeviceGuard g(device);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return V3DM_ERR_CUDA;
+  }
+  if (kernel == V3DM_KERNEL_TCGEN05 && tc_plan_create(&h->tc, device) != cudaSuccess) {
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return V3DM_ERR_CUDA;
+  }
+  *out = h;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_destroy(v3dm_matcher* h) {
+  if (!h) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  if (h->tc) tc_plan_destroy(h->tc);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return V3DM_OK;
+}
+
+int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
+  if (!h || nMaxL < 0 || nMaxR < 0) return V3DM_ERR_ARG;
+  if (nMaxL > V3DM_MAX_FEATURES || nMaxR > V3DM_MAX_FEATURES) return V3DM_ERR_SIZE;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  h->nMaxL = nMaxL;
+  h->nMaxR = nMaxR;
+  h->guidedAlloc = useGuided != 0;
+  int nMax = nMaxL > nMaxR ? nMaxL : nMaxR;
+  int nMin = nMaxL < nMaxR ? nMaxL : nMaxR;
+  // Operand rows are padded to whole 256-row tiles so TMA boxes never leave the buffer.
+  size_t rowsL = ((size_t)nMaxL + 255) / 256 * 256, rowsR = ((size_t)nMaxR + 255) / 256 * 256;
+  bool ok = dalloc(&h->dL, rowsL * kDescBytes) == cudaSuccess && dalloc(&h->dR, rowsR * kDescBytes) == cudaSuccess &&
+            dalloc(&h->dStage, (size_t)nMax * kDescBytes) == cudaSuccess &&
+            dalloc(&h->dLBest, (size_t)nMaxL + 1) == cudaSuccess && dalloc(&h->dLSec, (size_t)nMaxL + 1) == cudaSuccess &&
+            dalloc(&h->dRBest, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dRSec, (size_t)nMaxR + 1) == cudaSuccess &&
+            dalloc(&h->dScratch, (size_t)nMaxL + nMaxR + 1) == cudaSuccess &&
+            dalloc(&h->dPairs, 2 * (size_t)nMin + 2) == cudaSuccess && dalloc(&h->dInfo, kInfoWords) == cudaSuccess &&
+            cudaMallocHost(reinterpret_cast<void**>(&h->hInfo), kInfoWords * sizeof(int32_t)) == cudaSuccess;
+  if (ok && h->guidedAlloc)
+    ok = dalloc(&h->dLPos, 2 * (size_t)nMaxL + 2) == cudaSuccess && dalloc(&h->dRPos, 2 * (size_t)nMaxR + 2) == cudaSuccess &&
+         dalloc(&h->dGateL, (size_t)V3DM_MAX_GATES * nMaxL + 1) == cudaSuccess &&
+         dalloc(&h->dGateR, (size_t)V3DM_MAX_GATES * nMaxR + 1) == cudaSuccess;
+  if (ok) {
+    // Candidate list: about 1e-3 of all scores exceed T on SIFT-like data; start with room
+    // for 1/256 of them and grow when a call reports an overflow.
+    int nSeg = h->kernel == V3DM_KERNEL_SIMT ? 1 : tc_segments(h->tc);
+    long long total = (long long)nMaxL * (long long)nMaxR / 256;
+    long long segCap = total / nSeg + 1;
+    if (segCap < 4096) segCap = 4096;
+    ok = alloc_candidates(h, nSeg, segCap) == cudaSuccess;
+  }
+  if (ok) {
+    ok = cudaMemsetAsync(h->dLBest, 0, ((size_t)nMaxL + 1) * 8, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dLSec, 0, ((size_t)nMaxL + 1) * 4, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dRBest, 0, ((size_t)nMaxR + 1) * 8, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dRSec, 0, ((size_t)nMaxR + 1) * 4, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dL, 0, rowsL * kDescBytes, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dR, 0, rowsR * kDescBytes, h->stream) == cudaSuccess &&
+         cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream) == cudaSuccess &&
+         cudaStreamSynchronize(h->stream) == cudaSuccess;
+  }
+  if (!ok) {
+    free_buffers(h);
+    return V3DM_ERR_CUDA;
+  }
+  h->allocated = true;
+  return V3DM_OK;
+}
+
+int v3dm_deallocate(v3dm_matcher* h) {
+  if (!h) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  return V3DM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int set_features_u8(v3dm_matcher* h, bool left, int n, const uint8_t* desc, bool onDevice) {
+  if (!h || n < 0 || (n > 0 && !desc)) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  if (n > (left ? h->nMaxL : h->nMaxR)) return V3DM_ERR_SIZE;
+  DeviceGuard g(h->device);
+  uint8_t* dst = left ? h->dL : h->dR;
+  if (n > 0)
+    V3DM_CUDA_TRY(cudaMemcpyAsync(dst, desc, (size_t)n * kDescBytes,
+                                  onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+  (left ? h->nL : h->nR) = n;
+  h->tcBound = false;
+  return V3DM_OK;
+}
+
+int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
+  if (!h || n < 0 || (n > 0 && !desc)) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  if (n > (left ? h->nMaxL : h->nMaxR)) return V3DM_ERR_SIZE;
+  DeviceGuard g(h->device);
+  uint8_t* dst = left ? h->dL : h->dR;
+  if (n > 0) {
+    V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream));
+    V3DM_CUDA_TRY(cudaMemcpyAsync(h->dStage, desc, (size_t)n * kDescBytes * sizeof(float), cudaMemcpyHostToDevice,
+                                  h->stream));
+    V3DM_CUDA_TRY(launch_f32_to_u8(h->dStage, dst, n, h->dInfo + kInfoErr, h->stream));
+    V3DM_CUDA_TRY(cudaMemcpyAsync(h->hInfo + kInfoErr, h->dInfo + kInfoErr, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->hInfo[kInfoErr] & kErrNotU8) {
+      (left ? h->nL : h->nR) = 0;
+      cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream);
+      return V3DM_ERR_NOT_U8;
+    }
+  }
+  (left ? h->nL : h->nR) = n;
+  h->tcBound = false;
+  return V3DM_OK;
+}
+
+// Enqueues the fused matching kernel, the seconds pass and the finalize kernel for the
+// current gates.  The result lands in dPairs / dInfo on the handle's stream.
+int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
+  int32_t T = 0;
+  int st = host_candidate_threshold(minScore, minRatio, h->nGates > 0, &T);
+  if (st != V3DM_OK) return st;
+  MatchArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nL = h->nL;
+  a.nR = h->nR;
+  a.T = T;
+  a.lBest = h->dLBest;
+  a.lSec = h->dLSec;
+  a.rBest = h->dRBest;
+  a.rSec = h->dRSec;
+  a.cand = h->dCand;
+  a.segCount = h->dSegCount;
+  a.segCap = h->segCap;
+  a.nSeg = h->nSeg;
+  a.err = h->dInfo + kInfoErr;
+  a.nGates = h->nGates;
+  for (int i = 0; i < h->nGates; ++i) a.gates[i] = h->gates[i];
+  h->lastLaunches = 0;
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream));
+  if (h->nL > 0 && h->nR > 0 && T <= kMaxScore) {
+    if (h->kernel == V3DM_KERNEL_SIMT) {
+      V3DM_CUDA_TRY(launch_match_simt(h->dL, h->dR, a, h->stream));
+      h->lastLaunches += 1;
+    } else {
+      if (!h->tcBound) {
+        V3DM_CUDA_TRY(tc_plan_bind(h->tc, h->dL, h->nL, h->dR, h->nR));
+        h->tcBound = true;
+      }
+      int nl = 0;
+      V3DM_CUDA_TRY(launch_match_tc(h->tc, a, h->stream, &nl));
+      h->lastLaunches += nl;
+    }
+    V3DM_CUDA_TRY(launch_seconds(a, h->stream));
+    h->lastLaunches += 1;
+  }
+  V3DM_CUDA_TRY(launch_finalize(a, minScore, minRatio, h->dScratch, dPairs, h->dInfo, h->stream));
+  h->lastLaunches += 1;
+  h->pendingCheck = true;
+  return V3DM_OK;
+}
+
+// Reads the info block of the last call.  Returns V3DM_OK, an error, or -1 when the
+// candidate list overflowed (the list has been grown and the call must be repeated).
+int read_info(v3dm_matcher* h) {
+  V3DM_CUDA_TRY(cudaMemcpyAsync(h->hInfo, h->dInfo, kInfoWords * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->pendingCheck = false;
+  int err = h->hInfo[kInfoErr];
+  if (err & kErrWaitTimeout) return V3DM_ERR_TIMEOUT;
+  if (err) return V3DM_ERR_CUDA;
+  long long need = h->hInfo[kInfoMaxSeg];
+  if (need > h->segCap) {
+    V3DM_CUDA_TRY(alloc_candidates(h, h->nSeg, need + need / 4 + 1024));
+    return -1;
+  }
+  return V3DM_OK;
+}
+
+// Runs one matching call with host output, repeating it once the candidate list has grown.
+int run_host(v3dm_matcher* h, float minScore, float minRatio, int32_t* pairs, int cap, int* nOut) {
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    int st = enqueue_match(h, minScore, minRatio, h->dPairs);
+    if (st != V3DM_OK) return st;
+    st = read_info(h);
+    if (st == -1) continue;
+    if (st != V3DM_OK) return st;
+    int n = h->hInfo[kInfoPairs];
+    if (nOut) *nOut = n;
+    int ncopy = n < cap ? n : cap;
+    if (ncopy > 0) {
+      V3DM_CUDA_TRY(cudaMemcpyAsync(pairs, h->dPairs, (size_t)ncopy * 2 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                    h->stream));
+      V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    return n > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
+  }
+  return V3DM_ERR_CUDA;
+}
+
+int add_gate(v3dm_matcher* h, int type, const double* M, float thr, const float* lpos, const float* rpos,
+             bool onDevice) {
+  if (!h->guidedAlloc) return V3DM_ERR_NOT_ALLOCATED;
+  if (h->nGates >= V3DM_MAX_GATES) return V3DM_ERR_SIZE;
+  int gi = h->nGates;
+  const float* dl = lpos;
+  const float* dr = rpos;
+  if (!onDevice) {
+    if (h->nL > 0)
+      V3DM_CUDA_TRY(cudaMemcpyAsync(h->dLPos, lpos, (size_t)h->nL * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                                    h->stream));
+    if (h->nR > 0)
+      V3DM_CUDA_TRY(cudaMemcpyAsync(h->dRPos, rpos, (size_t)h->nR * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                                    h->stream));
+    dl = h->dLPos;
+    dr = h->dRPos;
+  }
+  float4* lv = h->dGateL + (size_t)gi * h->nMaxL;
+  float4* rv = h->dGateR + (size_t)gi * h->nMaxR;
+  V3DM_CUDA_TRY(launch_gate_precompute(type, M, dl, h->nL, dr, h->nR, lv, rv, h->stream));
+  GateParams& gp = h->gates[gi];
+  gp.type = type;
+  gp.sqrThr = thr * thr;  // float product, as the reference (.cu:591)
+  gp.lv = lv;
+  gp.rv = rv;
+  h->nGates = gi + 1;
+  return V3DM_OK;
+}
+
+int guided_common(v3dm_matcher* h, int type, const double* M, float thr, const float* lpos, const float* rpos,
+                  float minScore, float minRatio, int32_t* pairs, int cap, int* nOut) {
+  if (!h || !M || (cap > 0 && !pairs) || cap < 0) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  if ((h->nL > 0 && !lpos) || (h->nR > 0 && !rpos)) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int st = add_gate(h, type, M, thr, lpos, rpos, false);
+  if (st != V3DM_OK) return st;
+  return run_host(h, minScore, minRatio, pairs, cap, nOut);
+}
+
+}  // namespace
+
+extern "C" {
+
+int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, true, n, d, false); }
+int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, false, n, d, false); }
+int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, true, n, d); }
+int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, false, n, d); }
+
+int v3dm_putative(v3dm_matcher* h, float minScore, float minRatio, int32_t* pairs, int cap, int* nOut) {
+  if (!h || (cap > 0 && !pairs) || cap < 0) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  DeviceGuard g(h->device);
+  h->nGates = 0;
+  return run_host(h, minScore, minRatio, pairs, cap, nOut);
+}
+
+int v3dm_guided_F(v3dm_matcher* h, const double* F, float thr, const float* lpos, const float* rpos, float minScore,
+                  float minRatio, int32_t* pairs, int cap, int* nOut) {
+  return guided_common(h, 1, F, thr, lpos, rpos, minScore, minRatio, pairs, cap, nOut);
+}
+
+int v3dm_guided_H(v3dm_matcher* h, const double* H, float thr, const float* lpos, const float* rpos, float minScore,
+                  float minRatio, int32_t* pairs, int cap, int* nOut) {
+  return guided_common(h, 2, H, thr, lpos, rpos, minScore, minRatio, pairs, cap, nOut);
+}
+
+int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count) {
+  if (!h || !d_pairs || !d_count) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  DeviceGuard g(h->device);
+  h->nGates = 0;
+  int st = enqueue_match(h, minScore, minRatio, d_pairs);
+  if (st != V3DM_OK) return st;
+  V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+  return V3DM_OK;
+}
+
+int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, const float* d_lpos, const float* d_rpos,
+                         float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count) {
+  if (!h || !F || !d_pairs || !d_count) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  DeviceGuard g(h->device);
+  int st = add_gate(h, 1, F, thr, d_lpos, d_rpos, true);
+  if (st != V3DM_OK) return st;
+  st = enqueue_match(h, minScore, minRatio, d_pairs);
+  if (st != V3DM_OK) return st;
+  V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+  return V3DM_OK;
+}
+
+int v3dm_matcher_stream(v3dm_matcher* h, void** s) {
+  if (!h || !s) return V3DM_ERR_ARG;
+  *s = (void*)h->stream;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_wait(v3dm_matcher* h) {
+  if (!h) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  if (!h->pendingCheck) {
+    V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return V3DM_OK;
+  }
+  int st = read_info(h);
+  return st == -1 ? V3DM_ERR_CANDIDATES : st;
+}
+
+int v3dm_matcher_last_launches(v3dm_matcher* h, int* n) {
+  if (!h || !n) return V3DM_ERR_ARG;
+  *n = h->lastLaunches;
+  return V3DM_OK;
+}
+
+}  // extern "C"

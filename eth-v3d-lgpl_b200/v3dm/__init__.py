@@ -1,0 +1,280 @@
+"""Python mirror of the reference's matching interface over the C ABI of libv3dm.so.
+
+``SIFTMatching`` follows ``V3D_CUDA::SIFT_Matching`` (V3D/CUDA/v3d_cudamatching.h:15-67) and
+``VocabularyTreeTraversal`` follows ``V3D_CUDA::VocabularyTreeTraversal<BF, Depth>``
+(v3d_cudamatching.h:69-105): same member names in snake_case, same argument meaning and
+defaults (minScore 0.9, minRatio 0.8).  Where the reference prints and exits
+(v3d_cudamatching.cu:12-27) this wrapper raises ``V3DMError``.  The library has no CPU
+path: without the built libv3dm.so or without an sm_100 GPU every compute call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "libv3dm.so"
+HEADER_PATH = PKG_DIR.parent / "include" / "v3dm.h"
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_NOT_ALLOCATED = 3
+ERR_SIZE = 4
+ERR_CAPACITY = 5
+ERR_NOT_U8 = 6
+ERR_UNSUPPORTED = 7
+ERR_TIMEOUT = 8
+ERR_NO_DEVICE = 9
+ERR_CANDIDATES = 10
+
+KERNEL_TCGEN05 = 0
+KERNEL_SIMT = 1
+LEAF_GLOBAL = 0
+LEAF_LOCAL = 1
+MAX_FEATURES = 131072
+MAX_GATES = 8
+
+_lib = None
+
+
+class V3DMError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = lib().v3dm_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
+
+
+def lib() -> C.CDLL:
+    """The loaded libv3dm.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"libv3dm.so not built ({LIB_PATH}); run __graft_entry__.build()")
+        L = C.CDLL(str(LIB_PATH))
+        vp, i32, f32, f64p = C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_double)
+        L.v3dm_status_string.restype = C.c_char_p
+        L.v3dm_status_string.argtypes = [i32]
+        L.v3dm_matcher_create.argtypes = [C.POINTER(vp), i32, C.c_uint]
+        L.v3dm_matcher_destroy.argtypes = [vp]
+        L.v3dm_allocate.argtypes = [vp, i32, i32, i32]
+        L.v3dm_deallocate.argtypes = [vp]
+        for n in ("v3dm_set_left_f32", "v3dm_set_right_f32", "v3dm_set_left_u8", "v3dm_set_right_u8"):
+            getattr(L, n).argtypes = [vp, i32, vp]
+        L.v3dm_putative.argtypes = [vp, f32, f32, vp, i32, C.POINTER(i32)]
+        for n in ("v3dm_guided_F", "v3dm_guided_H"):
+            getattr(L, n).argtypes = [vp, f64p, f32, vp, vp, f32, f32, vp, i32, C.POINTER(i32)]
+        L.v3dm_putative_device.argtypes = [vp, f32, f32, vp, vp]
+        L.v3dm_guided_F_device.argtypes = [vp, f64p, f32, vp, vp, f32, f32, vp, vp]
+        L.v3dm_matcher_stream.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_matcher_wait.argtypes = [vp]
+        L.v3dm_matcher_last_launches.argtypes = [vp, C.POINTER(i32)]
+        L.v3dm_candidate_threshold.argtypes = [f32, f32, i32, C.POINTER(C.c_int32)]
+        L.v3dm_voctree_create.argtypes = [C.POINTER(vp), i32, i32, i32]
+        L.v3dm_voctree_destroy.argtypes = [vp]
+        L.v3dm_voctree_counts.argtypes = [i32, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.v3dm_voctree_allocate.argtypes = [vp, i32]
+        L.v3dm_voctree_set_nodes_f32.argtypes = [vp, vp]
+        L.v3dm_voctree_set_nodes_u8.argtypes = [vp, vp]
+        L.v3dm_voctree_quantize_f32.argtypes = [vp, i32, vp, vp, i32]
+        L.v3dm_voctree_quantize_u8.argtypes = [vp, i32, vp, vp, i32]
+        L.v3dm_voctree_quantize_u8_device.argtypes = [vp, i32, vp, vp, i32]
+        L.v3dm_voctree_stream.argtypes = [vp, C.POINTER(vp)]
+        _lib = L
+    return _lib
+
+
+def _check(status: int, what: str) -> None:
+    if status != OK:
+        raise V3DMError(status, what)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def candidate_threshold(min_score: float, min_ratio: float, gated: bool) -> int:
+    """Candidate threshold T of the fused selection (host computation, no GPU needed)."""
+    t = C.c_int32(0)
+    _check(lib().v3dm_candidate_threshold(min_score, min_ratio, int(gated), C.byref(t)), "candidate_threshold")
+    return t.value
+
+
+def _desc(desc: np.ndarray):
+    d = np.ascontiguousarray(desc)
+    if d.ndim != 2 or d.shape[1] != 128:
+        raise ValueError("descriptors must be an (n, 128) array")
+    if d.dtype == np.uint8:
+        return d, "u8"
+    return np.ascontiguousarray(d, dtype=np.float32), "f32"
+
+
+def _pos(pos: np.ndarray, n: int) -> np.ndarray:
+    p = np.ascontiguousarray(pos, dtype=np.float32)
+    if p.shape != (n, 2):
+        raise ValueError(f"positions must be ({n}, 2)")
+    return p
+
+
+class SIFTMatching:
+    """V3D_CUDA::SIFT_Matching over libv3dm.so (one CUDA stream per instance)."""
+
+    def __init__(self, device: int = 0, kernel: int = KERNEL_TCGEN05):
+        h = C.c_void_p()
+        _check(lib().v3dm_matcher_create(C.byref(h), device, kernel), "SIFT_Matching()")
+        self._h = h
+        self.n_left = 0
+        self.n_right = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().v3dm_matcher_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def allocate(self, n_max_left: int, n_max_right: int | None = None, use_guided_matching: bool = False):
+        """SIFT_Matching::allocate (v3d_cudamatching.h:33-37); sizes used as given."""
+        if n_max_right is None:
+            n_max_right = n_max_left
+        _check(lib().v3dm_allocate(self._h, int(n_max_left), int(n_max_right), int(use_guided_matching)), "allocate")
+
+    def deallocate(self):
+        _check(lib().v3dm_deallocate(self._h), "deallocate")
+
+    def set_left_features(self, desc: np.ndarray):
+        d, kind = _desc(desc)
+        fn = lib().v3dm_set_left_u8 if kind == "u8" else lib().v3dm_set_left_f32
+        _check(fn(self._h, d.shape[0], _ptr(d)), "setLeftFeatures")
+        self.n_left = d.shape[0]
+
+    def set_right_features(self, desc: np.ndarray):
+        d, kind = _desc(desc)
+        fn = lib().v3dm_set_right_u8 if kind == "u8" else lib().v3dm_set_right_f32
+        _check(fn(self._h, d.shape[0], _ptr(d)), "setRightFeatures")
+        self.n_right = d.shape[0]
+
+    def _result(self, fn, *args) -> np.ndarray:
+        cap = max(1, min(self.n_left, self.n_right))
+        out = np.empty((cap, 2), np.int32)
+        n = C.c_int(0)
+        _check(fn(self._h, *args, _ptr(out), cap, C.byref(n)), fn.__name__)
+        return out[: n.value].copy()
+
+    def find_putative_matches(self, min_score: float = 0.9, min_ratio: float = 0.8) -> np.ndarray:
+        """SIFT_Matching::findPutativeMatches (v3d_cudamatching.h:45-46): (n, 2) (left, right)."""
+        return self._result(lib().v3dm_putative, C.c_float(min_score), C.c_float(min_ratio))
+
+    def run_guided_matching(self, F, distance_threshold: float, left_positions, right_positions,
+                            min_score: float = 0.9, min_ratio: float = 0.8) -> np.ndarray:
+        """SIFT_Matching::runGuidedMatching (v3d_cudamatching.h:48-52)."""
+        Fm = np.ascontiguousarray(np.asarray(F, np.float64).reshape(3, 3))
+        lp, rp = _pos(left_positions, self.n_left), _pos(right_positions, self.n_right)
+        return self._result(lib().v3dm_guided_F, Fm.ctypes.data_as(C.POINTER(C.c_double)),
+                            C.c_float(distance_threshold), _ptr(lp), _ptr(rp), C.c_float(min_score),
+                            C.c_float(min_ratio))
+
+    def run_guided_homography_matching(self, H, distance_threshold: float, left_positions, right_positions,
+                                       min_score: float = 0.9, min_ratio: float = 0.8) -> np.ndarray:
+        """SIFT_Matching::runGuidedHomographyMatching (v3d_cudamatching.h:54-58)."""
+        Hm = np.ascontiguousarray(np.asarray(H, np.float64).reshape(3, 3))
+        lp, rp = _pos(left_positions, self.n_left), _pos(right_positions, self.n_right)
+        return self._result(lib().v3dm_guided_H, Hm.ctypes.data_as(C.POINTER(C.c_double)),
+                            C.c_float(distance_threshold), _ptr(lp), _ptr(rp), C.c_float(min_score),
+                            C.c_float(min_ratio))
+
+    # ---- device-resident calls (pointers are device addresses, e.g. torch data_ptr()) ----
+    def putative_device(self, min_score: float, min_ratio: float, d_pairs: int, d_count: int):
+        _check(lib().v3dm_putative_device(self._h, min_score, min_ratio, C.c_void_p(d_pairs), C.c_void_p(d_count)),
+               "putative_device")
+
+    def guided_F_device(self, F, thr: float, d_lpos: int, d_rpos: int, min_score: float, min_ratio: float,
+                        d_pairs: int, d_count: int):
+        Fm = np.ascontiguousarray(np.asarray(F, np.float64).reshape(3, 3))
+        _check(lib().v3dm_guided_F_device(self._h, Fm.ctypes.data_as(C.POINTER(C.c_double)), thr,
+                                          C.c_void_p(d_lpos), C.c_void_p(d_rpos), min_score, min_ratio,
+                                          C.c_void_p(d_pairs), C.c_void_p(d_count)), "guided_F_device")
+
+    def wait(self) -> None:
+        _check(lib().v3dm_matcher_wait(self._h), "wait")
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().v3dm_matcher_stream(self._h, C.byref(s)), "stream")
+        return s.value or 0
+
+    def last_launches(self) -> int:
+        n = C.c_int(0)
+        _check(lib().v3dm_matcher_last_launches(self._h, C.byref(n)), "last_launches")
+        return n.value
+
+
+def voctree_counts(branch_factor: int, depth: int):
+    nc, lc = C.c_int64(0), C.c_int64(0)
+    _check(lib().v3dm_voctree_counts(branch_factor, depth, C.byref(nc), C.byref(lc)), "voctree_counts")
+    return nc.value, lc.value
+
+
+class VocabularyTreeTraversal:
+    """V3D_CUDA::VocabularyTreeTraversal<BranchFactor, Depth> with a runtime shape."""
+
+    def __init__(self, branch_factor: int, depth: int, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_voctree_create(C.byref(h), device, branch_factor, depth), "VocabularyTreeTraversal()")
+        self._h = h
+        self.branch_factor, self.depth = branch_factor, depth
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().v3dm_voctree_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def get_node_count(self) -> int:
+        return voctree_counts(self.branch_factor, self.depth)[0]
+
+    def get_leave_count(self) -> int:
+        return voctree_counts(self.branch_factor, self.depth)[1]
+
+    def allocate(self, n_max_features: int):
+        _check(lib().v3dm_voctree_allocate(self._h, int(n_max_features)), "allocate")
+
+    def set_nodes(self, nodes: np.ndarray):
+        d = np.ascontiguousarray(nodes)
+        if d.shape != (self.get_node_count(), 128):
+            raise ValueError("nodes must be (node count, 128)")
+        if d.dtype == np.uint8:
+            _check(lib().v3dm_voctree_set_nodes_u8(self._h, _ptr(d)), "setNodes")
+        else:
+            d = np.ascontiguousarray(d, dtype=np.float32)
+            _check(lib().v3dm_voctree_set_nodes_f32(self._h, _ptr(d)), "setNodes")
+
+    def traverse_tree(self, features: np.ndarray, id_mode: int = LEAF_GLOBAL) -> np.ndarray:
+        d, kind = _desc(features)
+        out = np.empty(d.shape[0], np.int32)
+        fn = lib().v3dm_voctree_quantize_u8 if kind == "u8" else lib().v3dm_voctree_quantize_f32
+        _check(fn(self._h, d.shape[0], _ptr(d), _ptr(out), id_mode), "traverseTree")
+        return out
+
+    def quantize_device(self, n: int, d_keys: int, d_ids: int, id_mode: int = LEAF_GLOBAL):
+        _check(lib().v3dm_voctree_quantize_u8_device(self._h, n, C.c_void_p(d_keys), C.c_void_p(d_ids), id_mode),
+               "quantize_device")
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().v3dm_voctree_stream(self._h, C.byref(s)), "stream")
+        return s.value or 0

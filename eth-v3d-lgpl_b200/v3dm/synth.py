@@ -1,0 +1,217 @@
+"""Seeded synthetic workloads for the matching path (no dataset ships with the reference).
+
+The shapes and value distributions follow the five benchmark workloads of this project:
+
+* ``pair``       one image pair, 4096 x 4096 SIFT-like uint8 descriptors, 30% of the right
+                 set are noisy copies of random left descriptors;
+* ``stereo``     one 16384 x 16384 pair whose planted matches obey a fundamental matrix of a
+                 random stereo rig (for guided matching);
+* ``images``     many images with uneven feature counts and shared feature tracks (batched
+                 all-pairs matching);
+* ``voctree``    a hierarchical k-means vocabulary tree and query descriptors.
+
+Descriptor generator: i.i.d. Gamma(k=0.6, theta=1) components, L2-normalised, clamped at
+0.2, renormalised, scaled by 512, rounded and clamped to 0..255 (the SIFT normalisation of
+V3D/Base/v3d_feature.h:19-39 followed by the uint8 quantisation u = 512 * f).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MIN_SCORE = 0.7
+MIN_RATIO = 0.8
+
+
+def rng_for(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def sift_like(rng: np.random.Generator, n: int) -> np.ndarray:
+    """n x 128 uint8 SIFT-like descriptors."""
+    out = np.empty((n, 128), np.uint8)
+    step = 1 << 18
+    for s in range(0, n, step):
+        e = min(n, s + step)
+        x = rng.gamma(0.6, 1.0, size=(e - s, 128)).astype(np.float32)
+        x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+        np.minimum(x, 0.2, out=x)
+        x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+        out[s:e] = np.clip(np.rint(x * 512.0), 0, 255).astype(np.uint8)
+    return out
+
+
+def noisy_copy(rng: np.random.Generator, u: np.ndarray, sigma: float = 8.0) -> np.ndarray:
+    """Copies of uint8 descriptors with N(0, sigma^2) noise, re-rounded and clamped."""
+    v = u.astype(np.float32) + rng.normal(0.0, sigma, size=u.shape).astype(np.float32)
+    return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+
+
+def pair(seed: int = 0, n_left: int = 4096, n_right: int = 4096, planted: float = 0.3):
+    """One image pair.  Returns (L, R, truth) with truth[r] = planted left index or -1."""
+    rng = rng_for(seed)
+    L = sift_like(rng, n_left)
+    n_p = int(round(planted * n_right)) if n_left > 0 else 0
+    src = rng.integers(0, n_left, n_p)
+    R = np.concatenate([noisy_copy(rng, L[src]), sift_like(rng, n_right - n_p)])
+    truth = np.concatenate([src, -np.ones(n_right - n_p, np.int64)])
+    perm = rng.permutation(n_right)
+    return L, R[perm].copy(), truth[perm].copy()
+
+
+def rig(rng: np.random.Generator, f: float = 1200.0, width: int = 1600, height: int = 1200,
+        baseline: float = 0.3, max_yaw_deg: float = 10.0):
+    """Random stereo rig.  Returns (K, Rot, t, F) with X2 = Rot X1 + t and q^T F p = 0."""
+    K = np.array([[f, 0, width / 2.0], [0, f, height / 2.0], [0, 0, 1.0]])
+    yaw = np.deg2rad(rng.uniform(-max_yaw_deg, max_yaw_deg))
+    c, s = np.cos(yaw), np.sin(yaw)
+    Rot = np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+    C2 = np.array([baseline, 0.0, 0.0])
+    t = -Rot @ C2
+    tx = np.array([[0, -t[2], t[1]], [t[2], 0, -t[0]], [-t[1], t[0], 0]])
+    Ki = np.linalg.inv(K)
+    F = Ki.T @ tx @ Rot @ Ki
+    return K, Rot, t, F
+
+
+def stereo(seed: int = 1, n_left: int = 16384, n_right: int = 16384, planted: float = 0.3,
+           width: int = 1600, height: int = 1200, noise_px: float = 1.0):
+    """Guided-matching pair: (L, R, lpos, rpos, F, truth).  Planted right features are the
+    projections of the 3-D point behind a left keypoint (depth U(2, 20) m) plus N(0, 1 px)
+    noise, with noisy-copy descriptors; the rest are fresh features at uniform positions."""
+    rng = rng_for(seed)
+    K, Rot, t, F = rig(rng, width=width, height=height)
+    L = sift_like(rng, n_left)
+    lpos = np.stack([rng.uniform(0, width, n_left), rng.uniform(0, height, n_left)], 1)
+    n_p = min(int(round(planted * n_right)), n_left)
+    src = rng.choice(n_left, n_p, replace=False)
+    depth = rng.uniform(2.0, 20.0, n_p)
+    rays = np.linalg.inv(K) @ np.vstack([lpos[src].T, np.ones(n_p)])
+    X1 = rays * depth
+    X2 = Rot @ X1 + t[:, None]
+    q = K @ X2
+    qpos = (q[:2] / q[2]).T + rng.normal(0.0, noise_px, (n_p, 2))
+    R = np.concatenate([noisy_copy(rng, L[src]), sift_like(rng, n_right - n_p)])
+    rpos = np.concatenate([qpos, np.stack([rng.uniform(0, width, n_right - n_p),
+                                           rng.uniform(0, height, n_right - n_p)], 1)])
+    truth = np.concatenate([src, -np.ones(n_right - n_p, np.int64)])
+    perm = rng.permutation(n_right)
+    return (L, R[perm].copy(), lpos.astype(np.float32), rpos[perm].astype(np.float32), F,
+            truth[perm].copy())
+
+
+def images(seed: int = 2, n_images: int = 200, n_min: int = 1000, n_max: int = 12000,
+           track_frac: float = 0.15, track_len=(2, 8)):
+    """Image set for all-pairs matching.  Returns (desc, counts, offsets): desc is the
+    concatenation of all images' uint8 descriptors.  A track is a base descriptor observed
+    in a random subset of images with per-view N(0, 8^2) noise; track observations make up
+    track_frac of every image's features."""
+    rng = rng_for(seed)
+    counts = rng.integers(n_min, n_max + 1, n_images)
+    slots = np.rint(track_frac * counts).astype(np.int64)
+    remaining = slots.copy()
+    obs_img, obs_track = [], []
+    n_tracks = 0
+    while True:
+        avail = np.flatnonzero(remaining > 0)
+        if avail.size < 2:
+            break
+        k = min(int(rng.integers(track_len[0], track_len[1] + 1)), avail.size)
+        p = remaining[avail] / remaining[avail].sum()
+        members = rng.choice(avail, k, replace=False, p=p)
+        remaining[members] -= 1
+        obs_img.append(members)
+        obs_track.append(np.full(k, n_tracks))
+        n_tracks += 1
+    obs_img = np.concatenate(obs_img) if obs_img else np.zeros(0, np.int64)
+    obs_track = np.concatenate(obs_track) if obs_track else np.zeros(0, np.int64)
+    base = sift_like(rng, n_tracks)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    desc = np.empty((int(offsets[-1]), 128), np.uint8)
+    order = np.argsort(obs_img, kind="stable")
+    obs_img, obs_track = obs_img[order], obs_track[order]
+    starts = np.searchsorted(obs_img, np.arange(n_images))
+    ends = np.searchsorted(obs_img, np.arange(n_images), side="right")
+    for i in range(n_images):
+        tr = obs_track[starts[i]:ends[i]]
+        feats = np.concatenate([noisy_copy(rng, base[tr]), sift_like(rng, int(counts[i]) - tr.size)])
+        desc[offsets[i]:offsets[i + 1]] = feats[rng.permutation(int(counts[i]))]
+    return desc, counts.astype(np.int32), offsets
+
+
+def all_pairs(n_images: int) -> np.ndarray:
+    """All unordered pairs (i, j), i < j, left = i."""
+    i, j = np.triu_indices(n_images, 1)
+    return np.stack([i, j], 1).astype(np.int32)
+
+
+def hkm_tree(rng: np.random.Generator, data: np.ndarray, bf: int, depth: int, iters: int = 4,
+             chunk: int = 1 << 16) -> np.ndarray:
+    """Hierarchical k-means vocabulary tree with uint8-valued centres.
+
+    Returns nodeCount x 128 uint8 centres in breadth-first order without the root (the layout
+    of V3D/Base/v3d_voctree.h:22-34).  Points are assigned to the child with the largest dot
+    product, the rule the quantizer descends by.  Centres are rounded means; a cluster that
+    loses all its points keeps its previous centre; a node with fewer points than children
+    seeds the missing children from noisy copies of its points (or fresh descriptors)."""
+    n = data.shape[0]
+    node_of = np.zeros(n, np.int64)  # node index (global, -1 = root) of each point's current node
+    level_nodes = 1
+    out = []
+    parent_base = -1
+    for d in range(depth):
+        n_parents = level_nodes
+        # group points by parent (local parent index 0..n_parents-1)
+        local_parent = node_of - (parent_base if d > 0 else 0) if d > 0 else np.zeros(n, np.int64)
+        order = np.argsort(local_parent, kind="stable")
+        sp = local_parent[order]
+        starts = np.searchsorted(sp, np.arange(n_parents))
+        cnt = np.searchsorted(sp, np.arange(n_parents), side="right") - starts
+        # init: bf random members per parent (with replacement), noisy so duplicates split
+        pick = starts[:, None] + (rng.random((n_parents, bf)) * np.maximum(cnt, 1)[:, None]).astype(np.int64)
+        pick = np.minimum(pick, n - 1)
+        cent = data[order[pick.reshape(-1)]].reshape(n_parents, bf, 128)
+        cent = noisy_copy(rng, cent, 4.0)
+        empty = cnt == 0
+        if empty.any():
+            cent[empty] = sift_like(rng, int(empty.sum()) * bf).reshape(-1, bf, 128)
+        centf = cent.astype(np.float32)
+        for it in range(iters + 1):
+            child = np.empty(n, np.int64)
+            for s in range(0, n, chunk):
+                e = min(n, s + chunk)
+                c = centf[local_parent[s:e]]  # (m, bf, 128)
+                scores = np.einsum("mkd,md->mk", c, data[s:e].astype(np.float32))
+                child[s:e] = np.argmax(scores, axis=1)  # first max on ties
+            if it == iters:
+                break
+            idx = local_parent * bf + child
+            sums = np.zeros((n_parents * bf, 128), np.float64)
+            _segment_sum(sums, idx, data)
+            num = np.bincount(idx, minlength=n_parents * bf)
+            has = num > 0
+            newc = centf.reshape(-1, 128).copy()
+            newc[has] = np.clip(np.rint(sums[has] / num[has, None]), 0, 255)
+            centf = newc.reshape(n_parents, bf, 128).astype(np.float32)
+        out.append(centf.astype(np.uint8).reshape(-1, 128))
+        level_start = sum(bf ** (k + 1) for k in range(d))
+        node_of = level_start + local_parent * bf + child
+        parent_base = level_start
+        level_nodes = n_parents * bf
+    return np.concatenate(out, 0)
+
+
+def _segment_sum(sums: np.ndarray, idx: np.ndarray, data: np.ndarray) -> None:
+    """sums[k] = sum of data rows with idx == k."""
+    order = np.argsort(idx, kind="stable")
+    uniq, first = np.unique(idx[order], return_index=True)
+    sums[uniq] = np.add.reduceat(data[order].astype(np.float64), first, axis=0)
+
+
+def voctree(seed: int = 3, bf: int = 10, depth: int = 6, n_train: int = 500_000,
+            n_query: int = 2_000_000, iters: int = 4):
+    """(nodes, queries): an HKM tree trained on n_train descriptors and n_query queries."""
+    rng = rng_for(seed)
+    train = sift_like(rng, n_train)
+    nodes = hkm_tree(rng, train, bf, depth, iters)
+    queries = sift_like(rng, n_query)
+    return nodes, queries

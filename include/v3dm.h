@@ -1,0 +1,153 @@
+/*
+ * v3dm.h -- C ABI of the B200-native SIFT descriptor matching library (libv3dm.so).
+ *
+ * Drop-in boundary for ETH-V3D's CUDA matching path.  The reference exposes it as the C++
+ * structs V3D_CUDA::SIFT_Matching and V3D_CUDA::VocabularyTreeTraversal<BF, Depth>
+ * (V3D/CUDA/v3d_cudamatching.h:15-105); each entry point below names the member it
+ * replaces.  compat/CUDA/v3d_cudamatching.h (in the package directory) re-creates that
+ * C++ surface on top of these functions.
+ *
+ * Conventions (differences from the reference are deliberate and listed):
+ *   - every call returns a status code (V3DM_OK == 0); nothing prints or exits.  The
+ *     reference prints and calls exit() on CUDA errors (v3d_cudamatching.cu:12-27);
+ *   - a handle owns one CUDA stream and all its device buffers; calls on one handle are
+ *     serialised by the caller (the reference is single-threaded too);
+ *   - descriptors are 128 bytes (uint8) or 128 floats each, descriptor-contiguous, the
+ *     layout of SIFT_Feature::descriptor (V3D/Base/v3d_feature.h:17);
+ *   - scores of uint8 descriptors u, v are S * 2^-18 with S = sum u_i v_i: the exact FP32
+ *     score the reference computes for descriptors u/512, v/512;
+ *   - match pairs are (left index, right index) int32 pairs in ascending left order, the
+ *     order of the reference's mutual filter (v3d_cudamatching.cu:546-551);
+ *   - feature counts are taken as given (no rounding to multiples of 32); the compat
+ *     header applies the reference's rounding and clamping.
+ */
+#ifndef V3DM_H
+#define V3DM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define V3DM_API __attribute__((visibility("default")))
+#else
+#define V3DM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define V3DM_OK 0
+#define V3DM_ERR_ARG 1             /* null pointer, negative size, bad enum            */
+#define V3DM_ERR_CUDA 2            /* a CUDA runtime or driver call failed             */
+#define V3DM_ERR_NOT_ALLOCATED 3   /* call before allocate / set_nodes                 */
+#define V3DM_ERR_SIZE 4            /* count above the allocated maximum or 131072      */
+#define V3DM_ERR_CAPACITY 5        /* output buffer smaller than the result; the first
+                                      'cap' entries are written, *nOut holds the total */
+#define V3DM_ERR_NOT_U8 6          /* float descriptor not of the form u/512, u in 0..255 */
+#define V3DM_ERR_UNSUPPORTED 7     /* parameter combination outside the exact domain   */
+#define V3DM_ERR_TIMEOUT 8         /* a bounded device-side wait gave up               */
+#define V3DM_ERR_NO_DEVICE 9       /* no sm_100 device (the library has no CPU path)   */
+#define V3DM_ERR_CANDIDATES 10     /* a device-only call overflowed the candidate list; the
+                                      list has been grown, repeat the call             */
+
+V3DM_API const char* v3dm_status_string(int status);
+
+/* Largest feature count per image side (17-bit index field of the device state). */
+#define V3DM_MAX_FEATURES 131072
+/* Largest number of compounding guided gates on one putative result. */
+#define V3DM_MAX_GATES 8
+
+/* ---- matcher (V3D_CUDA::SIFT_Matching) -------------------------------------------- */
+typedef struct v3dm_matcher v3dm_matcher;
+
+/* Kernel selection flags for v3dm_matcher_create. */
+#define V3DM_KERNEL_TCGEN05 0u /* tcgen05 integer MMA with fused selection (default) */
+#define V3DM_KERNEL_SIMT 1u    /* dp4a SIMT kernel with the same fused selection     */
+
+/* Creates a matcher on CUDA device 'device'.  Replaces the constructor
+ * SIFT_Matching::SIFT_Matching (v3d_cudamatching.h:17-21). */
+V3DM_API int v3dm_matcher_create(v3dm_matcher** out, int device, unsigned kernel);
+V3DM_API int v3dm_matcher_destroy(v3dm_matcher* h);
+
+/* SIFT_Matching::allocate(nMaxLeft, nMaxRight, useGuidedMatching)
+ * (v3d_cudamatching.h:33, v3d_cudamatching.cu:439-474).  Sizes are used as given. */
+V3DM_API int v3dm_allocate(v3dm_matcher* h, int nMaxLeft, int nMaxRight, int useGuided);
+/* SIFT_Matching::deallocate (v3d_cudamatching.h:39, .cu:476-488). */
+V3DM_API int v3dm_deallocate(v3dm_matcher* h);
+
+/* SIFT_Matching::setLeftFeatures / setRightFeatures (v3d_cudamatching.h:41-42,
+ * .cu:490-520): float descriptors, which must be u/512-valued (else V3DM_ERR_NOT_U8). */
+V3DM_API int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* desc);
+V3DM_API int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* desc);
+/* Native uint8 descriptors (u = 512 * the reference's float value). */
+V3DM_API int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* desc);
+V3DM_API int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* desc);
+
+/* SIFT_Matching::findPutativeMatches(matches, minScore, minRatio)
+ * (v3d_cudamatching.h:45-46, .cu:522-552).  minRatio < 0 disables the ratio test.
+ * pairs: 2*cap int32 (left, right); *nOut = number of pairs.  Clears the guided gates. */
+V3DM_API int v3dm_putative(v3dm_matcher* h, float minScore, float minRatio, int32_t* pairs, int cap, int* nOut);
+
+/* SIFT_Matching::runGuidedMatching(F, thr, leftPos, rightPos, matches, minScore, minRatio)
+ * (v3d_cudamatching.h:48-52, .cu:554-623).  F: row-major 3x3 double with q^T F p = 0 for
+ * left p, right q.  Positions: interleaved (x, y) floats, one pair per current feature.
+ * Like the reference, the gate compounds with the gates of earlier guided calls since the
+ * last putative call. */
+V3DM_API int v3dm_guided_F(v3dm_matcher* h, const double* F, float thr, const float* leftPos, const float* rightPos,
+                  float minScore, float minRatio, int32_t* pairs, int cap, int* nOut);
+/* SIFT_Matching::runGuidedHomographyMatching (v3d_cudamatching.h:54-58, .cu:625-694). */
+V3DM_API int v3dm_guided_H(v3dm_matcher* h, const double* H, float thr, const float* leftPos, const float* rightPos,
+                  float minScore, float minRatio, int32_t* pairs, int cap, int* nOut);
+
+/* Device-resident variants (no host copies, no synchronisation): the result is written to
+ * device memory on the handle's stream.  d_pairs holds 2*min(nLeft, nRight) int32,
+ * d_count one int32.  Used to time the kernels with inputs resident in HBM. */
+V3DM_API int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count);
+V3DM_API int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, const float* d_leftPos,
+                         const float* d_rightPos, float minScore, float minRatio, int32_t* d_pairs,
+                         int32_t* d_count);
+/* Waits for the handle's stream and returns the status of the last device-only call. */
+V3DM_API int v3dm_matcher_wait(v3dm_matcher* h);
+/* The handle's CUDA stream (a cudaStream_t). */
+V3DM_API int v3dm_matcher_stream(v3dm_matcher* h, void** stream);
+/* Number of kernels the last matching call launched. */
+V3DM_API int v3dm_matcher_last_launches(v3dm_matcher* h, int* n);
+
+/* Candidate threshold of the fused selection: every score S >= T is examined exactly and
+ * no score below T can change a decision.  Exposed for tests.  Host-only, no device. */
+V3DM_API int v3dm_candidate_threshold(float minScore, float minRatio, int gated, int32_t* T);
+
+/* ---- vocabulary tree (V3D_CUDA::VocabularyTreeTraversal<BF, Depth>) --------------- */
+typedef struct v3dm_voctree v3dm_voctree;
+
+#define V3DM_LEAF_GLOBAL 0 /* node index of the leaf, as _cuda_traverseTree (.cu:791)        */
+#define V3DM_LEAF_LOCAL 1  /* leaf index within the last level, as VocabularyTree (v3d_voctree.h:78) */
+
+/* Constructor of VocabularyTreeTraversal<BF, Depth> (v3d_cudamatching.h:71, .cu:797-801);
+ * the shape is a runtime parameter here. */
+V3DM_API int v3dm_voctree_create(v3dm_voctree** out, int device, int branchFactor, int depth);
+V3DM_API int v3dm_voctree_destroy(v3dm_voctree* t);
+/* getNodeCount / getLeaveCount (v3d_cudamatching.h:80-99). */
+V3DM_API int v3dm_voctree_counts(int branchFactor, int depth, int64_t* nodeCount, int64_t* leafCount);
+/* allocate(nMaxFeatures) / deallocate (v3d_cudamatching.h:73-74, .cu:803-829). */
+V3DM_API int v3dm_voctree_allocate(v3dm_voctree* t, int nMax);
+/* setNodes(nodes) (v3d_cudamatching.h:76, .cu:831-843): nodeCount x 128 descriptors in
+ * breadth-first order without the root.  Float nodes and keys follow the matcher's
+ * convention: u/512 with u in 0..255 (else V3DM_ERR_NOT_U8).  For such data every FP32 dot
+ * product of the reference is exact, so leaf ids do not depend on summation order. */
+V3DM_API int v3dm_voctree_set_nodes_f32(v3dm_voctree* t, const float* nodes);
+V3DM_API int v3dm_voctree_set_nodes_u8(v3dm_voctree* t, const uint8_t* nodes);
+/* traverseTree(n, features, leaveIds) (v3d_cudamatching.h:78, .cu:845-863). */
+V3DM_API int v3dm_voctree_quantize_f32(v3dm_voctree* t, int n, const float* keys, int32_t* ids, int idMode);
+V3DM_API int v3dm_voctree_quantize_u8(v3dm_voctree* t, int n, const uint8_t* keys, int32_t* ids, int idMode);
+/* Device-resident variant: keys and ids in device memory, asynchronous on the tree's stream. */
+V3DM_API int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode);
+V3DM_API int v3dm_voctree_stream(v3dm_voctree* t, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* V3DM_H */

@@ -1,0 +1,190 @@
+"""ctypes loader for the parity oracle (liboracle.so) and the reference builds in _ref/.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, never by the library.  See v3dm_oracle.c for what each function restates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_VOCTREE = HERE / "_ref" / "libv3dref_voctree.so"
+REF_CUDA = HERE / "_ref" / "libv3dref_cuda.so"
+
+_lib = None
+
+
+class Gate(C.Structure):
+    _fields_ = [("type", C.c_int), ("m", C.c_double * 9), ("thr", C.c_float)]
+
+
+def build() -> None:
+    """Builds liboracle.so (and the _ref libraries when the reference sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    if Path(os.environ.get("V3D_REF_DIR", "/root/reference/V3D")).exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+        L.orc_match_u8.argtypes = [i32, i32, vp, vp, f32, f32, i32, vp, vp, vp, vp, vp, vp, i32]
+        L.orc_match_u8.restype = i32
+        L.orc_voctree_quantize_f32.argtypes = [i32, i32, vp, i32, vp, vp, i32, i32]
+        L.orc_voctree_quantize_u8.argtypes = [i32, i32, vp, i32, vp, vp, i32, i32]
+        L.orc_scores_u8.argtypes = [i32, i32, vp, vp, vp]
+        L.orc_ref_feature_count.argtypes = [i32, i32]
+        L.orc_ref_feature_count.restype = i32
+        L.orc_num_threads.restype = i32
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def _gates(gates):
+    arr = (Gate * max(1, len(gates)))()
+    for i, (typ, M, thr) in enumerate(gates):
+        arr[i].type = 1 if typ in ("F", 1) else 2
+        for k, v in enumerate(np.asarray(M, np.float64).reshape(9)):
+            arr[i].m[k] = float(v)
+        arr[i].thr = float(thr)
+    return arr
+
+
+def match(L: np.ndarray, R: np.ndarray, min_score: float = 0.9, min_ratio: float = 0.8, gates=(),
+          lpos=None, rpos=None, threads: int = 0, with_sides: bool = False):
+    """The reference's putative (no gates) or guided matching on uint8 descriptors.
+
+    gates: sequence of ("F" | "H", 3x3 matrix, threshold); they compound as successive
+    runGuidedMatching calls do.  Returns (n, 2) int32 pairs (left, right) ascending in left,
+    plus the per-left and per-right results when with_sides."""
+    L = np.ascontiguousarray(L, np.uint8)
+    R = np.ascontiguousarray(R, np.uint8)
+    nL, nR = L.shape[0], R.shape[0]
+    g = _gates(list(gates))
+    lp = np.ascontiguousarray(lpos, np.float32) if lpos is not None else np.zeros((1, 2), np.float32)
+    rp = np.ascontiguousarray(rpos, np.float32) if rpos is not None else np.zeros((1, 2), np.float32)
+    pairs = np.empty((max(1, min(nL, nR)), 2), np.int32)
+    colmax = np.empty(max(1, nL), np.int32)
+    rowmax = np.empty(max(1, nR), np.int32)
+    n = lib().orc_match_u8(nL, nR, L.ctypes.data, R.ctypes.data, min_score, min_ratio, len(gates),
+                           C.addressof(g), lp.ctypes.data, rp.ctypes.data, colmax.ctypes.data, rowmax.ctypes.data,
+                           pairs.ctypes.data, threads)
+    if n < 0:
+        raise ValueError("oracle rejected the arguments")
+    out = pairs[:n].copy()
+    if with_sides:
+        return out, colmax[:nL].copy(), rowmax[:nR].copy()
+    return out
+
+
+def scores(L: np.ndarray, R: np.ndarray) -> np.ndarray:
+    """Integer score matrix S[r, l] (small cases)."""
+    L = np.ascontiguousarray(L, np.uint8)
+    R = np.ascontiguousarray(R, np.uint8)
+    S = np.empty((R.shape[0], L.shape[0]), np.int32)
+    lib().orc_scores_u8(L.shape[0], R.shape[0], L.ctypes.data, R.ctypes.data, S.ctypes.data)
+    return S
+
+
+def voctree(bf: int, depth: int, nodes: np.ndarray, keys: np.ndarray, global_ids: bool = True,
+            threads: int = 0) -> np.ndarray:
+    keys_c = np.ascontiguousarray(keys)
+    nodes_c = np.ascontiguousarray(nodes)
+    out = np.empty(keys_c.shape[0], np.int32)
+    if keys_c.dtype == np.uint8:
+        rc = lib().orc_voctree_quantize_u8(bf, depth, nodes_c.ctypes.data, keys_c.shape[0], keys_c.ctypes.data,
+                                           out.ctypes.data, int(global_ids), threads)
+    else:
+        nodes_c = np.ascontiguousarray(nodes_c, np.float32)
+        keys_c = np.ascontiguousarray(keys_c, np.float32)
+        rc = lib().orc_voctree_quantize_f32(bf, depth, nodes_c.ctypes.data, keys_c.shape[0], keys_c.ctypes.data,
+                                            out.ctypes.data, int(global_ids), threads)
+    if rc != 0:
+        raise ValueError("oracle rejected the arguments")
+    return out
+
+
+def ref_feature_count(n: int, n_max_rounded: int) -> int:
+    return lib().orc_ref_feature_count(n, n_max_rounded)
+
+
+# ---- the reference's own code ---------------------------------------------------------------
+
+def ref_voctree_available() -> bool:
+    return REF_VOCTREE.exists()
+
+
+def ref_voctree(bf: int, depth: int, nodes_f32: np.ndarray, keys_f32: np.ndarray) -> np.ndarray:
+    """V3D::VocabularyTree<depth, bf, 128>::getVisualWord (leaf-local ids), compiled from the
+    reference headers."""
+    L = C.CDLL(str(REF_VOCTREE))
+    L.v3dref_voctree_quantize.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    n = np.ascontiguousarray(nodes_f32, np.float32)
+    k = np.ascontiguousarray(keys_f32, np.float32)
+    out = np.empty(k.shape[0], np.int32)
+    rc = L.v3dref_voctree_quantize(bf, depth, n.ctypes.data, k.shape[0], k.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"shape BF={bf} D={depth} not instantiated in ref_voctree_wrap.cpp")
+    return out
+
+
+def ref_cuda_available() -> bool:
+    return REF_CUDA.exists()
+
+
+_REF_CHILD = r"""
+import ctypes as C, sys, numpy as np
+d = np.load(sys.argv[1])
+L = C.CDLL(sys.argv[2])
+L.v3dref_match.argtypes = [C.c_int]*4 + [C.c_void_p]*2 + [C.c_float]*2 + [C.c_int] + [C.c_void_p]*6 + [C.c_void_p]
+Lf = np.ascontiguousarray(d['L'], np.float32); Rf = np.ascontiguousarray(d['R'], np.float32)
+gt = np.ascontiguousarray(d['gtypes'], np.int32); gm = np.ascontiguousarray(d['gmats'], np.float64)
+gth = np.ascontiguousarray(d['gthr'], np.float32)
+lp = np.ascontiguousarray(d['lpos'], np.float32); rp = np.ascontiguousarray(d['rpos'], np.float32)
+nL, nR = Lf.shape[0], Rf.shape[0]
+pairs = np.empty((max(1, min(nL, nR)), 2), np.int32); nput = C.c_int(0)
+n = L.v3dref_match(int(d['nmaxl']), int(d['nmaxr']), nL, nR, Lf.ctypes.data, Rf.ctypes.data,
+                   float(d['ms']), float(d['mr']), int(gt.size), gt.ctypes.data, gm.ctypes.data, gth.ctypes.data,
+                   lp.ctypes.data, rp.ctypes.data, pairs.ctypes.data, C.byref(nput))
+np.save(sys.argv[3], pairs[:max(n, 0)])
+sys.exit(0 if n >= 0 else 3)
+"""
+
+
+def ref_cuda_match(L_u8: np.ndarray, R_u8: np.ndarray, min_score: float, min_ratio: float, gates=(),
+                   lpos=None, rpos=None, workdir: str | None = None) -> np.ndarray:
+    """The reference's own SIFT_Matching (v3d_cudamatching.cu) on a GPU, fed u/512 floats.
+    Runs in a child process because the reference exits on any CUDA error.  Sizes must be
+    multiples of 32 (the reference's own requirement)."""
+    import tempfile
+    wd = Path(workdir or tempfile.mkdtemp(prefix="v3dref_"))
+    wd.mkdir(parents=True, exist_ok=True)
+    gates = list(gates)
+    nL, nR = L_u8.shape[0], R_u8.shape[0]
+    np.savez(wd / "in.npz", L=L_u8.astype(np.float32) / 512.0, R=R_u8.astype(np.float32) / 512.0,
+             gtypes=np.array([1 if t in ("F", 1) else 2 for t, _, _ in gates], np.int32),
+             gmats=np.array([np.asarray(M, np.float64).reshape(9) for _, M, _ in gates], np.float64).reshape(-1),
+             gthr=np.array([thr for _, _, thr in gates], np.float32),
+             lpos=np.zeros((nL, 2), np.float32) if lpos is None else lpos,
+             rpos=np.zeros((nR, 2), np.float32) if rpos is None else rpos,
+             nmaxl=nL, nmaxr=nR, ms=min_score, mr=min_ratio)
+    res = subprocess.run([sys.executable, "-c", _REF_CHILD, str(wd / "in.npz"), str(REF_CUDA), str(wd / "out.npy")],
+                         capture_output=True, text=True, timeout=600)
+    if res.returncode != 0:
+        raise RuntimeError(f"reference matcher failed ({res.returncode}): {res.stderr[-2000:]}")
+    return np.load(wd / "out.npy")

@@ -1,0 +1,45 @@
+"""The C ABI library loads and exports every symbol include/v3dm.h declares (no GPU needed)."""
+import ctypes as C
+import re
+
+import pytest
+
+
+def _declared(header):
+    return sorted(set(re.findall(r"V3DM_API\s+(?:const\s+char\s*\*|int)\s+(v3dm_\w+)\s*\(", header.read_text())))
+
+
+def test_exports_every_declared_symbol(v3dm_mod):
+    names = _declared(v3dm_mod.HEADER_PATH)
+    assert len(names) >= 25
+    lib = C.CDLL(str(v3dm_mod.LIB_PATH))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings(v3dm_mod):
+    lib = v3dm_mod.lib()
+    for s in range(0, 11):
+        assert lib.v3dm_status_string(s) and lib.v3dm_status_string(s) != b"unknown status"
+
+
+def test_no_cpu_fallback_without_gpu(v3dm_mod):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(v3dm_mod.V3DMError) as e:
+        v3dm_mod.SIFTMatching()
+    assert e.value.status == v3dm_mod.ERR_NO_DEVICE
+    with pytest.raises(v3dm_mod.V3DMError) as e:
+        v3dm_mod.VocabularyTreeTraversal(10, 3)
+    assert e.value.status == v3dm_mod.ERR_NO_DEVICE
+
+
+def test_null_arguments_are_rejected(v3dm_mod):
+    lib = v3dm_mod.lib()
+    assert lib.v3dm_matcher_create(None, 0, 0) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_allocate(None, 10, 10, 0) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_putative(None, 0.7, 0.8, None, 0, None) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_voctree_counts(0, 3, None, None) == v3dm_mod.ERR_ARG
+    assert v3dm_mod.voctree_counts(10, 6) == (1111110, 1000000)
+    assert v3dm_mod.voctree_counts(50, 3) == (127550, 125000)
