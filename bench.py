@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the SIFT matching path on B200.
+
+Default workload (one step): putative matching followed by F-guided matching (2 px gate) of one
+16384 x 16384 pair of uint8 SIFT-like descriptors, minScore 0.7, ratio 0.8 -- the single large
+guided pair.  Metric: image pairs per second.  `value` times the steps with descriptors and
+positions resident in HBM (device-output C-ABI calls); `e2e` times the same step through the
+host C-ABI calls (pinned host buffers in, host pairs out, copies inside the timed region).
+Other workloads (--workload pair | voctree) exist for exploration; the default line is the
+stereo one.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the path is one pair per
+GPU; pairs are independent), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for p in (str(ROOT / "eth-v3d-lgpl_b200"), str(ROOT)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+MIN_SCORE, MIN_RATIO, GATE_PX = 0.7, 0.8, 2.0
+N_SIDE = 16384
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["stereo", "pair", "voctree"], default="stereo")
+    ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=1)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if os.environ.get("V3DM_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, x: float, device=None) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs"), "bf16_tflops": d.get("bf16_tflops"), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "fallback"}
+
+
+def traffic_from_profiles(kernel_tag: str):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary, or None."""
+    for f in sorted((ROOT / "profiles").glob(f"*{kernel_tag}*.md")):
+        for line in f.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(gpu_index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_stereo(L, R, lpos, rpos, F, n_left_sample: int, threads: int = 0):
+    """Oracle putative + F-guided matching of n_left_sample lefts against all rights; returns
+    (seconds, fraction of the full pair covered)."""
+    from oracle import oracle
+    Ls, lp = L[:n_left_sample], lpos[:n_left_sample]
+    t0 = time.perf_counter()
+    oracle.match(Ls, R, MIN_SCORE, MIN_RATIO, threads=threads)
+    oracle.match(Ls, R, MIN_SCORE, MIN_RATIO, gates=[("F", F, GATE_PX)], lpos=lp, rpos=rpos, threads=threads)
+    dt = time.perf_counter() - t0
+    return dt, n_left_sample / L.shape[0]
+
+
+def run_reference_arm(args, ws, rank):
+    """The reference's CPU path (the oracle port: the reference has no CPU matcher of its own),
+    all host threads, on the same workload; each step is a bounded sample."""
+    from oracle import oracle
+    from v3dm import synth
+    if rank != 0:
+        return
+    L, R, lpos, rpos, F, _ = synth.stereo(args.seed, N_SIDE, N_SIDE)
+    sample = 2048
+    for _ in range(args.warmup):
+        cpu_stereo(L, R, lpos, rpos, F, sample)
+    times = []
+    for _ in range(args.steps):
+        dt, frac = cpu_stereo(L, R, lpos, rpos, F, sample)
+        times.append(dt / frac)
+    ms = 1000.0 * statistics.mean(times)
+    v = 1000.0 / ms
+    line = {
+        "impl": "reference", "metric": "image pairs/s (16384x16384 putative + F-guided)", "value": v,
+        "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": stereo_config(args, "cpu"),
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                         "sample": f"{sample} of 16384 lefts x all 16384 rights per step, extrapolated x8"},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def stereo_config(args, where):
+    return {"workload": "stereo pair 16384x16384 uint8 SIFT-like, putative + F-guided (2 px), "
+                        "minScore 0.7, ratio 0.8", "n_left": N_SIDE, "n_right": N_SIDE, "seed": args.seed,
+            "kernel": args.kernel if where == "gpu" else "oracle",
+            "l2": "flushed between steps (512 MiB write on the matcher stream, outside the step events)"}
+
+
+def run_stereo(args, ws, rank, local):
+    import torch
+
+    import v3dm
+    from v3dm import synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L, R, lpos, rpos, F, _ = synth.stereo(args.seed, N_SIDE, N_SIDE)
+    kern = v3dm.KERNEL_TCGEN05 if args.kernel == "tcgen05" else v3dm.KERNEL_SIMT
+    m = v3dm.SIFTMatching(local, kern)
+    m.allocate(N_SIDE, N_SIDE, True)
+    stream = torch.cuda.ExternalStream(m.stream(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    # ---------------- value: inputs resident in HBM ----------------
+    m.set_left_features(L)
+    m.set_right_features(R)
+    d_lpos = torch.from_numpy(lpos).to(dev)
+    d_rpos = torch.from_numpy(rpos).to(dev)
+    d_pairs = torch.empty((N_SIDE, 2), dtype=torch.int32, device=dev)
+    d_pairs2 = torch.empty((N_SIDE, 2), dtype=torch.int32, device=dev)
+    d_cnt = torch.zeros(2, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device():
+        n = 0
+        m.putative_device(MIN_SCORE, MIN_RATIO, d_pairs.data_ptr(), d_cnt.data_ptr())
+        n += m.last_launches()
+        m.guided_F_device(F, GATE_PX, d_lpos.data_ptr(), d_rpos.data_ptr(), MIN_SCORE, MIN_RATIO,
+                          d_pairs2.data_ptr(), d_cnt.data_ptr() + 4)
+        n += m.last_launches()
+        return n
+
+    for _ in range(args.warmup):
+        step_device()
+    m.wait()  # grows the candidate list if the warm-up overflowed it
+    for _ in range(2):
+        step_device()
+    m.wait()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    m.profile(True)
+    clocks = Clocks(local) if rank == 0 or True else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[i][0].record(stream)
+        launches += step_device()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop() if clocks else None
+    m.wait()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    ms = max_over_ranks(ws, statistics.mean(ms_steps), dev)
+    kms, kl = m.profile_read()
+    m.profile(False)
+    k_avg_ms = max_over_ranks(ws, kms / max(kl, 1), dev)
+    n_put = int(d_cnt[0].item())
+    n_gui = int(d_cnt[1].item())
+
+    # ---------------- e2e: host buffers through the C ABI ----------------
+    Lp = torch.from_numpy(L).pin_memory().numpy()
+    Rp = torch.from_numpy(R).pin_memory().numpy()
+    lpp = torch.from_numpy(lpos).pin_memory().numpy()
+    rpp = torch.from_numpy(rpos).pin_memory().numpy()
+
+    def step_host():
+        m.set_left_features(Lp)
+        m.set_right_features(Rp)
+        a = m.find_putative_matches(MIN_SCORE, MIN_RATIO)
+        b = m.run_guided_matching(F, GATE_PX, lpp, rpp, MIN_SCORE, MIN_RATIO)
+        return a.shape[0] + b.shape[0]
+
+    for _ in range(args.warmup):
+        step_host()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    npairs_out = 0
+    barrier(ws)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev2[i][0].record(stream)
+        npairs_out = step_host()
+        ev2[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_e2e = max_over_ranks(ws, statistics.mean([a.elapsed_time(b) for a, b in ev2]), dev)
+    h2d = L.nbytes + R.nbytes + lpos.nbytes + rpos.nbytes
+    d2h = npairs_out * 8 + 2 * 16
+    m.close()
+
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]  # kind::i8 runs at twice the kind::f16 rate
+    ops_per_launch = 2.0 * N_SIDE * N_SIDE * 128
+    achieved = ops_per_launch / (k_avg_ms * 1e-3) / 1e12
+    traffic = traffic_from_profiles("match_tc" if args.kernel == "tcgen05" else "match_simt")
+    line = {
+        "metric": "image pairs/s (16384x16384 putative + F-guided)", "value": ws * 1000.0 / ms, "unit": "pairs/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": stereo_config(args, "gpu"),
+        "int8_tops_per_kernel": achieved,
+        "pairs_found": {"putative": n_put, "guided": n_gui},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",
+                     "frac": achieved / int8_peak, "traffic": traffic,
+                     "peak_src": f"2 x {peaks['src']} bf16 dense ({peaks['bf16_tflops']} TFLOP/s burst)",
+                     "kernel_ms": k_avg_ms, "ops_per_launch": ops_per_launch},
+        "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        dt, frac = cpu_stereo(L, R, lpos, rpos, F, 2048)
+        line["cpu_baseline"] = {"value": frac / dt, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                                "sample": "2048 of 16384 lefts x all 16384 rights, putative + guided, "
+                                          "extrapolated x8"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank)
+        elif args.workload == "stereo":
+            run_stereo(args, ws, rank, local)
+        else:
+            raise SystemExit(f"workload {args.workload} is not wired into this bench yet")
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "v3dm_internal.h"
 
@@ -51,6 +52,10 @@ struct v3dm_matcher {
   TcPlan* tc = nullptr;
   bool tcBound = false;
   int lastLaunches = 0;
+  // Optional CUDA-event timing of the fused matching kernel (v3dm_matcher_profile).
+  bool profile = false;
+  std::vector<cudaEvent_t> evPool;
+  int evUsed = 0;
 };
 
 namespace {
@@ -289,6 +294,7 @@ int v3dm_matcher_destroy(v3dm_matcher* h) {
   cudaStreamSynchronize(h->stream);
   free_buffers(h);
   if (h->tc) tc_plan_destroy(h->tc);
+  for (cudaEvent_t e : h->evPool) cudaEventDestroy(e);
   cudaStreamDestroy(h->stream);
   delete h;
   return V3DM_OK;
@@ -420,6 +426,18 @@ int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPai
   h->lastLaunches = 0;
   V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream));
   if (h->nL > 0 && h->nR > 0 && T <= kMaxScore) {
+    cudaEvent_t evs[2] = {nullptr, nullptr};
+    if (h->profile) {
+      for (int i = 0; i < 2; ++i) {
+        if (h->evUsed == (int)h->evPool.size()) {
+          cudaEvent_t e;
+          V3DM_CUDA_TRY(cudaEventCreate(&e));
+          h->evPool.push_back(e);
+        }
+        evs[i] = h->evPool[h->evUsed++];
+      }
+      V3DM_CUDA_TRY(cudaEventRecord(evs[0], h->stream));
+    }
     if (h->kernel == V3DM_KERNEL_SIMT) {
       V3DM_CUDA_TRY(launch_match_simt(h->dL, h->dR, a, h->stream));
       h->lastLaunches += 1;
@@ -432,6 +450,7 @@ int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPai
       V3DM_CUDA_TRY(launch_match_tc(h->tc, a, h->stream, &nl));
       h->lastLaunches += nl;
     }
+    if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evs[1], h->stream));
     V3DM_CUDA_TRY(launch_seconds(a, h->stream));
     h->lastLaunches += 1;
   }
@@ -585,6 +604,31 @@ int v3dm_matcher_wait(v3dm_matcher* h) {
   }
   int st = read_info(h);
   return st == -1 ? V3DM_ERR_CANDIDATES : st;
+}
+
+int v3dm_matcher_profile(v3dm_matcher* h, int enable) {
+  if (!h) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->profile = enable != 0;
+  h->evUsed = 0;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_profile_read(v3dm_matcher* h, double* msTotal, int* launches) {
+  if (!h || !msTotal || !launches) return V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  double total = 0.0;
+  for (int i = 0; i + 1 < h->evUsed; i += 2) {
+    float ms = 0.f;
+    V3DM_CUDA_TRY(cudaEventElapsedTime(&ms, h->evPool[i], h->evPool[i + 1]));
+    total += ms;
+  }
+  *msTotal = total;
+  *launches = h->evUsed / 2;
+  h->evUsed = 0;
+  return V3DM_OK;
 }
 
 int v3dm_matcher_last_launches(v3dm_matcher* h, int* n) {

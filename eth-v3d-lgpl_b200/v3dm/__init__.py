@@ -72,6 +72,8 @@ def lib() -> C.CDLL:
         L.v3dm_matcher_stream.argtypes = [vp, C.POINTER(vp)]
         L.v3dm_matcher_wait.argtypes = [vp]
         L.v3dm_matcher_last_launches.argtypes = [vp, C.POINTER(i32)]
+        L.v3dm_matcher_profile.argtypes = [vp, i32]
+        L.v3dm_matcher_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i32)]
         L.v3dm_candidate_threshold.argtypes = [f32, f32, i32, C.POINTER(C.c_int32)]
         L.v3dm_voctree_create.argtypes = [C.POINTER(vp), i32, i32, i32]
         L.v3dm_voctree_destroy.argtypes = [vp]
@@ -215,6 +217,15 @@ class SIFTMatching:
         s = C.c_void_p()
         _check(lib().v3dm_matcher_stream(self._h, C.byref(s)), "stream")
         return s.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().v3dm_matcher_profile(self._h, int(enable)), "profile")
+
+    def profile_read(self):
+        """(summed milliseconds, launches) of the fused matching kernel since profile()."""
+        ms, n = C.c_double(0), C.c_int(0)
+        _check(lib().v3dm_matcher_profile_read(self._h, C.byref(ms), C.byref(n)), "profile_read")
+        return ms.value, n.value
 
     def last_launches(self) -> int:
         n = C.c_int(0)

@@ -112,6 +112,10 @@ V3DM_API int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, c
 V3DM_API int v3dm_matcher_wait(v3dm_matcher* h);
 /* The handle's CUDA stream (a cudaStream_t). */
 V3DM_API int v3dm_matcher_stream(v3dm_matcher* h, void** stream);
+/* CUDA-event timing of the fused matching kernel: enable (clears the record), then read
+ * the summed duration in milliseconds and the number of timed launches since. */
+V3DM_API int v3dm_matcher_profile(v3dm_matcher* h, int enable);
+V3DM_API int v3dm_matcher_profile_read(v3dm_matcher* h, double* msTotal, int* launches);
 /* Number of kernels the last matching call launched. */
 V3DM_API int v3dm_matcher_last_launches(v3dm_matcher* h, int* n);
 
