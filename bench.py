@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--tile-config", type=int, default=-1, help="fused-kernel tile configuration (-1: autotune)")
     return ap.parse_args()
 
 
@@ -227,6 +228,11 @@ def run_stereo(args, ws, rank, local):
         n += m.last_launches()
         return n
 
+    if args.tile_config < 0:
+        tuned_cfg, tuned_ms = m.autotune(MIN_SCORE, MIN_RATIO, 3)
+    else:
+        m.set_config(args.tile_config)
+    cfg_id, cfg_rows, cfg_cols = m.config()
     for _ in range(args.warmup):
         step_device()
     m.wait()  # grows the candidate list if the warm-up overflowed it
@@ -251,9 +257,11 @@ def run_stereo(args, ws, rank, local):
     m.wait()
     ms_steps = [a.elapsed_time(b) for a, b in ev]
     ms = max_over_ranks(ws, statistics.mean(ms_steps), dev)
-    kms, kl = m.profile_read()
+    kms, kl = m.profile_read(0)
+    kms_b, kl_b = m.profile_read(1)
     m.profile(False)
     k_avg_ms = max_over_ranks(ws, kms / max(kl, 1), dev)
+    kb_avg_ms = max_over_ranks(ws, kms_b / max(kl_b, 1), dev)
     n_put = int(d_cnt[0].item())
     n_gui = int(d_cnt[1].item())
 
@@ -302,11 +310,15 @@ def run_stereo(args, ws, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
         "config": stereo_config(args, "gpu"),
         "int8_tops_per_kernel": achieved,
+        "tile": {"config": cfg_id, "left_rows": cfg_rows, "right_cols": cfg_cols,
+                 "chosen_by": "autotune" if args.tile_config < 0 else "flag"},
         "pairs_found": {"putative": n_put, "guided": n_gui},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",
                      "frac": achieved / int8_peak, "traffic": traffic,
                      "peak_src": f"2 x {peaks['src']} bf16 dense ({peaks['bf16_tflops']} TFLOP/s burst)",
-                     "kernel_ms": k_avg_ms, "ops_per_launch": ops_per_launch},
+                     "kernel_ms": k_avg_ms, "ops_per_launch": ops_per_launch,
+                     "kernel": "k_side pass A (every left x every right)",
+                     "pass_b_ms": kb_avg_ms},
         "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,

@@ -47,23 +47,42 @@ struct v3dm_matcher {
   float* dRPos = nullptr;
   float4* dGateL = nullptr;       // V3DM_MAX_GATES x nMaxL
   float4* dGateR = nullptr;       // V3DM_MAX_GATES x nMaxR
+  GateParams* dGates = nullptr;   // device copy of gates[]
   int nGates = 0;
   GateParams gates[V3DM_MAX_GATES];
   TcPlan* tc = nullptr;
   bool tcBound = false;
+  TcMaps mapsA, mapsB;            // tensor maps of the two side passes
+  uint8_t* dRc = nullptr;         // descriptors of the chosen rights (second side pass)
+  int32_t* dLeftDec = nullptr;    // per left: accepted right or -1
+  int32_t* dRightDec = nullptr;   // per right: accepted left or -1
+  int* dChosenFlag = nullptr;     // per right: chosen by some left (cleared after each call)
+  int* dChosenList = nullptr;
+  int* dFlagA = nullptr;          // lefts to re-score exactly
+  int* dFlagB = nullptr;          // rights to re-score exactly
+  int* dCounters = nullptr;       // [0] chosen rights, [1] flagged lefts, [2] flagged rights
   int lastLaunches = 0;
   // Optional CUDA-event timing of the fused matching kernel (v3dm_matcher_profile).
   bool profile = false;
   std::vector<cudaEvent_t> evPool;
+  std::vector<int> evTag;         // per event pair: 0 = main kernel (SIMT, or tcgen05 pass A), 1 = pass B
   int evUsed = 0;
 };
 
 namespace {
 
-#define V3DM_CUDA_TRY(expr)                      \
-  do {                                           \
-    cudaError_t e_ = (expr);                     \
-    if (e_ != cudaSuccess) return V3DM_ERR_CUDA; \
+thread_local char g_lastError[256] = "";
+
+int cuda_fail(cudaError_t e, const char* what, int line) {
+  std::snprintf(g_lastError, sizeof(g_lastError), "%s (%s) at v3dm_api.cu:%d: %s", cudaGetErrorName(e),
+                cudaGetErrorString(e), line, what);
+  return V3DM_ERR_CUDA;
+}
+
+#define V3DM_CUDA_TRY(expr)                                      \
+  do {                                                           \
+    cudaError_t e_ = (expr);                                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr, __LINE__); \
   } while (0)
 
 template <class T>
@@ -96,6 +115,15 @@ void free_buffers(v3dm_matcher* h) {
   dfree(h->dRPos);
   dfree(h->dGateL);
   dfree(h->dGateR);
+  dfree(h->dGates);
+  dfree(h->dRc);
+  dfree(h->dLeftDec);
+  dfree(h->dRightDec);
+  dfree(h->dChosenFlag);
+  dfree(h->dChosenList);
+  dfree(h->dFlagA);
+  dfree(h->dFlagB);
+  dfree(h->dCounters);
   if (h->hInfo) cudaFreeHost(h->hInfo);
   h->hInfo = nullptr;
   h->allocated = false;
@@ -164,8 +192,9 @@ ThrKey g_thrKeys[16];
 int32_t g_thrVals[16];
 int g_thrN = 0, g_thrNext = 0;
 
-int compute_threshold(float minScore, float minRatio, bool gated, int32_t* Tout) {
-  // Smin: smallest S with score(S) > minScore (kMaxScore + 1 when none).
+// Smallest S with score(S) > minScore: no best below it can pass the min-score test
+// (kMaxScore + 1 when none can).
+int32_t smallest_passing_score(float minScore) {
   int32_t Smin;
   if (!(minScore == minScore)) {
     Smin = kMaxScore + 1;  // NaN: 's1 > minScore' is never true
@@ -177,6 +206,11 @@ int compute_threshold(float minScore, float minRatio, bool gated, int32_t* Tout)
     while (Smin > 0 && score_of(Smin - 1) > minScore) --Smin;
     while (Smin <= kMaxScore && !(score_of(Smin) > minScore)) ++Smin;
   }
+  return Smin;
+}
+
+int compute_threshold(float minScore, float minRatio, bool gated, int32_t* Tout) {
+  const int32_t Smin = smallest_passing_score(minScore);
   if (Smin > kMaxScore || minRatio < 0.0f || !(minRatio == minRatio)) {
     // Nothing can pass, or no ratio test, or a NaN ratio (never accepted): only the best
     // value matters and it cannot pass below Smin.
@@ -257,6 +291,8 @@ const char* v3dm_status_string(int s) {
   }
 }
 
+const char* v3dm_last_error(void) { return g_lastError; }
+
 int v3dm_candidate_threshold(float minScore, float minRatio, int gated, int32_t* T) {
   if (!T) return V3DM_ERR_ARG;
   return host_candidate_threshold(minScore, minRatio, gated != 0, T);
@@ -323,15 +359,25 @@ int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
   if (ok && h->guidedAlloc)
     ok = dalloc(&h->dLPos, 2 * (size_t)nMaxL + 2) == cudaSuccess && dalloc(&h->dRPos, 2 * (size_t)nMaxR + 2) == cudaSuccess &&
          dalloc(&h->dGateL, (size_t)V3DM_MAX_GATES * nMaxL + 1) == cudaSuccess &&
-         dalloc(&h->dGateR, (size_t)V3DM_MAX_GATES * nMaxR + 1) == cudaSuccess;
-  if (ok) {
-    // Candidate list: about 1e-3 of all scores exceed T on SIFT-like data; start with room
-    // for 1/256 of them and grow when a call reports an overflow.
-    int nSeg = h->kernel == V3DM_KERNEL_SIMT ? 1 : tc_segments(h->tc);
-    long long total = (long long)nMaxL * (long long)nMaxR / 256;
-    long long segCap = total / nSeg + 1;
+         dalloc(&h->dGateR, (size_t)V3DM_MAX_GATES * nMaxR + 1) == cudaSuccess &&
+         dalloc(&h->dGates, (size_t)V3DM_MAX_GATES) == cudaSuccess;
+  if (ok && h->kernel == V3DM_KERNEL_SIMT) {
+    // SIMT path: one candidate list; about 1e-3 of all scores exceed T on SIFT-like data.
+    // Start with room for 1/256 of them and grow when a call reports an overflow.
+    long long segCap = (long long)nMaxL * (long long)nMaxR / 256 + 1;
     if (segCap < 4096) segCap = 4096;
-    ok = alloc_candidates(h, nSeg, segCap) == cudaSuccess;
+    ok = alloc_candidates(h, 1, segCap) == cudaSuccess;
+  } else if (ok) {
+    // tcgen05 path: one list segment per epilogue warp, holding that warp's unit bests.
+    ok = alloc_candidates(h, tc_segments(h->tc), 2048) == cudaSuccess &&
+         dalloc(&h->dRc, rowsR * kDescBytes) == cudaSuccess && dalloc(&h->dLeftDec, (size_t)nMaxL + 1) == cudaSuccess &&
+         dalloc(&h->dRightDec, (size_t)nMaxR + 1) == cudaSuccess &&
+         dalloc(&h->dChosenFlag, (size_t)nMaxR + 1) == cudaSuccess &&
+         dalloc(&h->dChosenList, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dFlagA, (size_t)nMaxL + 1) == cudaSuccess &&
+         dalloc(&h->dFlagB, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dCounters, 4) == cudaSuccess;
+    if (ok)
+      ok = cudaMemsetAsync(h->dChosenFlag, 0, ((size_t)nMaxR + 1) * sizeof(int), h->stream) == cudaSuccess &&
+           cudaMemsetAsync(h->dRc, 0, rowsR * kDescBytes, h->stream) == cudaSuccess;
   }
   if (ok) {
     ok = cudaMemsetAsync(h->dLBest, 0, ((size_t)nMaxL + 1) * 8, h->stream) == cudaSuccess &&
@@ -401,9 +447,23 @@ int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
   return V3DM_OK;
 }
 
-// Enqueues the fused matching kernel, the seconds pass and the finalize kernel for the
-// current gates.  The result lands in dPairs / dInfo on the handle's stream.
-int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
+// Next pair of timing events (created on first use) tagged 'tag'.
+int event_pair(v3dm_matcher* h, int tag, cudaEvent_t* ev) {
+  for (int i = 0; i < 2; ++i) {
+    if (h->evUsed == (int)h->evPool.size()) {
+      cudaEvent_t e;
+      V3DM_CUDA_TRY(cudaEventCreate(&e));
+      h->evPool.push_back(e);
+      h->evTag.push_back(0);
+    }
+    h->evTag[h->evUsed] = tag;
+    ev[i] = h->evPool[h->evUsed++];
+  }
+  return V3DM_OK;
+}
+
+// SIMT path: candidate kernel, seconds pass, finalize.
+int enqueue_match_simt(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
   int32_t T = 0;
   int st = host_candidate_threshold(minScore, minRatio, h->nGates > 0, &T);
   if (st != V3DM_OK) return st;
@@ -423,41 +483,166 @@ int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPai
   a.err = h->dInfo + kInfoErr;
   a.nGates = h->nGates;
   for (int i = 0; i < h->nGates; ++i) a.gates[i] = h->gates[i];
-  h->lastLaunches = 0;
-  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream));
+  a.gatesDev = h->dGates;
   if (h->nL > 0 && h->nR > 0 && T <= kMaxScore) {
-    cudaEvent_t evs[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2];
     if (h->profile) {
-      for (int i = 0; i < 2; ++i) {
-        if (h->evUsed == (int)h->evPool.size()) {
-          cudaEvent_t e;
-          V3DM_CUDA_TRY(cudaEventCreate(&e));
-          h->evPool.push_back(e);
-        }
-        evs[i] = h->evPool[h->evUsed++];
-      }
-      V3DM_CUDA_TRY(cudaEventRecord(evs[0], h->stream));
+      int e = event_pair(h, 0, ev);
+      if (e != V3DM_OK) return e;
+      V3DM_CUDA_TRY(cudaEventRecord(ev[0], h->stream));
     }
-    if (h->kernel == V3DM_KERNEL_SIMT) {
-      V3DM_CUDA_TRY(launch_match_simt(h->dL, h->dR, a, h->stream));
-      h->lastLaunches += 1;
-    } else {
-      if (!h->tcBound) {
-        V3DM_CUDA_TRY(tc_plan_bind(h->tc, h->dL, h->nL, h->dR, h->nR));
-        h->tcBound = true;
-      }
-      int nl = 0;
-      V3DM_CUDA_TRY(launch_match_tc(h->tc, a, h->stream, &nl));
-      h->lastLaunches += nl;
-    }
-    if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evs[1], h->stream));
+    V3DM_CUDA_TRY(launch_match_simt(h->dL, h->dR, a, h->stream));
+    if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(ev[1], h->stream));
     V3DM_CUDA_TRY(launch_seconds(a, h->stream));
-    h->lastLaunches += 1;
+    h->lastLaunches += 2;
   }
   V3DM_CUDA_TRY(launch_finalize(a, minScore, minRatio, h->dScratch, dPairs, h->dInfo, h->stream));
   h->lastLaunches += 1;
-  h->pendingCheck = true;
   return V3DM_OK;
+}
+
+// tcgen05 path: side pass lefts x rights, decisions of the lefts, the chosen rights, side
+// pass chosen rights x lefts, their decisions, mutual filter.
+int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
+  const int32_t Smin = smallest_passing_score(minScore);
+  const bool gated = h->nGates > 0;
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dCounters, 0, 4 * sizeof(int), h->stream));
+  const int cfg = tc_get_config(h->tc);
+  if (!h->tcBound || h->mapsA.cfg != cfg) {
+    V3DM_CUDA_TRY(tc_side_maps(h->tc, &h->mapsA, h->dL, h->nL, h->dR, h->nR));
+    V3DM_CUDA_TRY(tc_side_maps(h->tc, &h->mapsB, h->dRc, h->nR, h->dL, h->nL));
+    h->tcBound = true;
+  }
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.Smin = Smin;
+  sa.list = h->dCand;
+  sa.segCount = h->dSegCount;
+  sa.segCap = h->segCap;
+  sa.nSeg = h->nSeg;
+  sa.err = h->dInfo + kInfoErr;
+  sa.nGates = h->nGates;
+  sa.gatesDev = h->dGates;
+  PostArgs pa;
+  std::memset(&pa, 0, sizeof(pa));
+  pa.list = h->dCand;
+  pa.segCount = h->dSegCount;
+  pa.segCap = h->segCap;
+  pa.nSeg = h->nSeg;
+  pa.minScore = minScore;
+  pa.minRatio = minRatio;
+  pa.gated = gated;
+  pa.err = h->dInfo + kInfoErr;
+  RescoreArgs ra;
+  std::memset(&ra, 0, sizeof(ra));
+  if (gated) {
+    int st = host_candidate_threshold(minScore, minRatio, true, &ra.T);
+    if (st != V3DM_OK) return st;
+  }
+  ra.nGates = h->nGates;
+  ra.gatesDev = h->dGates;
+  ra.minScore = minScore;
+  ra.minRatio = minRatio;
+  cudaEvent_t evA[2], evB[2];
+  // pass A: every left against every right
+  sa.nA = h->nL;
+  sa.nB = h->nR;
+  sa.aIsLeft = 1;
+  sa.best = h->dLBest;
+  sa.sec = h->dLSec;
+  if (h->profile) {
+    int e = event_pair(h, 0, evA);
+    if (e != V3DM_OK) return e;
+    V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
+  }
+  V3DM_CUDA_TRY(launch_side(h->tc, h->mapsA, sa, h->stream));
+  if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
+  pa.nRows = h->nL;
+  pa.best = h->dLBest;
+  pa.sec = h->dLSec;
+  pa.decision = h->dLeftDec;
+  pa.flagged = h->dFlagA;
+  pa.flaggedCount = h->dCounters + 1;
+  V3DM_CUDA_TRY(launch_post(pa, h->stream));
+  h->lastLaunches += 3;
+  if (gated) {
+    ra.descA = h->dL;
+    ra.descB = h->dR;
+    ra.nB = h->nR;
+    ra.aIsLeft = 1;
+    ra.flagged = h->dFlagA;
+    ra.flaggedCount = h->dCounters + 1;
+    ra.best = h->dLBest;
+    ra.sec = h->dLSec;
+    ra.decision = h->dLeftDec;
+    V3DM_CUDA_TRY(launch_rescore(ra, 64, h->stream));
+    h->lastLaunches += 1;
+  }
+  V3DM_CUDA_TRY(launch_choose(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dR, h->dRc,
+                              h->stream));
+  h->lastLaunches += 1;
+  // pass B: the chosen rights against every left
+  sa.nAptr = h->dCounters;
+  sa.nA = h->nR;
+  sa.nB = h->nL;
+  sa.amap = h->dChosenList;
+  sa.aIsLeft = 0;
+  sa.best = h->dRBest;
+  sa.sec = h->dRSec;
+  if (h->profile) {
+    int e = event_pair(h, 1, evB);
+    if (e != V3DM_OK) return e;
+    V3DM_CUDA_TRY(cudaEventRecord(evB[0], h->stream));
+  }
+  V3DM_CUDA_TRY(launch_side(h->tc, h->mapsB, sa, h->stream));
+  if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evB[1], h->stream));
+  pa.nRows = h->nR;
+  pa.rowsPtr = h->dCounters;
+  pa.amap = h->dChosenList;
+  pa.best = h->dRBest;
+  pa.sec = h->dRSec;
+  pa.decision = h->dRightDec;
+  pa.flagged = h->dFlagB;
+  pa.flaggedCount = h->dCounters + 2;
+  V3DM_CUDA_TRY(launch_post(pa, h->stream));
+  h->lastLaunches += 3;
+  if (gated) {
+    ra.descA = h->dR;
+    ra.descB = h->dL;
+    ra.nB = h->nL;
+    ra.aIsLeft = 0;
+    ra.flagged = h->dFlagB;
+    ra.flaggedCount = h->dCounters + 2;
+    ra.best = h->dRBest;
+    ra.sec = h->dRSec;
+    ra.decision = h->dRightDec;
+    V3DM_CUDA_TRY(launch_rescore(ra, 64, h->stream));
+    h->lastLaunches += 1;
+  }
+  V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
+                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->stream));
+  h->lastLaunches += 2;
+  return V3DM_OK;
+}
+
+// Enqueues one matching call for the current gates; the result lands in dPairs / dInfo on
+// the handle's stream.
+int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
+  h->lastLaunches = 0;
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream));
+  if (h->nGates > 0)
+    V3DM_CUDA_TRY(cudaMemcpyAsync(h->dGates, h->gates, sizeof(GateParams) * h->nGates, cudaMemcpyHostToDevice,
+                                  h->stream));
+  int st;
+  if (h->nL == 0 || h->nR == 0) {
+    st = V3DM_OK;  // no pairs: the info block already says so
+  } else if (h->kernel == V3DM_KERNEL_SIMT) {
+    st = enqueue_match_simt(h, minScore, minRatio, dPairs);
+  } else {
+    st = enqueue_match_tc(h, minScore, minRatio, dPairs);
+  }
+  if (st == V3DM_OK) h->pendingCheck = true;
+  return st;
 }
 
 // Reads the info block of the last call.  Returns V3DM_OK, an error, or -1 when the
@@ -616,18 +801,110 @@ int v3dm_matcher_profile(v3dm_matcher* h, int enable) {
 }
 
 int v3dm_matcher_profile_read(v3dm_matcher* h, double* msTotal, int* launches) {
-  if (!h || !msTotal || !launches) return V3DM_ERR_ARG;
+  return v3dm_matcher_profile_read_pass(h, 0, msTotal, launches);
+}
+
+int v3dm_matcher_profile_read_pass(v3dm_matcher* h, int pass, double* msTotal, int* launches) {
+  if (!h || !msTotal || !launches || pass < 0 || pass > 1) return V3DM_ERR_ARG;
   DeviceGuard g(h->device);
   V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   double total = 0.0;
+  int n = 0;
   for (int i = 0; i + 1 < h->evUsed; i += 2) {
+    if (h->evTag[i] != pass) continue;
     float ms = 0.f;
     V3DM_CUDA_TRY(cudaEventElapsedTime(&ms, h->evPool[i], h->evPool[i + 1]));
     total += ms;
+    ++n;
   }
   *msTotal = total;
-  *launches = h->evUsed / 2;
-  h->evUsed = 0;
+  *launches = n;
+  if (pass == 1 || !h->profile) h->evUsed = 0;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_num_configs(v3dm_matcher* h, int* n) {
+  if (!h || !n) return V3DM_ERR_ARG;
+  *n = h->kernel == V3DM_KERNEL_SIMT ? 1 : tc_num_configs();
+  return V3DM_OK;
+}
+
+int v3dm_matcher_get_config(v3dm_matcher* h, int* cfg, int* rowsPerGroup, int* colsPerTile) {
+  if (!h || !cfg) return V3DM_ERR_ARG;
+  if (h->kernel == V3DM_KERNEL_SIMT) {
+    *cfg = 0;
+    if (rowsPerGroup) *rowsPerGroup = 64;
+    if (colsPerTile) *colsPerTile = 64;
+    return V3DM_OK;
+  }
+  *cfg = tc_get_config(h->tc);
+  int r = 0, c = 0;
+  tc_config_shape(*cfg, &r, &c);
+  if (rowsPerGroup) *rowsPerGroup = r;
+  if (colsPerTile) *colsPerTile = c;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_set_config(v3dm_matcher* h, int cfg) {
+  if (!h) return V3DM_ERR_ARG;
+  if (h->kernel == V3DM_KERNEL_SIMT) return cfg == 0 ? V3DM_OK : V3DM_ERR_ARG;
+  DeviceGuard g(h->device);
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (tc_set_config(h->tc, cfg) != cudaSuccess) return V3DM_ERR_ARG;
+  return V3DM_OK;
+}
+
+int v3dm_matcher_autotune(v3dm_matcher* h, float minScore, float minRatio, int reps, int* best, double* msBest) {
+  if (!h || reps < 1) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  DeviceGuard g(h->device);
+  int n = h->kernel == V3DM_KERNEL_SIMT ? 1 : tc_num_configs();
+  int keepGates = h->nGates;
+  int bestCfg = 0;
+  double bestMs = 1e300;
+  for (int c = 0; c < n; ++c) {
+    if (h->kernel != V3DM_KERNEL_SIMT && tc_set_config(h->tc, c) != cudaSuccess) continue;
+    h->nGates = 0;
+    int st = run_host(h, minScore, minRatio, nullptr, 0, nullptr);  // warm-up, grows the list if needed
+    if (st != V3DM_OK && st != V3DM_ERR_CAPACITY) {
+      h->nGates = keepGates;
+      return st;
+    }
+    bool prof = h->profile;
+    h->profile = true;
+    h->evUsed = 0;
+    for (int r = 0; r < reps; ++r) {
+      st = enqueue_match(h, minScore, minRatio, h->dPairs);
+      if (st != V3DM_OK) {
+        h->profile = prof;
+        h->nGates = keepGates;
+        return st;
+      }
+    }
+    V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    double total = 0.0;
+    for (int i = 0; i + 1 < h->evUsed; i += 2) {
+      float ms = 0.f;
+      V3DM_CUDA_TRY(cudaEventElapsedTime(&ms, h->evPool[i], h->evPool[i + 1]));
+      total += ms;
+    }
+    h->evUsed = 0;
+    h->profile = prof;
+    st = read_info(h);
+    if (st != V3DM_OK && st != -1) {
+      h->nGates = keepGates;
+      return st;
+    }
+    double avg = total / reps;
+    if (avg < bestMs) {
+      bestMs = avg;
+      bestCfg = c;
+    }
+  }
+  h->nGates = keepGates;
+  if (h->kernel != V3DM_KERNEL_SIMT) tc_set_config(h->tc, bestCfg);
+  if (best) *best = bestCfg;
+  if (msBest) *msBest = bestMs;
   return V3DM_OK;
 }
 

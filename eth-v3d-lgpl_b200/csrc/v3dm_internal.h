@@ -1,9 +1,10 @@
 // v3dm_internal.h -- host-side structures shared by the library's translation units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/v3dm.h"
+#include "v3dm.h"
 #include "v3dm_common.cuh"
 
 namespace v3dm {
@@ -33,6 +34,7 @@ struct MatchArgs {
   int* err;
   int nGates;
   GateParams gates[V3DM_MAX_GATES];
+  const GateParams* gatesDev;      // device copy of gates[] (kernels index it at run time)
 };
 
 // Kernel launchers (v3dm_match.cu, v3dm_match_tc.cu).
@@ -44,15 +46,85 @@ cudaError_t launch_gate_precompute(int type, const double* m, const float* dLPos
                                    int nR, float4* lv, float4* rv, cudaStream_t s);
 cudaError_t launch_f32_to_u8(const float* src, uint8_t* dst, int n, int* err, cudaStream_t s);
 
-// tcgen05 path: per-matcher prepared operand maps (opaque, v3dm_match_tc.cu).
+// ---- tcgen05 path (v3dm_match_tc.cu, v3dm_pair.cu) ------------------------------------
+// One side pass scores the nA descriptors of side A against the nB descriptors of side B.
+struct SideArgs {
+  const int* nAptr;              // device count of A rows (null: use nA)
+  int nA;                        // A rows (upper bound when nAptr is set)
+  int nB;                        // B rows
+  int32_t Smin;                  // smallest score that can pass the min-score test
+  const int* amap;               // A row -> index on its side (null: identity)
+  int aIsLeft;                   // 1: A = lefts, B = rights; 0: A = rights, B = lefts
+  unsigned long long* best;      // per A index: best key over B (atomicMax)
+  unsigned int* sec;             // per A index: second score + 1 (exact, or a bound with gates)
+  unsigned long long* list;      // per-warp segments of (A index, unit best key) entries
+  int* segCount;
+  long long segCap;
+  int nSeg;
+  int* err;
+  int nGates;
+  const GateParams* gatesDev;    // device array of the call's gates
+};
+
 struct TcPlan;
+struct TcMaps {
+  CUtensorMap a, b;
+  int cfg;
+};
 cudaError_t tc_plan_create(TcPlan** p, int device);
 void tc_plan_destroy(TcPlan* p);
-// Rebuilds the operand tensor maps when the buffers or counts change.
-cudaError_t tc_plan_bind(TcPlan* p, const uint8_t* dL, int nL, const uint8_t* dR, int nR);
-// Number of candidate-list segments the tcgen05 kernel uses (one per CTA).
+int tc_num_configs();
+int tc_get_config(TcPlan* p);
+cudaError_t tc_set_config(TcPlan* p, int cfg);
+void tc_config_shape(int cfg, int* rowsPerGroup, int* colsPerTile);
+// Number of list segments a side pass uses (one per epilogue warp of a full grid).
 int tc_segments(TcPlan* p);
-cudaError_t launch_match_tc(TcPlan* p, const MatchArgs& a, cudaStream_t s, int* launches);
+// Tensor maps of a side pass for the plan's current configuration.
+cudaError_t tc_side_maps(TcPlan* p, TcMaps* m, const uint8_t* dA, int rowsA, const uint8_t* dB, int rowsB);
+cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st);
+
+// Decision and bookkeeping kernels around the side passes (v3dm_pair.cu).
+struct PostArgs {
+  int nRows;                     // rows of the pass (A side); with rowsPtr the device count
+  const int* rowsPtr;
+  const int* amap;               // row -> index (null: identity)
+  unsigned long long* best;
+  unsigned int* sec;
+  const unsigned long long* list;
+  int* segCount;                 // read, then cleared
+  long long segCap;
+  int nSeg;
+  float minScore, minRatio;
+  int gated;
+  int32_t* decision;             // per index: accepted partner or -1
+  int* flagged;                  // indices whose decision needs an exact re-score
+  int* flaggedCount;
+  int* err;
+};
+cudaError_t launch_post(const PostArgs& a, cudaStream_t s);
+// Exact re-score of the flagged descriptors of side A against side B.
+struct RescoreArgs {
+  const uint8_t* descA;          // side A descriptors by index
+  const uint8_t* descB;
+  int nB;
+  int aIsLeft;
+  int nGates;
+  const GateParams* gatesDev;
+  float minScore, minRatio;
+  int32_t T;                     // candidate threshold: scores below it cannot change a decision
+  const int* flagged;
+  const int* flaggedCount;
+  unsigned long long* best;
+  unsigned int* sec;
+  int32_t* decision;
+};
+cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s);
+// Rights accepted by some left: de-duplicated list, their descriptors gathered into dRc.
+cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                          const uint8_t* dR, uint8_t* dRc, cudaStream_t s);
+// Mutual filter and ordered compaction (blockCount: nL/2048 + 1 ints of scratch); clears chosenFlag.
+cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,
+                          int2* pairs, int32_t* info, cudaStream_t s);
 
 // Candidate threshold (v3dm_api.cu).
 int host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T);

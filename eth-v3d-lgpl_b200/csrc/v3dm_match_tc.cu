@@ -1,20 +1,37 @@
-// v3dm_match_tc.cu -- tcgen05 matching kernel for sm_100a.
+// v3dm_match_tc.cu -- tcgen05 side kernel for sm_100a: one persistent launch scores one side
+// of a pair against the other and keeps, for every descriptor of the A side, its best
+// candidate and an upper bound of its second-best score.  Two launches (lefts x rights,
+// then the chosen rights x lefts) replace cublasSgemm + the four maxima kernels of the
+// reference (v3d_cudamatching.cu:529-545); no score leaves the SM.
 //
-// Replaces cublasSgemm + the four maxima kernels of the reference
-// (v3d_cudamatching.cu:529-545) with one persistent kernel whose score tiles never leave
-// the SM:
-//   warp 0      TMA producer: left tile A (128 descriptors x 128 bytes) once per work unit,
-//               right tiles B (256 x 128 bytes) through a 4-stage ring, 128-byte swizzle;
+//   warp 0      TMA producer: an A group (NB blocks of 128 descriptors x 128 bytes) whenever
+//               the group changes, B tiles (BN x 128 bytes) through a ring of shared-memory
+//               stages, 128-byte swizzle;
 //   warp 1      allocates 512 TMEM columns and issues tcgen05.mma.kind::i8 (u8 x u8 -> s32,
-//               M=128, N=256, four K=32 steps per tile) into two 256-column accumulators;
-//   warps 2-9   epilogue: tcgen05.ld 32x32b.x32 chunks, per-lane maximum of 32 scores, and
-//               only when a score reaches the candidate threshold T (rare) the exact
-//               per-element path: guided gates, atomicMax of both best keys, candidate
-//               list append (shared-memory counter, per-CTA list segment).
-// A work unit is (left block of 128 rows, range of right tiles); units are dealt to CTAs
-// round-robin, every role walks the same sequence, and mbarriers order the hand-offs.
-// Every mbarrier wait is bounded: on timeout the CTA raises kErrWaitTimeout, drains its
-// own TMA loads and MMAs, frees TMEM and returns.
+//               M=128, N=BN, four K=32 steps per block) into 512/(NB*BN) accumulator stages;
+//   warps 2-17  epilogue, four per TMEM lane quadrant.  Lane i of a warp owns A descriptor
+//               'row' and reads its scores with tcgen05.ld (32 columns per chunk), hands the
+//               stage back, and per chunk does one of two things:
+//                 - all scores below Smin (the smallest score that can pass the min-score
+//                   test): W = max(W, chunk maximum + 1)                     (one op);
+//                 - some score >= Smin (true matches, ~1e-6 of unrelated pairs): an exact
+//                   lane-local pass over the chunk: guided gates for every score >= Smin,
+//                   chunk best (largest score, first index on ties, the reference's argMax
+//                   rule, v3d_cudamatching.cu:145) and the maximum of all other scores.
+//               At the end of a work unit the lane's best key goes to best[] (atomicMax) and
+//               a candidate-list entry, its W to sec[] (atomicMax).
+// Resulting per-descriptor values (after the list pass in v3dm_pair.cu): best = the exact
+// best over scores >= Smin that pass the gates; sec = the exact second-best score without
+// gates, an upper bound of it with gates (masked scores are counted).  The decision
+// accept(best, s2) is monotone in s2, so when accept(best, sec) == accept(best, none) the
+// decision is exact; otherwise the descriptor is re-scored exactly (rare).
+// The tile shape (NB, BN) and the stage counts are template parameters chosen at run time
+// (TcConfig).  NB=2 keeps 256 A rows resident and halves the B bytes per MMA compared with one
+// 128-row block; more TMEM stages hide the MMA -> epilogue -> MMA hand-off latency.
+// The work is the flattened sequence (A group, B tile); each CTA takes one contiguous range
+// of it.  Every role walks the same range; mbarriers order the hand-offs.  Every mbarrier wait
+// is bounded: on timeout the CTA raises kErrWaitTimeout, drains its own TMA loads and MMAs,
+// frees TMEM and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -27,31 +44,46 @@ namespace v3dm {
 
 namespace {
 
-constexpr int BM = 128;          // lefts per tile (TMEM lanes)
-constexpr int BN = 256;          // rights per tile (TMEM columns per accumulator)
-constexpr int kStages = 4;       // right-tile ring
-constexpr int kEpiWarps = 8;     // two per TMEM lane quadrant, each owning 128 columns
+constexpr int BM = 128;          // rows per MMA block (TMEM lanes)
+constexpr int kEpiWarps = 16;    // four per TMEM lane quadrant
 constexpr int kThreads = (2 + kEpiWarps) * 32;
-constexpr int kABytes = BM * kDescBytes;  // 16 KB
-constexpr int kBBytes = BN * kDescBytes;  // 32 KB
 constexpr int kTmemCols = 512;
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 
+template <int NB_, int BN_, int STAGES_>
+struct TcCfg {
+  static constexpr int NB = NB_;                 // 128-row MMA blocks per left group
+  static constexpr int BN = BN_;                 // rights per tile
+  static constexpr int kStages = STAGES_;        // right-tile ring depth
+  static constexpr int GM = BM * NB;             // left rows per group
+  static constexpr int kABytes = GM * kDescBytes;
+  static constexpr int kBBytes = BN * kDescBytes;
+  static constexpr int kAccCols = NB * BN;       // TMEM columns per accumulator stage
+  static constexpr int kAcc = kTmemCols / kAccCols;  // accumulator stages
+  // Epilogue split: the four warps of a lane quadrant own (block, column quarter or half):
+  // with NB == 2 a warp owns one block and half of the BN columns, with NB == 1 a quarter.
+  static constexpr int kWarpCols = NB == 2 ? BN / 2 : BN / 4;
+  static constexpr int kChunks = kWarpCols / 32;
+  static_assert(NB == 1 || NB == 2, "one or two blocks per group");
+  static_assert(kWarpCols >= 32 && kWarpCols % 32 == 0 && kChunks <= 2 && BN <= 256, "1..2 chunks per warp");
+  static_assert(kAcc >= 2, "at least two accumulator stages");
+};
+
+template <class C>
 struct Smem {
-  uint8_t a[2][kABytes];
-  uint8_t b[kStages][kBBytes];
-  unsigned long long fullB[kStages], emptyB[kStages];
+  uint8_t a[2][C::kABytes];
+  uint8_t b[C::kStages][C::kBBytes];
+  unsigned long long fullB[C::kStages], emptyB[C::kStages];
   unsigned long long fullA[2], emptyA[2];
-  unsigned long long accFull[2], accEmpty[2];
+  unsigned long long accFull[C::kAcc], accEmpty[C::kAcc];
   unsigned long long mmaDone;
   uint32_t tmemBase;
-  int candCount;
   int abort;
 };
-constexpr size_t kSmemBytes = sizeof(Smem) + 1024;  // + alignment slack
 
 struct TcShape {
-  int nLB, nRT, nSplit, nUnits;
+  int nGroups, nTiles;  // left groups, right tiles
+  long long nWork;      // nGroups * nTiles
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -84,15 +116,15 @@ __device__ __forceinline__ bool mbar_try(unsigned long long* b, uint32_t parity)
 
 // Bounded wait for the phase with the given parity.  Returns false on timeout or when
 // another role of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, Smem& s, int* err) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, int* abortFlag, int* err) {
   if (mbar_try(b, parity)) return true;
   long long t0 = clock64();
   while (true) {
     if (mbar_try(b, parity)) return true;
-    if (*reinterpret_cast<volatile int*>(&s.abort)) return false;
+    if (*reinterpret_cast<volatile int*>(abortFlag)) return false;
     if (clock64() - t0 > kWaitCycles) {
       atomicOr(err, kErrWaitTimeout);
-      *reinterpret_cast<volatile int*>(&s.abort) = 1;
+      *reinterpret_cast<volatile int*>(abortFlag) = 1;
       return false;
     }
   }
@@ -113,16 +145,19 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
          (2ull << 61);
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = unsigned 8-bit, both K-major,
-// N = 256, M = 128.
-constexpr uint32_t kIdesc = (2u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: kind::i8, D = s32, A = B = unsigned 8-bit, both K-major, N, M = 128.
+template <int N>
+__device__ __forceinline__ constexpr uint32_t idesc() {
+  return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
+template <int N>
 __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
-      "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate)
+      "l"(ad), "l"(bd), "r"(idesc<N>()), "r"(accumulate)
       : "memory");
 }
 
@@ -134,8 +169,9 @@ __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 32 lanes x 32 consecutive 32-bit columns; thread i receives lane (base + i).
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// Issues a load of 32 lanes x 32 consecutive 32-bit columns; thread i receives lane
+// (base + i).  The registers are valid only after tmem_wait().
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -145,9 +181,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
         "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_wait(uint32_t (&v)[N]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 32; ++i) asm volatile("" : "+r"(v[i]));  // uses stay after the wait
+  for (int i = 0; i < N; ++i) asm volatile("" : "+r"(v[i]));  // uses stay after the wait
 }
 
 // Maximum of three non-negative int32 scores through the three-input f32 max: a
@@ -159,40 +199,129 @@ __device__ __forceinline__ uint32_t max3_bits(uint32_t a, uint32_t b, uint32_t c
   return __float_as_uint(r);
 }
 
-__device__ __forceinline__ void unit_coords(const TcShape& sh, int u, int& lb, int& t0, int& t1) {
-  lb = u / sh.nSplit;
-  int sp = u - lb * sh.nSplit;
-  t0 = (int)((long long)sp * sh.nRT / sh.nSplit);
-  t1 = (int)((long long)(sp + 1) * sh.nRT / sh.nSplit);
+// Maximum of 32 scores: a balanced tree of two-input integer maxima (ALU pipe, short
+// latency, 16-way parallel at the first level).
+__device__ __forceinline__ uint32_t max32_bits(const uint32_t* v) {
+  uint32_t m[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) m[i] = max(v[i], v[i + 16]);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) m[i] = max(m[i], m[i + 8]);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) m[i] = max(m[i], m[i + 4]);
+  return max(max(m[0], m[2]), max(m[1], m[3]));
 }
 
-__device__ __noinline__ void candidate(const MatchArgs& a, Smem& s, int l, int r, int32_t S) {
-  if (a.nGates && gated_out(a, l, r)) return;
-  record_best(a, l, r, S);
-  int idx = atomicAdd(&s.candCount, 1);
-  if (idx < a.segCap) a.cand[(long long)blockIdx.x * a.segCap + idx] = cand_pack(l, r, S);
+// Work range of this CTA in the flattened (group, tile) sequence.
+__device__ __forceinline__ void cta_range(const TcShape& sh, long long& w0, long long& w1) {
+  w0 = sh.nWork * blockIdx.x / gridDim.x;
+  w1 = sh.nWork * (blockIdx.x + 1) / gridDim.x;
 }
 
+// Walks (group, tile) pairs of a work range with one division at the start: the per-tile
+// loops of the MMA issuer and the epilogue stay free of 64-bit divisions.
+struct WorkCursor {
+  int g, t, nTiles;
+  long long left;
+  __device__ __forceinline__ WorkCursor(long long w0, long long w1, int nT) : nTiles(nT), left(w1 - w0) {
+    g = (int)(w0 / nT);
+    t = (int)(w0 - (long long)g * nT);
+  }
+  __device__ __forceinline__ bool more() const { return left > 0; }
+  __device__ __forceinline__ void next() {
+    --left;
+    if (++t == nTiles) {
+      t = 0;
+      ++g;
+    }
+  }
+};
+
+// Gate test with the per-left and per-right terms already loaded (see gate_rejects).
+__device__ __forceinline__ bool gate_rejects_terms(int type, float sqrThr, float4 p, float4 q) {
+  if (type == 1) {
+    float num = __fadd_rn(__fadd_rn(__fmul_rn(q.x, p.x), __fmul_rn(q.y, p.y)), p.z);
+    num = __fmul_rn(num, num);
+    float denom = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.x, p.x), __fmul_rn(p.y, p.y)), __fmul_rn(q.z, q.z)),
+                            __fmul_rn(q.w, q.w));
+    return __fdiv_rn(num, denom) > sqrThr;
+  }
+  float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y);
+  return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > sqrThr;
+}
+
+// Gate test of element (left l, right r) against every gate of the call (global memory).
+__device__ __noinline__ bool gates_reject(const GateParams* gates, int nGates, int l, int r) {
+  for (int gi = 0; gi < nGates; ++gi)
+    if (gate_rejects(gates[gi], l, r)) return true;
+  return false;
+}
+
+// Exact lane-local pass over one 32-score chunk of A descriptor 'orig' (columns col0 ..):
+// updates the lane's best key lb and bound lw (both in "S + 1" units, 0 = none).
+__device__ __forceinline__ void rare_chunk(const SideArgs& a, const uint32_t (&v)[32], int col0, int orig,
+                                           unsigned long long& lb, uint32_t& lw) {
+  unsigned long long cb = 0;
+  uint32_t cw = 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int col = col0 + j;
+    if (col < a.nB) {
+      const int32_t S = (int32_t)v[j];
+      bool strong = S >= a.Smin;
+      if (strong && a.nGates)
+        strong = !gates_reject(a.gatesDev, a.nGates, a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
+      if (strong) {
+        const unsigned long long key = best_key(S, col);
+        if (key > cb) {
+          cw = max(cw, (uint32_t)(cb >> kIndexBits));
+          cb = key;
+        } else {
+          cw = max(cw, (uint32_t)(S + 1));
+        }
+      } else {
+        cw = max(cw, (uint32_t)(S + 1));
+      }
+    }
+  }
+  if (cb > lb) {
+    lw = max(lw, max((uint32_t)(lb >> kIndexBits), cw));
+    lb = cb;
+  } else {
+    lw = max(lw, max((uint32_t)(cb >> kIndexBits), cw));
+  }
+}
+
+template <class C>
 __global__ void __launch_bounds__(kThreads, 1)
-k_match_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcShape sh,
-           MatchArgs a) {
+k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
   extern __shared__ uint8_t smemRaw[];
-  Smem& s = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  Smem<C>& s = *reinterpret_cast<Smem<C>*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nA = a.nAptr ? *a.nAptr : a.nA;
+  TcShape sh;
+  sh.nGroups = (nA + C::GM - 1) / C::GM;
+  sh.nTiles = nTiles;
+  sh.nWork = (long long)sh.nGroups * nTiles;
+  if (sh.nWork == 0) {  // nothing to score (e.g. no right was chosen): uniform early exit
+    if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kEpiWarps + (warp - 2)] = 0;
+    return;
+  }
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kStages; ++i) {
+    for (int i = 0; i < C::kStages; ++i) {
       mbar_init(&s.fullB[i], 1);
       mbar_init(&s.emptyB[i], 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&s.fullA[i], 1);
       mbar_init(&s.emptyA[i], 1);
+    }
+    for (int i = 0; i < C::kAcc; ++i) {
       mbar_init(&s.accFull[i], 1);
       mbar_init(&s.accEmpty[i], kEpiWarps);
     }
     mbar_init(&s.mmaDone, 1);
-    s.candCount = 0;
     s.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -211,84 +340,94 @@ k_match_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     s.abort = 1;
   }
   __syncthreads();
+  long long w0, w1;
+  cta_range(sh, w0, w1);
 
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0;
-      uint32_t phase = 0, aPhase = 0;
-      int aBuf = 0;
-      uint32_t armedPhase[kStages];
-      bool armed[kStages];
-      for (int i = 0; i < kStages; ++i) armed[i] = false;
-      bool ok = true;
-      for (int u = blockIdx.x; u < sh.nUnits && ok; u += gridDim.x) {
-        int lb, t0, t1;
-        unit_coords(sh, u, lb, t0, t1);
-        if (!(ok = mbar_wait(&s.emptyA[aBuf], aPhase ^ 1, s, a.err))) break;
-        mbar_expect_tx(&s.fullA[aBuf], kABytes);
-        tma_load_2d(s.a[aBuf], &tmA, &s.fullA[aBuf], 0, lb * BM);
-        for (int t = t0; t < t1; ++t) {
-          if (!(ok = mbar_wait(&s.emptyB[stage], phase ^ 1, s, a.err))) break;
-          mbar_expect_tx(&s.fullB[stage], kBBytes);
-          tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, t * BN);
-          armed[stage] = true;
-          armedPhase[stage] = phase;
-          if (++stage == kStages) {
-            stage = 0;
-            phase ^= 1;
+      int stage = 0, aBuf = 1, prevG = -1;
+      uint32_t phase = 0, aPhase = 1;
+      uint32_t armedPhase[C::kStages];
+      bool armed[C::kStages];
+      for (int i = 0; i < C::kStages; ++i) armed[i] = false;
+      for (WorkCursor wc(w0, w1, sh.nTiles); wc.more(); wc.next()) {
+        const int g = wc.g, t = wc.t;
+        if (g != prevG) {
+          if (++aBuf == 2) {
+            aBuf = 0;
+            aPhase ^= 1;
           }
+          if (!mbar_wait(&s.emptyA[aBuf], aPhase ^ 1, &s.abort, a.err)) break;
+          mbar_expect_tx(&s.fullA[aBuf], C::kABytes);
+          tma_load_2d(s.a[aBuf], &tmA, &s.fullA[aBuf], 0, g * C::GM);
+          prevG = g;
         }
-        if (++aBuf == 2) {
-          aBuf = 0;
-          aPhase ^= 1;
+        if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
+        mbar_expect_tx(&s.fullB[stage], C::kBBytes);
+        tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, t * C::BN);
+        armed[stage] = true;
+        armedPhase[stage] = phase;
+        if (++stage == C::kStages) {
+          stage = 0;
+          phase ^= 1;
         }
       }
       // Drain: every load this thread issued has landed before the CTA may exit.
-      for (int i = 0; i < kStages; ++i)
+      for (int i = 0; i < C::kStages; ++i)
         if (armed[i]) {
           long long t0c = clock64();
           while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
           }
         }
+      if (prevG >= 0) {
+        long long t0c = clock64();
+        while (!mbar_try(&s.fullA[aBuf], aPhase) && clock64() - t0c < kWaitCycles) {
+        }
+      }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, acc = 0, aBuf = 0;
-      uint32_t phase = 0, accPhase = 0, aPhase = 0;
-      bool ok = true;
-      for (int u = blockIdx.x; u < sh.nUnits && ok; u += gridDim.x) {
-        int lb, t0, t1;
-        unit_coords(sh, u, lb, t0, t1);
-        if (!(ok = mbar_wait(&s.fullA[aBuf], aPhase, s, a.err))) break;
-        const uint32_t aAddr = smem_u32(s.a[aBuf]);
-        for (int t = t0; t < t1; ++t) {
-          if (!(ok = mbar_wait(&s.accEmpty[acc], accPhase ^ 1, s, a.err))) break;
-          if (!(ok = mbar_wait(&s.fullB[stage], phase, s, a.err))) break;
-          tc_fence_after();
-          const uint32_t bAddr = smem_u32(s.b[stage]);
-          const uint32_t d = tmem + (uint32_t)(acc * BN);
+      int stage = 0, acc = 0, aBuf = 1, prevG = -1;
+      uint32_t phase = 0, accPhase = 0, aPhase = 1;
+      uint32_t aAddr = 0;
+      for (WorkCursor wc(w0, w1, sh.nTiles); wc.more(); wc.next()) {
+        const int g = wc.g;
+        if (g != prevG) {
+          if (prevG >= 0) mma_commit(&s.emptyA[aBuf]);
+          if (++aBuf == 2) {
+            aBuf = 0;
+            aPhase ^= 1;
+          }
+          if (!mbar_wait(&s.fullA[aBuf], aPhase, &s.abort, a.err)) break;
+          aAddr = smem_u32(s.a[aBuf]);
+          prevG = g;
+        }
+        if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
+        if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) break;
+        tc_fence_after();
+        const uint32_t bAddr = smem_u32(s.b[stage]);
+#pragma unroll
+        for (int blk = 0; blk < C::NB; ++blk) {
+          const uint32_t d = tmem + (uint32_t)(acc * C::kAccCols + blk * C::BN);
+          const uint32_t ab = aAddr + (uint32_t)(blk * BM * kDescBytes);
 #pragma unroll
           for (int k = 0; k < kDescBytes / 32; ++k)
-            mma_i8(d, sdesc(aAddr + 32u * k), sdesc(bAddr + 32u * k), k > 0 ? 1u : 0u);
-          mma_commit(&s.emptyB[stage]);
-          mma_commit(&s.accFull[acc]);
-          if (++stage == kStages) {
-            stage = 0;
-            phase ^= 1;
-          }
-          if (++acc == 2) {
-            acc = 0;
-            accPhase ^= 1;
-          }
+            mma_i8<C::BN>(d, sdesc(ab + 32u * k), sdesc(bAddr + 32u * k), k > 0 ? 1u : 0u);
         }
-        mma_commit(&s.emptyA[aBuf]);
-        if (++aBuf == 2) {
-          aBuf = 0;
-          aPhase ^= 1;
+        mma_commit(&s.emptyB[stage]);
+        mma_commit(&s.accFull[acc]);
+        if (++stage == C::kStages) {
+          stage = 0;
+          phase ^= 1;
+        }
+        if (++acc == C::kAcc) {
+          acc = 0;
+          accPhase ^= 1;
         }
       }
+      if (prevG >= 0) mma_commit(&s.emptyA[aBuf]);
       // Every MMA this thread issued has completed before TMEM is released.
       mma_commit(&s.mmaDone);
       long long t0c = clock64();
@@ -297,60 +436,85 @@ k_match_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     }
   } else {
     // ---------------- epilogue ----------------
-    const int q = warp & 3;                // TMEM lane quadrant this warp may access
-    const int half = (warp - 2) >> 2;      // 0: columns 0..127, 1: columns 128..255
-    int acc = 0;
+    const int e = warp - 2;
+    const int q = warp & 3;                              // TMEM lane quadrant this warp may access
+    const int sub = e >> 2;                              // 0..3 within the quadrant
+    const int blk = C::NB == 2 ? (sub & 1) : 0;          // A block of the group
+    const int colOff = (C::NB == 2 ? (sub >> 1) : sub) * C::kWarpCols;  // first tile column of this warp
+    unsigned long long* const segBase = a.list + (long long)(blockIdx.x * kEpiWarps + e) * a.segCap;
+    int segN = 0;                                        // warp-uniform count of list entries written
+    int acc = 0, prevG = -1;
     uint32_t accPhase = 0;
     bool ok = !s.abort;
-    for (int u = blockIdx.x; u < sh.nUnits && ok; u += gridDim.x) {
-      int lb, t0, t1;
-      unit_coords(sh, u, lb, t0, t1);
-      const int l = lb * BM + q * 32 + lane;
-      const int32_t Tl = l < a.nL ? a.T : 0x7fffffff;
-      for (int t = t0; t < t1; ++t) {
-        ok = mbar_wait(&s.accFull[acc], accPhase, s, a.err);
-        ok = __all_sync(0xffffffffu, ok);
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * 128);
-#pragma unroll 1
-        for (int c = 0; c < 4; ++c) {
-          uint32_t v[32];
-          tmem_ld32(tbase + (uint32_t)(c * 32), v);
-          uint32_t m0 = max3_bits(v[0], v[1], v[2]), m1 = max3_bits(v[3], v[4], v[5]);
-          uint32_t m2 = max3_bits(v[6], v[7], v[8]), m3 = max3_bits(v[9], v[10], v[11]);
-          uint32_t m4 = max3_bits(v[12], v[13], v[14]), m5 = max3_bits(v[15], v[16], v[17]);
-          uint32_t m6 = max3_bits(v[18], v[19], v[20]), m7 = max3_bits(v[21], v[22], v[23]);
-          uint32_t m8 = max3_bits(v[24], v[25], v[26]), m9 = max3_bits(v[27], v[28], v[29]);
-          uint32_t n0 = max3_bits(m0, m1, m2), n1 = max3_bits(m3, m4, m5), n2 = max3_bits(m6, m7, m8);
-          uint32_t n3 = max3_bits(m9, v[30], v[31]);
-          uint32_t mx = max3_bits(n0, n1, max3_bits(n2, n3, 0u));
-          if (__any_sync(0xffffffffu, (int32_t)mx >= Tl)) {
-            const int col0 = t * BN + half * 128 + c * 32;
+    bool rowValid = false;
+    int orig = 0;
+    unsigned long long lb = 0;  // best key of this lane's descriptor in the current unit
+    uint32_t lw = 0;            // max + 1 of its other scores in the current unit
+    auto flush = [&]() {
+      // unit done: publish the lane's best key and bound
+      const bool hasBest = rowValid && lb != 0;
+      const unsigned m = __ballot_sync(0xffffffffu, hasBest);
+      if (hasBest) {
+        atomicMax(&a.best[orig], lb);
+        const int idx = segN + __popc(m & ((1u << lane) - 1u));
+        if (idx < a.segCap) segBase[idx] = (unsigned long long)(uint32_t)orig | (lb << kIndexBits);
+      }
+      segN += __popc(m);
+      if (rowValid && lw != 0) atomicMax(&a.sec[orig], lw);
+    };
+    for (WorkCursor wc(w0, w1, sh.nTiles); wc.more() && ok; wc.next()) {
+      const int g = wc.g, t = wc.t;
+      if (g != prevG) {
+        if (prevG >= 0) flush();
+        const int row = g * C::GM + blk * BM + q * 32 + lane;
+        rowValid = row < nA;
+        orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
+        lb = 0;
+        lw = 0;
+        prevG = g;
+      }
+      const int colBase = t * C::BN + colOff;
+      ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t tbase =
+          tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * C::kAccCols + blk * C::BN + colOff);
+      // All of this warp's scores into registers, then hand the stage back at once so the
+      // MMA never waits for the filtering below.
+      uint32_t v[C::kChunks][32];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const bool p = (int32_t)v[j] >= Tl && col0 + j < a.nR;
-              if (__any_sync(0xffffffffu, p)) {
-                if (p) candidate(a, s, l, col0 + j, (int32_t)v[j]);
-              }
-            }
-          }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
-        if (++acc == 2) {
-          acc = 0;
-          accPhase ^= 1;
+      for (int c = 0; c < C::kChunks; ++c) tmem_ld32(tbase + (uint32_t)(c * 32), v[c]);
+#pragma unroll
+      for (int c = 0; c < C::kChunks; ++c) tmem_wait(v[c]);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+#pragma unroll
+      for (int c = 0; c < C::kChunks; ++c) {
+        const int col0 = colBase + 32 * c;
+        if (col0 >= a.nB) break;  // chunks past the last B descriptor (warp-uniform)
+        // Columns past nB read TMA zero fill (0 <= every real score), so the chunk maximum
+        // stays the maximum of its real scores.
+        const uint32_t mx = max32_bits(v[c]);
+        const bool trig = rowValid && (int32_t)mx >= a.Smin;
+        if (rowValid && !trig) lw = max(lw, mx + 1u);
+        if (__any_sync(0xffffffffu, trig)) {
+          if (trig) rare_chunk(a, v[c], col0, orig, lb, lw);
         }
       }
+      if (++acc == C::kAcc) {
+        acc = 0;
+        accPhase ^= 1;
+      }
     }
+    if (prevG >= 0 && ok) flush();
+    if (lane == 0) a.segCount[blockIdx.x * kEpiWarps + e] = segN;
   }
 
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (threadIdx.x == 0) a.segCount[blockIdx.x] = s.candCount;
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
                               : "memory");
 }
@@ -381,14 +545,41 @@ bool encode_rows(CUtensorMap* map, const uint8_t* base, int rows, int boxRows) {
   return r == CUDA_SUCCESS;
 }
 
+
+// ---- configurations ------------------------------------------------------------------
+// Each entry instantiates the kernel for one tile shape; shared memory per CTA is
+// 2 * (NB*16 KB) for the left groups + stages * BN*128 bytes.
+using Cfg0 = TcCfg<1, 256, 4>;   // 128 x 256 tiles, 2 accumulator stages, 4-deep ring
+using Cfg1 = TcCfg<1, 128, 8>;   // 128 x 128 tiles, 4 accumulator stages
+using Cfg2 = TcCfg<2, 128, 8>;   // 256 x 128 tiles, 2 accumulator stages
+using Cfg3 = TcCfg<2, 64, 16>;   // 256 x 64 tiles, 4 accumulator stages
+using Cfg4 = TcCfg<1, 256, 6>;   // 128 x 256 tiles, 2 accumulator stages, 6-deep ring
+
+template <class C>
+cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles, const SideArgs& a, int grid,
+                       cudaStream_t st, bool& attrSet) {
+  const size_t smem = sizeof(Smem<C>) + 1024;
+  if (!attrSet) {
+    cudaError_t e = cudaFuncSetAttribute(k_side<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attrSet = true;
+  }
+  k_side<C><<<grid, kThreads, smem, st>>>(mA, mB, nTiles, a);
+  return cudaGetLastError();
+}
+
+constexpr int kNumCfg = 5;
+constexpr int kCfgNB[kNumCfg] = {Cfg0::NB, Cfg1::NB, Cfg2::NB, Cfg3::NB, Cfg4::NB};
+constexpr int kCfgBN[kNumCfg] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN};
+constexpr int kDefaultCfg = 0;
+
 }  // namespace
 
 struct TcPlan {
   int device = 0;
   int numSMs = 148;
-  CUtensorMap mapA, mapB;
-  int nL = 0, nR = 0;
-  bool attrSet = false;
+  int cfg = kDefaultCfg;
+  bool attrSet[kNumCfg] = {};
 };
 
 cudaError_t tc_plan_create(TcPlan** p, int device) {
@@ -406,48 +597,48 @@ cudaError_t tc_plan_create(TcPlan** p, int device) {
 
 void tc_plan_destroy(TcPlan* p) { delete p; }
 
-int tc_segments(TcPlan* p) { return p->numSMs; }
+int tc_segments(TcPlan* p) { return p->numSMs * kEpiWarps; }
 
-cudaError_t tc_plan_bind(TcPlan* p, const uint8_t* dL, int nL, const uint8_t* dR, int nR) {
-  if (nL <= 0 || nR <= 0) return cudaSuccess;
-  if (!encode_rows(&p->mapA, dL, nL, BM) || !encode_rows(&p->mapB, dR, nR, BN)) return cudaErrorInvalidValue;
-  p->nL = nL;
-  p->nR = nR;
+int tc_num_configs() { return kNumCfg; }
+
+int tc_get_config(TcPlan* p) { return p->cfg; }
+
+cudaError_t tc_set_config(TcPlan* p, int cfg) {
+  if (cfg < 0 || cfg >= kNumCfg) return cudaErrorInvalidValue;
+  p->cfg = cfg;
   return cudaSuccess;
 }
 
-cudaError_t launch_match_tc(TcPlan* p, const MatchArgs& a, cudaStream_t st, int* launches) {
-  *launches = 0;
-  if (a.nL <= 0 || a.nR <= 0) return cudaSuccess;
-  if (a.nL != p->nL || a.nR != p->nR) return cudaErrorInvalidValue;
-  if (!p->attrSet) {
-    cudaError_t e = cudaFuncSetAttribute(k_match_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-    if (e != cudaSuccess) return e;
-    p->attrSet = true;
+void tc_config_shape(int cfg, int* rowsPerGroup, int* colsPerTile) {
+  *rowsPerGroup = kCfgNB[cfg] * BM;
+  *colsPerTile = kCfgBN[cfg];
+}
+
+cudaError_t tc_side_maps(TcPlan* p, TcMaps* m, const uint8_t* dA, int rowsA, const uint8_t* dB, int rowsB) {
+  const int c = p->cfg;
+  if (rowsA <= 0 || rowsB <= 0) return cudaErrorInvalidValue;
+  if (!encode_rows(&m->a, dA, rowsA, kCfgNB[c] * BM) || !encode_rows(&m->b, dB, rowsB, kCfgBN[c]))
+    return cudaErrorInvalidValue;
+  m->cfg = c;
+  return cudaSuccess;
+}
+
+cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st) {
+  const int c = m.cfg;
+  const int bn = kCfgBN[c];
+  const int nTiles = (a.nB + bn - 1) / bn;
+  if (nTiles == 0) return cudaSuccess;
+  // Persistent grid: one CTA per SM (or fewer when the work is known to be small).
+  long long maxWork = (long long)((a.nA + kCfgNB[c] * BM - 1) / (kCfgNB[c] * BM)) * nTiles;
+  int grid = (int)std::min<long long>(p->numSMs, std::max<long long>(1, maxWork));
+  if (grid * kEpiWarps > a.nSeg) return cudaErrorInvalidValue;
+  switch (c) {
+    case 0: return launch_cfg<Cfg0>(m.a, m.b, nTiles, a, grid, st, p->attrSet[0]);
+    case 1: return launch_cfg<Cfg1>(m.a, m.b, nTiles, a, grid, st, p->attrSet[1]);
+    case 2: return launch_cfg<Cfg2>(m.a, m.b, nTiles, a, grid, st, p->attrSet[2]);
+    case 3: return launch_cfg<Cfg3>(m.a, m.b, nTiles, a, grid, st, p->attrSet[3]);
+    default: return launch_cfg<Cfg4>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
   }
-  TcShape sh;
-  sh.nLB = (a.nL + BM - 1) / BM;
-  sh.nRT = (a.nR + BN - 1) / BN;
-  // Split each left block's right range so that units fill the SMs evenly: minimise the
-  // makespan in tiles, counting half a tile of start-up per unit.
-  double bestCost = 1e300;
-  int bestSplit = 1;
-  for (int sp = 1; sp <= sh.nRT; ++sp) {
-    long long units = (long long)sh.nLB * sp;
-    long long waves = (units + p->numSMs - 1) / p->numSMs;
-    double cost = (double)waves * ((double)((sh.nRT + sp - 1) / sp) + 0.5);
-    if (cost < bestCost - 1e-9) {
-      bestCost = cost;
-      bestSplit = sp;
-    }
-  }
-  sh.nSplit = bestSplit;
-  sh.nUnits = sh.nLB * sh.nSplit;
-  int grid = std::min(p->numSMs, sh.nUnits);
-  if (grid > a.nSeg) return cudaErrorInvalidValue;
-  k_match_tc<<<grid, kThreads, kSmemBytes, st>>>(p->mapA, p->mapB, sh, a);
-  *launches = 1;
-  return cudaGetLastError();
 }
 
 }  // namespace v3dm

@@ -1,0 +1,275 @@
+// v3dm_pair.cu -- decisions and bookkeeping around the two tcgen05 side passes of a pair.
+//
+//   k_list     list pass (every unit best that is not the descriptor's overall best raises its
+//              second value);
+//   k_decide   the per-descriptor decision of the reference
+//              (v3d_cudamatching.cu:147-161 / :196-209, or the no-ratio test at :48 / :84).
+//              With guided gates the second value is an upper bound; when the decision with
+//              that bound differs from the decision with no second value at all, the
+//              descriptor is flagged for an exact re-score instead.
+//   k_rescore  exact re-score of flagged descriptors: every score against the other side,
+//              the gates, the masked value -1e20f (.cu:308, :340) and the reference's scan
+//              semantics (first index of the maximum, multiset second).
+//   k_choose   rights accepted by some left, de-duplicated, descriptors gathered for the
+//              second side pass (the mutual filter only ever reads these rights).
+//   k_mutual_count / k_mutual_write
+//              mutual filter (.cu:546-551) with an ordered compaction (ascending left).
+#include "v3dm_device.cuh"
+
+namespace v3dm {
+
+namespace {
+
+// List pass: one warp per segment; every unit best that is not the descriptor's overall
+// best raises its second value.  Segment counts are cleared for the next pass.
+__global__ void k_list(PostArgs a, int32_t* info) {
+  const int lane = threadIdx.x & 31;
+  const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
+    const int cnt = a.segCount[seg];
+    if (cnt == 0) continue;
+    if (lane == 0) {
+      atomicMax(&info[kInfoMaxSeg], cnt);
+      a.segCount[seg] = 0;
+    }
+    const long long n = cnt < a.segCap ? cnt : a.segCap;
+    const unsigned long long* e = a.list + (long long)seg * a.segCap;
+    for (long long i = lane; i < n; i += 32) {
+      const unsigned long long x = e[i];
+      const int idx = (int)(x & kIndexMask);
+      const unsigned long long key = x >> kIndexBits;
+      if (key != a.best[idx]) atomicMax(&a.sec[idx], (unsigned)(key >> kIndexBits));
+    }
+  }
+}
+
+// Decisions of the pass's descriptors; flags the ones whose gated bound straddles the
+// decision, clears the state of the others.
+__global__ void k_decide(PostArgs a) {
+  const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
+    const int idx = a.amap ? a.amap[r] : r;
+    const unsigned long long b = a.best[idx];
+    const unsigned s = a.sec[idx];
+    const int32_t d = decide(b, s, a.minScore, a.minRatio);
+    if (a.gated && b != 0 && s != 0 && d != decide(b, 0u, a.minScore, a.minRatio)) {
+      // the bound straddles the decision: exact re-score (k_rescore clears the state)
+      const int k = atomicAdd(a.flaggedCount, 1);
+      a.flagged[k] = idx;
+      a.decision[idx] = -1;
+      continue;
+    }
+    a.decision[idx] = d;
+    if (b) a.best[idx] = 0;
+    if (s) a.sec[idx] = 0;
+  }
+}
+
+struct Top2 {
+  float best;
+  int idx;
+  float second;
+};
+
+// Union of two scans; ties keep the lower index (the reference scans indices upwards).
+__device__ __forceinline__ Top2 top2_merge(Top2 x, Top2 y) {
+  const bool yWins = y.best > x.best || (y.best == x.best && y.idx < x.idx);
+  Top2 r;
+  if (yWins) {
+    r.best = y.best;
+    r.idx = y.idx;
+    r.second = fmaxf(x.best, y.second);
+  } else {
+    r.best = x.best;
+    r.idx = x.idx;
+    r.second = fmaxf(x.second, y.best);
+  }
+  return r;
+}
+
+constexpr int kRescoreThreads = 256;
+
+__global__ void __launch_bounds__(kRescoreThreads) k_rescore(RescoreArgs a) {
+  __shared__ uint32_t key[32];
+  __shared__ float sb[kRescoreThreads / 32], ss[kRescoreThreads / 32];
+  __shared__ int si[kRescoreThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int n = *a.flaggedCount;
+  for (int f = blockIdx.x; f < n; f += gridDim.x) {
+    const int idx = a.flagged[f];
+    __syncthreads();
+    if (tid < 32) key[tid] = reinterpret_cast<const uint32_t*>(a.descA + (size_t)idx * kDescBytes)[tid];
+    __syncthreads();
+    Top2 t{kNone, -1, kNone};
+    for (int j = tid; j < a.nB; j += kRescoreThreads) {
+      const uint4* bj = reinterpret_cast<const uint4*>(a.descB + (size_t)j * kDescBytes);
+      uint32_t S = 0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        const uint4 x = bj[w];
+        S = __dp4a(key[4 * w], x.x, S);
+        S = __dp4a(key[4 * w + 1], x.y, S);
+        S = __dp4a(key[4 * w + 2], x.z, S);
+        S = __dp4a(key[4 * w + 3], x.w, S);
+      }
+      // Scores below T, and masked scores, cannot change the decision (T is chosen so that
+      // any second value below it, the masked -1e20f included, decides like "none").
+      if ((int32_t)S < a.T) continue;
+      bool masked = false;
+      for (int gi = 0; gi < a.nGates && !masked; ++gi)
+        masked = gate_rejects(a.gatesDev[gi], a.aIsLeft ? idx : j, a.aIsLeft ? j : idx);
+      if (!masked) t = top2_merge(t, Top2{score_of((int32_t)S), j, kNone});
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      Top2 y;
+      y.best = __shfl_xor_sync(0xffffffffu, t.best, o);
+      y.idx = __shfl_xor_sync(0xffffffffu, t.idx, o);
+      y.second = __shfl_xor_sync(0xffffffffu, t.second, o);
+      t = top2_merge(t, y);
+    }
+    if (lane == 0) {
+      sb[wid] = t.best;
+      si[wid] = t.idx;
+      ss[wid] = t.second;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      Top2 r{kNone, -1, kNone};
+      for (int w = 0; w < kRescoreThreads / 32; ++w) r = top2_merge(r, Top2{sb[w], si[w], ss[w]});
+      a.decision[idx] = (r.idx >= 0 && accept_scores(r.best, r.second, a.minScore, a.minRatio)) ? r.idx : -1;
+      a.best[idx] = 0;
+      a.sec[idx] = 0;
+    }
+  }
+}
+
+__global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chosenFlag, int* chosenList,
+                         int* chosenCount, const uint8_t* __restrict__ dR, uint8_t* __restrict__ dRc) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nL; l += gridDim.x * blockDim.x) {
+    const int r = leftDec[l];
+    if (r < 0) continue;
+    if (atomicExch(&chosenFlag[r], 1) != 0) continue;
+    const int k = atomicAdd(chosenCount, 1);
+    chosenList[k] = r;
+    const uint4* src = reinterpret_cast<const uint4*>(dR + (size_t)r * kDescBytes);
+    uint4* dst = reinterpret_cast<uint4*>(dRc + (size_t)k * kDescBytes);
+#pragma unroll
+    for (int w = 0; w < kDescBytes / 16; ++w) dst[w] = src[w];
+  }
+}
+
+constexpr int kMutThreads = 256;
+constexpr int kMutPerBlock = 2048;  // lefts per block (8 per thread, contiguous)
+
+// Pass 1: number of mutual pairs among each block's contiguous range of lefts.
+__global__ void __launch_bounds__(kMutThreads)
+k_mutual_count(const int32_t* __restrict__ leftDec, int nL, const int32_t* __restrict__ rightDec,
+               int* __restrict__ blockCount) {
+  __shared__ int wsum[kMutThreads / 32];
+  const int base = blockIdx.x * kMutPerBlock;
+  int cnt = 0;
+  for (int k = base + threadIdx.x; k < min(base + kMutPerBlock, nL); k += kMutThreads) {
+    const int r = leftDec[k];
+    cnt += r >= 0 && rightDec[r] == k;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kMutThreads / 32; ++w) t += wsum[w];
+    blockCount[blockIdx.x] = t;
+  }
+}
+
+// Pass 2: each block offsets its pairs by the counts of the blocks before it and writes them
+// in ascending left order; clears the chosen-right flags.
+__global__ void __launch_bounds__(kMutThreads)
+k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __restrict__ rightDec, int* chosenFlag,
+               const int* __restrict__ blockCount, int nBlocks, int2* __restrict__ pairs, int32_t* info) {
+  __shared__ int blockOff;
+  __shared__ int wsum[kMutThreads / 32];
+  if (threadIdx.x < 32) {
+    int t = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += 32) t += blockCount[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) {
+      blockOff = t;
+      if (blockIdx.x == nBlocks - 1) info[kInfoPairs] = t + blockCount[blockIdx.x];
+    }
+  }
+  // each thread owns kMutPerBlock / kMutThreads consecutive lefts
+  constexpr int kPer = kMutPerBlock / kMutThreads;
+  const int beg = blockIdx.x * kMutPerBlock + threadIdx.x * kPer;
+  int r[kPer];
+  int cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int k = beg + i;
+    r[i] = k < nL ? leftDec[k] : -1;
+    const bool ok = r[i] >= 0 && rightDec[r[i]] == k;
+    if (r[i] >= 0) chosenFlag[r[i]] = 0;
+    if (!ok) r[i] = -1;
+    cnt += ok;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int inc = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < wid; ++w) before += wsum[w];
+  int off = blockOff + before + inc - cnt;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i)
+    if (r[i] >= 0) pairs[off++] = make_int2(beg + i, r[i]);
+}
+
+}  // namespace
+
+cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
+  int32_t* info = a.err - kInfoErr;
+  const int listBlocks = (a.nSeg * 32 + 255) / 256;
+  k_list<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, info);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int rows = a.nRows > 0 ? a.nRows : 1;
+  int blocks = (rows + 255) / 256;
+  k_decide<<<blocks < 1024 ? blocks : 1024, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s) {
+  k_rescore<<<grid, kRescoreThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                          const uint8_t* dR, uint8_t* dRc, cudaStream_t s) {
+  if (nL == 0) return cudaSuccess;
+  int blocks = (nL + 255) / 256;
+  if (blocks > 148) blocks = 148;
+  k_choose<<<blocks, 256, 0, s>>>(leftDec, nL, chosenFlag, chosenList, chosenCount, dR, dRc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,
+                          int2* pairs, int32_t* info, cudaStream_t s) {
+  const int nBlocks = (nL + kMutPerBlock - 1) / kMutPerBlock;
+  if (nBlocks == 0) return cudaSuccess;
+  k_mutual_count<<<nBlocks, kMutThreads, 0, s>>>(leftDec, nL, rightDec, blockCount);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_mutual_write<<<nBlocks, kMutThreads, 0, s>>>(leftDec, nL, rightDec, chosenFlag, blockCount, nBlocks, pairs, info);
+  return cudaGetLastError();
+}
+
+}  // namespace v3dm

@@ -45,6 +45,8 @@ class V3DMError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
         msg = lib().v3dm_status_string(status).decode() if _lib is not None else str(status)
+        if status == ERR_CUDA and _lib is not None:
+            msg += " [" + lib().v3dm_last_error().decode() + "]"
         super().__init__(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
 
 
@@ -58,6 +60,8 @@ def lib() -> C.CDLL:
         vp, i32, f32, f64p = C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_double)
         L.v3dm_status_string.restype = C.c_char_p
         L.v3dm_status_string.argtypes = [i32]
+        L.v3dm_last_error.restype = C.c_char_p
+        L.v3dm_last_error.argtypes = []
         L.v3dm_matcher_create.argtypes = [C.POINTER(vp), i32, C.c_uint]
         L.v3dm_matcher_destroy.argtypes = [vp]
         L.v3dm_allocate.argtypes = [vp, i32, i32, i32]
@@ -73,7 +77,12 @@ def lib() -> C.CDLL:
         L.v3dm_matcher_wait.argtypes = [vp]
         L.v3dm_matcher_last_launches.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_matcher_profile.argtypes = [vp, i32]
+        L.v3dm_matcher_num_configs.argtypes = [vp, C.POINTER(i32)]
+        L.v3dm_matcher_get_config.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+        L.v3dm_matcher_set_config.argtypes = [vp, i32]
+        L.v3dm_matcher_autotune.argtypes = [vp, f32, f32, i32, C.POINTER(i32), C.POINTER(C.c_double)]
         L.v3dm_matcher_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i32)]
+        L.v3dm_matcher_profile_read_pass.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
         L.v3dm_candidate_threshold.argtypes = [f32, f32, i32, C.POINTER(C.c_int32)]
         L.v3dm_voctree_create.argtypes = [C.POINTER(vp), i32, i32, i32]
         L.v3dm_voctree_destroy.argtypes = [vp]
@@ -132,9 +141,9 @@ class SIFTMatching:
         self.n_right = 0
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
-            lib().v3dm_matcher_destroy(self._h)
-            self._h = None
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_matcher_destroy(self._h)
+        self._h = None
 
     __del__ = close
 
@@ -218,13 +227,40 @@ class SIFTMatching:
         _check(lib().v3dm_matcher_stream(self._h, C.byref(s)), "stream")
         return s.value or 0
 
+    def num_configs(self) -> int:
+        n = C.c_int(0)
+        _check(lib().v3dm_matcher_num_configs(self._h, C.byref(n)), "num_configs")
+        return n.value
+
+    def config(self):
+        """(config id, left rows per group, right columns per tile) of the fused kernel."""
+        c, r, n = C.c_int(0), C.c_int(0), C.c_int(0)
+        _check(lib().v3dm_matcher_get_config(self._h, C.byref(c), C.byref(r), C.byref(n)), "get_config")
+        return c.value, r.value, n.value
+
+    def set_config(self, cfg: int) -> None:
+        _check(lib().v3dm_matcher_set_config(self._h, cfg), "set_config")
+
+    def autotune(self, min_score: float = 0.9, min_ratio: float = 0.8, reps: int = 3):
+        """Times every kernel configuration on the current features; keeps and returns the
+        fastest as (config id, milliseconds per call)."""
+        b, ms = C.c_int(0), C.c_double(0)
+        _check(lib().v3dm_matcher_autotune(self._h, min_score, min_ratio, reps, C.byref(b), C.byref(ms)),
+               "autotune")
+        return b.value, ms.value
+
     def profile(self, enable: bool = True) -> None:
         _check(lib().v3dm_matcher_profile(self._h, int(enable)), "profile")
 
-    def profile_read(self):
-        """(summed milliseconds, launches) of the fused matching kernel since profile()."""
+    def profile_read(self, pass_id: int | None = None):
+        """(summed milliseconds, launches) of the fused matching kernel since profile():
+        pass 0 = lefts x rights (the full contraction), pass 1 = chosen rights x lefts.
+        Without pass_id: pass 0, clearing the record."""
         ms, n = C.c_double(0), C.c_int(0)
-        _check(lib().v3dm_matcher_profile_read(self._h, C.byref(ms), C.byref(n)), "profile_read")
+        if pass_id is None:
+            _check(lib().v3dm_matcher_profile_read(self._h, C.byref(ms), C.byref(n)), "profile_read")
+        else:
+            _check(lib().v3dm_matcher_profile_read_pass(self._h, pass_id, C.byref(ms), C.byref(n)), "profile_read")
         return ms.value, n.value
 
     def last_launches(self) -> int:
@@ -249,9 +285,9 @@ class VocabularyTreeTraversal:
         self.branch_factor, self.depth = branch_factor, depth
 
     def close(self):
-        if getattr(self, "_h", None):
-            lib().v3dm_voctree_destroy(self._h)
-            self._h = None
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_voctree_destroy(self._h)
+        self._h = None
 
     __del__ = close
 

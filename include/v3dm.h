@@ -53,6 +53,9 @@ extern "C" {
                                       list has been grown, repeat the call             */
 
 V3DM_API const char* v3dm_status_string(int status);
+/* Detail of the last V3DM_ERR_CUDA raised by a matcher call on this thread (the CUDA error
+ * and the call that returned it); empty when none. */
+V3DM_API const char* v3dm_last_error(void);
 
 /* Largest feature count per image side (17-bit index field of the device state). */
 #define V3DM_MAX_FEATURES 131072
@@ -116,6 +119,18 @@ V3DM_API int v3dm_matcher_stream(v3dm_matcher* h, void** stream);
  * the summed duration in milliseconds and the number of timed launches since. */
 V3DM_API int v3dm_matcher_profile(v3dm_matcher* h, int enable);
 V3DM_API int v3dm_matcher_profile_read(v3dm_matcher* h, double* msTotal, int* launches);
+/* The same per pass of the tcgen05 path: pass 0 = lefts x rights (the full contraction),
+ * pass 1 = chosen rights x lefts.  Reading pass 1 clears the record. */
+V3DM_API int v3dm_matcher_profile_read_pass(v3dm_matcher* h, int pass, double* msTotal, int* launches);
+/* Tile configurations of the fused kernel (shape of the left group x right tile and the
+ * pipeline depths).  v3dm_matcher_autotune times every configuration on the current
+ * features (putative matching, 'reps' timed runs each), keeps the fastest and returns it;
+ * it is the tuner the batched and single-pair paths use to pick their tile shape. */
+V3DM_API int v3dm_matcher_num_configs(v3dm_matcher* h, int* n);
+V3DM_API int v3dm_matcher_get_config(v3dm_matcher* h, int* cfg, int* rowsPerGroup, int* colsPerTile);
+V3DM_API int v3dm_matcher_set_config(v3dm_matcher* h, int cfg);
+V3DM_API int v3dm_matcher_autotune(v3dm_matcher* h, float minScore, float minRatio, int reps, int* best,
+                                   double* msBest);
 /* Number of kernels the last matching call launched. */
 V3DM_API int v3dm_matcher_last_launches(v3dm_matcher* h, int* n);
 

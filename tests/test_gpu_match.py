@@ -154,3 +154,31 @@ def test_stereo_16384_guided(make_matcher, oracle_mod):
     np.testing.assert_array_equal(got, exp)
     # size-independent property: guided pairs agree with the planted geometry
     assert np.mean(truth[got[:, 1]] == got[:, 0]) > 0.99
+
+
+@pytest.mark.parametrize("nL,nR", [(300, 1000), (4095, 4097), (257, 63)])
+def test_every_tile_config(v3dm_mod, oracle_mod, nL, nR):
+    L, R, lp, rp, F, _ = synth.stereo(7 + nL, nL, nR)
+    exp_put = oracle_mod.match(L, R, 0.7, 0.8)
+    exp_gui = oracle_mod.match(L, R, 0.7, 0.8, gates=[("F", F, 2.0)], lpos=lp, rpos=rp)
+    with v3dm_mod.SIFTMatching(0, v3dm_mod.KERNEL_TCGEN05) as m:
+        m.allocate(nL, nR, True)
+        m.set_left_features(L)
+        m.set_right_features(R)
+        for cfg in range(m.num_configs()):
+            m.set_config(cfg)
+            np.testing.assert_array_equal(m.find_putative_matches(0.7, 0.8), exp_put, err_msg=f"config {cfg}")
+            np.testing.assert_array_equal(m.run_guided_matching(F, 2.0, lp, rp, 0.7, 0.8), exp_gui,
+                                          err_msg=f"config {cfg}")
+
+
+def test_autotune_keeps_results(v3dm_mod, oracle_mod):
+    L, R, _ = synth.pair(3, 3000, 3500)
+    with v3dm_mod.SIFTMatching(0, v3dm_mod.KERNEL_TCGEN05) as m:
+        m.allocate(3000, 3500)
+        m.set_left_features(L)
+        m.set_right_features(R)
+        best, ms = m.autotune(0.7, 0.8, 2)
+        assert 0 <= best < m.num_configs() and ms > 0
+        assert m.config()[0] == best
+        np.testing.assert_array_equal(m.find_putative_matches(0.7, 0.8), oracle_mod.match(L, R, 0.7, 0.8))
