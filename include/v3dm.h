@@ -138,6 +138,31 @@ V3DM_API int v3dm_matcher_last_launches(v3dm_matcher* h, int* n);
  * no score below T can change a decision.  Exposed for tests.  Host-only, no device. */
 V3DM_API int v3dm_candidate_threshold(float minScore, float minRatio, int gated, int32_t* T);
 
+/* ---- putative matching without device allocation --------------------------------- */
+/* No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory while they match (a host application that owns all GPU memory and gives plug-ins
+ * a fixed budget, a frame loop where cudaMalloc/cudaFree would synchronise the device, a
+ * service that must not hit out-of-memory halfway through a job).
+ *
+ * Same result as v3dm_putative (findPutativeMatches, v3d_cudamatching.cu:522-552) for uint8
+ * descriptors already in device memory, computed by the dp4a kernels.  All working memory is
+ * one fixed array inside the library's device image, held by every GPU that loads the
+ * library until the process exits; nothing is allocated per call.
+ *   d_left / d_right: nLeft / nRight x 128 uint8 in device memory of 'device';
+ *   d_pairs: room for 2 * min(nLeft, nRight) int32 (left, right pairs, ascending left);
+ *   d_count: one int32, the number of pairs, or -1 if a call exceeded the candidate limit;
+ *   stream: cudaStream_t the work is queued on (asynchronous; nothing is copied to the host).
+ * Limits: nLeft, nRight <= V3DM_NOALLOC_MAX_FEATURES (else V3DM_ERR_SIZE) and at most
+ * V3DM_NOALLOC_MAX_CANDIDATES scores at or above the candidate threshold per call.
+ * All calls share the one array: calls that overlap on the GPU race, so serialise them.
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress with that
+ * device current); make it before any stream capture begins. */
+#define V3DM_NOALLOC_MAX_FEATURES 8192
+#define V3DM_NOALLOC_MAX_CANDIDATES 524288
+V3DM_API int v3dm_putative_u8_noalloc(int device, const uint8_t* d_left, int nLeft, const uint8_t* d_right, int nRight,
+                                      float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count,
+                                      void* stream);
+
 /* ---- vocabulary tree (V3D_CUDA::VocabularyTreeTraversal<BF, Depth>) --------------- */
 typedef struct v3dm_voctree v3dm_voctree;
 
