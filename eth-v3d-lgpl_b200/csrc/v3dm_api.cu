@@ -576,7 +576,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
     ra.sec = h->dLSec;
     ra.decision = h->dLeftDec;
     V3DM_CUDA_TRY(launch_rescore(ra, 64, h->stream));
-    h->lastLaunches += 1;
+    h->lastLaunches += 2;
   }
   V3DM_CUDA_TRY(launch_choose(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dR, h->dRc,
                               h->stream));
@@ -617,7 +617,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
     ra.sec = h->dRSec;
     ra.decision = h->dRightDec;
     V3DM_CUDA_TRY(launch_rescore(ra, 64, h->stream));
-    h->lastLaunches += 1;
+    h->lastLaunches += 2;
   }
   V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
                               reinterpret_cast<int2*>(dPairs), h->dInfo, h->stream));

@@ -7,9 +7,8 @@
 //              With guided gates the second value is an upper bound; when the decision with
 //              that bound differs from the decision with no second value at all, the
 //              descriptor is flagged for an exact re-score instead.
-//   k_rescore  exact re-score of flagged descriptors: every score against the other side,
-//              the gates, the masked value -1e20f (.cu:308, :340) and the reference's scan
-//              semantics (first index of the maximum, multiset second).
+//   k_rescore  exact second value of flagged descriptors: every score against the other
+//              side that can matter, with the gates; k_rescore_decide then decides them.
 //   k_choose   rights accepted by some left, de-duplicated, descriptors gathered for the
 //              second side pass (the mutual filter only ever reads these rights).
 //   k_mutual_count / k_mutual_write
@@ -58,6 +57,7 @@ __global__ void k_decide(PostArgs a) {
       const int k = atomicAdd(a.flaggedCount, 1);
       a.flagged[k] = idx;
       a.decision[idx] = -1;
+      a.sec[idx] = 0;  // recomputed exactly by k_rescore
       continue;
     }
     a.decision[idx] = d;
@@ -66,82 +66,72 @@ __global__ void k_decide(PostArgs a) {
   }
 }
 
-struct Top2 {
-  float best;
-  int idx;
-  float second;
-};
-
-// Union of two scans; ties keep the lower index (the reference scans indices upwards).
-__device__ __forceinline__ Top2 top2_merge(Top2 x, Top2 y) {
-  const bool yWins = y.best > x.best || (y.best == x.best && y.idx < x.idx);
-  Top2 r;
-  if (yWins) {
-    r.best = y.best;
-    r.idx = y.idx;
-    r.second = fmaxf(x.best, y.second);
-  } else {
-    r.best = x.best;
-    r.idx = x.idx;
-    r.second = fmaxf(x.second, y.best);
-  }
-  return r;
-}
-
+// Exact second value of the flagged descriptors.  Their best key is already exact (the side
+// pass applies the gates to every score that can pass the min-score test); the second value
+// is the largest unmasked score other than the best.  Only scores >= T matter (T is chosen
+// so that any second value below it, the masked -1e20f included, decides like "none").
+// Each thread holds one descriptor of side B in registers and scores it against the flagged
+// descriptors, staged 64 at a time in shared memory.
 constexpr int kRescoreThreads = 256;
+constexpr int kRescoreStage = 64;
 
 __global__ void __launch_bounds__(kRescoreThreads) k_rescore(RescoreArgs a) {
-  __shared__ uint32_t key[32];
-  __shared__ float sb[kRescoreThreads / 32], ss[kRescoreThreads / 32];
-  __shared__ int si[kRescoreThreads / 32];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  __shared__ uint32_t sA[kRescoreStage][33];
+  __shared__ int sIdx[kRescoreStage];
+  __shared__ unsigned long long sBest[kRescoreStage];
+  const int tid = threadIdx.x;
+  const int j = blockIdx.x * kRescoreThreads + tid;
+  const bool valid = j < a.nB;
+  uint32_t b[32];
+  if (valid) {
+    const uint4* bj = reinterpret_cast<const uint4*>(a.descB + (size_t)j * kDescBytes);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const uint4 x = bj[w];
+      b[4 * w] = x.x;
+      b[4 * w + 1] = x.y;
+      b[4 * w + 2] = x.z;
+      b[4 * w + 3] = x.w;
+    }
+  }
   const int n = *a.flaggedCount;
-  for (int f = blockIdx.x; f < n; f += gridDim.x) {
-    const int idx = a.flagged[f];
+  for (int f0 = 0; f0 < n; f0 += kRescoreStage) {
+    const int nf = min(kRescoreStage, n - f0);
     __syncthreads();
-    if (tid < 32) key[tid] = reinterpret_cast<const uint32_t*>(a.descA + (size_t)idx * kDescBytes)[tid];
+    for (int i = tid; i < nf * 32; i += kRescoreThreads) {
+      const int f = i >> 5, w = i & 31;
+      const int idx = a.flagged[f0 + f];
+      sA[f][w] = reinterpret_cast<const uint32_t*>(a.descA + (size_t)idx * kDescBytes)[w];
+      if (w == 0) {
+        sIdx[f] = idx;
+        sBest[f] = a.best[idx];
+      }
+    }
     __syncthreads();
-    Top2 t{kNone, -1, kNone};
-    for (int j = tid; j < a.nB; j += kRescoreThreads) {
-      const uint4* bj = reinterpret_cast<const uint4*>(a.descB + (size_t)j * kDescBytes);
+    if (!valid) continue;
+    for (int f = 0; f < nf; ++f) {
       uint32_t S = 0;
 #pragma unroll
-      for (int w = 0; w < 8; ++w) {
-        const uint4 x = bj[w];
-        S = __dp4a(key[4 * w], x.x, S);
-        S = __dp4a(key[4 * w + 1], x.y, S);
-        S = __dp4a(key[4 * w + 2], x.z, S);
-        S = __dp4a(key[4 * w + 3], x.w, S);
-      }
-      // Scores below T, and masked scores, cannot change the decision (T is chosen so that
-      // any second value below it, the masked -1e20f included, decides like "none").
+      for (int w = 0; w < 32; ++w) S = __dp4a(sA[f][w], b[w], S);
       if ((int32_t)S < a.T) continue;
+      const int idx = sIdx[f];
+      if (best_key((int32_t)S, j) == sBest[f]) continue;  // the best itself
       bool masked = false;
       for (int gi = 0; gi < a.nGates && !masked; ++gi)
         masked = gate_rejects(a.gatesDev[gi], a.aIsLeft ? idx : j, a.aIsLeft ? j : idx);
-      if (!masked) t = top2_merge(t, Top2{score_of((int32_t)S), j, kNone});
+      if (!masked) atomicMax(&a.sec[idx], (unsigned)S + 1u);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      Top2 y;
-      y.best = __shfl_xor_sync(0xffffffffu, t.best, o);
-      y.idx = __shfl_xor_sync(0xffffffffu, t.idx, o);
-      y.second = __shfl_xor_sync(0xffffffffu, t.second, o);
-      t = top2_merge(t, y);
-    }
-    if (lane == 0) {
-      sb[wid] = t.best;
-      si[wid] = t.idx;
-      ss[wid] = t.second;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      Top2 r{kNone, -1, kNone};
-      for (int w = 0; w < kRescoreThreads / 32; ++w) r = top2_merge(r, Top2{sb[w], si[w], ss[w]});
-      a.decision[idx] = (r.idx >= 0 && accept_scores(r.best, r.second, a.minScore, a.minRatio)) ? r.idx : -1;
-      a.best[idx] = 0;
-      a.sec[idx] = 0;
-    }
+  }
+}
+
+// Decisions of the flagged descriptors from their exact second values; clears their state.
+__global__ void k_rescore_decide(RescoreArgs a) {
+  const int n = *a.flaggedCount;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
+    const int idx = a.flagged[f];
+    a.decision[idx] = decide(a.best[idx], a.sec[idx], a.minScore, a.minRatio);
+    a.best[idx] = 0;
+    a.sec[idx] = 0;
   }
 }
 
@@ -248,7 +238,14 @@ cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s) {
-  k_rescore<<<grid, kRescoreThreads, 0, s>>>(a);
+  (void)grid;
+  const int blocks = (a.nB + kRescoreThreads - 1) / kRescoreThreads;
+  if (blocks > 0) {
+    k_rescore<<<blocks, kRescoreThreads, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k_rescore_decide<<<16, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
