@@ -34,7 +34,8 @@ struct v3dm_matcher {
   unsigned int* dLSec = nullptr;         // per left: second value + 1
   unsigned long long* dRBest = nullptr;  // per right: best key
   unsigned int* dRSec = nullptr;         // per right: second value + 1
-  unsigned long long* dCand = nullptr;   // candidate list: nSeg x segCap
+  unsigned long long* dCand = nullptr;   // candidate list (SIMT) / chunk-record entries (tcgen05): nSeg x segCap
+  uint4* dRecords = nullptr;             // tcgen05 chunk records: nSeg x segCap x kRecordQuads
   int* dSegCount = nullptr;              // nSeg counts
   long long segCap = 0;
   int nSeg = 0;
@@ -139,9 +140,12 @@ void free_buffers(v3dm_matcher* h) {
 cudaError_t alloc_candidates(v3dm_matcher* h, int nSeg, long long segCap) {
   dfree(h->dCand);
   dfree(h->dSegCount);
+  dfree(h->dRecords);
   h->segCap = 0;
   h->nSeg = 0;
   cudaError_t e = dalloc(&h->dCand, (size_t)nSeg * (size_t)segCap);
+  if (e == cudaSuccess && h->kernel != V3DM_KERNEL_SIMT)
+    e = dalloc(&h->dRecords, (size_t)nSeg * (size_t)segCap * kRecordQuads);
   if (e == cudaSuccess) e = dalloc(&h->dSegCount, (size_t)nSeg);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->dSegCount, 0, (size_t)nSeg * sizeof(int), h->stream);
   if (e != cudaSuccess) return e;
@@ -369,7 +373,7 @@ int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
     ok = alloc_candidates(h, 1, segCap) == cudaSuccess;
   } else if (ok) {
     // tcgen05 path: one list segment per epilogue warp, holding that warp's unit bests.
-    ok = alloc_candidates(h, tc_segments(h->tc), 2048) == cudaSuccess &&
+    ok = alloc_candidates(h, tc_segments(h->tc), 64) == cudaSuccess &&
          dalloc(&h->dRc, rowsR * kDescBytes) == cudaSuccess && dalloc(&h->dLeftDec, (size_t)nMaxL + 1) == cudaSuccess &&
          dalloc(&h->dRightDec, (size_t)nMaxR + 1) == cudaSuccess &&
          dalloc(&h->dChosenFlag, (size_t)nMaxR + 1) == cudaSuccess &&
@@ -516,7 +520,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
-  sa.list = h->dCand;
+  sa.records = h->dRecords;
   sa.segCount = h->dSegCount;
   sa.segCap = h->segCap;
   sa.nSeg = h->nSeg;
@@ -525,8 +529,12 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   sa.gatesDev = h->dGates;
   PostArgs pa;
   std::memset(&pa, 0, sizeof(pa));
+  pa.records = h->dRecords;
   pa.list = h->dCand;
   pa.segCount = h->dSegCount;
+  pa.Smin = Smin;
+  pa.nGates = h->nGates;
+  pa.gatesDev = h->dGates;
   pa.segCap = h->segCap;
   pa.nSeg = h->nSeg;
   pa.minScore = minScore;
@@ -558,13 +566,15 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   V3DM_CUDA_TRY(launch_side(h->tc, h->mapsA, sa, h->stream));
   if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
   pa.nRows = h->nL;
+  pa.nB = h->nR;
+  pa.aIsLeft = 1;
   pa.best = h->dLBest;
   pa.sec = h->dLSec;
   pa.decision = h->dLeftDec;
   pa.flagged = h->dFlagA;
   pa.flaggedCount = h->dCounters + 1;
   V3DM_CUDA_TRY(launch_post(pa, h->stream));
-  h->lastLaunches += 3;
+  h->lastLaunches += 4;
   if (gated) {
     ra.descA = h->dL;
     ra.descB = h->dR;
@@ -597,6 +607,8 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   V3DM_CUDA_TRY(launch_side(h->tc, h->mapsB, sa, h->stream));
   if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evB[1], h->stream));
   pa.nRows = h->nR;
+  pa.nB = h->nL;
+  pa.aIsLeft = 0;
   pa.rowsPtr = h->dCounters;
   pa.amap = h->dChosenList;
   pa.best = h->dRBest;
@@ -605,7 +617,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   pa.flagged = h->dFlagB;
   pa.flaggedCount = h->dCounters + 2;
   V3DM_CUDA_TRY(launch_post(pa, h->stream));
-  h->lastLaunches += 3;
+  h->lastLaunches += 4;
   if (gated) {
     ra.descA = h->dR;
     ra.descB = h->dL;

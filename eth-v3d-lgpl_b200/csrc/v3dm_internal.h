@@ -57,14 +57,16 @@ struct SideArgs {
   int aIsLeft;                   // 1: A = lefts, B = rights; 0: A = rights, B = lefts
   unsigned long long* best;      // per A index: best key over B (atomicMax)
   unsigned int* sec;             // per A index: second score + 1 (exact, or a bound with gates)
-  unsigned long long* list;      // per-warp segments of (A index, unit best key) entries
-  int* segCount;
-  long long segCap;
+  uint4* records;                // per-warp segments of chunk records (kRecordQuads uint4 each)
+  int* segCount;                 // per segment: records written
+  long long segCap;              // records per segment
   int nSeg;
   int* err;
   int nGates;
   const GateParams* gatesDev;    // device array of the call's gates
 };
+// Chunk record: {A index, first B index, 0, 0} then the chunk's 32 scores.
+constexpr int kRecordQuads = 9;
 
 struct TcPlan;
 struct TcMaps {
@@ -90,10 +92,16 @@ struct PostArgs {
   const int* amap;               // row -> index (null: identity)
   unsigned long long* best;
   unsigned int* sec;
-  const unsigned long long* list;
+  const uint4* records;          // chunk records of the side pass
+  unsigned long long* list;      // one (A index, chunk best key) entry per record
   int* segCount;                 // read, then cleared
   long long segCap;
   int nSeg;
+  int nB;
+  int aIsLeft;
+  int32_t Smin;
+  int nGates;
+  const GateParams* gatesDev;
   float minScore, minRatio;
   int gated;
   int32_t* decision;             // per index: accepted partner or -1

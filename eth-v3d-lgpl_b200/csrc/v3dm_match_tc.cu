@@ -14,12 +14,13 @@
 //               stage back, and per chunk does one of two things:
 //                 - all scores below Smin (the smallest score that can pass the min-score
 //                   test): W = max(W, chunk maximum + 1)                     (one op);
-//                 - some score >= Smin (true matches, ~1e-6 of unrelated pairs): an exact
-//                   lane-local pass over the chunk: guided gates for every score >= Smin,
-//                   chunk best (largest score, first index on ties, the reference's argMax
-//                   rule, v3d_cudamatching.cu:145) and the maximum of all other scores.
-//               At the end of a work unit the lane's best key goes to best[] (atomicMax) and
-//               a candidate-list entry, its W to sec[] (atomicMax).
+//                 - some score >= Smin (true matches, ~1e-6 of unrelated pairs): the lane
+//                   writes a record (descriptor, first column, its 32 scores) to its warp's
+//                   segment; k_records (v3dm_pair.cu) does the exact work on it: guided
+//                   gates for every score >= Smin, chunk best (largest score, first index on
+//                   ties, the reference's argMax rule, v3d_cudamatching.cu:145), maximum of
+//                   the other scores.
+//               At the end of a work unit the lane's W goes to sec[] (atomicMax).
 // Resulting per-descriptor values (after the list pass in v3dm_pair.cu): best = the exact
 // best over scores >= Smin that pass the gates; sec = the exact second-best score without
 // gates, an upper bound of it with gates (masked scores are counted).  The decision
@@ -250,48 +251,6 @@ __device__ __forceinline__ bool gate_rejects_terms(int type, float sqrThr, float
   return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > sqrThr;
 }
 
-// Gate test of element (left l, right r) against every gate of the call (global memory).
-__device__ __noinline__ bool gates_reject(const GateParams* gates, int nGates, int l, int r) {
-  for (int gi = 0; gi < nGates; ++gi)
-    if (gate_rejects(gates[gi], l, r)) return true;
-  return false;
-}
-
-// Exact lane-local pass over one 32-score chunk of A descriptor 'orig' (columns col0 ..):
-// updates the lane's best key lb and bound lw (both in "S + 1" units, 0 = none).
-__device__ __forceinline__ void rare_chunk(const SideArgs& a, const uint32_t (&v)[32], int col0, int orig,
-                                           unsigned long long& lb, uint32_t& lw) {
-  unsigned long long cb = 0;
-  uint32_t cw = 0;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const int col = col0 + j;
-    if (col < a.nB) {
-      const int32_t S = (int32_t)v[j];
-      bool strong = S >= a.Smin;
-      if (strong && a.nGates)
-        strong = !gates_reject(a.gatesDev, a.nGates, a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
-      if (strong) {
-        const unsigned long long key = best_key(S, col);
-        if (key > cb) {
-          cw = max(cw, (uint32_t)(cb >> kIndexBits));
-          cb = key;
-        } else {
-          cw = max(cw, (uint32_t)(S + 1));
-        }
-      } else {
-        cw = max(cw, (uint32_t)(S + 1));
-      }
-    }
-  }
-  if (cb > lb) {
-    lw = max(lw, max((uint32_t)(lb >> kIndexBits), cw));
-    lb = cb;
-  } else {
-    lw = max(lw, max((uint32_t)(cb >> kIndexBits), cw));
-  }
-}
-
 template <class C>
 __global__ void __launch_bounds__(kThreads, 1)
 k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
@@ -441,25 +400,15 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     const int sub = e >> 2;                              // 0..3 within the quadrant
     const int blk = C::NB == 2 ? (sub & 1) : 0;          // A block of the group
     const int colOff = (C::NB == 2 ? (sub >> 1) : sub) * C::kWarpCols;  // first tile column of this warp
-    unsigned long long* const segBase = a.list + (long long)(blockIdx.x * kEpiWarps + e) * a.segCap;
-    int segN = 0;                                        // warp-uniform count of list entries written
+    uint4* const segBase = a.records + (long long)(blockIdx.x * kEpiWarps + e) * a.segCap * kRecordQuads;
+    int segN = 0;                                        // warp-uniform count of records written
     int acc = 0, prevG = -1;
     uint32_t accPhase = 0;
     bool ok = !s.abort;
     bool rowValid = false;
     int orig = 0;
-    unsigned long long lb = 0;  // best key of this lane's descriptor in the current unit
-    uint32_t lw = 0;            // max + 1 of its other scores in the current unit
+    uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
     auto flush = [&]() {
-      // unit done: publish the lane's best key and bound
-      const bool hasBest = rowValid && lb != 0;
-      const unsigned m = __ballot_sync(0xffffffffu, hasBest);
-      if (hasBest) {
-        atomicMax(&a.best[orig], lb);
-        const int idx = segN + __popc(m & ((1u << lane) - 1u));
-        if (idx < a.segCap) segBase[idx] = (unsigned long long)(uint32_t)orig | (lb << kIndexBits);
-      }
-      segN += __popc(m);
       if (rowValid && lw != 0) atomicMax(&a.sec[orig], lw);
     };
     for (WorkCursor wc(w0, w1, sh.nTiles); wc.more() && ok; wc.next()) {
@@ -469,7 +418,6 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         const int row = g * C::GM + blk * BM + q * 32 + lane;
         rowValid = row < nA;
         orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
-        lb = 0;
         lw = 0;
         prevG = g;
       }
@@ -500,7 +448,19 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         const bool trig = rowValid && (int32_t)mx >= a.Smin;
         if (rowValid && !trig) lw = max(lw, mx + 1u);
         if (__any_sync(0xffffffffu, trig)) {
-          if (trig) rare_chunk(a, v[c], col0, orig, lb, lw);
+          // rare: hand the chunk to k_records (its exact best, gates and other scores)
+          const unsigned m = __ballot_sync(0xffffffffu, trig);
+          if (trig) {
+            const int idx = segN + __popc(m & ((1u << lane) - 1u));
+            if (idx < a.segCap) {
+              uint4* rec = segBase + (long long)idx * kRecordQuads;
+              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, 0u, 0u);
+#pragma unroll
+              for (int k = 0; k < 8; ++k)
+                rec[1 + k] = make_uint4(v[c][4 * k], v[c][4 * k + 1], v[c][4 * k + 2], v[c][4 * k + 3]);
+            }
+          }
+          segN += __popc(m);
         }
       }
       if (++acc == C::kAcc) {

@@ -1,6 +1,7 @@
 // v3dm_pair.cu -- decisions and bookkeeping around the two tcgen05 side passes of a pair.
 //
-//   k_list     list pass (every unit best that is not the descriptor's overall best raises its
+//   k_records  exact work on the chunk records of a side pass (gates, chunk best, bound);
+//   k_list     list pass (every chunk best that is not the descriptor's overall best raises its
 //              second value);
 //   k_decide   the per-descriptor decision of the reference
 //              (v3d_cudamatching.cu:147-161 / :196-209, or the no-ratio test at :48 / :84).
@@ -19,7 +20,57 @@ namespace v3dm {
 
 namespace {
 
-// List pass: one warp per segment; every unit best that is not the descriptor's overall
+// Chunk records of a side pass: the exact lane-local work the side kernel leaves out.  For
+// every score >= Smin the gates decide whether it is a candidate; the chunk best is the
+// largest candidate (first column on ties), every other score of the chunk (candidates,
+// masked scores and scores below Smin alike) bounds the second value.  The best goes to
+// best[] and, as one entry per record, to the list the next pass reads.
+__global__ void k_records(PostArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
+    const int cnt = a.segCount[seg];
+    const long long n = cnt < a.segCap ? cnt : a.segCap;
+    const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
+    unsigned long long* entries = a.list + (long long)seg * a.segCap;
+    for (long long i = lane; i < n; i += 32) {
+      const uint4* rec = recs + i * kRecordQuads;
+      const uint4 head = rec[0];
+      const int orig = (int)head.x, col0 = (int)head.y;
+      unsigned long long cb = 0;
+      uint32_t cw = 0;
+      for (int k = 0; k < 8; ++k) {
+        const uint4 q = rec[1 + k];
+        const uint32_t sv[4] = {q.x, q.y, q.z, q.w};
+        for (int t = 0; t < 4; ++t) {
+          const int col = col0 + 4 * k + t;
+          if (col >= a.nB) break;
+          const int32_t S = (int32_t)sv[t];
+          bool strong = S >= a.Smin;
+          for (int gi = 0; gi < a.nGates && strong; ++gi)
+            strong = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
+          if (strong) {
+            const unsigned long long key = best_key(S, col);
+            if (key > cb) {
+              cw = max(cw, (uint32_t)(cb >> kIndexBits));
+              cb = key;
+            } else {
+              cw = max(cw, (uint32_t)(S + 1));
+            }
+          } else {
+            cw = max(cw, (uint32_t)(S + 1));
+          }
+        }
+      }
+      if (cb) atomicMax(&a.best[orig], cb);
+      if (cw) atomicMax(&a.sec[orig], cw);
+      entries[i] = cb ? ((unsigned long long)(uint32_t)orig | (cb << kIndexBits)) : 0ull;
+    }
+  }
+}
+
+// List pass: one warp per segment; every chunk best that is not the descriptor's overall
 // best raises its second value.  Segment counts are cleared for the next pass.
 __global__ void k_list(PostArgs a, int32_t* info) {
   const int lane = threadIdx.x & 31;
@@ -36,6 +87,7 @@ __global__ void k_list(PostArgs a, int32_t* info) {
     const unsigned long long* e = a.list + (long long)seg * a.segCap;
     for (long long i = lane; i < n; i += 32) {
       const unsigned long long x = e[i];
+      if (x == 0) continue;  // record without a candidate
       const int idx = (int)(x & kIndexMask);
       const unsigned long long key = x >> kIndexBits;
       if (key != a.best[idx]) atomicMax(&a.sec[idx], (unsigned)(key >> kIndexBits));
@@ -228,6 +280,9 @@ k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
   int32_t* info = a.err - kInfoErr;
   const int listBlocks = (a.nSeg * 32 + 255) / 256;
+  k_records<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a);
+  cudaError_t e0 = cudaGetLastError();
+  if (e0 != cudaSuccess) return e0;
   k_list<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, info);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
