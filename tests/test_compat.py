@@ -1,0 +1,92 @@
+"""The C++ compat header (the reference's V3D_CUDA class surface) compiles, links and matches
+the oracle, including the reference's rounding of feature counts to multiples of 32
+(V3D/CUDA/v3d_cudamatching.cu:444-519) and traverseTree's clamping (.cu:791-797)."""
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG, ROOT
+from v3dm import synth
+
+SRC = ROOT / "tests" / "compat_main.cpp"
+
+
+@pytest.fixture(scope="module")
+def compat_bin(tmp_path_factory, v3dm_mod):
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    out = tmp_path_factory.mktemp("compat") / "compat_main"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", str(PKG / "compat"), "-I", str(ROOT / "include"),
+           str(SRC), "-o", str(out), "-L", str(PKG), "-lv3dm", f"-Wl,-rpath,{PKG}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return out
+
+
+def _run(bin_path, mode, payload, tmp_path):
+    fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
+    fin.write_bytes(payload)
+    p = subprocess.run([str(bin_path), mode, str(fin), str(fout)], capture_output=True, text=True, timeout=600)
+    return p, fout
+
+
+def _match_payload(L, R, lp, rp, F, min_score, min_ratio, thr):
+    head = struct.pack("<iifff", L.shape[0], R.shape[0], min_score, min_ratio, thr)
+    return b"".join([head, np.asarray(F, np.float64).tobytes(), (L.astype(np.float32) / 512).tobytes(),
+                     (R.astype(np.float32) / 512).tobytes(), lp.astype(np.float32).tobytes(),
+                     rp.astype(np.float32).tobytes()])
+
+
+def _read_pairs(buf, off):
+    n = struct.unpack_from("<i", buf, off)[0]
+    pairs = np.frombuffer(buf, np.int32, 2 * n, off + 4).reshape(n, 2)
+    return pairs, off + 4 + 8 * n
+
+
+def test_header_compiles_and_links(compat_bin):
+    assert compat_bin.exists()
+
+
+def test_fails_loudly_without_gpu(compat_bin, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L, R, lp, rp, F, _ = synth.stereo(5, 64, 64)
+    p, _ = _run(compat_bin, "match", _match_payload(L, R, lp, rp, F, 0.7, 0.8, 2.0), tmp_path)
+    assert p.returncode == 1
+    assert "V3D_CUDA SIFT_Matching(): no sm_100 CUDA device" in p.stderr
+
+
+@pytest.mark.gpu
+def test_match_sequence_calls(compat_bin, oracle_mod, tmp_path):
+    """1000 x 1037 features: the header rounds both down (992, 1024) as the reference does."""
+    L, R, lp, rp, F, _ = synth.stereo(11, 1000, 1037)
+    p, fout = _run(compat_bin, "match", _match_payload(L, R, lp, rp, F, 0.7, 0.8, 2.0), tmp_path)
+    assert p.returncode == 0, p.stderr
+    buf = fout.read_bytes()
+    put, off = _read_pairs(buf, 0)
+    gui, off = _read_pairs(buf, off)
+    assert off == len(buf)
+    nl, nr = 992, 1024
+    np.testing.assert_array_equal(put, oracle_mod.match(L[:nl], R[:nr], 0.7, 0.8))
+    exp = oracle_mod.match(L[:nl], R[:nr], 0.7, 0.8, gates=[("F", F, 2.0)], lpos=lp[:nl], rpos=rp[:nr])
+    np.testing.assert_array_equal(gui, exp)
+    assert put.shape[0] > 100 and gui.shape[0] > 100
+
+
+@pytest.mark.gpu
+def test_match_using_voctree_calls(compat_bin, v3dm_mod, oracle_mod, tmp_path):
+    """VocabularyTreeTraversal<10, 3>: 1000 keys, allocate rounds to 992, traverseTree clamps."""
+    rng = synth.rng_for(21)
+    nodes = synth.sift_like(rng, v3dm_mod.voctree_counts(10, 3)[0])
+    keys = synth.sift_like(rng, 1000)
+    payload = b"".join([struct.pack("<i", 1000), (nodes.astype(np.float32) / 512).tobytes(),
+                        (keys.astype(np.float32) / 512).tobytes()])
+    p, fout = _run(compat_bin, "voctree", payload, tmp_path)
+    assert p.returncode == 0, p.stderr
+    assert "Reducing nFeatures" in p.stderr
+    ids = np.frombuffer(fout.read_bytes(), np.int32)
+    np.testing.assert_array_equal(ids[:992], oracle_mod.voctree(10, 3, nodes, keys[:992], True))
+    assert np.all(ids[992:] == -1)
