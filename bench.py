@@ -303,7 +303,7 @@ def run_stereo(args, ws, rank, local):
     int8_peak = 2.0 * peaks["bf16_tflops"]  # kind::i8 runs at twice the kind::f16 rate
     ops_per_launch = 2.0 * N_SIDE * N_SIDE * 128
     achieved = ops_per_launch / (k_avg_ms * 1e-3) / 1e12
-    traffic = traffic_from_profiles("match_tc" if args.kernel == "tcgen05" else "match_simt")
+    traffic = traffic_from_profiles("k_side" if args.kernel == "tcgen05" else "k_match_simt")
     line = {
         "metric": "image pairs/s (16384x16384 putative + F-guided)", "value": ws * 1000.0 / ms, "unit": "pairs/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

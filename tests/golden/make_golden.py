@@ -1,0 +1,111 @@
+"""Writes the golden fixtures of tests/golden/ from the reference's own code.
+
+    python tests/golden/make_golden.py voctree [outdir]   # CPU: V3D::VocabularyTree::getVisualWord
+    python tests/golden/make_golden.py match [outdir]     # GPU: V3D_CUDA::SIFT_Matching
+
+voctree: the reference's CPU vocabulary tree (V3D/Base/v3d_vocabularytree.h, built from the
+reference headers into oracle/_ref/libv3dref_voctree.so by `make -C oracle ref`), leaf-local
+ids, for every tree shape the wrapper instantiates that is small enough to store.
+match: the reference's CUDA matcher (V3D/CUDA/v3d_cudamatching.cu, built unmodified into
+oracle/_ref/libv3dref_cuda.so) on an sm_100 GPU: putative matching with and without the ratio
+test, guided F matching and compounding F + H gates, and a case with duplicated descriptors.
+
+Inputs are SIFT-like uint8 descriptors (values u/512 handed to the reference as floats) from
+v3dm.synth, stored in the fixtures together with the outputs, so the fixtures stand alone.
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT / "eth-v3d-lgpl_b200"))
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle  # noqa: E402
+from v3dm import synth  # noqa: E402
+
+# (branch factor, depth, number of keys); shapes instantiated in oracle/ref_voctree_wrap.cpp
+VOCTREE_CASES = [(2, 1, 100), (3, 2, 150), (4, 3, 250), (5, 4, 250), (10, 2, 250), (10, 3, 200)]
+
+H_GATE = np.array([[1.0, 0.01, 25.0], [0.0, 1.0, 3.0], [0.0, 0.0, 1.0]])
+
+
+def make_voctree(out: Path) -> None:
+    if not oracle.ref_voctree_available():
+        raise SystemExit("oracle/_ref/libv3dref_voctree.so missing: run `make -C oracle ref` first")
+    arrays = {}
+    for i, (bf, depth, n) in enumerate(VOCTREE_CASES):
+        rng = synth.rng_for(1000 + i)
+        n_nodes = sum(bf ** d for d in range(1, depth + 1))
+        nodes = synth.sift_like(rng, n_nodes)
+        keys = synth.sift_like(rng, n)
+        ids = oracle.ref_voctree(bf, depth, nodes.astype(np.float32) / 512, keys.astype(np.float32) / 512)
+        arrays[f"c{i}_shape"] = np.array([bf, depth], np.int32)
+        arrays[f"c{i}_nodes"] = nodes
+        arrays[f"c{i}_keys"] = keys
+        arrays[f"c{i}_leaf_local"] = ids
+    arrays["n_cases"] = np.array(len(VOCTREE_CASES), np.int32)
+    np.savez_compressed(out / "voctree_ref.npz", **arrays)
+    print("wrote", out / "voctree_ref.npz")
+
+
+def _tie_pair():
+    """Left and right sets with exact duplicates: ties in the best and second-best scores."""
+    rng = synth.rng_for(77)
+    base = synth.sift_like(rng, 160)
+    L = np.concatenate([base[:128], base[:64], base[128:160]])  # lefts 128..191 repeat lefts 0..63
+    R = np.concatenate([base[32:96], base[32:64], synth.sift_like(rng, 64), base[100:132]])
+    return L.copy(), R.copy()
+
+
+def make_match(out: Path) -> None:
+    if not oracle.ref_cuda_available():
+        raise SystemExit("oracle/_ref/libv3dref_cuda.so missing: run `make -C oracle ref` first")
+    arrays = {}
+    cases = []
+    L, R, _ = synth.pair(10, 512, 480)
+    arrays["pair_L"], arrays["pair_R"] = L, R
+    for ms, mr in ((0.7, 0.8), (0.9, 0.8), (0.7, -1.0), (0.8, 0.6)):
+        cases.append(("pair", ms, mr, []))
+    L, R, lp, rp, F, _ = synth.stereo(12, 512, 544)
+    arrays["stereo_L"], arrays["stereo_R"] = L, R
+    arrays["stereo_lpos"], arrays["stereo_rpos"], arrays["stereo_F"] = lp, rp, F
+    arrays["stereo_H"] = H_GATE
+    cases.append(("stereo", 0.7, 0.8, []))
+    cases.append(("stereo", 0.7, 0.8, [("F", 2.0)]))
+    cases.append(("stereo", 0.7, -1.0, [("F", 2.0)]))
+    cases.append(("stereo", 0.7, 0.8, [("H", 300.0)]))
+    cases.append(("stereo", 0.7, 0.8, [("F", 4.0), ("H", 600.0)]))
+    L, R = _tie_pair()
+    arrays["ties_L"], arrays["ties_R"] = L, R
+    for ms, mr in ((0.7, 0.8), (0.7, -1.0)):
+        cases.append(("ties", ms, mr, []))
+    for i, (inp, ms, mr, gates) in enumerate(cases):
+        Li, Ri = arrays[f"{inp}_L"], arrays[f"{inp}_R"]
+        g = [(t, arrays[f"{inp}_{t}"], thr) for t, thr in gates]
+        kw = {}
+        if gates:
+            kw = dict(lpos=arrays[f"{inp}_lpos"], rpos=arrays[f"{inp}_rpos"])
+        pairs = oracle.ref_cuda_match(Li, Ri, ms, mr, gates=g, **kw)
+        arrays[f"c{i}_input"] = np.array(inp)
+        arrays[f"c{i}_params"] = np.array([ms, mr], np.float32)
+        arrays[f"c{i}_gates"] = np.array([f"{t}:{thr!r}" for t, thr in gates])
+        arrays[f"c{i}_pairs"] = pairs.astype(np.int32)
+        print(f"case {i}: {inp} ms={ms} mr={mr} gates={gates} -> {pairs.shape[0]} pairs")
+    arrays["n_cases"] = np.array(len(cases), np.int32)
+    np.savez_compressed(out / "match_ref.npz", **arrays)
+    print("wrote", out / "match_ref.npz")
+
+
+def main(argv):
+    if len(argv) < 2 or argv[1] not in ("voctree", "match"):
+        raise SystemExit(__doc__)
+    out = Path(argv[2]) if len(argv) > 2 else HERE
+    out.mkdir(parents=True, exist_ok=True)
+    (make_voctree if argv[1] == "voctree" else make_match)(out)
+
+
+if __name__ == "__main__":
+    main(sys.argv)
