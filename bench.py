@@ -6,7 +6,8 @@ Default workload (one step): putative matching followed by F-guided matching (2 
 guided pair.  Metric: image pairs per second.  `value` times the steps with descriptors and
 positions resident in HBM (device-output C-ABI calls); `e2e` times the same step through the
 host C-ABI calls (pinned host buffers in, host pairs out, copies inside the timed region).
-Other workloads (--workload pair | voctree) exist for exploration; the default line is the
+Other workloads: --workload batch (all 19,900 pairs of 200 images in one batched call) and
+--workload voctree (2M descriptors through a BF 10, depth 6 tree); the default line is the
 stereo one.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -44,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "pair", "voctree"], default="stereo")
+    ap.add_argument("--workload", choices=["stereo", "batch", "voctree"], default="stereo")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
@@ -333,6 +334,233 @@ def run_stereo(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, ws, rank, local):
+    """All 19,900 pairs of 200 synthetic images (1000..12000 features, 15% shared tracks),
+    minScore 0.7, ratio 0.8: one batched call per step (two persistent side-pass launches,
+    replayed as a CUDA graph)."""
+    import torch
+
+    import v3dm
+    from v3dm import synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    desc, counts, offs = synth.images(args.seed + 1)
+    b = v3dm.BatchMatching(local)
+    b.set_images(desc, counts)
+    b.set_pairs(None)
+    ops, n_pairs = b.work()
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    if args.tile_config < 0:
+        cfg, sch, tune_ms = b.autotune(MIN_SCORE, MIN_RATIO, 1)
+    else:
+        b.set_config(args.tile_config, 0)
+    cfg, sch = b.config()
+    d_cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+        while b.wait() == v3dm.ERR_CANDIDATES:  # buffers grown: repeat
+            b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+        ev[i][1].record(stream)
+        launches += b.last_launches()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    assert b.wait() == v3dm.OK
+    ms = max_over_ranks(ws, statistics.mean(a.elapsed_time(c) for a, c in ev), dev)
+    n_out = int(d_cnt.item())
+    # pass timing with events (a separate run without the graph)
+    b.profile(True)
+    for _ in range(3):
+        b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+        assert b.wait() == v3dm.OK
+    ka, na = b.profile_read(0)
+    kb, nb = b.profile_read(1)
+    b.profile(False)
+    # e2e: images from pinned host memory, triples back to the host
+    desc_p = torch.from_numpy(desc).pin_memory().numpy()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for _ in range(2):
+        b.set_images(desc_p, counts)
+        b.match(MIN_SCORE, MIN_RATIO)
+    barrier(ws)
+    torch.cuda.synchronize()
+    n_host = 0
+    for i in range(args.steps):
+        ev2[i][0].record(stream)
+        b.set_images(desc_p, counts)
+        n_host = b.match(MIN_SCORE, MIN_RATIO).shape[0]
+        ev2[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(c) for a, c in ev2), dev)
+    b.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    k_ms = ka / max(na, 1)
+    achieved = ops / (k_ms * 1e-3) / 1e12
+    line = {
+        "metric": "image pairs/s (all 19,900 pairs of 200 images)", "value": ws * n_pairs * 1000.0 / ms,
+        "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "200 images, 1000..12000 uint8 SIFT-like features each, 15% shared tracks, all "
+                               "19,900 pairs, minScore 0.7, ratio 0.8", "pairs": n_pairs,
+                   "descriptors": int(counts.sum()), "seed": args.seed + 1,
+                   "l2": "inputs larger than L2 (166 MB of descriptors, 2 GB of per-pair state)"},
+        "aggregate_int8_tops": ops / (ms * 1e-3) / 1e12,
+        "tile": {"config": cfg, "schedule": sch, "chosen_by": "autotune" if args.tile_config < 0 else "flag"},
+        "pairs_found": n_out,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",
+                     "frac": achieved / int8_peak, "traffic": traffic_from_profiles("k_side_batch"),
+                     "peak_src": f"2 x {peaks['src']} bf16 dense ({peaks['bf16_tflops']} TFLOP/s burst)",
+                     "kernel_ms": k_ms, "ops_per_launch": ops, "kernel": "k_side pass A (every pair)",
+                     "pass_b_ms": kb / max(nb, 1)},
+        "e2e": {"value": ws * n_pairs * 1000.0 / ms_e2e, "unit": "pairs/s",
+                "h2d_bytes_per_step": int(desc.nbytes), "d2h_bytes_per_step": int(n_host * 12 + 48)},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        pairs = synth.all_pairs(len(counts))
+        rng = np.random.default_rng(0)
+        sample = rng.choice(len(pairs), 12, replace=False)
+        t0 = time.perf_counter()
+        s_ops = 0
+        for k in sample:
+            i, j = pairs[k]
+            oracle.match(desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]], MIN_SCORE, MIN_RATIO)
+            s_ops += 2 * 128 * int(counts[i]) * int(counts[j])
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n_pairs / (dt * ops / s_ops), "unit": "pairs/s",
+                                "cores": oracle.num_threads(), "kind": "port",
+                                "sample": "12 random pairs of the 19,900, extrapolated by int8 operations"}
+    print(json.dumps(line), flush=True)
+
+
+def run_voctree(args, ws, rank, local):
+    """Vocabulary-tree quantization: BF 10, depth 6 (1,111,110 nodes without the root, HKM
+    centres from 500k descriptors), 2,000,000 query descriptors.  Per-level figures come from
+    the same kernel on the depth-d prefix trees (breadth-first order makes the first d levels a
+    tree of depth d)."""
+    import torch
+
+    import v3dm
+    from v3dm import synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    bf, depth, n = 10, 6, 2_000_000
+    nodes, keys = synth.voctree(args.seed + 2, bf, depth, 500_000, n)
+    t = v3dm.VocabularyTreeTraversal(bf, depth, local)
+    t.allocate(n)
+    t.set_nodes(nodes)
+    stream = torch.cuda.ExternalStream(t.stream(), device=dev)
+    d_keys = torch.from_numpy(keys).to(dev)
+    d_ids = torch.empty(n, dtype=torch.int32, device=dev)
+
+    def timed(tree, steps):
+        s = torch.cuda.ExternalStream(tree.stream(), device=dev)
+        for _ in range(max(args.warmup, 3)):
+            tree.quantize_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        for a, c in evs:
+            a.record(s)
+            tree.quantize_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+            c.record(s)
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(c) for a, c in evs)
+
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = Clocks(local)
+    ms = max_over_ranks(ws, timed(t, args.steps), dev)
+    clk = clocks.stop()
+    ids = d_ids.cpu().numpy()
+    # per level: the same kernel on the depth-d prefix trees
+    level_ms, prev = [], 0.0
+    for d in range(1, depth + 1):
+        if d == depth:
+            td = ms
+        else:
+            tr = v3dm.VocabularyTreeTraversal(bf, d, local)
+            tr.allocate(n)
+            tr.set_nodes(nodes[: v3dm.voctree_counts(bf, d)[0]])
+            td = timed(tr, args.steps)
+            tr.close()
+        level_ms.append(td - prev)
+        prev = td
+    # e2e: keys from pinned host memory, ids back to the host
+    kp = torch.from_numpy(keys).pin_memory().numpy()
+    for _ in range(2):
+        t.traverse_tree(kp)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for a, c in ev2:
+        a.record(stream)
+        t.traverse_tree(kp)
+        c.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(c) for a, c in ev2), dev)
+    t.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    node_bytes = nodes.shape[0] * 128
+    alg_bytes = n * 128 + n * 4 + node_bytes
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    level_bytes = n * bf * 128
+    line = {
+        "metric": "descriptors/s (vocabulary-tree quantization, BF 10, depth 6)", "value": ws * n * 1000.0 / ms,
+        "unit": "desc/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "voctree BF 10 depth 6 (1,111,110 HKM nodes from 500k descriptors), 2,000,000 "
+                               "uint8 SIFT-like queries", "seed": args.seed + 2,
+                   "l2": "inputs larger than L2 (256 MB of keys, 142 MB of nodes)"},
+        "per_level": [{"level": d + 1, "ms": level_ms[d], "gathered_GBps": level_bytes / (level_ms[d] * 1e-3) / 1e9
+                       if level_ms[d] > 0 else None} for d in range(depth)],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profiles("k_voctree"),
+                     "peak_src": f"{peaks['src']} copy bandwidth",
+                     "bytes_per_launch": alg_bytes, "kernel": "k_voctree (all levels, one launch)"},
+        "e2e": {"value": ws * n * 1000.0 / ms_e2e, "unit": "desc/s", "h2d_bytes_per_step": int(keys.nbytes),
+                "d2h_bytes_per_step": int(n * 4)},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        sample = 200_000
+        kf = keys[:sample].astype(np.float32) / 512
+        nf = nodes.astype(np.float32) / 512
+        if oracle.ref_voctree_available():
+            t0 = time.perf_counter()
+            ref = oracle.ref_voctree(bf, depth, nf, kf)
+            dt = time.perf_counter() - t0
+            kind = "reference"
+            line["parity_sample"] = bool(np.array_equal(ref + sum(bf ** k for k in range(1, depth)),
+                                                        ids[:sample]))
+        else:
+            t0 = time.perf_counter()
+            oracle.voctree(bf, depth, nodes, keys[:sample], True)
+            dt = time.perf_counter() - t0
+            kind = "port"
+        line["cpu_baseline"] = {"value": sample / dt, "unit": "desc/s", "cores": oracle.num_threads(), "kind": kind,
+                                "sample": f"first {sample} of the 2,000,000 queries"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -341,8 +569,10 @@ def main():
             run_reference_arm(args, ws, rank)
         elif args.workload == "stereo":
             run_stereo(args, ws, rank, local)
-        else:
-            raise SystemExit(f"workload {args.workload} is not wired into this bench yet")
+        elif args.workload == "batch":
+            run_batch(args, ws, rank, local)
+        elif args.workload == "voctree":
+            run_voctree(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

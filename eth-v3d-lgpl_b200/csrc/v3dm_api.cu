@@ -75,8 +75,7 @@ namespace {
 thread_local char g_lastError[256] = "";
 
 int cuda_fail(cudaError_t e, const char* what, int line) {
-  std::snprintf(g_lastError, sizeof(g_lastError), "%s (%s) at v3dm_api.cu:%d: %s", cudaGetErrorName(e),
-                cudaGetErrorString(e), line, what);
+  record_cuda_error(e, "v3dm_api.cu", line, what);
   return V3DM_ERR_CUDA;
 }
 
@@ -250,6 +249,13 @@ int compute_threshold(float minScore, float minRatio, bool gated, int32_t* Tout)
 }
 
 }  // namespace
+
+int32_t v3dm::host_smallest_passing_score(float minScore) { return smallest_passing_score(minScore); }
+
+void v3dm::record_cuda_error(cudaError_t e, const char* file, int line, const char* what) {
+  std::snprintf(g_lastError, sizeof(g_lastError), "%s (%s) at %s:%d: %s", cudaGetErrorName(e), cudaGetErrorString(e),
+                file, line, what);
+}
 
 int v3dm::host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T) {
   ThrKey k;

@@ -1,0 +1,1154 @@
+// v3dm_batch.cu -- many image pairs matched with one persistent launch per side pass.
+//
+// The SfM apps match pairs one at a time (V3D/Apps/SfM/match_sequence.cpp:165-234): upload the
+// left image, then for every right image upload it and call findPutativeMatches.  Here every
+// pair's result is exactly that call's result (same rules, same order), but all pairs of a
+// batch run together:
+//   - the images live once in HBM, each padded with zero descriptors to a multiple of 256
+//     rows (a zero descriptor scores 0, which is <= every real score, so it never changes a
+//     chunk maximum);
+//   - pass A is one k_side launch over a row table with one row per (pair, group of 128 or 256
+//     lefts): the group against every tile of the pair's right image.  The state (best key,
+//     second bound, decision) is kept per (pair, left) in HBM;
+//   - every accepted left names one right.  Those rights (one per accepted left) are gathered
+//     per left image, so one pass-B row scores a group of them, from all pairs of that left
+//     image, against the left image;
+//   - pass B is one k_side launch over that row table.  Its decisions are the reference's row
+//     maxima (v3d_cudamatching.cu:164-210) for exactly the rights the mutual filter reads
+//     (.cu:546-551);
+//   - mutual filter and an ordered compaction into (pair, left, right) triples, grouped by pair
+//     (pairs in order of their left image, then table order), ascending left within a pair.
+// Every launch after the first reads its sizes from device memory, so the whole sequence is
+// captured once as a CUDA graph and replayed while the images, pairs and parameters stay the same.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "v3dm_device.cuh"
+
+namespace v3dm {
+
+namespace {
+
+struct BPair {          // one pair, in the batch's order (sorted by left image)
+  int li, ri;           // left and right image
+  int orig;             // index in the caller's pair table
+  int nL;               // descriptors of the left image
+  long long stateA0;    // first pass-A state of the pair
+};
+
+struct BImage {         // one image
+  int rowOff;           // first row in the padded image buffer
+  int n;                // descriptors
+  int pairBeg, pairEnd; // pairs (batch order) whose left image this is
+};
+
+struct BImageB {        // pass-B layout of one left image (written by k_bscan)
+  int cB;               // accepted lefts over all of its pairs
+  int padBase;          // first row of its chosen rights in the pass-B operand buffer
+  int rowStart;         // its first row in the pass-B row table
+  int pad;
+  long long stateB0;    // its first pass-B state
+};
+
+// Counter words of a batch call.
+constexpr int kCntStates = 0;     // pass-B states (0 after an overflow)
+constexpr int kCntRowsB = 1;      // pass-B rows (0 after an overflow)
+constexpr int kCntOverflow = 2;   // 1: pass-B buffers too small
+constexpr int kCntOut = 3;        // triples written
+constexpr int kCntNeedStates = 4; // sizes the pass-B buffers need
+constexpr int kCntNeedRows = 5;
+constexpr int kCntNeedTable = 6;
+constexpr int kCntWords = 8;
+
+constexpr int kScanThreads = 1024;
+constexpr int kChooseThreads = 256;
+constexpr int kBMutThreads = 256;
+constexpr int kBMutPerBlock = 2048;
+
+// Copies each image's descriptors to its padded place and zeroes its padding rows.
+__global__ void k_bscatter(const uint8_t* __restrict__ src, const long long* __restrict__ srcOff,
+                           const BImage* __restrict__ im, int nImages, uint8_t* __restrict__ dst) {
+  for (int i = blockIdx.x; i < nImages; i += gridDim.x) {
+    const BImage m = im[i];
+    const long long nq = (long long)m.n * (kDescBytes / 16);
+    const long long pq = (long long)((m.n + 255) & ~255) * (kDescBytes / 16);
+    const uint4* s = reinterpret_cast<const uint4*>(src + srcOff[i] * kDescBytes);
+    uint4* d = reinterpret_cast<uint4*>(dst + (size_t)m.rowOff * kDescBytes);
+    for (long long k = threadIdx.x; k < pq; k += blockDim.x) d[k] = k < nq ? s[k] : make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
+// Accepted lefts of every pair.
+__global__ void __launch_bounds__(kChooseThreads)
+k_bcount(const BPair* __restrict__ pairs, int nPairs, const int32_t* __restrict__ decA, int* __restrict__ cnt) {
+  __shared__ int wsum[kChooseThreads / 32];
+  for (int p = blockIdx.x; p < nPairs; p += gridDim.x) {
+    const BPair q = pairs[p];
+    int c = 0;
+    for (int l = threadIdx.x; l < q.nL; l += kChooseThreads) c += decA[q.stateA0 + l] >= 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < kChooseThreads / 32; ++w) t += wsum[w];
+      cnt[p] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Exclusive prefix sums of val(0..n-1), handed to out(i, prefix); returns the total.  One block.
+template <class V, class O>
+__device__ long long block_scan(int n, V val, O out, long long* sh) {
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int per = (n + T - 1) / T;
+  const int b = min(n, tid * per), e = min(n, b + per);
+  long long s = 0;
+  for (int i = b; i < e; ++i) s += val(i);
+  sh[tid] = s;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    const long long v = tid >= o ? sh[tid - o] : 0;
+    __syncthreads();
+    sh[tid] += v;
+    __syncthreads();
+  }
+  const long long total = sh[T - 1];
+  long long run = sh[tid] - s;
+  for (int i = b; i < e; ++i) {
+    const long long v = val(i);
+    out(i, run);
+    run += v;
+  }
+  __syncthreads();
+  return total;
+}
+
+// Pass-B layout: state and row offsets per pair and per left image, and the pass-B row table.
+// One block.  When a buffer is too small it records the sizes needed and leaves pass B empty.
+__global__ void __launch_bounds__(kScanThreads)
+k_bscan(const int* __restrict__ cnt, int nPairs, const BImage* __restrict__ im, int nImages, int GM, int BN,
+        long long capStates, long long capRows, long long capTable, long long* __restrict__ prefC,
+        BImageB* __restrict__ imgB, BatchRow* __restrict__ rowsB, int* __restrict__ counters) {
+  __shared__ long long sh[kScanThreads];
+  const long long SB = block_scan(
+      nPairs, [&](int i) { return (long long)cnt[i]; }, [&](int i, long long x) { prefC[i] = x; }, sh);
+  if (threadIdx.x == 0) prefC[nPairs] = SB;
+  __syncthreads();
+  auto chosen = [&](int i) { return prefC[im[i].pairEnd] - prefC[im[i].pairBeg]; };
+  const long long padTotal = block_scan(
+      nImages, [&](int i) { return (chosen(i) + GM - 1) / GM * GM; },
+      [&](int i, long long x) { imgB[i].padBase = (int)min(x, (long long)0x7fffffff); }, sh);
+  const long long rowTotal = block_scan(
+      nImages, [&](int i) { return (chosen(i) + GM - 1) / GM; },
+      [&](int i, long long x) {
+        imgB[i].rowStart = (int)min(x, (long long)0x7fffffff);
+        imgB[i].cB = (int)min(chosen(i), (long long)0x7fffffff);
+        imgB[i].stateB0 = prefC[im[i].pairBeg];
+      },
+      sh);
+  const bool over = SB > capStates || padTotal > capRows || rowTotal > capTable;
+  if (threadIdx.x == 0) {
+    counters[kCntStates] = over ? 0 : (int)SB;
+    counters[kCntRowsB] = over ? 0 : (int)rowTotal;
+    counters[kCntOverflow] = over ? 1 : 0;
+    counters[kCntNeedStates] = (int)min(SB, (long long)0x7fffffff);
+    counters[kCntNeedRows] = (int)min(padTotal, (long long)0x7fffffff);
+    counters[kCntNeedTable] = (int)min(rowTotal, (long long)0x7fffffff);
+  }
+  if (over) return;
+  for (int i = threadIdx.x; i < nImages; i += blockDim.x) {
+    const BImageB b = imgB[i];
+    const BImage m = im[i];
+    for (int g = 0; g * GM < b.cB; ++g) {
+      BatchRow r;
+      r.aRow = b.padBase + g * GM;
+      r.validRows = min(GM, b.cB - g * GM);
+      r.bRow0 = m.rowOff;
+      r.nB = m.n;
+      r.nTiles = (m.n + BN - 1) / BN;
+      r.pad = 0;
+      r.state0 = b.stateB0 + (long long)g * GM;
+      rowsB[b.rowStart + g] = r;
+    }
+  }
+}
+
+// Gathers, per pair and in ascending left order, the right named by every accepted left into
+// the pass-B operand buffer, with its (pair, left, right) identity.
+__global__ void __launch_bounds__(kChooseThreads)
+k_bchoose(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im,
+          const BImageB* __restrict__ imgB, const long long* __restrict__ prefC, const int32_t* __restrict__ decA,
+          const uint8_t* __restrict__ img, uint8_t* __restrict__ dAB, int* __restrict__ chosenLeft,
+          int* __restrict__ chosenRight, int* __restrict__ chosenPair, const int* __restrict__ counters) {
+  __shared__ int wsum[kChooseThreads / 32];
+  if (counters[kCntOverflow]) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int p = blockIdx.x; p < nPairs; p += gridDim.x) {
+    const long long s0 = prefC[p];
+    if (prefC[p + 1] == s0) continue;  // no accepted left (uniform over the block)
+    const BPair q = pairs[p];
+    const BImageB ib = imgB[q.li];
+    const long long rowBase = ib.padBase + (s0 - ib.stateB0);
+    const int rRowOff = im[q.ri].rowOff;
+    int run = 0;
+    for (int l0 = 0; l0 < q.nL; l0 += kChooseThreads) {
+      const int l = l0 + threadIdx.x;
+      const int d = l < q.nL ? decA[q.stateA0 + l] : -1;
+      const bool acc = d >= 0;
+      const unsigned m = __ballot_sync(0xffffffffu, acc);
+      if (lane == 0) wsum[w] = __popc(m);
+      __syncthreads();
+      int before = 0, tot = 0;
+#pragma unroll
+      for (int k = 0; k < kChooseThreads / 32; ++k) {
+        before += k < w ? wsum[k] : 0;
+        tot += wsum[k];
+      }
+      if (acc) {
+        const int k = run + before + __popc(m & ((1u << lane) - 1u));
+        const long long st = s0 + k;
+        chosenLeft[st] = l;
+        chosenRight[st] = d;
+        chosenPair[st] = q.orig;
+        const uint4* src = reinterpret_cast<const uint4*>(img + ((size_t)rRowOff + d) * kDescBytes);
+        uint4* dst = reinterpret_cast<uint4*>(dAB + (size_t)(rowBase + k) * kDescBytes);
+#pragma unroll
+        for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = src[x];
+      }
+      run += tot;
+      __syncthreads();
+    }
+  }
+}
+
+// Mutual filter over the pass-B states: state s is a match when the right's own decision
+// (decB[s]) names the left that chose it.  Pass 1: count per block of states.
+__global__ void __launch_bounds__(kBMutThreads)
+k_bmutual_count(const int* __restrict__ counters, const int32_t* __restrict__ decB, const int* __restrict__ chosenLeft,
+                int* __restrict__ blockCount) {
+  __shared__ int wsum[kBMutThreads / 32];
+  const int n = counters[kCntStates];
+  const int base = blockIdx.x * kBMutPerBlock;
+  int cnt = 0;
+  for (int s = base + threadIdx.x; s < min(base + kBMutPerBlock, n); s += kBMutThreads)
+    cnt += decB[s] == chosenLeft[s];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < kBMutThreads / 32; ++k) t += wsum[k];
+    blockCount[blockIdx.x] = t;
+  }
+}
+
+// Pass 2: ordered write of the (pair, left, right) triples.
+__global__ void __launch_bounds__(kBMutThreads)
+k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, const int* __restrict__ chosenLeft,
+                const int* __restrict__ chosenRight, const int* __restrict__ chosenPair,
+                const int* __restrict__ blockCount, int nBlocks, int3* __restrict__ out, int32_t* __restrict__ info) {
+  __shared__ int blockOff;
+  __shared__ int wsum[kBMutThreads / 32];
+  const int n = counters[kCntStates];
+  if (threadIdx.x < 32) {
+    int t = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += 32) t += blockCount[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) {
+      blockOff = t;
+      if (blockIdx.x == nBlocks - 1) {
+        counters[kCntOut] = t + blockCount[blockIdx.x];
+        info[kInfoPairs] = t + blockCount[blockIdx.x];
+      }
+    }
+  }
+  constexpr int kPer = kBMutPerBlock / kBMutThreads;
+  const int beg = blockIdx.x * kBMutPerBlock + threadIdx.x * kPer;
+  bool ok[kPer];
+  int cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int s = beg + i;
+    ok[i] = s < n && decB[s] == chosenLeft[s];
+    cnt += ok[i];
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int inc = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int k = 0; k < wid; ++k) before += wsum[k];
+  int off = blockOff + before + inc - cnt;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i)
+    if (ok[i]) {
+      const int s = beg + i;
+      out[off++] = make_int3(chosenPair[s], chosenLeft[s], chosenRight[s]);
+    }
+}
+
+}  // namespace
+
+}  // namespace v3dm
+
+using namespace v3dm;
+
+struct v3dm_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  TcPlan* tc = nullptr;
+  int schedule = 0;
+  // images
+  int nImages = 0;
+  std::vector<int> counts;
+  std::vector<long long> srcOff;   // first descriptor of each image in the caller's concatenation
+  std::vector<int> rowOff;         // first row of each image in the padded buffer
+  long long totalRows = 0;         // padded rows of all images
+  long long totalDesc = 0;
+  uint8_t* dImg = nullptr;
+  long long imgCap = 0;            // bytes
+  uint8_t* dStage = nullptr;
+  long long stageCap = 0;          // descriptors
+  long long* dSrcOff = nullptr;
+  BImage* dImages = nullptr;
+  int imagesCap = 0;
+  bool haveImages = false;
+  // pairs (batch order: stable sort by left image)
+  int nPairs = 0;
+  std::vector<int> pairLi, pairRi;  // caller's order
+  std::vector<BPair> bp;            // batch order
+  std::vector<BImage> bim;
+  BPair* dPairs = nullptr;
+  int pairsCap = 0;
+  long long SA = 0;                 // pass-A states
+  long long workOps = 0;            // sum over pairs of 2 * 128 * nL * nR
+  bool havePairs = false;
+  // pass A
+  BatchRow* dRowsA = nullptr;
+  long long rowsACap = 0;
+  int nRowsA = 0;
+  int rowsCfg = -1;                 // configuration the pass-A rows were built for
+  bool rowsDirty = true;
+  // per-state arrays (pass A states; pass B reuses the first SB entries of best/sec)
+  unsigned long long* dBest = nullptr;
+  unsigned int* dSec = nullptr;
+  int32_t* dDecA = nullptr;
+  long long stateCap = 0;
+  // chunk records of the side passes
+  uint4* dRecords = nullptr;
+  unsigned long long* dList = nullptr;
+  int* dSegCount = nullptr;
+  int nSeg = 0;
+  long long segCap = 0;
+  // pass B
+  int* dCnt = nullptr;
+  long long* dPrefC = nullptr;
+  BImageB* dImgB = nullptr;
+  uint8_t* dAB = nullptr;
+  BatchRow* dRowsB = nullptr;
+  int32_t* dDecB = nullptr;
+  int* dChosenLeft = nullptr;
+  int* dChosenRight = nullptr;
+  int* dChosenPair = nullptr;
+  int* dBlockCount = nullptr;
+  int3* dOut = nullptr;
+  long long capB = 0, capRowsB = 0, capTableB = 0;
+  // call state
+  int* dCounters = nullptr;
+  int32_t* dInfo = nullptr;
+  int32_t* hInfo = nullptr;         // pinned: info words then counter words
+  TcMaps mapsA, mapsB;
+  bool mapsValid = false;
+  int lastLaunches = 0;
+  // graph of one call
+  bool useGraph = true;
+  cudaGraphExec_t graph = nullptr;
+  uint32_t graphMs = 0, graphMr = 0;
+  int graphLaunches = 0;
+  bool pendingCheck = false;
+  // profiling
+  bool profile = false;
+  cudaEvent_t ev[4] = {};
+  double profMs[2] = {0.0, 0.0};
+  int profN[2] = {0, 0};
+  bool profPending = false;
+};
+
+namespace {
+
+int bfail(cudaError_t e, const char* what, int line) {
+  record_cuda_error(e, "v3dm_batch.cu", line, what);
+  return V3DM_ERR_CUDA;
+}
+
+#define V3DM_BTRY(expr)                                       \
+  do {                                                        \
+    cudaError_t e_ = (expr);                                  \
+    if (e_ != cudaSuccess) return bfail(e_, #expr, __LINE__); \
+  } while (0)
+
+struct BDeviceGuard {
+  int prev = -1;
+  explicit BDeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~BDeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+void bfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Ensures *p holds at least 'need' elements (contents are not kept).
+template <class T>
+cudaError_t ensure(T** p, long long* cap, long long need) {
+  if (need <= *cap && *p) return cudaSuccess;
+  bfree(*p);
+  *cap = 0;
+  long long n = need > 0 ? need : 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), (size_t)n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  *cap = n;
+  return cudaSuccess;
+}
+
+void drop_graph(v3dm_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+cudaError_t alloc_records(v3dm_batch* b, long long segCap) {
+  bfree(b->dRecords);
+  bfree(b->dList);
+  bfree(b->dSegCount);
+  b->segCap = 0;
+  const int nSeg = tc_segments(b->tc);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dRecords), (size_t)nSeg * segCap * kRecordQuads * sizeof(uint4));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->dList), (size_t)nSeg * segCap * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->dSegCount), (size_t)nSeg * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->dSegCount, 0, (size_t)nSeg * sizeof(int), b->stream);
+  if (e != cudaSuccess) return e;
+  b->nSeg = nSeg;
+  b->segCap = segCap;
+  return cudaSuccess;
+}
+
+// Pass-B buffers for capStates states.
+cudaError_t alloc_passB(v3dm_batch* b, long long capStates) {
+  int GM = 0, BN = 0;
+  tc_config_shape(tc_get_config(b->tc), &GM, &BN);
+  const long long capRows = capStates + (long long)b->nImages * 256 + 256;
+  const long long capTable = capStates / 128 + b->nImages + 1;
+  long long c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
+  bfree(b->dAB);
+  bfree(b->dRowsB);
+  bfree(b->dDecB);
+  bfree(b->dChosenLeft);
+  bfree(b->dChosenRight);
+  bfree(b->dChosenPair);
+  bfree(b->dBlockCount);
+  bfree(b->dOut);
+  b->capB = b->capRowsB = b->capTableB = 0;
+  cudaError_t e = ensure(&b->dAB, &c0, capRows * kDescBytes);
+  if (e == cudaSuccess) e = ensure(&b->dRowsB, &c1, capTable);
+  if (e == cudaSuccess) e = ensure(&b->dDecB, &c2, capStates);
+  if (e == cudaSuccess) e = ensure(&b->dChosenLeft, &c3, capStates);
+  if (e == cudaSuccess) e = ensure(&b->dChosenRight, &c4, capStates);
+  if (e == cudaSuccess) e = ensure(&b->dChosenPair, &c5, capStates);
+  if (e == cudaSuccess) e = ensure(&b->dBlockCount, &c6, capStates / kBMutPerBlock + 1);
+  if (e == cudaSuccess) e = ensure(&b->dOut, &c7, capStates);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->dAB, 0, (size_t)capRows * kDescBytes, b->stream);
+  if (e != cudaSuccess) return e;
+  b->capB = capStates;
+  b->capRowsB = capRows;
+  b->capTableB = capTable;
+  b->mapsValid = false;
+  return cudaSuccess;
+}
+
+// Pass-A rows for the current configuration.
+int build_rows(v3dm_batch* b) {
+  int GM = 0, BN = 0;
+  const int cfg = tc_get_config(b->tc);
+  tc_config_shape(cfg, &GM, &BN);
+  std::vector<BatchRow> rows;
+  for (const BPair& q : b->bp) {
+    const int nR = b->counts[q.ri];
+    if (q.nL == 0 || nR == 0) continue;
+    for (int g = 0; g * GM < q.nL; ++g) {
+      BatchRow r;
+      r.aRow = b->rowOff[q.li] + g * GM;
+      r.validRows = std::min(GM, q.nL - g * GM);
+      r.bRow0 = b->rowOff[q.ri];
+      r.nB = nR;
+      r.nTiles = (nR + BN - 1) / BN;
+      r.pad = 0;
+      r.state0 = q.stateA0 + (long long)g * GM;
+      rows.push_back(r);
+    }
+  }
+  if (rows.size() > 0x7fffffffULL) return V3DM_ERR_SIZE;
+  V3DM_BTRY(ensure(&b->dRowsA, &b->rowsACap, (long long)rows.size()));
+  if (!rows.empty())
+    V3DM_BTRY(cudaMemcpyAsync(b->dRowsA, rows.data(), rows.size() * sizeof(BatchRow), cudaMemcpyHostToDevice, b->stream));
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));  // 'rows' is pageable host memory
+  b->nRowsA = (int)rows.size();
+  b->rowsCfg = cfg;
+  b->rowsDirty = false;
+  b->mapsValid = false;
+  drop_graph(b);
+  return V3DM_OK;
+}
+
+int ensure_maps(v3dm_batch* b) {
+  if (b->mapsValid && b->mapsA.cfg == tc_get_config(b->tc)) return V3DM_OK;
+  V3DM_BTRY(tc_side_maps(b->tc, &b->mapsA, b->dImg, (int)b->totalRows, b->dImg, (int)b->totalRows));
+  V3DM_BTRY(tc_side_maps(b->tc, &b->mapsB, b->dAB, (int)b->capRowsB, b->dImg, (int)b->totalRows));
+  b->mapsValid = true;
+  return V3DM_OK;
+}
+
+// Enqueues one batch call (all launches read their sizes from device memory).
+int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents) {
+  int GM = 0, BN = 0;
+  tc_config_shape(tc_get_config(b->tc), &GM, &BN);
+  const int32_t Smin = host_smallest_passing_score(minScore);
+  int launches = 0;
+  V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntWords) * sizeof(int32_t), b->stream));
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.Smin = Smin;
+  sa.records = b->dRecords;
+  sa.segCount = b->dSegCount;
+  sa.segCap = b->segCap;
+  sa.nSeg = b->nSeg;
+  sa.err = b->dInfo + kInfoErr;
+  PostArgs pa;
+  std::memset(&pa, 0, sizeof(pa));
+  pa.records = b->dRecords;
+  pa.list = b->dList;
+  pa.segCount = b->dSegCount;
+  pa.segCap = b->segCap;
+  pa.nSeg = b->nSeg;
+  pa.Smin = Smin;
+  pa.minScore = minScore;
+  pa.minRatio = minRatio;
+  pa.best = b->dBest;
+  pa.sec = b->dSec;
+  pa.err = b->dInfo + kInfoErr;
+  // ---- pass A: every (pair, left group) against the pair's right image
+  sa.aIsLeft = 1;
+  sa.best = b->dBest;
+  sa.sec = b->dSec;
+  sa.rows = b->dRowsA;
+  sa.nRows = b->nRowsA;
+  sa.schedule = b->schedule;
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[0], b->stream));
+  V3DM_BTRY(launch_side_batch(b->tc, b->mapsA, sa, b->stream));
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[1], b->stream));
+  launches += b->nRowsA > 0;
+  pa.nRows = (int)b->SA;
+  pa.aIsLeft = 1;
+  pa.decision = b->dDecA;
+  V3DM_BTRY(launch_post(pa, b->stream));
+  launches += 3;
+  // ---- pass-B layout
+  const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
+  k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
+  V3DM_BTRY(cudaGetLastError());
+  k_bscan<<<1, kScanThreads, 0, b->stream>>>(b->dCnt, b->nPairs, b->dImages, b->nImages, GM, BN, b->capB,
+                                             b->capRowsB, b->capTableB, b->dPrefC, b->dImgB, b->dRowsB,
+                                             b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  k_bchoose<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, b->dImgB, b->dPrefC,
+                                                          b->dDecA, b->dImg, b->dAB, b->dChosenLeft, b->dChosenRight,
+                                                          b->dChosenPair, b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 3;
+  // ---- pass B: the rights the accepted lefts named, against their left image
+  sa.aIsLeft = 0;
+  sa.rows = b->dRowsB;
+  sa.nRowsPtr = b->dCounters + kCntRowsB;
+  sa.nRows = (int)std::min<long long>(b->capTableB, 0x7fffffff);
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
+  V3DM_BTRY(launch_side_batch(b->tc, b->mapsB, sa, b->stream));
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[3], b->stream));
+  pa.nRows = (int)std::min<long long>(b->capB, 0x7fffffff);
+  pa.rowsPtr = b->dCounters + kCntStates;
+  pa.aIsLeft = 0;
+  pa.decision = b->dDecB;
+  V3DM_BTRY(launch_post(pa, b->stream));
+  launches += 4;
+  // ---- mutual filter, ordered triples
+  const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
+  k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
+  V3DM_BTRY(cudaGetLastError());
+  k_bmutual_write<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft,
+                                                             b->dChosenRight, b->dChosenPair, b->dBlockCount,
+                                                             mutBlocks, b->dOut, b->dInfo);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 2;
+  V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntWords) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            b->stream));
+  b->lastLaunches = launches;
+  return V3DM_OK;
+}
+
+int prepare(v3dm_batch* b) {
+  if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->rowsDirty || b->rowsCfg != tc_get_config(b->tc)) {
+    int st = build_rows(b);
+    if (st != V3DM_OK) return st;
+  }
+  if (b->totalRows > 0) {
+    int st = ensure_maps(b);
+    if (st != V3DM_OK) return st;
+  }
+  V3DM_BTRY(tc_prepare_batch(b->tc, tc_get_config(b->tc)));
+  return V3DM_OK;
+}
+
+// One call: graph replay (or direct launches), then nothing else; the info block lands in
+// hInfo when the stream reaches it.
+int launch_call(v3dm_batch* b, float minScore, float minRatio) {
+  int st = prepare(b);
+  if (st != V3DM_OK) return st;
+  b->pendingCheck = true;
+  if (b->totalRows == 0 || b->nPairs == 0) {
+    V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntWords) * sizeof(int32_t), b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntWords) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                              b->stream));
+    b->lastLaunches = 0;
+    return V3DM_OK;
+  }
+  uint32_t ms, mr;
+  std::memcpy(&ms, &minScore, 4);
+  std::memcpy(&mr, &minRatio, 4);
+  if (b->profile) {
+    for (int i = 0; i < 4; ++i)
+      if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
+    st = enqueue_batch(b, minScore, minRatio, true);
+    if (st == V3DM_OK) b->profPending = true;
+    return st;
+  }
+  if (!b->useGraph) return enqueue_batch(b, minScore, minRatio, false);
+  if (!b->graph || b->graphMs != ms || b->graphMr != mr) {
+    drop_graph(b);
+    cudaGraph_t g = nullptr;
+    V3DM_BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    st = enqueue_batch(b, minScore, minRatio, false);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (st != V3DM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return bfail(e, "cudaStreamEndCapture", __LINE__);
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->graph = nullptr;
+      return bfail(e, "cudaGraphInstantiate", __LINE__);
+    }
+    b->graphMs = ms;
+    b->graphMr = mr;
+    b->graphLaunches = b->lastLaunches;
+  }
+  V3DM_BTRY(cudaGraphLaunch(b->graph, b->stream));
+  b->lastLaunches = b->graphLaunches;
+  return V3DM_OK;
+}
+
+// Waits for the last call and checks its info block.  Grows the buffers and returns
+// V3DM_ERR_CANDIDATES when a list or a pass-B buffer overflowed (the call must be repeated).
+int finish_call(v3dm_batch* b) {
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  b->pendingCheck = false;
+  if (b->profPending) {
+    float a = 0.f, c = 0.f;
+    V3DM_BTRY(cudaEventElapsedTime(&a, b->ev[0], b->ev[1]));
+    V3DM_BTRY(cudaEventElapsedTime(&c, b->ev[2], b->ev[3]));
+    b->profMs[0] += a;
+    b->profMs[1] += c;
+    ++b->profN[0];
+    ++b->profN[1];
+    b->profPending = false;
+  }
+  const int32_t* info = b->hInfo;
+  const int32_t* cnt = b->hInfo + kInfoWords;
+  if (info[kInfoErr] & kErrWaitTimeout) return V3DM_ERR_TIMEOUT;
+  if (info[kInfoErr]) return V3DM_ERR_CUDA;
+  bool grow = false;
+  if ((long long)info[kInfoMaxSeg] > b->segCap) {
+    long long cap = std::max<long long>(2 * b->segCap, (long long)info[kInfoMaxSeg] * 5 / 4 + 16);
+    V3DM_BTRY(alloc_records(b, cap));
+    grow = true;
+  }
+  if (cnt[kCntOverflow]) {
+    long long need = std::max<long long>((long long)cnt[kCntNeedStates] * 5 / 4 + 1024, 2 * b->capB);
+    V3DM_BTRY(alloc_passB(b, need));
+    b->mapsValid = false;
+    grow = true;
+  }
+  if (grow) {
+    drop_graph(b);
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+    return V3DM_ERR_CANDIDATES;
+  }
+  return V3DM_OK;
+}
+
+int run_host(v3dm_batch* b, float minScore, float minRatio) {
+  for (int attempt = 0; attempt < 6; ++attempt) {
+    int st = launch_call(b, minScore, minRatio);
+    if (st != V3DM_OK) return st;
+    st = finish_call(b);
+    if (st != V3DM_ERR_CANDIDATES) return st;
+  }
+  return V3DM_ERR_CANDIDATES;
+}
+
+void free_all(v3dm_batch* b) {
+  drop_graph(b);
+  bfree(b->dImg);
+  bfree(b->dStage);
+  bfree(b->dSrcOff);
+  bfree(b->dImages);
+  bfree(b->dPairs);
+  bfree(b->dRowsA);
+  bfree(b->dBest);
+  bfree(b->dSec);
+  bfree(b->dDecA);
+  bfree(b->dRecords);
+  bfree(b->dList);
+  bfree(b->dSegCount);
+  bfree(b->dCnt);
+  bfree(b->dPrefC);
+  bfree(b->dImgB);
+  bfree(b->dAB);
+  bfree(b->dRowsB);
+  bfree(b->dDecB);
+  bfree(b->dChosenLeft);
+  bfree(b->dChosenRight);
+  bfree(b->dChosenPair);
+  bfree(b->dBlockCount);
+  bfree(b->dOut);
+  b->dCounters = nullptr;  // points into dInfo
+  bfree(b->dInfo);
+  if (b->hInfo) cudaFreeHost(b->hInfo);
+  b->hInfo = nullptr;
+}
+
+// Layout of the images: padded row offsets, per-image table.
+int set_images(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* desc, bool onDevice) {
+  if (!b || nImages < 0 || (nImages > 0 && !counts)) return V3DM_ERR_ARG;
+  long long total = 0, rows = 0;
+  for (int i = 0; i < nImages; ++i) {
+    if (counts[i] < 0) return V3DM_ERR_ARG;
+    if (counts[i] > V3DM_MAX_FEATURES) return V3DM_ERR_SIZE;
+    total += counts[i];
+    rows += ((long long)counts[i] + 255) / 256 * 256;
+  }
+  if (total > 0 && !desc) return V3DM_ERR_ARG;
+  if (onDevice && (reinterpret_cast<uintptr_t>(desc) & 15)) return V3DM_ERR_ARG;
+  if (rows > 0x7fffff00LL) return V3DM_ERR_SIZE;
+  BDeviceGuard g(b->device);
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  // Same image sizes as before: the padded layout, the pair table and the row tables stay
+  // valid, only the descriptors change (the graph reads them from the same buffer).
+  const bool sameLayout = b->haveImages && nImages == b->nImages && std::equal(counts, counts + nImages, b->counts.begin());
+  if (sameLayout) {
+    if (total > 0) {
+      const uint8_t* src = desc;
+      if (!onDevice) {
+        V3DM_BTRY(ensure(&b->dStage, &b->stageCap, total * kDescBytes));
+        V3DM_BTRY(cudaMemcpyAsync(b->dStage, desc, (size_t)total * kDescBytes, cudaMemcpyHostToDevice, b->stream));
+        src = b->dStage;
+      }
+      k_bscatter<<<std::min(nImages, 1024), 256, 0, b->stream>>>(src, b->dSrcOff, b->dImages, nImages, b->dImg);
+      V3DM_BTRY(cudaGetLastError());
+    }
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+    return V3DM_OK;
+  }
+  drop_graph(b);
+  b->haveImages = false;
+  b->havePairs = false;  // pairs index the old images
+  b->nImages = nImages;
+  b->counts.assign(counts, counts + nImages);
+  b->srcOff.assign(nImages, 0);
+  b->rowOff.assign(nImages, 0);
+  long long so = 0, ro = 0;
+  for (int i = 0; i < nImages; ++i) {
+    b->srcOff[i] = so;
+    b->rowOff[i] = (int)ro;
+    so += counts[i];
+    ro += ((long long)counts[i] + 255) / 256 * 256;
+  }
+  b->totalDesc = total;
+  b->totalRows = rows;
+  V3DM_BTRY(ensure(&b->dImg, &b->imgCap, std::max<long long>(rows, 256) * kDescBytes));
+  if (nImages > b->imagesCap) {
+    bfree(b->dSrcOff);
+    bfree(b->dImages);
+    bfree(b->dImgB);
+    b->imagesCap = 0;
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dSrcOff), (size_t)nImages * sizeof(long long)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dImages), (size_t)nImages * sizeof(BImage)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dImgB), (size_t)nImages * sizeof(BImageB)));
+    b->imagesCap = nImages;
+  }
+  if (nImages > 0) {
+    V3DM_BTRY(cudaMemcpyAsync(b->dSrcOff, b->srcOff.data(), (size_t)nImages * sizeof(long long),
+                              cudaMemcpyHostToDevice, b->stream));
+    // The per-image table is completed with pair ranges by set_pairs; upload it with empty ranges.
+    b->bim.assign(nImages, BImage{});
+    for (int i = 0; i < nImages; ++i) b->bim[i] = BImage{b->rowOff[i], counts[i], 0, 0};
+    V3DM_BTRY(cudaMemcpyAsync(b->dImages, b->bim.data(), (size_t)nImages * sizeof(BImage), cudaMemcpyHostToDevice,
+                              b->stream));
+  }
+  if (total > 0) {
+    const uint8_t* src = desc;
+    if (!onDevice) {
+      V3DM_BTRY(ensure(&b->dStage, &b->stageCap, total * kDescBytes));
+      V3DM_BTRY(cudaMemcpyAsync(b->dStage, desc, (size_t)total * kDescBytes, cudaMemcpyHostToDevice, b->stream));
+      src = b->dStage;
+    }
+    k_bscatter<<<std::min(nImages, 1024), 256, 0, b->stream>>>(src, b->dSrcOff, b->dImages, nImages, b->dImg);
+    V3DM_BTRY(cudaGetLastError());
+  }
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));  // host vectors and the caller's buffer may change after return
+  b->haveImages = true;
+  b->mapsValid = false;
+  b->rowsDirty = true;
+  return V3DM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int v3dm_batch_create(v3dm_batch** out, int device) {
+  if (!out) return V3DM_ERR_ARG;
+  *out = nullptr;
+  int nDev = 0;
+  if (cudaGetDeviceCount(&nDev) != cudaSuccess || device < 0 || device >= nDev) return V3DM_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return V3DM_ERR_CUDA;
+  if (prop.major != 10) return V3DM_ERR_NO_DEVICE;
+  v3dm_batch* b = new (std::nothrow) v3dm_batch();
+  if (!b) return V3DM_ERR_ARG;
+  b->device = device;
+  BDeviceGuard g(device);
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            tc_plan_create(&b->tc, device) == cudaSuccess &&
+            cudaMalloc(reinterpret_cast<void**>(&b->dInfo), (kInfoWords + kCntWords) * sizeof(int32_t)) == cudaSuccess &&
+            cudaMallocHost(reinterpret_cast<void**>(&b->hInfo), (kInfoWords + kCntWords) * sizeof(int32_t)) == cudaSuccess;
+  if (ok) {
+    b->dCounters = b->dInfo + kInfoWords;  // the counter words follow the info words
+    ok = alloc_records(b, 256) == cudaSuccess;
+  }
+  if (!ok) {
+    free_all(b);
+    if (b->tc) tc_plan_destroy(b->tc);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return V3DM_ERR_CUDA;
+  }
+  *out = b;
+  return V3DM_OK;
+}
+
+int v3dm_batch_destroy(v3dm_batch* b) {
+  if (!b) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  cudaStreamSynchronize(b->stream);
+  free_all(b);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->tc) tc_plan_destroy(b->tc);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return V3DM_OK;
+}
+
+int v3dm_batch_set_images_u8(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* desc) {
+  return set_images(b, nImages, counts, desc, false);
+}
+
+int v3dm_batch_set_images_u8_device(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* d_desc) {
+  return set_images(b, nImages, counts, d_desc, true);
+}
+
+int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs) {
+  if (!b || nPairs < -1 || (nPairs > 0 && !pairs)) return V3DM_ERR_ARG;
+  if (!b->haveImages) return V3DM_ERR_NOT_ALLOCATED;
+  const int nI = b->nImages;
+  std::vector<int> li, ri;
+  if (nPairs == -1) {
+    for (int i = 0; i < nI; ++i)
+      for (int j = i + 1; j < nI; ++j) {
+        li.push_back(i);
+        ri.push_back(j);
+      }
+  } else {
+    li.resize(nPairs);
+    ri.resize(nPairs);
+    for (int p = 0; p < nPairs; ++p) {
+      li[p] = pairs[2 * p];
+      ri[p] = pairs[2 * p + 1];
+      if (li[p] < 0 || li[p] >= nI || ri[p] < 0 || ri[p] >= nI) return V3DM_ERR_ARG;
+    }
+  }
+  if (li.size() > 0x7ffffffULL) return V3DM_ERR_SIZE;
+  const int n = (int)li.size();
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return li[a] < li[c]; });
+  std::vector<BPair> bp(n);
+  long long SA = 0, ops = 0;
+  for (int k = 0; k < n; ++k) {
+    const int p = order[k];
+    bp[k] = BPair{li[p], ri[p], p, b->counts[li[p]], SA};
+    SA += b->counts[li[p]];
+    ops += 2LL * kDescBytes * b->counts[li[p]] * b->counts[ri[p]];
+  }
+  if (SA > 0x7ffffff0LL) return V3DM_ERR_SIZE;  // state indices are int32
+  BDeviceGuard g(b->device);
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  drop_graph(b);
+  b->havePairs = false;
+  for (int i = 0; i < nI; ++i) b->bim[i].pairBeg = b->bim[i].pairEnd = 0;
+  for (int k = 0; k < n;) {
+    int e = k;
+    while (e < n && bp[e].li == bp[k].li) ++e;
+    b->bim[bp[k].li].pairBeg = k;
+    b->bim[bp[k].li].pairEnd = e;
+    k = e;
+  }
+  if (n > b->pairsCap) {
+    bfree(b->dPairs);
+    bfree(b->dCnt);
+    bfree(b->dPrefC);
+    b->pairsCap = 0;
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dPairs), (size_t)n * sizeof(BPair)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dCnt), (size_t)n * sizeof(int)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dPrefC), (size_t)(n + 1) * sizeof(long long)));
+    b->pairsCap = n;
+  }
+  if (!b->dCnt) {
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dCnt), sizeof(int)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dPrefC), 2 * sizeof(long long)));
+  }
+  if (n > 0)
+    V3DM_BTRY(cudaMemcpyAsync(b->dPairs, bp.data(), (size_t)n * sizeof(BPair), cudaMemcpyHostToDevice, b->stream));
+  if (nI > 0)
+    V3DM_BTRY(cudaMemcpyAsync(b->dImages, b->bim.data(), (size_t)nI * sizeof(BImage), cudaMemcpyHostToDevice,
+                              b->stream));
+  // per-state arrays; best and sec start at zero and every call leaves them at zero
+  if (SA + 1 > b->stateCap) {
+    bfree(b->dBest);
+    bfree(b->dSec);
+    bfree(b->dDecA);
+    b->stateCap = 0;
+    const long long cap = SA + 1;
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dBest), (size_t)cap * sizeof(unsigned long long)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dSec), (size_t)cap * sizeof(unsigned int)));
+    V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dDecA), (size_t)cap * sizeof(int32_t)));
+    V3DM_BTRY(cudaMemsetAsync(b->dBest, 0, (size_t)cap * sizeof(unsigned long long), b->stream));
+    V3DM_BTRY(cudaMemsetAsync(b->dSec, 0, (size_t)cap * sizeof(unsigned int), b->stream));
+    b->stateCap = cap;
+  }
+  // pass-B buffers: a first guess of 1/32 of the pass-A states, grown on overflow
+  const long long wantB = std::max<long long>(65536, SA / 32);
+  if (b->capB < wantB || b->capB == 0) V3DM_BTRY(alloc_passB(b, wantB));
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  b->nPairs = n;
+  b->pairLi.swap(li);
+  b->pairRi.swap(ri);
+  b->bp.swap(bp);
+  b->SA = SA;
+  b->workOps = ops;
+  b->havePairs = true;
+  b->rowsDirty = true;
+  b->mapsValid = false;
+  return V3DM_OK;
+}
+
+int v3dm_batch_match(v3dm_batch* b, float minScore, float minRatio, int32_t* triples, long long cap, long long* nOut) {
+  if (!b || !nOut || cap < 0 || (cap > 0 && !triples)) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  int st = run_host(b, minScore, minRatio);
+  if (st != V3DM_OK) return st;
+  const long long n = b->hInfo[kInfoWords + kCntOut];
+  *nOut = n;
+  const long long m = std::min(n, cap);
+  if (m > 0) {
+    V3DM_BTRY(cudaMemcpyAsync(triples, b->dOut, (size_t)m * sizeof(int3), cudaMemcpyDeviceToHost, b->stream));
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  }
+  return n > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
+}
+
+int v3dm_batch_match_device(v3dm_batch* b, float minScore, float minRatio, int32_t* d_count) {
+  if (!b) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  int st = launch_call(b, minScore, minRatio);
+  if (st != V3DM_OK) return st;
+  if (d_count)
+    V3DM_BTRY(cudaMemcpyAsync(d_count, b->dInfo + kInfoWords + kCntOut, sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                              b->stream));
+  return V3DM_OK;
+}
+
+int v3dm_batch_wait(v3dm_batch* b) {
+  if (!b) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  if (!b->pendingCheck) {
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+    return V3DM_OK;
+  }
+  return finish_call(b);
+}
+
+int v3dm_batch_result_device(v3dm_batch* b, const int32_t** d_triples) {
+  if (!b || !d_triples) return V3DM_ERR_ARG;
+  *d_triples = reinterpret_cast<const int32_t*>(b->dOut);
+  return V3DM_OK;
+}
+
+int v3dm_batch_stream(v3dm_batch* b, void** stream) {
+  if (!b || !stream) return V3DM_ERR_ARG;
+  *stream = b->stream;
+  return V3DM_OK;
+}
+
+int v3dm_batch_use_graph(v3dm_batch* b, int enable) {
+  if (!b) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  cudaStreamSynchronize(b->stream);
+  b->useGraph = enable != 0;
+  if (!b->useGraph) drop_graph(b);
+  return V3DM_OK;
+}
+
+int v3dm_batch_set_config(v3dm_batch* b, int cfg, int schedule) {
+  if (!b || schedule < 0 || schedule > 1) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  cudaStreamSynchronize(b->stream);
+  if (tc_set_config(b->tc, cfg) != cudaSuccess) return V3DM_ERR_ARG;
+  if (b->schedule != schedule || b->rowsCfg != cfg) drop_graph(b);
+  b->schedule = schedule;
+  return V3DM_OK;
+}
+
+int v3dm_batch_get_config(v3dm_batch* b, int* cfg, int* schedule) {
+  if (!b || !cfg || !schedule) return V3DM_ERR_ARG;
+  *cfg = tc_get_config(b->tc);
+  *schedule = b->schedule;
+  return V3DM_OK;
+}
+
+int v3dm_batch_autotune(v3dm_batch* b, float minScore, float minRatio, int reps, int* bestCfg, int* bestSchedule,
+                        float* msOut) {
+  if (!b || reps < 1) return V3DM_ERR_ARG;
+  if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  BDeviceGuard g(b->device);
+  const int nCfg = tc_num_configs();
+  const bool graphWas = b->useGraph;
+  const bool profWas = b->profile;
+  b->useGraph = false;
+  b->profile = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  V3DM_BTRY(cudaEventCreate(&e0));
+  V3DM_BTRY(cudaEventCreate(&e1));
+  float bestMs = 1e30f;
+  int bc = tc_get_config(b->tc), bs = b->schedule;
+  int st = V3DM_OK;
+  for (int c = 0; c < nCfg && st == V3DM_OK; ++c)
+    for (int sch = 0; sch < 2 && st == V3DM_OK; ++sch) {
+      tc_set_config(b->tc, c);
+      b->schedule = sch;
+      st = run_host(b, minScore, minRatio);  // warm-up; grows buffers if needed
+      if (st != V3DM_OK) break;
+      float total = 0.f;
+      for (int r = 0; r < reps && st == V3DM_OK; ++r) {
+        cudaEventRecord(e0, b->stream);
+        st = launch_call(b, minScore, minRatio);
+        cudaEventRecord(e1, b->stream);
+        if (st == V3DM_OK) st = finish_call(b);
+        float ms = 0.f;
+        if (st == V3DM_OK) cudaEventElapsedTime(&ms, e0, e1);
+        total += ms;
+      }
+      const float avg = total / reps;
+      if (msOut) msOut[2 * c + sch] = avg;
+      if (st == V3DM_OK && avg < bestMs) {
+        bestMs = avg;
+        bc = c;
+        bs = sch;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tc_set_config(b->tc, bc);
+  b->schedule = bs;
+  b->useGraph = graphWas;
+  b->profile = profWas;
+  drop_graph(b);
+  if (bestCfg) *bestCfg = bc;
+  if (bestSchedule) *bestSchedule = bs;
+  return st;
+}
+
+int v3dm_batch_profile(v3dm_batch* b, int enable) {
+  if (!b) return V3DM_ERR_ARG;
+  b->profile = enable != 0;
+  b->profMs[0] = b->profMs[1] = 0.0;
+  b->profN[0] = b->profN[1] = 0;
+  return V3DM_OK;
+}
+
+int v3dm_batch_profile_read(v3dm_batch* b, int pass, double* msTotal, int* launches) {
+  if (!b || pass < 0 || pass > 1 || !msTotal || !launches) return V3DM_ERR_ARG;
+  *msTotal = b->profMs[pass];
+  *launches = b->profN[pass];
+  return V3DM_OK;
+}
+
+int v3dm_batch_last_launches(v3dm_batch* b, int* n) {
+  if (!b || !n) return V3DM_ERR_ARG;
+  *n = b->lastLaunches;
+  return V3DM_OK;
+}
+
+int v3dm_batch_work(v3dm_batch* b, long long* int8Ops, long long* nPairs) {
+  if (!b || !int8Ops || !nPairs) return V3DM_ERR_ARG;
+  *int8Ops = b->havePairs ? b->workOps : 0;
+  *nPairs = b->havePairs ? b->nPairs : 0;
+  return V3DM_OK;
+}
+
+}  // extern "C"

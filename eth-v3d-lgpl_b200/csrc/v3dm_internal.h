@@ -47,7 +47,20 @@ cudaError_t launch_gate_precompute(int type, const double* m, const float* dLPos
 cudaError_t launch_f32_to_u8(const float* src, uint8_t* dst, int n, int* err, cudaStream_t s);
 
 // ---- tcgen05 path (v3dm_match_tc.cu, v3dm_pair.cu) ------------------------------------
-// One side pass scores the nA descriptors of side A against the nB descriptors of side B.
+// One row of a batched side pass: one A group (up to rowsPerGroup descriptors of one image,
+// or of one list of chosen descriptors) against every tile of one B image.
+struct BatchRow {
+  int aRow;          // first row of the group in the A tensor
+  int validRows;     // descriptors in the group; rows past it are padding
+  int bRow0;         // first row of the B image in the B tensor
+  int nB;            // descriptors of the B image
+  int nTiles;        // ceil(nB / colsPerTile)
+  int pad;
+  long long state0;  // state index of the group's first descriptor
+};
+
+// One side pass scores the nA descriptors of side A against the nB descriptors of side B
+// (single pair), or walks a table of BatchRows (batched pass).
 struct SideArgs {
   const int* nAptr;              // device count of A rows (null: use nA)
   int nA;                        // A rows (upper bound when nAptr is set)
@@ -64,8 +77,13 @@ struct SideArgs {
   int* err;
   int nGates;
   const GateParams* gatesDev;    // device array of the call's gates
+  // batched pass only
+  const BatchRow* rows;          // row table
+  const int* nRowsPtr;           // device row count (null: use nRows)
+  int nRows;
+  int schedule;                  // 0: rows interleaved over the CTAs, 1: contiguous row ranges
 };
-// Chunk record: {A index, first B index, 0, 0} then the chunk's 32 scores.
+// Chunk record: {A index (state), first B index, B count, 0} then the chunk's 32 scores.
 constexpr int kRecordQuads = 9;
 
 struct TcPlan;
@@ -84,6 +102,10 @@ int tc_segments(TcPlan* p);
 // Tensor maps of a side pass for the plan's current configuration.
 cudaError_t tc_side_maps(TcPlan* p, TcMaps* m, const uint8_t* dA, int rowsA, const uint8_t* dB, int rowsB);
 cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st);
+// Batched side pass over a.rows (a.nRows, or *a.nRowsPtr rows): one persistent launch.
+cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st);
+// Sets the batched kernel's launch attributes for configuration cfg (before a stream capture).
+cudaError_t tc_prepare_batch(TcPlan* p, int cfg);
 
 // Decision and bookkeeping kernels around the side passes (v3dm_pair.cu).
 struct PostArgs {
@@ -93,7 +115,7 @@ struct PostArgs {
   unsigned long long* best;
   unsigned int* sec;
   const uint4* records;          // chunk records of the side pass
-  unsigned long long* list;      // one (A index, chunk best key) entry per record
+  unsigned long long* list;      // one entry per record: the chunk best key (0: none)
   int* segCount;                 // read, then cleared
   long long segCap;
   int nSeg;
@@ -136,5 +158,9 @@ cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDe
 
 // Candidate threshold (v3dm_api.cu).
 int host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T);
+// Records the detail v3dm_last_error() reports for this thread (v3dm_api.cu).
+void record_cuda_error(cudaError_t e, const char* file, int line, const char* what);
+// Smallest integer score S whose float score S * 2^-18 passes 's > minScore' (v3dm_api.cu).
+int32_t host_smallest_passing_score(float minScore);
 
 }  // namespace v3dm

@@ -38,6 +38,7 @@
 
 #include <algorithm>
 #include <new>
+#include <type_traits>
 
 #include "v3dm_device.cuh"
 
@@ -191,15 +192,6 @@ __device__ __forceinline__ void tmem_wait(uint32_t (&v)[N]) {
   for (int i = 0; i < N; ++i) asm volatile("" : "+r"(v[i]));  // uses stay after the wait
 }
 
-// Maximum of three non-negative int32 scores through the three-input f32 max: a
-// non-negative int32 below 2^23 read as f32 is a subnormal whose order is the integer
-// order, and max.f32 without .ftz keeps subnormals.
-__device__ __forceinline__ uint32_t max3_bits(uint32_t a, uint32_t b, uint32_t c) {
-  float r;
-  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(__uint_as_float(a)), "f"(__uint_as_float(b)), "f"(__uint_as_float(c)));
-  return __float_as_uint(r);
-}
-
 // Maximum of 32 scores: a balanced tree of two-input integer maxima (ALU pipe, short
 // latency, 16-way parallel at the first level).
 __device__ __forceinline__ uint32_t max32_bits(const uint32_t* v) {
@@ -219,53 +211,112 @@ __device__ __forceinline__ void cta_range(const TcShape& sh, long long& w0, long
   w1 = sh.nWork * (blockIdx.x + 1) / gridDim.x;
 }
 
-// Walks (group, tile) pairs of a work range with one division at the start: the per-tile
-// loops of the MMA issuer and the epilogue stay free of 64-bit divisions.
+// Single pair: walks (group, tile) pairs of a work range with one division at the start, so
+// the per-tile loops of the MMA issuer and the epilogue stay free of 64-bit divisions.
 struct WorkCursor {
   int g, t, nTiles;
   long long left;
-  __device__ __forceinline__ WorkCursor(long long w0, long long w1, int nT) : nTiles(nT), left(w1 - w0) {
+  bool fresh;  // first tile of a group
+  __device__ __forceinline__ WorkCursor(long long w0, long long w1, int nT) : nTiles(nT), left(w1 - w0), fresh(true) {
     g = (int)(w0 / nT);
     t = (int)(w0 - (long long)g * nT);
   }
   __device__ __forceinline__ bool more() const { return left > 0; }
   __device__ __forceinline__ void next() {
     --left;
+    fresh = false;
     if (++t == nTiles) {
       t = 0;
       ++g;
+      fresh = true;
     }
   }
 };
 
-// Gate test with the per-left and per-right terms already loaded (see gate_rejects).
-__device__ __forceinline__ bool gate_rejects_terms(int type, float sqrThr, float4 p, float4 q) {
-  if (type == 1) {
-    float num = __fadd_rn(__fadd_rn(__fmul_rn(q.x, p.x), __fmul_rn(q.y, p.y)), p.z);
-    num = __fmul_rn(num, num);
-    float denom = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.x, p.x), __fmul_rn(p.y, p.y)), __fmul_rn(q.z, q.z)),
-                            __fmul_rn(q.w, q.w));
-    return __fdiv_rn(num, denom) > sqrThr;
-  }
-  float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y);
-  return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > sqrThr;
+__device__ __forceinline__ BatchRow load_row(const BatchRow* rows, int r) {
+  const int4* p = reinterpret_cast<const int4*>(rows + r);
+  const int4 x = __ldg(p), y = __ldg(p + 1);
+  BatchRow b;
+  b.aRow = x.x;
+  b.validRows = x.y;
+  b.bRow0 = x.z;
+  b.nB = x.w;
+  b.nTiles = max(y.x, 1);  // every row advances the cursor by at least one tile
+  b.pad = y.y;
+  b.state0 = (long long)(((unsigned long long)(uint32_t)y.w << 32) | (uint32_t)y.z);
+  return b;
 }
 
-template <class C>
+// Batched pass: walks the rows of a row table, every tile of a row in order.  Schedule 0
+// gives CTA b the rows b, b + grid, b + 2 grid, ...: the CTAs then work on neighbouring rows
+// (the same B image) at the same time, so the B tiles are read from L2.  Schedule 1 gives
+// each CTA one contiguous range of rows.  The next row's entry is loaded a row ahead.
+struct BatchCursor {
+  const BatchRow* rows;
+  int R, step, Rend, t;
+  BatchRow cur, nxt;
+  bool fresh;
+  __device__ __forceinline__ BatchCursor(const BatchRow* rows_, int nRows, int schedule) : rows(rows_), t(0), fresh(true) {
+    cur = BatchRow{};
+    nxt = BatchRow{};
+    if (schedule == 0) {
+      R = blockIdx.x;
+      step = gridDim.x;
+      Rend = nRows;
+    } else {
+      R = (int)((long long)nRows * blockIdx.x / gridDim.x);
+      Rend = (int)((long long)nRows * (blockIdx.x + 1) / gridDim.x);
+      step = 1;
+    }
+    if (R < Rend) cur = load_row(rows, R);
+    if (R + step < Rend) nxt = load_row(rows, R + step);
+  }
+  __device__ __forceinline__ bool more() const { return R < Rend; }
+  __device__ __forceinline__ void next() {
+    fresh = false;
+    if (++t == cur.nTiles) {
+      t = 0;
+      R += step;
+      fresh = true;
+      cur = nxt;
+      if (R + step < Rend) nxt = load_row(rows, R + step);
+    }
+  }
+};
+
+// kBatch = false: one pair, the flattened (group, tile) range of this CTA (WorkCursor).
+// kBatch = true: rows of a.rows (BatchCursor); a row's state indices are state0 + row.
+template <class C, bool kBatch>
 __global__ void __launch_bounds__(kThreads, 1)
 k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
   extern __shared__ uint8_t smemRaw[];
   Smem<C>& s = *reinterpret_cast<Smem<C>*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nA = a.nAptr ? *a.nAptr : a.nA;
-  TcShape sh;
-  sh.nGroups = (nA + C::GM - 1) / C::GM;
-  sh.nTiles = nTiles;
-  sh.nWork = (long long)sh.nGroups * nTiles;
-  if (sh.nWork == 0) {  // nothing to score (e.g. no right was chosen): uniform early exit
-    if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kEpiWarps + (warp - 2)] = 0;
-    return;
+  using Cursor = typename std::conditional<kBatch, BatchCursor, WorkCursor>::type;
+  int nA = 0, nRows = 0;
+  TcShape sh{};
+  long long w0 = 0, w1 = 0;
+  if constexpr (kBatch) {
+    nRows = a.nRowsPtr ? *a.nRowsPtr : a.nRows;
+    if (nRows <= 0) {  // nothing to score: uniform early exit
+      if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kEpiWarps + (warp - 2)] = 0;
+      return;
+    }
+  } else {
+    nA = a.nAptr ? *a.nAptr : a.nA;
+    sh.nGroups = (nA + C::GM - 1) / C::GM;
+    sh.nTiles = nTiles;
+    sh.nWork = (long long)sh.nGroups * nTiles;
+    if (sh.nWork == 0) {  // nothing to score (e.g. no right was chosen): uniform early exit
+      if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kEpiWarps + (warp - 2)] = 0;
+      return;
+    }
+    cta_range(sh, w0, w1);
   }
+  auto make_cursor = [&]() -> Cursor {
+    if constexpr (kBatch) return BatchCursor(a.rows, nRows, a.schedule);
+    else return WorkCursor(w0, w1, sh.nTiles);
+  };
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < C::kStages; ++i) {
@@ -299,32 +350,36 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     s.abort = 1;
   }
   __syncthreads();
-  long long w0, w1;
-  cta_range(sh, w0, w1);
 
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, aBuf = 1, prevG = -1;
+      int stage = 0, aBuf = 1;
+      bool anyA = false;
       uint32_t phase = 0, aPhase = 1;
       uint32_t armedPhase[C::kStages];
       bool armed[C::kStages];
       for (int i = 0; i < C::kStages; ++i) armed[i] = false;
-      for (WorkCursor wc(w0, w1, sh.nTiles); wc.more(); wc.next()) {
-        const int g = wc.g, t = wc.t;
-        if (g != prevG) {
+      for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
+        if (wc.fresh) {
           if (++aBuf == 2) {
             aBuf = 0;
             aPhase ^= 1;
           }
           if (!mbar_wait(&s.emptyA[aBuf], aPhase ^ 1, &s.abort, a.err)) break;
           mbar_expect_tx(&s.fullA[aBuf], C::kABytes);
-          tma_load_2d(s.a[aBuf], &tmA, &s.fullA[aBuf], 0, g * C::GM);
-          prevG = g;
+          int aRow;
+          if constexpr (kBatch) aRow = wc.cur.aRow;
+          else aRow = wc.g * C::GM;
+          tma_load_2d(s.a[aBuf], &tmA, &s.fullA[aBuf], 0, aRow);
+          anyA = true;
         }
         if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
         mbar_expect_tx(&s.fullB[stage], C::kBBytes);
-        tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, t * C::BN);
+        int bRow;
+        if constexpr (kBatch) bRow = wc.cur.bRow0 + wc.t * C::BN;
+        else bRow = wc.t * C::BN;
+        tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, bRow);
         armed[stage] = true;
         armedPhase[stage] = phase;
         if (++stage == C::kStages) {
@@ -339,7 +394,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
           }
         }
-      if (prevG >= 0) {
+      if (anyA) {
         long long t0c = clock64();
         while (!mbar_try(&s.fullA[aBuf], aPhase) && clock64() - t0c < kWaitCycles) {
         }
@@ -348,20 +403,20 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, acc = 0, aBuf = 1, prevG = -1;
+      int stage = 0, acc = 0, aBuf = 1;
+      bool anyA = false;
       uint32_t phase = 0, accPhase = 0, aPhase = 1;
       uint32_t aAddr = 0;
-      for (WorkCursor wc(w0, w1, sh.nTiles); wc.more(); wc.next()) {
-        const int g = wc.g;
-        if (g != prevG) {
-          if (prevG >= 0) mma_commit(&s.emptyA[aBuf]);
+      for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
+        if (wc.fresh) {
+          if (anyA) mma_commit(&s.emptyA[aBuf]);
           if (++aBuf == 2) {
             aBuf = 0;
             aPhase ^= 1;
           }
           if (!mbar_wait(&s.fullA[aBuf], aPhase, &s.abort, a.err)) break;
           aAddr = smem_u32(s.a[aBuf]);
-          prevG = g;
+          anyA = true;
         }
         if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
         if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) break;
@@ -386,7 +441,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           accPhase ^= 1;
         }
       }
-      if (prevG >= 0) mma_commit(&s.emptyA[aBuf]);
+      if (anyA) mma_commit(&s.emptyA[aBuf]);
       // Every MMA this thread issued has completed before TMEM is released.
       mma_commit(&s.mmaDone);
       long long t0c = clock64();
@@ -400,28 +455,36 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     const int sub = e >> 2;                              // 0..3 within the quadrant
     const int blk = C::NB == 2 ? (sub & 1) : 0;          // A block of the group
     const int colOff = (C::NB == 2 ? (sub >> 1) : sub) * C::kWarpCols;  // first tile column of this warp
+    const int rowInGroup = blk * BM + q * 32 + lane;
     uint4* const segBase = a.records + (long long)(blockIdx.x * kEpiWarps + e) * a.segCap * kRecordQuads;
     int segN = 0;                                        // warp-uniform count of records written
-    int acc = 0, prevG = -1;
+    int acc = 0;
+    bool started = false;
     uint32_t accPhase = 0;
     bool ok = !s.abort;
     bool rowValid = false;
     int orig = 0;
+    int nB = a.nB;
     uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
     auto flush = [&]() {
       if (rowValid && lw != 0) atomicMax(&a.sec[orig], lw);
     };
-    for (WorkCursor wc(w0, w1, sh.nTiles); wc.more() && ok; wc.next()) {
-      const int g = wc.g, t = wc.t;
-      if (g != prevG) {
-        if (prevG >= 0) flush();
-        const int row = g * C::GM + blk * BM + q * 32 + lane;
-        rowValid = row < nA;
-        orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
+    for (Cursor wc = make_cursor(); wc.more() && ok; wc.next()) {
+      if (wc.fresh) {
+        if (started) flush();
+        started = true;
+        if constexpr (kBatch) {
+          rowValid = rowInGroup < wc.cur.validRows;
+          orig = rowValid ? (int)(wc.cur.state0 + rowInGroup) : 0;
+          nB = wc.cur.nB;
+        } else {
+          const int row = wc.g * C::GM + rowInGroup;
+          rowValid = row < nA;
+          orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
+        }
         lw = 0;
-        prevG = g;
       }
-      const int colBase = t * C::BN + colOff;
+      const int colBase = wc.t * C::BN + colOff;
       ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
@@ -441,9 +504,10 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
 #pragma unroll
       for (int c = 0; c < C::kChunks; ++c) {
         const int col0 = colBase + 32 * c;
-        if (col0 >= a.nB) break;  // chunks past the last B descriptor (warp-uniform)
-        // Columns past nB read TMA zero fill (0 <= every real score), so the chunk maximum
-        // stays the maximum of its real scores.
+        if (col0 >= nB) break;  // chunks past the last B descriptor (warp-uniform)
+        // Columns past nB read zero descriptors (TMA zero fill, or the zero padding of a
+        // batch image), and 0 <= every real score, so the chunk maximum stays the maximum of
+        // its real scores.
         const uint32_t mx = max32_bits(v[c]);
         const bool trig = rowValid && (int32_t)mx >= a.Smin;
         if (rowValid && !trig) lw = max(lw, mx + 1u);
@@ -454,7 +518,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
             const int idx = segN + __popc(m & ((1u << lane) - 1u));
             if (idx < a.segCap) {
               uint4* rec = segBase + (long long)idx * kRecordQuads;
-              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, 0u, 0u);
+              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)nB, 0u);
 #pragma unroll
               for (int k = 0; k < 8; ++k)
                 rec[1 + k] = make_uint4(v[c][4 * k], v[c][4 * k + 1], v[c][4 * k + 2], v[c][4 * k + 3]);
@@ -468,7 +532,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         accPhase ^= 1;
       }
     }
-    if (prevG >= 0 && ok) flush();
+    if (started && ok) flush();
     if (lane == 0) a.segCount[blockIdx.x * kEpiWarps + e] = segN;
   }
 
@@ -515,16 +579,16 @@ using Cfg2 = TcCfg<2, 128, 8>;   // 256 x 128 tiles, 2 accumulator stages
 using Cfg3 = TcCfg<2, 64, 16>;   // 256 x 64 tiles, 4 accumulator stages
 using Cfg4 = TcCfg<1, 256, 6>;   // 128 x 256 tiles, 2 accumulator stages, 6-deep ring
 
-template <class C>
+template <class C, bool kBatch>
 cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles, const SideArgs& a, int grid,
                        cudaStream_t st, bool& attrSet) {
   const size_t smem = sizeof(Smem<C>) + 1024;
   if (!attrSet) {
-    cudaError_t e = cudaFuncSetAttribute(k_side<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_side<C, kBatch>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attrSet = true;
   }
-  k_side<C><<<grid, kThreads, smem, st>>>(mA, mB, nTiles, a);
+  k_side<C, kBatch><<<grid, kThreads, smem, st>>>(mA, mB, nTiles, a);
   return cudaGetLastError();
 }
 
@@ -540,6 +604,7 @@ struct TcPlan {
   int numSMs = 148;
   int cfg = kDefaultCfg;
   bool attrSet[kNumCfg] = {};
+  bool attrSetBatch[kNumCfg] = {};
 };
 
 cudaError_t tc_plan_create(TcPlan** p, int device) {
@@ -593,11 +658,49 @@ cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStrea
   int grid = (int)std::min<long long>(p->numSMs, std::max<long long>(1, maxWork));
   if (grid * kEpiWarps > a.nSeg) return cudaErrorInvalidValue;
   switch (c) {
-    case 0: return launch_cfg<Cfg0>(m.a, m.b, nTiles, a, grid, st, p->attrSet[0]);
-    case 1: return launch_cfg<Cfg1>(m.a, m.b, nTiles, a, grid, st, p->attrSet[1]);
-    case 2: return launch_cfg<Cfg2>(m.a, m.b, nTiles, a, grid, st, p->attrSet[2]);
-    case 3: return launch_cfg<Cfg3>(m.a, m.b, nTiles, a, grid, st, p->attrSet[3]);
-    default: return launch_cfg<Cfg4>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
+    case 0: return launch_cfg<Cfg0, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[0]);
+    case 1: return launch_cfg<Cfg1, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[1]);
+    case 2: return launch_cfg<Cfg2, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[2]);
+    case 3: return launch_cfg<Cfg3, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[3]);
+    default: return launch_cfg<Cfg4, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
+  }
+}
+
+template <class C>
+cudaError_t set_batch_attr(bool& attrSet) {
+  if (attrSet) return cudaSuccess;
+  const size_t smem = sizeof(Smem<C>) + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_side<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) attrSet = true;
+  return e;
+}
+
+cudaError_t tc_prepare_batch(TcPlan* p, int cfg) {
+  switch (cfg) {
+    case 0: return set_batch_attr<Cfg0>(p->attrSetBatch[0]);
+    case 1: return set_batch_attr<Cfg1>(p->attrSetBatch[1]);
+    case 2: return set_batch_attr<Cfg2>(p->attrSetBatch[2]);
+    case 3: return set_batch_attr<Cfg3>(p->attrSetBatch[3]);
+    case 4: return set_batch_attr<Cfg4>(p->attrSetBatch[4]);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st) {
+  const int c = m.cfg;
+  // Persistent grid: one CTA per SM (fewer when the row count is known to be small).
+  int grid = p->numSMs;
+  if (!a.nRowsPtr) {
+    if (a.nRows <= 0) return cudaSuccess;
+    grid = std::min(grid, a.nRows);
+  }
+  if (grid * kEpiWarps > a.nSeg || a.schedule < 0 || a.schedule > 1) return cudaErrorInvalidValue;
+  switch (c) {
+    case 0: return launch_cfg<Cfg0, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[0]);
+    case 1: return launch_cfg<Cfg1, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[1]);
+    case 2: return launch_cfg<Cfg2, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[2]);
+    case 3: return launch_cfg<Cfg3, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[3]);
+    default: return launch_cfg<Cfg4, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[4]);
   }
 }
 

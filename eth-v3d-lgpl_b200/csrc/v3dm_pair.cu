@@ -37,7 +37,7 @@ __global__ void k_records(PostArgs a) {
     for (long long i = lane; i < n; i += 32) {
       const uint4* rec = recs + i * kRecordQuads;
       const uint4 head = rec[0];
-      const int orig = (int)head.x, col0 = (int)head.y;
+      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z;
       unsigned long long cb = 0;
       uint32_t cw = 0;
       for (int k = 0; k < 8; ++k) {
@@ -45,7 +45,7 @@ __global__ void k_records(PostArgs a) {
         const uint32_t sv[4] = {q.x, q.y, q.z, q.w};
         for (int t = 0; t < 4; ++t) {
           const int col = col0 + 4 * k + t;
-          if (col >= a.nB) break;
+          if (col >= nB) break;
           const int32_t S = (int32_t)sv[t];
           bool strong = S >= a.Smin;
           for (int gi = 0; gi < a.nGates && strong; ++gi)
@@ -65,13 +65,14 @@ __global__ void k_records(PostArgs a) {
       }
       if (cb) atomicMax(&a.best[orig], cb);
       if (cw) atomicMax(&a.sec[orig], cw);
-      entries[i] = cb ? ((unsigned long long)(uint32_t)orig | (cb << kIndexBits)) : 0ull;
+      entries[i] = cb;  // 0: no candidate in the chunk
     }
   }
 }
 
 // List pass: one warp per segment; every chunk best that is not the descriptor's overall
-// best raises its second value.  Segment counts are cleared for the next pass.
+// best raises its second value (the descriptor is read from the chunk's record).  Segment
+// counts are cleared for the next pass.
 __global__ void k_list(PostArgs a, int32_t* info) {
   const int lane = threadIdx.x & 31;
   const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -85,11 +86,11 @@ __global__ void k_list(PostArgs a, int32_t* info) {
     }
     const long long n = cnt < a.segCap ? cnt : a.segCap;
     const unsigned long long* e = a.list + (long long)seg * a.segCap;
+    const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
     for (long long i = lane; i < n; i += 32) {
-      const unsigned long long x = e[i];
-      if (x == 0) continue;  // record without a candidate
-      const int idx = (int)(x & kIndexMask);
-      const unsigned long long key = x >> kIndexBits;
+      const unsigned long long key = e[i];
+      if (key == 0) continue;  // record without a candidate
+      const int idx = (int)recs[i * kRecordQuads].x;
       if (key != a.best[idx]) atomicMax(&a.sec[idx], (unsigned)(key >> kIndexBits));
     }
   }

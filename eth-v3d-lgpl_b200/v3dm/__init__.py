@@ -94,6 +94,25 @@ def lib() -> C.CDLL:
         L.v3dm_voctree_quantize_u8.argtypes = [vp, i32, vp, vp, i32]
         L.v3dm_voctree_quantize_u8_device.argtypes = [vp, i32, vp, vp, i32]
         L.v3dm_voctree_stream.argtypes = [vp, C.POINTER(vp)]
+        i64, i64p = C.c_longlong, C.POINTER(C.c_longlong)
+        L.v3dm_batch_create.argtypes = [C.POINTER(vp), i32]
+        L.v3dm_batch_destroy.argtypes = [vp]
+        L.v3dm_batch_set_images_u8.argtypes = [vp, i32, vp, vp]
+        L.v3dm_batch_set_images_u8_device.argtypes = [vp, i32, vp, vp]
+        L.v3dm_batch_set_pairs.argtypes = [vp, i32, vp]
+        L.v3dm_batch_match.argtypes = [vp, f32, f32, vp, i64, i64p]
+        L.v3dm_batch_match_device.argtypes = [vp, f32, f32, vp]
+        L.v3dm_batch_wait.argtypes = [vp]
+        L.v3dm_batch_result_device.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_batch_stream.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_batch_use_graph.argtypes = [vp, i32]
+        L.v3dm_batch_set_config.argtypes = [vp, i32, i32]
+        L.v3dm_batch_get_config.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+        L.v3dm_batch_autotune.argtypes = [vp, f32, f32, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_float)]
+        L.v3dm_batch_profile.argtypes = [vp, i32]
+        L.v3dm_batch_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
+        L.v3dm_batch_last_launches.argtypes = [vp, C.POINTER(i32)]
+        L.v3dm_batch_work.argtypes = [vp, i64p, i64p]
         _lib = L
     return _lib
 
@@ -325,3 +344,127 @@ class VocabularyTreeTraversal:
         s = C.c_void_p()
         _check(lib().v3dm_voctree_stream(self._h, C.byref(s)), "stream")
         return s.value or 0
+
+
+class BatchMatching:
+    """Many image pairs matched together (the apps' per-pair findPutativeMatches loop,
+    V3D/Apps/SfM/match_sequence.cpp:165-234).  Each pair's result equals
+    SIFTMatching.find_putative_matches on the two images."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_batch_create(C.byref(h), device), "batch_create")
+        self._h = h
+        self.n_pairs = 0
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_batch_destroy(self._h)
+        self._h = None
+
+    __del__ = close
+
+    def set_images(self, desc: np.ndarray, counts) -> None:
+        """desc: (sum(counts), 128) uint8, the images' descriptors concatenated."""
+        d = np.ascontiguousarray(desc, dtype=np.uint8)
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        if d.ndim != 2 or d.shape[1] != 128 or int(c.sum()) != d.shape[0]:
+            raise ValueError("desc must be (sum(counts), 128) uint8")
+        _check(lib().v3dm_batch_set_images_u8(self._h, c.shape[0], _ptr(c), _ptr(d)), "batch_set_images")
+
+    def set_images_device(self, d_desc: int, counts) -> None:
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        _check(lib().v3dm_batch_set_images_u8_device(self._h, c.shape[0], _ptr(c), C.c_void_p(d_desc)),
+               "batch_set_images_device")
+
+    def set_pairs(self, pairs=None) -> None:
+        """pairs: (n, 2) int32 (left image, right image); None = every (i, j), i < j."""
+        if pairs is None:
+            _check(lib().v3dm_batch_set_pairs(self._h, -1, None), "batch_set_pairs")
+            n = C.c_longlong(0)
+            ops = C.c_longlong(0)
+            _check(lib().v3dm_batch_work(self._h, C.byref(ops), C.byref(n)), "batch_work")
+            self.n_pairs = n.value
+            return
+        p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        _check(lib().v3dm_batch_set_pairs(self._h, p.shape[0], _ptr(p)), "batch_set_pairs")
+        self.n_pairs = p.shape[0]
+
+    def match(self, min_score: float = 0.9, min_ratio: float = 0.8, cap: int | None = None) -> np.ndarray:
+        """(n, 3) int32 (pair index, left, right), grouped by pair, ascending left in a pair."""
+        cap = cap if cap is not None else max(1 << 20, getattr(self, "_last_n", 0))
+        while True:
+            out = np.empty((max(1, cap), 3), np.int32)
+            n = C.c_longlong(0)
+            st = lib().v3dm_batch_match(self._h, min_score, min_ratio, _ptr(out), cap, C.byref(n))
+            if st == ERR_CAPACITY:
+                cap = n.value
+                continue
+            _check(st, "batch_match")
+            self._last_n = n.value
+            return out[: n.value].copy()
+
+    def match_per_pair(self, min_score: float = 0.9, min_ratio: float = 0.8):
+        """List with one (n, 2) (left, right) array per pair of the table."""
+        t = self.match(min_score, min_ratio)
+        order = np.argsort(t[:, 0], kind="stable")
+        t = t[order]
+        bounds = np.searchsorted(t[:, 0], np.arange(self.n_pairs + 1))
+        return [t[bounds[k]:bounds[k + 1], 1:].copy() for k in range(self.n_pairs)]
+
+    def match_device(self, min_score: float, min_ratio: float, d_count: int = 0) -> None:
+        _check(lib().v3dm_batch_match_device(self._h, min_score, min_ratio, C.c_void_p(d_count) if d_count else None),
+               "batch_match_device")
+
+    def wait(self) -> int:
+        """Checks the last device call; returns its status (ERR_CANDIDATES: repeat the call)."""
+        st = lib().v3dm_batch_wait(self._h)
+        if st not in (OK, ERR_CANDIDATES):
+            _check(st, "batch_wait")
+        return st
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().v3dm_batch_stream(self._h, C.byref(s)), "batch_stream")
+        return s.value or 0
+
+    def use_graph(self, enable: bool = True) -> None:
+        _check(lib().v3dm_batch_use_graph(self._h, int(enable)), "batch_use_graph")
+
+    def set_config(self, cfg: int, schedule: int = 0) -> None:
+        _check(lib().v3dm_batch_set_config(self._h, cfg, schedule), "batch_set_config")
+
+    def config(self):
+        c, s = C.c_int(0), C.c_int(0)
+        _check(lib().v3dm_batch_get_config(self._h, C.byref(c), C.byref(s)), "batch_get_config")
+        return c.value, s.value
+
+    def autotune(self, min_score: float = 0.9, min_ratio: float = 0.8, reps: int = 2):
+        """Times every (configuration, schedule); keeps the fastest.  Returns (cfg, schedule,
+        ms array indexed [cfg, schedule])."""
+        c, s = C.c_int(0), C.c_int(0)
+        ms = (C.c_float * 64)(*([-1.0] * 64))
+        _check(lib().v3dm_batch_autotune(self._h, min_score, min_ratio, reps, C.byref(c), C.byref(s), ms),
+               "batch_autotune")
+        t = np.array(ms[:], np.float32)
+        n = int(np.flatnonzero(t >= 0).max()) // 2 + 1
+        return c.value, s.value, t[: 2 * n].reshape(n, 2)
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().v3dm_batch_profile(self._h, int(enable)), "batch_profile")
+
+    def profile_read(self, pass_id: int):
+        ms, n = C.c_double(0), C.c_int(0)
+        _check(lib().v3dm_batch_profile_read(self._h, pass_id, C.byref(ms), C.byref(n)), "batch_profile_read")
+        return ms.value, n.value
+
+    def last_launches(self) -> int:
+        n = C.c_int(0)
+        _check(lib().v3dm_batch_last_launches(self._h, C.byref(n)), "batch_last_launches")
+        return n.value
+
+    def work(self):
+        """(int8 operations of the pair table, number of pairs)."""
+        ops, n = C.c_longlong(0), C.c_longlong(0)
+        _check(lib().v3dm_batch_work(self._h, C.byref(ops), C.byref(n)), "batch_work")
+        return ops.value, n.value

@@ -163,6 +163,60 @@ V3DM_API int v3dm_putative_u8_noalloc(int device, const uint8_t* d_left, int nLe
                                       float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count,
                                       void* stream);
 
+/* ---- batched matching of many image pairs ------------------------------------------ */
+/* Replaces the apps' loop over image pairs (V3D/Apps/SfM/match_sequence.cpp:165-234 and
+ * match_using_voctree.cpp:290-336: setLeftFeatures once per left image, then
+ * setRightFeatures + findPutativeMatches per right image).  Each pair's result equals that
+ * findPutativeMatches call (v3d_cudamatching.cu:522-552) on the two images' descriptors as
+ * given (no rounding to multiples of 32); all pairs run in two persistent launches. */
+typedef struct v3dm_batch v3dm_batch;
+
+V3DM_API int v3dm_batch_create(v3dm_batch** out, int device);
+V3DM_API int v3dm_batch_destroy(v3dm_batch* b);
+/* nImages images with counts[i] uint8 descriptors each, concatenated (image 0 first,
+ * 128 bytes per descriptor).  Host memory, or device memory (16-byte aligned) for the
+ * _device variant.  New image counts invalidate the pair table (set it again); the same
+ * counts keep it, so a new image set of the same sizes only uploads descriptors. */
+V3DM_API int v3dm_batch_set_images_u8(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* desc);
+V3DM_API int v3dm_batch_set_images_u8_device(v3dm_batch* b, int nImages, const int32_t* counts,
+                                             const uint8_t* d_desc);
+/* nPairs (left image, right image) int32 pairs; nPairs == -1 (pairs NULL) means every
+ * (i, j) with i < j, left = i, in row-major order. */
+V3DM_API int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs);
+/* findPutativeMatches(minScore, minRatio) of every pair.  Output: *nOut (pair, left, right)
+ * int32 triples, grouped by pair (pairs ordered by left image, then by table index),
+ * ascending left within a pair; the first 'cap' are written (V3DM_ERR_CAPACITY if more). */
+V3DM_API int v3dm_batch_match(v3dm_batch* b, float minScore, float minRatio, int32_t* triples, long long cap,
+                              long long* nOut);
+/* Device-resident variant: enqueues the call on the batch's stream (replayed as a CUDA graph
+ * while images, pairs, parameters and configuration stay the same) and copies the triple
+ * count to d_count (device int32, may be NULL).  v3dm_batch_wait checks the call; it returns
+ * V3DM_ERR_CANDIDATES when an internal list overflowed (it has been grown: repeat the call).
+ * The triples stay in the batch's buffer (v3dm_batch_result_device) until the next call. */
+V3DM_API int v3dm_batch_match_device(v3dm_batch* b, float minScore, float minRatio, int32_t* d_count);
+V3DM_API int v3dm_batch_wait(v3dm_batch* b);
+V3DM_API int v3dm_batch_result_device(v3dm_batch* b, const int32_t** d_triples);
+V3DM_API int v3dm_batch_stream(v3dm_batch* b, void** stream);
+/* CUDA-graph replay on (default) or off. */
+V3DM_API int v3dm_batch_use_graph(v3dm_batch* b, int enable);
+/* Tile configuration (as v3dm_matcher_set_config) and row schedule: 0 = rows interleaved over
+ * the persistent CTAs (neighbouring CTAs share the right image in L2), 1 = contiguous row
+ * ranges per CTA. */
+V3DM_API int v3dm_batch_set_config(v3dm_batch* b, int cfg, int schedule);
+V3DM_API int v3dm_batch_get_config(v3dm_batch* b, int* cfg, int* schedule);
+/* Times every (configuration, schedule) on the current batch (reps calls each) and keeps the
+ * fastest; ms[2 * cfg + schedule] receives the averages (ms may be NULL). */
+V3DM_API int v3dm_batch_autotune(v3dm_batch* b, float minScore, float minRatio, int reps, int* bestCfg,
+                                 int* bestSchedule, float* ms);
+/* CUDA-event timing of the two side-pass launches (pass 0 = lefts x rights of every pair,
+ * pass 1 = chosen rights x lefts); calls run without the graph while it is on. */
+V3DM_API int v3dm_batch_profile(v3dm_batch* b, int enable);
+V3DM_API int v3dm_batch_profile_read(v3dm_batch* b, int pass, double* msTotal, int* launches);
+V3DM_API int v3dm_batch_last_launches(v3dm_batch* b, int* n);
+/* Algorithmic work of the current pair table: sum over pairs of 2 * 128 * nLeft * nRight
+ * int8 operations, and the number of pairs. */
+V3DM_API int v3dm_batch_work(v3dm_batch* b, long long* int8Ops, long long* nPairs);
+
 /* ---- vocabulary tree (V3D_CUDA::VocabularyTreeTraversal<BF, Depth>) --------------- */
 typedef struct v3dm_voctree v3dm_voctree;
 
