@@ -45,11 +45,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "batch", "voctree"], default="stereo")
+    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal"], default="stereo")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--tile-config", type=int, default=-1, help="fused-kernel tile configuration (-1: autotune)")
+    ap.add_argument("--images", type=int, default=200, help="batch workload: number of images")
+    ap.add_argument("--cells", type=int, default=16, help="proposal workload: cells of the projection")
+    ap.add_argument("--probes", type=int, default=4, help="proposal workload: probed cells per left")
+    ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
+    ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     return ap.parse_args()
 
 
@@ -304,7 +309,7 @@ def run_stereo(args, ws, rank, local):
     int8_peak = 2.0 * peaks["bf16_tflops"]  # kind::i8 runs at twice the kind::f16 rate
     ops_per_launch = 2.0 * N_SIDE * N_SIDE * 128
     achieved = ops_per_launch / (k_avg_ms * 1e-3) / 1e12
-    traffic = traffic_from_profiles("k_side" if args.kernel == "tcgen05" else "k_match_simt")
+    traffic = traffic_from_profiles("k_side_stereo" if args.kernel == "tcgen05" else "k_match_simt")
     line = {
         "metric": "image pairs/s (16384x16384 putative + F-guided)", "value": ws * 1000.0 / ms, "unit": "pairs/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -344,7 +349,7 @@ def run_batch(args, ws, rank, local):
     from v3dm import synth
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    desc, counts, offs = synth.images(args.seed + 1)
+    desc, counts, offs = synth.images(args.seed + 1, n_images=args.images)
     b = v3dm.BatchMatching(local)
     b.set_images(desc, counts)
     b.set_pairs(None)
@@ -409,14 +414,14 @@ def run_batch(args, ws, rank, local):
     k_ms = ka / max(na, 1)
     achieved = ops / (k_ms * 1e-3) / 1e12
     line = {
-        "metric": "image pairs/s (all 19,900 pairs of 200 images)", "value": ws * n_pairs * 1000.0 / ms,
+        "metric": f"image pairs/s (all {n_pairs} pairs of {args.images} images)", "value": ws * n_pairs * 1000.0 / ms,
         "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": "200 images, 1000..12000 uint8 SIFT-like features each, 15% shared tracks, all "
-                               "19,900 pairs, minScore 0.7, ratio 0.8", "pairs": n_pairs,
+        "config": {"workload": f"{args.images} images, 1000..12000 uint8 SIFT-like features each, 15% shared "
+                               f"tracks, all {n_pairs} pairs, minScore 0.7, ratio 0.8", "pairs": n_pairs,
                    "descriptors": int(counts.sum()), "seed": args.seed + 1,
-                   "l2": "inputs larger than L2 (166 MB of descriptors, 2 GB of per-pair state)"},
+                   "l2": f"inputs larger than L2 ({desc.nbytes / 1e6:.0f} MB of descriptors and the per-pair state)"},
         "aggregate_int8_tops": ops / (ms * 1e-3) / 1e12,
         "tile": {"config": cfg, "schedule": sch, "chosen_by": "autotune" if args.tile_config < 0 else "flag"},
         "pairs_found": n_out,
@@ -444,7 +449,7 @@ def run_batch(args, ws, rank, local):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": n_pairs / (dt * ops / s_ops), "unit": "pairs/s",
                                 "cores": oracle.num_threads(), "kind": "port",
-                                "sample": "12 random pairs of the 19,900, extrapolated by int8 operations"}
+                                "sample": f"12 random pairs of the {n_pairs}, extrapolated by int8 operations"}
     print(json.dumps(line), flush=True)
 
 
@@ -561,6 +566,126 @@ def run_voctree(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_proposal(args, ws, rank, local):
+    """Learned candidate proposal against exhaustive matching on the same GPU: 200 test images
+    x 8000 features (19,900 pairs), the projection trained on matches that exhaustive matching
+    found in 100 held-out images of the same generator."""
+    import torch
+
+    import v3dm
+    from v3dm import proposal, synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    tr_desc, tr_counts, tr_offs = synth.images(args.seed + 40, n_images=100, n_min=8000, n_max=8000)
+    te_desc, te_counts, te_offs = synth.images(args.seed + 41, n_images=200, n_min=8000, n_max=8000)
+    b = v3dm.BatchMatching(local)
+    b.set_images(tr_desc, tr_counts)
+    b.set_pairs(None)
+    t_tr = time.perf_counter()
+    anchors, positives = proposal.mine_pairs(tr_desc, tr_offs, synth.all_pairs(100), b.match(MIN_SCORE, MIN_RATIO))
+    net = v3dm.Projection(local, seed=args.seed)
+    losses = proposal.train(net, anchors, positives, steps=args.train_steps, batch=2048,
+                            temperature=args.temperature, lr=2e-3, device=local)
+    net.set_cells(proposal.fit_cells(net.embed(tr_desc), args.cells, seed=args.seed))
+    train_s = time.perf_counter() - t_tr
+    b.set_images(te_desc, te_counts)
+    b.set_pairs(None)
+    ops, n_pairs = b.work()
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    d_cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def timed(call):
+        for _ in range(max(args.warmup, 3)):
+            call()
+            while b.wait() == v3dm.ERR_CANDIDATES:
+                call()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        n = 0
+        for a0, a1 in ev:
+            a0.record(stream)
+            call()
+            a1.record(stream)
+            n += b.last_launches()
+        torch.cuda.synchronize()
+        assert b.wait() == v3dm.OK
+        return max_over_ranks(ws, statistics.mean(x.elapsed_time(y) for x, y in ev), dev), n
+
+    ms_exh, _ = timed(lambda: b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
+    exh = b.match(MIN_SCORE, MIN_RATIO)
+    clocks = Clocks(local)
+    ms_prop, launches = timed(lambda: b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
+    clk = clocks.stop()
+    got = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO)
+    rec, prec = proposal.recall(exh, got)
+    scored, exhaustive = b.proposal_scored()
+    b.profile(True)
+    for _ in range(3):
+        b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+        assert b.wait() == v3dm.OK
+    ka, na = b.profile_read(0)
+    b.profile(False)
+    # ablation: the same cells fitted to the untrained network
+    net0 = v3dm.Projection(local, seed=args.seed)
+    net0.set_cells(proposal.fit_cells(net0.embed(tr_desc), args.cells, seed=args.seed))
+    ms0, _ = timed(lambda: b.match_proposal_device(net0, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
+    rec0, prec0 = proposal.recall(exh, b.match_proposal(net0, args.probes, MIN_SCORE, MIN_RATIO))
+    scored0, _ = b.proposal_scored()
+    net0.close()
+    # e2e: descriptors from pinned host memory, triples back
+    desc_p = torch.from_numpy(te_desc).pin_memory().numpy()
+    for _ in range(2):
+        b.set_images(desc_p, te_counts)
+        b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    n_host = 0
+    for a0, a1 in ev2:
+        a0.record(stream)
+        b.set_images(desc_p, te_counts)
+        n_host = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO).shape[0]
+        a1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(ws, statistics.mean(x.elapsed_time(y) for x, y in ev2), dev)
+    net.close()
+    b.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    k_ms = ka / max(na, 1)
+    ops_prop = 2.0 * 128 * scored
+    achieved = ops_prop / (k_ms * 1e-3) / 1e12
+    line = {
+        "metric": "image pairs/s (learned proposal, all 19,900 pairs of 200 images x 8000 features)",
+        "value": ws * n_pairs * 1000.0 / ms_prop, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_prop, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": {"workload": "200 test images x 8000 uint8 SIFT-like features, 15% shared tracks, all 19,900 pairs, "
+                               "minScore 0.7, ratio 0.8; projection 128-64-32 trained on 100 held-out images",
+                   "cells": args.cells, "probes": args.probes, "train_steps": args.train_steps,
+                   "temperature": args.temperature, "train_pairs": int(anchors.shape[0]),
+                   "l2": "inputs larger than L2 (205 MB of descriptors)"},
+        "exhaustive": {"value": ws * n_pairs * 1000.0 / ms_exh, "unit": "pairs/s", "ms_per_step": ms_exh},
+        "speedup_vs_exhaustive": ms_exh / ms_prop,
+        "recall": rec, "precision": prec, "matches_exhaustive": int(len(exh)), "matches_proposal": int(len(got)),
+        "scored_fraction": scored / exhaustive,
+        "ablation_untrained": {"recall": rec0, "precision": prec0, "scored_fraction": scored0 / exhaustive,
+                               "ms_per_step": ms0},
+        "training": {"seconds": train_s, "loss_first": losses[0][1], "loss_last": losses[-1][1]},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",
+                     "frac": achieved / int8_peak, "traffic": None,
+                     "peak_src": f"2 x {peaks['src']} bf16 dense ({peaks['bf16_tflops']} TFLOP/s burst)",
+                     "kernel_ms": k_ms, "ops_per_launch": ops_prop,
+                     "kernel": "k_side pass A over the candidate blocks (scored pairs x 256 ops)"},
+        "e2e": {"value": ws * n_pairs * 1000.0 / ms_e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(te_desc.nbytes),
+                "d2h_bytes_per_step": int(n_host * 12 + 64)},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -573,6 +698,8 @@ def main():
             run_batch(args, ws, rank, local)
         elif args.workload == "voctree":
             run_voctree(args, ws, rank, local)
+        elif args.workload == "proposal":
+            run_proposal(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -62,7 +62,7 @@ constexpr int kCntOut = 3;        // triples written
 constexpr int kCntNeedStates = 4; // sizes the pass-B buffers need
 constexpr int kCntNeedRows = 5;
 constexpr int kCntNeedTable = 6;
-constexpr int kCntWords = 8;
+constexpr int kCntAll = 12;      // batch and proposal counter words
 
 constexpr int kScanThreads = 1024;
 constexpr int kChooseThreads = 256;
@@ -301,6 +301,260 @@ k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, co
     }
 }
 
+// ---- proposal matching (learned cells) --------------------------------------------------
+// Layout of the proposal: every image's descriptors are copied into an A layout, once per
+// probed cell and grouped by (image, cell), and into a B layout grouped by (image, best cell).
+// A pair (i, j) is scored block by block: the lefts of i that probe cell c against the rights of
+// j whose best cell is c.  mapA / mapB give each layout row's index within its image.
+
+constexpr int kCntRowsP = 8;      // counter words of the proposal (after the batch ones)
+constexpr int kCntOverP = 9;      // 1: the proposal row table was too small
+constexpr int kCntScored = 10;    // two words: scored (left, right) pairs, 64-bit
+
+// Per image and cell: rows whose probed cells include the cell (A) and rows whose best cell
+// it is (B).
+__global__ void k_pcount(const BImage* __restrict__ im, int nImages, const uint8_t* __restrict__ cell, int probes,
+                         int C, int* __restrict__ cntA, int* __restrict__ cntB) {
+  extern __shared__ int pcSh[];
+  for (int i = blockIdx.x; i < nImages; i += gridDim.x) {
+    for (int t = threadIdx.x; t < 2 * C; t += blockDim.x) pcSh[t] = 0;
+    __syncthreads();
+    const BImage m = im[i];
+    for (int r = threadIdx.x; r < m.n; r += blockDim.x) {
+      const uint8_t* cr = cell + (size_t)(m.rowOff + r) * probes;
+      for (int q = 0; q < probes; ++q) atomicAdd(&pcSh[cr[q]], 1);
+      atomicAdd(&pcSh[C + cr[0]], 1);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < C; t += blockDim.x) {
+      cntA[i * C + t] = pcSh[t];
+      cntB[i * C + t] = pcSh[C + t];
+    }
+    __syncthreads();
+  }
+}
+
+// Block offsets of the A and B layouts (exclusive prefix sums over (image, cell)).  One block.
+__global__ void __launch_bounds__(kScanThreads)
+k_pscan_cells(const int* __restrict__ cntA, const int* __restrict__ cntB, int n, int* __restrict__ offA,
+              int* __restrict__ offB) {
+  __shared__ long long sh[kScanThreads];
+  block_scan(n, [&](int i) { return (long long)cntA[i]; }, [&](int i, long long x) { offA[i] = (int)x; }, sh);
+  block_scan(n, [&](int i) { return (long long)cntB[i]; }, [&](int i, long long x) { offB[i] = (int)x; }, sh);
+}
+
+// Copies the descriptors into the A and B layouts (order within a block is arbitrary: every
+// result depends on the index maps, not on the order).
+__global__ void k_pscatter(const BImage* __restrict__ im, int nImages, const uint8_t* __restrict__ cell, int probes,
+                           int C, const int* __restrict__ offA, const int* __restrict__ offB,
+                           const uint8_t* __restrict__ img, uint8_t* __restrict__ la, int* __restrict__ mapA,
+                           uint8_t* __restrict__ lb, int* __restrict__ mapB) {
+  extern __shared__ int psSh[];
+  for (int i = blockIdx.x; i < nImages; i += gridDim.x) {
+    for (int t = threadIdx.x; t < 2 * C; t += blockDim.x) psSh[t] = 0;
+    __syncthreads();
+    const BImage m = im[i];
+    for (int r = threadIdx.x; r < m.n; r += blockDim.x) {
+      const uint8_t* cr = cell + (size_t)(m.rowOff + r) * probes;
+      const uint4* src = reinterpret_cast<const uint4*>(img + (size_t)(m.rowOff + r) * kDescBytes);
+      uint4 d[kDescBytes / 16];
+#pragma unroll
+      for (int x = 0; x < kDescBytes / 16; ++x) d[x] = src[x];
+      for (int q = 0; q < probes; ++q) {
+        const int c = cr[q];
+        const int pos = offA[i * C + c] + atomicAdd(&psSh[c], 1);
+        uint4* dst = reinterpret_cast<uint4*>(la + (size_t)pos * kDescBytes);
+#pragma unroll
+        for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = d[x];
+        mapA[pos] = r;
+      }
+      const int c0 = cr[0];
+      const int pos = offB[i * C + c0] + atomicAdd(&psSh[C + c0], 1);
+      uint4* dst = reinterpret_cast<uint4*>(lb + (size_t)pos * kDescBytes);
+#pragma unroll
+      for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = d[x];
+      mapB[pos] = r;
+    }
+    __syncthreads();
+  }
+}
+
+// Rows of every pair: one per (cell with rights, group of GM lefts probing it); also counts the
+// scored (left, right) pairs.
+__global__ void k_prowcount(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im, int C, int GM,
+                            const int* __restrict__ cntA, const int* __restrict__ cntB, int* __restrict__ rowCnt,
+                            unsigned long long* __restrict__ scored) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nPairs) return;
+  const BPair q = pairs[p];
+  int rows = 0;
+  unsigned long long sc = 0;
+  if (im[q.ri].n > 0)
+    for (int c = 0; c < C; ++c) {
+      const int a = cntA[q.li * C + c], b = cntB[q.ri * C + c];
+      if (a > 0 && b > 0) {
+        rows += (a + GM - 1) / GM;
+        sc += (unsigned long long)a * b;
+      }
+    }
+  rowCnt[p] = rows;
+  if (sc) atomicAdd(scored, sc);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_pscan_rows(const int* __restrict__ rowCnt, int nPairs, long long capRows, int* __restrict__ rowStart,
+             int* __restrict__ counters) {
+  __shared__ long long sh[kScanThreads];
+  const long long total = block_scan(
+      nPairs, [&](int i) { return (long long)rowCnt[i]; }, [&](int i, long long x) { rowStart[i] = (int)x; }, sh);
+  if (threadIdx.x == 0) {
+    const bool over = total > capRows;
+    counters[kCntRowsP] = over ? 0 : (int)total;
+    counters[kCntOverP] = over ? 1 : 0;
+  }
+}
+
+__global__ void k_prows(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im, int C, int GM,
+                        int BN, const int* __restrict__ cntA, const int* __restrict__ cntB,
+                        const int* __restrict__ offA, const int* __restrict__ offB, const int* __restrict__ rowStart,
+                        const int* __restrict__ counters, BatchRow* __restrict__ rows) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nPairs || counters[kCntOverP]) return;
+  const BPair q = pairs[p];
+  if (im[q.ri].n == 0) return;
+  int at = rowStart[p];
+  for (int c = 0; c < C; ++c) {
+    const int a = cntA[q.li * C + c], b = cntB[q.ri * C + c];
+    if (a == 0 || b == 0) continue;
+    for (int g = 0; g * GM < a; ++g) {
+      BatchRow r;
+      r.aRow = offA[q.li * C + c] + g * GM;
+      r.validRows = min(GM, a - g * GM);
+      r.bRow0 = offB[q.ri * C + c];
+      r.nB = b;
+      r.nTiles = (b + BN - 1) / BN;
+      r.pad = 0;
+      r.state0 = q.stateA0;
+      rows[at++] = r;
+    }
+  }
+}
+
+// Pass-B states of the proposal: exclusive prefix of the accepted lefts per pair.  One block.
+__global__ void __launch_bounds__(kScanThreads)
+k_pscan_states(const int* __restrict__ cnt, int nPairs, long long capStates, long long* __restrict__ prefC,
+               int* __restrict__ counters) {
+  __shared__ long long sh[kScanThreads];
+  const long long SB = block_scan(
+      nPairs, [&](int i) { return (long long)cnt[i]; }, [&](int i, long long x) { prefC[i] = x; }, sh);
+  if (threadIdx.x == 0) {
+    prefC[nPairs] = SB;
+    const bool over = SB > capStates;
+    counters[kCntStates] = over ? 0 : (int)SB;
+    counters[kCntOverflow] = over ? 1 : 0;
+    counters[kCntNeedStates] = (int)min(SB, (long long)0x7fffffff);
+  }
+}
+
+// The accepted lefts of every pair in ascending order, with the right each one named.
+__global__ void __launch_bounds__(kChooseThreads)
+k_pchoose(const BPair* __restrict__ pairs, int nPairs, const long long* __restrict__ prefC,
+          const int32_t* __restrict__ decA, int* __restrict__ chosenLeft, int* __restrict__ chosenRight,
+          int* __restrict__ chosenPair, int* __restrict__ chosenSorted, const int* __restrict__ counters) {
+  __shared__ int wsum[kChooseThreads / 32];
+  if (counters[kCntOverflow]) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int p = blockIdx.x; p < nPairs; p += gridDim.x) {
+    const long long s0 = prefC[p];
+    if (prefC[p + 1] == s0) continue;
+    const BPair q = pairs[p];
+    int run = 0;
+    for (int l0 = 0; l0 < q.nL; l0 += kChooseThreads) {
+      const int l = l0 + threadIdx.x;
+      const int d = l < q.nL ? decA[q.stateA0 + l] : -1;
+      const bool acc = d >= 0;
+      const unsigned m = __ballot_sync(0xffffffffu, acc);
+      if (lane == 0) wsum[w] = __popc(m);
+      __syncthreads();
+      int before = 0, tot = 0;
+#pragma unroll
+      for (int k = 0; k < kChooseThreads / 32; ++k) {
+        before += k < w ? wsum[k] : 0;
+        tot += wsum[k];
+      }
+      if (acc) {
+        const long long st = s0 + run + before + __popc(m & ((1u << lane) - 1u));
+        chosenLeft[st] = l;
+        chosenRight[st] = d;
+        chosenPair[st] = q.orig;
+        chosenSorted[st] = p;
+      }
+      run += tot;
+      __syncthreads();
+    }
+  }
+}
+
+// Row decision of every chosen right over its candidate lefts (the lefts of the pair's left
+// image that probe the right's best cell), exactly: one warp per pass-B state, the right's
+// descriptor in every lane's registers, lanes striding over the candidates.
+__global__ void __launch_bounds__(256)
+k_ppassb(const BPair* __restrict__ pairs, const BImage* __restrict__ im, const uint8_t* __restrict__ cell, int probes,
+         int C, const int* __restrict__ cntA, const int* __restrict__ offA, const uint8_t* __restrict__ la,
+         const int* __restrict__ mapA, const uint8_t* __restrict__ img, const int* __restrict__ chosenRight,
+         const int* __restrict__ chosenSorted, const int* __restrict__ counters, float minScore, float minRatio,
+         int32_t* __restrict__ decB) {
+  const int n = counters[kCntStates];
+  const int lane = threadIdx.x & 31;
+  const int warpG = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int s = warpG; s < n; s += nWarps) {
+    const BPair q = pairs[chosenSorted[s]];
+    const int r = chosenRight[s];
+    const int rRow = im[q.ri].rowOff + r;
+    const int c1 = cell[(size_t)rRow * probes];
+    const int cnt = cntA[q.li * C + c1];
+    const int base = offA[q.li * C + c1];
+    uint4 rv[kDescBytes / 16];
+    const uint4* rs = reinterpret_cast<const uint4*>(img + (size_t)rRow * kDescBytes);
+#pragma unroll
+    for (int x = 0; x < kDescBytes / 16; ++x) rv[x] = __ldg(rs + x);
+    unsigned long long best = 0;
+    uint32_t sec = 0;
+    for (int j = lane; j < cnt; j += 32) {
+      const uint4* ls = reinterpret_cast<const uint4*>(la + (size_t)(base + j) * kDescBytes);
+      uint32_t S = 0;
+#pragma unroll
+      for (int x = 0; x < kDescBytes / 16; ++x) {
+        const uint4 w = __ldg(ls + x);
+        S = __dp4a(rv[x].x, w.x, S);
+        S = __dp4a(rv[x].y, w.y, S);
+        S = __dp4a(rv[x].z, w.z, S);
+        S = __dp4a(rv[x].w, w.w, S);
+      }
+      const unsigned long long key = best_key((int32_t)S, __ldg(mapA + base + j));
+      if (key > best) {
+        sec = max(sec, (uint32_t)(best >> kIndexBits));
+        best = key;
+      } else {
+        sec = max(sec, S + 1u);
+      }
+    }
+    // warp: the largest key; the second is the largest of the other lanes' bests and every
+    // lane's own second
+    unsigned long long gb = best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long t = __shfl_xor_sync(0xffffffffu, gb, o);
+      gb = t > gb ? t : gb;
+    }
+    uint32_t gs = best != gb ? (uint32_t)(best >> kIndexBits) : sec;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gs = max(gs, __shfl_xor_sync(0xffffffffu, gs, o));
+    if (lane == 0) decB[s] = decide(gb, gs, minScore, minRatio);
+  }
+}
+
 }  // namespace
 
 }  // namespace v3dm
@@ -380,6 +634,40 @@ struct v3dm_batch {
   uint32_t graphMs = 0, graphMr = 0;
   int graphLaunches = 0;
   bool pendingCheck = false;
+  // proposal matching (learned cells)
+  uint8_t* dCell = nullptr;         // per padded image row: its probed cells, best first
+  long long cellCap = 0;
+  int* dCntA = nullptr;             // per (image, cell): A-layout rows, B-layout rows, offsets
+  int* dCntB = nullptr;
+  int* dOffA = nullptr;
+  int* dOffB = nullptr;
+  long long cellTabCap = 0;
+  uint8_t* dLA = nullptr;           // A layout: every descriptor once per probed cell
+  long long laCap = 0;              // bytes
+  int* dMapA = nullptr;
+  long long mapACap = 0;
+  uint8_t* dLB = nullptr;           // B layout: every descriptor once, under its best cell
+  long long lbCap = 0;
+  int* dMapB = nullptr;
+  long long mapBCap = 0;
+  int* dRowCnt = nullptr;           // per pair: proposal rows and their first index
+  int* dRowStart = nullptr;
+  long long pairTabCap = 0;
+  BatchRow* dRowsP = nullptr;
+  long long rowsPCap = 0;
+  long long rowsPNeed = 0;
+  long long laRows = 0, lbRows = 0;
+  int* dChosenSorted = nullptr;     // per pass-B state: the pair's index in batch order
+  long long chosenSortedCap = 0;
+  TcMaps mapsP;
+  bool mapsPValid = false;
+  const uint8_t* mapsPla = nullptr;
+  const uint8_t* mapsPlb = nullptr;
+  cudaGraphExec_t graphP = nullptr;
+  uint32_t gpMs = 0, gpMr = 0;
+  int gpProbes = 0, gpCells = 0, gpLaunches = 0;
+  const v3dm_projection* gpProj = nullptr;
+  long long exhaustivePairs = 0;    // sum over pairs of nL * nR
   // profiling
   bool profile = false;
   cudaEvent_t ev[4] = {};
@@ -438,6 +726,8 @@ cudaError_t ensure(T** p, long long* cap, long long need) {
 void drop_graph(v3dm_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
+  if (b->graphP) cudaGraphExecDestroy(b->graphP);
+  b->graphP = nullptr;
 }
 
 cudaError_t alloc_records(v3dm_batch* b, long long segCap) {
@@ -471,6 +761,8 @@ cudaError_t alloc_passB(v3dm_batch* b, long long capStates) {
   bfree(b->dChosenPair);
   bfree(b->dBlockCount);
   bfree(b->dOut);
+  bfree(b->dChosenSorted);
+  b->chosenSortedCap = 0;
   b->capB = b->capRowsB = b->capTableB = 0;
   cudaError_t e = ensure(&b->dAB, &c0, capRows * kDescBytes);
   if (e == cudaSuccess) e = ensure(&b->dRowsB, &c1, capTable);
@@ -480,6 +772,7 @@ cudaError_t alloc_passB(v3dm_batch* b, long long capStates) {
   if (e == cudaSuccess) e = ensure(&b->dChosenPair, &c5, capStates);
   if (e == cudaSuccess) e = ensure(&b->dBlockCount, &c6, capStates / kBMutPerBlock + 1);
   if (e == cudaSuccess) e = ensure(&b->dOut, &c7, capStates);
+  if (e == cudaSuccess) e = ensure(&b->dChosenSorted, &b->chosenSortedCap, capStates);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->dAB, 0, (size_t)capRows * kDescBytes, b->stream);
   if (e != cudaSuccess) return e;
   b->capB = capStates;
@@ -537,7 +830,7 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   tc_config_shape(tc_get_config(b->tc), &GM, &BN);
   const int32_t Smin = host_smallest_passing_score(minScore);
   int launches = 0;
-  V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntWords) * sizeof(int32_t), b->stream));
+  V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
@@ -611,7 +904,7 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
                                                              mutBlocks, b->dOut, b->dInfo);
   V3DM_BTRY(cudaGetLastError());
   launches += 2;
-  V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntWords) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+  V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             b->stream));
   b->lastLaunches = launches;
   return V3DM_OK;
@@ -638,8 +931,8 @@ int launch_call(v3dm_batch* b, float minScore, float minRatio) {
   if (st != V3DM_OK) return st;
   b->pendingCheck = true;
   if (b->totalRows == 0 || b->nPairs == 0) {
-    V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntWords) * sizeof(int32_t), b->stream));
-    V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntWords) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+    V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                               b->stream));
     b->lastLaunches = 0;
     return V3DM_OK;
@@ -706,6 +999,10 @@ int finish_call(v3dm_batch* b) {
     V3DM_BTRY(alloc_records(b, cap));
     grow = true;
   }
+  if (cnt[kCntOverP]) {
+    b->rowsPNeed = std::max<long long>(2 * b->rowsPCap, 1024);
+    grow = true;
+  }
   if (cnt[kCntOverflow]) {
     long long need = std::max<long long>((long long)cnt[kCntNeedStates] * 5 / 4 + 1024, 2 * b->capB);
     V3DM_BTRY(alloc_passB(b, need));
@@ -728,6 +1025,223 @@ int run_host(v3dm_batch* b, float minScore, float minRatio) {
     if (st != V3DM_ERR_CANDIDATES) return st;
   }
   return V3DM_ERR_CANDIDATES;
+}
+
+// ---- proposal matching ----------------------------------------------------------------
+
+// Buffers and tensor maps of a proposal call with 'probes' probed cells and C cells.
+int prepare_proposal(v3dm_batch* b, int probes, int C) {
+  int st = prepare(b);
+  if (st != V3DM_OK) return st;
+  int GM = 0, BN = 0;
+  tc_config_shape(tc_get_config(b->tc), &GM, &BN);
+  const long long laRows = std::max<long long>(b->totalDesc * probes, 256);
+  const long long lbRows = std::max<long long>(b->totalDesc, 256);
+  long long rowsBound = 0;
+  for (const BPair& q : b->bp)
+    if (b->counts[q.ri] > 0 && q.nL > 0) rowsBound += ((long long)q.nL * probes + GM - 1) / GM + C;
+  rowsBound = std::max<long long>(std::max(rowsBound, b->rowsPNeed), 1);
+  if (rowsBound > 0x7fffffffLL || laRows > 0x7fffffffLL) return V3DM_ERR_SIZE;
+  const uint8_t* la0 = b->dLA;
+  const uint8_t* lb0 = b->dLB;
+  const BatchRow* rp0 = b->dRowsP;
+  V3DM_BTRY(ensure(&b->dCell, &b->cellCap, std::max<long long>(b->totalRows, 1) * probes));
+  const long long tab = (long long)std::max(b->nImages, 1) * C;
+  if (tab > b->cellTabCap) {
+    long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    bfree(b->dCntA);
+    bfree(b->dCntB);
+    bfree(b->dOffA);
+    bfree(b->dOffB);
+    b->cellTabCap = 0;
+    V3DM_BTRY(ensure(&b->dCntA, &c0, tab));
+    V3DM_BTRY(ensure(&b->dCntB, &c1, tab));
+    V3DM_BTRY(ensure(&b->dOffA, &c2, tab));
+    V3DM_BTRY(ensure(&b->dOffB, &c3, tab));
+    b->cellTabCap = tab;
+  }
+  V3DM_BTRY(ensure(&b->dLA, &b->laCap, laRows * kDescBytes));
+  V3DM_BTRY(ensure(&b->dMapA, &b->mapACap, laRows));
+  V3DM_BTRY(ensure(&b->dLB, &b->lbCap, lbRows * kDescBytes));
+  V3DM_BTRY(ensure(&b->dMapB, &b->mapBCap, lbRows));
+  if (b->nPairs > b->pairTabCap) {
+    long long c0 = 0, c1 = 0;
+    bfree(b->dRowCnt);
+    bfree(b->dRowStart);
+    b->pairTabCap = 0;
+    V3DM_BTRY(ensure(&b->dRowCnt, &c0, b->nPairs));
+    V3DM_BTRY(ensure(&b->dRowStart, &c1, b->nPairs));
+    b->pairTabCap = b->nPairs;
+  }
+  V3DM_BTRY(ensure(&b->dRowsP, &b->rowsPCap, rowsBound));
+  if (b->dLA != la0 || b->dLB != lb0 || b->dRowsP != rp0 || !b->mapsPValid || b->laRows != laRows ||
+      b->lbRows != lbRows || b->mapsP.cfg != tc_get_config(b->tc)) {
+    V3DM_BTRY(tc_side_maps(b->tc, &b->mapsP, b->dLA, (int)laRows, b->dLB, (int)lbRows));
+    b->mapsPValid = true;
+    b->laRows = laRows;
+    b->lbRows = lbRows;
+    if (b->graphP) cudaGraphExecDestroy(b->graphP);
+    b->graphP = nullptr;
+  }
+  return V3DM_OK;
+}
+
+int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, float minScore, float minRatio,
+                     bool withEvents) {
+  int GM = 0, BN = 0;
+  tc_config_shape(tc_get_config(b->tc), &GM, &BN);
+  const int C = proj_cells(proj);
+  const int32_t Smin = host_smallest_passing_score(minScore);
+  const int nI = b->nImages;
+  const int imgGrid = std::max(1, std::min(nI, 1024));
+  const int pairGrid = std::max(1, (b->nPairs + 255) / 256);
+  int launches = 0;
+  V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
+  // cells of every descriptor, layouts, row table
+  V3DM_BTRY(proj_assign(proj, b->dImg, b->totalRows, probes, b->dCell, b->stream));
+  k_pcount<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, C, b->dCntA, b->dCntB);
+  V3DM_BTRY(cudaGetLastError());
+  k_pscan_cells<<<1, kScanThreads, 0, b->stream>>>(b->dCntA, b->dCntB, nI * C, b->dOffA, b->dOffB);
+  V3DM_BTRY(cudaGetLastError());
+  k_pscatter<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, C, b->dOffA,
+                                                               b->dOffB, b->dImg, b->dLA, b->dMapA, b->dLB, b->dMapB);
+  V3DM_BTRY(cudaGetLastError());
+  k_prowcount<<<pairGrid, 256, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, C, GM, b->dCntA, b->dCntB,
+                                               b->dRowCnt,
+                                               reinterpret_cast<unsigned long long*>(b->dCounters + kCntScored));
+  V3DM_BTRY(cudaGetLastError());
+  k_pscan_rows<<<1, kScanThreads, 0, b->stream>>>(b->dRowCnt, b->nPairs, b->rowsPCap, b->dRowStart, b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  k_prows<<<pairGrid, 256, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, C, GM, BN, b->dCntA, b->dCntB,
+                                           b->dOffA, b->dOffB, b->dRowStart, b->dCounters, b->dRowsP);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 7;
+  // pass A: each left against the rights under its probed cells
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.Smin = Smin;
+  sa.records = b->dRecords;
+  sa.segCount = b->dSegCount;
+  sa.segCap = b->segCap;
+  sa.nSeg = b->nSeg;
+  sa.err = b->dInfo + kInfoErr;
+  sa.aIsLeft = 1;
+  sa.best = b->dBest;
+  sa.sec = b->dSec;
+  sa.amap = b->dMapA;
+  sa.rows = b->dRowsP;
+  sa.nRowsPtr = b->dCounters + kCntRowsP;
+  sa.nRows = (int)b->rowsPCap;
+  sa.schedule = b->schedule;
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[0], b->stream));
+  V3DM_BTRY(launch_side_batch(b->tc, b->mapsP, sa, b->stream));
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[1], b->stream));
+  PostArgs pa;
+  std::memset(&pa, 0, sizeof(pa));
+  pa.records = b->dRecords;
+  pa.bmap = b->dMapB;
+  pa.list = b->dList;
+  pa.segCount = b->dSegCount;
+  pa.segCap = b->segCap;
+  pa.nSeg = b->nSeg;
+  pa.Smin = Smin;
+  pa.minScore = minScore;
+  pa.minRatio = minRatio;
+  pa.best = b->dBest;
+  pa.sec = b->dSec;
+  pa.err = b->dInfo + kInfoErr;
+  pa.nRows = (int)b->SA;
+  pa.aIsLeft = 1;
+  pa.decision = b->dDecA;
+  V3DM_BTRY(launch_post(pa, b->stream));
+  launches += 4;
+  // pass B: each accepted left's right against the lefts probing the right's best cell
+  const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
+  k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
+  V3DM_BTRY(cudaGetLastError());
+  k_pscan_states<<<1, kScanThreads, 0, b->stream>>>(b->dCnt, b->nPairs, b->capB, b->dPrefC, b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  k_pchoose<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dPrefC, b->dDecA, b->dChosenLeft,
+                                                          b->dChosenRight, b->dChosenPair, b->dChosenSorted,
+                                                          b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
+  k_ppassb<<<148 * 8, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, C, b->dCntA, b->dOffA, b->dLA,
+                                           b->dMapA, b->dImg, b->dChosenRight, b->dChosenSorted, b->dCounters,
+                                           minScore, minRatio, b->dDecB);
+  V3DM_BTRY(cudaGetLastError());
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[3], b->stream));
+  const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
+  k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
+  V3DM_BTRY(cudaGetLastError());
+  k_bmutual_write<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft,
+                                                             b->dChosenRight, b->dChosenPair, b->dBlockCount,
+                                                             mutBlocks, b->dOut, b->dInfo);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 6;
+  V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            b->stream));
+  b->lastLaunches = launches;
+  return V3DM_OK;
+}
+
+int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, float minScore, float minRatio) {
+  if (!proj || probes < 1 || probes > V3DM_PROJ_MAX_PROBES) return V3DM_ERR_ARG;
+  const int C = proj_cells(proj);
+  if (C < 1) return V3DM_ERR_NOT_ALLOCATED;
+  if (probes > C) return V3DM_ERR_ARG;
+  if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  b->pendingCheck = true;
+  if (b->totalRows == 0 || b->nPairs == 0) {
+    V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                              b->stream));
+    b->lastLaunches = 0;
+    return V3DM_OK;
+  }
+  int st = prepare_proposal(b, probes, C);
+  if (st != V3DM_OK) return st;
+  // the projection's parameters and cells may have been written on its own stream
+  V3DM_BTRY(cudaStreamSynchronize(proj_stream(proj)));
+  uint32_t ms, mr;
+  std::memcpy(&ms, &minScore, 4);
+  std::memcpy(&mr, &minRatio, 4);
+  if (b->profile) {
+    for (int i = 0; i < 4; ++i)
+      if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
+    st = enqueue_proposal(b, proj, probes, minScore, minRatio, true);
+    if (st == V3DM_OK) b->profPending = true;
+    return st;
+  }
+  if (!b->useGraph) return enqueue_proposal(b, proj, probes, minScore, minRatio, false);
+  if (!b->graphP || b->gpMs != ms || b->gpMr != mr || b->gpProbes != probes || b->gpCells != C || b->gpProj != proj) {
+    if (b->graphP) cudaGraphExecDestroy(b->graphP);
+    b->graphP = nullptr;
+    cudaGraph_t g = nullptr;
+    V3DM_BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    st = enqueue_proposal(b, proj, probes, minScore, minRatio, false);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (st != V3DM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return bfail(e, "cudaStreamEndCapture", __LINE__);
+    e = cudaGraphInstantiate(&b->graphP, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->graphP = nullptr;
+      return bfail(e, "cudaGraphInstantiate", __LINE__);
+    }
+    b->gpMs = ms;
+    b->gpMr = mr;
+    b->gpProbes = probes;
+    b->gpCells = C;
+    b->gpProj = proj;
+    b->gpLaunches = b->lastLaunches;
+  }
+  V3DM_BTRY(cudaGraphLaunch(b->graphP, b->stream));
+  b->lastLaunches = b->gpLaunches;
+  return V3DM_OK;
 }
 
 void free_all(v3dm_batch* b) {
@@ -755,6 +1269,19 @@ void free_all(v3dm_batch* b) {
   bfree(b->dChosenPair);
   bfree(b->dBlockCount);
   bfree(b->dOut);
+  bfree(b->dCell);
+  bfree(b->dCntA);
+  bfree(b->dCntB);
+  bfree(b->dOffA);
+  bfree(b->dOffB);
+  bfree(b->dLA);
+  bfree(b->dMapA);
+  bfree(b->dLB);
+  bfree(b->dMapB);
+  bfree(b->dRowCnt);
+  bfree(b->dRowStart);
+  bfree(b->dRowsP);
+  bfree(b->dChosenSorted);
   b->dCounters = nullptr;  // points into dInfo
   bfree(b->dInfo);
   if (b->hInfo) cudaFreeHost(b->hInfo);
@@ -864,8 +1391,8 @@ int v3dm_batch_create(v3dm_batch** out, int device) {
   BDeviceGuard g(device);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             tc_plan_create(&b->tc, device) == cudaSuccess &&
-            cudaMalloc(reinterpret_cast<void**>(&b->dInfo), (kInfoWords + kCntWords) * sizeof(int32_t)) == cudaSuccess &&
-            cudaMallocHost(reinterpret_cast<void**>(&b->hInfo), (kInfoWords + kCntWords) * sizeof(int32_t)) == cudaSuccess;
+            cudaMalloc(reinterpret_cast<void**>(&b->dInfo), (kInfoWords + kCntAll) * sizeof(int32_t)) == cudaSuccess &&
+            cudaMallocHost(reinterpret_cast<void**>(&b->hInfo), (kInfoWords + kCntAll) * sizeof(int32_t)) == cudaSuccess;
   if (ok) {
     b->dCounters = b->dInfo + kInfoWords;  // the counter words follow the info words
     ok = alloc_records(b, 256) == cudaSuccess;
@@ -928,12 +1455,13 @@ int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs) {
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return li[a] < li[c]; });
   std::vector<BPair> bp(n);
-  long long SA = 0, ops = 0;
+  long long SA = 0, ops = 0, exh = 0;
   for (int k = 0; k < n; ++k) {
     const int p = order[k];
     bp[k] = BPair{li[p], ri[p], p, b->counts[li[p]], SA};
     SA += b->counts[li[p]];
     ops += 2LL * kDescBytes * b->counts[li[p]] * b->counts[ri[p]];
+    exh += (long long)b->counts[li[p]] * b->counts[ri[p]];
   }
   if (SA > 0x7ffffff0LL) return V3DM_ERR_SIZE;  // state indices are int32
   BDeviceGuard g(b->device);
@@ -991,6 +1519,7 @@ int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs) {
   b->bp.swap(bp);
   b->SA = SA;
   b->workOps = ops;
+  b->exhaustivePairs = exh;
   b->havePairs = true;
   b->rowsDirty = true;
   b->mapsValid = false;
@@ -1031,6 +1560,48 @@ int v3dm_batch_wait(v3dm_batch* b) {
     return V3DM_OK;
   }
   return finish_call(b);
+}
+
+int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore, float minRatio,
+                              int32_t* triples, long long cap, long long* nOut) {
+  if (!b || !nOut || cap < 0 || (cap > 0 && !triples)) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  int st = V3DM_ERR_CANDIDATES;
+  for (int attempt = 0; attempt < 6 && st == V3DM_ERR_CANDIDATES; ++attempt) {
+    st = launch_call_proposal(b, proj, probes, minScore, minRatio);
+    if (st != V3DM_OK) return st;
+    st = finish_call(b);
+  }
+  if (st != V3DM_OK) return st;
+  const long long n = b->hInfo[kInfoWords + kCntOut];
+  *nOut = n;
+  const long long m = std::min(n, cap);
+  if (m > 0) {
+    V3DM_BTRY(cudaMemcpyAsync(triples, b->dOut, (size_t)m * sizeof(int3), cudaMemcpyDeviceToHost, b->stream));
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  }
+  return n > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
+}
+
+int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
+                                     float minRatio, int32_t* d_count) {
+  if (!b) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  int st = launch_call_proposal(b, proj, probes, minScore, minRatio);
+  if (st != V3DM_OK) return st;
+  if (d_count)
+    V3DM_BTRY(cudaMemcpyAsync(d_count, b->dInfo + kInfoWords + kCntOut, sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                              b->stream));
+  return V3DM_OK;
+}
+
+int v3dm_batch_proposal_scored(v3dm_batch* b, long long* scored, long long* exhaustive) {
+  if (!b || !scored || !exhaustive) return V3DM_ERR_ARG;
+  unsigned long long sc = 0;
+  std::memcpy(&sc, b->hInfo + kInfoWords + kCntScored, sizeof(sc));
+  *scored = (long long)sc;
+  *exhaustive = b->havePairs ? b->exhaustivePairs : 0;
+  return V3DM_OK;
 }
 
 int v3dm_batch_result_device(v3dm_batch* b, const int32_t** d_triples) {

@@ -66,7 +66,9 @@ struct SideArgs {
   int nA;                        // A rows (upper bound when nAptr is set)
   int nB;                        // B rows
   int32_t Smin;                  // smallest score that can pass the min-score test
-  const int* amap;               // A row -> index on its side (null: identity)
+  const int* amap;               // single pair: A row -> index on its side (null: identity);
+                                 // batched pass: absolute A row -> index within its image
+                                 // (null: the row's place in its group)
   int aIsLeft;                   // 1: A = lefts, B = rights; 0: A = rights, B = lefts
   unsigned long long* best;      // per A index: best key over B (atomicMax)
   unsigned int* sec;             // per A index: second score + 1 (exact, or a bound with gates)
@@ -83,7 +85,8 @@ struct SideArgs {
   int nRows;
   int schedule;                  // 0: rows interleaved over the CTAs, 1: contiguous row ranges
 };
-// Chunk record: {A index (state), first B index, B count, 0} then the chunk's 32 scores.
+// Chunk record: {A index (state), first B column, B count, first B row of the tile's image
+// block} then the chunk's 32 scores.
 constexpr int kRecordQuads = 9;
 
 struct TcPlan;
@@ -115,6 +118,7 @@ struct PostArgs {
   unsigned long long* best;
   unsigned int* sec;
   const uint4* records;          // chunk records of the side pass
+  const int* bmap;               // absolute B row -> index within its image (null: the column)
   unsigned long long* list;      // one entry per record: the chunk best key (0: none)
   int* segCount;                 // read, then cleared
   long long segCap;
@@ -158,6 +162,13 @@ cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDe
 
 // Candidate threshold (v3dm_api.cu).
 int host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T);
+// Learned projection (v3dm_proposal.cu): the 'probes' best cells of n descriptors (n x probes
+// bytes) on stream s, the number of cells, and the projection's stream.
+cudaError_t proj_assign(const v3dm_projection* p, const uint8_t* dDesc, long long n, int probes, uint8_t* dCells,
+                        cudaStream_t s);
+int proj_cells(const v3dm_projection* p);
+cudaStream_t proj_stream(const v3dm_projection* p);
+
 // Records the detail v3dm_last_error() reports for this thread (v3dm_api.cu).
 void record_cuda_error(cudaError_t e, const char* file, int line, const char* what);
 // Smallest integer score S whose float score S * 2^-18 passes 's > minScore' (v3dm_api.cu).

@@ -465,6 +465,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     bool rowValid = false;
     int orig = 0;
     int nB = a.nB;
+    int bRow0 = 0;
     uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
     auto flush = [&]() {
       if (rowValid && lw != 0) atomicMax(&a.sec[orig], lw);
@@ -475,8 +476,9 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         started = true;
         if constexpr (kBatch) {
           rowValid = rowInGroup < wc.cur.validRows;
-          orig = rowValid ? (int)(wc.cur.state0 + rowInGroup) : 0;
+          orig = rowValid ? (int)(wc.cur.state0 + (a.amap ? __ldg(a.amap + wc.cur.aRow + rowInGroup) : rowInGroup)) : 0;
           nB = wc.cur.nB;
+          bRow0 = wc.cur.bRow0;
         } else {
           const int row = wc.g * C::GM + rowInGroup;
           rowValid = row < nA;
@@ -505,9 +507,14 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
       for (int c = 0; c < C::kChunks; ++c) {
         const int col0 = colBase + 32 * c;
         if (col0 >= nB) break;  // chunks past the last B descriptor (warp-uniform)
-        // Columns past nB read zero descriptors (TMA zero fill, or the zero padding of a
-        // batch image), and 0 <= every real score, so the chunk maximum stays the maximum of
-        // its real scores.
+        if (col0 + 32 > nB) {
+          // The chunk holding the last B descriptor: the columns past it hold zero fill, zero
+          // padding or the next block's descriptors; a 0 there is <= every real score, so the
+          // chunk maximum stays the maximum of its real scores.
+#pragma unroll
+          for (int k = 0; k < 32; ++k)
+            if (col0 + k >= nB) v[c][k] = 0u;
+        }
         const uint32_t mx = max32_bits(v[c]);
         const bool trig = rowValid && (int32_t)mx >= a.Smin;
         if (rowValid && !trig) lw = max(lw, mx + 1u);
@@ -518,7 +525,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
             const int idx = segN + __popc(m & ((1u << lane) - 1u));
             if (idx < a.segCap) {
               uint4* rec = segBase + (long long)idx * kRecordQuads;
-              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)nB, 0u);
+              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)nB, (uint32_t)bRow0);
 #pragma unroll
               for (int k = 0; k < 8; ++k)
                 rec[1 + k] = make_uint4(v[c][4 * k], v[c][4 * k + 1], v[c][4 * k + 2], v[c][4 * k + 3]);

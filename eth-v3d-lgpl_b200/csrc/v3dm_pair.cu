@@ -37,7 +37,7 @@ __global__ void k_records(PostArgs a) {
     for (long long i = lane; i < n; i += 32) {
       const uint4* rec = recs + i * kRecordQuads;
       const uint4 head = rec[0];
-      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z;
+      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z, bRow0 = (int)head.w;
       unsigned long long cb = 0;
       uint32_t cw = 0;
       for (int k = 0; k < 8; ++k) {
@@ -51,7 +51,7 @@ __global__ void k_records(PostArgs a) {
           for (int gi = 0; gi < a.nGates && strong; ++gi)
             strong = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
           if (strong) {
-            const unsigned long long key = best_key(S, col);
+            const unsigned long long key = best_key(S, a.bmap ? __ldg(a.bmap + bRow0 + col) : col);
             if (key > cb) {
               cw = max(cw, (uint32_t)(cb >> kIndexBits));
               cb = key;

@@ -113,6 +113,19 @@ def lib() -> C.CDLL:
         L.v3dm_batch_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
         L.v3dm_batch_last_launches.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_batch_work.argtypes = [vp, i64p, i64p]
+        fp = C.POINTER(C.c_float)
+        L.v3dm_projection_create.argtypes = [C.POINTER(vp), i32, C.c_ulonglong]
+        L.v3dm_projection_destroy.argtypes = [vp]
+        L.v3dm_projection_get_params.argtypes = [vp, vp]
+        L.v3dm_projection_set_params.argtypes = [vp, vp]
+        L.v3dm_projection_loss_grad.argtypes = [vp, vp, vp, i32, f32, fp, vp]
+        L.v3dm_projection_train_step.argtypes = [vp, vp, vp, i32, f32, f32, fp]
+        L.v3dm_projection_embed.argtypes = [vp, vp, i32, vp]
+        L.v3dm_projection_set_cells.argtypes = [vp, i32, vp]
+        L.v3dm_projection_assign.argtypes = [vp, vp, i32, i32, vp]
+        L.v3dm_batch_match_proposal.argtypes = [vp, vp, i32, f32, f32, vp, i64, i64p]
+        L.v3dm_batch_match_proposal_device.argtypes = [vp, vp, i32, f32, f32, vp]
+        L.v3dm_batch_proposal_scored.argtypes = [vp, i64p, i64p]
         _lib = L
     return _lib
 
@@ -406,11 +419,42 @@ class BatchMatching:
 
     def match_per_pair(self, min_score: float = 0.9, min_ratio: float = 0.8):
         """List with one (n, 2) (left, right) array per pair of the table."""
-        t = self.match(min_score, min_ratio)
+        return self.split_pairs(self.match(min_score, min_ratio))
+
+    def split_pairs(self, t: np.ndarray):
+        """(pair, left, right) triples -> one (n, 2) array per pair of the table."""
         order = np.argsort(t[:, 0], kind="stable")
         t = t[order]
         bounds = np.searchsorted(t[:, 0], np.arange(self.n_pairs + 1))
         return [t[bounds[k]:bounds[k + 1], 1:].copy() for k in range(self.n_pairs)]
+
+    def match_proposal(self, projection, probes: int, min_score: float = 0.9, min_ratio: float = 0.8,
+                       cap: int | None = None) -> np.ndarray:
+        """Candidate-proposal matching (v3dm_batch_match_proposal): triples like match()."""
+        cap = cap if cap is not None else max(1 << 20, getattr(self, "_last_n", 0))
+        while True:
+            out = np.empty((max(1, cap), 3), np.int32)
+            n = C.c_longlong(0)
+            st = lib().v3dm_batch_match_proposal(self._h, projection.handle, probes, min_score, min_ratio, _ptr(out),
+                                                 cap, C.byref(n))
+            if st == ERR_CAPACITY:
+                cap = n.value
+                continue
+            _check(st, "batch_match_proposal")
+            self._last_n = n.value
+            return out[: n.value].copy()
+
+    def match_proposal_device(self, projection, probes: int, min_score: float, min_ratio: float,
+                              d_count: int = 0) -> None:
+        _check(lib().v3dm_batch_match_proposal_device(self._h, projection.handle, probes, min_score, min_ratio,
+                                                      C.c_void_p(d_count) if d_count else None),
+               "batch_match_proposal_device")
+
+    def proposal_scored(self):
+        """(pairs of descriptors the last proposal call scored, sum over pairs of nL * nR)."""
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        _check(lib().v3dm_batch_proposal_scored(self._h, C.byref(a), C.byref(b)), "batch_proposal_scored")
+        return a.value, b.value
 
     def match_device(self, min_score: float, min_ratio: float, d_count: int = 0) -> None:
         _check(lib().v3dm_batch_match_device(self._h, min_score, min_ratio, C.c_void_p(d_count) if d_count else None),
@@ -468,3 +512,75 @@ class BatchMatching:
         ops, n = C.c_longlong(0), C.c_longlong(0)
         _check(lib().v3dm_batch_work(self._h, C.byref(ops), C.byref(n)), "batch_work")
         return ops.value, n.value
+
+
+PROJ_PARAMS = 10336
+PROJ_MAX_CELLS = 64
+PROJ_MAX_PROBES = 4
+PROJ_MAX_BATCH = 4096
+
+
+class Projection:
+    """The learned 128 -> 64 -> 32 projection of the proposal matcher (v3dm_projection_*)."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_projection_create(C.byref(h), device, seed), "projection_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_projection_destroy(self._h)
+        self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def params(self) -> np.ndarray:
+        out = np.empty(PROJ_PARAMS, np.float32)
+        _check(lib().v3dm_projection_get_params(self._h, _ptr(out)), "projection_get_params")
+        return out
+
+    def set_params(self, params) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        if p.shape != (PROJ_PARAMS,):
+            raise ValueError(f"params must have {PROJ_PARAMS} entries")
+        _check(lib().v3dm_projection_set_params(self._h, _ptr(p)), "projection_set_params")
+
+    def loss_grad(self, anchors: np.ndarray, positives: np.ndarray, temperature: float):
+        a = np.ascontiguousarray(anchors, np.uint8)
+        p = np.ascontiguousarray(positives, np.uint8)
+        g = np.empty(PROJ_PARAMS, np.float32)
+        loss = C.c_float(0)
+        _check(lib().v3dm_projection_loss_grad(self._h, _ptr(a), _ptr(p), a.shape[0], temperature, C.byref(loss),
+                                               _ptr(g)), "projection_loss_grad")
+        return loss.value, g
+
+    def train_step(self, d_anchors: int, d_positives: int, batch: int, temperature: float, lr: float,
+                   want_loss: bool = False):
+        loss = C.c_float(0)
+        _check(lib().v3dm_projection_train_step(self._h, C.c_void_p(d_anchors), C.c_void_p(d_positives), batch,
+                                                temperature, lr, C.byref(loss) if want_loss else None),
+               "projection_train_step")
+        return loss.value if want_loss else None
+
+    def embed(self, desc: np.ndarray) -> np.ndarray:
+        d = np.ascontiguousarray(desc, np.uint8)
+        z = np.empty((d.shape[0], 32), np.float32)
+        _check(lib().v3dm_projection_embed(self._h, _ptr(d), d.shape[0], _ptr(z)), "projection_embed")
+        return z
+
+    def set_cells(self, centroids: np.ndarray) -> None:
+        c = np.ascontiguousarray(centroids, np.float32)
+        if c.ndim != 2 or c.shape[1] != 32:
+            raise ValueError("centroids must be (C, 32)")
+        _check(lib().v3dm_projection_set_cells(self._h, c.shape[0], _ptr(c)), "projection_set_cells")
+
+    def assign(self, desc: np.ndarray, probes: int) -> np.ndarray:
+        d = np.ascontiguousarray(desc, np.uint8)
+        out = np.empty((d.shape[0], probes), np.uint8)
+        _check(lib().v3dm_projection_assign(self._h, _ptr(d), d.shape[0], probes, _ptr(out)), "projection_assign")
+        return out

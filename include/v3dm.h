@@ -217,6 +217,54 @@ V3DM_API int v3dm_batch_last_launches(v3dm_batch* b, int* n);
  * int8 operations, and the number of pairs. */
 V3DM_API int v3dm_batch_work(v3dm_batch* b, long long* int8Ops, long long* nPairs);
 
+/* Candidate-proposal matching of every pair (no counterpart in the reference; see the learned
+ * projection below): left l and right r are candidates when r's best cell of the projection
+ * is among l's 'probes' best cells; decisions, ratio test and mutual filter are the
+ * reference's (.cu:133-210, :546-551) applied to the candidate scores, which are exact uint8
+ * scores.  Same output as v3dm_batch_match.  A true match is found when its two descriptors
+ * share a probed cell; recall against v3dm_batch_match is what the projection is trained for. */
+typedef struct v3dm_projection v3dm_projection;
+V3DM_API int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
+                                       float minRatio, int32_t* triples, long long cap, long long* nOut);
+V3DM_API int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
+                                              float minRatio, int32_t* d_count);
+/* (left, right) pairs the last proposal call scored, and the exhaustive count sum(nL * nR). */
+V3DM_API int v3dm_batch_proposal_scored(v3dm_batch* b, long long* scored, long long* exhaustive);
+
+/* ---- learned candidate proposal ----------------------------------------------------- */
+/* No counterpart in the reference: a learned projection f(x) = W2 relu(W1 x + b1) + b2
+ * (128 -> 64 -> 32, x = u / 512, BF16 weights, FP32 accumulation, FP32 master copies) trained
+ * on the GPU with a symmetric InfoNCE loss on matched descriptor pairs, and C cells (unit
+ * centroids) in its output space.  The proposal matcher (v3dm_batch_match_proposal) scores a
+ * left descriptor exactly, in uint8, against the right descriptors whose best cell is among
+ * the left's 'probes' best cells; exhaustive matching stays the reference result.
+ * Parameter layout (V3DM_PROJ_PARAMS floats): W1[64][128], b1[64], W2[32][64], b2[32]. */
+#define V3DM_PROJ_PARAMS 10336
+#define V3DM_PROJ_MAX_CELLS 64
+#define V3DM_PROJ_MAX_PROBES 4
+#define V3DM_PROJ_MAX_BATCH 4096
+
+/* Creates the network with seeded He-uniform weights and zero biases. */
+V3DM_API int v3dm_projection_create(v3dm_projection** out, int device, unsigned long long seed);
+V3DM_API int v3dm_projection_destroy(v3dm_projection* p);
+V3DM_API int v3dm_projection_get_params(v3dm_projection* p, float* params);
+/* Sets the FP32 master parameters (and their BF16 copies); resets the optimiser state. */
+V3DM_API int v3dm_projection_set_params(v3dm_projection* p, const float* params);
+/* Loss and gradient (V3DM_PROJ_PARAMS floats, grad may be NULL) of a batch of B matched pairs
+ * (anchors[k], positives[k]), uint8 descriptors in host memory, temperature T; no update. */
+V3DM_API int v3dm_projection_loss_grad(v3dm_projection* p, const uint8_t* anchors, const uint8_t* positives, int B,
+                                       float temperature, float* loss, float* grad);
+/* One Adam step (beta 0.9 / 0.999) on a batch in device memory; *loss (host, may be NULL)
+ * receives the batch loss before the step. */
+V3DM_API int v3dm_projection_train_step(v3dm_projection* p, const uint8_t* d_anchors, const uint8_t* d_positives,
+                                        int B, float temperature, float lr, float* loss);
+/* Unit-length 32-d outputs of n descriptors (host memory). */
+V3DM_API int v3dm_projection_embed(v3dm_projection* p, const uint8_t* desc, int n, float* z);
+/* The C cells (C x 32 floats, unit vectors). */
+V3DM_API int v3dm_projection_set_cells(v3dm_projection* p, int nCells, const float* centroids);
+/* The 'probes' best cells of n descriptors, best first (n x probes bytes, host memory). */
+V3DM_API int v3dm_projection_assign(v3dm_projection* p, const uint8_t* desc, int n, int probes, uint8_t* cells);
+
 /* ---- vocabulary tree (V3D_CUDA::VocabularyTreeTraversal<BF, Depth>) --------------- */
 typedef struct v3dm_voctree v3dm_voctree;
 
