@@ -8,6 +8,7 @@
 // guided calls compound.  Here no score matrix exists; a guided call re-runs the fused
 // kernel with every gate recorded since the last putative call, which yields the same
 // masked matrix and therefore the same matches.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -63,6 +64,18 @@ struct v3dm_matcher {
   int* dFlagB = nullptr;          // rights to re-score exactly
   int* dCounters = nullptr;       // [0] chosen rights, [1] flagged lefts, [2] flagged rights
   int lastLaunches = 0;
+  // Float descriptors that are not u/512 (tcgen05 kernel): BF16 hi/lo operand layouts
+  // (v3dm_match_f.cu), 6 planes of cap rows x 128 bytes each.
+  bool floatL = false, floatR = false;  // the side's current descriptors are float
+  int capFL = 0, capFR = 0;
+  uint8_t* dLfA = nullptr;  // lefts, A layout (pass A operand)
+  uint8_t* dLfB = nullptr;  // lefts, B layout (pass B operand)
+  uint8_t* dRfA = nullptr;  // rights, A layout (gathered into dRcf)
+  uint8_t* dRfB = nullptr;  // rights, B layout (pass A operand)
+  uint8_t* dRcf = nullptr;  // chosen rights, A layout (pass B operand)
+  bool fBound = false;
+  CUtensorMap fmA_A, fmA_B, fmB_A, fmB_B;
+  int numSMs = 148;
   // Optional CUDA-event timing of the fused matching kernel (v3dm_matcher_profile).
   bool profile = false;
   std::vector<cudaEvent_t> evPool;
@@ -124,6 +137,14 @@ void free_buffers(v3dm_matcher* h) {
   dfree(h->dFlagA);
   dfree(h->dFlagB);
   dfree(h->dCounters);
+  dfree(h->dLfA);
+  dfree(h->dLfB);
+  dfree(h->dRfA);
+  dfree(h->dRfB);
+  dfree(h->dRcf);
+  h->floatL = h->floatR = false;
+  h->capFL = h->capFR = 0;
+  h->fBound = false;
   if (h->hInfo) cudaFreeHost(h->hInfo);
   h->hInfo = nullptr;
   h->allocated = false;
@@ -325,6 +346,7 @@ int v3dm_matcher_create(v3dm_matcher** out, int device, unsigned kernel) {
     delete h;
     return V3DM_ERR_CUDA;
   }
+  h->numSMs = prop.multiProcessorCount;
   if (kernel == V3DM_KERNEL_TCGEN05 && tc_plan_create(&h->tc, device) != cudaSuccess) {
     cudaStreamDestroy(h->stream);
     delete h;
@@ -429,8 +451,70 @@ int set_features_u8(v3dm_matcher* h, bool left, int n, const uint8_t* desc, bool
     V3DM_CUDA_TRY(cudaMemcpyAsync(dst, desc, (size_t)n * kDescBytes,
                                   onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
   (left ? h->nL : h->nR) = n;
+  (left ? h->floatL : h->floatR) = false;
   h->tcBound = false;
   return V3DM_OK;
+}
+
+// Float operand layouts of both sides (allocated on first use, kept until deallocate).
+cudaError_t alloc_float(v3dm_matcher* h) {
+  if (h->dLfA) return cudaSuccess;
+  const int capL = std::max(256, (h->nMaxL + 255) / 256 * 256), capR = std::max(256, (h->nMaxR + 255) / 256 * 256);
+  cudaError_t e = dalloc(&h->dLfA, (size_t)capL * kFloatRowBytes);
+  if (e == cudaSuccess) e = dalloc(&h->dLfB, (size_t)capL * kFloatRowBytes);
+  if (e == cudaSuccess) e = dalloc(&h->dRfA, (size_t)capR * kFloatRowBytes);
+  if (e == cudaSuccess) e = dalloc(&h->dRfB, (size_t)capR * kFloatRowBytes);
+  if (e == cudaSuccess) e = dalloc(&h->dRcf, (size_t)capR * kFloatRowBytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dLfA, 0, (size_t)capL * kFloatRowBytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dLfB, 0, (size_t)capL * kFloatRowBytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dRfA, 0, (size_t)capR * kFloatRowBytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dRfB, 0, (size_t)capR * kFloatRowBytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dRcf, 0, (size_t)capR * kFloatRowBytes, h->stream);
+  if (e != cudaSuccess) {
+    dfree(h->dLfA);
+    dfree(h->dLfB);
+    dfree(h->dRfA);
+    dfree(h->dRfB);
+    dfree(h->dRcf);
+    return e;
+  }
+  h->capFL = capL;
+  h->capFR = capR;
+  h->fBound = false;
+  return cudaSuccess;
+}
+
+// The staged floats (h->dStage, n descriptors) into the side's BF16 hi/lo layouts.
+int stage_to_float(v3dm_matcher* h, bool left, int n) {
+  V3DM_CUDA_TRY(alloc_float(h));
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream));
+  V3DM_CUDA_TRY(launch_hilo(h->dStage, nullptr, n, left ? h->capFL : h->capFR, left ? h->dLfA : h->dRfA,
+                            left ? h->dLfB : h->dRfB, h->dInfo + kInfoErr, h->stream));
+  V3DM_CUDA_TRY(cudaMemcpyAsync(h->hInfo + kInfoErr, h->dInfo + kInfoErr, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                h->stream));
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->hInfo[kInfoErr]) {  // a value that is not finite
+    (left ? h->nL : h->nR) = 0;
+    cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream);
+    return V3DM_ERR_ARG;
+  }
+  (left ? h->nL : h->nR) = n;
+  (left ? h->floatL : h->floatR) = true;
+  h->tcBound = false;
+  return V3DM_OK;
+}
+
+// Float descriptors scored with the BF16 hi/lo split whatever their values.
+int set_features_bf16x3(v3dm_matcher* h, bool left, int n, const float* desc) {
+  if (!h || n < 0 || (n > 0 && !desc)) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  if (h->kernel == V3DM_KERNEL_SIMT) return V3DM_ERR_UNSUPPORTED;
+  if (n > (left ? h->nMaxL : h->nMaxR)) return V3DM_ERR_SIZE;
+  DeviceGuard g(h->device);
+  if (n > 0)
+    V3DM_CUDA_TRY(cudaMemcpyAsync(h->dStage, desc, (size_t)n * kDescBytes * sizeof(float), cudaMemcpyHostToDevice,
+                                  h->stream));
+  return stage_to_float(h, left, n);
 }
 
 int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
@@ -447,12 +531,17 @@ int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
     V3DM_CUDA_TRY(cudaMemcpyAsync(h->hInfo + kInfoErr, h->dInfo + kInfoErr, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (h->hInfo[kInfoErr] & kErrNotU8) {
-      (left ? h->nL : h->nR) = 0;
       cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream);
-      return V3DM_ERR_NOT_U8;
+      if (h->kernel == V3DM_KERNEL_SIMT) {
+        (left ? h->nL : h->nR) = 0;
+        return V3DM_ERR_NOT_U8;
+      }
+      // not of the form u/512: the tcgen05 handle scores these with the BF16 hi/lo split
+      return stage_to_float(h, left, n);
     }
   }
   (left ? h->nL : h->nR) = n;
+  (left ? h->floatL : h->floatR) = false;
   h->tcBound = false;
   return V3DM_OK;
 }
@@ -643,6 +732,92 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   return V3DM_OK;
 }
 
+// Float path (either side holds float descriptors): the same two side passes and decisions with
+// BF16 hi/lo scores (v3dm_match_f.cu).  A side holding u/512 descriptors gets its float layouts
+// from its uint8 values, which is exact.
+int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
+  const float Tf = host_float_threshold(minScore, minRatio);
+  V3DM_CUDA_TRY(alloc_float(h));
+  if (!h->floatL)
+    V3DM_CUDA_TRY(launch_hilo(nullptr, h->dL, h->nL, h->capFL, h->dLfA, h->dLfB, h->dInfo + kInfoErr, h->stream));
+  if (!h->floatR)
+    V3DM_CUDA_TRY(launch_hilo(nullptr, h->dR, h->nR, h->capFR, h->dRfA, h->dRfB, h->dInfo + kInfoErr, h->stream));
+  if (!h->fBound) {
+    V3DM_CUDA_TRY(f_maps(&h->fmA_A, h->dLfA, h->capFL, &h->fmA_B, h->dRfB, h->capFR));
+    V3DM_CUDA_TRY(f_maps(&h->fmB_A, h->dRcf, h->capFR, &h->fmB_B, h->dLfB, h->capFL));
+    h->fBound = true;
+  }
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dCounters, 0, 4 * sizeof(int), h->stream));
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.records = h->dRecords;
+  sa.segCount = h->dSegCount;
+  sa.segCap = h->segCap;
+  sa.nSeg = h->nSeg;
+  sa.err = h->dInfo + kInfoErr;
+  PostArgs pa;
+  std::memset(&pa, 0, sizeof(pa));
+  pa.records = h->dRecords;
+  pa.list = h->dCand;
+  pa.segCount = h->dSegCount;
+  pa.segCap = h->segCap;
+  pa.nSeg = f_segments(h->numSMs);
+  pa.nGates = h->nGates;
+  pa.gatesDev = h->dGates;
+  pa.minScore = minScore;
+  pa.minRatio = minRatio;
+  pa.err = h->dInfo + kInfoErr;
+  cudaEvent_t evA[2], evB[2];
+  // pass A: every left against every right
+  sa.nA = h->nL;
+  sa.nB = h->nR;
+  sa.aIsLeft = 1;
+  sa.best = h->dLBest;
+  sa.sec = h->dLSec;
+  if (h->profile) {
+    int e = event_pair(h, 0, evA);
+    if (e != V3DM_OK) return e;
+    V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
+  }
+  V3DM_CUDA_TRY(launch_side_f(h->fmA_A, h->fmA_B, sa, Tf, nullptr, h->numSMs, h->stream));
+  if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
+  pa.nRows = h->nL;
+  pa.aIsLeft = 1;
+  pa.best = h->dLBest;
+  pa.sec = h->dLSec;
+  pa.decision = h->dLeftDec;
+  V3DM_CUDA_TRY(launch_post_f(pa, Tf, h->stream));
+  V3DM_CUDA_TRY(launch_choose_f(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dRfA, h->capFR,
+                                h->dRcf, h->capFR, h->stream));
+  // pass B: the chosen rights against every left
+  sa.nAptr = h->dCounters;
+  sa.nA = h->nR;
+  sa.nB = h->nL;
+  sa.amap = h->dChosenList;
+  sa.aIsLeft = 0;
+  sa.best = h->dRBest;
+  sa.sec = h->dRSec;
+  if (h->profile) {
+    int e = event_pair(h, 1, evB);
+    if (e != V3DM_OK) return e;
+    V3DM_CUDA_TRY(cudaEventRecord(evB[0], h->stream));
+  }
+  V3DM_CUDA_TRY(launch_side_f(h->fmB_A, h->fmB_B, sa, Tf, nullptr, h->numSMs, h->stream));
+  if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evB[1], h->stream));
+  pa.nRows = h->nR;
+  pa.rowsPtr = h->dCounters;
+  pa.amap = h->dChosenList;
+  pa.aIsLeft = 0;
+  pa.best = h->dRBest;
+  pa.sec = h->dRSec;
+  pa.decision = h->dRightDec;
+  V3DM_CUDA_TRY(launch_post_f(pa, Tf, h->stream));
+  V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
+                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->stream));
+  h->lastLaunches = (h->floatL ? 0 : 1) + (h->floatR ? 0 : 1) + 11;
+  return V3DM_OK;
+}
+
 // Enqueues one matching call for the current gates; the result lands in dPairs / dInfo on
 // the handle's stream.
 int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
@@ -656,6 +831,8 @@ int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPai
     st = V3DM_OK;  // no pairs: the info block already says so
   } else if (h->kernel == V3DM_KERNEL_SIMT) {
     st = enqueue_match_simt(h, minScore, minRatio, dPairs);
+  } else if (h->floatL || h->floatR) {
+    st = enqueue_match_f(h, minScore, minRatio, dPairs);
   } else {
     st = enqueue_match_tc(h, minScore, minRatio, dPairs);
   }
@@ -749,6 +926,55 @@ int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_feat
 int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, false, n, d, false); }
 int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, true, n, d); }
 int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, false, n, d); }
+int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, true, n, d); }
+int v3dm_set_right_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, false, n, d); }
+
+int v3dm_float_threshold(float minScore, float minRatio, float* T) {
+  if (!T) return V3DM_ERR_ARG;
+  *T = host_float_threshold(minScore, minRatio);
+  return V3DM_OK;
+}
+
+int v3dm_scores_f32(v3dm_matcher* h, float* scores) {
+  if (!h || !scores) return V3DM_ERR_ARG;
+  if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
+  if (h->kernel == V3DM_KERNEL_SIMT) return V3DM_ERR_UNSUPPORTED;
+  const long long n = (long long)h->nL * h->nR;
+  if (n > (1LL << 26)) return V3DM_ERR_SIZE;
+  if (n == 0) return V3DM_OK;
+  DeviceGuard g(h->device);
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  V3DM_CUDA_TRY(alloc_float(h));
+  if (!h->floatL)
+    V3DM_CUDA_TRY(launch_hilo(nullptr, h->dL, h->nL, h->capFL, h->dLfA, h->dLfB, h->dInfo + kInfoErr, h->stream));
+  if (!h->floatR)
+    V3DM_CUDA_TRY(launch_hilo(nullptr, h->dR, h->nR, h->capFR, h->dRfA, h->dRfB, h->dInfo + kInfoErr, h->stream));
+  if (!h->fBound) {
+    V3DM_CUDA_TRY(f_maps(&h->fmA_A, h->dLfA, h->capFL, &h->fmA_B, h->dRfB, h->capFR));
+    V3DM_CUDA_TRY(f_maps(&h->fmB_A, h->dRcf, h->capFR, &h->fmB_B, h->dLfB, h->capFL));
+    h->fBound = true;
+  }
+  float* dS = nullptr;
+  V3DM_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&dS), (size_t)n * sizeof(float)));
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.records = h->dRecords;
+  sa.segCount = h->dSegCount;
+  sa.segCap = h->segCap;
+  sa.nSeg = h->nSeg;
+  sa.err = h->dInfo + kInfoErr;
+  sa.nA = h->nL;
+  sa.nB = h->nR;
+  sa.aIsLeft = 1;
+  // Tf = +inf: no chunk is handed over, only the dump is written
+  cudaError_t e = launch_side_f(h->fmA_A, h->fmA_B, sa, INFINITY, dS, h->numSMs, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(scores, dS, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dS);
+  if (e != cudaSuccess) return cuda_fail(e, "scores_f32", __LINE__);
+  return V3DM_OK;
+}
 
 int v3dm_putative(v3dm_matcher* h, float minScore, float minRatio, int32_t* pairs, int cap, int* nOut) {
   if (!h || (cap > 0 && !pairs) || cap < 0) return V3DM_ERR_ARG;

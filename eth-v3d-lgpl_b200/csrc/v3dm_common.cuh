@@ -19,6 +19,7 @@
 // The final decision therefore equals the reference's scan over all scores.
 #pragma once
 #include <stdint.h>
+#include <cstring>
 
 #ifdef __CUDACC__
 #define V3DM_HD __host__ __device__ __forceinline__
@@ -83,6 +84,41 @@ V3DM_HD int32_t decide(uint64_t bestKey, uint32_t secondP1, float minScore, floa
   int32_t idx = (int32_t)(kIndexMask - (uint32_t)(bestKey & kIndexMask));
   float s2 = secondP1 ? score_of((int32_t)secondP1 - 1) : kNone;
   return accept_scores(score_of(S1), s2, minScore, minRatio) ? idx : -1;
+}
+
+// ---- float scores (BF16 hi/lo path) ------------------------------------------------------
+// Order-preserving map of a float to a 32-bit key (larger float -> larger key, every real value
+// -> key >= 1, so 0 can mean "none").
+V3DM_HD uint32_t f32_order(float f) {
+#ifdef __CUDA_ARCH__
+  const uint32_t u = __float_as_uint(f);
+#else
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+#endif
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+V3DM_HD float f32_unorder(uint32_t k) {
+  const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+// Best key of a float score: larger score, then lower index.
+V3DM_HD uint64_t best_key_f(float s, int32_t idx) {
+  return ((uint64_t)f32_order(s) << kIndexBits) | (uint64_t)(kIndexMask - (uint32_t)idx);
+}
+// Decision of one feature from a float best key and the ordered second score (0: none).
+V3DM_HD int32_t decide_f(uint64_t bestKey, uint32_t secondOrd, float minScore, float minRatio) {
+  if (bestKey == 0) return -1;
+  const float s1 = f32_unorder((uint32_t)(bestKey >> kIndexBits));
+  const int32_t idx = (int32_t)(kIndexMask - (uint32_t)(bestKey & kIndexMask));
+  const float s2 = secondOrd ? f32_unorder(secondOrd) : kNone;
+  return accept_scores(s1, s2, minScore, minRatio) ? idx : -1;
 }
 
 // Guided gate, one per guided call since the last putative call (the reference masks the

@@ -136,6 +136,22 @@ struct PostArgs {
   int* err;
 };
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s);
+// The list pass alone (k_list).
+cudaError_t launch_list(const PostArgs& a, int32_t* info, cudaStream_t s);
+
+// ---- float descriptors: BF16 hi/lo scores (v3dm_match_f.cu) ------------------------------
+// Operand layouts: 6 planes of rowsCap x 128 bytes (64 BF16 values of a K slice per row).
+constexpr int kFloatRowBytes = 768;
+int f_segments(int numSMs);
+cudaError_t f_maps(CUtensorMap* mA, const void* dA, int rowsA, CUtensorMap* mB, const void* dB, int rowsB);
+cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf, float* dump,
+                          int numSMs, cudaStream_t st);
+cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s);
+cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, void* la, void* lb, int* err,
+                        cudaStream_t s);
+cudaError_t launch_choose_f(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                            const void* rA, int capA, void* rc, int capC, cudaStream_t s);
+float host_float_threshold(float minScore, float minRatio);
 // Exact re-score of the flagged descriptors of side A against side B.
 struct RescoreArgs {
   const uint8_t* descA;          // side A descriptors by index

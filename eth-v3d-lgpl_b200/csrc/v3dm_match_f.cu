@@ -1,0 +1,485 @@
+// v3dm_match_f.cu -- float descriptors: scores from a BF16 hi/lo split on the tensor cores.
+//
+// The reference scores float descriptors with cublasSgemm (v3d_cudamatching.cu:529-530).  For
+// descriptors that are not of the exact u/512 form (the integer path's domain), each value x is
+// split into hi = bf16(x) and lo = bf16(x - hi), and
+//   score(a, b) = hi_a . hi_b + lo_a . hi_b + hi_a . lo_b       (the lo . lo term is dropped)
+// is one K = 384 GEMM with FP32 accumulation: A rows hold [hi | lo | hi], B rows [hi | hi | lo]
+// (tcgen05.mma.kind::f16, BF16 x BF16 -> F32 in TMEM).  For u/512 inputs hi is exact and lo = 0,
+// so the scores equal the integer path's exactly.
+//
+// Selection differs from the integer path in one point: the side kernel hands over every
+// 32-score chunk whose maximum reaches Tf, the float candidate threshold -- the smallest score a
+// second value must reach to change any decision (scores below it never matter, see
+// host_float_threshold).  k_records_f then sees every score that matters, so the best and the
+// second value are exact for the float scores and no re-score pass exists.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "v3dm_device.cuh"
+#include "v3dm_tcgen05.cuh"
+
+namespace v3dm {
+
+namespace {
+
+constexpr int kFM = 128;            // rows per MMA (TMEM lanes)
+constexpr int kFN = 64;             // B rows per tile
+constexpr int kFStages = 2;         // B tile ring
+constexpr int kFPlanes = 6;         // 128-byte K planes per row (384 BF16 values)
+constexpr int kFSteps = 24;         // K = 16 per MMA
+constexpr int kFAcc = 4;            // TMEM accumulator stages of kFN columns
+constexpr int kFTmemCols = 256;
+constexpr int kFEpiWarps = 4;       // one per TMEM lane quadrant
+constexpr int kFThreads = (2 + kFEpiWarps) * 32;
+
+struct SmemF {
+  uint8_t a[kFPlanes][kFM][128];              // 96 KB, one A group
+  uint8_t b[kFStages][kFPlanes][kFN][128];    // 2 x 48 KB
+  unsigned long long fullB[kFStages], emptyB[kFStages];
+  unsigned long long fullA, emptyA;
+  unsigned long long accFull[kFAcc], accEmpty[kFAcc];
+  unsigned long long mmaDone;
+  uint32_t tmemBase;
+  int abort;
+};
+
+// kind::f16, D = F32, A = B = BF16, both K-major, M = 128, N = kFN.
+__device__ __forceinline__ constexpr uint32_t idesc_f16() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kFN >> 3) << 17) | ((uint32_t)(kFM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(ad), "l"(bd), "r"(idesc_f16()), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ float fmax32(const float* v) {
+  float m[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) m[i] = fmaxf(v[i], v[i + 16]);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) m[i] = fmaxf(m[i], m[i + 8]);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], m[i + 4]);
+  return fmaxf(fmaxf(m[0], m[2]), fmaxf(m[1], m[3]));
+}
+
+// One pair: side A (nA rows, amap as in k_side) against side B (nB rows).  Same roles and
+// bounded waits as k_side; the A group is single-buffered (96 KB).  With 'dump' set (small
+// diagnostic calls) every score is also written to dump[index * nB + column].
+__global__ void __launch_bounds__(kFThreads, 1)
+k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, SideArgs a, float Tf,
+         float* dump) {
+  extern __shared__ uint8_t smemRaw[];
+  SmemF& s = *reinterpret_cast<SmemF*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nA = a.nAptr ? *a.nAptr : a.nA;
+  const int nTiles = (a.nB + kFN - 1) / kFN;
+  const long long nWork = (long long)((nA + kFM - 1) / kFM) * nTiles;
+  if (nWork == 0) {
+    if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kFEpiWarps + (warp - 2)] = 0;
+    return;
+  }
+  const long long w0 = nWork * blockIdx.x / gridDim.x, w1 = nWork * (blockIdx.x + 1) / gridDim.x;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kFStages; ++i) {
+      mbar_init(&s.fullB[i], 1);
+      mbar_init(&s.emptyB[i], 1);
+    }
+    mbar_init(&s.fullA, 1);
+    mbar_init(&s.emptyA, 1);
+    for (int i = 0; i < kFAcc; ++i) {
+      mbar_init(&s.accFull[i], 1);
+      mbar_init(&s.accEmpty[i], kFEpiWarps);
+    }
+    mbar_init(&s.mmaDone, 1);
+    s.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmemBase)),
+                 "r"(kFTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmemBase;
+  __syncthreads();
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0 && !s.abort) {
+      int stage = 0, groups = 0;
+      uint32_t phase = 0;
+      uint32_t armedPhase[kFStages] = {};
+      bool armed[kFStages] = {};
+      for (long long w = w0; w < w1; ++w) {
+        const int g = (int)(w / nTiles), t = (int)(w - (long long)g * nTiles);
+        if (w == w0 || t == 0) {
+          // the previous group's MMAs must be done with the single A buffer
+          if (groups > 0 && !mbar_wait(&s.emptyA, (groups - 1) & 1, &s.abort, a.err)) break;
+          mbar_expect_tx(&s.fullA, (uint32_t)sizeof(s.a));
+          tma_load_3d(&s.a[0][0][0], &tmA, &s.fullA, 0, g * kFM, 0);
+          ++groups;
+        }
+        if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
+        mbar_expect_tx(&s.fullB[stage], (uint32_t)sizeof(s.b[0]));
+        tma_load_3d(&s.b[stage][0][0][0], &tmB, &s.fullB[stage], 0, t * kFN, 0);
+        armed[stage] = true;
+        armedPhase[stage] = phase;
+        if (++stage == kFStages) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      // Drain: every load this thread issued has landed before the CTA may exit.
+      for (int i = 0; i < kFStages; ++i)
+        if (armed[i]) {
+          long long t0c = clock64();
+          while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
+          }
+        }
+      if (groups > 0) {
+        long long t0c = clock64();
+        while (!mbar_try(&s.fullA, (groups - 1) & 1) && clock64() - t0c < kWaitCycles) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0 && !s.abort) {
+      int stage = 0, acc = 0, groups = 0;
+      uint32_t phase = 0, accPhase = 0;
+      const uint32_t aBase = smem_u32(&s.a[0][0][0]);
+      for (long long w = w0; w < w1; ++w) {
+        const int t = (int)(w % nTiles);
+        if (w == w0 || t == 0) {
+          if (groups > 0) mma_commit(&s.emptyA);  // A buffer free once the previous group's MMAs end
+          if (!mbar_wait(&s.fullA, groups & 1, &s.abort, a.err)) break;
+          ++groups;
+        }
+        if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
+        if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) break;
+        tc_fence_after();
+        const uint32_t bBase = smem_u32(&s.b[stage][0][0][0]);
+        const uint32_t d = tmem + (uint32_t)(acc * kFN);
+#pragma unroll
+        for (int k = 0; k < kFSteps; ++k) {
+          const uint32_t off = (uint32_t)((k & 3) * 32);
+          const uint32_t pl = (uint32_t)(k >> 2);
+          mma_bf16(d, sdesc(aBase + pl * (kFM * 128) + off), sdesc(bBase + pl * (kFN * 128) + off), k > 0 ? 1u : 0u);
+        }
+        mma_commit(&s.emptyB[stage]);
+        mma_commit(&s.accFull[acc]);
+        if (++stage == kFStages) {
+          stage = 0;
+          phase ^= 1;
+        }
+        if (++acc == kFAcc) {
+          acc = 0;
+          accPhase ^= 1;
+        }
+      }
+      // Every MMA this thread issued has completed before TMEM is released.
+      mma_commit(&s.mmaDone);
+      long long t0c = clock64();
+      while (!mbar_try(&s.mmaDone, 0) && clock64() - t0c < kWaitCycles) {
+      }
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int e = warp - 2;
+    const int q = warp & 3;
+    uint4* const segBase = a.records + (long long)(blockIdx.x * kFEpiWarps + e) * a.segCap * kRecordQuads;
+    int segN = 0;
+    int acc = 0;
+    uint32_t accPhase = 0;
+    bool ok = !s.abort;
+    for (long long w = w0; w < w1 && ok; ++w) {
+      const int g = (int)(w / nTiles), t = (int)(w - (long long)g * nTiles);
+      const int row = g * kFM + q * 32 + lane;
+      const bool rowValid = row < nA;
+      const int orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
+      ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kFN);
+      uint32_t v[2][32];
+      tmem_ld32(tbase, v[0]);
+      tmem_ld32(tbase + 32u, v[1]);
+      tmem_wait(v[0]);
+      tmem_wait(v[1]);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int col0 = t * kFN + 32 * c;
+        if (col0 >= a.nB) break;  // warp-uniform
+        float f[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) f[k] = (col0 + k < a.nB) ? __uint_as_float(v[c][k]) : -INFINITY;
+        if (dump && rowValid)
+          for (int k = 0; k < 32 && col0 + k < a.nB; ++k) dump[(size_t)orig * a.nB + col0 + k] = f[k];
+        const float mx = fmax32(f);
+        const bool trig = rowValid && mx >= Tf;
+        if (__any_sync(0xffffffffu, trig)) {
+          const unsigned m = __ballot_sync(0xffffffffu, trig);
+          if (trig) {
+            const int idx = segN + __popc(m & ((1u << lane) - 1u));
+            if (idx < a.segCap) {
+              uint4* rec = segBase + (long long)idx * kRecordQuads;
+              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)a.nB, 0u);
+#pragma unroll
+              for (int k = 0; k < 8; ++k)
+                rec[1 + k] = make_uint4(v[c][4 * k], v[c][4 * k + 1], v[c][4 * k + 2], v[c][4 * k + 3]);
+            }
+          }
+          segN += __popc(m);
+        }
+      }
+      if (++acc == kFAcc) {
+        acc = 0;
+        accPhase ^= 1;
+      }
+    }
+    if (lane == 0) a.segCount[blockIdx.x * kFEpiWarps + e] = segN;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kFTmemCols)
+                              : "memory");
+}
+
+// Exact float selection on the chunk records: every unmasked score >= Tf is a candidate; the
+// chunk best is the largest candidate (first column on ties), the other candidates bound the
+// second value.  Scores below Tf (and masked ones, which the reference sets to -1e20) cannot
+// change a decision and are left out.
+__global__ void k_records_f(PostArgs a, float Tf) {
+  const int lane = threadIdx.x & 31;
+  const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
+    const int cnt = a.segCount[seg];
+    const long long n = cnt < a.segCap ? cnt : a.segCap;
+    const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
+    unsigned long long* entries = a.list + (long long)seg * a.segCap;
+    for (long long i = lane; i < n; i += 32) {
+      const uint4* rec = recs + i * kRecordQuads;
+      const uint4 head = rec[0];
+      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z;
+      unsigned long long cb = 0;
+      uint32_t cw = 0;
+      for (int k = 0; k < 8; ++k) {
+        const uint4 qd = rec[1 + k];
+        const uint32_t sv[4] = {qd.x, qd.y, qd.z, qd.w};
+        for (int t = 0; t < 4; ++t) {
+          const int col = col0 + 4 * k + t;
+          if (col >= nB) break;
+          const float sc = __uint_as_float(sv[t]);
+          if (!(sc >= Tf)) continue;
+          bool masked = false;
+          for (int gi = 0; gi < a.nGates && !masked; ++gi)
+            masked = gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
+          if (masked) continue;
+          const unsigned long long key = best_key_f(sc, col);
+          if (key > cb) {
+            cw = max(cw, (uint32_t)(cb >> kIndexBits));
+            cb = key;
+          } else {
+            cw = max(cw, f32_order(sc));
+          }
+        }
+      }
+      if (cb) atomicMax(&a.best[orig], cb);
+      if (cw) atomicMax(&a.sec[orig], cw);
+      entries[i] = cb;
+    }
+  }
+}
+
+__global__ void k_decide_f(PostArgs a) {
+  const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
+    const int idx = a.amap ? a.amap[r] : r;
+    const unsigned long long b = a.best[idx];
+    const unsigned s = a.sec[idx];
+    a.decision[idx] = decide_f(b, s, a.minScore, a.minRatio);
+    if (b) a.best[idx] = 0;
+    if (s) a.sec[idx] = 0;
+  }
+}
+
+// A and B layouts of n descriptors: float values (or uint8 values u, read as u / 512) split
+// into BF16 hi and lo.  A row = [hi | lo | hi], B row = [hi | hi | lo] (384 values along K),
+// stored planar: plane p holds K positions 64p .. 64p + 63 of every row, rowsCap rows of 128 B
+// per plane.  Sets *err when a value is not finite.
+__global__ void k_hilo(const float* __restrict__ f, const uint8_t* __restrict__ u, int n, int rowsCap,
+                       __nv_bfloat16* __restrict__ la, __nv_bfloat16* __restrict__ lb, int* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)n * kDescBytes) return;
+  const long long d = i / kDescBytes;
+  const int k = (int)(i % kDescBytes);
+  const float x = f ? f[i] : (float)u[i] * (1.0f / 512.0f);
+  if (!isfinite(x)) atomicOr(err, kErrNotU8);
+  const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+  const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+  const int half = k >> 6, off = k & 63;
+  auto at = [&](__nv_bfloat16* base, int seg) -> __nv_bfloat16& {
+    return base[((size_t)(2 * seg + half) * rowsCap + d) * 64 + off];
+  };
+  at(la, 0) = hi;
+  at(la, 1) = lo;
+  at(la, 2) = hi;
+  at(lb, 0) = hi;
+  at(lb, 1) = hi;
+  at(lb, 2) = lo;
+}
+
+// Rights accepted by some left: de-duplicated, their A-layout rows gathered for pass B.
+__global__ void k_choose_f(const int32_t* __restrict__ leftDec, int nL, int* chosenFlag, int* chosenList,
+                           int* chosenCount, const uint8_t* __restrict__ rA, int capA, uint8_t* __restrict__ rc,
+                           int capC) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nL; l += gridDim.x * blockDim.x) {
+    const int r = leftDec[l];
+    if (r < 0) continue;
+    if (atomicExch(&chosenFlag[r], 1) != 0) continue;
+    const int k = atomicAdd(chosenCount, 1);
+    chosenList[k] = r;
+    for (int p = 0; p < kFPlanes; ++p) {
+      const uint4* src = reinterpret_cast<const uint4*>(rA + ((size_t)p * capA + r) * 128);
+      uint4* dst = reinterpret_cast<uint4*>(rc + ((size_t)p * capC + k) * 128);
+#pragma unroll
+      for (int w = 0; w < 8; ++w) dst[w] = src[w];
+    }
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode_f() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3-D BF16 map over a planar layout (64 values of a K slice, row, plane), box (64, boxRows, 6),
+// 128-byte swizzle: one load fills 6 swizzled [boxRows][128 B] blocks.
+bool encode_f(CUtensorMap* map, const void* base, int rows, int boxRows) {
+  auto fn = get_encode_f();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {64, (cuuint64_t)rows, (cuuint64_t)kFPlanes};
+  cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
+  cuuint32_t box[3] = {64, (cuuint32_t)boxRows, (cuuint32_t)kFPlanes};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int f_segments(int numSMs) { return numSMs * kFEpiWarps; }
+
+cudaError_t f_maps(CUtensorMap* mA, const void* dA, int rowsA, CUtensorMap* mB, const void* dB, int rowsB) {
+  if (rowsA < kFM || rowsB < kFN) return cudaErrorInvalidValue;
+  if (!encode_f(mA, dA, rowsA, kFM) || !encode_f(mB, dB, rowsB, kFN)) return cudaErrorInvalidValue;
+  return cudaSuccess;
+}
+
+cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf, float* dump,
+                          int numSMs, cudaStream_t st) {
+  const size_t smem = sizeof(SmemF) + 1024;
+  static bool attrSet[128] = {};  // per device ordinal
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  if (!attrSet[dev]) {
+    e = cudaFuncSetAttribute(k_side_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attrSet[dev] = true;
+  }
+  const int nTiles = (a.nB + kFN - 1) / kFN;
+  if (nTiles == 0) return cudaSuccess;
+  const long long maxWork = (long long)((a.nA + kFM - 1) / kFM) * nTiles;
+  const int grid = (int)std::min<long long>(numSMs, std::max<long long>(1, maxWork));
+  if (grid * kFEpiWarps > a.nSeg) return cudaErrorInvalidValue;
+  k_side_f<<<grid, kFThreads, smem, st>>>(mA, mB, a, Tf, dump);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s) {
+  int32_t* info = a.err - kInfoErr;
+  const int listBlocks = (a.nSeg * 32 + 255) / 256;
+  k_records_f<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, Tf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = launch_list(a, info, s);
+  if (e != cudaSuccess) return e;
+  const int rows = a.nRows > 0 ? a.nRows : 1;
+  const int blocks = (rows + 255) / 256;
+  k_decide_f<<<blocks < 1024 ? blocks : 1024, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, void* la, void* lb, int* err,
+                        cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (n > rowsCap) return cudaErrorInvalidValue;
+  const long long total = (long long)n * kDescBytes;
+  k_hilo<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(f, u, n, rowsCap, static_cast<__nv_bfloat16*>(la),
+                                                         static_cast<__nv_bfloat16*>(lb), err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_f(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                            const void* rA, int capA, void* rc, int capC, cudaStream_t s) {
+  if (nL == 0) return cudaSuccess;
+  int blocks = (nL + 255) / 256;
+  if (blocks > 148) blocks = 148;
+  k_choose_f<<<blocks, 256, 0, s>>>(leftDec, nL, chosenFlag, chosenList, chosenCount,
+                                    static_cast<const uint8_t*>(rA), capA, static_cast<uint8_t*>(rc), capC);
+  return cudaGetLastError();
+}
+
+// Smallest float score a second value must reach to change any decision.  accept(s1, s2) is
+// monotone: for a fixed s1 it can only turn false as s2 grows, for a fixed s2 only true as s1
+// grows, so the boundary at s1 = the smallest float above minScore bounds every s1.  Without a
+// ratio test (or when no second value can matter) only candidates above minScore are needed.
+float host_float_threshold(float minScore, float minRatio) {
+  const float s1min = std::nextafter(minScore, INFINITY);
+  if (!(minRatio == minRatio) || minRatio < 0.0f || !(minScore == minScore)) return s1min;
+  if (!accept_scores(s1min, kNone, minScore, minRatio)) return s1min;
+  if (accept_scores(s1min, INFINITY, minScore, minRatio)) return s1min;
+  // accept(s1min, unorder(lo)) is true, accept(s1min, unorder(hi)) false
+  uint32_t lo = f32_order(kNone), hi = f32_order(INFINITY);
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (accept_scores(s1min, f32_unorder(mid), minScore, minRatio)) lo = mid;
+    else hi = mid;
+  }
+  const float t = f32_unorder(hi);  // the smallest second value that can flip a decision
+  return t < s1min ? t : s1min;
+}
+
+}  // namespace v3dm

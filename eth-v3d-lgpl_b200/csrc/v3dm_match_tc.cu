@@ -41,6 +41,7 @@
 #include <type_traits>
 
 #include "v3dm_device.cuh"
+#include "v3dm_tcgen05.cuh"
 
 namespace v3dm {
 
@@ -50,7 +51,6 @@ constexpr int BM = 128;          // rows per MMA block (TMEM lanes)
 constexpr int kEpiWarps = 16;    // four per TMEM lane quadrant
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr int kTmemCols = 512;
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 
 template <int NB_, int BN_, int STAGES_>
 struct TcCfg {
@@ -88,65 +88,6 @@ struct TcShape {
   long long nWork;      // nGroups * nTiles
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(unsigned long long* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase with the given parity.  Returns false on timeout or when
-// another role of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, int* abortFlag, int* err) {
-  if (mbar_try(b, parity)) return true;
-  long long t0 = clock64();
-  while (true) {
-    if (mbar_try(b, parity)) return true;
-    if (*reinterpret_cast<volatile int*>(abortFlag)) return false;
-    if (clock64() - t0 > kWaitCycles) {
-      atomicOr(err, kErrWaitTimeout);
-      *reinterpret_cast<volatile int*>(abortFlag) = 1;
-      return false;
-    }
-  }
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, unsigned long long* bar, int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor of a K-major operand stored as 128-byte rows with the
-// 128-byte swizzle: 8-row core groups 1024 bytes apart (SBO), version 1, layout SWIZZLE_128B.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
-         (2ull << 61);
-}
-
 // Instruction descriptor: kind::i8, D = s32, A = B = unsigned 8-bit, both K-major, N, M = 128.
 template <int N>
 __device__ __forceinline__ constexpr uint32_t idesc() {
@@ -161,35 +102,6 @@ __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t ad, uint64_t bd,
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
       "l"(ad), "l"(bd), "r"(idesc<N>()), "r"(accumulate)
       : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(unsigned long long* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Issues a load of 32 lanes x 32 consecutive 32-bit columns; thread i receives lane
-// (base + i).  The registers are valid only after tmem_wait().
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
-        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-      : "r"(taddr));
-}
-
-template <int N>
-__device__ __forceinline__ void tmem_wait(uint32_t (&v)[N]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < N; ++i) asm volatile("" : "+r"(v[i]));  // uses stay after the wait
 }
 
 // Maximum of 32 scores: a balanced tree of two-input integer maxima (ALU pipe, short

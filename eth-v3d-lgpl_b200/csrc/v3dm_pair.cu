@@ -293,6 +293,12 @@ cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_list(const PostArgs& a, int32_t* info, cudaStream_t s) {
+  const int listBlocks = (a.nSeg * 32 + 255) / 256;
+  k_list<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, info);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s) {
   (void)grid;
   const int blocks = (a.nB + kRescoreThreads - 1) / kRescoreThreads;

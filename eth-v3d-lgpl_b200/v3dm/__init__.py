@@ -66,8 +66,11 @@ def lib() -> C.CDLL:
         L.v3dm_matcher_destroy.argtypes = [vp]
         L.v3dm_allocate.argtypes = [vp, i32, i32, i32]
         L.v3dm_deallocate.argtypes = [vp]
-        for n in ("v3dm_set_left_f32", "v3dm_set_right_f32", "v3dm_set_left_u8", "v3dm_set_right_u8"):
+        for n in ("v3dm_set_left_f32", "v3dm_set_right_f32", "v3dm_set_left_u8", "v3dm_set_right_u8",
+                  "v3dm_set_left_f32_bf16x3", "v3dm_set_right_f32_bf16x3"):
             getattr(L, n).argtypes = [vp, i32, vp]
+        L.v3dm_scores_f32.argtypes = [vp, vp]
+        L.v3dm_float_threshold.argtypes = [f32, f32, C.POINTER(C.c_float)]
         L.v3dm_putative.argtypes = [vp, f32, f32, vp, i32, C.POINTER(i32)]
         for n in ("v3dm_guided_F", "v3dm_guided_H"):
             getattr(L, n).argtypes = [vp, f64p, f32, vp, vp, f32, f32, vp, i32, C.POINTER(i32)]
@@ -146,6 +149,13 @@ def candidate_threshold(min_score: float, min_ratio: float, gated: bool) -> int:
     return t.value
 
 
+def float_threshold(min_score: float, min_ratio: float) -> float:
+    """Float candidate threshold of the BF16 hi/lo path (host computation, no GPU needed)."""
+    t = C.c_float(0)
+    _check(lib().v3dm_float_threshold(min_score, min_ratio, C.byref(t)), "float_threshold")
+    return t.value
+
+
 def _desc(desc: np.ndarray):
     d = np.ascontiguousarray(desc)
     if d.ndim != 2 or d.shape[1] != 128:
@@ -169,6 +179,7 @@ class SIFTMatching:
         h = C.c_void_p()
         _check(lib().v3dm_matcher_create(C.byref(h), device, kernel), "SIFT_Matching()")
         self._h = h
+        self.kernel = kernel
         self.n_left = 0
         self.n_right = 0
 
@@ -209,6 +220,23 @@ class SIFTMatching:
         fn = lib().v3dm_set_right_u8 if kind == "u8" else lib().v3dm_set_right_f32
         _check(fn(self._h, d.shape[0], _ptr(d)), "setRightFeatures")
         self.n_right = d.shape[0]
+
+    def set_left_features_bf16x3(self, desc: np.ndarray):
+        """Float descriptors scored with the BF16 hi/lo split whatever their values."""
+        d = np.ascontiguousarray(desc, dtype=np.float32)
+        _check(lib().v3dm_set_left_f32_bf16x3(self._h, d.shape[0], _ptr(d)), "setLeftFeatures(bf16x3)")
+        self.n_left = d.shape[0]
+
+    def set_right_features_bf16x3(self, desc: np.ndarray):
+        d = np.ascontiguousarray(desc, dtype=np.float32)
+        _check(lib().v3dm_set_right_f32_bf16x3(self._h, d.shape[0], _ptr(d)), "setRightFeatures(bf16x3)")
+        self.n_right = d.shape[0]
+
+    def scores_f32(self) -> np.ndarray:
+        """BF16 hi/lo scores of the current descriptors, (n_left, n_right) float32."""
+        out = np.empty((self.n_left, self.n_right), np.float32)
+        _check(lib().v3dm_scores_f32(self._h, _ptr(out)), "scores_f32")
+        return out
 
     def _result(self, fn, *args) -> np.ndarray:
         cap = max(1, min(self.n_left, self.n_right))

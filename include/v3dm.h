@@ -81,9 +81,24 @@ V3DM_API int v3dm_allocate(v3dm_matcher* h, int nMaxLeft, int nMaxRight, int use
 V3DM_API int v3dm_deallocate(v3dm_matcher* h);
 
 /* SIFT_Matching::setLeftFeatures / setRightFeatures (v3d_cudamatching.h:41-42,
- * .cu:490-520): float descriptors, which must be u/512-valued (else V3DM_ERR_NOT_U8). */
+ * .cu:490-520): float descriptors (see below for values that are not u/512). */
 V3DM_API int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* desc);
 V3DM_API int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* desc);
+/* Float descriptors that are not of the form u/512 are scored, on a tcgen05 handle, with a
+ * BF16 hi/lo split (x = hi + lo, score = hi.hi + lo.hi + hi.lo, FP32 accumulation on the
+ * tensor cores) in place of the reference's FP32 cublasSgemm (.cu:529-530); decisions, ratio
+ * test and mutual filter are the reference's on those scores.  The SIMT handle returns
+ * V3DM_ERR_NOT_U8 for them.  u/512 descriptors use the exact integer path.  The _bf16x3
+ * variants take the BF16 hi/lo path for any float descriptors (u/512 ones included, for which
+ * it is exact).  Non-finite values: V3DM_ERR_ARG. */
+V3DM_API int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* desc);
+V3DM_API int v3dm_set_right_f32_bf16x3(v3dm_matcher* h, int n, const float* desc);
+/* Diagnostic: the BF16 hi/lo scores of the current descriptors, nLeft x nRight floats (row =
+ * left), at most 2^26 of them. */
+V3DM_API int v3dm_scores_f32(v3dm_matcher* h, float* scores);
+/* Float candidate threshold of the BF16 hi/lo path: second values below it never change a
+ * decision of findPutativeMatches(minScore, minRatio). */
+V3DM_API int v3dm_float_threshold(float minScore, float minRatio, float* T);
 /* Native uint8 descriptors (u = 512 * the reference's float value). */
 V3DM_API int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* desc);
 V3DM_API int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* desc);

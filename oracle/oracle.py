@@ -171,12 +171,20 @@ def ref_cuda_match(L_u8: np.ndarray, R_u8: np.ndarray, min_score: float, min_rat
     """The reference's own SIFT_Matching (v3d_cudamatching.cu) on a GPU, fed u/512 floats.
     Runs in a child process because the reference exits on any CUDA error.  Sizes must be
     multiples of 32 (the reference's own requirement)."""
+    return ref_cuda_match_f32(L_u8.astype(np.float32) / 512.0, R_u8.astype(np.float32) / 512.0, min_score,
+                              min_ratio, gates, lpos, rpos, workdir)
+
+
+def ref_cuda_match_f32(L_f32: np.ndarray, R_f32: np.ndarray, min_score: float, min_ratio: float, gates=(),
+                       lpos=None, rpos=None, workdir: str | None = None) -> np.ndarray:
+    """The reference's own SIFT_Matching on arbitrary float descriptors (its FP32 cublasSgemm
+    scores, built with --use_fast_math as the reference builds it)."""
     import tempfile
     wd = Path(workdir or tempfile.mkdtemp(prefix="v3dref_"))
     wd.mkdir(parents=True, exist_ok=True)
     gates = list(gates)
-    nL, nR = L_u8.shape[0], R_u8.shape[0]
-    np.savez(wd / "in.npz", L=L_u8.astype(np.float32) / 512.0, R=R_u8.astype(np.float32) / 512.0,
+    nL, nR = L_f32.shape[0], R_f32.shape[0]
+    np.savez(wd / "in.npz", L=np.asarray(L_f32, np.float32), R=np.asarray(R_f32, np.float32),
              gtypes=np.array([1 if t in ("F", 1) else 2 for t, _, _ in gates], np.int32),
              gmats=np.array([np.asarray(M, np.float64).reshape(9) for _, M, _ in gates], np.float64).reshape(-1),
              gthr=np.array([thr for _, _, thr in gates], np.float32),

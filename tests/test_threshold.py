@@ -67,3 +67,26 @@ def test_threshold_nan_and_unsupported(v3dm_mod):
     with pytest.raises(v3dm_mod.V3DMError) as e:
         v3dm_mod.candidate_threshold(-1.0, 1e-35, True)
     assert e.value.status == v3dm_mod.ERR_UNSUPPORTED
+
+
+# ---- float candidate threshold of the BF16 hi/lo path ------------------------------------
+@pytest.mark.parametrize("ms,mr", [(0.7, 0.8), (0.9, 0.8), (0.8, 0.6), (0.5, 0.95), (0.99, 0.99), (0.7, -1.0),
+                                   (-0.3, 0.8), (0.0, 0.5), (0.7, 0.0), (0.7, 1.5)])
+def test_float_threshold_is_valid_and_tight(v3dm_mod, ms, mr):
+    Tf = f32(v3dm_mod.float_threshold(ms, mr))
+    s1min = np.nextafter(f32(ms), f32(np.inf))
+    assert Tf <= s1min
+    rng = np.random.default_rng(0)
+    s1 = np.concatenate([s1min + np.arange(0, 4096, dtype=np.float32) * np.spacing(s1min),
+                         rng.uniform(float(s1min), 2.5, 20000).astype(np.float32)]).astype(np.float32)
+    below = np.nextafter(Tf, f32(-np.inf))
+    for s2 in (below, f32(-1e20), Tf - f32(0.25), rng.uniform(min(-1.0, float(below) - 1.0), float(below), 1).astype(np.float32)[0]):
+        if s2 >= Tf:
+            continue
+        np.testing.assert_array_equal(_accept(s1, s2, ms, mr), _accept(s1, f32(-1e30), ms, mr))
+    if Tf < s1min:  # tight: a second value of Tf changes the decision of the weakest best
+        assert _accept(np.array([s1min]), Tf, ms, mr)[0] != _accept(np.array([s1min]), f32(-1e30), ms, mr)[0]
+
+
+def test_float_threshold_for_the_benchmark_parameters(v3dm_mod):
+    assert abs(v3dm_mod.float_threshold(0.7, 0.8) - 0.625) < 1e-6
