@@ -63,6 +63,9 @@ struct v3dm_matcher {
   int* dFlagA = nullptr;          // lefts to re-score exactly
   int* dFlagB = nullptr;          // rights to re-score exactly
   int* dCounters = nullptr;       // [0] chosen rights, [1] flagged lefts, [2] flagged rights
+                                  // (the 4 words after the info block, cleared with it)
+  int32_t* countOut = nullptr;    // device-only calls: where the pair count also goes
+  bool countWritten = false;      // the last enqueue wrote *countOut itself
   int lastLaunches = 0;
   // Float descriptors that are not u/512 (tcgen05 kernel): BF16 hi/lo operand layouts
   // (v3dm_match_f.cu), 6 planes of cap rows x 128 bytes each.
@@ -136,7 +139,7 @@ void free_buffers(v3dm_matcher* h) {
   dfree(h->dChosenList);
   dfree(h->dFlagA);
   dfree(h->dFlagB);
-  dfree(h->dCounters);
+  h->dCounters = nullptr;  // points into dInfo
   dfree(h->dLfA);
   dfree(h->dLfB);
   dfree(h->dRfA);
@@ -386,7 +389,7 @@ int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
             dalloc(&h->dLBest, (size_t)nMaxL + 1) == cudaSuccess && dalloc(&h->dLSec, (size_t)nMaxL + 1) == cudaSuccess &&
             dalloc(&h->dRBest, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dRSec, (size_t)nMaxR + 1) == cudaSuccess &&
             dalloc(&h->dScratch, (size_t)nMaxL + nMaxR + 1) == cudaSuccess &&
-            dalloc(&h->dPairs, 2 * (size_t)nMin + 2) == cudaSuccess && dalloc(&h->dInfo, kInfoWords) == cudaSuccess &&
+            dalloc(&h->dPairs, 2 * (size_t)nMin + 2) == cudaSuccess && dalloc(&h->dInfo, kInfoWords + 4) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&h->hInfo), kInfoWords * sizeof(int32_t)) == cudaSuccess;
   if (ok && h->guidedAlloc)
     ok = dalloc(&h->dLPos, 2 * (size_t)nMaxL + 2) == cudaSuccess && dalloc(&h->dRPos, 2 * (size_t)nMaxR + 2) == cudaSuccess &&
@@ -406,7 +409,8 @@ int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
          dalloc(&h->dRightDec, (size_t)nMaxR + 1) == cudaSuccess &&
          dalloc(&h->dChosenFlag, (size_t)nMaxR + 1) == cudaSuccess &&
          dalloc(&h->dChosenList, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dFlagA, (size_t)nMaxL + 1) == cudaSuccess &&
-         dalloc(&h->dFlagB, (size_t)nMaxR + 1) == cudaSuccess && dalloc(&h->dCounters, 4) == cudaSuccess;
+         dalloc(&h->dFlagB, (size_t)nMaxR + 1) == cudaSuccess;
+    if (ok) h->dCounters = h->dInfo + kInfoWords;
     if (ok)
       ok = cudaMemsetAsync(h->dChosenFlag, 0, ((size_t)nMaxR + 1) * sizeof(int), h->stream) == cudaSuccess &&
            cudaMemsetAsync(h->dRc, 0, rowsR * kDescBytes, h->stream) == cudaSuccess;
@@ -605,7 +609,6 @@ int enqueue_match_simt(v3dm_matcher* h, float minScore, float minRatio, int32_t*
 int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
   const int32_t Smin = smallest_passing_score(minScore);
   const bool gated = h->nGates > 0;
-  V3DM_CUDA_TRY(cudaMemsetAsync(h->dCounters, 0, 4 * sizeof(int), h->stream));
   const int cfg = tc_get_config(h->tc);
   if (!h->tcBound || h->mapsA.cfg != cfg) {
     V3DM_CUDA_TRY(tc_side_maps(h->tc, &h->mapsA, h->dL, h->nL, h->dR, h->nR));
@@ -625,7 +628,6 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   PostArgs pa;
   std::memset(&pa, 0, sizeof(pa));
   pa.records = h->dRecords;
-  pa.list = h->dCand;
   pa.segCount = h->dSegCount;
   pa.Smin = Smin;
   pa.nGates = h->nGates;
@@ -668,8 +670,16 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   pa.decision = h->dLeftDec;
   pa.flagged = h->dFlagA;
   pa.flaggedCount = h->dCounters + 1;
+  if (!gated) {  // choose the accepted rights while deciding (no re-score can change a decision)
+    pa.chooseFlag = h->dChosenFlag;
+    pa.chooseList = h->dChosenList;
+    pa.chooseCount = h->dCounters;
+    pa.chooseSrc = h->dR;
+    pa.chooseDst = h->dRc;
+  }
   V3DM_CUDA_TRY(launch_post(pa, h->stream));
-  h->lastLaunches += 4;
+  pa.chooseFlag = nullptr;
+  h->lastLaunches += 3;
   if (gated) {
     ra.descA = h->dL;
     ra.descB = h->dR;
@@ -683,9 +693,11 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
     V3DM_CUDA_TRY(launch_rescore(ra, 64, h->stream));
     h->lastLaunches += 2;
   }
-  V3DM_CUDA_TRY(launch_choose(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dR, h->dRc,
-                              h->stream));
-  h->lastLaunches += 1;
+  if (gated) {
+    V3DM_CUDA_TRY(launch_choose(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dR, h->dRc,
+                                h->stream));
+    h->lastLaunches += 1;
+  }
   // pass B: the chosen rights against every left
   sa.nAptr = h->dCounters;
   sa.nA = h->nR;
@@ -712,7 +724,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   pa.flagged = h->dFlagB;
   pa.flaggedCount = h->dCounters + 2;
   V3DM_CUDA_TRY(launch_post(pa, h->stream));
-  h->lastLaunches += 4;
+  h->lastLaunches += 3;
   if (gated) {
     ra.descA = h->dR;
     ra.descB = h->dL;
@@ -727,7 +739,8 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
     h->lastLaunches += 2;
   }
   V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
-                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->stream));
+                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->countOut, h->stream));
+  h->countWritten = h->countOut != nullptr;
   h->lastLaunches += 2;
   return V3DM_OK;
 }
@@ -747,7 +760,6 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
     V3DM_CUDA_TRY(f_maps(&h->fmB_A, h->dRcf, h->capFR, &h->fmB_B, h->dLfB, h->capFL));
     h->fBound = true;
   }
-  V3DM_CUDA_TRY(cudaMemsetAsync(h->dCounters, 0, 4 * sizeof(int), h->stream));
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.records = h->dRecords;
@@ -758,7 +770,6 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
   PostArgs pa;
   std::memset(&pa, 0, sizeof(pa));
   pa.records = h->dRecords;
-  pa.list = h->dCand;
   pa.segCount = h->dSegCount;
   pa.segCap = h->segCap;
   pa.nSeg = f_segments(h->numSMs);
@@ -786,9 +797,16 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
   pa.best = h->dLBest;
   pa.sec = h->dLSec;
   pa.decision = h->dLeftDec;
+  pa.chooseFlag = h->dChosenFlag;  // accepted rights chosen while deciding
+  pa.chooseList = h->dChosenList;
+  pa.chooseCount = h->dCounters;
+  pa.chooseSrc = h->dRfA;
+  pa.chooseDst = h->dRcf;
+  pa.chooseCapSrc = h->capFR;
+  pa.chooseCapDst = h->capFR;
+  pa.choosePlanes = 6;
   V3DM_CUDA_TRY(launch_post_f(pa, Tf, h->stream));
-  V3DM_CUDA_TRY(launch_choose_f(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dRfA, h->capFR,
-                                h->dRcf, h->capFR, h->stream));
+  pa.chooseFlag = nullptr;
   // pass B: the chosen rights against every left
   sa.nAptr = h->dCounters;
   sa.nA = h->nR;
@@ -813,8 +831,9 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
   pa.decision = h->dRightDec;
   V3DM_CUDA_TRY(launch_post_f(pa, Tf, h->stream));
   V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
-                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->stream));
-  h->lastLaunches = (h->floatL ? 0 : 1) + (h->floatR ? 0 : 1) + 11;
+                              reinterpret_cast<int2*>(dPairs), h->dInfo, h->countOut, h->stream));
+  h->countWritten = h->countOut != nullptr;
+  h->lastLaunches = (h->floatL ? 0 : 1) + (h->floatR ? 0 : 1) + 8;
   return V3DM_OK;
 }
 
@@ -822,7 +841,10 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
 // the handle's stream.
 int enqueue_match(v3dm_matcher* h, float minScore, float minRatio, int32_t* dPairs) {
   h->lastLaunches = 0;
-  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, kInfoWords * sizeof(int32_t), h->stream));
+  h->countWritten = false;
+  // the info block and, right after it on the tcgen05 path, the call's counters
+  V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo, 0, (h->dCounters ? kInfoWords + 4 : kInfoWords) * sizeof(int32_t),
+                                h->stream));
   if (h->nGates > 0)
     V3DM_CUDA_TRY(cudaMemcpyAsync(h->dGates, h->gates, sizeof(GateParams) * h->nGates, cudaMemcpyHostToDevice,
                                   h->stream));
@@ -999,9 +1021,12 @@ int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_
   if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
   DeviceGuard g(h->device);
   h->nGates = 0;
+  h->countOut = d_count;
   int st = enqueue_match(h, minScore, minRatio, d_pairs);
+  h->countOut = nullptr;
   if (st != V3DM_OK) return st;
-  V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+  if (!h->countWritten)
+    V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
   return V3DM_OK;
 }
 
@@ -1012,9 +1037,12 @@ int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, const floa
   DeviceGuard g(h->device);
   int st = add_gate(h, 1, F, thr, d_lpos, d_rpos, true);
   if (st != V3DM_OK) return st;
+  h->countOut = d_count;
   st = enqueue_match(h, minScore, minRatio, d_pairs);
+  h->countOut = nullptr;
   if (st != V3DM_OK) return st;
-  V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
+  if (!h->countWritten)
+    V3DM_CUDA_TRY(cudaMemcpyAsync(d_count, h->dInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, h->stream));
   return V3DM_OK;
 }
 

@@ -842,7 +842,6 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   PostArgs pa;
   std::memset(&pa, 0, sizeof(pa));
   pa.records = b->dRecords;
-  pa.list = b->dList;
   pa.segCount = b->dSegCount;
   pa.segCap = b->segCap;
   pa.nSeg = b->nSeg;
@@ -1140,7 +1139,6 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, flo
   std::memset(&pa, 0, sizeof(pa));
   pa.records = b->dRecords;
   pa.bmap = b->dMapB;
-  pa.list = b->dList;
   pa.segCount = b->dSegCount;
   pa.segCap = b->segCap;
   pa.nSeg = b->nSeg;

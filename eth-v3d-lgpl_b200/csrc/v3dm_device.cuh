@@ -4,6 +4,13 @@
 
 namespace v3dm {
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may start while the kernel
+// before it in the stream is finishing.  pdl_wait() blocks until that kernel has completed and
+// its writes are visible (it returns at once for a normal launch); pdl_launch_dependents()
+// lets the next kernel's blocks be scheduled.  Every kernel here calls both first thing.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // A candidate (l, r, S): both best keys take it with an atomicMax whose result is unused
 // (a fire-and-forget reduction, so the issuing warp does not wait for L2).
 __device__ __forceinline__ void record_best(const MatchArgs& a, int l, int r, int32_t S) {

@@ -9,6 +9,22 @@
 
 namespace v3dm {
 
+// Launches kernel k with programmatic stream serialization (see pdl_wait in v3dm_device.cuh).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 // Device error flags (bitwise OR into MatchArgs::err).
 constexpr int kErrWaitTimeout = 1;  // a bounded mbarrier wait in the tcgen05 kernel gave up
 constexpr int kErrNotU8 = 2;        // a float descriptor was not u/512-valued
@@ -119,7 +135,6 @@ struct PostArgs {
   unsigned int* sec;
   const uint4* records;          // chunk records of the side pass
   const int* bmap;               // absolute B row -> index within its image (null: the column)
-  unsigned long long* list;      // one entry per record: the chunk best key (0: none)
   int* segCount;                 // read, then cleared
   long long segCap;
   int nSeg;
@@ -134,10 +149,18 @@ struct PostArgs {
   int* flagged;                  // indices whose decision needs an exact re-score
   int* flaggedCount;
   int* err;
+  // Optional (pass A of one pair): every accepted partner is also 'chosen' right here -- flagged,
+  // listed once, and its descriptor row gathered for pass B (planar BF16 rows when choosePlanes
+  // is 6, else 128-byte rows).
+  int* chooseFlag;
+  int* chooseList;
+  int* chooseCount;
+  const uint8_t* chooseSrc;
+  uint8_t* chooseDst;
+  int chooseCapSrc, chooseCapDst;
+  int choosePlanes;
 };
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s);
-// The list pass alone (k_list).
-cudaError_t launch_list(const PostArgs& a, int32_t* info, cudaStream_t s);
 
 // ---- float descriptors: BF16 hi/lo scores (v3dm_match_f.cu) ------------------------------
 // Operand layouts: 6 planes of rowsCap x 128 bytes (64 BF16 values of a K slice per row).
@@ -149,8 +172,6 @@ cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const Si
 cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s);
 cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, void* la, void* lb, int* err,
                         cudaStream_t s);
-cudaError_t launch_choose_f(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
-                            const void* rA, int capA, void* rc, int capC, cudaStream_t s);
 float host_float_threshold(float minScore, float minRatio);
 // Exact re-score of the flagged descriptors of side A against side B.
 struct RescoreArgs {
@@ -173,8 +194,9 @@ cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
                           const uint8_t* dR, uint8_t* dRc, cudaStream_t s);
 // Mutual filter and ordered compaction (blockCount: nL/2048 + 1 ints of scratch); clears chosenFlag.
+// The pair count goes to info[kInfoPairs] and, when countOut is set, to *countOut.
 cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,
-                          int2* pairs, int32_t* info, cudaStream_t s);
+                          int2* pairs, int32_t* info, int32_t* countOut, cudaStream_t s);
 
 // Candidate threshold (v3dm_api.cu).
 int host_candidate_threshold(float minScore, float minRatio, bool gated, int32_t* T);

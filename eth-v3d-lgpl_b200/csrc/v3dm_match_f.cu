@@ -80,6 +80,8 @@ __device__ __forceinline__ float fmax32(const float* v) {
 __global__ void __launch_bounds__(kFThreads, 1)
 k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, SideArgs a, float Tf,
          float* dump) {
+  pdl_wait();
+  pdl_launch_dependents();
   extern __shared__ uint8_t smemRaw[];
   SmemF& s = *reinterpret_cast<SmemF*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -268,16 +270,20 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
 // Exact float selection on the chunk records: every unmasked score >= Tf is a candidate; the
 // chunk best is the largest candidate (first column on ties), the other candidates bound the
 // second value.  Scores below Tf (and masked ones, which the reference sets to -1e20) cannot
-// change a decision and are left out.
+// change a decision and are left out.  Chunk bests merge as in k_records (the key that loses
+// the atomic comparison is a second candidate).
 __global__ void k_records_f(PostArgs a, float Tf) {
+  pdl_wait();
+  pdl_launch_dependents();
+  int32_t* info = a.err - kInfoErr;
   const int lane = threadIdx.x & 31;
   const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
     const int cnt = a.segCount[seg];
     const long long n = cnt < a.segCap ? cnt : a.segCap;
+    if (cnt == 0) continue;
     const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
-    unsigned long long* entries = a.list + (long long)seg * a.segCap;
     for (long long i = lane; i < n; i += 32) {
       const uint4* rec = recs + i * kRecordQuads;
       const uint4 head = rec[0];
@@ -305,20 +311,40 @@ __global__ void k_records_f(PostArgs a, float Tf) {
           }
         }
       }
-      if (cb) atomicMax(&a.best[orig], cb);
+      if (cb) {
+        const unsigned long long old = atomicMax(&a.best[orig], cb);
+        if (old) atomicMax(&a.sec[orig], (unsigned)((old < cb ? old : cb) >> kIndexBits));
+      }
       if (cw) atomicMax(&a.sec[orig], cw);
-      entries[i] = cb;
+    }
+    if (lane == 0) {
+      atomicMax(&info[kInfoMaxSeg], cnt);
+      a.segCount[seg] = 0;
     }
   }
 }
 
 __global__ void k_decide_f(PostArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
   const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
     const int idx = a.amap ? a.amap[r] : r;
     const unsigned long long b = a.best[idx];
     const unsigned s = a.sec[idx];
-    a.decision[idx] = decide_f(b, s, a.minScore, a.minRatio);
+    const int32_t d = decide_f(b, s, a.minScore, a.minRatio);
+    a.decision[idx] = d;
+    if (a.chooseFlag && d >= 0 && atomicExch(&a.chooseFlag[d], 1) == 0) {
+      // chosen for pass B: listed once, planar row gathered
+      const int k = atomicAdd(a.chooseCount, 1);
+      a.chooseList[k] = d;
+      for (int p = 0; p < kFPlanes; ++p) {
+        const uint4* src = reinterpret_cast<const uint4*>(a.chooseSrc + ((size_t)p * a.chooseCapSrc + d) * 128);
+        uint4* dst = reinterpret_cast<uint4*>(a.chooseDst + ((size_t)p * a.chooseCapDst + k) * 128);
+#pragma unroll
+        for (int w = 0; w < 8; ++w) dst[w] = src[w];
+      }
+    }
     if (b) a.best[idx] = 0;
     if (s) a.sec[idx] = 0;
   }
@@ -348,25 +374,6 @@ __global__ void k_hilo(const float* __restrict__ f, const uint8_t* __restrict__ 
   at(lb, 0) = hi;
   at(lb, 1) = hi;
   at(lb, 2) = lo;
-}
-
-// Rights accepted by some left: de-duplicated, their A-layout rows gathered for pass B.
-__global__ void k_choose_f(const int32_t* __restrict__ leftDec, int nL, int* chosenFlag, int* chosenList,
-                           int* chosenCount, const uint8_t* __restrict__ rA, int capA, uint8_t* __restrict__ rc,
-                           int capC) {
-  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nL; l += gridDim.x * blockDim.x) {
-    const int r = leftDec[l];
-    if (r < 0) continue;
-    if (atomicExch(&chosenFlag[r], 1) != 0) continue;
-    const int k = atomicAdd(chosenCount, 1);
-    chosenList[k] = r;
-    for (int p = 0; p < kFPlanes; ++p) {
-      const uint4* src = reinterpret_cast<const uint4*>(rA + ((size_t)p * capA + r) * 128);
-      uint4* dst = reinterpret_cast<uint4*>(rc + ((size_t)p * capC + k) * 128);
-#pragma unroll
-      for (int w = 0; w < 8; ++w) dst[w] = src[w];
-    }
-  }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_f() {
@@ -424,22 +431,16 @@ cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const Si
   const long long maxWork = (long long)((a.nA + kFM - 1) / kFM) * nTiles;
   const int grid = (int)std::min<long long>(numSMs, std::max<long long>(1, maxWork));
   if (grid * kFEpiWarps > a.nSeg) return cudaErrorInvalidValue;
-  k_side_f<<<grid, kFThreads, smem, st>>>(mA, mB, a, Tf, dump);
-  return cudaGetLastError();
+  return launch_pdl(k_side_f, dim3(grid), dim3(kFThreads), smem, st, mA, mB, a, Tf, dump);
 }
 
 cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s) {
-  int32_t* info = a.err - kInfoErr;
   const int listBlocks = (a.nSeg * 32 + 255) / 256;
-  k_records_f<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, Tf);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  e = launch_list(a, info, s);
+  cudaError_t e = launch_pdl(k_records_f, dim3(listBlocks < 512 ? listBlocks : 512), dim3(256), 0, s, a, Tf);
   if (e != cudaSuccess) return e;
   const int rows = a.nRows > 0 ? a.nRows : 1;
   const int blocks = (rows + 255) / 256;
-  k_decide_f<<<blocks < 1024 ? blocks : 1024, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_decide_f, dim3(blocks < 1024 ? blocks : 1024), dim3(256), 0, s, a);
 }
 
 cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, void* la, void* lb, int* err,
@@ -449,16 +450,6 @@ cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, vo
   const long long total = (long long)n * kDescBytes;
   k_hilo<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(f, u, n, rowsCap, static_cast<__nv_bfloat16*>(la),
                                                          static_cast<__nv_bfloat16*>(lb), err);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_choose_f(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
-                            const void* rA, int capA, void* rc, int capC, cudaStream_t s) {
-  if (nL == 0) return cudaSuccess;
-  int blocks = (nL + 255) / 256;
-  if (blocks > 148) blocks = 148;
-  k_choose_f<<<blocks, 256, 0, s>>>(leftDec, nL, chosenFlag, chosenList, chosenCount,
-                                    static_cast<const uint8_t*>(rA), capA, static_cast<uint8_t*>(rc), capC);
   return cudaGetLastError();
 }
 

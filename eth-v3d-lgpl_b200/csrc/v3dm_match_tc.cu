@@ -201,6 +201,8 @@ struct BatchCursor {
 template <class C, bool kBatch>
 __global__ void __launch_bounds__(kThreads, 1)
 k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
   extern __shared__ uint8_t smemRaw[];
   Smem<C>& s = *reinterpret_cast<Smem<C>*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -507,8 +509,7 @@ cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles,
     if (e != cudaSuccess) return e;
     attrSet = true;
   }
-  k_side<C, kBatch><<<grid, kThreads, smem, st>>>(mA, mB, nTiles, a);
-  return cudaGetLastError();
+  return launch_pdl(k_side<C, kBatch>, dim3(grid), dim3(kThreads), smem, st, mA, mB, nTiles, a);
 }
 
 constexpr int kNumCfg = 5;

@@ -20,20 +20,32 @@ namespace v3dm {
 
 namespace {
 
+// Merges a chunk best into a descriptor's state: best[] keeps the largest key, and whichever
+// key loses the atomic comparison -- the new one, or the best it displaces -- is a second
+// candidate.  Every key but the final best loses exactly one comparison, so sec[] ends as
+// the exact largest of the other chunk bests (ties are impossible: keys carry the index).
+__device__ __forceinline__ void merge_chunk_best(unsigned long long* best, unsigned int* sec, unsigned long long cb) {
+  const unsigned long long old = atomicMax(best, cb);
+  if (old) atomicMax(sec, (unsigned)((old < cb ? old : cb) >> kIndexBits));
+}
+
 // Chunk records of a side pass: the exact lane-local work the side kernel leaves out.  For
 // every score >= Smin the gates decide whether it is a candidate; the chunk best is the
 // largest candidate (first column on ties), every other score of the chunk (candidates,
-// masked scores and scores below Smin alike) bounds the second value.  The best goes to
-// best[] and, as one entry per record, to the list the next pass reads.
+// masked scores and scores below Smin alike) bounds the second value.  One warp per record
+// segment; the segment's count is recorded (overflow check) and cleared for the next pass.
 __global__ void k_records(PostArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
+  int32_t* info = a.err - kInfoErr;
   const int lane = threadIdx.x & 31;
   const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
     const int cnt = a.segCount[seg];
     const long long n = cnt < a.segCap ? cnt : a.segCap;
+    if (cnt == 0) continue;
     const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
-    unsigned long long* entries = a.list + (long long)seg * a.segCap;
     for (long long i = lane; i < n; i += 32) {
       const uint4* rec = recs + i * kRecordQuads;
       const uint4 head = rec[0];
@@ -63,42 +75,42 @@ __global__ void k_records(PostArgs a) {
           }
         }
       }
-      if (cb) atomicMax(&a.best[orig], cb);
+      if (cb) merge_chunk_best(&a.best[orig], &a.sec[orig], cb);
       if (cw) atomicMax(&a.sec[orig], cw);
-      entries[i] = cb;  // 0: no candidate in the chunk
     }
-  }
-}
-
-// List pass: one warp per segment; every chunk best that is not the descriptor's overall
-// best raises its second value (the descriptor is read from the chunk's record).  Segment
-// counts are cleared for the next pass.
-__global__ void k_list(PostArgs a, int32_t* info) {
-  const int lane = threadIdx.x & 31;
-  const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
-    const int cnt = a.segCount[seg];
-    if (cnt == 0) continue;
     if (lane == 0) {
       atomicMax(&info[kInfoMaxSeg], cnt);
       a.segCount[seg] = 0;
     }
-    const long long n = cnt < a.segCap ? cnt : a.segCap;
-    const unsigned long long* e = a.list + (long long)seg * a.segCap;
-    const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
-    for (long long i = lane; i < n; i += 32) {
-      const unsigned long long key = e[i];
-      if (key == 0) continue;  // record without a candidate
-      const int idx = (int)recs[i * kRecordQuads].x;
-      if (key != a.best[idx]) atomicMax(&a.sec[idx], (unsigned)(key >> kIndexBits));
+  }
+}
+
+// Chooses right r for pass B (once): flag, list entry, descriptor row gathered.
+__device__ __forceinline__ void choose_one(const PostArgs& a, int r) {
+  if (atomicExch(&a.chooseFlag[r], 1) != 0) return;
+  const int k = atomicAdd(a.chooseCount, 1);
+  a.chooseList[k] = r;
+  if (a.choosePlanes) {
+    for (int p = 0; p < a.choosePlanes; ++p) {
+      const uint4* src = reinterpret_cast<const uint4*>(a.chooseSrc + ((size_t)p * a.chooseCapSrc + r) * 128);
+      uint4* dst = reinterpret_cast<uint4*>(a.chooseDst + ((size_t)p * a.chooseCapDst + k) * 128);
+#pragma unroll
+      for (int w = 0; w < 8; ++w) dst[w] = src[w];
     }
+  } else {
+    const uint4* src = reinterpret_cast<const uint4*>(a.chooseSrc + (size_t)r * kDescBytes);
+    uint4* dst = reinterpret_cast<uint4*>(a.chooseDst + (size_t)k * kDescBytes);
+#pragma unroll
+    for (int w = 0; w < kDescBytes / 16; ++w) dst[w] = src[w];
   }
 }
 
 // Decisions of the pass's descriptors; flags the ones whose gated bound straddles the
-// decision, clears the state of the others.
+// decision, clears the state of the others.  With a.chooseFlag set, accepted partners are
+// chosen for pass B right away.
 __global__ void k_decide(PostArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
   const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
     const int idx = a.amap ? a.amap[r] : r;
@@ -114,6 +126,7 @@ __global__ void k_decide(PostArgs a) {
       continue;
     }
     a.decision[idx] = d;
+    if (a.chooseFlag && d >= 0) choose_one(a, d);
     if (b) a.best[idx] = 0;
     if (s) a.sec[idx] = 0;
   }
@@ -129,6 +142,8 @@ constexpr int kRescoreThreads = 256;
 constexpr int kRescoreStage = 64;
 
 __global__ void __launch_bounds__(kRescoreThreads) k_rescore(RescoreArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
   __shared__ uint32_t sA[kRescoreStage][33];
   __shared__ int sIdx[kRescoreStage];
   __shared__ unsigned long long sBest[kRescoreStage];
@@ -179,6 +194,8 @@ __global__ void __launch_bounds__(kRescoreThreads) k_rescore(RescoreArgs a) {
 
 // Decisions of the flagged descriptors from their exact second values; clears their state.
 __global__ void k_rescore_decide(RescoreArgs a) {
+  pdl_wait();
+  pdl_launch_dependents();
   const int n = *a.flaggedCount;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
     const int idx = a.flagged[f];
@@ -190,6 +207,8 @@ __global__ void k_rescore_decide(RescoreArgs a) {
 
 __global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chosenFlag, int* chosenList,
                          int* chosenCount, const uint8_t* __restrict__ dR, uint8_t* __restrict__ dRc) {
+  pdl_wait();
+  pdl_launch_dependents();
   for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nL; l += gridDim.x * blockDim.x) {
     const int r = leftDec[l];
     if (r < 0) continue;
@@ -210,6 +229,8 @@ constexpr int kMutPerBlock = 2048;  // lefts per block (8 per thread, contiguous
 __global__ void __launch_bounds__(kMutThreads)
 k_mutual_count(const int32_t* __restrict__ leftDec, int nL, const int32_t* __restrict__ rightDec,
                int* __restrict__ blockCount) {
+  pdl_wait();
+  pdl_launch_dependents();
   __shared__ int wsum[kMutThreads / 32];
   const int base = blockIdx.x * kMutPerBlock;
   int cnt = 0;
@@ -232,7 +253,10 @@ k_mutual_count(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
 // in ascending left order; clears the chosen-right flags.
 __global__ void __launch_bounds__(kMutThreads)
 k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __restrict__ rightDec, int* chosenFlag,
-               const int* __restrict__ blockCount, int nBlocks, int2* __restrict__ pairs, int32_t* info) {
+               const int* __restrict__ blockCount, int nBlocks, int2* __restrict__ pairs, int32_t* info,
+               int32_t* countOut) {
+  pdl_wait();
+  pdl_launch_dependents();
   __shared__ int blockOff;
   __shared__ int wsum[kMutThreads / 32];
   if (threadIdx.x < 32) {
@@ -242,7 +266,10 @@ k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (threadIdx.x == 0) {
       blockOff = t;
-      if (blockIdx.x == nBlocks - 1) info[kInfoPairs] = t + blockCount[blockIdx.x];
+      if (blockIdx.x == nBlocks - 1) {
+        info[kInfoPairs] = t + blockCount[blockIdx.x];
+        if (countOut) *countOut = t + blockCount[blockIdx.x];
+      }
     }
   }
   // each thread owns kMutPerBlock / kMutThreads consecutive lefts
@@ -279,36 +306,22 @@ k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
 }  // namespace
 
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
-  int32_t* info = a.err - kInfoErr;
   const int listBlocks = (a.nSeg * 32 + 255) / 256;
-  k_records<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a);
-  cudaError_t e0 = cudaGetLastError();
-  if (e0 != cudaSuccess) return e0;
-  k_list<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, info);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k_records, dim3(listBlocks < 512 ? listBlocks : 512), dim3(256), 0, s, a);
   if (e != cudaSuccess) return e;
   int rows = a.nRows > 0 ? a.nRows : 1;
   int blocks = (rows + 255) / 256;
-  k_decide<<<blocks < 1024 ? blocks : 1024, 256, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_list(const PostArgs& a, int32_t* info, cudaStream_t s) {
-  const int listBlocks = (a.nSeg * 32 + 255) / 256;
-  k_list<<<listBlocks < 512 ? listBlocks : 512, 256, 0, s>>>(a, info);
-  return cudaGetLastError();
+  return launch_pdl(k_decide, dim3(blocks < 1024 ? blocks : 1024), dim3(256), 0, s, a);
 }
 
 cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s) {
   (void)grid;
   const int blocks = (a.nB + kRescoreThreads - 1) / kRescoreThreads;
   if (blocks > 0) {
-    k_rescore<<<blocks, kRescoreThreads, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_pdl(k_rescore, dim3(blocks), dim3(kRescoreThreads), 0, s, a);
     if (e != cudaSuccess) return e;
   }
-  k_rescore_decide<<<16, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_rescore_decide, dim3(16), dim3(256), 0, s, a);
 }
 
 cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
@@ -316,19 +329,17 @@ cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* 
   if (nL == 0) return cudaSuccess;
   int blocks = (nL + 255) / 256;
   if (blocks > 148) blocks = 148;
-  k_choose<<<blocks, 256, 0, s>>>(leftDec, nL, chosenFlag, chosenList, chosenCount, dR, dRc);
-  return cudaGetLastError();
+  return launch_pdl(k_choose, dim3(blocks), dim3(256), 0, s, leftDec, nL, chosenFlag, chosenList, chosenCount, dR, dRc);
 }
 
 cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,
-                          int2* pairs, int32_t* info, cudaStream_t s) {
+                          int2* pairs, int32_t* info, int32_t* countOut, cudaStream_t s) {
   const int nBlocks = (nL + kMutPerBlock - 1) / kMutPerBlock;
   if (nBlocks == 0) return cudaSuccess;
-  k_mutual_count<<<nBlocks, kMutThreads, 0, s>>>(leftDec, nL, rightDec, blockCount);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k_mutual_count, dim3(nBlocks), dim3(kMutThreads), 0, s, leftDec, nL, rightDec, blockCount);
   if (e != cudaSuccess) return e;
-  k_mutual_write<<<nBlocks, kMutThreads, 0, s>>>(leftDec, nL, rightDec, chosenFlag, blockCount, nBlocks, pairs, info);
-  return cudaGetLastError();
+  return launch_pdl(k_mutual_write, dim3(nBlocks), dim3(kMutThreads), 0, s, leftDec, nL, rightDec, chosenFlag,
+                    blockCount, nBlocks, pairs, info, countOut);
 }
 
 }  // namespace v3dm
