@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--cache-dir", default="", help="voctree workload: keep the generated tree and queries here")
     ap.add_argument("--cells", type=int, default=16, help="proposal workload: cells of the projection")
     ap.add_argument("--probes", type=int, default=4, help="proposal workload: probed cells per left")
+    ap.add_argument("--probes-right", type=int, default=1, help="proposal workload: cells each right is listed under")
+    ap.add_argument("--proposal-config", type=int, default=5, help="proposal workload: tile configuration")
     ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     return ap.parse_args()
@@ -621,39 +623,42 @@ def run_proposal(args, ws, rank, local):
         assert b.wait() == v3dm.OK
         return max_over_ranks(ws, statistics.mean(x.elapsed_time(y) for x, y in ev), dev), n
 
+    b.autotune(MIN_SCORE, MIN_RATIO, 1)  # exhaustive at its fastest configuration
+    exh_cfg = b.config()
     ms_exh, _ = timed(lambda: b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
     exh = b.match(MIN_SCORE, MIN_RATIO)
+    b.set_config(args.proposal_config, 0)
     clocks = Clocks(local)
-    ms_prop, launches = timed(lambda: b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
+    ms_prop, launches = timed(lambda: b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right))
     clk = clocks.stop()
-    got = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO)
+    got = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right)
     rec, prec = proposal.recall(exh, got)
     scored, exhaustive = b.proposal_scored()
     b.profile(True)
     for _ in range(3):
-        b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr())
+        b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right)
         assert b.wait() == v3dm.OK
     ka, na = b.profile_read(0)
     b.profile(False)
     # ablation: the same cells fitted to the untrained network
     net0 = v3dm.Projection(local, seed=args.seed)
     net0.set_cells(proposal.fit_cells(net0.embed(tr_desc), args.cells, seed=args.seed))
-    ms0, _ = timed(lambda: b.match_proposal_device(net0, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
-    rec0, prec0 = proposal.recall(exh, b.match_proposal(net0, args.probes, MIN_SCORE, MIN_RATIO))
+    ms0, _ = timed(lambda: b.match_proposal_device(net0, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right))
+    rec0, prec0 = proposal.recall(exh, b.match_proposal(net0, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right))
     scored0, _ = b.proposal_scored()
     net0.close()
     # e2e: descriptors from pinned host memory, triples back
     desc_p = torch.from_numpy(te_desc).pin_memory().numpy()
     for _ in range(2):
         b.set_images(desc_p, te_counts)
-        b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO)
+        b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right)
     ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
     n_host = 0
     for a0, a1 in ev2:
         a0.record(stream)
         b.set_images(desc_p, te_counts)
-        n_host = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO).shape[0]
+        n_host = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right).shape[0]
         a1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(ws, statistics.mean(x.elapsed_time(y) for x, y in ev2), dev)
@@ -673,7 +678,9 @@ def run_proposal(args, ws, rank, local):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
         "config": {"workload": "200 test images x 8000 uint8 SIFT-like features, 15% shared tracks, all 19,900 pairs, "
                                "minScore 0.7, ratio 0.8; projection 128-64-32 trained on 100 held-out images",
-                   "cells": args.cells, "probes": args.probes, "train_steps": args.train_steps,
+                   "cells": args.cells, "probes": args.probes, "probes_right": args.probes_right,
+                   "tile_config": args.proposal_config, "exhaustive_tile_config": list(exh_cfg),
+                   "train_steps": args.train_steps,
                    "temperature": args.temperature, "train_pairs": int(anchors.shape[0]),
                    "l2": "inputs larger than L2 (205 MB of descriptors)"},
         "exhaustive": {"value": ws * n_pairs * 1000.0 / ms_exh, "unit": "pairs/s", "ms_per_step": ms_exh},

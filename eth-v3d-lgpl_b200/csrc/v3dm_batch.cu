@@ -303,9 +303,11 @@ k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, co
 
 // ---- proposal matching (learned cells) --------------------------------------------------
 // Layout of the proposal: every image's descriptors are copied into an A layout, once per
-// probed cell and grouped by (image, cell), and into a B layout grouped by (image, best cell).
-// A pair (i, j) is scored block by block: the lefts of i that probe cell c against the rights of
-// j whose best cell is c.  mapA / mapB give each layout row's index within its image.
+// left-probed cell (its first probesL cells), and into a B layout, once per right-probed cell
+// (its first probesR cells), both grouped by (image, cell).  A pair (i, j) is scored block by
+// block: the lefts of i probing cell c against the rights of j probing c.  A (left, right) that
+// shares several probed cells is scored in each of them with the same key; the merges treat
+// equal keys as one candidate.  mapA / mapB give each layout row's index within its image.
 
 constexpr int kCntRowsP = 8;      // counter words of the proposal (after the batch ones)
 constexpr int kCntOverP = 9;      // 1: the proposal row table was too small
@@ -314,7 +316,7 @@ constexpr int kCntScored = 10;    // two words: scored (left, right) pairs, 64-b
 // Per image and cell: rows whose probed cells include the cell (A) and rows whose best cell
 // it is (B).
 __global__ void k_pcount(const BImage* __restrict__ im, int nImages, const uint8_t* __restrict__ cell, int probes,
-                         int C, int* __restrict__ cntA, int* __restrict__ cntB) {
+                         int probesL, int probesR, int C, int* __restrict__ cntA, int* __restrict__ cntB) {
   extern __shared__ int pcSh[];
   for (int i = blockIdx.x; i < nImages; i += gridDim.x) {
     for (int t = threadIdx.x; t < 2 * C; t += blockDim.x) pcSh[t] = 0;
@@ -322,8 +324,8 @@ __global__ void k_pcount(const BImage* __restrict__ im, int nImages, const uint8
     const BImage m = im[i];
     for (int r = threadIdx.x; r < m.n; r += blockDim.x) {
       const uint8_t* cr = cell + (size_t)(m.rowOff + r) * probes;
-      for (int q = 0; q < probes; ++q) atomicAdd(&pcSh[cr[q]], 1);
-      atomicAdd(&pcSh[C + cr[0]], 1);
+      for (int q = 0; q < probesL; ++q) atomicAdd(&pcSh[cr[q]], 1);
+      for (int q = 0; q < probesR; ++q) atomicAdd(&pcSh[C + cr[q]], 1);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < C; t += blockDim.x) {
@@ -346,7 +348,7 @@ k_pscan_cells(const int* __restrict__ cntA, const int* __restrict__ cntB, int n,
 // Copies the descriptors into the A and B layouts (order within a block is arbitrary: every
 // result depends on the index maps, not on the order).
 __global__ void k_pscatter(const BImage* __restrict__ im, int nImages, const uint8_t* __restrict__ cell, int probes,
-                           int C, const int* __restrict__ offA, const int* __restrict__ offB,
+                           int probesL, int probesR, int C, const int* __restrict__ offA, const int* __restrict__ offB,
                            const uint8_t* __restrict__ img, uint8_t* __restrict__ la, int* __restrict__ mapA,
                            uint8_t* __restrict__ lb, int* __restrict__ mapB) {
   extern __shared__ int psSh[];
@@ -360,7 +362,7 @@ __global__ void k_pscatter(const BImage* __restrict__ im, int nImages, const uin
       uint4 d[kDescBytes / 16];
 #pragma unroll
       for (int x = 0; x < kDescBytes / 16; ++x) d[x] = src[x];
-      for (int q = 0; q < probes; ++q) {
+      for (int q = 0; q < probesL; ++q) {
         const int c = cr[q];
         const int pos = offA[i * C + c] + atomicAdd(&psSh[c], 1);
         uint4* dst = reinterpret_cast<uint4*>(la + (size_t)pos * kDescBytes);
@@ -368,12 +370,14 @@ __global__ void k_pscatter(const BImage* __restrict__ im, int nImages, const uin
         for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = d[x];
         mapA[pos] = r;
       }
-      const int c0 = cr[0];
-      const int pos = offB[i * C + c0] + atomicAdd(&psSh[C + c0], 1);
-      uint4* dst = reinterpret_cast<uint4*>(lb + (size_t)pos * kDescBytes);
+      for (int q = 0; q < probesR; ++q) {
+        const int c = cr[q];
+        const int pos = offB[i * C + c] + atomicAdd(&psSh[C + c], 1);
+        uint4* dst = reinterpret_cast<uint4*>(lb + (size_t)pos * kDescBytes);
 #pragma unroll
-      for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = d[x];
-      mapB[pos] = r;
+        for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = d[x];
+        mapB[pos] = r;
+      }
     }
     __syncthreads();
   }
@@ -500,7 +504,7 @@ k_pchoose(const BPair* __restrict__ pairs, int nPairs, const long long* __restri
 // descriptor in every lane's registers, lanes striding over the candidates.
 __global__ void __launch_bounds__(256)
 k_ppassb(const BPair* __restrict__ pairs, const BImage* __restrict__ im, const uint8_t* __restrict__ cell, int probes,
-         int C, const int* __restrict__ cntA, const int* __restrict__ offA, const uint8_t* __restrict__ la,
+         int probesR, int C, const int* __restrict__ cntA, const int* __restrict__ offA, const uint8_t* __restrict__ la,
          const int* __restrict__ mapA, const uint8_t* __restrict__ img, const int* __restrict__ chosenRight,
          const int* __restrict__ chosenSorted, const int* __restrict__ counters, float minScore, float minRatio,
          int32_t* __restrict__ decB) {
@@ -512,32 +516,34 @@ k_ppassb(const BPair* __restrict__ pairs, const BImage* __restrict__ im, const u
     const BPair q = pairs[chosenSorted[s]];
     const int r = chosenRight[s];
     const int rRow = im[q.ri].rowOff + r;
-    const int c1 = cell[(size_t)rRow * probes];
-    const int cnt = cntA[q.li * C + c1];
-    const int base = offA[q.li * C + c1];
     uint4 rv[kDescBytes / 16];
     const uint4* rs = reinterpret_cast<const uint4*>(img + (size_t)rRow * kDescBytes);
 #pragma unroll
     for (int x = 0; x < kDescBytes / 16; ++x) rv[x] = __ldg(rs + x);
     unsigned long long best = 0;
     uint32_t sec = 0;
-    for (int j = lane; j < cnt; j += 32) {
-      const uint4* ls = reinterpret_cast<const uint4*>(la + (size_t)(base + j) * kDescBytes);
-      uint32_t S = 0;
+    for (int pr = 0; pr < probesR; ++pr) {  // the lefts probing any cell the right probes
+      const int c1 = cell[(size_t)rRow * probes + pr];
+      const int cnt = cntA[q.li * C + c1];
+      const int base = offA[q.li * C + c1];
+      for (int j = lane; j < cnt; j += 32) {
+        const uint4* ls = reinterpret_cast<const uint4*>(la + (size_t)(base + j) * kDescBytes);
+        uint32_t S = 0;
 #pragma unroll
-      for (int x = 0; x < kDescBytes / 16; ++x) {
-        const uint4 w = __ldg(ls + x);
-        S = __dp4a(rv[x].x, w.x, S);
-        S = __dp4a(rv[x].y, w.y, S);
-        S = __dp4a(rv[x].z, w.z, S);
-        S = __dp4a(rv[x].w, w.w, S);
-      }
-      const unsigned long long key = best_key((int32_t)S, __ldg(mapA + base + j));
-      if (key > best) {
-        sec = max(sec, (uint32_t)(best >> kIndexBits));
-        best = key;
-      } else {
-        sec = max(sec, S + 1u);
+        for (int x = 0; x < kDescBytes / 16; ++x) {
+          const uint4 w = __ldg(ls + x);
+          S = __dp4a(rv[x].x, w.x, S);
+          S = __dp4a(rv[x].y, w.y, S);
+          S = __dp4a(rv[x].z, w.z, S);
+          S = __dp4a(rv[x].w, w.w, S);
+        }
+        const unsigned long long key = best_key((int32_t)S, __ldg(mapA + base + j));
+        if (key > best) {
+          sec = max(sec, (uint32_t)(best >> kIndexBits));
+          best = key;
+        } else if (key != best) {  // an equal key is the same left seen in another cell
+          sec = max(sec, S + 1u);
+        }
       }
     }
     // warp: the largest key; the second is the largest of the other lanes' bests and every
@@ -1029,16 +1035,17 @@ int run_host(v3dm_batch* b, float minScore, float minRatio) {
 // ---- proposal matching ----------------------------------------------------------------
 
 // Buffers and tensor maps of a proposal call with 'probes' probed cells and C cells.
-int prepare_proposal(v3dm_batch* b, int probes, int C) {
+int prepare_proposal(v3dm_batch* b, int probesL, int probesR, int C) {
+  const int probes = std::max(probesL, probesR);
   int st = prepare(b);
   if (st != V3DM_OK) return st;
   int GM = 0, BN = 0;
   tc_config_shape(tc_get_config(b->tc), &GM, &BN);
-  const long long laRows = std::max<long long>(b->totalDesc * probes, 256);
-  const long long lbRows = std::max<long long>(b->totalDesc, 256);
+  const long long laRows = std::max<long long>(b->totalDesc * probesL, 256);
+  const long long lbRows = std::max<long long>(b->totalDesc * probesR, 256);
   long long rowsBound = 0;
   for (const BPair& q : b->bp)
-    if (b->counts[q.ri] > 0 && q.nL > 0) rowsBound += ((long long)q.nL * probes + GM - 1) / GM + C;
+    if (b->counts[q.ri] > 0 && q.nL > 0) rowsBound += ((long long)q.nL * probesL + GM - 1) / GM + C;
   rowsBound = std::max<long long>(std::max(rowsBound, b->rowsPNeed), 1);
   if (rowsBound > 0x7fffffffLL || laRows > 0x7fffffffLL) return V3DM_ERR_SIZE;
   const uint8_t* la0 = b->dLA;
@@ -1085,8 +1092,9 @@ int prepare_proposal(v3dm_batch* b, int probes, int C) {
   return V3DM_OK;
 }
 
-int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, float minScore, float minRatio,
-                     bool withEvents) {
+int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, int probesR, float minScore,
+                     float minRatio, bool withEvents) {
+  const int probes = std::max(probesL, probesR);
   int GM = 0, BN = 0;
   tc_config_shape(tc_get_config(b->tc), &GM, &BN);
   const int C = proj_cells(proj);
@@ -1098,11 +1106,13 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, flo
   V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
   // cells of every descriptor, layouts, row table
   V3DM_BTRY(proj_assign(proj, b->dImg, b->totalRows, probes, b->dCell, b->stream));
-  k_pcount<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, C, b->dCntA, b->dCntB);
+  k_pcount<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, probesL, probesR, C,
+                                                             b->dCntA, b->dCntB);
   V3DM_BTRY(cudaGetLastError());
   k_pscan_cells<<<1, kScanThreads, 0, b->stream>>>(b->dCntA, b->dCntB, nI * C, b->dOffA, b->dOffB);
   V3DM_BTRY(cudaGetLastError());
-  k_pscatter<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, C, b->dOffA,
+  k_pscatter<<<imgGrid, 256, 2 * C * sizeof(int), b->stream>>>(b->dImages, nI, b->dCell, probes, probesL, probesR, C,
+                                                               b->dOffA,
                                                                b->dOffB, b->dImg, b->dLA, b->dMapA, b->dLB, b->dMapB);
   V3DM_BTRY(cudaGetLastError());
   k_prowcount<<<pairGrid, 256, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, C, GM, b->dCntA, b->dCntB,
@@ -1164,7 +1174,8 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, flo
                                                           b->dCounters);
   V3DM_BTRY(cudaGetLastError());
   if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
-  k_ppassb<<<148 * 8, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, C, b->dCntA, b->dOffA, b->dLA,
+  k_ppassb<<<148 * 8, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA, b->dOffA,
+                                           b->dLA,
                                            b->dMapA, b->dImg, b->dChosenRight, b->dChosenSorted, b->dCounters,
                                            minScore, minRatio, b->dDecB);
   V3DM_BTRY(cudaGetLastError());
@@ -1183,11 +1194,14 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, flo
   return V3DM_OK;
 }
 
-int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes, float minScore, float minRatio) {
-  if (!proj || probes < 1 || probes > V3DM_PROJ_MAX_PROBES) return V3DM_ERR_ARG;
+int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, int probesR, float minScore,
+                         float minRatio) {
+  if (!proj || probesL < 1 || probesL > V3DM_PROJ_MAX_PROBES || probesR < 1 || probesR > V3DM_PROJ_MAX_PROBES)
+    return V3DM_ERR_ARG;
   const int C = proj_cells(proj);
   if (C < 1) return V3DM_ERR_NOT_ALLOCATED;
-  if (probes > C) return V3DM_ERR_ARG;
+  if (probesL > C || probesR > C) return V3DM_ERR_ARG;
+  const int probes = probesL * 8 + probesR;  // graph key
   if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
   b->pendingCheck = true;
   if (b->totalRows == 0 || b->nPairs == 0) {
@@ -1197,7 +1211,7 @@ int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes,
     b->lastLaunches = 0;
     return V3DM_OK;
   }
-  int st = prepare_proposal(b, probes, C);
+  int st = prepare_proposal(b, probesL, probesR, C);
   if (st != V3DM_OK) return st;
   // the projection's parameters and cells may have been written on its own stream
   V3DM_BTRY(cudaStreamSynchronize(proj_stream(proj)));
@@ -1207,17 +1221,17 @@ int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probes,
   if (b->profile) {
     for (int i = 0; i < 4; ++i)
       if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
-    st = enqueue_proposal(b, proj, probes, minScore, minRatio, true);
+    st = enqueue_proposal(b, proj, probesL, probesR, minScore, minRatio, true);
     if (st == V3DM_OK) b->profPending = true;
     return st;
   }
-  if (!b->useGraph) return enqueue_proposal(b, proj, probes, minScore, minRatio, false);
+  if (!b->useGraph) return enqueue_proposal(b, proj, probesL, probesR, minScore, minRatio, false);
   if (!b->graphP || b->gpMs != ms || b->gpMr != mr || b->gpProbes != probes || b->gpCells != C || b->gpProj != proj) {
     if (b->graphP) cudaGraphExecDestroy(b->graphP);
     b->graphP = nullptr;
     cudaGraph_t g = nullptr;
     V3DM_BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    st = enqueue_proposal(b, proj, probes, minScore, minRatio, false);
+    st = enqueue_proposal(b, proj, probesL, probesR, minScore, minRatio, false);
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (st != V3DM_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1560,13 +1574,13 @@ int v3dm_batch_wait(v3dm_batch* b) {
   return finish_call(b);
 }
 
-int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore, float minRatio,
-                              int32_t* triples, long long cap, long long* nOut) {
+int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probesLeft, int probesRight, float minScore,
+                              float minRatio, int32_t* triples, long long cap, long long* nOut) {
   if (!b || !nOut || cap < 0 || (cap > 0 && !triples)) return V3DM_ERR_ARG;
   BDeviceGuard g(b->device);
   int st = V3DM_ERR_CANDIDATES;
   for (int attempt = 0; attempt < 6 && st == V3DM_ERR_CANDIDATES; ++attempt) {
-    st = launch_call_proposal(b, proj, probes, minScore, minRatio);
+    st = launch_call_proposal(b, proj, probesLeft, probesRight, minScore, minRatio);
     if (st != V3DM_OK) return st;
     st = finish_call(b);
   }
@@ -1581,11 +1595,11 @@ int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probes, 
   return n > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
 }
 
-int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
-                                     float minRatio, int32_t* d_count) {
+int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probesLeft, int probesRight,
+                                     float minScore, float minRatio, int32_t* d_count) {
   if (!b) return V3DM_ERR_ARG;
   BDeviceGuard g(b->device);
-  int st = launch_call_proposal(b, proj, probes, minScore, minRatio);
+  int st = launch_call_proposal(b, proj, probesLeft, probesRight, minScore, minRatio);
   if (st != V3DM_OK) return st;
   if (d_count)
     V3DM_BTRY(cudaMemcpyAsync(d_count, b->dInfo + kInfoWords + kCntOut, sizeof(int32_t), cudaMemcpyDeviceToDevice,

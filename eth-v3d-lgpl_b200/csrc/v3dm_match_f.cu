@@ -313,7 +313,7 @@ __global__ void k_records_f(PostArgs a, float Tf) {
       }
       if (cb) {
         const unsigned long long old = atomicMax(&a.best[orig], cb);
-        if (old) atomicMax(&a.sec[orig], (unsigned)((old < cb ? old : cb) >> kIndexBits));
+        if (old && old != cb) atomicMax(&a.sec[orig], (unsigned)((old < cb ? old : cb) >> kIndexBits));
       }
       if (cw) atomicMax(&a.sec[orig], cw);
     }

@@ -52,11 +52,12 @@ constexpr int kEpiWarps = 16;    // four per TMEM lane quadrant
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr int kTmemCols = 512;
 
-template <int NB_, int BN_, int STAGES_>
+template <int NB_, int BN_, int STAGES_, int ASLOTS_ = 2>
 struct TcCfg {
   static constexpr int NB = NB_;                 // 128-row MMA blocks per left group
   static constexpr int BN = BN_;                 // rights per tile
   static constexpr int kStages = STAGES_;        // right-tile ring depth
+  static constexpr int kASlots = ASLOTS_;        // left-group buffers (more: short rows prefetch further)
   static constexpr int GM = BM * NB;             // left rows per group
   static constexpr int kABytes = GM * kDescBytes;
   static constexpr int kBBytes = BN * kDescBytes;
@@ -73,10 +74,10 @@ struct TcCfg {
 
 template <class C>
 struct Smem {
-  uint8_t a[2][C::kABytes];
+  uint8_t a[C::kASlots][C::kABytes];
   uint8_t b[C::kStages][C::kBBytes];
   unsigned long long fullB[C::kStages], emptyB[C::kStages];
-  unsigned long long fullA[2], emptyA[2];
+  unsigned long long fullA[C::kASlots], emptyA[C::kASlots];
   unsigned long long accFull[C::kAcc], accEmpty[C::kAcc];
   unsigned long long mmaDone;
   uint32_t tmemBase;
@@ -237,7 +238,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
       mbar_init(&s.fullB[i], 1);
       mbar_init(&s.emptyB[i], 1);
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < C::kASlots; ++i) {
       mbar_init(&s.fullA[i], 1);
       mbar_init(&s.emptyA[i], 1);
     }
@@ -268,15 +269,15 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, aBuf = 1;
-      bool anyA = false;
+      int stage = 0, aBuf = C::kASlots - 1;
       uint32_t phase = 0, aPhase = 1;
-      uint32_t armedPhase[C::kStages];
-      bool armed[C::kStages];
+      uint32_t armedPhase[C::kStages], armedAPhase[C::kASlots];
+      bool armed[C::kStages], armedA[C::kASlots];
       for (int i = 0; i < C::kStages; ++i) armed[i] = false;
+      for (int i = 0; i < C::kASlots; ++i) armedA[i] = false;
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
         if (wc.fresh) {
-          if (++aBuf == 2) {
+          if (++aBuf == C::kASlots) {
             aBuf = 0;
             aPhase ^= 1;
           }
@@ -286,7 +287,8 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           if constexpr (kBatch) aRow = wc.cur.aRow;
           else aRow = wc.g * C::GM;
           tma_load_2d(s.a[aBuf], &tmA, &s.fullA[aBuf], 0, aRow);
-          anyA = true;
+          armedA[aBuf] = true;
+          armedAPhase[aBuf] = aPhase;
         }
         if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
         mbar_expect_tx(&s.fullB[stage], C::kBBytes);
@@ -308,23 +310,24 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
           }
         }
-      if (anyA) {
-        long long t0c = clock64();
-        while (!mbar_try(&s.fullA[aBuf], aPhase) && clock64() - t0c < kWaitCycles) {
+      for (int i = 0; i < C::kASlots; ++i)
+        if (armedA[i]) {
+          long long t0c = clock64();
+          while (!mbar_try(&s.fullA[i], armedAPhase[i]) && clock64() - t0c < kWaitCycles) {
+          }
         }
-      }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, acc = 0, aBuf = 1;
+      int stage = 0, acc = 0, aBuf = C::kASlots - 1;
       bool anyA = false;
       uint32_t phase = 0, accPhase = 0, aPhase = 1;
       uint32_t aAddr = 0;
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
         if (wc.fresh) {
           if (anyA) mma_commit(&s.emptyA[aBuf]);
-          if (++aBuf == 2) {
+          if (++aBuf == C::kASlots) {
             aBuf = 0;
             aPhase ^= 1;
           }
@@ -499,6 +502,8 @@ using Cfg1 = TcCfg<1, 128, 8>;   // 128 x 128 tiles, 4 accumulator stages
 using Cfg2 = TcCfg<2, 128, 8>;   // 256 x 128 tiles, 2 accumulator stages
 using Cfg3 = TcCfg<2, 64, 16>;   // 256 x 64 tiles, 4 accumulator stages
 using Cfg4 = TcCfg<1, 256, 6>;   // 128 x 256 tiles, 2 accumulator stages, 6-deep ring
+using Cfg5 = TcCfg<1, 256, 4, 4>;   // as Cfg0 with 4 left-group buffers (rows of few tiles)
+using Cfg6 = TcCfg<1, 128, 6, 6>;   // 128 x 128 tiles, 6 left-group buffers
 
 template <class C, bool kBatch>
 cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles, const SideArgs& a, int grid,
@@ -512,9 +517,9 @@ cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles,
   return launch_pdl(k_side<C, kBatch>, dim3(grid), dim3(kThreads), smem, st, mA, mB, nTiles, a);
 }
 
-constexpr int kNumCfg = 5;
-constexpr int kCfgNB[kNumCfg] = {Cfg0::NB, Cfg1::NB, Cfg2::NB, Cfg3::NB, Cfg4::NB};
-constexpr int kCfgBN[kNumCfg] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN};
+constexpr int kNumCfg = 7;
+constexpr int kCfgNB[kNumCfg] = {Cfg0::NB, Cfg1::NB, Cfg2::NB, Cfg3::NB, Cfg4::NB, Cfg5::NB, Cfg6::NB};
+constexpr int kCfgBN[kNumCfg] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN};
 constexpr int kDefaultCfg = 0;
 
 }  // namespace
@@ -582,7 +587,9 @@ cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStrea
     case 1: return launch_cfg<Cfg1, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[1]);
     case 2: return launch_cfg<Cfg2, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[2]);
     case 3: return launch_cfg<Cfg3, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[3]);
-    default: return launch_cfg<Cfg4, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
+    case 4: return launch_cfg<Cfg4, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
+    case 5: return launch_cfg<Cfg5, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[5]);
+    default: return launch_cfg<Cfg6, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[6]);
   }
 }
 
@@ -602,6 +609,8 @@ cudaError_t tc_prepare_batch(TcPlan* p, int cfg) {
     case 2: return set_batch_attr<Cfg2>(p->attrSetBatch[2]);
     case 3: return set_batch_attr<Cfg3>(p->attrSetBatch[3]);
     case 4: return set_batch_attr<Cfg4>(p->attrSetBatch[4]);
+    case 5: return set_batch_attr<Cfg5>(p->attrSetBatch[5]);
+    case 6: return set_batch_attr<Cfg6>(p->attrSetBatch[6]);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -620,7 +629,9 @@ cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cud
     case 1: return launch_cfg<Cfg1, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[1]);
     case 2: return launch_cfg<Cfg2, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[2]);
     case 3: return launch_cfg<Cfg3, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[3]);
-    default: return launch_cfg<Cfg4, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[4]);
+    case 4: return launch_cfg<Cfg4, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[4]);
+    case 5: return launch_cfg<Cfg5, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[5]);
+    default: return launch_cfg<Cfg6, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[6]);
   }
 }
 

@@ -23,10 +23,12 @@ namespace {
 // Merges a chunk best into a descriptor's state: best[] keeps the largest key, and whichever
 // key loses the atomic comparison -- the new one, or the best it displaces -- is a second
 // candidate.  Every key but the final best loses exactly one comparison, so sec[] ends as
-// the exact largest of the other chunk bests (ties are impossible: keys carry the index).
+// the exact largest of the other chunk bests.  A key carries the other side's index, so two
+// equal keys are the same (left, right) scored twice (the proposal matcher's symmetric
+// probing can score a pair in two cell blocks): it is one candidate, not a second value.
 __device__ __forceinline__ void merge_chunk_best(unsigned long long* best, unsigned int* sec, unsigned long long cb) {
   const unsigned long long old = atomicMax(best, cb);
-  if (old) atomicMax(sec, (unsigned)((old < cb ? old : cb) >> kIndexBits));
+  if (old && old != cb) atomicMax(sec, (unsigned)((old < cb ? old : cb) >> kIndexBits));
 }
 
 // Chunk records of a side pass: the exact lane-local work the side kernel leaves out.  For

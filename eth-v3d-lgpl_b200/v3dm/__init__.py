@@ -126,8 +126,8 @@ def lib() -> C.CDLL:
         L.v3dm_projection_embed.argtypes = [vp, vp, i32, vp]
         L.v3dm_projection_set_cells.argtypes = [vp, i32, vp]
         L.v3dm_projection_assign.argtypes = [vp, vp, i32, i32, vp]
-        L.v3dm_batch_match_proposal.argtypes = [vp, vp, i32, f32, f32, vp, i64, i64p]
-        L.v3dm_batch_match_proposal_device.argtypes = [vp, vp, i32, f32, f32, vp]
+        L.v3dm_batch_match_proposal.argtypes = [vp, vp, i32, i32, f32, f32, vp, i64, i64p]
+        L.v3dm_batch_match_proposal_device.argtypes = [vp, vp, i32, i32, f32, f32, vp]
         L.v3dm_batch_proposal_scored.argtypes = [vp, i64p, i64p]
         _lib = L
     return _lib
@@ -457,14 +457,15 @@ class BatchMatching:
         return [t[bounds[k]:bounds[k + 1], 1:].copy() for k in range(self.n_pairs)]
 
     def match_proposal(self, projection, probes: int, min_score: float = 0.9, min_ratio: float = 0.8,
-                       cap: int | None = None) -> np.ndarray:
-        """Candidate-proposal matching (v3dm_batch_match_proposal): triples like match()."""
+                       cap: int | None = None, probes_right: int = 1) -> np.ndarray:
+        """Candidate-proposal matching (v3dm_batch_match_proposal): triples like match().
+        probes: cells probed per left; probes_right: cells each right is listed under."""
         cap = cap if cap is not None else max(1 << 20, getattr(self, "_last_n", 0))
         while True:
             out = np.empty((max(1, cap), 3), np.int32)
             n = C.c_longlong(0)
-            st = lib().v3dm_batch_match_proposal(self._h, projection.handle, probes, min_score, min_ratio, _ptr(out),
-                                                 cap, C.byref(n))
+            st = lib().v3dm_batch_match_proposal(self._h, projection.handle, probes, probes_right, min_score,
+                                                 min_ratio, _ptr(out), cap, C.byref(n))
             if st == ERR_CAPACITY:
                 cap = n.value
                 continue
@@ -473,9 +474,9 @@ class BatchMatching:
             return out[: n.value].copy()
 
     def match_proposal_device(self, projection, probes: int, min_score: float, min_ratio: float,
-                              d_count: int = 0) -> None:
-        _check(lib().v3dm_batch_match_proposal_device(self._h, projection.handle, probes, min_score, min_ratio,
-                                                      C.c_void_p(d_count) if d_count else None),
+                              d_count: int = 0, probes_right: int = 1) -> None:
+        _check(lib().v3dm_batch_match_proposal_device(self._h, projection.handle, probes, probes_right, min_score,
+                                                      min_ratio, C.c_void_p(d_count) if d_count else None),
                "batch_match_proposal_device")
 
     def proposal_scored(self):

@@ -233,16 +233,18 @@ V3DM_API int v3dm_batch_last_launches(v3dm_batch* b, int* n);
 V3DM_API int v3dm_batch_work(v3dm_batch* b, long long* int8Ops, long long* nPairs);
 
 /* Candidate-proposal matching of every pair (no counterpart in the reference; see the learned
- * projection below): left l and right r are candidates when r's best cell of the projection
- * is among l's 'probes' best cells; decisions, ratio test and mutual filter are the
- * reference's (.cu:133-210, :546-551) applied to the candidate scores, which are exact uint8
- * scores.  Same output as v3dm_batch_match.  A true match is found when its two descriptors
- * share a probed cell; recall against v3dm_batch_match is what the projection is trained for. */
+ * projection below): left l and right r are candidates when one of l's 'probesLeft' best cells
+ * of the projection is one of r's 'probesRight' best cells; decisions, ratio test and mutual
+ * filter are the reference's (.cu:133-210, :546-551) applied to the candidate scores, which
+ * are exact uint8 scores.  Same output as v3dm_batch_match.  A true match is found when its
+ * two descriptors share a probed cell; recall against v3dm_batch_match is what the projection
+ * is trained for. */
 typedef struct v3dm_projection v3dm_projection;
-V3DM_API int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
-                                       float minRatio, int32_t* triples, long long cap, long long* nOut);
-V3DM_API int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probes, float minScore,
-                                              float minRatio, int32_t* d_count);
+V3DM_API int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int probesLeft, int probesRight,
+                                       float minScore, float minRatio, int32_t* triples, long long cap,
+                                       long long* nOut);
+V3DM_API int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probesLeft,
+                                              int probesRight, float minScore, float minRatio, int32_t* d_count);
 /* (left, right) pairs the last proposal call scored, and the exhaustive count sum(nL * nR). */
 V3DM_API int v3dm_batch_proposal_scored(v3dm_batch* b, long long* scored, long long* exhaustive);
 

@@ -99,7 +99,8 @@ def test_every_config_and_schedule(v3dm_mod, small_set):
     b.set_images(desc, counts)
     b.set_pairs(None)
     ref = None
-    for cfg in range(5):
+    n_cfg = v3dm_mod.SIFTMatching().num_configs()
+    for cfg in range(n_cfg):
         for sch in (0, 1):
             b.set_config(cfg, sch)
             got = b.match(0.7, 0.8)
@@ -107,7 +108,7 @@ def test_every_config_and_schedule(v3dm_mod, small_set):
                 ref = got
             np.testing.assert_array_equal(got, ref, err_msg=f"cfg {cfg} schedule {sch}")
     c, s, ms = b.autotune(0.7, 0.8, 1)
-    assert b.config() == (c, s) and ms.shape == (5, 2) and np.all(ms > 0)
+    assert b.config() == (c, s) and ms.shape == (n_cfg, 2) and np.all(ms > 0)
     np.testing.assert_array_equal(b.match(0.7, 0.8), ref)
     b.close()
 

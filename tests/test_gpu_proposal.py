@@ -71,23 +71,27 @@ def _net_with_cells(v3dm_mod, desc, n_cells, seed=3):
     return net
 
 
-@pytest.mark.parametrize("probes,ms,mr", [(1, 0.7, 0.8), (2, 0.7, 0.8), (3, 0.6, 0.9), (2, 0.7, -1.0)])
-def test_proposal_equals_masked_reference(v3dm_mod, small, probes, ms, mr):
+@pytest.mark.parametrize("probes,probes_right,ms,mr", [(1, 1, 0.7, 0.8), (2, 1, 0.7, 0.8), (3, 1, 0.6, 0.9),
+                                                        (2, 1, 0.7, -1.0), (2, 2, 0.7, 0.8), (3, 2, 0.6, 0.9),
+                                                        (1, 3, 0.7, 0.8)])
+def test_proposal_equals_masked_reference(v3dm_mod, small, probes, probes_right, ms, mr):
+    """Candidates: a left probing one of the cells a right probes (symmetric probing scores a
+    pair once per shared cell; the result must not depend on it)."""
     desc, counts, offs = small
     net = _net_with_cells(v3dm_mod, desc, 6)
     b = v3dm_mod.BatchMatching()
     b.set_images(desc, counts)
     b.set_pairs(None)
-    per = b.split_pairs(b.match_proposal(net, probes, ms, mr))
-    cells = net.assign(desc, probes)
+    per = b.split_pairs(b.match_proposal(net, probes, ms, mr, probes_right=probes_right))
+    cells = net.assign(desc, max(probes, probes_right))
     pairs = synth.all_pairs(len(counts))
     for k, (i, j) in enumerate(pairs):
-        ci, cj = cells[offs[i]:offs[i + 1]], cells[offs[j]:offs[j + 1]]
-        mask = (ci[:, :, None] == cj[None, None, :, 0]).any(1)  # [left, right]
+        ci, cj = cells[offs[i]:offs[i + 1], :probes], cells[offs[j]:offs[j + 1], :probes_right]
+        mask = (ci[:, :, None, None] == cj[None, None, :, :]).any(axis=(1, 3))  # [left, right]
         exp = _masked_match(desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]], mask, ms, mr)
         np.testing.assert_array_equal(per[k], exp, err_msg=f"pair {k} ({i}, {j})")
     scored, exhaustive = b.proposal_scored()
-    assert 0 < scored <= exhaustive
+    assert 0 < scored <= exhaustive * min(probes, probes_right)  # once per shared cell
     b.close()
     net.close()
 
@@ -103,6 +107,10 @@ def test_all_cells_probed_equals_exhaustive(v3dm_mod):
     np.testing.assert_array_equal(got, exh)
     scored, exhaustive = b.proposal_scored()
     assert scored == exhaustive
+    # every right listed under all 4 cells, every left probing 2: each pair is scored twice, in
+    # two cell blocks, and the result is still exhaustive matching
+    np.testing.assert_array_equal(b.match_proposal(net, 2, 0.7, 0.8, probes_right=4), exh)
+    assert b.proposal_scored()[0] == 2 * exhaustive
     # graph replay and the graph-free path agree
     again = b.match_proposal(net, 4, 0.7, 0.8)
     b.use_graph(False)
