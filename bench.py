@@ -589,7 +589,8 @@ def run_proposal(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     tr_desc, tr_counts, tr_offs = synth.images(args.seed + 40, n_images=100, n_min=8000, n_max=8000)
-    te_desc, te_counts, te_offs = synth.images(args.seed + 41, n_images=200, n_min=8000, n_max=8000)
+    te_desc, te_counts, te_offs, te_track = synth.images(args.seed + 41, n_images=200, n_min=8000, n_max=8000,
+                                                         tracks=True)
     b = v3dm.BatchMatching(local)
     b.set_images(tr_desc, tr_counts)
     b.set_pairs(None)
@@ -633,6 +634,11 @@ def run_proposal(args, ws, rank, local):
     clk = clocks.stop()
     got = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right)
     rec, prec = proposal.recall(exh, got)
+    # recall of the exhaustive matches that join two views of one track (the rest are chance
+    # matches between unrelated descriptors, which no candidate proposal can find)
+    pairs_all = synth.all_pairs(200)
+    inl = synth.inlier_mask(exh, pairs_all, te_offs, te_track)
+    rec_in, _ = proposal.recall(exh[inl], got)
     scored, exhaustive = b.proposal_scored()
     b.profile(True)
     for _ in range(3):
@@ -644,7 +650,9 @@ def run_proposal(args, ws, rank, local):
     net0 = v3dm.Projection(local, seed=args.seed)
     net0.set_cells(proposal.fit_cells(net0.embed(tr_desc), args.cells, seed=args.seed))
     ms0, _ = timed(lambda: b.match_proposal_device(net0, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right))
-    rec0, prec0 = proposal.recall(exh, b.match_proposal(net0, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right))
+    got0 = b.match_proposal(net0, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right)
+    rec0, prec0 = proposal.recall(exh, got0)
+    rec0_in, _ = proposal.recall(exh[inl], got0)
     scored0, _ = b.proposal_scored()
     net0.close()
     # e2e: descriptors from pinned host memory, triples back
@@ -685,9 +693,11 @@ def run_proposal(args, ws, rank, local):
                    "l2": "inputs larger than L2 (205 MB of descriptors)"},
         "exhaustive": {"value": ws * n_pairs * 1000.0 / ms_exh, "unit": "pairs/s", "ms_per_step": ms_exh},
         "speedup_vs_exhaustive": ms_exh / ms_prop,
-        "recall": rec, "precision": prec, "matches_exhaustive": int(len(exh)), "matches_proposal": int(len(got)),
+        "recall": rec, "precision": prec, "recall_inliers": rec_in,
+        "matches_exhaustive": int(len(exh)), "inliers_exhaustive": int(inl.sum()), "matches_proposal": int(len(got)),
         "scored_fraction": scored / exhaustive,
-        "ablation_untrained": {"recall": rec0, "precision": prec0, "scored_fraction": scored0 / exhaustive,
+        "ablation_untrained": {"recall": rec0, "precision": prec0, "recall_inliers": rec0_in,
+                               "scored_fraction": scored0 / exhaustive,
                                "ms_per_step": ms0},
         "training": {"seconds": train_s, "loss_first": losses[0][1], "loss_last": losses[-1][1]},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",

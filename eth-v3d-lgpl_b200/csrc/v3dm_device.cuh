@@ -11,6 +11,17 @@ namespace v3dm {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Merges a chunk best into a descriptor's state: best[] keeps the largest key, and whichever
+// key loses the atomic comparison -- the new one, or the best it displaces -- is a second
+// candidate.  Every key but the final best loses exactly one comparison, so sec[] ends as
+// the exact largest of the other chunk bests.  A key carries the other side's index, so two
+// equal keys are the same (left, right) scored twice (the proposal matcher's symmetric
+// probing can score a pair in two cell blocks): it is one candidate, not a second value.
+__device__ __forceinline__ void merge_chunk_best(unsigned long long* best, unsigned int* sec, unsigned long long cb) {
+  const unsigned long long old = atomicMax(best, cb);
+  if (old && old != cb) atomicMax(sec, (unsigned)((old < cb ? old : cb) >> kIndexBits));
+}
+
 // A candidate (l, r, S): both best keys take it with an atomicMax whose result is unused
 // (a fire-and-forget reduction, so the issuing warp does not wait for L2).
 __device__ __forceinline__ void record_best(const MatchArgs& a, int l, int r, int32_t S) {

@@ -271,54 +271,64 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
 // chunk best is the largest candidate (first column on ties), the other candidates bound the
 // second value.  Scores below Tf (and masked ones, which the reference sets to -1e20) cannot
 // change a decision and are left out.  Chunk bests merge as in k_records (the key that loses
-// the atomic comparison is a second candidate).
+// the atomic comparison is a second candidate); the lane layout is k_records' as well (eight
+// lanes per record, four scores each, four records per warp at a time).
 __global__ void k_records_f(PostArgs a, float Tf) {
   pdl_wait();
   pdl_launch_dependents();
   int32_t* info = a.err - kInfoErr;
   const int lane = threadIdx.x & 31;
+  const int grp = lane >> 3, part = lane & 7;
   const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
     const int cnt = a.segCount[seg];
-    const long long n = cnt < a.segCap ? cnt : a.segCap;
     if (cnt == 0) continue;
+    const int n = (long long)cnt < a.segCap ? cnt : (int)a.segCap;
     const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
-    for (long long i = lane; i < n; i += 32) {
-      const uint4* rec = recs + i * kRecordQuads;
-      const uint4 head = rec[0];
+    for (int i0 = 0; i0 < n; i0 += 4) {
+      const int i = i0 + grp;
+      const bool have = i < n;
+      uint4 head = make_uint4(0u, 0u, 0u, 0u), q = head;
+      if (have) {
+        head = recs[(long long)i * kRecordQuads];
+        q = recs[(long long)i * kRecordQuads + 1 + part];
+      }
       const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z;
+      const uint32_t sv[4] = {q.x, q.y, q.z, q.w};
+      unsigned long long key[4];
       unsigned long long cb = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int col = col0 + 4 * part + t;
+        const float sc = __uint_as_float(sv[t]);
+        bool cand = have && col < nB && sc >= Tf;
+        for (int gi = 0; gi < a.nGates && cand; ++gi)
+          cand = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
+        key[t] = cand ? best_key_f(sc, col) : 0ull;
+        cb = key[t] > cb ? key[t] : cb;
+      }
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, cb, off);
+        cb = o > cb ? o : cb;
+      }
       uint32_t cw = 0;
-      for (int k = 0; k < 8; ++k) {
-        const uint4 qd = rec[1 + k];
-        const uint32_t sv[4] = {qd.x, qd.y, qd.z, qd.w};
-        for (int t = 0; t < 4; ++t) {
-          const int col = col0 + 4 * k + t;
-          if (col >= nB) break;
-          const float sc = __uint_as_float(sv[t]);
-          if (!(sc >= Tf)) continue;
-          bool masked = false;
-          for (int gi = 0; gi < a.nGates && !masked; ++gi)
-            masked = gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
-          if (masked) continue;
-          const unsigned long long key = best_key_f(sc, col);
-          if (key > cb) {
-            cw = max(cw, (uint32_t)(cb >> kIndexBits));
-            cb = key;
-          } else {
-            cw = max(cw, f32_order(sc));
-          }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (key[t] != 0ull && key[t] != cb) cw = max(cw, (uint32_t)(key[t] >> kIndexBits));
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) cw = max(cw, __shfl_xor_sync(0xffffffffu, cw, off));
+      if (have && part == 0) {
+        if (cb) {
+          const unsigned long long old = atomicMax(&a.best[orig], cb);
+          if (old && old != cb) atomicMax(&a.sec[orig], (unsigned)((old < cb ? old : cb) >> kIndexBits));
         }
+        if (cw) atomicMax(&a.sec[orig], cw);
       }
-      if (cb) {
-        const unsigned long long old = atomicMax(&a.best[orig], cb);
-        if (old && old != cb) atomicMax(&a.sec[orig], (unsigned)((old < cb ? old : cb) >> kIndexBits));
-      }
-      if (cw) atomicMax(&a.sec[orig], cw);
     }
     if (lane == 0) {
-      atomicMax(&info[kInfoMaxSeg], cnt);
+      if ((long long)cnt > a.segCap) atomicMax(&info[kInfoMaxSeg], cnt);  // overflow only
       a.segCount[seg] = 0;
     }
   }
@@ -327,6 +337,7 @@ __global__ void k_records_f(PostArgs a, float Tf) {
 __global__ void k_decide_f(PostArgs a) {
   pdl_wait();
   pdl_launch_dependents();
+  const int lane = threadIdx.x & 31;
   const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
     const int idx = a.amap ? a.amap[r] : r;
@@ -334,15 +345,27 @@ __global__ void k_decide_f(PostArgs a) {
     const unsigned s = a.sec[idx];
     const int32_t d = decide_f(b, s, a.minScore, a.minRatio);
     a.decision[idx] = d;
-    if (a.chooseFlag && d >= 0 && atomicExch(&a.chooseFlag[d], 1) == 0) {
-      // chosen for pass B: listed once, planar row gathered
-      const int k = atomicAdd(a.chooseCount, 1);
-      a.chooseList[k] = d;
-      for (int p = 0; p < kFPlanes; ++p) {
-        const uint4* src = reinterpret_cast<const uint4*>(a.chooseSrc + ((size_t)p * a.chooseCapSrc + d) * 128);
-        uint4* dst = reinterpret_cast<uint4*>(a.chooseDst + ((size_t)p * a.chooseCapDst + k) * 128);
+    if (a.chooseFlag) {
+      // chosen for pass B: listed once (the claiming lanes of a warp take consecutive slots
+      // with one counter update), planar row gathered
+      const bool claim = d >= 0 && atomicExch(&a.chooseFlag[d], 1) == 0;
+      const unsigned act = __activemask();
+      const unsigned m = __ballot_sync(act, claim);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.chooseCount, __popc(m));
+        base = __shfl_sync(act, base, leader);
+        if (claim) {
+          const int k = base + __popc(m & ((1u << lane) - 1u));
+          a.chooseList[k] = d;
+          for (int p = 0; p < kFPlanes; ++p) {
+            const uint4* src = reinterpret_cast<const uint4*>(a.chooseSrc + ((size_t)p * a.chooseCapSrc + d) * 128);
+            uint4* dst = reinterpret_cast<uint4*>(a.chooseDst + ((size_t)p * a.chooseCapDst + k) * 128);
 #pragma unroll
-        for (int w = 0; w < 8; ++w) dst[w] = src[w];
+            for (int w = 0; w < 8; ++w) dst[w] = src[w];
+          }
+        }
       }
     }
     if (b) a.best[idx] = 0;

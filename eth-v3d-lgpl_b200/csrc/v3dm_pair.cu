@@ -1,8 +1,7 @@
 // v3dm_pair.cu -- decisions and bookkeeping around the two tcgen05 side passes of a pair.
 //
-//   k_records  exact work on the chunk records of a side pass (gates, chunk best, bound);
-//   k_list     list pass (every chunk best that is not the descriptor's overall best raises its
-//              second value);
+//   k_records  exact work on the chunk records of a side pass (gates, chunk best, bound), merged
+//              into each descriptor's best key and second value;
 //   k_decide   the per-descriptor decision of the reference
 //              (v3d_cudamatching.cu:147-161 / :196-209, or the no-ratio test at :48 / :84).
 //              With guided gates the second value is an upper bound; when the decision with
@@ -20,77 +19,87 @@ namespace v3dm {
 
 namespace {
 
-// Merges a chunk best into a descriptor's state: best[] keeps the largest key, and whichever
-// key loses the atomic comparison -- the new one, or the best it displaces -- is a second
-// candidate.  Every key but the final best loses exactly one comparison, so sec[] ends as
-// the exact largest of the other chunk bests.  A key carries the other side's index, so two
-// equal keys are the same (left, right) scored twice (the proposal matcher's symmetric
-// probing can score a pair in two cell blocks): it is one candidate, not a second value.
-__device__ __forceinline__ void merge_chunk_best(unsigned long long* best, unsigned int* sec, unsigned long long cb) {
-  const unsigned long long old = atomicMax(best, cb);
-  if (old && old != cb) atomicMax(sec, (unsigned)((old < cb ? old : cb) >> kIndexBits));
-}
-
 // Chunk records of a side pass: the exact lane-local work the side kernel leaves out.  For
 // every score >= Smin the gates decide whether it is a candidate; the chunk best is the
 // largest candidate (first column on ties), every other score of the chunk (candidates,
-// masked scores and scores below Smin alike) bounds the second value.  One warp per record
-// segment; the segment's count is recorded (overflow check) and cleared for the next pass.
+// masked scores and scores below Smin alike) bounds the second value.  kRecWarps warps share
+// a record segment; a warp takes four records at a time: the eight lanes of a record hold
+// four scores each (one coalesced 16-byte load), reduce the best key across the group, then
+// the largest other score.  k_decide clears the segment counts for the next pass and reports
+// an overflowing count (the host grows the list when it exceeds the capacity).
+constexpr int kRecWarps = 4;
+
 __global__ void k_records(PostArgs a) {
   pdl_wait();
   pdl_launch_dependents();
-  int32_t* info = a.err - kInfoErr;
   const int lane = threadIdx.x & 31;
+  const int grp = lane >> 3;   // record of the four this lane works on
+  const int part = lane & 7;   // its four scores: columns 4 * part .. 4 * part + 3
   const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int seg = warpGlobal; seg < a.nSeg; seg += nWarps) {
+  for (int w = warpGlobal; w < a.nSeg * kRecWarps; w += nWarps) {
+    const int seg = w / kRecWarps, sub = w % kRecWarps;
     const int cnt = a.segCount[seg];
-    const long long n = cnt < a.segCap ? cnt : a.segCap;
     if (cnt == 0) continue;
+    const int n = (long long)cnt < a.segCap ? cnt : (int)a.segCap;
     const uint4* recs = a.records + (long long)seg * a.segCap * kRecordQuads;
-    for (long long i = lane; i < n; i += 32) {
-      const uint4* rec = recs + i * kRecordQuads;
-      const uint4 head = rec[0];
-      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z, bRow0 = (int)head.w;
-      unsigned long long cb = 0;
-      uint32_t cw = 0;
-      for (int k = 0; k < 8; ++k) {
-        const uint4 q = rec[1 + k];
-        const uint32_t sv[4] = {q.x, q.y, q.z, q.w};
-        for (int t = 0; t < 4; ++t) {
-          const int col = col0 + 4 * k + t;
-          if (col >= nB) break;
-          const int32_t S = (int32_t)sv[t];
-          bool strong = S >= a.Smin;
-          for (int gi = 0; gi < a.nGates && strong; ++gi)
-            strong = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
-          if (strong) {
-            const unsigned long long key = best_key(S, a.bmap ? __ldg(a.bmap + bRow0 + col) : col);
-            if (key > cb) {
-              cw = max(cw, (uint32_t)(cb >> kIndexBits));
-              cb = key;
-            } else {
-              cw = max(cw, (uint32_t)(S + 1));
-            }
-          } else {
-            cw = max(cw, (uint32_t)(S + 1));
-          }
-        }
+    for (int i0 = 4 * sub; i0 < n; i0 += 4 * kRecWarps) {
+      const int i = i0 + grp;
+      const bool have = i < n;
+      uint4 head = make_uint4(0u, 0u, 0u, 0u), q = head;
+      if (have) {
+        head = recs[(long long)i * kRecordQuads];
+        q = recs[(long long)i * kRecordQuads + 1 + part];
       }
-      if (cb) merge_chunk_best(&a.best[orig], &a.sec[orig], cb);
-      if (cw) atomicMax(&a.sec[orig], cw);
-    }
-    if (lane == 0) {
-      atomicMax(&info[kInfoMaxSeg], cnt);
-      a.segCount[seg] = 0;
+      const int orig = (int)head.x, col0 = (int)head.y, nB = (int)head.z, bRow0 = (int)head.w;
+      const uint32_t sv[4] = {q.x, q.y, q.z, q.w};
+      unsigned long long key[4];
+      bool valid[4];
+      unsigned long long cb = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int col = col0 + 4 * part + t;
+        valid[t] = have && col < nB;
+        const int32_t S = (int32_t)sv[t];
+        bool strong = valid[t] && S >= a.Smin;
+        for (int gi = 0; gi < a.nGates && strong; ++gi)
+          strong = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
+        key[t] = strong ? best_key(S, a.bmap ? __ldg(a.bmap + bRow0 + col) : col) : 0ull;
+        cb = key[t] > cb ? key[t] : cb;
+      }
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, cb, off);
+        cb = o > cb ? o : cb;
+      }
+      // every valid score but the chunk best's own bounds the second value
+      uint32_t cw = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (valid[t] && !(key[t] != 0ull && key[t] == cb)) cw = max(cw, sv[t] + 1u);
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) cw = max(cw, __shfl_xor_sync(0xffffffffu, cw, off));
+      if (have && part == 0) {
+        if (cb) merge_chunk_best(&a.best[orig], &a.sec[orig], cb);
+        if (cw) atomicMax(&a.sec[orig], cw);
+      }
     }
   }
 }
 
-// Chooses right r for pass B (once): flag, list entry, descriptor row gathered.
-__device__ __forceinline__ void choose_one(const PostArgs& a, int r) {
-  if (atomicExch(&a.chooseFlag[r], 1) != 0) return;
-  const int k = atomicAdd(a.chooseCount, 1);
+// Clears the segment counts after k_records (a separate launch: every warp of a segment reads
+// the count first); reports an overflowing count.
+__device__ __forceinline__ void clear_segments(const PostArgs& a) {
+  int32_t* info = a.err - kInfoErr;
+  for (int seg = blockIdx.x * blockDim.x + threadIdx.x; seg < a.nSeg; seg += gridDim.x * blockDim.x) {
+    const int cnt = a.segCount[seg];
+    if ((long long)cnt > a.segCap) atomicMax(&info[kInfoMaxSeg], cnt);
+    if (cnt) a.segCount[seg] = 0;
+  }
+}
+
+// Copies right r's descriptor row to slot k of the pass-B operand.
+__device__ __forceinline__ void gather_chosen(const PostArgs& a, int r, int k) {
   a.chooseList[k] = r;
   if (a.choosePlanes) {
     for (int p = 0; p < a.choosePlanes; ++p) {
@@ -109,28 +118,42 @@ __device__ __forceinline__ void choose_one(const PostArgs& a, int r) {
 
 // Decisions of the pass's descriptors; flags the ones whose gated bound straddles the
 // decision, clears the state of the others.  With a.chooseFlag set, accepted partners are
-// chosen for pass B right away.
+// chosen for pass B right away: the first left to name a right claims it (flag exchange),
+// and the claiming lanes of a warp take consecutive list slots with one counter update.
 __global__ void k_decide(PostArgs a) {
   pdl_wait();
   pdl_launch_dependents();
+  clear_segments(a);
+  const int lane = threadIdx.x & 31;
   const int nRows = a.rowsPtr ? *a.rowsPtr : a.nRows;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
     const int idx = a.amap ? a.amap[r] : r;
     const unsigned long long b = a.best[idx];
     const unsigned s = a.sec[idx];
-    const int32_t d = decide(b, s, a.minScore, a.minRatio);
+    int32_t d = decide(b, s, a.minScore, a.minRatio);
     if (a.gated && b != 0 && s != 0 && d != decide(b, 0u, a.minScore, a.minRatio)) {
       // the bound straddles the decision: exact re-score (k_rescore clears the state)
       const int k = atomicAdd(a.flaggedCount, 1);
       a.flagged[k] = idx;
-      a.decision[idx] = -1;
       a.sec[idx] = 0;  // recomputed exactly by k_rescore
-      continue;
+      d = -1;
+    } else {
+      if (b) a.best[idx] = 0;
+      if (s) a.sec[idx] = 0;
     }
     a.decision[idx] = d;
-    if (a.chooseFlag && d >= 0) choose_one(a, d);
-    if (b) a.best[idx] = 0;
-    if (s) a.sec[idx] = 0;
+    if (a.chooseFlag) {
+      const bool claim = d >= 0 && atomicExch(&a.chooseFlag[d], 1) == 0;
+      const unsigned act = __activemask();
+      const unsigned m = __ballot_sync(act, claim);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.chooseCount, __popc(m));
+        base = __shfl_sync(act, base, leader);
+        if (claim) gather_chosen(a, d, base + __popc(m & ((1u << lane) - 1u)));
+      }
+    }
   }
 }
 
@@ -211,11 +234,21 @@ __global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chose
                          int* chosenCount, const uint8_t* __restrict__ dR, uint8_t* __restrict__ dRc) {
   pdl_wait();
   pdl_launch_dependents();
+  const int lane = threadIdx.x & 31;
   for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nL; l += gridDim.x * blockDim.x) {
     const int r = leftDec[l];
-    if (r < 0) continue;
-    if (atomicExch(&chosenFlag[r], 1) != 0) continue;
-    const int k = atomicAdd(chosenCount, 1);
+    // the first left to name a right claims it; the claiming lanes of a warp take
+    // consecutive list slots with one counter update
+    const bool claim = r >= 0 && atomicExch(&chosenFlag[r], 1) == 0;
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, claim);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(chosenCount, __popc(m));
+    base = __shfl_sync(act, base, leader);
+    if (!claim) continue;
+    const int k = base + __popc(m & ((1u << lane) - 1u));
     chosenList[k] = r;
     const uint4* src = reinterpret_cast<const uint4*>(dR + (size_t)r * kDescBytes);
     uint4* dst = reinterpret_cast<uint4*>(dRc + (size_t)k * kDescBytes);
@@ -225,7 +258,7 @@ __global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chose
 }
 
 constexpr int kMutThreads = 256;
-constexpr int kMutPerBlock = 2048;  // lefts per block (8 per thread, contiguous)
+constexpr int kMutPerBlock = kMutThreads;  // one left per thread: every load of a thread in flight at once
 
 // Pass 1: number of mutual pairs among each block's contiguous range of lefts.
 __global__ void __launch_bounds__(kMutThreads)
@@ -234,12 +267,9 @@ k_mutual_count(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
   pdl_wait();
   pdl_launch_dependents();
   __shared__ int wsum[kMutThreads / 32];
-  const int base = blockIdx.x * kMutPerBlock;
-  int cnt = 0;
-  for (int k = base + threadIdx.x; k < min(base + kMutPerBlock, nL); k += kMutThreads) {
-    const int r = leftDec[k];
-    cnt += r >= 0 && rightDec[r] == k;
-  }
+  const int k = blockIdx.x * kMutPerBlock + threadIdx.x;
+  const int r = k < nL ? leftDec[k] : -1;
+  int cnt = r >= 0 && rightDec[r] == k;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
@@ -251,65 +281,53 @@ k_mutual_count(const int32_t* __restrict__ leftDec, int nL, const int32_t* __res
   }
 }
 
-// Pass 2: each block offsets its pairs by the counts of the blocks before it and writes them
-// in ascending left order; clears the chosen-right flags.
+// Pass 2: each block offsets its pairs by the counts of the blocks before it (summed by the
+// whole block) and writes them in ascending left order; clears the chosen-right flags.
 __global__ void __launch_bounds__(kMutThreads)
 k_mutual_write(const int32_t* __restrict__ leftDec, int nL, const int32_t* __restrict__ rightDec, int* chosenFlag,
                const int* __restrict__ blockCount, int nBlocks, int2* __restrict__ pairs, int32_t* info,
                int32_t* countOut) {
   pdl_wait();
   pdl_launch_dependents();
-  __shared__ int blockOff;
   __shared__ int wsum[kMutThreads / 32];
-  if (threadIdx.x < 32) {
-    int t = 0;
-    for (int b = threadIdx.x; b < (int)blockIdx.x; b += 32) t += blockCount[b];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (threadIdx.x == 0) {
-      blockOff = t;
-      if (blockIdx.x == nBlocks - 1) {
-        info[kInfoPairs] = t + blockCount[blockIdx.x];
-        if (countOut) *countOut = t + blockCount[blockIdx.x];
-      }
-    }
-  }
-  // each thread owns kMutPerBlock / kMutThreads consecutive lefts
-  constexpr int kPer = kMutPerBlock / kMutThreads;
-  const int beg = blockIdx.x * kMutPerBlock + threadIdx.x * kPer;
-  int r[kPer];
-  int cnt = 0;
-#pragma unroll
-  for (int i = 0; i < kPer; ++i) {
-    const int k = beg + i;
-    r[i] = k < nL ? leftDec[k] : -1;
-    const bool ok = r[i] >= 0 && rightDec[r[i]] == k;
-    if (r[i] >= 0) chosenFlag[r[i]] = 0;
-    if (!ok) r[i] = -1;
-    cnt += ok;
-  }
+  __shared__ int wbefore[kMutThreads / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int k = blockIdx.x * kMutPerBlock + threadIdx.x;
+  const int r = k < nL ? leftDec[k] : -1;
+  const bool ok = r >= 0 && rightDec[r] == k;
+  if (r >= 0) chosenFlag[r] = 0;
+  int t = 0;
+  for (int b = threadIdx.x; b < (int)blockIdx.x; b += kMutThreads) t += blockCount[b];
+  const int cnt = ok ? 1 : 0;
   int inc = cnt;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int v = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= o) inc += v;
   }
-  if (lane == 31) wsum[wid] = inc;
-  __syncthreads();
-  int before = 0;
-  for (int w = 0; w < wid; ++w) before += wsum[w];
-  int off = blockOff + before + inc - cnt;
 #pragma unroll
-  for (int i = 0; i < kPer; ++i)
-    if (r[i] >= 0) pairs[off++] = make_int2(beg + i, r[i]);
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 31) wsum[wid] = inc;
+  if (lane == 0) wbefore[wid] = t;
+  __syncthreads();
+  int blockOff = 0, before = 0;
+  for (int w = 0; w < kMutThreads / 32; ++w) {
+    blockOff += wbefore[w];
+    if (w < wid) before += wsum[w];
+  }
+  if (ok) pairs[blockOff + before + inc - cnt] = make_int2(k, r);
+  if (threadIdx.x == kMutThreads - 1 && blockIdx.x == nBlocks - 1) {
+    const int total = blockOff + before + inc;
+    info[kInfoPairs] = total;
+    if (countOut) *countOut = total;
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s) {
-  const int listBlocks = (a.nSeg * 32 + 255) / 256;
-  cudaError_t e = launch_pdl(k_records, dim3(listBlocks < 512 ? listBlocks : 512), dim3(256), 0, s, a);
+  const int recBlocks = (a.nSeg * kRecWarps * 32 + 255) / 256;
+  cudaError_t e = launch_pdl(k_records, dim3(recBlocks < 2048 ? recBlocks : 2048), dim3(256), 0, s, a);
   if (e != cudaSuccess) return e;
   int rows = a.nRows > 0 ? a.nRows : 1;
   int blocks = (rows + 255) / 256;

@@ -100,11 +100,12 @@ def stereo(seed: int = 1, n_left: int = 16384, n_right: int = 16384, planted: fl
 
 
 def images(seed: int = 2, n_images: int = 200, n_min: int = 1000, n_max: int = 12000,
-           track_frac: float = 0.15, track_len=(2, 8)):
+           track_frac: float = 0.15, track_len=(2, 8), tracks: bool = False):
     """Image set for all-pairs matching.  Returns (desc, counts, offsets): desc is the
     concatenation of all images' uint8 descriptors.  A track is a base descriptor observed
     in a random subset of images with per-view N(0, 8^2) noise; track observations make up
-    track_frac of every image's features."""
+    track_frac of every image's features.  With tracks=True a fourth array gives every
+    descriptor's track id (-1: an unrelated descriptor); the descriptors are the same."""
     rng = rng_for(seed)
     counts = rng.integers(n_min, n_max + 1, n_images)
     slots = np.rint(track_frac * counts).astype(np.int64)
@@ -131,11 +132,23 @@ def images(seed: int = 2, n_images: int = 200, n_min: int = 1000, n_max: int = 1
     obs_img, obs_track = obs_img[order], obs_track[order]
     starts = np.searchsorted(obs_img, np.arange(n_images))
     ends = np.searchsorted(obs_img, np.arange(n_images), side="right")
+    track_id = np.full(int(offsets[-1]), -1, np.int64)
     for i in range(n_images):
         tr = obs_track[starts[i]:ends[i]]
         feats = np.concatenate([noisy_copy(rng, base[tr]), sift_like(rng, int(counts[i]) - tr.size)])
-        desc[offsets[i]:offsets[i + 1]] = feats[rng.permutation(int(counts[i]))]
+        perm = rng.permutation(int(counts[i]))
+        desc[offsets[i]:offsets[i + 1]] = feats[perm]
+        track_id[offsets[i]:offsets[i + 1]] = np.concatenate([tr, np.full(int(counts[i]) - tr.size, -1)])[perm]
+    if tracks:
+        return desc, counts.astype(np.int32), offsets, track_id
     return desc, counts.astype(np.int32), offsets
+
+
+def inlier_mask(triples: np.ndarray, pairs: np.ndarray, offsets: np.ndarray, track_id: np.ndarray) -> np.ndarray:
+    """True for the match triples (pair, left, right) that join two views of one track."""
+    tl = track_id[offsets[pairs[triples[:, 0], 0]] + triples[:, 1]]
+    tr = track_id[offsets[pairs[triples[:, 0], 1]] + triples[:, 2]]
+    return (tl >= 0) & (tl == tr)
 
 
 def all_pairs(n_images: int) -> np.ndarray:
