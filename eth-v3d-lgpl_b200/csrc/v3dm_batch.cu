@@ -62,7 +62,7 @@ constexpr int kCntOut = 3;        // triples written
 constexpr int kCntNeedStates = 4; // sizes the pass-B buffers need
 constexpr int kCntNeedRows = 5;
 constexpr int kCntNeedTable = 6;
-constexpr int kCntAll = 12;      // batch and proposal counter words
+constexpr int kCntAll = 16;      // batch and proposal counter words
 
 constexpr int kScanThreads = 1024;
 constexpr int kChooseThreads = 256;
@@ -312,6 +312,7 @@ k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, co
 constexpr int kCntRowsP = 8;      // counter words of the proposal (after the batch ones)
 constexpr int kCntOverP = 9;      // 1: the proposal row table was too small
 constexpr int kCntScored = 10;    // two words: scored (left, right) pairs, 64-bit
+constexpr int kCntRowsPB = 12;    // rows of the proposal's pass B
 
 // Per image and cell: rows whose probed cells include the cell (A) and rows whose best cell
 // it is (B).
@@ -383,34 +384,47 @@ __global__ void k_pscatter(const BImage* __restrict__ im, int nImages, const uin
   }
 }
 
-// Rows of every pair: one per (cell with rights, group of GM lefts probing it); also counts the
-// scored (left, right) pairs.
-__global__ void k_prowcount(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im, int C, int GM,
-                            const int* __restrict__ cntA, const int* __restrict__ cntB, int* __restrict__ rowCnt,
+// Row table of the proposal, cell-major: for every cell c, every left image i, every group g
+// of GM lefts of i probing c, one row per pair (i, j) of the batch whose right image has
+// rights under c, in batch order.  Consecutive rows then share their A block (the group), and
+// the rows of one cell -- whose right blocks are what the CTAs read at the same time -- are
+// together in the table.  One warp per (cell, left image) unit u = c * nImages + i.
+// Pass 1 counts the unit's rows and the scored (left, right) pairs.
+__global__ void k_prowcount(const BPair* __restrict__ pairs, const BImage* __restrict__ im, int nImages, int C,
+                            int GM, const int* __restrict__ cntA, const int* __restrict__ cntB, int* __restrict__ rowCnt,
                             unsigned long long* __restrict__ scored) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nPairs) return;
-  const BPair q = pairs[p];
-  int rows = 0;
-  unsigned long long sc = 0;
-  if (im[q.ri].n > 0)
-    for (int c = 0; c < C; ++c) {
-      const int a = cntA[q.li * C + c], b = cntB[q.ri * C + c];
-      if (a > 0 && b > 0) {
-        rows += (a + GM - 1) / GM;
-        sc += (unsigned long long)a * b;
+  const int lane = threadIdx.x & 31;
+  const int nUnits = nImages * C;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < nUnits; u += (gridDim.x * blockDim.x) >> 5) {
+    const int c = u / nImages, i = u - c * nImages;
+    const int a = cntA[i * C + c];
+    const BImage m = im[i];
+    int partners = 0;
+    unsigned long long sb = 0;
+    if (a > 0)
+      for (int p = m.pairBeg + lane; p < m.pairEnd; p += 32) {
+        const int b = cntB[pairs[p].ri * C + c];
+        partners += b > 0;
+        sb += (unsigned long long)b;
       }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      partners += __shfl_xor_sync(0xffffffffu, partners, o);
+      sb += __shfl_xor_sync(0xffffffffu, sb, o);
     }
-  rowCnt[p] = rows;
-  if (sc) atomicAdd(scored, sc);
+    if (lane == 0) {
+      rowCnt[u] = partners * ((a + GM - 1) / GM);
+      if (sb) atomicAdd(scored, sb * (unsigned long long)a);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kScanThreads)
-k_pscan_rows(const int* __restrict__ rowCnt, int nPairs, long long capRows, int* __restrict__ rowStart,
+k_pscan_rows(const int* __restrict__ rowCnt, int nUnits, long long capRows, int* __restrict__ rowStart,
              int* __restrict__ counters) {
   __shared__ long long sh[kScanThreads];
   const long long total = block_scan(
-      nPairs, [&](int i) { return (long long)rowCnt[i]; }, [&](int i, long long x) { rowStart[i] = (int)x; }, sh);
+      nUnits, [&](int i) { return (long long)rowCnt[i]; }, [&](int i, long long x) { rowStart[i] = (int)x; }, sh);
   if (threadIdx.x == 0) {
     const bool over = total > capRows;
     counters[kCntRowsP] = over ? 0 : (int)total;
@@ -418,28 +432,42 @@ k_pscan_rows(const int* __restrict__ rowCnt, int nPairs, long long capRows, int*
   }
 }
 
-__global__ void k_prows(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im, int C, int GM,
+// Pass 2 writes the unit's rows: groups outer, the partner pairs inner in batch order.
+__global__ void k_prows(const BPair* __restrict__ pairs, const BImage* __restrict__ im, int nImages, int C, int GM,
                         int BN, const int* __restrict__ cntA, const int* __restrict__ cntB,
                         const int* __restrict__ offA, const int* __restrict__ offB, const int* __restrict__ rowStart,
                         const int* __restrict__ counters, BatchRow* __restrict__ rows) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nPairs || counters[kCntOverP]) return;
-  const BPair q = pairs[p];
-  if (im[q.ri].n == 0) return;
-  int at = rowStart[p];
-  for (int c = 0; c < C; ++c) {
-    const int a = cntA[q.li * C + c], b = cntB[q.ri * C + c];
-    if (a == 0 || b == 0) continue;
+  if (counters[kCntOverP]) return;
+  const int lane = threadIdx.x & 31;
+  const int nUnits = nImages * C;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < nUnits; u += (gridDim.x * blockDim.x) >> 5) {
+    const int c = u / nImages, i = u - c * nImages;
+    const int a = cntA[i * C + c];
+    if (a == 0) continue;
+    const BImage m = im[i];
+    int at = rowStart[u];
     for (int g = 0; g * GM < a; ++g) {
-      BatchRow r;
-      r.aRow = offA[q.li * C + c] + g * GM;
-      r.validRows = min(GM, a - g * GM);
-      r.bRow0 = offB[q.ri * C + c];
-      r.nB = b;
-      r.nTiles = (b + BN - 1) / BN;
-      r.pad = 0;
-      r.state0 = q.stateA0;
-      rows[at++] = r;
+      for (int p0 = m.pairBeg; p0 < m.pairEnd; p0 += 32) {
+        const int p = p0 + lane;
+        int b = 0, ri = 0;
+        if (p < m.pairEnd) {
+          ri = pairs[p].ri;
+          b = cntB[ri * C + c];
+        }
+        const unsigned mk = __ballot_sync(0xffffffffu, b > 0);
+        if (b > 0) {
+          BatchRow r;
+          r.aRow = offA[i * C + c] + g * GM;
+          r.validRows = min(GM, a - g * GM);
+          r.bRow0 = offB[ri * C + c];
+          r.nB = b;
+          r.nTiles = (b + BN - 1) / BN;
+          r.pad = 0;
+          r.state0 = pairs[p].stateA0;
+          rows[at + __popc(mk & ((1u << lane) - 1u))] = r;
+        }
+        at += __popc(mk);
+      }
     }
   }
 }
@@ -499,65 +527,95 @@ k_pchoose(const BPair* __restrict__ pairs, int nPairs, const long long* __restri
   }
 }
 
-// Row decision of every chosen right over its candidate lefts (the lefts of the pair's left
-// image that probe the right's best cell), exactly: one warp per pass-B state, the right's
-// descriptor in every lane's registers, lanes striding over the candidates.
-__global__ void __launch_bounds__(256)
-k_ppassb(const BPair* __restrict__ pairs, const BImage* __restrict__ im, const uint8_t* __restrict__ cell, int probes,
-         int probesR, int C, const int* __restrict__ cntA, const int* __restrict__ offA, const uint8_t* __restrict__ la,
-         const int* __restrict__ mapA, const uint8_t* __restrict__ img, const int* __restrict__ chosenRight,
-         const int* __restrict__ chosenSorted, const int* __restrict__ counters, float minScore, float minRatio,
-         int32_t* __restrict__ decB) {
-  const int n = counters[kCntStates];
-  const int lane = threadIdx.x & 31;
-  const int warpG = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int s = warpG; s < n; s += nWarps) {
-    const BPair q = pairs[chosenSorted[s]];
-    const int r = chosenRight[s];
-    const int rRow = im[q.ri].rowOff + r;
-    uint4 rv[kDescBytes / 16];
-    const uint4* rs = reinterpret_cast<const uint4*>(img + (size_t)rRow * kDescBytes);
-#pragma unroll
-    for (int x = 0; x < kDescBytes / 16; ++x) rv[x] = __ldg(rs + x);
-    unsigned long long best = 0;
-    uint32_t sec = 0;
-    for (int pr = 0; pr < probesR; ++pr) {  // the lefts probing any cell the right probes
-      const int c1 = cell[(size_t)rRow * probes + pr];
-      const int cnt = cntA[q.li * C + c1];
-      const int base = offA[q.li * C + c1];
-      for (int j = lane; j < cnt; j += 32) {
-        const uint4* ls = reinterpret_cast<const uint4*>(la + (size_t)(base + j) * kDescBytes);
-        uint32_t S = 0;
-#pragma unroll
-        for (int x = 0; x < kDescBytes / 16; ++x) {
-          const uint4 w = __ldg(ls + x);
-          S = __dp4a(rv[x].x, w.x, S);
-          S = __dp4a(rv[x].y, w.y, S);
-          S = __dp4a(rv[x].z, w.z, S);
-          S = __dp4a(rv[x].w, w.w, S);
-        }
-        const unsigned long long key = best_key((int32_t)S, __ldg(mapA + base + j));
-        if (key > best) {
-          sec = max(sec, (uint32_t)(best >> kIndexBits));
-          best = key;
-        } else if (key != best) {  // an equal key is the same left seen in another cell
-          sec = max(sec, S + 1u);
-        }
-      }
+// Pass B of the proposal on the tensor cores.  Every pass-B state (an accepted left l of pair
+// (i, j) and the right r it names) becomes one entry per cell c that r probes and in which
+// image i has lefts; an entry is scored against the lefts of (i, c) in the A layout, the same
+// block pass A used, so the entries of a state together cover exactly r's candidates (a left
+// probing several of r's cells is seen once per such cell with the same key).  Entries are
+// grouped by unit u = i * C + c; a row of the pass-B table is a group of up to GM entries of
+// one unit against that unit's left block.  The side kernel gathers the entries' right
+// descriptors itself (no copy of them is made).
+
+// Pass 1: entries per unit.
+__global__ void k_pbcount(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
+                          const uint8_t* __restrict__ cell, int probes, int probesR, int C,
+                          const int* __restrict__ cntA, const int* __restrict__ chosenRight,
+                          const int* __restrict__ chosenSorted, const int* __restrict__ counters,
+                          int* __restrict__ cntE) {
+  const int n = counters[kCntStates];  // 0 after a state overflow
+  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
+    const BPair q = pairs[chosenSorted[st]];
+    const int rRow = im[q.ri].rowOff + chosenRight[st];
+    for (int pr = 0; pr < probesR; ++pr) {
+      const int u = q.li * C + cell[(size_t)rRow * probes + pr];
+      if (cntA[u] > 0) atomicAdd(&cntE[u], 1);
     }
-    // warp: the largest key; the second is the largest of the other lanes' bests and every
-    // lane's own second
-    unsigned long long gb = best;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long t = __shfl_xor_sync(0xffffffffu, gb, o);
-      gb = t > gb ? t : gb;
+  }
+}
+
+// Entry offsets and row starts per unit (exclusive prefix sums; offE has nUnits + 1 entries).
+// One block.  A row table too small for the rows raises the overflow flag (the host grows
+// the pass-B buffers, and with them the table, and repeats the call); k_pbrows then writes
+// nothing.
+__global__ void __launch_bounds__(kScanThreads)
+k_pbscan(const int* __restrict__ cntE, int nUnits, int GM, long long capRows, int* __restrict__ offE,
+         int* __restrict__ rowStartE, int* __restrict__ counters) {
+  __shared__ long long sh[kScanThreads];
+  const long long total = block_scan(
+      nUnits, [&](int u) { return (long long)cntE[u]; }, [&](int u, long long x) { offE[u] = (int)x; }, sh);
+  __syncthreads();
+  const long long rows = block_scan(
+      nUnits, [&](int u) { return (long long)((cntE[u] + GM - 1) / GM); },
+      [&](int u, long long x) { rowStartE[u] = (int)x; }, sh);
+  if (threadIdx.x == 0) {
+    offE[nUnits] = (int)total;
+    const bool over = rows > capRows;
+    counters[kCntRowsPB] = over ? 0 : (int)rows;
+    if (over) counters[kCntOverflow] = 1;
+  }
+}
+
+// Pass 2: every entry's source row (the right's descriptor row in the image buffer) and
+// state.  Counts down cntE, which ends at zero for the next call.
+__global__ void k_pbscatter(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
+                            const uint8_t* __restrict__ cell, int probes, int probesR, int C,
+                            const int* __restrict__ cntA, const int* __restrict__ chosenRight,
+                            const int* __restrict__ chosenSorted, const int* __restrict__ counters,
+                            const int* __restrict__ offE, int* __restrict__ cntE, int* __restrict__ srcRowE,
+                            int* __restrict__ stateE) {
+  const int n = counters[kCntStates];  // the states k_pbcount counted: cntE ends at zero
+  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
+    const BPair q = pairs[chosenSorted[st]];
+    const int rRow = im[q.ri].rowOff + chosenRight[st];
+    for (int pr = 0; pr < probesR; ++pr) {
+      const int u = q.li * C + cell[(size_t)rRow * probes + pr];
+      if (cntA[u] == 0) continue;
+      const int pos = offE[u] + atomicSub(&cntE[u], 1) - 1;
+      srcRowE[pos] = rRow;
+      stateE[pos] = st;
     }
-    uint32_t gs = best != gb ? (uint32_t)(best >> kIndexBits) : sec;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) gs = max(gs, __shfl_xor_sync(0xffffffffu, gs, o));
-    if (lane == 0) decB[s] = decide(gb, gs, minScore, minRatio);
+  }
+}
+
+// Pass 3: the rows (one thread per unit).
+__global__ void k_pbrows(int nUnits, int GM, int BN, const int* __restrict__ cntA, const int* __restrict__ offA,
+                         const int* __restrict__ offE, const int* __restrict__ rowStartE,
+                         const int* __restrict__ counters, BatchRow* __restrict__ rows) {
+  if (counters[kCntOverflow]) return;
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nUnits; u += gridDim.x * blockDim.x) {
+    const int e0 = offE[u], ne = offE[u + 1] - e0;
+    int at = rowStartE[u];
+    for (int g = 0; g * GM < ne; ++g) {
+      BatchRow r;
+      r.aRow = e0 + g * GM;
+      r.validRows = min(GM, ne - g * GM);
+      r.bRow0 = offA[u];
+      r.nB = cntA[u];
+      r.nTiles = (cntA[u] + BN - 1) / BN;
+      r.pad = 0;
+      r.state0 = 0;
+      rows[at++] = r;
+    }
   }
 }
 
@@ -667,6 +725,19 @@ struct v3dm_batch {
   long long chosenSortedCap = 0;
   TcMaps mapsP;
   bool mapsPValid = false;
+  // proposal pass B (gathered entries)
+  int* dCntE = nullptr;             // per unit: entries (zero between calls)
+  int* dOffE = nullptr;             // per unit + 1: first entry
+  int* dRowStartE = nullptr;        // per unit: first pass-B row
+  long long unitTabCap = 0;
+  int* dSrcRowE = nullptr;          // per entry: descriptor row of its right in the image buffer
+  int* dStateE = nullptr;           // per entry: its pass-B state
+  long long entryCap = 0;
+  BatchRow* dRowsPB = nullptr;
+  long long rowsPBCap = 0;
+  CUtensorMap mapPB;                // B of pass B: the A layout, gather-configuration tiles
+  const uint8_t* mapPBla = nullptr;
+  long long mapPBrows = 0;
   const uint8_t* mapsPla = nullptr;
   const uint8_t* mapsPlb = nullptr;
   cudaGraphExec_t graphP = nullptr;
@@ -1070,22 +1141,54 @@ int prepare_proposal(v3dm_batch* b, int probesL, int probesR, int C) {
   V3DM_BTRY(ensure(&b->dMapA, &b->mapACap, laRows));
   V3DM_BTRY(ensure(&b->dLB, &b->lbCap, lbRows * kDescBytes));
   V3DM_BTRY(ensure(&b->dMapB, &b->mapBCap, lbRows));
-  if (b->nPairs > b->pairTabCap) {
+  if (tab > b->pairTabCap) {  // one entry per (cell, left image) unit
     long long c0 = 0, c1 = 0;
     bfree(b->dRowCnt);
     bfree(b->dRowStart);
     b->pairTabCap = 0;
-    V3DM_BTRY(ensure(&b->dRowCnt, &c0, b->nPairs));
-    V3DM_BTRY(ensure(&b->dRowStart, &c1, b->nPairs));
-    b->pairTabCap = b->nPairs;
+    V3DM_BTRY(ensure(&b->dRowCnt, &c0, tab));
+    V3DM_BTRY(ensure(&b->dRowStart, &c1, tab));
+    b->pairTabCap = tab;
   }
   V3DM_BTRY(ensure(&b->dRowsP, &b->rowsPCap, rowsBound));
+  // pass B: entries <= states x probesR, rows <= entries / GM + units
+  if (tab + 1 > b->unitTabCap) {
+    long long c0 = 0, c1 = 0, c2 = 0;
+    bfree(b->dCntE);
+    bfree(b->dOffE);
+    bfree(b->dRowStartE);
+    b->unitTabCap = 0;
+    V3DM_BTRY(ensure(&b->dCntE, &c0, tab + 1));
+    V3DM_BTRY(ensure(&b->dOffE, &c1, tab + 1));
+    V3DM_BTRY(ensure(&b->dRowStartE, &c2, tab + 1));
+    V3DM_BTRY(cudaMemsetAsync(b->dCntE, 0, (size_t)(tab + 1) * sizeof(int), b->stream));
+    b->unitTabCap = tab + 1;
+  }
+  const long long entries = std::max<long long>(b->capB * probesR, 1);
+  if (entries > 0x7fffffffLL) return V3DM_ERR_SIZE;
+  if (entries > b->entryCap) {
+    long long c0 = 0, c1 = 0;
+    bfree(b->dSrcRowE);
+    bfree(b->dStateE);
+    b->entryCap = 0;
+    V3DM_BTRY(ensure(&b->dSrcRowE, &c0, entries));
+    V3DM_BTRY(ensure(&b->dStateE, &c1, entries));
+    b->entryCap = entries;
+  }
+  V3DM_BTRY(ensure(&b->dRowsPB, &b->rowsPBCap, entries / tc_gather_rows() + tab + 1));
   if (b->dLA != la0 || b->dLB != lb0 || b->dRowsP != rp0 || !b->mapsPValid || b->laRows != laRows ||
       b->lbRows != lbRows || b->mapsP.cfg != tc_get_config(b->tc)) {
     V3DM_BTRY(tc_side_maps(b->tc, &b->mapsP, b->dLA, (int)laRows, b->dLB, (int)lbRows));
     b->mapsPValid = true;
     b->laRows = laRows;
     b->lbRows = lbRows;
+    if (b->graphP) cudaGraphExecDestroy(b->graphP);
+    b->graphP = nullptr;
+  }
+  if (b->mapPBla != b->dLA || b->mapPBrows != laRows) {
+    V3DM_BTRY(tc_gather_map(&b->mapPB, b->dLA, (int)laRows));
+    b->mapPBla = b->dLA;
+    b->mapPBrows = laRows;
     if (b->graphP) cudaGraphExecDestroy(b->graphP);
     b->graphP = nullptr;
   }
@@ -1101,7 +1204,6 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
   const int32_t Smin = host_smallest_passing_score(minScore);
   const int nI = b->nImages;
   const int imgGrid = std::max(1, std::min(nI, 1024));
-  const int pairGrid = std::max(1, (b->nPairs + 255) / 256);
   int launches = 0;
   V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
   // cells of every descriptor, layouts, row table
@@ -1115,14 +1217,14 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
                                                                b->dOffA,
                                                                b->dOffB, b->dImg, b->dLA, b->dMapA, b->dLB, b->dMapB);
   V3DM_BTRY(cudaGetLastError());
-  k_prowcount<<<pairGrid, 256, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, C, GM, b->dCntA, b->dCntB,
-                                               b->dRowCnt,
+  const int unitGrid = std::max(1, std::min((nI * C + 7) / 8, 4 * 148));
+  k_prowcount<<<unitGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, nI, C, GM, b->dCntA, b->dCntB, b->dRowCnt,
                                                reinterpret_cast<unsigned long long*>(b->dCounters + kCntScored));
   V3DM_BTRY(cudaGetLastError());
-  k_pscan_rows<<<1, kScanThreads, 0, b->stream>>>(b->dRowCnt, b->nPairs, b->rowsPCap, b->dRowStart, b->dCounters);
+  k_pscan_rows<<<1, kScanThreads, 0, b->stream>>>(b->dRowCnt, nI * C, b->rowsPCap, b->dRowStart, b->dCounters);
   V3DM_BTRY(cudaGetLastError());
-  k_prows<<<pairGrid, 256, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, C, GM, BN, b->dCntA, b->dCntB,
-                                           b->dOffA, b->dOffB, b->dRowStart, b->dCounters, b->dRowsP);
+  k_prows<<<unitGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, nI, C, GM, BN, b->dCntA, b->dCntB, b->dOffA,
+                                           b->dOffB, b->dRowStart, b->dCounters, b->dRowsP);
   V3DM_BTRY(cudaGetLastError());
   launches += 7;
   // pass A: each left against the rights under its probed cells
@@ -1162,8 +1264,8 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
   pa.aIsLeft = 1;
   pa.decision = b->dDecA;
   V3DM_BTRY(launch_post(pa, b->stream));
-  launches += 4;
-  // pass B: each accepted left's right against the lefts probing the right's best cell
+  launches += 3;
+  // pass B: each accepted left's right against the lefts that share a probed cell with it
   const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
   k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
   V3DM_BTRY(cudaGetLastError());
@@ -1173,13 +1275,61 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
                                                           b->dChosenRight, b->dChosenPair, b->dChosenSorted,
                                                           b->dCounters);
   V3DM_BTRY(cudaGetLastError());
-  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
-  k_ppassb<<<148 * 8, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA, b->dOffA,
-                                           b->dLA,
-                                           b->dMapA, b->dImg, b->dChosenRight, b->dChosenSorted, b->dCounters,
-                                           minScore, minRatio, b->dDecB);
+  const int GB = tc_gather_rows();
+  const int stateGrid = 4 * 148;
+  k_pbcount<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA,
+                                              b->dChosenRight, b->dChosenSorted, b->dCounters, b->dCntE);
   V3DM_BTRY(cudaGetLastError());
+  k_pbscan<<<1, kScanThreads, 0, b->stream>>>(b->dCntE, nI * C, GB, b->rowsPBCap, b->dOffE, b->dRowStartE,
+                                              b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  k_pbscatter<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA,
+                                                b->dChosenRight, b->dChosenSorted, b->dCounters, b->dOffE, b->dCntE,
+                                                b->dSrcRowE, b->dStateE);
+  V3DM_BTRY(cudaGetLastError());
+  k_pbrows<<<std::max(1, (nI * C + 255) / 256), 256, 0, b->stream>>>(nI * C, GB, tc_gather_cols(), b->dCntA, b->dOffA, b->dOffE,
+                                                                     b->dRowStartE, b->dCounters, b->dRowsPB);
+  V3DM_BTRY(cudaGetLastError());
+  SideArgs sb;
+  std::memset(&sb, 0, sizeof(sb));
+  sb.Smin = Smin;
+  sb.records = b->dRecords;
+  sb.segCount = b->dSegCount;
+  sb.segCap = b->segCap;
+  sb.nSeg = b->nSeg;
+  sb.err = b->dInfo + kInfoErr;
+  sb.aIsLeft = 0;
+  sb.best = b->dBest;
+  sb.sec = b->dSec;
+  sb.amap = b->dStateE;
+  sb.rows = b->dRowsPB;
+  sb.nRowsPtr = b->dCounters + kCntRowsPB;
+  sb.nRows = (int)std::min<long long>(b->rowsPBCap, 0x7fffffff);
+  sb.schedule = 2;
+  sb.aSrc = b->dImg;
+  sb.aSrcRow = b->dSrcRowE;
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
+  V3DM_BTRY(launch_side_gather(b->tc, b->mapPB, sb, b->stream));
   if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[3], b->stream));
+  PostArgs pb;
+  std::memset(&pb, 0, sizeof(pb));
+  pb.records = b->dRecords;
+  pb.bmap = b->dMapA;
+  pb.segCount = b->dSegCount;
+  pb.segCap = b->segCap;
+  pb.nSeg = b->nSeg;
+  pb.Smin = Smin;
+  pb.minScore = minScore;
+  pb.minRatio = minRatio;
+  pb.best = b->dBest;
+  pb.sec = b->dSec;
+  pb.err = b->dInfo + kInfoErr;
+  pb.nRows = (int)std::min<long long>(b->capB, 0x7fffffff);
+  pb.rowsPtr = b->dCounters + kCntStates;
+  pb.aIsLeft = 0;
+  pb.decision = b->dDecB;
+  V3DM_BTRY(launch_post(pb, b->stream));
+  launches += 7;  // four layout kernels, side pass, records, decisions
   const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
   k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
   V3DM_BTRY(cudaGetLastError());
@@ -1187,7 +1337,7 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
                                                              b->dChosenRight, b->dChosenPair, b->dBlockCount,
                                                              mutBlocks, b->dOut, b->dInfo);
   V3DM_BTRY(cudaGetLastError());
-  launches += 6;
+  launches += 5;  // pass-B states (count, scan, choose), mutual filter (two)
   V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             b->stream));
   b->lastLaunches = launches;
@@ -1201,7 +1351,7 @@ int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL
   const int C = proj_cells(proj);
   if (C < 1) return V3DM_ERR_NOT_ALLOCATED;
   if (probesL > C || probesR > C) return V3DM_ERR_ARG;
-  const int probes = probesL * 8 + probesR;  // graph key
+  const int probes = probesL * 16 + probesR;  // graph key
   if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
   b->pendingCheck = true;
   if (b->totalRows == 0 || b->nPairs == 0) {
@@ -1292,6 +1442,12 @@ void free_all(v3dm_batch* b) {
   bfree(b->dMapB);
   bfree(b->dRowCnt);
   bfree(b->dRowStart);
+  bfree(b->dCntE);
+  bfree(b->dOffE);
+  bfree(b->dRowStartE);
+  bfree(b->dSrcRowE);
+  bfree(b->dStateE);
+  bfree(b->dRowsPB);
   bfree(b->dRowsP);
   bfree(b->dChosenSorted);
   b->dCounters = nullptr;  // points into dInfo
@@ -1638,7 +1794,7 @@ int v3dm_batch_use_graph(v3dm_batch* b, int enable) {
 }
 
 int v3dm_batch_set_config(v3dm_batch* b, int cfg, int schedule) {
-  if (!b || schedule < 0 || schedule > 1) return V3DM_ERR_ARG;
+  if (!b || schedule < 0 || schedule > 2) return V3DM_ERR_ARG;
   BDeviceGuard g(b->device);
   cudaStreamSynchronize(b->stream);
   if (tc_set_config(b->tc, cfg) != cudaSuccess) return V3DM_ERR_ARG;

@@ -99,7 +99,11 @@ struct SideArgs {
   const BatchRow* rows;          // row table
   const int* nRowsPtr;           // device row count (null: use nRows)
   int nRows;
-  int schedule;                  // 0: rows interleaved over the CTAs, 1: contiguous row ranges
+  int schedule;                  // 0: rows interleaved over the CTAs, 1: contiguous row ranges,
+                                 // 2: chunks of consecutive rows interleaved over the CTAs
+  // gathered A (launch_side_gather): A row e of the row table is descriptor aSrcRow[e] of aSrc
+  const uint8_t* aSrc;
+  const int* aSrcRow;
 };
 // Chunk record: {A index (state), first B column, B count, first B row of the tile's image
 // block} then the chunk's 32 scores.
@@ -125,6 +129,13 @@ cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStrea
 cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStream_t st);
 // Sets the batched kernel's launch attributes for configuration cfg (before a stream capture).
 cudaError_t tc_prepare_batch(TcPlan* p, int cfg);
+// Batched pass whose A blocks are gathered row by row (SideArgs::aSrc / aSrcRow) instead of
+// loaded as tiles; B through the tensor map of tc_gather_map.  Its left groups have
+// tc_gather_rows() rows.
+int tc_gather_rows();
+int tc_gather_cols();
+cudaError_t tc_gather_map(CUtensorMap* m, const uint8_t* dB, int rowsB);
+cudaError_t launch_side_gather(TcPlan* p, const CUtensorMap& mB, const SideArgs& a, cudaStream_t st);
 
 // Decision and bookkeeping kernels around the side passes (v3dm_pair.cu).
 struct PostArgs {

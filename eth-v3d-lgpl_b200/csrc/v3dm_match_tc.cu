@@ -130,7 +130,9 @@ struct WorkCursor {
   int g, t, nTiles;
   long long left;
   bool fresh;  // first tile of a group
-  __device__ __forceinline__ WorkCursor(long long w0, long long w1, int nT) : nTiles(nT), left(w1 - w0), fresh(true) {
+  bool newA;   // the group's A block differs from the previous one (always, with fresh)
+  __device__ __forceinline__ WorkCursor(long long w0, long long w1, int nT)
+      : nTiles(nT), left(w1 - w0), fresh(true), newA(true) {
     g = (int)(w0 / nT);
     t = (int)(w0 - (long long)g * nT);
   }
@@ -143,7 +145,9 @@ struct WorkCursor {
       ++g;
       fresh = true;
     }
+    newA = fresh;
   }
+  __device__ __forceinline__ void prefetch_rows() const {}
 };
 
 __device__ __forceinline__ BatchRow load_row(const BatchRow* rows, int r) {
@@ -160,48 +164,98 @@ __device__ __forceinline__ BatchRow load_row(const BatchRow* rows, int r) {
   return b;
 }
 
+constexpr int kChunkRows = 32;  // schedule 2: rows per chunk
+constexpr int kRowAhead = 6;    // the producer prefetches the row entry this many rows ahead
+
 // Batched pass: walks the rows of a row table, every tile of a row in order.  Schedule 0
 // gives CTA b the rows b, b + grid, b + 2 grid, ...: the CTAs then work on neighbouring rows
 // (the same B image) at the same time, so the B tiles are read from L2.  Schedule 1 gives
-// each CTA one contiguous range of rows.  The next row's entry is loaded a row ahead.
+// each CTA one contiguous range of rows.  Schedule 2 deals out chunks of kChunkRows
+// consecutive rows the way schedule 0 deals out rows: consecutive rows that share their A
+// block (short rows of one left block against many right blocks) keep it in shared memory,
+// and the CTAs still work on neighbouring rows.  The next row's entry is loaded a row ahead;
+// the producer also prefetches entries kRowAhead rows ahead into L1.  newA says whether the
+// current row's A block differs from the previous row's (a row's A block is identified by
+// its first row aRow).
 struct BatchCursor {
   const BatchRow* rows;
-  int R, step, Rend, t;
+  int R, Rend, t, schedule;
   BatchRow cur, nxt;
-  bool fresh;
-  __device__ __forceinline__ BatchCursor(const BatchRow* rows_, int nRows, int schedule) : rows(rows_), t(0), fresh(true) {
+  bool fresh, newA;
+  __device__ __forceinline__ int step_from(int r) const {
+    if (schedule == 0) return r + (int)gridDim.x;
+    if (schedule == 1) return r + 1;
+    ++r;
+    return (r % kChunkRows) == 0 ? r + ((int)gridDim.x - 1) * kChunkRows : r;
+  }
+  __device__ __forceinline__ BatchCursor(const BatchRow* rows_, int nRows, int sch)
+      : rows(rows_), t(0), schedule(sch), fresh(true), newA(true) {
     cur = BatchRow{};
     nxt = BatchRow{};
     if (schedule == 0) {
       R = blockIdx.x;
-      step = gridDim.x;
       Rend = nRows;
-    } else {
+    } else if (schedule == 1) {
       R = (int)((long long)nRows * blockIdx.x / gridDim.x);
       Rend = (int)((long long)nRows * (blockIdx.x + 1) / gridDim.x);
-      step = 1;
+    } else {
+      R = blockIdx.x * kChunkRows;
+      Rend = nRows;
     }
     if (R < Rend) cur = load_row(rows, R);
-    if (R + step < Rend) nxt = load_row(rows, R + step);
+    const int R1 = step_from(R);
+    if (R1 < Rend) nxt = load_row(rows, R1);
   }
   __device__ __forceinline__ bool more() const { return R < Rend; }
   __device__ __forceinline__ void next() {
     fresh = false;
+    newA = false;
     if (++t == cur.nTiles) {
       t = 0;
-      R += step;
+      R = step_from(R);
       fresh = true;
+      newA = nxt.aRow != cur.aRow;
       cur = nxt;
-      if (R + step < Rend) nxt = load_row(rows, R + step);
+      const int R1 = step_from(R);
+      if (R1 < Rend) nxt = load_row(rows, R1);
     }
+  }
+  // The row entry kRowAhead rows ahead, into L1 (the other roles of the CTA read it later).
+  __device__ __forceinline__ void prefetch_rows() const {
+    int r = R;
+#pragma unroll
+    for (int i = 0; i < kRowAhead; ++i) r = step_from(r);
+    if (r < Rend) asm volatile("prefetch.global.L1 [%0];" ::"l"(rows + r));
   }
 };
 
+// Gathered A blocks (kGather): the producer warp copies each A row from a.aSrc (row
+// a.aSrcRow[entry]) into the 128-byte-swizzled shared layout the TMA would write (16-byte
+// chunk k of row r at r * 128 + ((k ^ (r & 7)) << 4)), rows past the block's valid count
+// zero-filled.  The copies are cp.async (generic proxy): each lane waits for its own copies,
+// fences them toward the async proxy the tensor core reads through, and lane 0 then arrives
+// on the slot's full barrier.  kGatherDepth newer gathers may stay in flight while an older
+// one is completed.
+constexpr int kGatherDepth = 3;
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t srcBytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // kBatch = false: one pair, the flattened (group, tile) range of this CTA (WorkCursor).
 // kBatch = true: rows of a.rows (BatchCursor); a row's state indices are state0 + row.
-template <class C, bool kBatch>
+// kGather = true (batched pass only): A blocks gathered row by row from a.aSrc (tmA unused).
+template <class C, bool kBatch, bool kGather = false>
 __global__ void __launch_bounds__(kThreads, 1)
 k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
+  static_assert(!kGather || kBatch, "gathered A blocks only in the batched pass");
   pdl_wait();
   pdl_launch_dependents();
   extern __shared__ uint8_t smemRaw[];
@@ -267,6 +321,108 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
   __syncthreads();
 
   if (warp == 0) {
+   if constexpr (kGather) {
+    // ---------------- producer, gathered A: the whole warp ----------------
+    if (!s.abort) {
+      int stage = 0, aBuf = C::kASlots - 1;
+      uint32_t phase = 0, aPhase = 1;
+      uint32_t armedPhase[C::kStages];
+      bool armed[C::kStages];
+      for (int i = 0; i < C::kStages; ++i) armed[i] = false;
+      int pend[kGatherDepth + 1] = {};  // slots whose gather still needs its arrive, oldest first
+      int nPend = 0;
+      int preRow = -1;                   // A block whose entry indices pre[] holds
+      int pre[C::GM / 32];
+#pragma unroll
+      for (int k = 0; k < C::GM / 32; ++k) pre[k] = -1;
+      auto arrive_oldest = [&]() {
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s.fullA[pend[0]]);
+        for (int i = 1; i <= kGatherDepth; ++i)
+          if (i < nPend) pend[i - 1] = pend[i];
+        --nPend;
+      };
+      auto arrive_all = [&]() {
+        cp_async_wait<0>();
+        while (nPend > 0) arrive_oldest();
+      };
+      // blocking wait by lane 0 (after handing over every pending gather, so that the MMA
+      // can drain what the wait depends on); the result is broadcast
+      auto wait_slot = [&](unsigned long long* bar, uint32_t par) -> bool {
+        if (mbar_try(bar, par)) return true;
+        arrive_all();
+        int okl = 1;
+        if (lane == 0) okl = mbar_wait(bar, par, &s.abort, a.err) ? 1 : 0;
+        return __shfl_sync(0xffffffffu, okl, 0) != 0;
+      };
+      for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
+        if (wc.fresh && lane == 0) wc.prefetch_rows();
+        if (wc.newA) {
+          if (++aBuf == C::kASlots) {
+            aBuf = 0;
+            aPhase ^= 1;
+          }
+          if (!wait_slot(&s.emptyA[aBuf], aPhase ^ 1)) break;
+          const int aRow = wc.cur.aRow, nValid = wc.cur.validRows;
+          int src[C::GM / 32];
+#pragma unroll
+          for (int k = 0; k < C::GM / 32; ++k) {
+            const int rr = lane + 32 * k;
+            src[k] = aRow == preRow ? pre[k] : (rr < nValid ? __ldg(a.aSrcRow + aRow + rr) : -1);
+          }
+          const uint32_t dst0 = smem_u32(s.a[aBuf]);
+#pragma unroll
+          for (int k = 0; k < C::GM / 32; ++k) {
+            const int rr = lane + 32 * k;
+            const uint8_t* g = a.aSrc + (src[k] >= 0 ? (size_t)src[k] * kDescBytes : (size_t)0);
+            const uint32_t nb = src[k] >= 0 ? 16u : 0u;  // 0: zero fill
+            const uint32_t d = dst0 + (uint32_t)rr * 128u;
+#pragma unroll
+            for (int ch = 0; ch < 8; ++ch) cp_async16(d + (uint32_t)((ch ^ (rr & 7)) << 4), g + 16 * ch, nb);
+          }
+          cp_async_commit();
+          // the next row's entry indices, read now and used at its turn (the loads overlap)
+          if (wc.nxt.aRow != aRow) {
+            preRow = wc.nxt.aRow;
+#pragma unroll
+            for (int k = 0; k < C::GM / 32; ++k) {
+              const int rr = lane + 32 * k;
+              pre[k] = rr < wc.nxt.validRows ? __ldg(a.aSrcRow + preRow + rr) : -1;
+            }
+          }
+          pend[nPend++] = aBuf;
+          if (nPend > kGatherDepth) {
+            cp_async_wait<kGatherDepth>();
+            arrive_oldest();
+          }
+        }
+        if (!wait_slot(&s.emptyB[stage], phase ^ 1)) break;
+        if (lane == 0) {
+          mbar_expect_tx(&s.fullB[stage], C::kBBytes);
+          int bRow = 0;
+          if constexpr (kBatch) bRow = wc.cur.bRow0 + wc.t * C::BN;
+          tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, bRow);
+        }
+        armed[stage] = true;
+        armedPhase[stage] = phase;
+        if (++stage == C::kStages) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      // every gather has landed (and is handed over) and every load lane 0 issued has landed
+      // before the CTA may exit
+      arrive_all();
+      if (lane == 0)
+        for (int i = 0; i < C::kStages; ++i)
+          if (armed[i]) {
+            long long t0c = clock64();
+            while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
+            }
+          }
+    }
+   } else {
     // ---------------- TMA producer ----------------
     if (lane == 0 && !s.abort) {
       int stage = 0, aBuf = C::kASlots - 1;
@@ -276,7 +432,8 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
       for (int i = 0; i < C::kStages; ++i) armed[i] = false;
       for (int i = 0; i < C::kASlots; ++i) armedA[i] = false;
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
-        if (wc.fresh) {
+        if (wc.fresh) wc.prefetch_rows();
+        if (wc.newA) {
           if (++aBuf == C::kASlots) {
             aBuf = 0;
             aPhase ^= 1;
@@ -317,6 +474,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           }
         }
     }
+   }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && !s.abort) {
@@ -325,7 +483,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
       uint32_t phase = 0, accPhase = 0, aPhase = 1;
       uint32_t aAddr = 0;
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
-        if (wc.fresh) {
+        if (wc.newA) {
           if (anyA) mma_commit(&s.emptyA[aBuf]);
           if (++aBuf == C::kASlots) {
             aBuf = 0;
@@ -381,6 +539,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     bool ok = !s.abort;
     bool rowValid = false;
     int orig = 0;
+    int aLocal = 0;  // batched pass: index of this lane's A row within its image
     int nB = a.nB;
     int bRow0 = 0;
     uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
@@ -393,7 +552,9 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         started = true;
         if constexpr (kBatch) {
           rowValid = rowInGroup < wc.cur.validRows;
-          orig = rowValid ? (int)(wc.cur.state0 + (a.amap ? __ldg(a.amap + wc.cur.aRow + rowInGroup) : rowInGroup)) : 0;
+          if (wc.newA)  // the A block's index map is read once per block, not once per row
+            aLocal = rowValid ? (a.amap ? __ldg(a.amap + wc.cur.aRow + rowInGroup) : rowInGroup) : 0;
+          orig = rowValid ? (int)(wc.cur.state0 + aLocal) : 0;
           nB = wc.cur.nB;
           bRow0 = wc.cur.bRow0;
         } else {
@@ -505,16 +666,17 @@ using Cfg4 = TcCfg<1, 256, 6>;   // 128 x 256 tiles, 2 accumulator stages, 6-dee
 using Cfg5 = TcCfg<1, 256, 4, 4>;   // as Cfg0 with 4 left-group buffers (rows of few tiles)
 using Cfg6 = TcCfg<1, 128, 6, 6>;   // 128 x 128 tiles, 6 left-group buffers
 
-template <class C, bool kBatch>
+template <class C, bool kBatch, bool kGather = false>
 cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles, const SideArgs& a, int grid,
                        cudaStream_t st, bool& attrSet) {
   const size_t smem = sizeof(Smem<C>) + 1024;
   if (!attrSet) {
-    cudaError_t e = cudaFuncSetAttribute(k_side<C, kBatch>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_side<C, kBatch, kGather>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attrSet = true;
   }
-  return launch_pdl(k_side<C, kBatch>, dim3(grid), dim3(kThreads), smem, st, mA, mB, nTiles, a);
+  return launch_pdl(k_side<C, kBatch, kGather>, dim3(grid), dim3(kThreads), smem, st, mA, mB, nTiles, a);
 }
 
 constexpr int kNumCfg = 7;
@@ -530,6 +692,7 @@ struct TcPlan {
   int cfg = kDefaultCfg;
   bool attrSet[kNumCfg] = {};
   bool attrSetBatch[kNumCfg] = {};
+  bool attrSetGather = false;
 };
 
 cudaError_t tc_plan_create(TcPlan** p, int device) {
@@ -623,7 +786,7 @@ cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cud
     if (a.nRows <= 0) return cudaSuccess;
     grid = std::min(grid, a.nRows);
   }
-  if (grid * kEpiWarps > a.nSeg || a.schedule < 0 || a.schedule > 1) return cudaErrorInvalidValue;
+  if (grid * kEpiWarps > a.nSeg || a.schedule < 0 || a.schedule > 2) return cudaErrorInvalidValue;
   switch (c) {
     case 0: return launch_cfg<Cfg0, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[0]);
     case 1: return launch_cfg<Cfg1, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[1]);
@@ -633,6 +796,29 @@ cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cud
     case 5: return launch_cfg<Cfg5, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[5]);
     default: return launch_cfg<Cfg6, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[6]);
   }
+}
+
+// Gathered-A batched pass: one fixed configuration (128 x 128 tiles, six A slots, so that
+// several gathers are in flight while short rows are scored).
+using CfgG = Cfg6;
+
+int tc_gather_rows() { return CfgG::GM; }
+int tc_gather_cols() { return CfgG::BN; }
+
+cudaError_t tc_gather_map(CUtensorMap* m, const uint8_t* dB, int rowsB) {
+  if (rowsB <= 0) return cudaErrorInvalidValue;
+  return encode_rows(m, dB, rowsB, CfgG::BN) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_side_gather(TcPlan* p, const CUtensorMap& mB, const SideArgs& a, cudaStream_t st) {
+  int grid = p->numSMs;
+  if (!a.nRowsPtr) {
+    if (a.nRows <= 0) return cudaSuccess;
+    grid = std::min(grid, a.nRows);
+  }
+  if (grid * kEpiWarps > a.nSeg || a.schedule < 0 || a.schedule > 2 || !a.aSrc || !a.aSrcRow)
+    return cudaErrorInvalidValue;
+  return launch_cfg<CfgG, true, true>(mB, mB, 0, a, grid, st, p->attrSetGather);
 }
 
 }  // namespace v3dm

@@ -544,8 +544,8 @@ class BatchMatching:
 
 
 PROJ_PARAMS = 10336
-PROJ_MAX_CELLS = 64
-PROJ_MAX_PROBES = 4
+PROJ_MAX_CELLS = 256
+PROJ_MAX_PROBES = 8
 PROJ_MAX_BATCH = 4096
 
 

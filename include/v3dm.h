@@ -216,7 +216,9 @@ V3DM_API int v3dm_batch_stream(v3dm_batch* b, void** stream);
 V3DM_API int v3dm_batch_use_graph(v3dm_batch* b, int enable);
 /* Tile configuration (as v3dm_matcher_set_config) and row schedule: 0 = rows interleaved over
  * the persistent CTAs (neighbouring CTAs share the right image in L2), 1 = contiguous row
- * ranges per CTA. */
+ * ranges per CTA, 2 = chunks of 32 consecutive rows interleaved over the CTAs (consecutive rows
+ * that share their left block keep it on chip; meant for the proposal matcher's short rows).
+ * The autotune below tries schedules 0 and 1 of the exhaustive matcher. */
 V3DM_API int v3dm_batch_set_config(v3dm_batch* b, int cfg, int schedule);
 V3DM_API int v3dm_batch_get_config(v3dm_batch* b, int* cfg, int* schedule);
 /* Times every (configuration, schedule) on the current batch (reps calls each) and keeps the
@@ -253,12 +255,13 @@ V3DM_API int v3dm_batch_proposal_scored(v3dm_batch* b, long long* scored, long l
  * (128 -> 64 -> 32, x = u / 512, BF16 weights, FP32 accumulation, FP32 master copies) trained
  * on the GPU with a symmetric InfoNCE loss on matched descriptor pairs, and C cells (unit
  * centroids) in its output space.  The proposal matcher (v3dm_batch_match_proposal) scores a
- * left descriptor exactly, in uint8, against the right descriptors whose best cell is among
- * the left's 'probes' best cells; exhaustive matching stays the reference result.
+ * left descriptor exactly, in uint8, against the right descriptors that share a cell with it:
+ * one of the left's probesLeft best cells among the right's probesRight best cells;
+ * exhaustive matching stays the reference result.
  * Parameter layout (V3DM_PROJ_PARAMS floats): W1[64][128], b1[64], W2[32][64], b2[32]. */
 #define V3DM_PROJ_PARAMS 10336
-#define V3DM_PROJ_MAX_CELLS 64
-#define V3DM_PROJ_MAX_PROBES 4
+#define V3DM_PROJ_MAX_CELLS 256
+#define V3DM_PROJ_MAX_PROBES 8
 #define V3DM_PROJ_MAX_BATCH 4096
 
 /* Creates the network with seeded He-uniform weights and zero biases. */

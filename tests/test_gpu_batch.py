@@ -101,7 +101,7 @@ def test_every_config_and_schedule(v3dm_mod, small_set):
     ref = None
     n_cfg = v3dm_mod.SIFTMatching().num_configs()
     for cfg in range(n_cfg):
-        for sch in (0, 1):
+        for sch in (0, 1, 2):
             b.set_config(cfg, sch)
             got = b.match(0.7, 0.8)
             if ref is None:

@@ -71,17 +71,20 @@ def _net_with_cells(v3dm_mod, desc, n_cells, seed=3):
     return net
 
 
-@pytest.mark.parametrize("probes,probes_right,ms,mr", [(1, 1, 0.7, 0.8), (2, 1, 0.7, 0.8), (3, 1, 0.6, 0.9),
-                                                        (2, 1, 0.7, -1.0), (2, 2, 0.7, 0.8), (3, 2, 0.6, 0.9),
-                                                        (1, 3, 0.7, 0.8)])
-def test_proposal_equals_masked_reference(v3dm_mod, small, probes, probes_right, ms, mr):
+@pytest.mark.parametrize("probes,probes_right,ms,mr,n_cells,schedule",
+                         [(1, 1, 0.7, 0.8, 6, 0), (2, 1, 0.7, 0.8, 6, 0), (3, 1, 0.6, 0.9, 6, 0),
+                          (2, 1, 0.7, -1.0, 6, 0), (2, 2, 0.7, 0.8, 6, 0), (3, 2, 0.6, 0.9, 6, 0),
+                          (1, 3, 0.7, 0.8, 6, 0), (2, 2, 0.7, 0.8, 6, 2), (3, 2, 0.6, 0.9, 6, 1),
+                          (5, 6, 0.7, 0.8, 40, 2), (8, 8, 0.7, 0.8, 256, 2)])
+def test_proposal_equals_masked_reference(v3dm_mod, small, probes, probes_right, ms, mr, n_cells, schedule):
     """Candidates: a left probing one of the cells a right probes (symmetric probing scores a
-    pair once per shared cell; the result must not depend on it)."""
+    pair once per shared cell; the result must not depend on it), for every row schedule."""
     desc, counts, offs = small
-    net = _net_with_cells(v3dm_mod, desc, 6)
+    net = _net_with_cells(v3dm_mod, desc, n_cells)
     b = v3dm_mod.BatchMatching()
     b.set_images(desc, counts)
     b.set_pairs(None)
+    b.set_config(b.config()[0], schedule)
     per = b.split_pairs(b.match_proposal(net, probes, ms, mr, probes_right=probes_right))
     cells = net.assign(desc, max(probes, probes_right))
     pairs = synth.all_pairs(len(counts))
