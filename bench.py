@@ -52,10 +52,11 @@ def parse():
     ap.add_argument("--tile-config", type=int, default=-1, help="fused-kernel tile configuration (-1: autotune)")
     ap.add_argument("--images", type=int, default=200, help="batch workload: number of images")
     ap.add_argument("--cache-dir", default="", help="voctree workload: keep the generated tree and queries here")
-    ap.add_argument("--cells", type=int, default=16, help="proposal workload: cells of the projection")
+    ap.add_argument("--cells", type=int, default=128, help="proposal workload: cells of the projection")
     ap.add_argument("--probes", type=int, default=4, help="proposal workload: probed cells per left")
-    ap.add_argument("--probes-right", type=int, default=1, help="proposal workload: cells each right is listed under")
-    ap.add_argument("--proposal-config", type=int, default=5, help="proposal workload: tile configuration")
+    ap.add_argument("--probes-right", type=int, default=4, help="proposal workload: cells each right is listed under")
+    ap.add_argument("--proposal-config", type=int, default=0, help="proposal workload: tile configuration")
+    ap.add_argument("--proposal-schedule", type=int, default=2, help="proposal workload: row schedule")
     ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     return ap.parse_args()
@@ -628,7 +629,7 @@ def run_proposal(args, ws, rank, local):
     exh_cfg = b.config()
     ms_exh, _ = timed(lambda: b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
     exh = b.match(MIN_SCORE, MIN_RATIO)
-    b.set_config(args.proposal_config, 0)
+    b.set_config(args.proposal_config, args.proposal_schedule)
     clocks = Clocks(local)
     ms_prop, launches = timed(lambda: b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right))
     clk = clocks.stop()
@@ -687,7 +688,8 @@ def run_proposal(args, ws, rank, local):
         "config": {"workload": "200 test images x 8000 uint8 SIFT-like features, 15% shared tracks, all 19,900 pairs, "
                                "minScore 0.7, ratio 0.8; projection 128-64-32 trained on 100 held-out images",
                    "cells": args.cells, "probes": args.probes, "probes_right": args.probes_right,
-                   "tile_config": args.proposal_config, "exhaustive_tile_config": list(exh_cfg),
+                   "tile_config": args.proposal_config, "row_schedule": args.proposal_schedule,
+                   "exhaustive_tile_config": list(exh_cfg),
                    "train_steps": args.train_steps,
                    "temperature": args.temperature, "train_pairs": int(anchors.shape[0]),
                    "l2": "inputs larger than L2 (205 MB of descriptors)"},

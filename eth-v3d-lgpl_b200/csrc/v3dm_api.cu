@@ -618,6 +618,7 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
+  if (host_candidate_threshold(minScore, minRatio, gated, &sa.Tsec) != V3DM_OK) sa.Tsec = 0;
   sa.records = h->dRecords;
   sa.segCount = h->dSegCount;
   sa.segCap = h->segCap;

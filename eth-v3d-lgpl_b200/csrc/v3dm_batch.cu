@@ -911,6 +911,7 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
+  if (host_candidate_threshold(minScore, minRatio, false, &sa.Tsec) != V3DM_OK) sa.Tsec = 0;
   sa.records = b->dRecords;
   sa.segCount = b->dSegCount;
   sa.segCap = b->segCap;
@@ -1231,6 +1232,7 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
+  if (host_candidate_threshold(minScore, minRatio, false, &sa.Tsec) != V3DM_OK) sa.Tsec = 0;
   sa.records = b->dRecords;
   sa.segCount = b->dSegCount;
   sa.segCap = b->segCap;
@@ -1293,6 +1295,7 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
   SideArgs sb;
   std::memset(&sb, 0, sizeof(sb));
   sb.Smin = Smin;
+  if (host_candidate_threshold(minScore, minRatio, false, &sb.Tsec) != V3DM_OK) sb.Tsec = 0;
   sb.records = b->dRecords;
   sb.segCount = b->dSegCount;
   sb.segCap = b->segCap;

@@ -82,6 +82,7 @@ struct SideArgs {
   int nA;                        // A rows (upper bound when nAptr is set)
   int nB;                        // B rows
   int32_t Smin;                  // smallest score that can pass the min-score test
+  int32_t Tsec;                  // second scores below this decide like none (0: keep every bound)
   const int* amap;               // single pair: A row -> index on its side (null: identity);
                                  // batched pass: absolute A row -> index within its image
                                  // (null: the row's place in its group)

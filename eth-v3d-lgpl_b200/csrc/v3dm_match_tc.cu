@@ -543,8 +543,9 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     int nB = a.nB;
     int bRow0 = 0;
     uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
+    // a bound below Tsec cannot change the decision: no atomic for it
     auto flush = [&]() {
-      if (rowValid && lw != 0) atomicMax(&a.sec[orig], lw);
+      if (rowValid && lw > (uint32_t)a.Tsec) atomicMax(&a.sec[orig], lw);
     };
     for (Cursor wc = make_cursor(); wc.more() && ok; wc.next()) {
       if (wc.fresh) {

@@ -247,7 +247,8 @@ V3DM_API int v3dm_batch_match_proposal(v3dm_batch* b, v3dm_projection* proj, int
                                        long long* nOut);
 V3DM_API int v3dm_batch_match_proposal_device(v3dm_batch* b, v3dm_projection* proj, int probesLeft,
                                               int probesRight, float minScore, float minRatio, int32_t* d_count);
-/* (left, right) pairs the last proposal call scored, and the exhaustive count sum(nL * nR). */
+/* (left, right) scores pass A of the last proposal call computed (a pair that shares several
+ * probed cells is scored once per shared cell), and the exhaustive count sum(nL * nR). */
 V3DM_API int v3dm_batch_proposal_scored(v3dm_batch* b, long long* scored, long long* exhaustive);
 
 /* ---- learned candidate proposal ----------------------------------------------------- */
