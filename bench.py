@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--probes-right", type=int, default=4, help="proposal workload: cells each right is listed under")
     ap.add_argument("--proposal-config", type=int, default=0, help="proposal workload: tile configuration")
     ap.add_argument("--proposal-schedule", type=int, default=2, help="proposal workload: row schedule")
+    ap.add_argument("--prop-images", type=int, default=200, help="proposal workload: test images (8000 features)")
+    ap.add_argument("--prop-train-images", type=int, default=100, help="proposal workload: held-out training images")
     ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     return ap.parse_args()
@@ -589,14 +591,15 @@ def run_proposal(args, ws, rank, local):
     from v3dm import proposal, synth
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    tr_desc, tr_counts, tr_offs = synth.images(args.seed + 40, n_images=100, n_min=8000, n_max=8000)
-    te_desc, te_counts, te_offs, te_track = synth.images(args.seed + 41, n_images=200, n_min=8000, n_max=8000,
+    n_tr, n_te = args.prop_train_images, args.prop_images
+    tr_desc, tr_counts, tr_offs = synth.images(args.seed + 40, n_images=n_tr, n_min=8000, n_max=8000)
+    te_desc, te_counts, te_offs, te_track = synth.images(args.seed + 41, n_images=n_te, n_min=8000, n_max=8000,
                                                          tracks=True)
     b = v3dm.BatchMatching(local)
     b.set_images(tr_desc, tr_counts)
     b.set_pairs(None)
     t_tr = time.perf_counter()
-    anchors, positives = proposal.mine_pairs(tr_desc, tr_offs, synth.all_pairs(100), b.match(MIN_SCORE, MIN_RATIO))
+    anchors, positives = proposal.mine_pairs(tr_desc, tr_offs, synth.all_pairs(n_tr), b.match(MIN_SCORE, MIN_RATIO))
     net = v3dm.Projection(local, seed=args.seed)
     losses = proposal.train(net, anchors, positives, steps=args.train_steps, batch=2048,
                             temperature=args.temperature, lr=2e-3, device=local)
@@ -625,19 +628,24 @@ def run_proposal(args, ws, rank, local):
         assert b.wait() == v3dm.OK
         return max_over_ranks(ws, statistics.mean(x.elapsed_time(y) for x, y in ev), dev), n
 
-    b.autotune(MIN_SCORE, MIN_RATIO, 1)  # exhaustive at its fastest configuration
+    if args.tile_config < 0:
+        b.autotune(MIN_SCORE, MIN_RATIO, 1)  # exhaustive at its fastest configuration
+    else:
+        b.set_config(args.tile_config, 0)
     exh_cfg = b.config()
     ms_exh, _ = timed(lambda: b.match_device(MIN_SCORE, MIN_RATIO, d_cnt.data_ptr()))
     exh = b.match(MIN_SCORE, MIN_RATIO)
     b.set_config(args.proposal_config, args.proposal_schedule)
     clocks = Clocks(local)
+    torch.cuda.nvtx.range_push("proposal")  # profilers can select the proposal launches by this range
     ms_prop, launches = timed(lambda: b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right))
+    torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
     got = b.match_proposal(net, args.probes, MIN_SCORE, MIN_RATIO, probes_right=args.probes_right)
     rec, prec = proposal.recall(exh, got)
     # recall of the exhaustive matches that join two views of one track (the rest are chance
     # matches between unrelated descriptors, which no candidate proposal can find)
-    pairs_all = synth.all_pairs(200)
+    pairs_all = synth.all_pairs(n_te)
     inl = synth.inlier_mask(exh, pairs_all, te_offs, te_track)
     rec_in, _ = proposal.recall(exh[inl], got)
     scored, exhaustive = b.proposal_scored()
@@ -681,18 +689,19 @@ def run_proposal(args, ws, rank, local):
     ops_prop = 2.0 * 128 * scored
     achieved = ops_prop / (k_ms * 1e-3) / 1e12
     line = {
-        "metric": "image pairs/s (learned proposal, all 19,900 pairs of 200 images x 8000 features)",
+        "metric": f"image pairs/s (learned proposal, all {n_pairs:,} pairs of {n_te} images x 8000 features)",
         "value": ws * n_pairs * 1000.0 / ms_prop, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_prop, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
-        "config": {"workload": "200 test images x 8000 uint8 SIFT-like features, 15% shared tracks, all 19,900 pairs, "
-                               "minScore 0.7, ratio 0.8; projection 128-64-32 trained on 100 held-out images",
+        "config": {"workload": f"{n_te} test images x 8000 uint8 SIFT-like features, 15% shared tracks, all {n_pairs:,} pairs, "
+                               f"minScore 0.7, ratio 0.8; projection 128-64-32 trained on {n_tr} held-out images",
                    "cells": args.cells, "probes": args.probes, "probes_right": args.probes_right,
                    "tile_config": args.proposal_config, "row_schedule": args.proposal_schedule,
                    "exhaustive_tile_config": list(exh_cfg),
                    "train_steps": args.train_steps,
                    "temperature": args.temperature, "train_pairs": int(anchors.shape[0]),
-                   "l2": "inputs larger than L2 (205 MB of descriptors)"},
+                   "l2": f"inputs {'larger' if te_desc.nbytes > 126e6 else 'smaller'} than L2 "
+                         f"({te_desc.nbytes / 1e6:.0f} MB of descriptors)"},
         "exhaustive": {"value": ws * n_pairs * 1000.0 / ms_exh, "unit": "pairs/s", "ms_per_step": ms_exh},
         "speedup_vs_exhaustive": ms_exh / ms_prop,
         "recall": rec, "precision": prec, "recall_inliers": rec_in,
