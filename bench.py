@@ -204,7 +204,11 @@ def stereo_config(args, where):
     return {"workload": "stereo pair 16384x16384 uint8 SIFT-like, putative + F-guided (2 px), "
                         "minScore 0.7, ratio 0.8", "n_left": N_SIDE, "n_right": N_SIDE, "seed": args.seed,
             "kernel": args.kernel if where == "gpu" else "oracle",
-            "l2": "flushed between steps (512 MiB write on the matcher stream, outside the step events)"}
+            "l2": "flushed between steps (512 MiB write on the matcher stream, outside the step events)",
+            "work_per_step": "one full 16384 x 16384 contraction (the putative call's); the guided call reuses its "
+                             "chunk records and applies the gates, as the reference's guided call masks the "
+                             "putative call's stored score matrix" if where == "gpu" else
+                             "putative and guided matching of the sample"}
 
 
 def run_stereo(args, ws, rank, local):

@@ -37,6 +37,13 @@ struct v3dm_matcher {
   unsigned int* dRSec = nullptr;         // per right: second value + 1
   unsigned long long* dCand = nullptr;   // candidate list (SIMT) / chunk-record entries (tcgen05): nSeg x segCap
   uint4* dRecords = nullptr;             // tcgen05 chunk records: nSeg x segCap x kRecordQuads
+  // Pass-A cache (tcgen05): the side kernel applies no gates, so the chunk records and per-left
+  // bounds of a pass A serve every later call on the same features with the same Smin (the
+  // guided calls after a putative call, as the reference masks its stored score matrix).
+  uint4* dRecordsA = nullptr;            // pass-A chunk records: nSeg x segCap x kRecordQuads
+  int32_t* dPassA = nullptr;             // nSeg record counts, then nMaxL + 1 per-left bounds
+  bool passAValid = false;
+  int32_t passASmin = 0, passATsec = 0;
   int* dSegCount = nullptr;              // nSeg counts
   long long segCap = 0;
   int nSeg = 0;
@@ -124,6 +131,9 @@ void free_buffers(v3dm_matcher* h) {
   dfree(h->dRSec);
   dfree(h->dCand);
   dfree(h->dSegCount);
+  dfree(h->dRecords);
+  dfree(h->dRecordsA);
+  dfree(h->dPassA);
   dfree(h->dScratch);
   dfree(h->dPairs);
   dfree(h->dInfo);
@@ -152,6 +162,7 @@ void free_buffers(v3dm_matcher* h) {
   h->hInfo = nullptr;
   h->allocated = false;
   h->tcBound = false;
+  h->passAValid = false;
   h->nL = h->nR = 0;
   h->nGates = 0;
   h->segCap = 0;
@@ -164,11 +175,15 @@ cudaError_t alloc_candidates(v3dm_matcher* h, int nSeg, long long segCap) {
   dfree(h->dCand);
   dfree(h->dSegCount);
   dfree(h->dRecords);
+  dfree(h->dRecordsA);
   h->segCap = 0;
   h->nSeg = 0;
+  h->passAValid = false;
   cudaError_t e = dalloc(&h->dCand, (size_t)nSeg * (size_t)segCap);
   if (e == cudaSuccess && h->kernel != V3DM_KERNEL_SIMT)
     e = dalloc(&h->dRecords, (size_t)nSeg * (size_t)segCap * kRecordQuads);
+  if (e == cudaSuccess && h->kernel != V3DM_KERNEL_SIMT)
+    e = dalloc(&h->dRecordsA, (size_t)nSeg * (size_t)segCap * kRecordQuads);
   if (e == cudaSuccess) e = dalloc(&h->dSegCount, (size_t)nSeg);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->dSegCount, 0, (size_t)nSeg * sizeof(int), h->stream);
   if (e != cudaSuccess) return e;
@@ -405,6 +420,7 @@ int v3dm_allocate(v3dm_matcher* h, int nMaxL, int nMaxR, int useGuided) {
   } else if (ok) {
     // tcgen05 path: one list segment per epilogue warp, holding that warp's unit bests.
     ok = alloc_candidates(h, tc_segments(h->tc), 64) == cudaSuccess &&
+         dalloc(&h->dPassA, (size_t)tc_segments(h->tc) + nMaxL + 1) == cudaSuccess &&
          dalloc(&h->dRc, rowsR * kDescBytes) == cudaSuccess && dalloc(&h->dLeftDec, (size_t)nMaxL + 1) == cudaSuccess &&
          dalloc(&h->dRightDec, (size_t)nMaxR + 1) == cudaSuccess &&
          dalloc(&h->dChosenFlag, (size_t)nMaxR + 1) == cudaSuccess &&
@@ -457,6 +473,7 @@ int set_features_u8(v3dm_matcher* h, bool left, int n, const uint8_t* desc, bool
   (left ? h->nL : h->nR) = n;
   (left ? h->floatL : h->floatR) = false;
   h->tcBound = false;
+  h->passAValid = false;
   return V3DM_OK;
 }
 
@@ -505,6 +522,7 @@ int stage_to_float(v3dm_matcher* h, bool left, int n) {
   (left ? h->nL : h->nR) = n;
   (left ? h->floatL : h->floatR) = true;
   h->tcBound = false;
+  h->passAValid = false;
   return V3DM_OK;
 }
 
@@ -547,6 +565,7 @@ int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
   (left ? h->nL : h->nR) = n;
   (left ? h->floatL : h->floatR) = false;
   h->tcBound = false;
+  h->passAValid = false;
   return V3DM_OK;
 }
 
@@ -650,19 +669,51 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   ra.minScore = minScore;
   ra.minRatio = minRatio;
   cudaEvent_t evA[2], evB[2];
-  // pass A: every left against every right
+  // pass A: every left against every right, into the pass-A cache (records and per-left
+  // bounds).  A guided call uses the cache instead when it holds this pass: same features,
+  // same Smin, and bounds kept down to a threshold no higher than this call's -- as the
+  // reference's guided calls mask the score matrix its putative call stored.  A putative
+  // call always computes the pass (and refreshes the cache).
+  int32_t* segCountA = h->dPassA;
+  unsigned int* boundA = reinterpret_cast<unsigned int*>(h->dPassA + h->nSeg);
+  int32_t tNeed = 0;
+  if (host_candidate_threshold(minScore, minRatio, gated, &tNeed) != V3DM_OK) tNeed = 0;
+  const bool reuseA = gated && h->passAValid && h->passASmin == Smin && h->passATsec <= tNeed;
   sa.nA = h->nL;
   sa.nB = h->nR;
   sa.aIsLeft = 1;
   sa.best = h->dLBest;
-  sa.sec = h->dLSec;
-  if (h->profile) {
-    int e = event_pair(h, 0, evA);
-    if (e != V3DM_OK) return e;
-    V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
+  if (!reuseA) {
+    // bounds below the smaller of the ungated and gated thresholds of these parameters are
+    // dropped, so the guided calls that follow can use this pass
+    int32_t tu = 0, tg = 0;
+    if (host_candidate_threshold(minScore, minRatio, false, &tu) != V3DM_OK) tu = 0;
+    if (host_candidate_threshold(minScore, minRatio, true, &tg) != V3DM_OK) tg = 0;
+    sa.Tsec = std::min(std::min(tu, tg), tNeed);
+    sa.sec = boundA;
+    sa.records = h->dRecordsA;
+    sa.segCount = segCountA;
+    V3DM_CUDA_TRY(cudaMemsetAsync(h->dPassA, 0, ((size_t)h->nSeg + h->nL) * sizeof(int32_t), h->stream));
+    if (h->profile) {
+      int e = event_pair(h, 0, evA);
+      if (e != V3DM_OK) return e;
+      V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
+    }
+    V3DM_CUDA_TRY(launch_side(h->tc, h->mapsA, sa, h->stream));
+    if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
+    h->passAValid = true;
+    h->passASmin = Smin;
+    h->passATsec = sa.Tsec;
+    h->lastLaunches += 1;
   }
-  V3DM_CUDA_TRY(launch_side(h->tc, h->mapsA, sa, h->stream));
-  if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
+  sa.sec = h->dLSec;
+  sa.records = h->dRecords;
+  sa.segCount = h->dSegCount;
+  sa.Tsec = tNeed;
+  pa.records = h->dRecordsA;
+  pa.segCount = segCountA;
+  pa.keepSegments = 1;
+  pa.secBound = boundA;
   pa.nRows = h->nL;
   pa.nB = h->nR;
   pa.aIsLeft = 1;
@@ -680,7 +731,11 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
   }
   V3DM_CUDA_TRY(launch_post(pa, h->stream));
   pa.chooseFlag = nullptr;
-  h->lastLaunches += 3;
+  pa.records = h->dRecords;
+  pa.segCount = h->dSegCount;
+  pa.keepSegments = 0;
+  pa.secBound = nullptr;
+  h->lastLaunches += 2;
   if (gated) {
     ra.descA = h->dL;
     ra.descB = h->dR;

@@ -147,9 +147,11 @@ struct PostArgs {
   unsigned int* sec;
   const uint4* records;          // chunk records of the side pass
   const int* bmap;               // absolute B row -> index within its image (null: the column)
-  int* segCount;                 // read, then cleared
+  int* segCount;                 // read, then cleared (kept when keepSegments is set)
   long long segCap;
   int nSeg;
+  int keepSegments;              // the records stay valid for a later call (pass-A cache)
+  const unsigned int* secBound;  // optional second bound per index, read-only (pass-A cache)
   int nB;
   int aIsLeft;
   int32_t Smin;

@@ -94,7 +94,7 @@ __device__ __forceinline__ void clear_segments(const PostArgs& a) {
   for (int seg = blockIdx.x * blockDim.x + threadIdx.x; seg < a.nSeg; seg += gridDim.x * blockDim.x) {
     const int cnt = a.segCount[seg];
     if ((long long)cnt > a.segCap) atomicMax(&info[kInfoMaxSeg], cnt);
-    if (cnt) a.segCount[seg] = 0;
+    if (cnt && !a.keepSegments) a.segCount[seg] = 0;
   }
 }
 
@@ -129,7 +129,7 @@ __global__ void k_decide(PostArgs a) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nRows; r += gridDim.x * blockDim.x) {
     const int idx = a.amap ? a.amap[r] : r;
     const unsigned long long b = a.best[idx];
-    const unsigned s = a.sec[idx];
+    const unsigned s = a.secBound ? max(a.sec[idx], a.secBound[idx]) : a.sec[idx];
     int32_t d = decide(b, s, a.minScore, a.minRatio);
     if (a.gated && b != 0 && s != 0 && d != decide(b, 0u, a.minScore, a.minRatio)) {
       // the bound straddles the decision: exact re-score (k_rescore clears the state)

@@ -149,6 +149,29 @@ def test_guided_homography_and_compounding(make_matcher, oracle_mod):
     np.testing.assert_array_equal(m.find_putative_matches(0.7, 0.8), oracle_mod.match(L, R, 0.7, 0.8))
 
 
+def test_guided_reuses_putative_pass(make_matcher, oracle_mod):
+    """A guided call after a putative call on the same features reuses that call's pass A
+    (records and bounds) when its minimum score is the same and its threshold allows it, and
+    recomputes otherwise; new features drop the stored pass.  Every result is the reference's."""
+    L, R, lp, rp, F, _ = synth.stereo(9, 2500, 2600)
+    m = make_matcher(2600, 2600, guided=True)
+    m.set_left_features(L)
+    m.set_right_features(R)
+    for ms, mr in [(0.7, 0.8), (0.7, 0.95), (0.7, 0.6), (0.75, 0.8), (0.6, -1.0)]:
+        np.testing.assert_array_equal(m.find_putative_matches(0.7, 0.8), oracle_mod.match(L, R, 0.7, 0.8))
+        got = m.run_guided_matching(F, 2.0, lp, rp, ms, mr)
+        exp = oracle_mod.match(L, R, ms, mr, gates=[("F", F, 2.0)], lpos=lp, rpos=rp)
+        np.testing.assert_array_equal(got, exp, err_msg=f"minScore {ms} ratio {mr}")
+    # new left features: the next guided call cannot use the stored pass
+    L2, R2, lp2, rp2, F2, _ = synth.stereo(10, 2400, 2600)
+    m.find_putative_matches(0.7, 0.8)
+    m.set_left_features(L2)
+    m.set_right_features(R2)
+    got = m.run_guided_matching(F2, 2.0, lp2, rp2, 0.7, 0.8)
+    np.testing.assert_array_equal(got, oracle_mod.match(L2, R2, 0.7, 0.8, gates=[("F", F2, 2.0)], lpos=lp2,
+                                                        rpos=rp2))
+
+
 def test_stereo_16384_guided(make_matcher, oracle_mod):
     """The 16384 x 16384 guided workload: putative and guided pairs bit-exact."""
     L, R, lp, rp, F, truth = synth.stereo(1)
