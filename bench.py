@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float"], default="stereo")
+    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest"],
+                    default="stereo")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
@@ -838,6 +839,112 @@ def run_float(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_ingest(args, ws, rank, local):
+    """Feature-file ingestion: 200 binary feature archives (the reference's .features format) of
+    8000 SIFT-like features each, read into device-resident u8 descriptors ready for the batched
+    matcher (v3dm_loader_load: host threads parse the files into pinned memory, one copy to the
+    device, u8 re-quantisation there).  The files are written once (to --cache-dir when given,
+    else a temporary directory) and read from the page cache."""
+    import tempfile
+
+    import torch
+
+    import v3dm
+    from v3dm import synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_img, n_feat = args.images, 8000
+    root = Path(args.cache_dir) / f"features_{args.seed}_{n_img}" if args.cache_dir else \
+        Path(tempfile.mkdtemp(prefix="v3dm_features_"))
+    root.mkdir(parents=True, exist_ok=True)
+    desc, counts, offs = synth.images(args.seed + 50, n_images=n_img, n_min=n_feat, n_max=n_feat)
+    rng = np.random.default_rng(args.seed)
+    paths = []
+    for i in range(n_img):
+        p = root / f"view{i:04d}.features"
+        if not p.exists():
+            synth.write_features(p, synth.feature_arrays(rng, int(counts[i]), desc[offs[i]:offs[i + 1]]))
+        paths.append(str(p))
+    file_bytes = sum(os.path.getsize(p) for p in paths)
+    ld = v3dm.Loader(local)
+    for p in paths:  # page cache
+        with open(p, "rb") as fh:
+            while fh.read(1 << 24):
+                pass
+    for _ in range(max(args.warmup, 3)):
+        kept = ld.load(paths)
+    total = int(kept.sum())
+    assert total == n_img * n_feat
+    # the loaded descriptors are the images' u8 descriptors
+    d_ptr, nt = ld.descriptors_device()
+    check = torch.empty(nt * 128, dtype=torch.uint8, device=dev)
+    src = torch.as_tensor(type("V", (), {"__cuda_array_interface__": {
+        "shape": (nt * 128,), "typestr": "|u1", "data": (d_ptr, False), "version": 3}})(), device=dev)
+    check.copy_(src)
+    assert np.array_equal(check.cpu().numpy().reshape(nt, 128), desc)
+    # each step: every file from the page cache to device-resident u8 descriptors; the events are
+    # recorded on the device around the (blocking) call
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    for a0, a1 in evs:
+        a0.record()
+        ld.load(paths)
+        a1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, statistics.mean(a.elapsed_time(c) for a, c in evs), dev)
+    # the device kernel on its own: u8 re-quantisation of the same number of floats
+    x = torch.rand(total * 128, device=dev)
+    q = torch.empty(total * 128, dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        v3dm.quantize_u8_device(x.data_ptr(), x.numel(), q.data_ptr(), 0)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(10)]
+    for a0, a1 in kev:
+        a0.record()
+        v3dm.quantize_u8_device(x.data_ptr(), x.numel(), q.data_ptr(), 0)
+        a1.record()
+    torch.cuda.synchronize()
+    k_ms = statistics.mean(a.elapsed_time(c) for a, c in kev)
+    ld.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    k_bytes = total * 128 * 5  # 4-byte float in, 1-byte code out
+    k_gbs = k_bytes / (k_ms * 1e-3) / 1e9
+    line = {
+        "metric": f"features/s ingested ({n_img} binary feature files x {n_feat} features to device u8)",
+        "value": ws * total * 1000.0 / ms, "unit": "features/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32->u8", "data": "synthetic (seeded generator), written in the reference's "
+                                                       "binary archive format",
+        "config": {"workload": f"{n_img} .features files x {n_feat} SIFT features (540 B each, "
+                               f"{file_bytes / 1e6:.0f} MB), page-cached, to device-resident u8",
+                   "files": n_img, "features_per_file": n_feat, "file_bytes": file_bytes,
+                   "host_threads": os.cpu_count(), "l2": "not applicable: each step streams the files once"},
+        "roofline": {"bound": "hbm", "achieved": k_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": k_gbs / peaks["hbm_gbs"], "traffic": None,
+                     "peak_src": f"{peaks['src']} copy bandwidth", "kernel_ms": k_ms, "bytes_per_launch": k_bytes,
+                     "kernel": "k_quantize_u8 (5 bytes per value)"},
+        "e2e": {"value": ws * total * 1000.0 / ms, "unit": "features/s", "h2d_bytes_per_step": total * 128 * 4,
+                "d2h_bytes_per_step": 0},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        if oracle.ref_features_available():
+            sample = paths[:20]
+            t0 = time.perf_counter()
+            nref = sum(oracle.ref_features_count(p) for p in sample)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": nref / dt, "unit": "features/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{len(sample)} of the {n_img} files read with the reference's "
+                                              "serializeDataFromFile, one thread (as the apps read them)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -854,6 +961,8 @@ def main():
             run_proposal(args, ws, rank, local)
         elif args.workload == "float":
             run_float(args, ws, rank, local)
+        elif args.workload == "ingest":
+            run_ingest(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -336,6 +336,7 @@ const char* v3dm_status_string(int s) {
     case V3DM_ERR_TIMEOUT: return "device wait timed out";
     case V3DM_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case V3DM_ERR_CANDIDATES: return "candidate list overflow (list grown; repeat the call)";
+    case V3DM_ERR_IO: return "feature file missing, not a binary feature archive, or truncated";
     default: return "unknown status";
   }
 }
@@ -1002,6 +1003,8 @@ extern "C" {
 
 int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, true, n, d, false); }
 int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, false, n, d, false); }
+int v3dm_set_left_u8_device(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, true, n, d, true); }
+int v3dm_set_right_u8_device(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, false, n, d, true); }
 int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, true, n, d); }
 int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, false, n, d); }
 int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, true, n, d); }

@@ -175,6 +175,8 @@ struct PostArgs {
   int choosePlanes;
 };
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s);
+// u8 re-quantisation of nValues floats (a multiple of 4), v3dm_features.cu.
+cudaError_t launch_quantize_u8(const float* d_x, long long nValues, uint8_t* d_out, cudaStream_t s);
 
 // ---- float descriptors: BF16 hi/lo scores (v3dm_match_f.cu) ------------------------------
 // Operand layouts: 6 planes of rowsCap x 128 bytes (64 BF16 values of a K slice per row).

@@ -67,8 +67,16 @@ def lib() -> C.CDLL:
         L.v3dm_allocate.argtypes = [vp, i32, i32, i32]
         L.v3dm_deallocate.argtypes = [vp]
         for n in ("v3dm_set_left_f32", "v3dm_set_right_f32", "v3dm_set_left_u8", "v3dm_set_right_u8",
-                  "v3dm_set_left_f32_bf16x3", "v3dm_set_right_f32_bf16x3"):
+                  "v3dm_set_left_f32_bf16x3", "v3dm_set_right_f32_bf16x3", "v3dm_set_left_u8_device",
+                  "v3dm_set_right_u8_device"):
             getattr(L, n).argtypes = [vp, i32, vp]
+        L.v3dm_features_read.argtypes = [C.c_char_p, i32, C.POINTER(i32)] + [vp] * 6
+        L.v3dm_quantize_u8_device.argtypes = [vp, C.c_longlong, vp, vp]
+        L.v3dm_loader_create.argtypes = [i32, C.POINTER(vp)]
+        L.v3dm_loader_destroy.argtypes = [vp]
+        L.v3dm_loader_load.argtypes = [vp, i32, C.POINTER(C.c_char_p), i32, i32, vp]
+        L.v3dm_loader_positions.argtypes = [vp, vp]
+        L.v3dm_loader_descriptors_device.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_longlong)]
         L.v3dm_scores_f32.argtypes = [vp, vp]
         L.v3dm_float_threshold.argtypes = [f32, f32, C.POINTER(C.c_float)]
         L.v3dm_putative.argtypes = [vp, f32, f32, vp, i32, C.POINTER(i32)]
@@ -220,6 +228,15 @@ class SIFTMatching:
         fn = lib().v3dm_set_right_u8 if kind == "u8" else lib().v3dm_set_right_f32
         _check(fn(self._h, d.shape[0], _ptr(d)), "setRightFeatures")
         self.n_right = d.shape[0]
+
+    def set_left_features_device(self, d_desc: int, n: int):
+        """u8 descriptors already in device memory (v3dm_set_left_u8_device)."""
+        _check(lib().v3dm_set_left_u8_device(self._h, n, C.c_void_p(d_desc)), "setLeftFeatures")
+        self.n_left = n
+
+    def set_right_features_device(self, d_desc: int, n: int):
+        _check(lib().v3dm_set_right_u8_device(self._h, n, C.c_void_p(d_desc)), "setRightFeatures")
+        self.n_right = n
 
     def set_left_features_bf16x3(self, desc: np.ndarray):
         """Float descriptors scored with the BF16 hi/lo split whatever their values."""
@@ -612,4 +629,79 @@ class Projection:
         d = np.ascontiguousarray(desc, np.uint8)
         out = np.empty((d.shape[0], probes), np.uint8)
         _check(lib().v3dm_projection_assign(self._h, _ptr(d), d.shape[0], probes, _ptr(out)), "projection_assign")
+        return out
+
+
+# ---- feature files ----------------------------------------------------------------------------
+
+LOAD_ROUND32 = 1
+ERR_IO = 11
+
+
+def features_read(path: str) -> dict:
+    """v3dm_features_read: the reference's binary feature archive (SerializableVector<SIFT_Feature>)
+    as arrays: ids (n), positions (n, 2), directions (n, 2), scales (n), magnitudes (n),
+    descriptors (n, 128) float32."""
+    n = C.c_int32(0)
+    p = str(path).encode()
+    _check(lib().v3dm_features_read(p, 0, C.byref(n), None, None, None, None, None, None), "features_read")
+    m = n.value
+    out = {"ids": np.empty(m, np.int32), "positions": np.empty((m, 2), np.float32),
+           "directions": np.empty((m, 2), np.float32), "scales": np.empty(m, np.float32),
+           "magnitudes": np.empty(m, np.float32), "descriptors": np.empty((m, 128), np.float32)}
+    _check(lib().v3dm_features_read(p, m, C.byref(n), *[_ptr(out[k]) for k in
+                                                         ("ids", "positions", "directions", "scales",
+                                                          "magnitudes", "descriptors")]), "features_read")
+    return out
+
+
+def quantize_u8_device(d_values: int, n_values: int, d_out: int, stream: int = 0) -> None:
+    """v3dm_quantize_u8_device on device pointers (n_values a multiple of 4)."""
+    _check(lib().v3dm_quantize_u8_device(C.c_void_p(d_values), C.c_longlong(n_values), C.c_void_p(d_out),
+                                         C.c_void_p(stream)), "quantize_u8_device")
+
+
+class Loader:
+    """Feature-file loader (v3dm_loader_*): many files at once, descriptors re-quantised to u8
+    on the device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_loader_create(device, C.byref(h)), "loader_create")
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            lib().v3dm_loader_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def load(self, paths, max_per_image: int = 0, flags: int = 0) -> np.ndarray:
+        """Reads the files; returns the kept feature count of each."""
+        arr = (C.c_char_p * len(paths))(*[str(p).encode() for p in paths])
+        counts = np.zeros(len(paths), np.int32)
+        _check(lib().v3dm_loader_load(self._h, len(paths), arr, max_per_image, flags, _ptr(counts)), "loader_load")
+        return counts
+
+    def descriptors_device(self):
+        """(device pointer of the u8 descriptors, their count)."""
+        p, n = C.c_void_p(), C.c_longlong(0)
+        _check(lib().v3dm_loader_descriptors_device(self._h, C.byref(p), C.byref(n)), "loader_descriptors_device")
+        return p.value or 0, n.value
+
+    def positions(self) -> np.ndarray:
+        _, n = self.descriptors_device()
+        out = np.empty((n, 2), np.float32)
+        _check(lib().v3dm_loader_positions(self._h, _ptr(out)), "loader_positions")
         return out

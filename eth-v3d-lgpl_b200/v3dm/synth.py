@@ -228,3 +228,33 @@ def voctree(seed: int = 3, bf: int = 10, depth: int = 6, n_train: int = 500_000,
     nodes = hkm_tree(rng, train, bf, depth, iters)
     queries = sift_like(rng, n_query)
     return nodes, queries
+
+
+def feature_arrays(rng: np.random.Generator, n: int, desc_u8: np.ndarray | None = None) -> dict:
+    """Arrays of n SIFT_Feature records: ids, positions (n, 2) in a 1600 x 1200 image,
+    directions, scales, magnitudes and float descriptors (u/512 of SIFT-like u8 when desc_u8 is
+    None)."""
+    if desc_u8 is None:
+        desc_u8 = sift_like(rng, n)
+    ang = rng.uniform(-np.pi, np.pi, n)
+    return {"ids": np.arange(n, dtype=np.int32),
+            "positions": np.stack([rng.uniform(0, 1600, n), rng.uniform(0, 1200, n)], 1).astype(np.float32),
+            "directions": np.stack([np.cos(ang), np.sin(ang)], 1).astype(np.float32),
+            "scales": rng.uniform(1.0, 12.0, n).astype(np.float32),
+            "magnitudes": rng.uniform(0.0, 1.0, n).astype(np.float32),
+            "descriptors": (desc_u8.astype(np.float32) / 512.0).astype(np.float32)}
+
+
+def write_features(path, f: dict) -> None:
+    """The reference's binary feature archive of f (the layout serializeDataToFile writes for a
+    SerializableVector<SIFT_Feature>): "V3DBIN", uint32 count, then per feature int32 id and 134
+    little-endian floats."""
+    n = f["ids"].shape[0]
+    rec = np.zeros(n, dtype=np.dtype([("id", "<i4"), ("six", "<f4", (6,)), ("desc", "<f4", (128,))]))
+    rec["id"] = f["ids"]
+    rec["six"] = np.concatenate([f["positions"], f["directions"], f["scales"][:, None], f["magnitudes"][:, None]], 1)
+    rec["desc"] = f["descriptors"]
+    with open(path, "wb") as fh:
+        fh.write(b"V3DBIN")
+        fh.write(np.uint32(n).astype("<u4").tobytes())
+        fh.write(rec.tobytes())

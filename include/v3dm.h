@@ -51,6 +51,8 @@ extern "C" {
 #define V3DM_ERR_NO_DEVICE 9       /* no sm_100 device (the library has no CPU path)   */
 #define V3DM_ERR_CANDIDATES 10     /* a device-only call overflowed the candidate list; the
                                       list has been grown, repeat the call             */
+#define V3DM_ERR_IO 11             /* a feature file cannot be opened, is not a binary
+                                      feature archive, or is shorter than its count    */
 
 V3DM_API const char* v3dm_status_string(int status);
 /* Detail of the last V3DM_ERR_CUDA raised by a matcher call on this thread (the CUDA error
@@ -102,6 +104,9 @@ V3DM_API int v3dm_float_threshold(float minScore, float minRatio, float* T);
 /* Native uint8 descriptors (u = 512 * the reference's float value). */
 V3DM_API int v3dm_set_left_u8(v3dm_matcher* h, int n, const uint8_t* desc);
 V3DM_API int v3dm_set_right_u8(v3dm_matcher* h, int n, const uint8_t* desc);
+/* The same with descriptors already in device memory (for instance a loader's, below). */
+V3DM_API int v3dm_set_left_u8_device(v3dm_matcher* h, int n, const uint8_t* d_desc);
+V3DM_API int v3dm_set_right_u8_device(v3dm_matcher* h, int n, const uint8_t* d_desc);
 
 /* SIFT_Matching::findPutativeMatches(matches, minScore, minRatio)
  * (v3d_cudamatching.h:45-46, .cu:522-552).  minRatio < 0 disables the ratio test.
@@ -312,6 +317,41 @@ V3DM_API int v3dm_voctree_quantize_u8(v3dm_voctree* t, int n, const uint8_t* key
 /* Device-resident variant: keys and ids in device memory, asynchronous on the tree's stream. */
 V3DM_API int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode);
 V3DM_API int v3dm_voctree_stream(v3dm_voctree* t, void** stream);
+
+/* ---- feature files ------------------------------------------------------------------ */
+/* serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) for the binary archive
+ * (v3d_serialization.h:983-1017; SIFT_Feature fields v3d_feature.h:12-47): "V3DBIN", uint32
+ * count, then per feature int32 id, position[2], direction[2], scale, magnitude, descriptor[128].
+ * *n = number of features.  With every array NULL only *n is set; otherwise cap must be >= *n
+ * (else V3DM_ERR_CAPACITY).  NULL arrays are skipped.  positions / directions: 2n floats,
+ * descriptors: 128n floats.  A text archive ("V3DTXT") gives V3DM_ERR_UNSUPPORTED, an unknown
+ * tag, a missing or a short file V3DM_ERR_IO. */
+V3DM_API int v3dm_features_read(const char* path, int cap, int32_t* n, int32_t* ids, float* positions,
+                                float* directions, float* scales, float* magnitudes, float* descriptors);
+/* u8 re-quantisation on the device: out = round(512 * x) (half to even) clamped to 0..255,
+ * NaN -> 0; the identity for descriptors of the form u/512.  nValues a multiple of 4.  No
+ * counterpart in the reference (its matcher takes the floats). */
+V3DM_API int v3dm_quantize_u8_device(const float* d_values, long long nValues, uint8_t* d_out, void* stream);
+
+/* Loader: the apps read one feature file per image and copy each pair's descriptors to the
+ * matcher (match_sequence.cpp:124-146, 183-186, 214-231).  A loader reads many files at once
+ * (host threads, one file each at a time), keeps the positions on the host, and copies all
+ * descriptors to the device in one transfer from pinned memory, re-quantised there to u8 for the
+ * u8 matchers (v3dm_batch_set_images_u8_device, v3dm_set_left_u8_device).  No counterpart in
+ * the reference. */
+typedef struct v3dm_loader v3dm_loader;
+#define V3DM_LOAD_ROUND32 1 /* keep a multiple of 32 features per file, as the apps' '& 0xffe0' */
+V3DM_API int v3dm_loader_create(int device, v3dm_loader** out);
+V3DM_API int v3dm_loader_destroy(v3dm_loader* ld);
+/* Reads nFiles files; counts[i] = features kept from file i (its first ones: at most
+ * maxPerImage when > 0, a multiple of 32 with V3DM_LOAD_ROUND32).  Returns when the device
+ * descriptors are ready; they stay until the next load. */
+V3DM_API int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* paths, int maxPerImage, int flags,
+                              int32_t* counts);
+/* Positions of the kept features (2 floats each), files in order. */
+V3DM_API int v3dm_loader_positions(v3dm_loader* ld, float* positions);
+/* Device u8 descriptors of the kept features (128 bytes each), files in order, and their count. */
+V3DM_API int v3dm_loader_descriptors_device(v3dm_loader* ld, const uint8_t** d_desc, long long* total);
 
 #ifdef __cplusplus
 }

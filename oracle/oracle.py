@@ -17,6 +17,7 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_VOCTREE = HERE / "_ref" / "libv3dref_voctree.so"
 REF_CUDA = HERE / "_ref" / "libv3dref_cuda.so"
+REF_FEATURES = HERE / "_ref" / "libv3dref_features.so"
 
 _lib = None
 
@@ -196,3 +197,53 @@ def ref_cuda_match_f32(L_f32: np.ndarray, R_f32: np.ndarray, min_score: float, m
     if res.returncode != 0:
         raise RuntimeError(f"reference matcher failed ({res.returncode}): {res.stderr[-2000:]}")
     return np.load(wd / "out.npy")
+
+
+# ---- the reference's feature-file serializer -------------------------------------------------
+
+FEATURE_FIELDS = ("ids", "positions", "directions", "scales", "magnitudes", "descriptors")
+
+
+def ref_features_available() -> bool:
+    return REF_FEATURES.exists()
+
+
+def _ref_features_lib():
+    L = C.CDLL(str(REF_FEATURES))
+    L.ref_features_write.argtypes = [C.c_char_p, C.c_int] + [C.c_void_p] * 6
+    L.ref_features_read.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int)] + [C.c_void_p] * 6
+    return L
+
+
+def ref_features_write(path: str, f: dict) -> None:
+    """serializeDataToFile(path, SerializableVector<SIFT_Feature>) of the reference (binary)."""
+    L = _ref_features_lib()
+    n = f["ids"].shape[0]
+    a = [np.ascontiguousarray(f[k], np.int32 if k == "ids" else np.float32) for k in FEATURE_FIELDS]
+    if L.ref_features_write(str(path).encode(), n, *[x.ctypes.data for x in a]) != 0:
+        raise OSError(f"reference writer failed on {path}")
+
+
+def ref_features_count(path: str) -> int:
+    """One full serializeDataFromFile of the reference; returns the feature count (the arrays are
+    not copied out)."""
+    L = _ref_features_lib()
+    n = C.c_int(0)
+    if L.ref_features_read(str(path).encode(), 0, C.byref(n), *([None] * 6)) != 0:
+        raise OSError(f"reference reader failed on {path}")
+    return n.value
+
+
+def ref_features_read(path: str) -> dict:
+    """serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) of the reference."""
+    L = _ref_features_lib()
+    n = C.c_int(0)
+    if L.ref_features_read(str(path).encode(), 0, C.byref(n), *([None] * 6)) != 0:
+        raise OSError(f"reference reader failed on {path}")
+    m = n.value
+    out = {"ids": np.empty(m, np.int32), "positions": np.empty((m, 2), np.float32),
+           "directions": np.empty((m, 2), np.float32), "scales": np.empty(m, np.float32),
+           "magnitudes": np.empty(m, np.float32), "descriptors": np.empty((m, 128), np.float32)}
+    if L.ref_features_read(str(path).encode(), m, C.byref(n), *[out[k].ctypes.data for k in FEATURE_FIELDS]) != 0:
+        raise OSError(f"reference reader failed on {path}")
+    return out

@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py voctree [outdir]   # CPU: V3D::VocabularyTree::getVisualWord
     python tests/golden/make_golden.py match [outdir]     # GPU: V3D_CUDA::SIFT_Matching
+    python tests/golden/make_golden.py features [outdir]  # CPU: V3D::serializeDataToFile / FromFile
 
 voctree: the reference's CPU vocabulary tree (V3D/Base/v3d_vocabularytree.h, built from the
 reference headers into oracle/_ref/libv3dref_voctree.so by `make -C oracle ref`), leaf-local
@@ -9,6 +10,11 @@ ids, for every tree shape the wrapper instantiates that is small enough to store
 match: the reference's CUDA matcher (V3D/CUDA/v3d_cudamatching.cu, built unmodified into
 oracle/_ref/libv3dref_cuda.so) on an sm_100 GPU: putative matching with and without the ratio
 test, guided F matching and compounding F + H gates, and a case with duplicated descriptors.
+
+features: a binary feature archive written by the reference's serializer (oracle/_ref/
+libv3dref_features.so, from V3D/Base/v3d_serialization.h and v3d_feature.h) and the arrays its
+reader returns for it.  The records hold edge values (negative ids, NaN, infinities, negative
+zero, denormals) so that the check is on the bytes.
 
 Inputs are SIFT-like uint8 descriptors (values u/512 handed to the reference as floats) from
 v3dm.synth, stored in the fixtures together with the outputs, so the fixtures stand alone.
@@ -99,12 +105,32 @@ def make_match(out: Path) -> None:
     print("wrote", out / "match_ref.npz")
 
 
+def make_features(out: Path) -> None:
+    if not oracle.ref_features_available():
+        raise SystemExit("oracle/_ref/libv3dref_features.so missing: run `make -C oracle ref` first")
+    rng = synth.rng_for(4242)
+    f = synth.feature_arrays(rng, 45)
+    f["ids"][:5] = [-1, -2147483648, 2147483647, 0, 7]
+    edge = np.array([np.nan, np.inf, -np.inf, -0.0, 1e-45, -3.5, 1e30, 0.5 / 512], np.float32)
+    f["descriptors"][0, :edge.size] = edge
+    f["positions"][1] = [np.nan, -0.0]
+    f["scales"][2] = np.inf
+    path = out / "features_ref.features"
+    oracle.ref_features_write(path, f)
+    back = oracle.ref_features_read(path)
+    for k in oracle.FEATURE_FIELDS:
+        assert back[k].tobytes() == np.ascontiguousarray(f[k]).tobytes(), k
+    np.savez_compressed(out / "features_ref.npz", **back)
+    print("wrote", path, "and", out / "features_ref.npz")
+
+
 def main(argv):
-    if len(argv) < 2 or argv[1] not in ("voctree", "match"):
+    makers = {"voctree": make_voctree, "match": make_match, "features": make_features}
+    if len(argv) < 2 or argv[1] not in makers:
         raise SystemExit(__doc__)
     out = Path(argv[2]) if len(argv) > 2 else HERE
     out.mkdir(parents=True, exist_ok=True)
-    (make_voctree if argv[1] == "voctree" else make_match)(out)
+    makers[argv[1]](out)
 
 
 if __name__ == "__main__":
