@@ -6,9 +6,10 @@ Default workload (one step): putative matching followed by F-guided matching (2 
 guided pair.  Metric: image pairs per second.  `value` times the steps with descriptors and
 positions resident in HBM (device-output C-ABI calls); `e2e` times the same step through the
 host C-ABI calls (pinned host buffers in, host pairs out, copies inside the timed region).
-Other workloads: --workload batch (all 19,900 pairs of 200 images in one batched call) and
---workload voctree (2M descriptors through a BF 10, depth 6 tree); the default line is the
-stereo one.
+Other workloads: --workload batch (all 19,900 pairs of 200 images in one batched call),
+--workload voctree (2M descriptors through a BF 10, depth 6 tree), --workload retrieval (the
+voctree app's image-retrieval scoring of a 4096-image sequence), and others listed under
+--workload; the default line is the stereo one.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -45,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest"],
+    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest", "retrieval"],
                     default="stereo")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,6 +63,7 @@ def parse():
     ap.add_argument("--prop-train-images", type=int, default=100, help="proposal workload: held-out training images")
     ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
+    ap.add_argument("--rt-images", type=int, default=4096, help="retrieval workload: images in the sequence")
     return ap.parse_args()
 
 
@@ -173,6 +175,12 @@ def cpu_stereo(L, R, lpos, rpos, F, n_left_sample: int, threads: int = 0):
 
 
 def run_reference_arm(args, ws, rank):
+    if args.workload == "retrieval":
+        return run_reference_retrieval(args, ws, rank)
+    return run_reference_stereo(args, ws, rank)
+
+
+def run_reference_stereo(args, ws, rank):
     """The reference's CPU path (the oracle port: the reference has no CPU matcher of its own),
     all host threads, on the same workload; each step is a bounded sample."""
     from oracle import oracle
@@ -945,6 +953,180 @@ def run_ingest(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+RT_LEAVES, RT_BEST, RT_PMATCH = 125_000, 20, 0.1  # VocabularyTree<3, 50, 128>; the app's defaults
+
+
+def retrieval_config(n_img, n_words):
+    return {"workload": f"retrieval scoring of a {n_img}-image sequence ({n_words} visual words, 2000..6000 per "
+                        f"image), {RT_LEAVES}-leaf vocabulary (VocabularyTree<3,50,128>), "
+                        f"POTENTIAL_VIEWS_COUNT {RT_BEST}, VISUAL_WORD_MATCH_PROPABILITY {RT_PMATCH}",
+            "images": n_img, "words": n_words, "leaves": RT_LEAVES, "n_best": RT_BEST, "p_match": RT_PMATCH,
+            "l2": "flushed between steps (512 MiB write)"}
+
+
+def retrieval_words(args, n_img):
+    from v3dm import synth
+    return synth.sequence_words(args.seed + 3, n_images=n_img, n_leaves=RT_LEAVES)
+
+
+def ref_retrieval_sample(off, w, stride, phase):
+    """One pass of the reference's loop (every image inserted, every stride-th image queried);
+    returns (estimated seconds of the whole loop, seconds run, queries)."""
+    from oracle import oracle
+    n_img = off.shape[0] - 1
+    t0 = time.perf_counter()
+    tq, ti, nq, _ = oracle.ref_retrieval_sampled(RT_LEAVES, off, w, RT_PMATCH, RT_BEST, stride, phase)
+    return ti + tq * n_img / max(nq, 1), time.perf_counter() - t0, nq
+
+
+def run_reference_retrieval(args, ws, rank):
+    """The reference's own LeafDocuments loop (match_using_voctree.cpp:176-222, compiled from the
+    reference into oracle/_ref), one thread as the app runs it.  A step is one pass with every
+    image inserted and every 512th image queried (phase varied per step); the whole loop's time
+    is the insertions plus the sampled queries scaled to all images."""
+    from oracle import oracle
+    if rank != 0:
+        return
+    if not oracle.ref_retrieval_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libv3dref_retrieval.so not built"}))
+        return
+    off, w = retrieval_words(args, args.rt_images)
+    stride = 512
+    small = off[:min(args.rt_images, 512) + 1]
+    for k in range(args.warmup):  # warm-up on the first 512 images
+        ref_retrieval_sample(small, w[:small[-1]], stride, 0)
+    est = []
+    for k in range(args.steps):
+        est.append(ref_retrieval_sample(off, w, stride, (k * 37) % stride)[0])
+    ms = 1000.0 * statistics.mean(est)
+    v = args.rt_images * 1000.0 / ms
+    sample = (f"each step one pass of the loop over all {args.rt_images} images (all inserted) with every "
+              f"{stride}th image queried; whole-loop time = insertions + sampled queries x {stride}")
+    line = {
+        "impl": "reference", "metric": "images/s retrieval-scored (voctree binomial scores + nBest selection)",
+        "value": v, "unit": "images/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded visual-word sequence)", "config": retrieval_config(args.rt_images, int(off[-1])),
+        "cpu_baseline": {"value": v, "unit": "images/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_retrieval(args, ws, rank, local):
+    """Retrieval scoring of one image sequence per GPU (independent replicas): the voctree app's
+    loop of computeBinomialScores + insertDocument over 4096 images with 2000..6000 visual words
+    each, in one call.  value: words, offsets and outputs in device memory
+    (v3dm_retrieval_binomial_device); e2e: host words from pinned memory in, host results out
+    (v3dm_retrieval_binomial)."""
+    import torch
+
+    import v3dm
+    from oracle import oracle
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_img = args.rt_images
+    off, w = retrieval_words(args, n_img)
+    r = v3dm.Retrieval(local)
+    stream = torch.cuda.ExternalStream(r.stream(), device=dev)
+    dw = torch.from_numpy(w).to(dev)
+    docs = torch.empty((n_img, RT_BEST), dtype=torch.int32, device=dev)
+    sc = torch.empty((n_img, RT_BEST), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device():
+        r.binomial_device(RT_LEAVES, off, dw.data_ptr(), RT_PMATCH, RT_BEST, docs.data_ptr(), sc.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        step_device()
+    r.wait()
+    # the whole result against the oracle (bit-exact docs and scores)
+    exp_docs, exp_sc = oracle.retrieval(RT_LEAVES, off, w, RT_PMATCH, RT_BEST)
+    assert np.array_equal(docs.cpu().numpy(), exp_docs)
+    assert np.array_equal(sc.cpu().numpy().view(np.uint32), exp_sc.view(np.uint32))
+    recall = float(np.mean([np.isin([i - 1, i - 2], exp_docs[i]).mean() for i in range(2, n_img)]))
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    for a0, a1 in evs:
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a0.record(stream)
+        step_device()
+        a1.record(stream)
+    r.wait()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in evs), dev)
+    # kernel times (a separate pass with per-kernel events)
+    r.profile(True)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        step_device()
+    r.wait()
+    k_ms, k_n = r.profile_read(1)
+    p_ms, p_n = r.profile_read(0)
+    r.profile(False)
+    k_ms /= max(k_n, 1)
+    p_ms /= max(p_n, 1)
+
+    # e2e: pinned host words in, host results out, through the host C-ABI call
+    wp = torch.from_numpy(w).pin_memory().numpy()
+    for _ in range(max(args.warmup, 3)):
+        r.binomial(RT_LEAVES, off, wp, RT_PMATCH, RT_BEST)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    for a0, a1 in ev2:
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a0.record(stream)
+        hd, hs = r.binomial(RT_LEAVES, off, wp, RT_PMATCH, RT_BEST)
+        a1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in ev2), dev)
+    assert np.array_equal(hd, exp_docs)
+    r.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    # algorithmic bytes of k_rt_score: per query image i, its words (4 B each), the first
+    # ceil(i / 32) 32-bit words of the bitmap row of each of its words, its offsets / logarithms
+    # (40 B per earlier image) and its outputs (8 B per kept image)
+    cnt = np.diff(off).astype(np.int64)
+    nw = (np.arange(n_img, dtype=np.int64) + 31) // 32
+    k_bytes = int(4 * cnt.sum() + 4 * (cnt * nw).sum() + 40 * (np.arange(n_img, dtype=np.int64)).sum()
+                  + 8 * n_img * RT_BEST)
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    line = {
+        "metric": "images/s retrieval-scored (voctree binomial scores + nBest selection)",
+        "value": ws * n_img * 1000.0 / ms, "unit": "images/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded visual-word sequence)", "config": retrieval_config(n_img, int(off[-1])),
+        "neighbour_recall": recall,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profiles("k_rt_score"),
+                     "peak_src": f"{peaks['src']} copy bandwidth", "kernel_ms": k_ms, "bytes_per_launch": k_bytes,
+                     "kernel": "k_rt_score (bitmap rows of every query word; the bitmap stays in L2)",
+                     "bitmap_kernel_ms": p_ms},
+        "e2e": {"value": ws * n_img * 1000.0 / ms_e2e, "unit": "images/s",
+                "h2d_bytes_per_step": int(w.nbytes + off.nbytes + 32 * n_img),
+                "d2h_bytes_per_step": int(n_img * RT_BEST * 8)},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1 and oracle.ref_retrieval_available():
+        est, ran, nq = ref_retrieval_sample(off, w, 256, 0)
+        line["cpu_baseline"] = {"value": n_img / est, "unit": "images/s", "cores": 1, "kind": "reference",
+                                "sample": f"the reference's loop over all {n_img} images (all inserted), {nq} "
+                                          f"queried (every 256th); whole-loop time = insertions + sampled "
+                                          f"queries x 256 ({ran:.1f} s run)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -963,6 +1145,8 @@ def main():
             run_float(args, ws, rank, local)
         elif args.workload == "ingest":
             run_ingest(args, ws, rank, local)
+        elif args.workload == "retrieval":
+            run_retrieval(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

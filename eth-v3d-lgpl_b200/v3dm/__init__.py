@@ -137,6 +137,15 @@ def lib() -> C.CDLL:
         L.v3dm_batch_match_proposal.argtypes = [vp, vp, i32, i32, f32, f32, vp, i64, i64p]
         L.v3dm_batch_match_proposal_device.argtypes = [vp, vp, i32, i32, f32, f32, vp]
         L.v3dm_batch_proposal_scored.argtypes = [vp, i64p, i64p]
+        L.v3dm_retrieval_create.argtypes = [C.POINTER(vp), i32]
+        L.v3dm_retrieval_destroy.argtypes = [vp]
+        L.v3dm_retrieval_binomial.argtypes = [vp, i32, i32, vp, vp, C.c_double, i32, vp, vp]
+        L.v3dm_retrieval_binomial_device.argtypes = [vp, i32, i32, vp, vp, C.c_double, i32, vp, vp]
+        L.v3dm_retrieval_wait.argtypes = [vp]
+        L.v3dm_retrieval_stream.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_retrieval_pairs.argtypes = [i32, i32, vp, i64, vp, i64p]
+        L.v3dm_retrieval_profile.argtypes = [vp, i32]
+        L.v3dm_retrieval_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
         _lib = L
     return _lib
 
@@ -705,3 +714,124 @@ class Loader:
         out = np.empty((n, 2), np.float32)
         _check(lib().v3dm_loader_positions(self._h, _ptr(out)), "loader_positions")
         return out
+
+
+RETRIEVAL_MAX_IMAGES = 32768
+RETRIEVAL_MAX_BEST = 1024
+
+
+def _offsets_words(offsets, words):
+    off = np.ascontiguousarray(offsets, np.int32)
+    w = np.ascontiguousarray(words, np.int32)
+    if off.ndim != 1 or off.shape[0] < 1 or (off.shape[0] > 1 and off[-1] > w.shape[0]):
+        raise ValueError("offsets must hold nImages + 1 entries, the last one <= len(words)")
+    return off, w
+
+
+class Retrieval:
+    """Retrieval scoring of a whole image sequence (v3dm_retrieval_*): the voctree app's image
+    loop over LeafDocuments::computeBinomialScores / insertDocument
+    (match_using_voctree.cpp:176-222, V3D/Base/v3d_voctree.h:143-278) in one call."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_retrieval_create(C.byref(h), device), "retrieval_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_retrieval_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def binomial(self, n_leaves: int, offsets, words, p_match: float = 0.1, n_best: int = 20):
+        """(best_docs, best_scores), nImages x n_best: row i = the min(n_best, i) best earlier
+        images of image i, best first, then -1 / 0."""
+        off, w = _offsets_words(offsets, words)
+        n = off.shape[0] - 1
+        docs = np.empty((n, n_best), np.int32)
+        sc = np.empty((n, n_best), np.float32)
+        _check(lib().v3dm_retrieval_binomial(self._h, n_leaves, n, _ptr(off), _ptr(w), float(p_match), n_best,
+                                             _ptr(docs), _ptr(sc)), "retrieval_binomial")
+        return docs, sc
+
+    def binomial_device(self, n_leaves: int, offsets, d_words: int, p_match: float, n_best: int, d_docs: int,
+                        d_scores: int) -> None:
+        off = np.ascontiguousarray(offsets, np.int32)
+        _check(lib().v3dm_retrieval_binomial_device(self._h, n_leaves, off.shape[0] - 1, _ptr(off),
+                                                    C.c_void_p(d_words), float(p_match), n_best,
+                                                    C.c_void_p(d_docs), C.c_void_p(d_scores)),
+               "retrieval_binomial_device")
+
+    def wait(self) -> None:
+        _check(lib().v3dm_retrieval_wait(self._h), "retrieval_wait")
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().v3dm_retrieval_profile(self._h, int(enable)), "retrieval_profile")
+
+    def profile_read(self, kernel: int):
+        """(milliseconds, launches) of kernel 0 (bitmap) or 1 (scores) since the last read."""
+        ms, n = C.c_double(0.0), C.c_int(0)
+        _check(lib().v3dm_retrieval_profile_read(self._h, kernel, C.byref(ms), C.byref(n)), "retrieval_profile_read")
+        return ms.value, n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().v3dm_retrieval_stream(self._h, C.byref(s)), "retrieval_stream")
+        return s.value or 0
+
+
+def retrieval_pairs(best_docs: np.ndarray) -> np.ndarray:
+    """The app's putativePairwiseMatches as (view1, view2) pairs, view1 the retrieved earlier
+    image, ordered by view1 then view2 (v3dm_retrieval_pairs): the pair table of
+    BatchMatching.set_pairs."""
+    d = np.ascontiguousarray(best_docs, np.int32)
+    n, k = (d.shape[0], d.shape[1]) if d.ndim == 2 else (0, 1)
+    cnt = C.c_longlong(0)
+    _check(lib().v3dm_retrieval_pairs(n, k, _ptr(d), 0, None, C.byref(cnt)), "retrieval_pairs")
+    out = np.empty((cnt.value, 2), np.int32)
+    _check(lib().v3dm_retrieval_pairs(n, k, _ptr(d), cnt.value, _ptr(out), C.byref(cnt)), "retrieval_pairs")
+    return out
+
+
+class LeafDocuments:
+    """V3D::LeafDocuments (v3d_voctree.h:105-289) for code written against its incremental
+    interface: insert_document(words) and compute_binomial_scores(p_match, words, n_best).
+    Each query runs the whole-sequence scoring of Retrieval on the inserted documents plus the
+    query and keeps the last row; the batched Retrieval.binomial is the fast path."""
+
+    def __init__(self, n_leaves: int, device: int = 0):
+        self.n_leaves = int(n_leaves)
+        self._docs: list[np.ndarray] = []
+        self._r = Retrieval(device)
+
+    def insert_document(self, visual_words) -> int:
+        """Returns the document id (0, 1, ... in insertion order)."""
+        w = np.ascontiguousarray(visual_words, np.int32)
+        if w.size and (w.min() < 0 or w.max() >= self.n_leaves):
+            raise V3DMError(ERR_ARG, "insertDocument")
+        self._docs.append(w)
+        return len(self._docs) - 1
+
+    def compute_binomial_scores(self, p_match: float, visual_words, n_best: int = -1):
+        """[(score, document id)] ascending, the n_best best (every document when n_best < 0)."""
+        nd = len(self._docs)
+        k = nd if n_best < 0 or n_best > nd else n_best
+        if nd == 0 or k == 0:
+            return []
+        parts = self._docs + [np.ascontiguousarray(visual_words, np.int32)]
+        off = np.zeros(nd + 2, np.int32)
+        off[1:] = np.cumsum([p.shape[0] for p in parts])
+        docs, sc = self._r.binomial(self.n_leaves, off, np.concatenate(parts), p_match, k)
+        return [(float(sc[nd, j]), int(docs[nd, j])) for j in range(k)]

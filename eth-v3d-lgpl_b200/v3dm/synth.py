@@ -8,7 +8,8 @@ The shapes and value distributions follow the five benchmark workloads of this p
                  random stereo rig (for guided matching);
 * ``images``     many images with uneven feature counts and shared feature tracks (batched
                  all-pairs matching);
-* ``voctree``    a hierarchical k-means vocabulary tree and query descriptors.
+* ``voctree``    a hierarchical k-means vocabulary tree and query descriptors;
+* ``sequence_words``  the visual words of an image sequence (retrieval scoring).
 
 Descriptor generator: i.i.d. Gamma(k=0.6, theta=1) components, L2-normalised, clamped at
 0.2, renormalised, scaled by 512, rounded and clamped to 0..255 (the SIFT normalisation of
@@ -258,3 +259,39 @@ def write_features(path, f: dict) -> None:
         fh.write(b"V3DBIN")
         fh.write(np.uint32(n).astype("<u4").tobytes())
         fh.write(rec.tobytes())
+
+
+def sequence_words(seed: int = 4, n_images: int = 2048, n_leaves: int = 125_000, n_min: int = 2000,
+                   n_max: int = 6000, window: int = 8, keep: float = 0.6, zipf: float = 0.5):
+    """Visual words of an image sequence: a scene of points, each with a word drawn from a Zipf
+    law over the leaves (popular leaves are shared by many unrelated points; exponent 0.5: the
+    most frequent of 125,000 leaves holds 0.14% of the words, about 180 times the mean); image i
+    sees the points of a window that slides by 1/window of its width per image, each with
+    probability 'keep', plus random background words.  Images within a few indices of each other share
+    words.  Returns (offsets, words) with offsets[n_images + 1], words int32 in 0..n_leaves-1."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(n_min, n_max + 1, n_images)
+    per_view = int(np.mean(counts) / keep * 0.7)  # points in a window
+    step = max(1, per_view // window)
+    n_points = step * (n_images - 1) + per_view
+    rank = np.arange(1, n_leaves + 1, dtype=np.float64) ** -zipf
+    cdf = np.cumsum(rank / rank.sum())
+    perm = rng.permutation(n_leaves).astype(np.int32)  # popular leaves spread over the tree
+
+    def zipf_words(n):
+        return perm[np.minimum(np.searchsorted(cdf, rng.random(n)), n_leaves - 1)]
+
+    point_word = zipf_words(n_points)
+    parts = []
+    for i in range(n_images):
+        seen = point_word[i * step:i * step + per_view]
+        seen = seen[rng.random(seen.shape[0]) < keep]
+        n = int(counts[i])
+        if seen.shape[0] >= n:
+            w = seen[rng.permutation(seen.shape[0])[:n]]
+        else:
+            w = np.concatenate([seen, zipf_words(n - seen.shape[0])])
+        parts.append(w[rng.permutation(n)].astype(np.int32))
+    offsets = np.zeros(n_images + 1, np.int32)
+    offsets[1:] = np.cumsum(counts)
+    return offsets, np.concatenate(parts) if parts else np.zeros(0, np.int32)

@@ -353,6 +353,49 @@ V3DM_API int v3dm_loader_positions(v3dm_loader* ld, float* positions);
 /* Device u8 descriptors of the kept features (128 bytes each), files in order, and their count. */
 V3DM_API int v3dm_loader_descriptors_device(v3dm_loader* ld, const uint8_t** d_desc, long long* total);
 
+/* ---- retrieval scoring (V3D::LeafDocuments, v3d_voctree.h:105-289) ------------------- */
+/* The image loop of match_using_voctree.cpp:176-222 over visual words: image i is scored
+ * against every earlier image with computeBinomialScores(pMatch, words of i, scores,
+ * nBest) (v3d_voctree.h:233-278) and then inserted (insertDocument, :143-163).  All images are
+ * scored in one call; results are bit-identical to that loop (scores as floats, ties of equal
+ * scores by image index).  Scores are finite while every image's p = nFeatures / nLeaves
+ * satisfies p + pMatch < 1 and no two empty images meet; outside that domain the reference
+ * computes infinities or NaN (its std::sort order is then unspecified: NaN scores rank last
+ * here, by image index). */
+typedef struct v3dm_retrieval v3dm_retrieval;
+#define V3DM_RETRIEVAL_MAX_IMAGES 32768
+#define V3DM_RETRIEVAL_MAX_BEST 1024
+V3DM_API int v3dm_retrieval_create(v3dm_retrieval** out, int device);
+V3DM_API int v3dm_retrieval_destroy(v3dm_retrieval* r);
+/* words: the leaf-local visual words (VocabularyTree::getVisualWord, v3d_voctree.h:56-58; the
+ * V3DM_LEAF_LOCAL ids of v3dm_voctree_quantize_*) of every image, images concatenated, image i
+ * at words[offsets[i] .. offsets[i + 1]) (host offsets, nImages + 1 entries, offsets[0] = 0).
+ * nLeaves = the tree's leaf count.  Outputs nImages x nBest: row i holds the min(nBest, i) best
+ * earlier images of image i, best first, and their scores, then -1 / 0.  A word outside
+ * 0..nLeaves-1 gives V3DM_ERR_ARG (it is skipped). */
+V3DM_API int v3dm_retrieval_binomial(v3dm_retrieval* r, int nLeaves, int nImages, const int32_t* offsets,
+                                     const int32_t* words, double pMatch, int nBest, int32_t* bestDocs,
+                                     float* bestScores);
+/* Device-resident variant: words and outputs in device memory, enqueued on the retrieval's
+ * stream; v3dm_retrieval_wait returns the call's status (V3DM_ERR_ARG for a word out of range). */
+V3DM_API int v3dm_retrieval_binomial_device(v3dm_retrieval* r, int nLeaves, int nImages, const int32_t* offsets,
+                                            const int32_t* d_words, double pMatch, int nBest, int32_t* d_bestDocs,
+                                            float* d_bestScores);
+V3DM_API int v3dm_retrieval_wait(v3dm_retrieval* r);
+V3DM_API int v3dm_retrieval_stream(v3dm_retrieval* r, void** stream);
+/* CUDA-event timing of the two kernels of each call (kernel 0 = the inverted-file bitmap with
+ * its clearing, 1 = counting, scores and selection); read returns the milliseconds and
+ * launches since the last read of that kernel. */
+V3DM_API int v3dm_retrieval_profile(v3dm_retrieval* r, int enable);
+V3DM_API int v3dm_retrieval_profile_read(v3dm_retrieval* r, int kernel, double* msTotal, int* launches);
+/* The app's putativePairwiseMatches (match_using_voctree.cpp:196-216) from the bestDocs table
+ * (host): (view1, view2) int32 pairs, view1 = the retrieved earlier image, view2 = the query,
+ * ordered by view1 then view2 -- the pair table v3dm_batch_set_pairs takes.  *nPairs = the
+ * count; with pairs NULL only the count; else the first 'cap' (V3DM_ERR_CAPACITY if more).
+ * Host code, no device. */
+V3DM_API int v3dm_retrieval_pairs(int nImages, int nBest, const int32_t* bestDocs, long long cap, int32_t* pairs,
+                                  long long* nPairs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@ LIB = HERE / "liboracle.so"
 REF_VOCTREE = HERE / "_ref" / "libv3dref_voctree.so"
 REF_CUDA = HERE / "_ref" / "libv3dref_cuda.so"
 REF_FEATURES = HERE / "_ref" / "libv3dref_features.so"
+REF_RETRIEVAL = HERE / "_ref" / "libv3dref_retrieval.so"
 
 _lib = None
 
@@ -48,6 +49,8 @@ def lib() -> C.CDLL:
         L.orc_ref_feature_count.argtypes = [i32, i32]
         L.orc_ref_feature_count.restype = i32
         L.orc_num_threads.restype = i32
+        L.orc_retrieval_binomial.argtypes = [i32, i32, vp, vp, C.c_double, i32, vp, vp, i32]
+        L.orc_retrieval_binomial.restype = i32
         _lib = L
     return _lib
 
@@ -118,6 +121,21 @@ def voctree(bf: int, depth: int, nodes: np.ndarray, keys: np.ndarray, global_ids
     if rc != 0:
         raise ValueError("oracle rejected the arguments")
     return out
+
+
+def retrieval(n_leaves: int, offsets: np.ndarray, words: np.ndarray, p_match: float, n_best: int,
+              threads: int = 0):
+    """The voctree app's image loop over LeafDocuments::computeBinomialScores (restated):
+    (best_docs, best_scores), nImages x n_best, -1 / 0 past the i-th entry of row i."""
+    off = np.ascontiguousarray(offsets, np.int32)
+    w = np.ascontiguousarray(words, np.int32)
+    n = off.shape[0] - 1
+    docs = np.empty((n, n_best), np.int32)
+    sc = np.empty((n, n_best), np.float32)
+    if lib().orc_retrieval_binomial(n_leaves, n, off.ctypes.data, w.ctypes.data, float(p_match), n_best,
+                                    docs.ctypes.data, sc.ctypes.data, threads) != 0:
+        raise ValueError("oracle rejected the arguments")
+    return docs, sc
 
 
 def ref_feature_count(n: int, n_max_rounded: int) -> int:
@@ -247,3 +265,43 @@ def ref_features_read(path: str) -> dict:
     if L.ref_features_read(str(path).encode(), m, C.byref(n), *[out[k].ctypes.data for k in FEATURE_FIELDS]) != 0:
         raise OSError(f"reference reader failed on {path}")
     return out
+
+
+# ---- the reference's inverted files ---------------------------------------------------------
+
+def ref_retrieval_available() -> bool:
+    return REF_RETRIEVAL.exists()
+
+
+def ref_retrieval(n_leaves: int, offsets: np.ndarray, words: np.ndarray, p_match: float, n_best: int):
+    """The image loop of match_using_voctree.cpp:176-222 on the reference's LeafDocuments
+    (computeBinomialScores, then insertDocument), one thread.  Same outputs as retrieval()."""
+    L = C.CDLL(str(REF_RETRIEVAL))
+    L.ref_retrieval.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
+                                C.c_void_p]
+    off = np.ascontiguousarray(offsets, np.int32)
+    w = np.ascontiguousarray(words, np.int32)
+    n = off.shape[0] - 1
+    docs = np.empty((n, n_best), np.int32)
+    sc = np.empty((n, n_best), np.float32)
+    if L.ref_retrieval(n_leaves, n, off.ctypes.data, w.ctypes.data, float(p_match), n_best, docs.ctypes.data,
+                       sc.ctypes.data) != 0:
+        raise ValueError("reference retrieval failed")
+    return docs, sc
+
+
+def ref_retrieval_sampled(n_leaves: int, offsets: np.ndarray, words: np.ndarray, p_match: float, n_best: int,
+                          stride: int, phase: int = 0):
+    """The reference's loop with every image inserted and the images i % stride == phase
+    queried: (seconds of those queries, seconds of all insertions, number of queries, sum of
+    their best documents' ids)."""
+    L = C.CDLL(str(REF_RETRIEVAL))
+    L.ref_retrieval_sampled.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_int,
+                                        C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+    off = np.ascontiguousarray(offsets, np.int32)
+    w = np.ascontiguousarray(words, np.int32)
+    tq, ti, nq, cs = C.c_double(), C.c_double(), C.c_int(), C.c_longlong()
+    L.ref_retrieval_sampled(n_leaves, off.shape[0] - 1, off.ctypes.data, w.ctypes.data, float(p_match), n_best,
+                            stride, phase, C.byref(tq), C.byref(ti), C.byref(nq), C.byref(cs))
+    return tq.value, ti.value, nq.value, cs.value

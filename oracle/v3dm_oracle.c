@@ -16,6 +16,9 @@
  *   mutual filter       V3D/CUDA/v3d_cudamatching.cu:546-551   (repeated at :616-621 and :687-692)
  *   voctree descent     V3D/CUDA/v3d_cudamatching.cu:705-792   (global node id of the leaf)
  *                       V3D/Base/v3d_voctree.h:63-99           (CPU version, leaf-local id)
+ *   retrieval scores    V3D/Base/v3d_voctree.h:143-278         LeafDocuments insertDocument /
+ *                       getDocumentHistogram / computeBinomialScores, in the image loop of
+ *                       V3D/Apps/SfM/match_using_voctree.cpp:176-222
  *
  * Domain and pinned arithmetic.
  *   Descriptors are uint8 values u fed to the reference as floats u/512.  Every FP32 product
@@ -352,6 +355,109 @@ int orc_voctree_quantize_u8(int bf, int depth, const uint8_t* nodes, int n, cons
 void orc_scores_u8(int nL, int nR, const uint8_t* L, const uint8_t* R, int32_t* S) {
     for (int r = 0; r < nR; ++r)
         for (int l = 0; l < nL; ++l) S[(size_t)r * nL + l] = dot_u8(L + (size_t)l * 128, R + (size_t)r * 128);
+}
+
+/* ----------------------------------------------------------------------------------- */
+/* Retrieval scoring.  Image i queries the inverted files of images 0..i-1 and is then   */
+/* inserted (match_using_voctree.cpp:187-220).  getDocumentHistogram (v3d_voctree.h:     */
+/* 165-177) adds 1 to document d for every query feature whose leaf lists d, and a leaf  */
+/* lists a document once (insertDocument, :143-163, stores a word histogram).  The score */
+/* of d is computeBinomialScores' expression (:250-270) in double with the C library's   */
+/* log, stored as float, and std::sort / partial_sort order the (score, d) pairs         */
+/* (:273-276).  Since every inverted file lists documents in insertion order, the files  */
+/* of all images are built first and query i reads the part below i, so queries run in   */
+/* parallel.  NaN scores (both images empty) rank after every number, by index here; the */
+/* reference's sort order is unspecified for them.                                      */
+typedef struct {
+    float score;
+    int doc;
+} orc_doc_score;
+
+static int orc_doc_score_cmp(const void* pa, const void* pb) {
+    const orc_doc_score* a = (const orc_doc_score*)pa;
+    const orc_doc_score* b = (const orc_doc_score*)pb;
+    const int an = isnan(a->score), bn = isnan(b->score);
+    if (an != bn) return an ? 1 : -1;
+    if (!an) {
+        if (a->score < b->score) return -1;
+        if (b->score < a->score) return 1;
+    }
+    return (a->doc > b->doc) - (a->doc < b->doc);
+}
+
+int orc_retrieval_binomial(int nLeaves, int nImages, const int* offsets, const int* words, double pMatch,
+                           int nBest, int* bestDocs, float* bestScores, int threads) {
+    if (nLeaves < 1 || nImages < 0 || nBest < 1) return -1;
+    for (int j = 0; j < (nImages > 0 ? offsets[nImages] : 0); ++j)
+        if (words[j] < 0 || words[j] >= nLeaves) return -1;
+    /* inverted files: per leaf the images that have it, ascending, each once */
+    int* fileStart = (int*)calloc((size_t)nLeaves + 1, sizeof(int));
+    int* last = (int*)malloc((size_t)nLeaves * sizeof(int));
+    for (int w = 0; w < nLeaves; ++w) last[w] = -1;
+    for (int d = 0; d < nImages; ++d)
+        for (int j = offsets[d]; j < offsets[d + 1]; ++j)
+            if (last[words[j]] != d) {
+                last[words[j]] = d;
+                ++fileStart[words[j] + 1];
+            }
+    for (int w = 0; w < nLeaves; ++w) fileStart[w + 1] += fileStart[w];
+    int* files = (int*)malloc((size_t)(fileStart[nLeaves] > 0 ? fileStart[nLeaves] : 1) * sizeof(int));
+    int* fill = (int*)malloc((size_t)nLeaves * sizeof(int));
+    memcpy(fill, fileStart, (size_t)nLeaves * sizeof(int));
+    for (int w = 0; w < nLeaves; ++w) last[w] = -1;
+    for (int d = 0; d < nImages; ++d)
+        for (int j = offsets[d]; j < offsets[d + 1]; ++j)
+            if (last[words[j]] != d) {
+                last[words[j]] = d;
+                files[fill[words[j]]++] = d;
+            }
+    free(fill);
+    free(last);
+    const double normalizer = 1.0 / nLeaves;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+#pragma omp parallel
+    {
+        int* hist = (int*)malloc((size_t)(nImages > 0 ? nImages : 1) * sizeof(int));
+        orc_doc_score* sc = (orc_doc_score*)malloc((size_t)(nImages > 0 ? nImages : 1) * sizeof(orc_doc_score));
+#pragma omp for schedule(dynamic, 4)
+        for (int i = 0; i < nImages; ++i) {
+            memset(hist, 0, (size_t)i * sizeof(int));
+            for (int j = offsets[i]; j < offsets[i + 1]; ++j) {
+                const int w = words[j];
+                for (int p = fileStart[w]; p < fileStart[w + 1] && files[p] < i; ++p) hist[files[p]] += 1;
+            }
+            const int nq = offsets[i + 1] - offsets[i];
+            for (int d = 0; d < i; ++d) {
+                const int nd = offsets[d + 1] - offsets[d];
+                const double k = hist[d];
+                const double n = nd < nq ? nd : nq;
+                const double pRandom = (nd > nq ? nd : nq) * normalizer;
+                const double logP0 = log(pRandom);
+                const double log1P0 = log(1.0 - pRandom);
+                const double pMatching = pRandom + pMatch < 1.0 ? pRandom + pMatch : 1.0;
+                const double logP1 = log(pMatching);
+                const double log1P1 = log(1.0 - pMatching);
+                const double z0 = k * logP0 + (n - k) * log1P0;
+                const double z1 = k * logP1 + (n - k) * log1P1;
+                sc[d].score = (float)(z0 - z1);
+                sc[d].doc = d;
+            }
+            qsort(sc, (size_t)i, sizeof(orc_doc_score), orc_doc_score_cmp);
+            for (int j = 0; j < nBest; ++j) {
+                bestDocs[(size_t)i * nBest + j] = j < i ? sc[j].doc : -1;
+                bestScores[(size_t)i * nBest + j] = j < i ? sc[j].score : 0.0f;
+            }
+        }
+        free(sc);
+        free(hist);
+    }
+    free(files);
+    free(fileStart);
+    return 0;
 }
 
 int orc_num_threads(void) {

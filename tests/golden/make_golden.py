@@ -3,6 +3,7 @@
     python tests/golden/make_golden.py voctree [outdir]   # CPU: V3D::VocabularyTree::getVisualWord
     python tests/golden/make_golden.py match [outdir]     # GPU: V3D_CUDA::SIFT_Matching
     python tests/golden/make_golden.py features [outdir]  # CPU: V3D::serializeDataToFile / FromFile
+    python tests/golden/make_golden.py retrieval [outdir] # CPU: V3D::LeafDocuments binomial scores
 
 voctree: the reference's CPU vocabulary tree (V3D/Base/v3d_vocabularytree.h, built from the
 reference headers into oracle/_ref/libv3dref_voctree.so by `make -C oracle ref`), leaf-local
@@ -15,6 +16,12 @@ features: a binary feature archive written by the reference's serializer (oracle
 libv3dref_features.so, from V3D/Base/v3d_serialization.h and v3d_feature.h) and the arrays its
 reader returns for it.  The records hold edge values (negative ids, NaN, infinities, negative
 zero, denormals) so that the check is on the bytes.
+
+retrieval: the image loop of match_using_voctree.cpp:176-222 (computeBinomialScores, then
+insertDocument) on the reference's LeafDocuments (oracle/_ref/libv3dref_retrieval.so, from
+V3D/Base/v3d_voctree.h), on seeded visual-word sequences (v3dm.synth.sequence_words) and hand-made
+edge cases: an empty image, identical images (equal scores, ranked by index), repeated words,
+n_best above the image count, pMatch 0, a query whose every word is unseen.
 
 Inputs are SIFT-like uint8 descriptors (values u/512 handed to the reference as floats) from
 v3dm.synth, stored in the fixtures together with the outputs, so the fixtures stand alone.
@@ -124,8 +131,55 @@ def make_features(out: Path) -> None:
     print("wrote", path, "and", out / "features_ref.npz")
 
 
+def _retrieval_cases():
+    """(name, n_leaves, offsets, words, p_match, n_best)."""
+    cases = []
+    off, w = synth.sequence_words(11, n_images=48, n_leaves=2000, n_min=30, n_max=120, window=6, zipf=1.1)
+    cases.append(("seq48", 2000, off, w, 0.1, 6))
+    off, w = synth.sequence_words(12, n_images=70, n_leaves=5000, n_min=100, n_max=300, window=4, zipf=1.3)
+    cases.append(("seq70_zipf", 5000, off, w, 0.05, 12))
+    rng = np.random.default_rng(13)
+    imgs = [rng.integers(0, 300, 40), np.zeros(0, np.int64), rng.integers(0, 300, 25)]
+    imgs.append(imgs[0].copy())                       # identical to image 0
+    imgs.append(imgs[0].copy())                       # and again: equal scores, ranked by index
+    imgs.append(np.repeat(rng.integers(0, 300, 6), 7))  # repeated words
+    imgs.append(np.arange(300, 330))                  # words no earlier image has
+    imgs.append(rng.integers(0, 300, 1))
+    imgs += [rng.integers(0, 300, int(n)) for n in rng.integers(5, 60, 12)]
+    off = np.zeros(len(imgs) + 1, np.int32)
+    off[1:] = np.cumsum([x.shape[0] for x in imgs])
+    w = np.concatenate(imgs).astype(np.int32)
+    cases.append(("edges", 400, off, w, 0.1, 5))
+    cases.append(("edges_all", 400, off, w, 0.0, 40))  # n_best above the image count
+    off1 = np.array([0, 3], np.int32)
+    cases.append(("single", 10, off1, np.array([1, 2, 2], np.int32), 0.1, 3))
+    return cases
+
+
+def make_retrieval(out: Path) -> None:
+    if not oracle.ref_retrieval_available():
+        raise SystemExit("oracle/_ref/libv3dref_retrieval.so missing: run `make -C oracle ref` first")
+    arrays = {}
+    names = []
+    for name, n_leaves, off, w, pm, nb in _retrieval_cases():
+        docs, sc = oracle.ref_retrieval(n_leaves, off, w, pm, nb)
+        assert np.isfinite(sc).all()
+        names.append(name)
+        arrays[f"{name}_n_leaves"] = np.array(n_leaves, np.int32)
+        arrays[f"{name}_offsets"] = off.astype(np.int32)
+        arrays[f"{name}_words"] = w.astype(np.int32)
+        arrays[f"{name}_p_match"] = np.array(pm, np.float64)
+        arrays[f"{name}_docs"] = docs
+        arrays[f"{name}_scores"] = sc
+        print(f"{name}: {off.shape[0] - 1} images, {w.shape[0]} words, n_best {nb}")
+    arrays["names"] = np.array(names)
+    np.savez_compressed(out / "retrieval_ref.npz", **arrays)
+    print("wrote", out / "retrieval_ref.npz")
+
+
 def main(argv):
-    makers = {"voctree": make_voctree, "match": make_match, "features": make_features}
+    makers = {"voctree": make_voctree, "match": make_match, "features": make_features,
+              "retrieval": make_retrieval}
     if len(argv) < 2 or argv[1] not in makers:
         raise SystemExit(__doc__)
     out = Path(argv[2]) if len(argv) > 2 else HERE
