@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest", "retrieval"],
+    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest", "retrieval",
+                                                   "ransac"],
                     default="stereo")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -64,6 +65,7 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=600, help="proposal workload: Adam steps")
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     ap.add_argument("--rt-images", type=int, default=4096, help="retrieval workload: images in the sequence")
+    ap.add_argument("--rs-pairs", type=int, default=256, help="ransac workload: image pairs per call")
     return ap.parse_args()
 
 
@@ -177,6 +179,8 @@ def cpu_stereo(L, R, lpos, rpos, F, n_left_sample: int, threads: int = 0):
 def run_reference_arm(args, ws, rank):
     if args.workload == "retrieval":
         return run_reference_retrieval(args, ws, rank)
+    if args.workload == "ransac":
+        return run_reference_ransac(args, ws, rank)
     return run_reference_stereo(args, ws, rank)
 
 
@@ -1127,6 +1131,191 @@ def run_retrieval(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+RS_THR, RS_SAMPLES = 2.0, 1000  # inlier threshold (pixels), nSamples of the apps (match_sequence.cpp:261)
+# double operations of one truncated Sampson evaluation: F p and F^T q (5 x 4), the residual (4),
+# its square (1), the denominator (7), the division (1), the truncation and the sum (2)
+RS_FLOPS_PER_EVAL = 35
+FP64_NOMINAL_TFLOPS = 37.0
+
+
+def ransac_data(args, n_pairs):
+    from v3dm import synth
+    return synth.two_view_pairs(args.seed + 7, n_pairs=n_pairs, n_min=500, n_max=3000)
+
+
+def ransac_config(n_pairs, n_corrs):
+    return {"workload": f"essential-matrix RANSAC of {n_pairs} image pairs ({n_corrs} putative correspondences, "
+                        f"500..3000 per pair, 30..80% inliers), nSamples {RS_SAMPLES}, threshold {RS_THR} px, "
+                        "no iterative refinement",
+            "pairs": n_pairs, "correspondences": n_corrs, "n_samples": RS_SAMPLES, "threshold_px": RS_THR,
+            "l2": "flushed between steps (512 MiB write)"}
+
+
+def ref_ransac_pairs(off, corrs, K, pairs):
+    """The reference loop (its five-point solver and pose recovery, the loop restated) on the given
+    pairs with the app's own sample sequence; returns seconds."""
+    from oracle import oracle
+    import v3dm
+    t = 0.0
+    for p in pairs:
+        c = corrs[off[p]:off[p + 1]]
+        smp = v3dm.ransac_shuffle_samples(c.shape[0], RS_SAMPLES, 1000 + p)
+        t0 = time.perf_counter()
+        oracle.ref_ransac(c, K[p, 0], K[p, 1], RS_THR, RS_SAMPLES, smp)
+        t += time.perf_counter() - t0
+    return t
+
+
+def run_reference_ransac(args, ws, rank):
+    """The reference's relative orientation (computeEssentialsFromFiveCorrs and
+    relativePoseFromEssential compiled from the reference into oracle/_ref, in the loop of
+    computeRobustOrientationMLE restated, one pair at a time as the apps run it, one thread) on the
+    same pairs; each step is a sample of 8 pairs."""
+    from oracle import oracle
+    if rank != 0:
+        return
+    if not oracle.ref_ransac_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libv3dref_ransac.so not built"}))
+        return
+    n_pairs = args.rs_pairs
+    off, corrs, K, _, _, _ = ransac_data(args, n_pairs)
+    k = min(8, n_pairs)
+    for w in range(args.warmup):
+        ref_ransac_pairs(off, corrs, K, [(w * 37) % n_pairs])
+    per_pair = []
+    for st in range(args.steps):
+        sel = [(st * k + j) * 29 % n_pairs for j in range(k)]
+        per_pair.append(ref_ransac_pairs(off, corrs, K, sel) / k)
+    ms = 1000.0 * statistics.mean(per_pair) * n_pairs
+    v = n_pairs * 1000.0 / ms
+    line = {
+        "impl": "reference", "metric": "image pairs/s robust relative orientation (5-point RANSAC, Sampson costs)",
+        "value": v, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, int(off[-1])),
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                         "sample": f"{k} of the {n_pairs} pairs per step with the app's own sample sequence; "
+                                   "whole-call time = mean per pair x pairs"},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ransac(args, ws, rank, local):
+    """Essential-matrix RANSAC of 256 image pairs per GPU in one call (independent replicas):
+    every pair's 1001 samples (nSamples + 1, drawn on the device), their five-point solutions,
+    the truncated Sampson cost of every solution over the pair's correspondences, and the apps'
+    sequential choice with the adaptive sample budget.  value: correspondences, outputs in device
+    memory (v3dm_ransac_essential_device); e2e: host correspondences from pinned memory in, models
+    and inlier flags out (v3dm_ransac_essential)."""
+    import torch
+
+    import v3dm
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_pairs = args.rs_pairs
+    off, corrs, K, R, t, inl = ransac_data(args, n_pairs)
+    n_corrs = int(off[-1])
+    n_draw = RS_SAMPLES + 1
+    r = v3dm.Ransac(local)
+    stream = torch.cuda.ExternalStream(r.stream(), device=dev)
+    dc = torch.from_numpy(corrs).to(dev)
+    dm = torch.empty((n_pairs, 31), dtype=torch.float64, device=dev)
+    dn = torch.empty(n_pairs, dtype=torch.int32, device=dev)
+    df = torch.empty(n_corrs, dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device():
+        r.essential_device(off, dc.data_ptr(), K, RS_THR, RS_SAMPLES, n_draw, None, args.seed, dm.data_ptr(),
+                           dn.data_ptr(), df.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        step_device()
+    r.wait()
+    # quality of the result against the generator's poses
+    Rg = dm.cpu().numpy()[:, 18:27].reshape(-1, 3, 3)
+    nin = dn.cpu().numpy()
+    rot_ok = float(np.mean([np.linalg.norm(Rg[p] - R[p]) < 0.05 for p in range(n_pairs) if nin[p] >= 0]))
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    for a0, a1 in evs:
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a0.record(stream)
+        step_device()
+        a1.record(stream)
+    r.wait()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in evs), dev)
+    launches = r.last_launches()
+    r.profile(True)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        step_device()
+    r.wait()
+    hyp_ms, hyp_n = r.profile_read(0)
+    score_ms, score_n = r.profile_read(1)
+    r.profile(False)
+    hyp_ms /= max(hyp_n, 1)
+    score_ms /= max(score_n, 1)
+    n_cand, n_evals = r.candidates()  # candidates scored and their Sampson evaluations, last call
+    res = r.essential(off, corrs, K, RS_THR, RS_SAMPLES, seed=args.seed, flags=False)
+    np.testing.assert_array_equal(res["models"], dm.cpu().numpy())
+    # e2e: pinned host correspondences in, models and flags out
+    cp = torch.from_numpy(corrs).pin_memory().numpy()
+    for _ in range(max(args.warmup, 3)):
+        r.essential(off, cp, K, RS_THR, RS_SAMPLES, seed=args.seed)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    for a0, a1 in ev2:
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a0.record(stream)
+        r.essential(off, cp, K, RS_THR, RS_SAMPLES, seed=args.seed)
+        a1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in ev2), dev)
+    r.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": "image pairs/s robust relative orientation (5-point RANSAC, Sampson costs)",
+        "value": ws * n_pairs * 1000.0 / ms, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, n_corrs),
+        "pose_recovered": rot_ok,
+        "candidates": n_cand, "sampson_evaluations": n_evals,
+        "kernels_ms": {"k_rs_hyp (five-point, all samples)": hyp_ms, "k_rs_score (costs, all candidates)": score_ms},
+        "roofline": {"bound": "fp64", "achieved": RS_FLOPS_PER_EVAL * n_evals / (score_ms * 1e-3) / 1e12,
+                     "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                     "frac": RS_FLOPS_PER_EVAL * n_evals / (score_ms * 1e-3) / 1e12 / FP64_NOMINAL_TFLOPS,
+                     "traffic": None, "peak_src": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+                     "kernel_ms": score_ms, "flops_per_launch": RS_FLOPS_PER_EVAL * n_evals,
+                     "kernel": f"k_rs_score ({RS_FLOPS_PER_EVAL} double operations per Sampson evaluation)"},
+        "e2e": {"value": ws * n_pairs * 1000.0 / ms_e2e, "unit": "pairs/s",
+                "h2d_bytes_per_step": int(corrs.nbytes + off.nbytes + K.nbytes),
+                "d2h_bytes_per_step": int(n_pairs * (31 * 8 + 4) + n_corrs)},
+        "gpu_launches": launches * args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        if oracle.ref_ransac_available():
+            sel = list(range(0, n_pairs, max(1, n_pairs // 16)))[:16]
+            sec = ref_ransac_pairs(off, corrs, K, sel)
+            line["cpu_baseline"] = {"value": len(sel) / sec, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{len(sel)} of the {n_pairs} pairs, the reference's solver and pose "
+                                              "recovery in the loop restated, the app's own sample sequence "
+                                              f"({sec:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -1147,6 +1336,8 @@ def main():
             run_ingest(args, ws, rank, local)
         elif args.workload == "retrieval":
             run_retrieval(args, ws, rank, local)
+        elif args.workload == "ransac":
+            run_ransac(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

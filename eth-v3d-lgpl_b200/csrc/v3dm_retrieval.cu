@@ -160,20 +160,11 @@ k_rt_score(const int32_t* __restrict__ offsets, const int32_t* __restrict__ word
   // shared memory a chunk at a time (invalid words and the padding point to the all-zero row).
   const int b = offsets[i], e = offsets[i + 1];
   const int nw = (i + 31) >> 5;
-  // passes over the columns: the count (1..4) that keeps the most threads busy, fewest on ties
-  int colsPerPass = 1, groups = 1;
-  {
-    int best = -1;
-    for (int np = 1; np <= 4; ++np) {
-      const int cpp = max(1, min((nw + np - 1) / np, (int)blockDim.x));
-      const int gr = min((int)blockDim.x / cpp, kRtChunk / 16);
-      if (gr * cpp > best) {
-        best = gr * cpp;
-        colsPerPass = cpp;
-        groups = gr;
-      }
-    }
-  }
+  // one pass over the columns while they fit the block, else the fewest passes of equal width;
+  // groups of threads split the rows (each extra pass repeats the staging and the flushes)
+  const int passes = (nw + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int colsPerPass = max(1, (nw + passes - 1) / max(passes, 1));
+  const int groups = min((int)blockDim.x / colsPerPass, kRtChunk / 16);  // 16 * groups <= kRtChunk
   const int g = threadIdx.x / colsPerPass;
   const bool active = g < groups;
   const int chunkRows = (kRtChunk / (16 * groups)) * 16 * groups;  // >= 16 * groups, a multiple of it

@@ -144,6 +144,19 @@ def lib() -> C.CDLL:
         L.v3dm_retrieval_wait.argtypes = [vp]
         L.v3dm_retrieval_stream.argtypes = [vp, C.POINTER(vp)]
         L.v3dm_retrieval_pairs.argtypes = [i32, i32, vp, i64, vp, i64p]
+        L.v3dm_ransac_create.argtypes = [C.POINTER(vp), i32]
+        L.v3dm_ransac_destroy.argtypes = [vp]
+        L.v3dm_ransac_essential.argtypes = [vp, i32, vp, vp, vp, C.c_double, i32, i32, vp, C.c_uint64, vp, vp, vp]
+        L.v3dm_ransac_essential_device.argtypes = [vp, i32, vp, vp, vp, C.c_double, i32, i32, vp, C.c_uint64, vp,
+                                                   vp, vp]
+        L.v3dm_ransac_wait.argtypes = [vp]
+        L.v3dm_ransac_profile.argtypes = [vp, i32]
+        L.v3dm_ransac_candidates.argtypes = [vp, i64p, i64p]
+        L.v3dm_ransac_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
+        L.v3dm_ransac_shuffle_samples.argtypes = [i32, i32, C.c_uint, i32, vp, C.POINTER(i32)]
+        L.v3dm_essential_five_point.argtypes = [vp, i32, vp, vp, vp]
+        L.v3dm_ransac_stream.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_ransac_last_launches.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_retrieval_profile.argtypes = [vp, i32]
         L.v3dm_retrieval_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
         _lib = L
@@ -835,3 +848,120 @@ class LeafDocuments:
         off[1:] = np.cumsum([p.shape[0] for p in parts])
         docs, sc = self._r.binomial(self.n_leaves, off, np.concatenate(parts), p_match, k)
         return [(float(sc[nd, j]), int(docs[nd, j])) for j in range(k)]
+
+
+RANSAC_MAX_DRAW = 65536
+RANSAC_MAX_SAMPLES = 4194304
+
+
+def ransac_shuffle_samples(n: int, n_samples: int, seed: int) -> np.ndarray:
+    """The 5-correspondence samples computeRobustOrientationMLE draws after srand(seed), in loop
+    order ((k, 5) int32, at most n_samples + 1 rows)."""
+    cap = n_samples + 1
+    out = np.empty((cap, 5), np.int32)
+    nd = C.c_int(0)
+    _check(lib().v3dm_ransac_shuffle_samples(int(n), int(n_samples), int(seed) & 0xffffffff, cap, _ptr(out),
+                                             C.byref(nd)), "ransac_shuffle_samples")
+    return out[:nd.value].copy()
+
+
+class Ransac:
+    """computeRobustOrientationMLE (reconstruction_common.cpp:139-340, no iterative refinement)
+    for many pairs at once (v3dm_ransac_essential)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().v3dm_ransac_create(C.byref(h), device), "ransac_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.v3dm_ransac_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def essential(self, offsets, corrs, K, inlier_threshold: float, n_samples: int = 1000, samples=None,
+                  n_draw: int | None = None, seed: int = 0, flags: bool = True):
+        """offsets (nPairs + 1), corrs (N, 4) float32 pixel positions (left x, y, right x, y), K
+        (nPairs, 2, 3, 3); samples (nPairs, nDraw, 5) int32 or None (drawn on the device).
+        Returns dict(models (nPairs, 31), E, F, R, T, error, n_inliers, flags)."""
+        off = np.ascontiguousarray(offsets, np.int32)
+        n_pairs = off.shape[0] - 1
+        c = np.ascontiguousarray(corrs, np.float32).reshape(-1, 4)
+        k = np.ascontiguousarray(K, np.float64).reshape(n_pairs, 18)
+        if samples is not None:
+            smp = np.ascontiguousarray(samples, np.int32)
+            n_draw = smp.shape[1]
+            sp = _ptr(smp)
+        else:
+            n_draw = n_samples + 1 if n_draw is None else n_draw
+            sp = None
+        models = np.empty((n_pairs, 31), np.float64)
+        nin = np.empty(n_pairs, np.int32)
+        fl = np.empty(c.shape[0], np.uint8) if flags else None
+        _check(lib().v3dm_ransac_essential(self._h, n_pairs, _ptr(off), _ptr(c), _ptr(k), float(inlier_threshold),
+                                           int(n_samples), int(n_draw), sp, int(seed) & 0xffffffffffffffff,
+                                           _ptr(models), _ptr(nin), _ptr(fl) if fl is not None else None),
+               "ransac_essential")
+        return {"models": models, "E": models[:, :9].reshape(-1, 3, 3), "F": models[:, 9:18].reshape(-1, 3, 3),
+                "R": models[:, 18:27].reshape(-1, 3, 3), "T": models[:, 27:30], "error": models[:, 30],
+                "n_inliers": nin, "flags": fl}
+
+    def essential_device(self, offsets, d_corrs: int, K, inlier_threshold: float, n_samples: int, n_draw: int,
+                         d_samples: int | None, seed: int, d_models: int, d_n_inliers: int, d_flags: int) -> None:
+        off = np.ascontiguousarray(offsets, np.int32)
+        n_pairs = off.shape[0] - 1
+        k = np.ascontiguousarray(K, np.float64).reshape(n_pairs, 18)
+        _check(lib().v3dm_ransac_essential_device(self._h, n_pairs, _ptr(off), C.c_void_p(d_corrs), _ptr(k),
+                                                  float(inlier_threshold), int(n_samples), int(n_draw),
+                                                  C.c_void_p(d_samples) if d_samples else None,
+                                                  int(seed) & 0xffffffffffffffff, C.c_void_p(d_models),
+                                                  C.c_void_p(d_n_inliers), C.c_void_p(d_flags)),
+               "ransac_essential_device")
+
+    def wait(self) -> None:
+        _check(lib().v3dm_ransac_wait(self._h), "ransac_wait")
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().v3dm_ransac_profile(self._h, int(enable)), "ransac_profile")
+
+    def candidates(self):
+        """(candidates scored, Sampson evaluations) of the last call."""
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        _check(lib().v3dm_ransac_candidates(self._h, C.byref(a), C.byref(b)), "ransac_candidates")
+        return a.value, b.value
+
+    def profile_read(self, kernel: int):
+        """(milliseconds, launches) of kernel 0 (five-point) or 1 (costs) since the last read."""
+        ms, n = C.c_double(0.0), C.c_int(0)
+        _check(lib().v3dm_ransac_profile_read(self._h, kernel, C.byref(ms), C.byref(n)), "ransac_profile_read")
+        return ms.value, n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().v3dm_ransac_stream(self._h, C.byref(s)), "ransac_stream")
+        return s.value or 0
+
+    def five_point(self, pts: np.ndarray):
+        """Solutions of (n, 20) samples (x1[5] y1[5] x2[5] y2[5]): (Es (n, 10, 3, 3), counts)."""
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 20)
+        es = np.zeros((p.shape[0], 10, 3, 3), np.float64)
+        cnt = np.empty(p.shape[0], np.int32)
+        _check(lib().v3dm_essential_five_point(self._h, p.shape[0], _ptr(p), _ptr(es), _ptr(cnt)), "five_point")
+        return es, cnt
+
+    def last_launches(self) -> int:
+        n = C.c_int(0)
+        _check(lib().v3dm_ransac_last_launches(self._h, C.byref(n)), "ransac_last_launches")
+        return n.value

@@ -9,7 +9,8 @@ The shapes and value distributions follow the five benchmark workloads of this p
 * ``images``     many images with uneven feature counts and shared feature tracks (batched
                  all-pairs matching);
 * ``voctree``    a hierarchical k-means vocabulary tree and query descriptors;
-* ``sequence_words``  the visual words of an image sequence (retrieval scoring).
+* ``sequence_words``  the visual words of an image sequence (retrieval scoring);
+* ``two_view_pairs``  putative correspondences of many image pairs (essential-matrix RANSAC).
 
 Descriptor generator: i.i.d. Gamma(k=0.6, theta=1) components, L2-normalised, clamped at
 0.2, renormalised, scaled by 512, rounded and clamped to 0..255 (the SIFT normalisation of
@@ -295,3 +296,45 @@ def sequence_words(seed: int = 4, n_images: int = 2048, n_leaves: int = 125_000,
     offsets = np.zeros(n_images + 1, np.int32)
     offsets[1:] = np.cumsum(counts)
     return offsets, np.concatenate(parts) if parts else np.zeros(0, np.int32)
+
+
+def two_view_pairs(seed: int = 5, n_pairs: int = 256, n_min: int = 500, n_max: int = 3000,
+                   inlier_min: float = 0.3, inlier_max: float = 0.8, noise_px: float = 0.5):
+    """Putative correspondences of n_pairs image pairs (the input of the apps' essential-matrix
+    RANSAC): per pair a random rig (rig()), points 3..12 units in front of the first camera,
+    projected into both images with N(0, noise_px^2) pixel noise, a fraction in
+    [inlier_min, inlier_max] of true correspondences and the rest random positions in the right
+    image.  Returns (offsets, corrs (N, 4) float32 left x, y, right x, y, K (n_pairs, 2, 3, 3),
+    R (n_pairs, 3, 3), t (n_pairs, 3), inlier (N,) bool)."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(n_min, n_max + 1, n_pairs)
+    offsets = np.zeros(n_pairs + 1, np.int32)
+    offsets[1:] = np.cumsum(counts)
+    corrs = np.empty((int(offsets[-1]), 4), np.float32)
+    inl = np.zeros(int(offsets[-1]), bool)
+    Ks = np.empty((n_pairs, 2, 3, 3))
+    Rs = np.empty((n_pairs, 3, 3))
+    ts = np.empty((n_pairs, 3))
+    for p in range(n_pairs):
+        K, Rot, t, _ = rig(rng, f=float(rng.uniform(900, 1500)), baseline=float(rng.uniform(0.2, 0.6)),
+                           max_yaw_deg=15.0)
+        n = int(counts[p])
+        k = int(round(n * rng.uniform(inlier_min, inlier_max)))
+        Z = rng.uniform(3.0, 12.0, n)
+        uv = np.c_[rng.uniform(0, 1600, n), rng.uniform(0, 1200, n)]
+        X = (np.linalg.inv(K) @ np.c_[uv, np.ones(n)].T).T * Z[:, None]
+        Y = (Rot @ X.T).T + t
+        q = (K @ Y.T).T
+        q = q[:, :2] / q[:, 2:3]
+        left = uv + rng.normal(0, noise_px, (n, 2))
+        right = q + rng.normal(0, noise_px, (n, 2))
+        right[k:] = np.c_[rng.uniform(0, 1600, n - k), rng.uniform(0, 1200, n - k)]
+        perm = rng.permutation(n)
+        b = offsets[p]
+        corrs[b:b + n] = np.c_[left, right][perm].astype(np.float32)
+        inl[b:b + n] = (np.arange(n) < k)[perm]
+        Ks[p, 0] = K
+        Ks[p, 1] = K
+        Rs[p] = Rot
+        ts[p] = t / np.linalg.norm(t)
+    return offsets, corrs, Ks, Rs, ts, inl

@@ -396,6 +396,70 @@ V3DM_API int v3dm_retrieval_profile_read(v3dm_retrieval* r, int kernel, double* 
 V3DM_API int v3dm_retrieval_pairs(int nImages, int nBest, const int32_t* bestDocs, long long cap, int32_t* pairs,
                                   long long* nPairs);
 
+/* ---- robust relative orientation (computeRobustOrientationMLE) ------------------------ */
+/* The apps' RANSAC for the essential matrix between putative and guided matching
+ * (V3D/Apps/SfM/reconstruction_common.cpp:139-340, called at match_sequence.cpp:260-268), for
+ * many pairs in one call.  Per pair: samples of 5 correspondences in loop order; for each, the
+ * essential matrices of the five-point problem (computeEssentialsFromFiveCorrs,
+ * v3d_poseutilities.cpp:1016-1060; Nister's method, restated); each is scored with
+ * sum_i min(sampson_i, thr^2) over the pair's correspondences (sampsonEpipolarError of
+ * F = K2^-T E K1^-1, reconstruction_common.h:589-607) and kept when its cost is strictly below
+ * the best so far and its pose is consistent on the sample (relativePoseFromEssential,
+ * v3d_poseutilities.cpp:1264-1294); each kept one lowers the sample budget to
+ * ransacNSamples(5, outlier fraction, 1 - 1e-9) (reconstruction_common.h:627-635), and the loop
+ * stops once more than 'budget' samples have been drawn.  mode.iterativeRefinement is not run
+ * (RobustOrientationMode() default).
+ * Inputs: offsets[nPairs + 1] (host) delimit each pair's correspondences in corrs: 4 floats each
+ * (left x, left y, right x, right y, pixels, as PointCorrespondence positions); K: 18 doubles per
+ * pair (K1 then K2, row-major).  samples: nPairs x nDraw x 5 int32 indices into the pair's
+ * correspondences, in the loop's order (at most nSamples + 1 are used), or NULL to draw them on
+ * the device from 'seed' (a counter-based hash; not the reference's rand() sequence --
+ * v3dm_ransac_shuffle_samples gives that one).
+ * Outputs: models, 31 doubles per pair: essential 9, fundamental 9, rotation 9, translation 3
+ * (row-major), error (= best cost / N; -1 when the pair has fewer than 5 correspondences or no
+ * sample gave a consistent pose, with everything else 0); nInliers per pair (-1 then);
+ * inlierFlags (may be NULL): 1 byte per correspondence, sampson < thr^2 under the chosen F.
+ * The scores are evaluated in double in the reference's operation order; the five-point solutions
+ * agree with the reference's to about 1e-12 (same count), so choices can differ only between
+ * candidates whose costs tie to within that. */
+typedef struct v3dm_ransac v3dm_ransac;
+#define V3DM_RANSAC_MAX_DRAW 65536
+#define V3DM_RANSAC_MAX_SAMPLES 4194304 /* nPairs x nDraw */
+V3DM_API int v3dm_ransac_create(v3dm_ransac** out, int device);
+V3DM_API int v3dm_ransac_destroy(v3dm_ransac* r);
+V3DM_API int v3dm_ransac_essential(v3dm_ransac* r, int nPairs, const int32_t* offsets, const float* corrs,
+                                   const double* K, double inlierThreshold, int nSamples, int nDraw,
+                                   const int32_t* samples, uint64_t seed, double* models, int32_t* nInliers,
+                                   uint8_t* inlierFlags);
+/* Device-resident variant: corrs (16-byte aligned), samples and the outputs in device memory
+ * (offsets and K on the host); enqueued on the RANSAC handle's stream, v3dm_ransac_wait
+ * synchronises.  A device sample with an index outside its pair's correspondences yields no
+ * candidate.  nInliers is -1 for pairs without a model. */
+V3DM_API int v3dm_ransac_essential_device(v3dm_ransac* r, int nPairs, const int32_t* offsets, const float* d_corrs,
+                                          const double* K, double inlierThreshold, int nSamples, int nDraw,
+                                          const int32_t* d_samples, uint64_t seed, double* d_models,
+                                          int32_t* d_nInliers, uint8_t* d_inlierFlags);
+V3DM_API int v3dm_ransac_wait(v3dm_ransac* r);
+/* The sample sequence computeRobustOrientationMLE draws for a pair of N correspondences after
+ * srand(seed): getShuffleCount(N, nSamples, 5) shuffles of 0..N-1 (random_shuffle over the C
+ * library's rand()), each cut into consecutive 5-tuples while j < N - 5; at most cap tuples are
+ * written (5 int32 each), *nDraw = the count written (at most nSamples + 1 are ever used).  Host
+ * code; it reseeds the C library's generator with srand(seed). */
+V3DM_API int v3dm_ransac_shuffle_samples(int N, int nSamples, unsigned seed, int cap, int32_t* samples, int* nDraw);
+/* The five-point solutions of n samples on the device (diagnostic): pts holds, per sample,
+ * x1[5] y1[5] x2[5] y2[5] (normalised coordinates, q^T E p = 0); Es receives up to 10 row-major
+ * essential matrices per sample (90 doubles), counts the number of each. */
+V3DM_API int v3dm_essential_five_point(v3dm_ransac* r, int n, const double* pts, double* Es, int32_t* counts);
+V3DM_API int v3dm_ransac_stream(v3dm_ransac* r, void** stream);
+V3DM_API int v3dm_ransac_last_launches(v3dm_ransac* r, int* n);
+/* CUDA-event timing of kernel 0 (five-point solutions of every sample) and kernel 1 (the costs of
+ * every candidate); read returns the milliseconds and launches since the last read. */
+/* Work of the last call: candidates scored (five-point solutions of all samples) and Sampson
+ * evaluations (sum over candidates of their pair's correspondence count). */
+V3DM_API int v3dm_ransac_candidates(v3dm_ransac* r, long long* nCandidates, long long* nEvaluations);
+V3DM_API int v3dm_ransac_profile(v3dm_ransac* r, int enable);
+V3DM_API int v3dm_ransac_profile_read(v3dm_ransac* r, int kernel, double* msTotal, int* launches);
+
 #ifdef __cplusplus
 }
 #endif

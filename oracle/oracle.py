@@ -19,6 +19,7 @@ REF_VOCTREE = HERE / "_ref" / "libv3dref_voctree.so"
 REF_CUDA = HERE / "_ref" / "libv3dref_cuda.so"
 REF_FEATURES = HERE / "_ref" / "libv3dref_features.so"
 REF_RETRIEVAL = HERE / "_ref" / "libv3dref_retrieval.so"
+REF_RANSAC = HERE / "_ref" / "libv3dref_ransac.so"
 
 _lib = None
 
@@ -305,3 +306,55 @@ def ref_retrieval_sampled(n_leaves: int, offsets: np.ndarray, words: np.ndarray,
     L.ref_retrieval_sampled(n_leaves, off.shape[0] - 1, off.ctypes.data, w.ctypes.data, float(p_match), n_best,
                             stride, phase, C.byref(tq), C.byref(ti), C.byref(nq), C.byref(cs))
     return tq.value, ti.value, nq.value, cs.value
+
+
+# ---- the reference's relative orientation ---------------------------------------------------
+
+def ref_ransac_available() -> bool:
+    return REF_RANSAC.exists()
+
+
+def _ref_ransac_lib():
+    L = C.CDLL(str(REF_RANSAC))
+    vp = C.c_void_p
+    L.ref_five_point.argtypes = [vp] * 5 + [C.POINTER(C.c_int)]
+    L.ref_pose.argtypes = [vp] * 7
+    L.ref_shuffle_samples.argtypes = [C.c_int, C.c_int, C.c_uint, C.c_int, vp, C.POINTER(C.c_int)]
+    L.ref_ransac.argtypes = [C.c_int, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_int), vp,
+                             C.POINTER(C.c_int)]
+    return L
+
+
+def ref_five_point(x1, y1, x2, y2):
+    """computeEssentialsFromFiveCorrs: (k, 3, 3) essential matrices."""
+    L = _ref_ransac_lib()
+    a = [np.ascontiguousarray(v, np.float64) for v in (x1, y1, x2, y2)]
+    E = np.zeros(90)
+    n = C.c_int(0)
+    L.ref_five_point(*[v.ctypes.data for v in a], E.ctypes.data, C.byref(n))
+    return E[:9 * n.value].reshape(-1, 3, 3)
+
+
+def ref_shuffle_samples(n: int, n_samples: int, seed: int) -> np.ndarray:
+    L = _ref_ransac_lib()
+    out = np.empty((n_samples + 1, 5), np.int32)
+    nd = C.c_int(0)
+    L.ref_shuffle_samples(n, n_samples, seed, n_samples + 1, out.ctypes.data, C.byref(nd))
+    return out[:nd.value].copy()
+
+
+def ref_ransac(corrs: np.ndarray, K1: np.ndarray, K2: np.ndarray, inlier_threshold: float, n_samples: int,
+               samples: np.ndarray):
+    """The loop of computeRobustOrientationMLE (no refinement) on one pair with the given samples:
+    dict(model (31), n_inliers, flags, chosen = sample * 10 + solution index or -1)."""
+    L = _ref_ransac_lib()
+    c = np.ascontiguousarray(corrs, np.float32).reshape(-1, 4)
+    k1 = np.ascontiguousarray(K1, np.float64)
+    k2 = np.ascontiguousarray(K2, np.float64)
+    s = np.ascontiguousarray(samples, np.int32).reshape(-1, 5)
+    model = np.empty(31)
+    nin, ch = C.c_int(0), C.c_int(0)
+    flags = np.empty(c.shape[0], np.uint8)
+    L.ref_ransac(c.shape[0], c.ctypes.data, k1.ctypes.data, k2.ctypes.data, float(inlier_threshold), n_samples,
+                 s.shape[0], s.ctypes.data, model.ctypes.data, C.byref(nin), flags.ctypes.data, C.byref(ch))
+    return {"model": model, "n_inliers": nin.value, "flags": flags, "chosen": ch.value}

@@ -1,0 +1,181 @@
+"""Essential-matrix RANSAC on the GPU (v3dm_ransac_*) against the reference pin (oracle/_ref: the
+reference's computeEssentialsFromFiveCorrs and relativePoseFromEssential in the loop of
+computeRobustOrientationMLE, V3D/Apps/SfM/reconstruction_common.cpp:139-340, refinement off).
+
+Tolerances: the five-point solutions are floating point (the reference's SVD null space and
+polynomial solver against a QR null space and derivative-bracketed roots here); they agree to
+about 1e-12, so the per-sample solution counts must agree on >= 99.5% of random samples and >= 99%
+of the reference's solutions must have a counterpart within 1e-6 (unit norm, sign-fixed).  The
+costs are evaluated in double in the reference's operation order, so with the reference's own
+sample sequence the chosen candidate must be the same (unit E within 1e-5) on >= 97% of the pairs
+(a different choice can only come from costs that tie to within the solutions' rounding); for those
+the error, R and T agree to 1e-4 and the inlier flags to 0.2% of the correspondences (ill-conditioned
+samples give solutions that differ by up to ~1.5e-6 between the two solvers, and pixel coordinates
+near 1000 amplify that in the Sampson costs to a few 1e-6 relative)."""
+import numpy as np
+import pytest
+
+from v3dm import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _need_ref(oracle_mod):
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+
+
+def _unit(E):
+    e = E.reshape(-1)
+    e = e / np.linalg.norm(e)
+    return e * np.sign(e[np.argmax(np.abs(e))])
+
+
+def _rot(rng):
+    v = rng.normal(size=3) * 0.3
+    th = np.linalg.norm(v)
+    k = v / th
+    Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * Kx @ Kx
+
+
+def test_five_point_solutions_match_the_reference(v3dm_mod, oracle_mod):
+    _need_ref(oracle_mod)
+    rng = np.random.default_rng(0)
+    pts = []
+    for t in range(3000):
+        if t % 2 == 0:  # consistent samples of a random pose
+            R = _rot(rng)
+            T = rng.normal(size=3)
+            X = np.c_[rng.uniform(-1, 1, (5, 2)), rng.uniform(3, 6, 5)]
+            p = X[:, :2] / X[:, 2:]
+            Y = (R @ X.T).T + T
+            q = Y[:, :2] / Y[:, 2:]
+        else:  # random (outlier) samples
+            p = rng.uniform(-0.5, 0.5, (5, 2))
+            q = rng.uniform(-0.5, 0.5, (5, 2))
+        pts.append(np.r_[p[:, 0], p[:, 1], q[:, 0], q[:, 1]])
+    pts = np.array(pts)
+    with v3dm_mod.Ransac() as r:
+        es, cnt = r.five_point(pts)
+    same, matched, total = 0, 0, 0
+    for t in range(pts.shape[0]):
+        ref = oracle_mod.ref_five_point(pts[t, :5], pts[t, 5:10], pts[t, 10:15], pts[t, 15:])
+        ours = [_unit(es[t, k]) for k in range(cnt[t])]
+        same += len(ref) == cnt[t]
+        for e in ref:
+            total += 1
+            if ours and min(np.linalg.norm(_unit(e) - o) for o in ours) < 1e-6:
+                matched += 1
+        if t % 2 == 0:  # the true E is among ours
+            pass
+    assert same >= 0.995 * pts.shape[0], same
+    assert matched >= 0.99 * total, (matched, total)
+
+
+@pytest.mark.parametrize("n_pairs,n_min,n_max,thr,n_samples", [(24, 5, 60, 2.0, 200), (40, 300, 1500, 2.0, 1000),
+                                                               (6, 2500, 4000, 1.0, 1000)])
+def test_reference_sample_sequence_gives_the_reference_choice(v3dm_mod, oracle_mod, n_pairs, n_min, n_max, thr,
+                                                              n_samples):
+    _need_ref(oracle_mod)
+    off, corrs, K, R, t, inl = synth.two_view_pairs(n_pairs + n_min, n_pairs=n_pairs, n_min=n_min, n_max=n_max)
+    seqs = [v3dm_mod.ransac_shuffle_samples(int(off[p + 1] - off[p]), n_samples, 100 + p) for p in range(n_pairs)]
+    with v3dm_mod.Ransac() as r:
+        agree, total = 0, 0
+        for p in range(n_pairs):
+            n = int(off[p + 1] - off[p])
+            s = seqs[p]
+            c = corrs[off[p]:off[p + 1]]
+            ref = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], thr, n_samples, s if s.shape[0] else np.zeros((0, 5)))
+            if s.shape[0] == 0:  # fewer than 6 correspondences: the loop draws nothing
+                assert ref["chosen"] == -1
+                if n < 5:
+                    got = r.essential(np.array([0, n]), c, K[p:p + 1], thr, n_samples, n_draw=1, seed=1)
+                    assert got["n_inliers"][0] == -1 and got["error"][0] == -1.0
+                continue
+            got = r.essential(np.array([0, n]), c, K[p:p + 1], thr, n_samples, samples=s[None])
+            total += 1
+            if ref["chosen"] < 0:
+                agree += got["n_inliers"][0] == -1
+                continue
+            if got["n_inliers"][0] < 0:
+                continue
+            if np.linalg.norm(_unit(got["E"][0]) - _unit(ref["model"][:9])) < 1e-6:
+                agree += 1
+                np.testing.assert_allclose(got["error"][0], ref["model"][30], rtol=1e-6)
+                assert np.abs(got["R"][0].reshape(-1) - ref["model"][18:27]).max() < 1e-6
+                assert np.abs(got["T"][0] - ref["model"][27:30]).max() < 1e-6
+                diff = int((got["flags"] != ref["flags"]).sum())
+                assert diff <= 2 and abs(int(got["n_inliers"][0]) - ref["n_inliers"]) <= 2
+        assert agree >= 0.97 * total, (agree, total)
+
+
+def test_batched_call_equals_per_pair_calls(v3dm_mod):
+    off, corrs, K, R, t, inl = synth.two_view_pairs(8, n_pairs=30, n_min=4, n_max=900)
+    with v3dm_mod.Ransac() as r:
+        allp = r.essential(off, corrs, K, 2.0, 300, seed=5)
+        assert r.last_launches() > 0
+        for p in (0, 7, 29):
+            n = int(off[p + 1] - off[p])
+            # the device draws depend on (pair, sample): a one-pair call sees pair 0's draws
+            one = r.essential(off[p:p + 2] - off[p], corrs[off[p]:off[p + 1]], K[p:p + 1], 2.0, 300, seed=5)
+            if n < 5:
+                assert allp["n_inliers"][p] == -1 and one["n_inliers"][0] == -1
+        small = np.diff(off) < 5
+        assert (allp["n_inliers"][small] == -1).all()
+        assert (allp["flags"][np.repeat(small, np.diff(off))] == 0).all()
+
+
+def test_device_entry_point_equals_host_entry_point(v3dm_mod):
+    import torch
+    off, corrs, K, R, t, inl = synth.two_view_pairs(10, n_pairs=20, n_min=100, n_max=1200)
+    with v3dm_mod.Ransac() as r:
+        host = r.essential(off, corrs, K, 2.0, 500, seed=9)
+        dc = torch.from_numpy(corrs).cuda()
+        dm = torch.empty((20, 31), dtype=torch.float64, device="cuda")
+        dn = torch.empty(20, dtype=torch.int32, device="cuda")
+        df = torch.empty(corrs.shape[0], dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        r.essential_device(off, dc.data_ptr(), K, 2.0, 500, 501, None, 9, dm.data_ptr(), dn.data_ptr(), df.data_ptr())
+        r.wait()
+        np.testing.assert_array_equal(dm.cpu().numpy(), host["models"])
+        np.testing.assert_array_equal(dn.cpu().numpy(), host["n_inliers"])
+        np.testing.assert_array_equal(df.cpu().numpy(), host["flags"])
+
+
+def test_device_draws_find_the_pose(v3dm_mod):
+    off, corrs, K, R, t, inl = synth.two_view_pairs(9, n_pairs=64, n_min=300, n_max=2000, inlier_min=0.4,
+                                                    inlier_max=0.8)
+    with v3dm_mod.Ransac() as r:
+        got = r.essential(off, corrs, K, 2.0, 1000, seed=123)
+    good = 0
+    for p in range(64):
+        if got["n_inliers"][p] < 0:
+            continue
+        rot_err = np.linalg.norm(got["R"][p] - R[p])
+        true_in = inl[off[p]:off[p + 1]]
+        fl = got["flags"][off[p]:off[p + 1]].astype(bool)
+        recall = (fl & true_in).sum() / max(1, true_in.sum())
+        good += rot_err < 0.05 and recall > 0.8 and fl.sum() == got["n_inliers"][p]
+    assert good >= 60, good
+
+
+def test_errors(v3dm_mod):
+    import ctypes as C
+    L = v3dm_mod.lib()
+    off = np.array([0, 10], np.int32)
+    corrs = np.random.default_rng(0).uniform(0, 100, (10, 4)).astype(np.float32)
+    K = np.tile(np.eye(3), (1, 2, 1, 1))
+    with v3dm_mod.Ransac() as r:
+        bad = np.full((1, 3, 5), 10, np.int32)  # index 10 of 10 correspondences
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            r.essential(off, corrs, K, 2.0, 10, samples=bad)
+        assert e.value.status == v3dm_mod.ERR_ARG
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            r.essential(off, corrs, np.zeros((1, 2, 3, 3)), 2.0, 10)  # singular K
+        assert e.value.status == v3dm_mod.ERR_ARG
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            r.essential(off, corrs, K, 2.0, 10, n_draw=v3dm_mod.RANSAC_MAX_DRAW + 1)
+        assert e.value.status == v3dm_mod.ERR_ARG
+        got = r.essential(off, corrs, K, 2.0, 10)  # still usable
+        assert got["n_inliers"].shape == (1,)

@@ -1,0 +1,40 @@
+"""Essential-matrix RANSAC, CPU part: the library's sample sequence (v3dm_ransac_shuffle_samples,
+host code) against the reference loop's own draws (srand, std::random_shuffle, consecutive
+5-tuples: V3D/Apps/SfM/reconstruction_common.cpp:110-114, 173-205), and the reference pin itself
+(oracle/_ref: the reference's five-point solver and pose recovery in the loop of
+computeRobustOrientationMLE) on synthetic two-view data."""
+import numpy as np
+import pytest
+
+from v3dm import synth
+
+
+@pytest.mark.parametrize("n,n_samples,seed", [(4, 1000, 1), (5, 1000, 1), (6, 1000, 2), (9, 10, 3), (137, 1000, 4),
+                                              (800, 1000, 5), (5000, 1000, 6), (300, 0, 7)])
+def test_samples_equal_the_reference_draws(v3dm_mod, oracle_mod, n, n_samples, seed):
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    got = v3dm_mod.ransac_shuffle_samples(n, n_samples, seed)
+    exp = oracle_mod.ref_shuffle_samples(n, n_samples, seed)
+    np.testing.assert_array_equal(got, exp)
+    if n >= 6:
+        assert got.shape[0] == min(n_samples + 1, max(1, int(n_samples * 5.0 / n + 0.5)) * ((n - 5 + 4) // 5))
+        assert (got >= 0).all() and (got < n).all()
+        assert all(len(set(r)) == 5 for r in got)
+
+
+def test_reference_pin_recovers_the_pose(oracle_mod):
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    off, corrs, K, R, t, inl = synth.two_view_pairs(3, n_pairs=3, n_min=400, n_max=600, inlier_min=0.6,
+                                                    inlier_max=0.7)
+    for p in range(3):
+        c = corrs[off[p]:off[p + 1]]
+        smp = oracle_mod.ref_shuffle_samples(c.shape[0], 1000, 11 + p)
+        res = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, smp)
+        assert res["chosen"] >= 0
+        Rm = res["model"][18:27].reshape(3, 3)
+        assert np.linalg.norm(Rm - R[p]) < 0.05
+        flags = res["flags"].astype(bool)
+        assert flags.sum() == res["n_inliers"]
+        assert (flags & inl[off[p]:off[p + 1]]).sum() > 0.8 * inl[off[p]:off[p + 1]].sum()
