@@ -12,12 +12,15 @@
 // Here all pairs and all samples run at once:
 //   k_rs_normalize  correspondences normalised by K^-1 (the solver's input);
 //   k_rs_draw       (optional) 5 distinct correspondences per sample from a counter-based hash;
+// then rounds of 128 samples per pair (pairs whose loop has ended are skipped):
 //   k_rs_hyp        one thread per sample: five-point solver, F, pose consistency -> slots;
-//   k_rs_compact    one CTA per pair: the candidates in loop order, densely;
+//   k_rs_compact    one CTA per pair: the round's candidates in loop order, densely;
 //   k_rs_score      a CTA per (pair, 128 candidates): the pair's correspondences staged in
 //                   shared memory, one candidate per thread, cost and inlier count in double;
 //   k_rs_select     one thread per pair: the loop's sequential rule (strictly lower cost, pose
-//                   consistent, adaptive sample budget) over the candidates in loop order;
+//                   consistent, adaptive sample budget) over the round's candidates in loop
+//                   order, its state carried to the next round;
+// and at the end
 //   k_rs_finish     pose, error and inlier flags of the chosen candidate.
 // The loop's iterative refinement (mode.iterativeRefinement) is not run.
 #include <algorithm>
@@ -37,7 +40,8 @@ namespace {
 constexpr int kRsMaxSol = 10;        // solutions per sample
 constexpr int kRsSlotDoubles = 18;   // E, F
 constexpr int kRsScoreThreads = 128;
-constexpr int kRsStage = 1024;       // correspondences staged per round in k_rs_score
+constexpr int kRsStage = 1024;       // correspondences staged at a time in k_rs_score
+constexpr int kRsRound = 128;        // samples per pair per round
 
 struct RsDeviceGuard {
   int prev = -1;
@@ -116,16 +120,43 @@ __global__ void k_rs_draw(const int32_t* __restrict__ offsets, int nPairs, int n
   for (int k = got; k < 5; ++k) s[k] = (s[k - 1] + 1) % n;  // unreachable in practice (n >= 5)
 }
 
-// One thread per (pair, sample): candidates into slots (pair, sample, r), their count, pose flag.
+// The loop's state per pair, carried from round to round.
+struct RsState {
+  double minError;  // best cost so far (1e30: none)
+  int budget;       // nSamples, lowered by each accepted candidate
+  int drawn;        // samples consumed
+  int chosen;       // sample of the accepted candidate, -1: none
+  int done;         // the loop has ended for this pair
+};
+
+__global__ void k_rs_init(const int32_t* __restrict__ offsets, int nPairs, int nSamples, RsState* __restrict__ st) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nPairs) return;
+  RsState s;
+  s.minError = 1e30;
+  s.budget = nSamples;
+  s.drawn = 0;
+  s.chosen = -1;
+  s.done = offsets[p + 1] - offsets[p] < 5;
+  st[p] = s;
+}
+
+// One thread per (pair, sample of this round): candidates into the round's slots (pair, j, r),
+// their count and pose flag.  Pairs whose loop has ended are skipped.
 __global__ void __launch_bounds__(64)
-k_rs_hyp(const int32_t* __restrict__ offsets, int nPairs, int nDraw, const int32_t* __restrict__ samples,
-         const double4* __restrict__ norm, const double* __restrict__ invK, double* __restrict__ slots,
-         uint8_t* __restrict__ slotOk, int8_t* __restrict__ counts) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nPairs * nDraw) return;
-  const int p = (int)(t / nDraw);
+k_rs_hyp(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
+         const int32_t* __restrict__ samples, const double4* __restrict__ norm, const double* __restrict__ invK,
+         const RsState* __restrict__ st, double* __restrict__ slots, uint8_t* __restrict__ slotOk,
+         int8_t* __restrict__ counts) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // p * kRsRound + j
+  const int p = (int)(t / kRsRound), j = (int)(t % kRsRound);
+  if (p >= nPairs) return;
+  if (j >= len || st[p].done) {
+    counts[t] = 0;
+    return;
+  }
   const int b = offsets[p], n = offsets[p + 1] - b;
-  const int32_t* s = samples + t * 5;
+  const int32_t* s = samples + ((long long)p * nDraw + s0 + j) * 5;
   bool valid = n >= 5;
   for (int k = 0; k < 5 && valid; ++k) valid = s[k] >= 0 && s[k] < n;
   if (!valid) {
@@ -145,8 +176,8 @@ k_rs_hyp(const int32_t* __restrict__ offsets, int nPairs, int nDraw, const int32
   const double* iK1 = invK + 18 * p;
   const double* iK2 = invK + 18 * p + 9;
   double iK2t[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) iK2t[3 * i + j] = iK2[3 * j + i];
+  for (int a = 0; a < 3; ++a)
+    for (int c = 0; c < 3; ++c) iK2t[3 * a + c] = iK2[3 * c + a];
   for (int r = 0; r < ns; ++r) {
     double* slot = slots + (t * kRsMaxSol + r) * kRsSlotDoubles;
     double tmp[9], F[9], R[9], T[3];
@@ -174,43 +205,44 @@ __global__ void k_rs_five_point(int n, const double* __restrict__ pts, double* _
   counts[t] = ns;
 }
 
-// One CTA per pair: slot ids (sample * 10 + r) of the candidates in loop order.
-__global__ void k_rs_compact(int nDraw, const int8_t* __restrict__ counts, int32_t* __restrict__ list,
-                             int32_t* __restrict__ listN) {
+// One CTA per pair: the round's candidate slots (j * 10 + r) in loop order; work counters.
+__global__ void k_rs_compact(const int32_t* __restrict__ offsets, const int8_t* __restrict__ counts,
+                             int32_t* __restrict__ list, int32_t* __restrict__ listN,
+                             unsigned long long* __restrict__ work) {
+  static_assert(kRsRound <= 1024, "one thread per sample of the round");
   const int p = blockIdx.x;
-  __shared__ int base;
   __shared__ int warpSum[32];
-  if (threadIdx.x == 0) base = 0;
-  __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int s0 = 0; s0 < nDraw; s0 += blockDim.x) {
-    const int s = s0 + threadIdx.x;
-    const int c = s < nDraw ? counts[(long long)p * nDraw + s] : 0;
-    int inc = c;
+  const int j = threadIdx.x;
+  const int c = j < kRsRound ? counts[(long long)p * kRsRound + j] : 0;
+  int inc = c;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += v;
-    }
-    if (lane == 31) warpSum[wid] = inc;
-    __syncthreads();
-    int before = base;
-    for (int w = 0; w < wid; ++w) before += warpSum[w];
-    int32_t* out = list + (long long)p * nDraw * kRsMaxSol;
-    for (int r = 0; r < c; ++r) out[before + inc - c + r] = s * kRsMaxSol + r;
-    __syncthreads();
-    if (threadIdx.x == 0)
-      for (int w = 0; w < nw; ++w) base += warpSum[w];
-    __syncthreads();
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
   }
-  if (threadIdx.x == 0) listN[p] = base;
+  if (lane == 31) warpSum[wid] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < wid; ++w) before += warpSum[w];
+  int32_t* out = list + (long long)p * kRsRound * kRsMaxSol;
+  for (int r = 0; r < c; ++r) out[before + inc - c + r] = j * kRsMaxSol + r;
+  if (threadIdx.x == 0) {
+    int total = 0;
+    for (int w = 0; w < nw; ++w) total += warpSum[w];
+    listN[p] = total;
+    if (total) {
+      atomicAdd(&work[0], (unsigned long long)total);
+      atomicAdd(&work[1], (unsigned long long)total * (unsigned long long)(offsets[p + 1] - offsets[p]));
+    }
+  }
 }
 
 // CTA (pair, chunk): cost = sum_i min(d_i, thr2) and the count of d_i < thr2 for 128 candidates.
 __global__ void __launch_bounds__(kRsScoreThreads)
-k_rs_score(const int32_t* __restrict__ offsets, int nDraw, const float4* __restrict__ corrs,
-           const int32_t* __restrict__ list, const int32_t* __restrict__ listN, const double* __restrict__ slots,
-           double thr2, double* __restrict__ cost, int32_t* __restrict__ inl) {
+k_rs_score(const int32_t* __restrict__ offsets, const float4* __restrict__ corrs, const int32_t* __restrict__ list,
+           const int32_t* __restrict__ listN, const double* __restrict__ slots, double thr2,
+           double* __restrict__ cost, int32_t* __restrict__ inl) {
   const int p = blockIdx.x;
   const int h = blockIdx.y * kRsScoreThreads + threadIdx.x;
   const int H = listN[p];
@@ -221,7 +253,7 @@ k_rs_score(const int32_t* __restrict__ offsets, int nDraw, const float4* __restr
   long long slot = 0;
   double F[9];
   if (mine) {
-    slot = (long long)p * nDraw * kRsMaxSol + list[(long long)p * nDraw * kRsMaxSol + h];
+    slot = (long long)p * kRsRound * kRsMaxSol + list[(long long)p * kRsRound * kRsMaxSol + h];
     for (int k = 0; k < 9; ++k) F[k] = slots[slot * kRsSlotDoubles + 9 + k];
   }
   double sum = 0.0;
@@ -254,66 +286,65 @@ __device__ __forceinline__ int rs_budget(double outlierRatio) {
   return (int)N;
 }
 
-// One thread per pair: the loop's choice.  best[p] = slot or -1; bestCost[p].
-__global__ void k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int nSamples,
+// One thread per pair: the loop over this round's samples in order (the rule of
+// reconstruction_common.cpp:177-335 without refinement); the accepted candidate's E and F are kept.
+__global__ void k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
                             const int8_t* __restrict__ counts, const uint8_t* __restrict__ slotOk,
                             const double* __restrict__ cost, const int32_t* __restrict__ inl,
-                            long long* __restrict__ best, double* __restrict__ bestCost) {
+                            const double* __restrict__ slots, RsState* __restrict__ st, double* __restrict__ bestEF) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nPairs) return;
+  RsState s = st[p];
+  if (s.done) return;
   const int n = offsets[p + 1] - offsets[p];
-  long long chosen = -1;
-  double minError = 1e30;
-  int budget = nSamples, drawn = 0;
-  if (n >= 5) {
-    for (int s = 0; s < nDraw; ++s) {
-      if (drawn > budget) break;
-      ++drawn;
-      const long long t = (long long)p * nDraw + s;
-      const int ns = counts[t];
-      for (int r = 0; r < ns; ++r) {
-        const long long slot = t * kRsMaxSol + r;
-        if (!(cost[slot] < minError)) continue;
-        if (!slotOk[slot]) continue;
-        minError = cost[slot];
-        chosen = slot;
-        const float frac = (float)(inl[slot] - 5) / (float)(n - 5);
-        budget = min(budget, rs_budget(1.0 - (double)frac));
-      }
+  for (int j = 0; j < len; ++j) {
+    if (s.drawn > s.budget) break;
+    ++s.drawn;
+    const long long t = (long long)p * kRsRound + j;
+    const int ns = counts[t];
+    for (int r = 0; r < ns; ++r) {
+      const long long slot = t * kRsMaxSol + r;
+      if (!(cost[slot] < s.minError)) continue;
+      if (!slotOk[slot]) continue;
+      s.minError = cost[slot];
+      s.chosen = s0 + j;
+      for (int k = 0; k < kRsSlotDoubles; ++k) bestEF[(size_t)p * kRsSlotDoubles + k] = slots[slot * kRsSlotDoubles + k];
+      const float frac = (float)(inl[slot] - 5) / (float)(n - 5);
+      s.budget = min(s.budget, rs_budget(1.0 - (double)frac));
     }
   }
-  best[p] = chosen;
-  bestCost[p] = minError;
+  if (s.drawn > s.budget || s0 + len >= nDraw) s.done = 1;  // the next sample would end the loop
+  st[p] = s;
 }
 
 // One thread per pair: E, F, R, T and error of the choice.
 __global__ void k_rs_finish(const int32_t* __restrict__ offsets, int nPairs, int nDraw,
                             const int32_t* __restrict__ samples, const double4* __restrict__ norm,
-                            const double* __restrict__ slots, const long long* __restrict__ best,
-                            const double* __restrict__ bestCost, double* __restrict__ out) {
+                            const RsState* __restrict__ st, const double* __restrict__ bestEF,
+                            double* __restrict__ out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nPairs) return;
   double* o = out + (size_t)p * 31;  // E 9, F 9, R 9, T 3, error 1
-  const long long slot = best[p];
-  if (slot < 0) {
+  const RsState s = st[p];
+  if (s.chosen < 0) {
     for (int k = 0; k < 30; ++k) o[k] = 0.0;
     o[30] = -1.0;
     return;
   }
-  const long long t = slot / kRsMaxSol;
   const int b = offsets[p], n = offsets[p + 1] - b;
+  const int32_t* smp = samples + ((long long)p * nDraw + s.chosen) * 5;
   double x1[5], y1[5], x2[5], y2[5];
   for (int k = 0; k < 5; ++k) {
-    const double4 v = norm[b + samples[t * 5 + k]];
+    const double4 v = norm[b + smp[k]];
     x1[k] = v.x;
     y1[k] = v.y;
     x2[k] = v.z;
     y2[k] = v.w;
   }
-  const double* sl = slots + slot * kRsSlotDoubles;
-  for (int k = 0; k < 18; ++k) o[k] = sl[k];
-  ess::essential_pose(sl, 5, x1, y1, x2, y2, o + 18, o + 27);
-  o[30] = bestCost[p] / n;
+  const double* ef = bestEF + (size_t)p * kRsSlotDoubles;
+  for (int k = 0; k < 18; ++k) o[k] = ef[k];
+  ess::essential_pose(ef, 5, x1, y1, x2, y2, o + 18, o + 27);
+  o[30] = s.minError / n;
 }
 
 // nIn = -1 for the pairs without a model.
@@ -405,10 +436,12 @@ struct v3dm_ransac {
   size_t costCap = 0;
   int32_t* dInl = nullptr;
   size_t inlCap = 0;
-  long long* dBest = nullptr;
-  size_t bestCap = 0;
-  double* dBestCost = nullptr;
-  size_t bestCostCap = 0;
+  void* dState = nullptr;  // RsState per pair
+  size_t stateCap = 0;
+  double* dBestEF = nullptr;
+  size_t bestEFCap = 0;
+  unsigned long long* dWork = nullptr;  // candidates, Sampson evaluations of the last call
+  size_t workCap = 0;
   double* dOut = nullptr;
   size_t outCap = 0;
   uint8_t* dFlags = nullptr;
@@ -438,44 +471,60 @@ cudaError_t rs_mark(v3dm_ransac* r, int k) {
 // Everything from normalisation to inlier flags, on r's stream; inputs already on the device.
 int rs_enqueue(v3dm_ransac* r, int nPairs, int nCorrs, int nDraw, int nSamples, bool draw, uint64_t seed,
                double thr2, const float4* dCorrs, int32_t* dSamples, double* dOut, int32_t* dNIn, uint8_t* dFlags) {
-  const size_t nT = (size_t)nPairs * nDraw;
+  const size_t nR = (size_t)nPairs * kRsRound;  // sample slots of one round
   V3DM_RS_TRY(rs_grow(r->dNorm, r->normCap, (size_t)nCorrs));
-  V3DM_RS_TRY(rs_grow(r->dSlots, r->slotCap, nT * kRsMaxSol * kRsSlotDoubles));
-  V3DM_RS_TRY(rs_grow(r->dSlotOk, r->okCap, nT * kRsMaxSol));
-  V3DM_RS_TRY(rs_grow(r->dCounts, r->countCap, nT));
-  V3DM_RS_TRY(rs_grow(r->dList, r->listCap, nT * kRsMaxSol));
+  V3DM_RS_TRY(rs_grow(r->dSlots, r->slotCap, nR * kRsMaxSol * kRsSlotDoubles));
+  V3DM_RS_TRY(rs_grow(r->dSlotOk, r->okCap, nR * kRsMaxSol));
+  V3DM_RS_TRY(rs_grow(r->dCounts, r->countCap, nR));
+  V3DM_RS_TRY(rs_grow(r->dList, r->listCap, nR * kRsMaxSol));
   V3DM_RS_TRY(rs_grow(r->dListN, r->listNCap, (size_t)nPairs));
-  V3DM_RS_TRY(rs_grow(r->dCost, r->costCap, nT * kRsMaxSol));
-  V3DM_RS_TRY(rs_grow(r->dInl, r->inlCap, nT * kRsMaxSol));
-  V3DM_RS_TRY(rs_grow(r->dBest, r->bestCap, (size_t)nPairs));
-  V3DM_RS_TRY(rs_grow(r->dBestCost, r->bestCostCap, (size_t)nPairs));
+  V3DM_RS_TRY(rs_grow(r->dCost, r->costCap, nR * kRsMaxSol));
+  V3DM_RS_TRY(rs_grow(r->dInl, r->inlCap, nR * kRsMaxSol));
+  {
+    char* st = static_cast<char*>(r->dState);
+    V3DM_RS_TRY(rs_grow(st, r->stateCap, (size_t)nPairs * sizeof(RsState)));
+    r->dState = st;
+  }
+  V3DM_RS_TRY(rs_grow(r->dBestEF, r->bestEFCap, (size_t)nPairs * kRsSlotDoubles));
+  V3DM_RS_TRY(rs_grow(r->dWork, r->workCap, (size_t)2));
+  RsState* state = static_cast<RsState*>(r->dState);
   int launches = 0;
+  V3DM_RS_TRY(cudaMemsetAsync(r->dWork, 0, 2 * sizeof(unsigned long long), r->stream));
   if (nCorrs > 0) {
     k_rs_normalize<<<std::min((nCorrs + 255) / 256, 148 * 16), 256, 0, r->stream>>>(r->dOffsets, nPairs, nCorrs,
                                                                                   dCorrs, r->dInvK, r->dNorm);
     ++launches;
   }
-  const unsigned tBlocks = (unsigned)((nT + 63) / 64);
+  const size_t nT = (size_t)nPairs * nDraw;
   if (draw) {
     k_rs_draw<<<(unsigned)((nT + 255) / 256), 256, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, seed, dSamples);
     ++launches;
   }
-  V3DM_RS_TRY(rs_mark(r, 0));
-  k_rs_hyp<<<tBlocks, 64, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm, r->dInvK, r->dSlots,
-                                           r->dSlotOk, r->dCounts);
-  V3DM_RS_TRY(rs_mark(r, 0));
-  k_rs_compact<<<nPairs, 256, 0, r->stream>>>(nDraw, r->dCounts, r->dList, r->dListN);
-  const unsigned chunks = (unsigned)((nDraw * kRsMaxSol + kRsScoreThreads - 1) / kRsScoreThreads);
-  V3DM_RS_TRY(rs_mark(r, 1));
-  k_rs_score<<<dim3(nPairs, chunks), kRsScoreThreads, 0, r->stream>>>(r->dOffsets, nDraw, dCorrs, r->dList,
-                                                                     r->dListN, r->dSlots, thr2, r->dCost, r->dInl);
-  V3DM_RS_TRY(rs_mark(r, 1));
-  k_rs_select<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, nSamples, r->dCounts,
-                                                           r->dSlotOk, r->dCost, r->dInl, r->dBest, r->dBestCost);
-  k_rs_finish<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm,
-                                                           r->dSlots, r->dBest, r->dBestCost, dOut);
+  k_rs_init<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nSamples, state);
+  ++launches;
+  // rounds of kRsRound samples per pair; pairs whose loop has ended are skipped
+  for (int s0 = 0; s0 < nDraw; s0 += kRsRound) {
+    const int len = std::min(kRsRound, nDraw - s0);
+    V3DM_RS_TRY(rs_mark(r, 0));
+    k_rs_hyp<<<(unsigned)((nR + 63) / 64), 64, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, dSamples,
+                                                                r->dNorm, r->dInvK, state, r->dSlots, r->dSlotOk,
+                                                                r->dCounts);
+    V3DM_RS_TRY(rs_mark(r, 0));
+    k_rs_compact<<<nPairs, kRsRound, 0, r->stream>>>(r->dOffsets, r->dCounts, r->dList, r->dListN, r->dWork);
+    const unsigned chunks = (unsigned)((kRsRound * kRsMaxSol + kRsScoreThreads - 1) / kRsScoreThreads);
+    V3DM_RS_TRY(rs_mark(r, 1));
+    k_rs_score<<<dim3(nPairs, chunks), kRsScoreThreads, 0, r->stream>>>(r->dOffsets, dCorrs, r->dList, r->dListN,
+                                                                       r->dSlots, thr2, r->dCost, r->dInl);
+    V3DM_RS_TRY(rs_mark(r, 1));
+    k_rs_select<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts,
+                                                             r->dSlotOk, r->dCost, r->dInl, r->dSlots, state,
+                                                             r->dBestEF);
+    launches += 4;
+  }
+  k_rs_finish<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm, state,
+                                                           r->dBestEF, dOut);
   V3DM_RS_TRY(cudaMemsetAsync(dNIn, 0, (size_t)nPairs * sizeof(int32_t), r->stream));
-  launches += 5;
+  launches += 1;
   if (nCorrs > 0) {
     k_rs_inliers<<<std::min((nCorrs + 255) / 256, 148 * 16), 256, 0, r->stream>>>(
         r->dOffsets, nPairs, nCorrs, dCorrs, dOut, thr2, dFlags, dNIn);
@@ -516,9 +565,9 @@ int v3dm_ransac_destroy(v3dm_ransac* r) {
   if (!r) return V3DM_OK;
   RsDeviceGuard g(r->device);
   cudaStreamSynchronize(r->stream);
-  void* bufs[] = {r->dOffsets, r->dCorrs, r->dNorm, r->dInvK,  r->dSamples,   r->dSlots, r->dSlotOk, r->dCounts,
-                  r->dList,    r->dListN, r->dCost, r->dInl,   r->dBest,      r->dBestCost, r->dOut, r->dFlags,
-                  r->dNIn};
+  void* bufs[] = {r->dOffsets, r->dCorrs, r->dNorm, r->dInvK, r->dSamples, r->dSlots, r->dSlotOk, r->dCounts,
+                  r->dList,    r->dListN, r->dCost, r->dInl,  r->dState,   r->dBestEF, r->dWork,  r->dOut,
+                  r->dFlags,   r->dNIn};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 2; ++k)
@@ -635,17 +684,10 @@ int v3dm_ransac_candidates(v3dm_ransac* r, long long* nCandidates, long long* nE
   if (!r || !nCandidates || !nEvaluations) return V3DM_ERR_ARG;
   RsDeviceGuard g(r->device);
   V3DM_RS_TRY(cudaStreamSynchronize(r->stream));
-  const int nPairs = r->hOffsets.empty() ? 0 : (int)r->hOffsets.size() - 1;
-  std::vector<int32_t> h((size_t)nPairs);
-  if (nPairs > 0)
-    V3DM_RS_TRY(cudaMemcpy(h.data(), r->dListN, (size_t)nPairs * sizeof(int32_t), cudaMemcpyDeviceToHost));
-  long long c = 0, ev = 0;
-  for (int p = 0; p < nPairs; ++p) {
-    c += h[p];
-    ev += (long long)h[p] * (r->hOffsets[p + 1] - r->hOffsets[p]);
-  }
-  *nCandidates = c;
-  *nEvaluations = ev;
+  unsigned long long w[2] = {0, 0};
+  if (r->dWork) V3DM_RS_TRY(cudaMemcpy(w, r->dWork, sizeof(w), cudaMemcpyDeviceToHost));
+  *nCandidates = (long long)w[0];
+  *nEvaluations = (long long)w[1];
   return V3DM_OK;
 }
 
