@@ -1155,11 +1155,10 @@ def ref_ransac_pairs(off, corrs, K, pairs):
     """The reference loop (its five-point solver and pose recovery, the loop restated) on the given
     pairs with the app's own sample sequence; returns seconds."""
     from oracle import oracle
-    import v3dm
     t = 0.0
     for p in pairs:
         c = corrs[off[p]:off[p + 1]]
-        smp = v3dm.ransac_shuffle_samples(c.shape[0], RS_SAMPLES, 1000 + p)
+        smp = oracle.ref_shuffle_samples(c.shape[0], RS_SAMPLES, 1000 + p)  # the reference's own draws
         t0 = time.perf_counter()
         oracle.ref_ransac(c, K[p, 0], K[p, 1], RS_THR, RS_SAMPLES, smp)
         t += time.perf_counter() - t0
