@@ -91,7 +91,6 @@ V3DM_HD void quad_exp(int k, int& a, int& b, int& c) {
   c = tc[k];
 }
 V3DM_HD int quad_index(int a, int b, int c) {
-#pragma unroll
   for (int k = 0; k < 10; ++k) {
     int qa, qb, qc;
     quad_exp(k, qa, qb, qc);
@@ -101,11 +100,8 @@ V3DM_HD int quad_index(int a, int b, int c) {
 }
 
 V3DM_HD void mul_lin_lin(const double* u, const double* v, double* q) {  // q (10) = u v
-#pragma unroll
   for (int k = 0; k < 10; ++k) q[k] = 0.0;
-#pragma unroll
   for (int i = 0; i < 4; ++i)
-#pragma unroll
     for (int j = 0; j < 4; ++j) {
       int a1, b1, c1, a2, b2, c2;
       lin_exp(i, a1, b1, c1);
@@ -115,9 +111,7 @@ V3DM_HD void mul_lin_lin(const double* u, const double* v, double* q) {  // q (1
 }
 
 V3DM_HD void mul_quad_lin_acc(const double* q, const double* v, double s, double* cub) {  // cub (20) += s q v
-#pragma unroll
   for (int i = 0; i < 10; ++i)
-#pragma unroll
     for (int j = 0; j < 4; ++j) {
       int a1, b1, c1, a2, b2, c2;
       quad_exp(i, a1, b1, c1);

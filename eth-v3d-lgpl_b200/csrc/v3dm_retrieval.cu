@@ -36,15 +36,14 @@ namespace {
 
 constexpr int kRtThreads = 512;
 constexpr int kRtPresenceThreads = 256;
-constexpr int kRtChunks = 8;  // word-upload chunks of a host-input call
 
 struct RtLogs {  // the four logarithms of one image's p0 = nFeatures * (1 / nLeaves)
   double lp0, l1p0, lp1, l1p1;
 };
 
 __global__ void k_rt_presence(const int32_t* __restrict__ offsets, const int32_t* __restrict__ words, int nLeaves,
-                              int w32, uint32_t* __restrict__ bits, int* __restrict__ err, int iBase) {
-  const int i = iBase + blockIdx.x;
+                              int w32, uint32_t* __restrict__ bits, int* __restrict__ err) {
+  const int i = blockIdx.x;
   const int b = offsets[i], e = offsets[i + 1];
   for (int j = b + threadIdx.x; j < e; j += blockDim.x) {
     const int w = words[j];
@@ -138,7 +137,7 @@ __device__ __forceinline__ void rt_add16(RtPlanes& p, const uint32_t (&x)[16]) {
 }
 
 __global__ void __launch_bounds__(kRtThreads, 2)
-k_rt_score(const int32_t* __restrict__ offsets, const int32_t* __restrict__ words, int nLeaves, int iLast, int w32,
+k_rt_score(const int32_t* __restrict__ offsets, const int32_t* __restrict__ words, int nLeaves, int nImages, int w32,
            const uint32_t* __restrict__ bits, const RtLogs* __restrict__ logs, int nBest,
            int32_t* __restrict__ bestDocs, float* __restrict__ bestScores) {
   extern __shared__ unsigned long long rtSh[];
@@ -149,7 +148,7 @@ k_rt_score(const int32_t* __restrict__ offsets, const int32_t* __restrict__ word
   __shared__ unsigned long long shPrefix;
   __shared__ int shRem, shCnt;
 
-  const int i = iLast - blockIdx.x;  // the longest queries first
+  const int i = nImages - 1 - blockIdx.x;  // the longest queries first
   const uint32_t tailMask = (i & 31) ? (1u << (i & 31)) - 1u : 0xffffffffu;  // images before i
   for (int d = threadIdx.x; d < i; d += blockDim.x) kd[d] = 0;
   if (threadIdx.x == 0) shCnt = 0;
@@ -330,9 +329,6 @@ struct v3dm_retrieval {
   int32_t* hOffsets[2] = {nullptr, nullptr};
   cudaEvent_t slotDone[2] = {nullptr, nullptr};
   int slot = 0;
-  // host-input calls: words copied in chunks on copyStream, each chunk's kernels start when it lands
-  cudaStream_t copyStream = nullptr;
-  cudaEvent_t chunkIn[kRtChunks] = {};
   // CUDA-event timing of the two kernels (v3dm_retrieval_profile): pending event pairs
   bool profile = false;
   std::vector<cudaEvent_t> prof[2];
@@ -384,12 +380,10 @@ cudaError_t rt_mark(v3dm_retrieval* r, int k) {
   return cudaEventRecord(ev, r->stream);
 }
 
-// Both kernels on r's stream; words in device memory, or copied there from hWords (when not
-// NULL) in chunks of images on copyStream, each chunk's bitmap rows and queries launched as soon
-// as its words have landed (query i needs the words of images 0..i only).  The host computes the
-// logarithms while the first words are copied and the bitmap is built.
+// Both kernels on r's stream; words in device memory.  The host computes the logarithms while
+// the bitmap is built.
 int rt_enqueue(v3dm_retrieval* r, int nLeaves, int nImages, const int32_t* offsets, const int32_t* dWords,
-               const int32_t* hWords, double pMatch, int nBest, int32_t* dDocs, float* dScores) {
+               double pMatch, int nBest, int32_t* dDocs, float* dScores) {
   const int w32 = (nImages + 31) / 32;
   const size_t bitWords = ((size_t)nLeaves + 1) * w32;  // the last row stays zero
   if (bitWords > r->bitsCap || nImages + 1 > r->imagesCap) V3DM_RT_TRY(cudaStreamSynchronize(r->stream));
@@ -425,63 +419,26 @@ int rt_enqueue(v3dm_retrieval* r, int nLeaves, int nImages, const int32_t* offse
                               cudaMemcpyHostToDevice, r->stream));
   V3DM_RT_TRY(cudaMemsetAsync(r->dBits, 0, bitWords * sizeof(uint32_t), r->stream));
   V3DM_RT_TRY(cudaMemsetAsync(r->dErr, 0, sizeof(int), r->stream));
-  // chunks of images with about equal word counts (one chunk for device words)
-  int bounds[kRtChunks + 1];
-  int nChunks = 1;
-  bounds[0] = 0;
-  bounds[1] = nImages;
-  if (hWords) {
-    nChunks = std::min(kRtChunks, nImages);
-    const long long total = offsets[nImages];
-    int i = 0;
-    for (int c = 1; c < nChunks; ++c) {
-      const long long target = total * c / nChunks;
-      while (i < nImages && offsets[i] < target) ++i;
-      bounds[c] = std::max(i, bounds[c - 1]);
-    }
-    bounds[nChunks] = nImages;
-    V3DM_RT_TRY(cudaEventRecord(r->chunkIn[0], r->stream));  // the copies follow the staging above
-    V3DM_RT_TRY(cudaStreamWaitEvent(r->copyStream, r->chunkIn[0], 0));
-    for (int c = 0; c < nChunks; ++c) {
-      const size_t w0 = (size_t)offsets[bounds[c]], w1 = (size_t)offsets[bounds[c + 1]];
-      if (w1 > w0)
-        V3DM_RT_TRY(cudaMemcpyAsync(const_cast<int32_t*>(dWords) + w0, hWords + w0, (w1 - w0) * sizeof(int32_t),
-                                    cudaMemcpyHostToDevice, r->copyStream));
-      V3DM_RT_TRY(cudaEventRecord(r->chunkIn[c], r->copyStream));
-    }
+  V3DM_RT_TRY(rt_mark(r, 0));
+  k_rt_presence<<<nImages, kRtPresenceThreads, 0, r->stream>>>(r->dOffsets, dWords, nLeaves, w32, r->dBits, r->dErr);
+  V3DM_RT_TRY(cudaGetLastError());
+  V3DM_RT_TRY(rt_mark(r, 0));
+  // p0 = nFeatures * (1 / nLeaves) and its logarithms, in the expressions of v3d_voctree.h:252-265
+  const double normalizer = 1.0 / (double)nLeaves;
+  for (int i = 0; i < nImages; ++i) {
+    const double p0 = (offsets[i + 1] - offsets[i]) * normalizer;
+    const double p1 = std::min(1.0, p0 + pMatch);
+    hLogs[i] = RtLogs{std::log(p0), std::log(1.0 - p0), std::log(p1), std::log(1.0 - p1)};
   }
+  V3DM_RT_TRY(cudaMemcpyAsync(r->dLogs, hLogs, (size_t)nImages * sizeof(RtLogs), cudaMemcpyHostToDevice, r->stream));
+  V3DM_RT_TRY(cudaEventRecord(r->slotDone[s], r->stream));
   const size_t smem = (size_t)nBest * sizeof(unsigned long long) + (size_t)nImages * sizeof(uint32_t);
   V3DM_RT_TRY(cudaFuncSetAttribute(k_rt_score, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  for (int c = 0; c < nChunks; ++c) {
-    const int i0 = bounds[c], i1 = bounds[c + 1];
-    if (hWords) V3DM_RT_TRY(cudaStreamWaitEvent(r->stream, r->chunkIn[c], 0));
-    if (i1 > i0) {
-      V3DM_RT_TRY(rt_mark(r, 0));
-      k_rt_presence<<<i1 - i0, kRtPresenceThreads, 0, r->stream>>>(r->dOffsets, dWords, nLeaves, w32, r->dBits,
-                                                                   r->dErr, i0);
-      V3DM_RT_TRY(cudaGetLastError());
-      V3DM_RT_TRY(rt_mark(r, 0));
-    }
-    if (c == 0) {
-      // p0 = nFeatures * (1 / nLeaves) and its logarithms, in the expressions of v3d_voctree.h:252-265
-      const double normalizer = 1.0 / (double)nLeaves;
-      for (int i = 0; i < nImages; ++i) {
-        const double p0 = (offsets[i + 1] - offsets[i]) * normalizer;
-        const double p1 = std::min(1.0, p0 + pMatch);
-        hLogs[i] = RtLogs{std::log(p0), std::log(1.0 - p0), std::log(p1), std::log(1.0 - p1)};
-      }
-      V3DM_RT_TRY(cudaMemcpyAsync(r->dLogs, hLogs, (size_t)nImages * sizeof(RtLogs), cudaMemcpyHostToDevice,
-                                  r->stream));
-      V3DM_RT_TRY(cudaEventRecord(r->slotDone[s], r->stream));
-    }
-    if (i1 > i0) {
-      V3DM_RT_TRY(rt_mark(r, 1));
-      k_rt_score<<<i1 - i0, kRtThreads, smem, r->stream>>>(r->dOffsets, dWords, nLeaves, i1 - 1, w32, r->dBits,
-                                                           r->dLogs, nBest, dDocs, dScores);
-      V3DM_RT_TRY(cudaGetLastError());
-      V3DM_RT_TRY(rt_mark(r, 1));
-    }
-  }
+  V3DM_RT_TRY(rt_mark(r, 1));
+  k_rt_score<<<nImages, kRtThreads, smem, r->stream>>>(r->dOffsets, dWords, nLeaves, nImages, w32, r->dBits, r->dLogs,
+                                                       nBest, dDocs, dScores);
+  V3DM_RT_TRY(cudaGetLastError());
+  V3DM_RT_TRY(rt_mark(r, 1));
   V3DM_RT_TRY(cudaMemcpyAsync(r->hErr, r->dErr, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
   return V3DM_OK;
 }
@@ -506,21 +463,14 @@ int v3dm_retrieval_create(v3dm_retrieval** out, int device) {
       cudaMalloc(reinterpret_cast<void**>(&r->dErr), sizeof(int)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->hErr), sizeof(int)) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->slotDone[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&r->slotDone[1], cudaEventDisableTiming) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaEventCreateWithFlags(&r->slotDone[1], cudaEventDisableTiming) != cudaSuccess) {
     if (r->slotDone[0]) cudaEventDestroy(r->slotDone[0]);
-    if (r->slotDone[1]) cudaEventDestroy(r->slotDone[1]);
     if (r->stream) cudaStreamDestroy(r->stream);
     if (r->dErr) cudaFree(r->dErr);
     if (r->hErr) cudaFreeHost(r->hErr);
     delete r;
     return V3DM_ERR_CUDA;
   }
-  for (int c = 0; c < kRtChunks; ++c)
-    if (cudaEventCreateWithFlags(&r->chunkIn[c], cudaEventDisableTiming) != cudaSuccess) {
-      v3dm_retrieval_destroy(r);
-      return V3DM_ERR_CUDA;
-    }
   *r->hErr = 0;
   *out = r;
   return V3DM_OK;
@@ -544,12 +494,6 @@ int v3dm_retrieval_destroy(v3dm_retrieval* r) {
     cudaEventDestroy(r->slotDone[k]);
     for (cudaEvent_t ev : r->prof[k]) cudaEventDestroy(ev);
   }
-  for (int c = 0; c < kRtChunks; ++c)
-    if (r->chunkIn[c]) cudaEventDestroy(r->chunkIn[c]);
-  if (r->copyStream) {
-    cudaStreamSynchronize(r->copyStream);
-    cudaStreamDestroy(r->copyStream);
-  }
   cudaStreamDestroy(r->stream);
   delete r;
   return V3DM_OK;
@@ -570,7 +514,7 @@ int v3dm_retrieval_binomial_device(v3dm_retrieval* r, int nLeaves, int nImages, 
   if (nImages == 0) return V3DM_OK;
   if ((offsets[nImages] > 0 && !d_words) || !d_bestDocs || !d_bestScores) return V3DM_ERR_ARG;
   RtDeviceGuard g(r->device);
-  return rt_enqueue(r, nLeaves, nImages, offsets, d_words, nullptr, pMatch, nBest, d_bestDocs, d_bestScores);
+  return rt_enqueue(r, nLeaves, nImages, offsets, d_words, pMatch, nBest, d_bestDocs, d_bestScores);
 }
 
 int v3dm_retrieval_profile(v3dm_retrieval* r, int enable) {
@@ -631,8 +575,9 @@ int v3dm_retrieval_binomial(v3dm_retrieval* r, int nLeaves, int nImages, const i
     V3DM_RT_TRY(cudaMalloc(reinterpret_cast<void**>(&r->dScores), nOut * sizeof(float)));
     r->bestCap = nOut;
   }
-  st = rt_enqueue(r, nLeaves, nImages, offsets, r->dWords, nWords > 0 ? words : nullptr, pMatch, nBest, r->dDocs,
-                  r->dScores);
+  if (nWords > 0)
+    V3DM_RT_TRY(cudaMemcpyAsync(r->dWords, words, nWords * sizeof(int32_t), cudaMemcpyHostToDevice, r->stream));
+  st = rt_enqueue(r, nLeaves, nImages, offsets, r->dWords, pMatch, nBest, r->dDocs, r->dScores);
   if (st != V3DM_OK) return st;
   V3DM_RT_TRY(cudaMemcpyAsync(bestDocs, r->dDocs, nOut * sizeof(int32_t), cudaMemcpyDeviceToHost, r->stream));
   V3DM_RT_TRY(cudaMemcpyAsync(bestScores, r->dScores, nOut * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
