@@ -1260,8 +1260,9 @@ def run_ransac(args, ws, rank, local):
     hyp_ms, hyp_n = r.profile_read(0)
     score_ms, score_n = r.profile_read(1)
     r.profile(False)
-    hyp_ms /= max(hyp_n, 1)
-    score_ms /= max(score_n, 1)
+    rounds = hyp_n // max(args.steps, 1)  # launches of each kernel per call (one per round)
+    hyp_ms /= args.steps  # per call, all rounds
+    score_ms /= args.steps
     n_cand, n_evals = r.candidates()  # candidates scored and their Sampson evaluations, last call
     res = r.essential(off, corrs, K, RS_THR, RS_SAMPLES, seed=args.seed, flags=False)
     np.testing.assert_array_equal(res["models"], dm.cpu().numpy())
@@ -1290,13 +1291,15 @@ def run_ransac(args, ws, rank, local):
         "dtype": "f64", "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, n_corrs),
         "pose_recovered": rot_ok,
         "candidates": n_cand, "sampson_evaluations": n_evals,
-        "kernels_ms": {"k_rs_hyp (five-point, all samples)": hyp_ms, "k_rs_score (costs, all candidates)": score_ms},
+        "kernels_ms_per_call": {"k_rs_hyp (five-point solutions)": hyp_ms, "k_rs_score (costs of the candidates)": score_ms,
+                                "rounds": rounds},
         "roofline": {"bound": "fp64", "achieved": RS_FLOPS_PER_EVAL * n_evals / (score_ms * 1e-3) / 1e12,
                      "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
                      "frac": RS_FLOPS_PER_EVAL * n_evals / (score_ms * 1e-3) / 1e12 / FP64_NOMINAL_TFLOPS,
                      "traffic": None, "peak_src": "nominal B200 FP64 (no measured FP64 peak on this pool)",
-                     "kernel_ms": score_ms, "flops_per_launch": RS_FLOPS_PER_EVAL * n_evals,
-                     "kernel": f"k_rs_score ({RS_FLOPS_PER_EVAL} double operations per Sampson evaluation)"},
+                     "kernel_ms": score_ms, "flops_per_call": RS_FLOPS_PER_EVAL * n_evals,
+                     "kernel": f"k_rs_score, all rounds of one call ({RS_FLOPS_PER_EVAL} double operations per "
+                               "Sampson evaluation)"},
         "e2e": {"value": ws * n_pairs * 1000.0 / ms_e2e, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(corrs.nbytes + off.nbytes + K.nbytes),
                 "d2h_bytes_per_step": int(n_pairs * (31 * 8 + 4) + n_corrs)},

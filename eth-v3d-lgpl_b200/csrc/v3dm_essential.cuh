@@ -444,6 +444,30 @@ V3DM_HD double sampson(const double* F, float px, float py, float qx, float qy) 
   return ddiv(num, denom);
 }
 
+// The truncated Sampson term min(d, thr2) of sampsonEpipolarError(corr, F) = d and whether
+// d < thr2, for a correspondence given in double (the float positions converted): the division
+// is skipped when num > thr2 * denom * (1 + 1e-12), where the rounded quotient is certainly >= thr2
+// (the margin is far above the rounding of the comparison's product), so the result is that of
+// the exact expression in every case.
+V3DM_HD double sampson_truncated(const double* F, double p0, double p1, double q0, double q1, double thr2,
+                                 bool& inlier) {
+  const double Fp0 = dadd(dadd(F[2], dmul(F[0], p0)), dmul(F[1], p1));
+  const double Fp1 = dadd(dadd(F[5], dmul(F[3], p0)), dmul(F[4], p1));
+  const double Fp2 = dadd(dadd(F[8], dmul(F[6], p0)), dmul(F[7], p1));
+  const double Ftq0 = dadd(dadd(F[6], dmul(F[0], q0)), dmul(F[3], q1));
+  const double Ftq1 = dadd(dadd(F[7], dmul(F[1], q0)), dmul(F[4], q1));
+  const double tmp = dadd(dadd(dmul(q0, Fp0), dmul(q1, Fp1)), Fp2);
+  const double num = dmul(tmp, tmp);
+  const double denom = dadd(dadd(dadd(dmul(Fp0, Fp0), dmul(Fp1, Fp1)), dmul(Ftq0, Ftq0)), dmul(Ftq1, Ftq1));
+  if (num > thr2 * denom * (1.0 + 1e-12)) {  // denom > 0 here; the quotient is >= thr2
+    inlier = false;
+    return thr2;
+  }
+  const double d = ddiv(num, denom);
+  inlier = d < thr2;
+  return thr2 < d ? thr2 : d;  // std::min(d, thr2)
+}
+
 // C = A B for row-major 3 x 3 matrices, each entry summed over k = 0, 1, 2 in order.
 V3DM_HD void mat3_mul(const double* A, const double* B, double* C) {
   for (int i = 0; i < 3; ++i)

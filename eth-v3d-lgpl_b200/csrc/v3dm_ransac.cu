@@ -247,7 +247,7 @@ k_rs_score(const int32_t* __restrict__ offsets, const float4* __restrict__ corrs
   const int h = blockIdx.y * kRsScoreThreads + threadIdx.x;
   const int H = listN[p];
   if (blockIdx.y * kRsScoreThreads >= H) return;  // uniform over the CTA
-  __shared__ float4 st[kRsStage];
+  __shared__ double4 st[kRsStage];  // the positions converted once per CTA
   const int b = offsets[p], n = offsets[p + 1] - b;
   const bool mine = h < H;
   long long slot = 0;
@@ -261,14 +261,17 @@ k_rs_score(const int32_t* __restrict__ offsets, const float4* __restrict__ corrs
   for (int c0 = 0; c0 < n; c0 += kRsStage) {
     const int m = min(kRsStage, n - c0);
     __syncthreads();
-    for (int k = threadIdx.x; k < m; k += blockDim.x) st[k] = corrs[b + c0 + k];
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+      const float4 c = corrs[b + c0 + k];
+      st[k] = make_double4(c.x, c.y, c.z, c.w);
+    }
     __syncthreads();
     if (mine)
       for (int k = 0; k < m; ++k) {
-        const float4 c = st[k];
-        const double d = ess::sampson(F, c.x, c.y, c.z, c.w);
-        sum = ess::dadd(sum, thr2 < d ? thr2 : d);  // std::min(d, thr2)
-        cnt += d < thr2;
+        const double4 c = st[k];
+        bool in;
+        sum = ess::dadd(sum, ess::sampson_truncated(F, c.x, c.y, c.z, c.w, thr2, in));
+        cnt += in;
       }
   }
   if (mine) {
