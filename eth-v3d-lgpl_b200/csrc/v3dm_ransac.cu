@@ -17,9 +17,9 @@
 //   k_rs_compact    one CTA per pair: the round's candidates in loop order, densely;
 //   k_rs_score      a CTA per (pair, 128 candidates): the pair's correspondences staged in
 //                   shared memory, one candidate per thread, cost and inlier count in double;
-//   k_rs_select     one thread per pair: the loop's sequential rule (strictly lower cost, pose
-//                   consistent, adaptive sample budget) over the round's candidates in loop
-//                   order, its state carried to the next round;
+//   k_rs_select     one warp per pair: the round's candidates staged in shared memory, then the
+//                   loop's sequential rule (strictly lower cost, pose consistent, adaptive sample
+//                   budget) over them in loop order, its state carried to the next round;
 // and at the end
 //   k_rs_finish     pose, error and inlier flags of the chosen candidate.
 // The loop's iterative refinement (mode.iterativeRefinement) is not run.
@@ -289,35 +289,62 @@ __device__ __forceinline__ int rs_budget(double outlierRatio) {
   return (int)N;
 }
 
-// One thread per pair: the loop over this round's samples in order (the rule of
-// reconstruction_common.cpp:177-335 without refinement); the accepted candidate's E and F are kept.
-__global__ void k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
-                            const int8_t* __restrict__ counts, const uint8_t* __restrict__ slotOk,
-                            const double* __restrict__ cost, const int32_t* __restrict__ inl,
-                            const double* __restrict__ slots, RsState* __restrict__ st, double* __restrict__ bestEF) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nPairs) return;
+// One warp per pair: the round's costs, pose flags and inlier counts staged in shared memory by
+// the warp (coalesced), then lane 0 walks the loop over the round's samples in order (the rule of
+// reconstruction_common.cpp:177-335 without refinement); the last accepted candidate's E and F are
+// kept (the warp copies them).
+__global__ void __launch_bounds__(32)
+k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
+            const int8_t* __restrict__ counts, const uint8_t* __restrict__ slotOk, const double* __restrict__ cost,
+            const int32_t* __restrict__ inl, const double* __restrict__ slots, RsState* __restrict__ st,
+            double* __restrict__ bestEF) {
+  const int p = blockIdx.x;
+  const int lane = threadIdx.x;
+  __shared__ double sCost[kRsRound * kRsMaxSol];
+  __shared__ int32_t sInl[kRsRound * kRsMaxSol];
+  __shared__ uint8_t sOk[kRsRound * kRsMaxSol];
+  __shared__ int8_t sCnt[kRsRound];
+  __shared__ int sAccepted;
   RsState s = st[p];
-  if (s.done) return;
-  const int n = offsets[p + 1] - offsets[p];
-  for (int j = 0; j < len; ++j) {
-    if (s.drawn > s.budget) break;
-    ++s.drawn;
-    const long long t = (long long)p * kRsRound + j;
-    const int ns = counts[t];
-    for (int r = 0; r < ns; ++r) {
-      const long long slot = t * kRsMaxSol + r;
-      if (!(cost[slot] < s.minError)) continue;
-      if (!slotOk[slot]) continue;
-      s.minError = cost[slot];
-      s.chosen = s0 + j;
-      for (int k = 0; k < kRsSlotDoubles; ++k) bestEF[(size_t)p * kRsSlotDoubles + k] = slots[slot * kRsSlotDoubles + k];
-      const float frac = (float)(inl[slot] - 5) / (float)(n - 5);
-      s.budget = min(s.budget, rs_budget(1.0 - (double)frac));
+  if (s.done) return;  // uniform over the warp
+  const long long base = (long long)p * kRsRound;
+  for (int j = lane; j < len; j += 32) sCnt[j] = counts[base + j];
+  __syncwarp();
+  for (int idx = lane; idx < len * kRsMaxSol; idx += 32) {
+    const int j = idx / kRsMaxSol, r = idx - j * kRsMaxSol;
+    if (r < sCnt[j]) {
+      sCost[idx] = cost[base * kRsMaxSol + idx];
+      sInl[idx] = inl[base * kRsMaxSol + idx];
+      sOk[idx] = slotOk[base * kRsMaxSol + idx];
     }
   }
-  if (s.drawn > s.budget || s0 + len >= nDraw) s.done = 1;  // the next sample would end the loop
-  st[p] = s;
+  __syncwarp();
+  if (lane == 0) {
+    const int n = offsets[p + 1] - offsets[p];
+    int accepted = -1;
+    for (int j = 0; j < len; ++j) {
+      if (s.drawn > s.budget) break;
+      ++s.drawn;
+      const int ns = sCnt[j];
+      for (int r = 0; r < ns; ++r) {
+        const int idx = j * kRsMaxSol + r;
+        if (!(sCost[idx] < s.minError)) continue;
+        if (!sOk[idx]) continue;
+        s.minError = sCost[idx];
+        s.chosen = s0 + j;
+        accepted = idx;
+        const float frac = (float)(sInl[idx] - 5) / (float)(n - 5);
+        s.budget = min(s.budget, rs_budget(1.0 - (double)frac));
+      }
+    }
+    if (s.drawn > s.budget || s0 + len >= nDraw) s.done = 1;  // the next sample would end the loop
+    st[p] = s;
+    sAccepted = accepted;
+  }
+  __syncwarp();
+  const int accepted = sAccepted;
+  if (accepted >= 0 && lane < kRsSlotDoubles)
+    bestEF[(size_t)p * kRsSlotDoubles + lane] = slots[(base * kRsMaxSol + accepted) * kRsSlotDoubles + lane];
 }
 
 // One thread per pair: E, F, R, T and error of the choice.
@@ -519,9 +546,8 @@ int rs_enqueue(v3dm_ransac* r, int nPairs, int nCorrs, int nDraw, int nSamples, 
     k_rs_score<<<dim3(nPairs, chunks), kRsScoreThreads, 0, r->stream>>>(r->dOffsets, dCorrs, r->dList, r->dListN,
                                                                        r->dSlots, thr2, r->dCost, r->dInl);
     V3DM_RS_TRY(rs_mark(r, 1));
-    k_rs_select<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts,
-                                                             r->dSlotOk, r->dCost, r->dInl, r->dSlots, state,
-                                                             r->dBestEF);
+    k_rs_select<<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
+                                               r->dCost, r->dInl, r->dSlots, state, r->dBestEF);
     launches += 4;
   }
   k_rs_finish<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm, state,
