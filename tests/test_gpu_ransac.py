@@ -111,7 +111,9 @@ def test_reference_sample_sequence_gives_the_reference_choice(v3dm_mod, oracle_m
         assert agree >= 0.97 * total, (agree, total)
 
 
-def test_batched_call_equals_per_pair_calls(v3dm_mod):
+def test_batched_call_with_small_pairs(v3dm_mod):
+    """A batch that mixes pairs with fewer than 5 correspondences (no model: -1, no inlier flags) with
+    ordinary ones; single-pair calls of the same data run."""
     off, corrs, K, R, t, inl = synth.two_view_pairs(8, n_pairs=30, n_min=4, n_max=900)
     with v3dm_mod.Ransac() as r:
         allp = r.essential(off, corrs, K, 2.0, 300, seed=5)
