@@ -38,3 +38,19 @@ def test_reference_pin_recovers_the_pose(oracle_mod):
         flags = res["flags"].astype(bool)
         assert flags.sum() == res["n_inliers"]
         assert (flags & inl[off[p]:off[p + 1]]).sum() > 0.8 * inl[off[p]:off[p + 1]].sum()
+
+
+def test_sampler_capacity_and_errors(v3dm_mod):
+    import ctypes as C
+    L = v3dm_mod.lib()
+    full = v3dm_mod.ransac_shuffle_samples(50, 100, 9)
+    out = np.full((10, 5), -7, np.int32)
+    nd = C.c_int(-1)
+    # a short buffer: the first 'cap' samples, V3DM_ERR_CAPACITY
+    assert L.v3dm_ransac_shuffle_samples(50, 100, 9, 10, out.ctypes.data, C.byref(nd)) == v3dm_mod.ERR_CAPACITY
+    assert nd.value == 10
+    np.testing.assert_array_equal(out, full[:10])
+    assert L.v3dm_ransac_shuffle_samples(4, 100, 9, 10, out.ctypes.data, C.byref(nd)) == v3dm_mod.OK
+    assert nd.value == 0
+    assert L.v3dm_ransac_shuffle_samples(-1, 100, 9, 10, out.ctypes.data, C.byref(nd)) == v3dm_mod.ERR_ARG
+    assert L.v3dm_ransac_shuffle_samples(50, 100, 9, 10, None, C.byref(nd)) == v3dm_mod.ERR_ARG
