@@ -628,6 +628,7 @@ static int rs_check(int nPairs, const int32_t* offsets, const double* K, double 
   for (int p = 0; p < nPairs; ++p)
     if (offsets[p + 1] < offsets[p]) return V3DM_ERR_ARG;
   if ((size_t)nPairs * (size_t)nDraw > (size_t)V3DM_RANSAC_MAX_SAMPLES) return V3DM_ERR_SIZE;
+  if (nPairs > V3DM_RANSAC_MAX_PAIRS) return V3DM_ERR_SIZE;  // a round's buffers: ~184 KB per pair
   return V3DM_OK;
 }
 

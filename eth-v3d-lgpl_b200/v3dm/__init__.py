@@ -852,6 +852,7 @@ class LeafDocuments:
 
 RANSAC_MAX_DRAW = 65536
 RANSAC_MAX_SAMPLES = 4194304
+RANSAC_MAX_PAIRS = 32768
 
 
 def ransac_shuffle_samples(n: int, n_samples: int, seed: int) -> np.ndarray:

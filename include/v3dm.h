@@ -425,6 +425,7 @@ V3DM_API int v3dm_retrieval_pairs(int nImages, int nBest, const int32_t* bestDoc
 typedef struct v3dm_ransac v3dm_ransac;
 #define V3DM_RANSAC_MAX_DRAW 65536
 #define V3DM_RANSAC_MAX_SAMPLES 4194304 /* nPairs x nDraw */
+#define V3DM_RANSAC_MAX_PAIRS 32768     /* pairs per call (the buffers of one round of 128 samples) */
 V3DM_API int v3dm_ransac_create(v3dm_ransac** out, int device);
 V3DM_API int v3dm_ransac_destroy(v3dm_ransac* r);
 V3DM_API int v3dm_ransac_essential(v3dm_ransac* r, int nPairs, const int32_t* offsets, const float* corrs,

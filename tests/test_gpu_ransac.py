@@ -180,5 +180,13 @@ def test_errors(v3dm_mod):
         with pytest.raises(v3dm_mod.V3DMError) as e:
             r.essential(off, corrs, K, 2.0, 10, n_draw=v3dm_mod.RANSAC_MAX_DRAW + 1)
         assert e.value.status == v3dm_mod.ERR_ARG
+        n_big = v3dm_mod.RANSAC_MAX_PAIRS + 1  # pairs per call above the limit (checked before any work)
+        off_big = np.zeros(n_big + 1, np.int32)
+        K_big = np.tile(np.eye(3), (n_big, 2, 1, 1))
+        models = np.empty((1, 31))
+        nin = np.empty(1, np.int32)
+        assert L.v3dm_ransac_essential(r._h, n_big, off_big.ctypes.data, None, K_big.ctypes.data, C.c_double(2.0), 10,
+                                       1, None, C.c_uint64(0), models.ctypes.data, nin.ctypes.data,
+                                       None) == v3dm_mod.ERR_SIZE
         got = r.essential(off, corrs, K, 2.0, 10)  # still usable
         assert got["n_inliers"].shape == (1,)
