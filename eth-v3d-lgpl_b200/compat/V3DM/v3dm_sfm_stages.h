@@ -1,0 +1,167 @@
+// -*- C++ -*-
+// compat/V3DM/v3dm_sfm_stages.h -- two SfM-app stages around the matcher, batched on libv3dm.so,
+// with the apps' own containers:
+//   - retrieveSequence(): the voctree app's retrieval loop (V3D/Apps/SfM/match_using_voctree.cpp:
+//     176-222: LeafDocuments::computeBinomialScores, then insertDocument, for every image) in one
+//     call, filling the same per-image score lists (nBestDocuments entries, best first) and the same
+//     putativePairwiseMatches map (view1 -> set of view2);
+//   - computeRobustOrientationBatch(): computeRobustOrientationMLE
+//     (V3D/Apps/SfM/reconstruction_common.cpp:139-340, RobustOrientationMode() default, i.e. without
+//     the iterative refinement) for many pairs at once; pair p draws its samples as that function
+//     does after srand(seed + p).
+// The result and matrix types are templates: any type with the members of
+// RobustOrientationResult (essential, fundamental, rotation [i][j], translation [k], inliers,
+// error) and correspondences with left.pos[k] / right.pos[k] work, the reference's included.
+// Errors print and exit like the matcher header, or throw std::runtime_error with
+// V3DM_COMPAT_THROW.
+#ifndef V3DM_SFM_STAGES_H
+#define V3DM_SFM_STAGES_H
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "v3dm.h"
+
+namespace V3D_B200 {
+
+namespace detail {
+
+inline void check(int status, const char* what) {
+  if (status == V3DM_OK) return;
+  std::string msg = std::string("V3D_B200 ") + what + ": " + v3dm_status_string(status);
+  if (status == V3DM_ERR_CUDA) msg += std::string(" [") + v3dm_last_error() + "]";
+#ifdef V3DM_COMPAT_THROW
+  throw std::runtime_error(msg);
+#else
+  std::fprintf(stderr, "%s\n", msg.c_str());
+  std::exit(EXIT_FAILURE);
+#endif
+}
+
+}  // namespace detail
+
+// visualWords[i]: the leaf-local words of image i (VocabularyTree::getVisualWord, or
+// v3dm_voctree_quantize_* with V3DM_LEAF_LOCAL); nLeaves = the tree's visualWordCount().
+// scores[i] = the first min(nBestDocuments, i) entries of the app's 'scores' for image i.
+inline void retrieveSequence(int nLeaves, std::vector<std::vector<int> > const& visualWords, double pMatch,
+                             int nBestDocuments, std::vector<std::vector<std::pair<float, int> > >& scores,
+                             std::map<int, std::set<int> >& putativePairwiseMatches, int device = 0) {
+  const int n = (int)visualWords.size();
+  scores.assign(n, std::vector<std::pair<float, int> >());
+  putativePairwiseMatches.clear();
+  if (n == 0 || nBestDocuments < 1) return;
+  std::vector<int32_t> offsets(n + 1, 0), words;
+  for (int i = 0; i < n; ++i) {
+    offsets[i + 1] = offsets[i] + (int32_t)visualWords[i].size();
+    words.insert(words.end(), visualWords[i].begin(), visualWords[i].end());
+  }
+  std::vector<int32_t> docs((size_t)n * nBestDocuments);
+  std::vector<float> sc((size_t)n * nBestDocuments);
+  v3dm_retrieval* r = nullptr;
+  detail::check(v3dm_retrieval_create(&r, device), "retrieveSequence()");
+  const int st = v3dm_retrieval_binomial(r, nLeaves, n, offsets.data(), words.data(), pMatch, nBestDocuments,
+                                         docs.data(), sc.data());
+  v3dm_retrieval_destroy(r);
+  detail::check(st, "retrieveSequence()");
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < nBestDocuments; ++j) {
+      const int d = docs[(size_t)i * nBestDocuments + j];
+      if (d < 0) break;
+      scores[i].push_back(std::make_pair(sc[(size_t)i * nBestDocuments + j], d));
+      putativePairwiseMatches[d].insert(i);
+    }
+}
+
+// corrs[p]: the putative correspondences of pair p; K1[p], K2[p]: its calibrations (indexable as
+// K[i][j]).  res[p] receives the result; pairs with fewer than 6 correspondences (for which the
+// reference draws no sample; it throws below 5) or without a consistent sample get error -1 and no
+// inliers.
+template <typename Corr, typename Mat3, typename Result>
+inline void computeRobustOrientationBatch(std::vector<std::vector<Corr> > const& corrs, std::vector<Mat3> const& K1,
+                                          std::vector<Mat3> const& K2, double inlierThreshold, int nSamples,
+                                          std::vector<Result>& res, unsigned seed, int device = 0) {
+  const int nPairs = (int)corrs.size();
+  res.assign(nPairs, Result());
+  if (nPairs == 0) return;
+  if ((int)K1.size() != nPairs || (int)K2.size() != nPairs)
+    detail::check(V3DM_ERR_ARG, "computeRobustOrientationBatch(): one K1 and one K2 per pair");
+  const int nDraw = nSamples + 1;
+  // the reference's draws per pair; pairs for which it draws nothing (fewer than 6
+  // correspondences) stay out of the batch and get no model
+  std::vector<int> batch;  // pair of each batch entry
+  std::vector<int32_t> samplesAll;
+  for (int p = 0; p < nPairs; ++p) {
+    std::vector<int32_t> s((size_t)nDraw * 5);
+    int nd = 0;
+    detail::check(v3dm_ransac_shuffle_samples((int)corrs[p].size(), nSamples, seed + (unsigned)p, nDraw, s.data(),
+                                              &nd),
+                  "computeRobustOrientationBatch()");
+    if (nd == 0) continue;
+    // a shorter sequence is padded with its last sample: a repeated sample's candidates never
+    // beat the best so far, so the result is that of the sequence itself
+    for (int k = nd; k < nDraw; ++k)
+      for (int j = 0; j < 5; ++j) s[(size_t)5 * k + j] = s[(size_t)5 * (nd - 1) + j];
+    batch.push_back(p);
+    samplesAll.insert(samplesAll.end(), s.begin(), s.end());
+  }
+  for (int p = 0; p < nPairs; ++p) {
+    res[p].error = -1.0;
+    res[p].inliers.clear();
+  }
+  const int nb = (int)batch.size();
+  if (nb == 0) return;
+  std::vector<int32_t> offsets(nb + 1, 0);
+  for (int q = 0; q < nb; ++q) offsets[q + 1] = offsets[q] + (int32_t)corrs[batch[q]].size();
+  std::vector<float> c((size_t)offsets[nb] * 4);
+  std::vector<double> K((size_t)nb * 18);
+  for (int q = 0; q < nb; ++q) {
+    const int p = batch[q];
+    for (size_t i = 0; i < corrs[p].size(); ++i) {
+      float* o = c.data() + 4 * ((size_t)offsets[q] + i);
+      o[0] = corrs[p][i].left.pos[0];
+      o[1] = corrs[p][i].left.pos[1];
+      o[2] = corrs[p][i].right.pos[0];
+      o[3] = corrs[p][i].right.pos[1];
+    }
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        K[(size_t)q * 18 + 3 * a + b] = K1[p][a][b];
+        K[(size_t)q * 18 + 9 + 3 * a + b] = K2[p][a][b];
+      }
+  }
+  std::vector<double> models((size_t)nb * 31);
+  std::vector<int32_t> nIn(nb);
+  std::vector<uint8_t> flags((size_t)offsets[nb] + 1);
+  v3dm_ransac* r = nullptr;
+  detail::check(v3dm_ransac_create(&r, device), "computeRobustOrientationBatch()");
+  const int st = v3dm_ransac_essential(r, nb, offsets.data(), c.data(), K.data(), inlierThreshold, nSamples, nDraw,
+                                       samplesAll.data(), 0, models.data(), nIn.data(), flags.data());
+  v3dm_ransac_destroy(r);
+  detail::check(st, "computeRobustOrientationBatch()");
+  for (int q = 0; q < nb; ++q) {
+    const int p = batch[q];
+    const double* m = models.data() + (size_t)q * 31;
+    if (m[30] < 0.0) continue;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        res[p].essential[a][b] = m[3 * a + b];
+        res[p].fundamental[a][b] = m[9 + 3 * a + b];
+        res[p].rotation[a][b] = m[18 + 3 * a + b];
+      }
+    for (int k = 0; k < 3; ++k) res[p].translation[k] = m[27 + k];
+    res[p].error = m[30];
+    for (int i = 0; i < (int)corrs[p].size(); ++i)
+      if (flags[(size_t)offsets[q] + i]) res[p].inliers.push_back(i);
+  }
+}
+
+}  // namespace V3D_B200
+
+#endif  // V3DM_SFM_STAGES_H

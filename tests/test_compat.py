@@ -90,3 +90,30 @@ def test_match_using_voctree_calls(compat_bin, v3dm_mod, oracle_mod, tmp_path):
     ids = np.frombuffer(fout.read_bytes(), np.int32)
     np.testing.assert_array_equal(ids[:992], oracle_mod.voctree(10, 3, nodes, keys[:992], True))
     assert np.all(ids[992:] == -1)
+
+
+@pytest.fixture(scope="module")
+def stages_bin(tmp_path_factory, v3dm_mod):
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    out = tmp_path_factory.mktemp("stages") / "compat_stages"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", str(PKG / "compat"), "-I", str(ROOT / "include"),
+           str(ROOT / "tests" / "compat_stages.cpp"), "-o", str(out), "-L", str(PKG), "-lv3dm", f"-Wl,-rpath,{PKG}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return out
+
+
+def test_stages_header_compiles_and_links(stages_bin):
+    """compat/V3DM/v3dm_sfm_stages.h (retrieval loop and robust orientation of many pairs) with the
+    apps' member names."""
+    assert stages_bin.exists()
+
+
+@pytest.mark.parametrize("mode,who", [("r", "computeRobustOrientationBatch()"), ("w", "retrieveSequence()")])
+def test_stages_fail_loudly_without_gpu(stages_bin, mode, who):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = subprocess.run([str(stages_bin), mode], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 1
+    assert f"V3D_B200 {who}: no sm_100" in p.stderr
