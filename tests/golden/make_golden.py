@@ -4,6 +4,7 @@
     python tests/golden/make_golden.py match [outdir]     # GPU: V3D_CUDA::SIFT_Matching
     python tests/golden/make_golden.py features [outdir]  # CPU: V3D::serializeDataToFile / FromFile
     python tests/golden/make_golden.py retrieval [outdir] # CPU: V3D::LeafDocuments binomial scores
+    python tests/golden/make_golden.py ransac [outdir]    # CPU: five-point solver, robust orientation loop
 
 voctree: the reference's CPU vocabulary tree (V3D/Base/v3d_vocabularytree.h, built from the
 reference headers into oracle/_ref/libv3dref_voctree.so by `make -C oracle ref`), leaf-local
@@ -22,6 +23,11 @@ insertDocument) on the reference's LeafDocuments (oracle/_ref/libv3dref_retrieva
 V3D/Base/v3d_voctree.h), on seeded visual-word sequences (v3dm.synth.sequence_words) and hand-made
 edge cases: an empty image, identical images (equal scores, ranked by index), repeated words,
 n_best above the image count, pMatch 0, a query whose every word is unseen.
+
+ransac: the reference's computeEssentialsFromFiveCorrs on 300 normalised samples (half from a true
+pose, half random), and its relativePoseFromEssential + the loop of computeRobustOrientationMLE
+(oracle/_ref/libv3dref_ransac.so, from V3D/Geometry/v3d_poseutilities.cpp) on 6 synthetic pairs with
+the reference's own sample draws (srand(seed), std::random_shuffle).
 
 Inputs are SIFT-like uint8 descriptors (values u/512 handed to the reference as floats) from
 v3dm.synth, stored in the fixtures together with the outputs, so the fixtures stand alone.
@@ -177,9 +183,56 @@ def make_retrieval(out: Path) -> None:
     print("wrote", out / "retrieval_ref.npz")
 
 
+def make_ransac(out: Path) -> None:
+    if not oracle.ref_ransac_available():
+        raise SystemExit("oracle/_ref/libv3dref_ransac.so missing: run `make -C oracle ref` first")
+    rng = np.random.default_rng(77)
+    pts, sols, counts = [], [], []
+    for t in range(300):
+        if t % 2 == 0:
+            v = rng.normal(size=3) * 0.3
+            th = np.linalg.norm(v)
+            k = v / th
+            Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+            R = np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * Kx @ Kx
+            X = np.c_[rng.uniform(-1, 1, (5, 2)), rng.uniform(3, 6, 5)]
+            p = X[:, :2] / X[:, 2:]
+            Y = (R @ X.T).T + rng.normal(size=3)
+            q = Y[:, :2] / Y[:, 2:]
+        else:
+            p = rng.uniform(-0.5, 0.5, (5, 2))
+            q = rng.uniform(-0.5, 0.5, (5, 2))
+        row = np.r_[p[:, 0], p[:, 1], q[:, 0], q[:, 1]]
+        E = oracle.ref_five_point(row[:5], row[5:10], row[10:15], row[15:])
+        E10 = np.zeros((10, 3, 3))
+        E10[:len(E)] = E
+        pts.append(row)
+        sols.append(E10)
+        counts.append(len(E))
+    arrays = {"fp_pts": np.array(pts), "fp_E": np.array(sols), "fp_counts": np.array(counts, np.int32)}
+    off, corrs, K, R, t, inl = synth.two_view_pairs(78, n_pairs=6, n_min=200, n_max=1200)
+    models, nins, chosen, samples, flags = [], [], [], [], []
+    for p in range(6):
+        c = corrs[off[p]:off[p + 1]]
+        s = oracle.ref_shuffle_samples(c.shape[0], 1000, 500 + p)
+        res = oracle.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, s)
+        models.append(res["model"])
+        nins.append(res["n_inliers"])
+        chosen.append(res["chosen"])
+        samples.append(s)
+        flags.append(res["flags"])
+    arrays.update(rs_offsets=off, rs_corrs=corrs, rs_K=K, rs_models=np.array(models),
+                  rs_n_inliers=np.array(nins, np.int32), rs_chosen=np.array(chosen, np.int32),
+                  rs_flags=np.concatenate(flags), rs_seeds=np.arange(500, 506, dtype=np.int32))
+    for p in range(6):
+        arrays[f"rs_samples_{p}"] = samples[p]
+    np.savez_compressed(out / "ransac_ref.npz", **arrays)
+    print("wrote", out / "ransac_ref.npz", "solutions", int(np.sum(counts)), "chosen", chosen)
+
+
 def main(argv):
     makers = {"voctree": make_voctree, "match": make_match, "features": make_features,
-              "retrieval": make_retrieval}
+              "retrieval": make_retrieval, "ransac": make_ransac}
     if len(argv) < 2 or argv[1] not in makers:
         raise SystemExit(__doc__)
     out = Path(argv[2]) if len(argv) > 2 else HERE

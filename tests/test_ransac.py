@@ -54,3 +54,35 @@ def test_sampler_capacity_and_errors(v3dm_mod):
     assert nd.value == 0
     assert L.v3dm_ransac_shuffle_samples(-1, 100, 9, 10, out.ctypes.data, C.byref(nd)) == v3dm_mod.ERR_ARG
     assert L.v3dm_ransac_shuffle_samples(50, 100, 9, 10, None, C.byref(nd)) == v3dm_mod.ERR_ARG
+
+
+def _fixture():
+    from pathlib import Path
+    return np.load(Path(__file__).resolve().parent / "golden" / "ransac_ref.npz")
+
+
+def test_sampler_equals_the_fixture_draws(v3dm_mod):
+    """The committed fixture holds the reference's own draws (srand + std::random_shuffle); the
+    library's sampler reproduces them without the reference build."""
+    z = _fixture()
+    off = z["rs_offsets"]
+    for p in range(6):
+        got = v3dm_mod.ransac_shuffle_samples(int(off[p + 1] - off[p]), 1000, int(z["rs_seeds"][p]))
+        np.testing.assert_array_equal(got, z[f"rs_samples_{p}"])
+
+
+def test_reference_pin_reproduces_the_fixture(oracle_mod):
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    z = _fixture()
+    pts, E, cnt = z["fp_pts"], z["fp_E"], z["fp_counts"]
+    for t in range(0, pts.shape[0], 7):
+        got = oracle_mod.ref_five_point(pts[t, :5], pts[t, 5:10], pts[t, 10:15], pts[t, 15:])
+        assert len(got) == cnt[t]
+        np.testing.assert_array_equal(got, E[t, :cnt[t]])
+    off, corrs, K = z["rs_offsets"], z["rs_corrs"], z["rs_K"]
+    for p in range(6):
+        res = oracle_mod.ref_ransac(corrs[off[p]:off[p + 1]], K[p, 0], K[p, 1], 2.0, 1000, z[f"rs_samples_{p}"])
+        assert res["chosen"] == z["rs_chosen"][p] and res["n_inliers"] == z["rs_n_inliers"][p]
+        np.testing.assert_array_equal(res["model"], z["rs_models"][p])
+        np.testing.assert_array_equal(res["flags"], z["rs_flags"][off[p]:off[p + 1]])
