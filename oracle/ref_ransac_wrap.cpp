@@ -5,9 +5,10 @@
 // INFRASTRUCTURE ONLY: the parity pin and the timed CPU baseline of the RANSAC workload.
 //
 // reconstruction_common.cpp itself does not build from a few files (its header needs the apps'
-// SQLite database classes), so ref_ransac restates its loop (mode.iterativeRefinement = false,
-// the RobustOrientationMode() default) on the reference's own solver, pose recovery, matrix
-// inverse and products, with the samples given rather than drawn; ref_shuffle_samples draws them
+// SQLite database classes), so ref_ransac_mode restates its loop -- with or without
+// mode.iterativeRefinement, whose refinement is the reference's own refineRelativePose -- on the
+// reference's own solver, pose recovery, matrix inverse and products, with the samples given rather
+// than drawn; ref_ransac is the default mode (no refinement); ref_shuffle_samples draws the samples
 // the way that loop does (srand(seed), std::random_shuffle, consecutive 5-tuples).
 #include <algorithm>
 #include <cmath>
@@ -105,11 +106,14 @@ int ref_shuffle_samples(int N, int nSamples, unsigned seed, int cap, int* sample
   return 0;
 }
 
-// The loop of computeRobustOrientationMLE without refinement, on the given samples (nDraw of
-// them, in order).  model: E 9, F 9, R 9, T 3, error (-1 when nothing was accepted); *nInliers
-// and flags (N bytes) from the chosen F; *chosen = sample * 10 + solution index, or -1.
-int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold, int nSamples,
-               int nDraw, const int* samples, double* model, int* nInliers, unsigned char* flags, int* chosen) {
+// The loop of computeRobustOrientationMLE on the given samples (nDraw of them, in order), with
+// (refine != 0) or without mode.iterativeRefinement (reconstruction_common.cpp:255-305: the
+// accepted pose refined by refineRelativePose on the inliers of its F, then E, F, cost and inlier
+// count from the refined pose).  model: E 9, F 9, R 9, T 3, error (-1 when nothing was accepted);
+// *nInliers and flags (N bytes) from the chosen F; *chosen = sample * 10 + solution index, or -1.
+int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold,
+                    int nSamples, int nDraw, const int* samples, int refine, double* model, int* nInliers,
+                    unsigned char* flags, int* chosen) {
   int const minSize = 5;
   double const sqrInlierThreshold = inlierThreshold * inlierThreshold;
   for (int k = 0; k < 30; ++k) model[k] = 0.0;
@@ -159,6 +163,33 @@ int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, do
         Matrix3x3d R;
         Vector3d t;
         if (!relativePoseFromEssential(Es[r], 5, x1, y1, x2, y2, R, t)) continue;
+        if (refine) {
+          std::vector<Vector2d> left, right;
+          for (int i = 0; i < N; ++i)
+            if (sampson(fund, corrs[4 * i], corrs[4 * i + 1], corrs[4 * i + 2], corrs[4 * i + 3]) <
+                sqrInlierThreshold) {
+              Vector2d l, q;
+              l[0] = corrs[4 * i];
+              l[1] = corrs[4 * i + 1];
+              q[0] = corrs[4 * i + 2];
+              q[1] = corrs[4 * i + 3];
+              left.push_back(l);
+              right.push_back(q);
+            }
+          refineRelativePose(left, right, mat(K1), mat(K2), R, t, inlierThreshold);
+          Matrix3x3d const E_refined = computeEssentialFromRelativePose(R, t);
+          Matrix3x3d const F_refined = invK2_t * E_refined * invK1;
+          double curError_refined = 0;
+          nIn = 0;
+          for (int i = 0; i < N; ++i) {
+            double const dist = sampson(F_refined, corrs[4 * i], corrs[4 * i + 1], corrs[4 * i + 2], corrs[4 * i + 3]);
+            curError_refined += std::min(dist, sqrInlierThreshold);
+            if (dist < sqrInlierThreshold) ++nIn;
+          }
+          fund = F_refined;
+          Es[r] = E_refined;
+          curError = std::min(curError, curError_refined);
+        }
         minError = curError;
         put(Es[r], model);
         put(fund, model + 9);
@@ -182,6 +213,12 @@ int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, do
   }
   *nInliers = n;
   return 0;
+}
+
+int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold, int nSamples,
+               int nDraw, const int* samples, double* model, int* nInliers, unsigned char* flags, int* chosen) {
+  return ref_ransac_mode(N, corrs, K1, K2, inlierThreshold, nSamples, nDraw, samples, 0, model, nInliers, flags,
+                         chosen);
 }
 
 }  // extern "C"

@@ -86,3 +86,21 @@ def test_reference_pin_reproduces_the_fixture(oracle_mod):
         assert res["chosen"] == z["rs_chosen"][p] and res["n_inliers"] == z["rs_n_inliers"][p]
         np.testing.assert_array_equal(res["model"], z["rs_models"][p])
         np.testing.assert_array_equal(res["flags"], z["rs_flags"][off[p]:off[p + 1]])
+
+
+def test_reference_pin_with_refinement(oracle_mod):
+    """The pin's refined mode (the apps' mode.iterativeRefinement: the reference's
+    refineRelativePose on each accepted pose) runs and keeps the pose; the default mode is the
+    fixture's."""
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    off, corrs, K, R, t, inl = synth.two_view_pairs(12, n_pairs=3, n_min=300, n_max=700, inlier_min=0.5,
+                                                    inlier_max=0.7)
+    for p in range(3):
+        c = corrs[off[p]:off[p + 1]]
+        smp = oracle_mod.ref_shuffle_samples(c.shape[0], 1000, 40 + p)
+        plain = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, smp)
+        refined = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, smp, refine=True)
+        assert refined["chosen"] >= 0 and plain["chosen"] >= 0
+        assert np.linalg.norm(refined["model"][18:27].reshape(3, 3) - R[p]) < 0.05
+        assert refined["model"][30] <= plain["model"][30] * 1.05
