@@ -102,3 +102,15 @@ def test_pair_table_errors(v3dm_mod):
     bad = np.array([[-1], [1]], np.int32)  # image 1 cannot retrieve itself
     assert L.v3dm_retrieval_pairs(2, 1, bad.ctypes.data, 0, None, C.byref(n)) == v3dm_mod.ERR_ARG
     assert L.v3dm_retrieval_pairs(2, 0, docs.ctypes.data, 0, None, C.byref(n)) == v3dm_mod.ERR_ARG
+
+
+@pytest.mark.parametrize("p_match,n_best,n_min,n_max", [(0.0, 3, 1, 30), (0.3, 60, 1, 20), (0.1, 1, 1, 1),
+                                                        (0.05, 7, 100, 400)])
+def test_oracle_matches_reference_varied(oracle_mod, p_match, n_best, n_min, n_max):
+    """pMatch 0 and 0.3, nBest above the image count, images of a single word."""
+    if not oracle_mod.ref_retrieval_available():
+        pytest.skip("reference LeafDocuments not built (oracle/_ref)")
+    off, w = synth.sequence_words(int(p_match * 100) + n_best, n_images=45, n_leaves=2000, n_min=n_min, n_max=n_max,
+                                  window=4, zipf=0.9)
+    exp = oracle_mod.ref_retrieval(2000, off, w, p_match, n_best)
+    _same(*oracle_mod.retrieval(2000, off, w, p_match, n_best), *exp)
