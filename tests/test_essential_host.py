@@ -1,0 +1,88 @@
+"""The library's five-point solver and pose test (eth-v3d-lgpl_b200/csrc/v3dm_essential.cuh, the
+source the RANSAC kernels run) built for the host and held to the reference's
+computeEssentialsFromFiveCorrs and relativePoseFromEssential (oracle/_ref) on random samples: the
+same solution count on >= 99.5% of samples, >= 99% of the reference's solutions within 1e-6 (unit
+norm, sign-fixed), and the same pose decisions for matched solutions, with R and T within 1e-4 (a
+solution that agrees to ~1e-6 can give a pose that agrees to a few 1e-6)."""
+import ctypes as C
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG, ROOT
+
+
+@pytest.fixture(scope="module")
+def host_lib(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    out = tmp_path_factory.mktemp("ess") / "libessential_host.so"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-I", str(PKG / "csrc"),
+                    str(ROOT / "tests" / "essential_host.cpp"), "-o", str(out)], check=True, capture_output=True,
+                   text=True)
+    L = C.CDLL(str(out))
+    L.host_five_point.argtypes = [C.c_void_p] * 5
+    L.host_five_point.restype = C.c_int
+    L.host_pose.argtypes = [C.c_void_p] * 7
+    L.host_pose.restype = C.c_int
+    return L
+
+
+def _unit(E):
+    e = E.reshape(-1)
+    e = e / np.linalg.norm(e)
+    return e * np.sign(e[np.argmax(np.abs(e))])
+
+
+def _samples(n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for t in range(n):
+        if t % 2 == 0:
+            v = rng.normal(size=3) * 0.3
+            th = np.linalg.norm(v)
+            k = v / th
+            Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+            R = np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * Kx @ Kx
+            X = np.c_[rng.uniform(-1, 1, (5, 2)), rng.uniform(3, 6, 5)]
+            p = X[:, :2] / X[:, 2:]
+            Y = (R @ X.T).T + rng.normal(size=3)
+            q = Y[:, :2] / Y[:, 2:]
+        else:
+            p = rng.uniform(-0.5, 0.5, (5, 2))
+            q = rng.uniform(-0.5, 0.5, (5, 2))
+        out.append([np.ascontiguousarray(a) for a in (p[:, 0], p[:, 1], q[:, 0], q[:, 1])])
+    return out
+
+
+def test_solutions_and_poses_match_the_reference(host_lib, oracle_mod):
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    ref_lib = oracle_mod._ref_ransac_lib()
+    same = matched = total = pose_checked = 0
+    samples = _samples(1500, 21)
+    for a in samples:
+        E = np.zeros(90)
+        n = host_lib.host_five_point(*[v.ctypes.data for v in a], E.ctypes.data)
+        ours = E[:9 * n].reshape(-1, 9)
+        ref = oracle_mod.ref_five_point(*a).reshape(-1, 9)
+        same += len(ref) == n
+        for e in ref:
+            total += 1
+            d = [np.linalg.norm(_unit(e) - _unit(o)) for o in ours]
+            if d and min(d) < 1e-6:
+                matched += 1
+                o = ours[int(np.argmin(d))]
+                R1, T1, R2, T2 = np.zeros(9), np.zeros(3), np.zeros(9), np.zeros(3)
+                ok1 = host_lib.host_pose(o.ctypes.data, *[v.ctypes.data for v in a], R1.ctypes.data, T1.ctypes.data)
+                ok2 = ref_lib.ref_pose(e.ctypes.data, *[v.ctypes.data for v in a], R2.ctypes.data, T2.ctypes.data)
+                if abs(float(np.min(np.linalg.svd(e.reshape(3, 3), compute_uv=False)))) < 1e-9:
+                    assert ok1 == ok2
+                    if ok1:
+                        pose_checked += 1
+                        assert np.abs(R1 - R2).max() < 1e-4 and np.abs(T1 - T2).max() < 1e-4
+    assert same >= 0.995 * len(samples), same
+    assert matched >= 0.99 * total, (matched, total)
+    assert pose_checked > 100
