@@ -15,3 +15,14 @@ extern "C" int host_pose(const double* E, const double* x1, const double* y1, co
                          double* R, double* T) {
   return v3dm::ess::essential_pose(E, 5, x1, y1, x2, y2, R, T) ? 1 : 0;
 }
+
+// The Sampson error, the truncated term and its inlier flag for n correspondences under F.
+extern "C" void host_sampson(const double* F, int n, const float* c, double thr2, double* d, double* trunc,
+                             unsigned char* inlier) {
+  for (int i = 0; i < n; ++i) {
+    d[i] = v3dm::ess::sampson(F, c[4 * i], c[4 * i + 1], c[4 * i + 2], c[4 * i + 3]);
+    bool in = false;
+    trunc[i] = v3dm::ess::sampson_truncated(F, c[4 * i], c[4 * i + 1], c[4 * i + 2], c[4 * i + 3], thr2, in);
+    inlier[i] = in;
+  }
+}

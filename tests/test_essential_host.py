@@ -86,3 +86,38 @@ def test_solutions_and_poses_match_the_reference(host_lib, oracle_mod):
     assert same >= 0.995 * len(samples), same
     assert matched >= 0.99 * total, (matched, total)
     assert pose_checked > 100
+
+
+def test_truncated_sampson_is_exact(host_lib):
+    """sampson_truncated (the cost kernel's term: the division skipped where the quotient is
+    certainly above the threshold) equals min(sampsonEpipolarError, thr^2) bit for bit, with the same
+    inlier decision, on random F scales and thresholds, and with thresholds equal to computed errors
+    (exact ties)."""
+    host_lib.host_sampson.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
+    rng = np.random.default_rng(5)
+    for trial in range(40):
+        F = rng.normal(size=9) * 10.0 ** rng.uniform(-8, -2)
+        thr2 = float(rng.choice([0.0, 1e-6, 1.0, 4.0, 100.0]))
+        n = 4000
+        c = rng.uniform(0, 1600, (n, 4)).astype(np.float32)
+        d = np.empty(n)
+        tr = np.empty(n)
+        fl = np.empty(n, np.uint8)
+        host_lib.host_sampson(F.ctypes.data, n, c.ctypes.data, thr2, d.ctypes.data, tr.ctypes.data, fl.ctypes.data)
+        exp = np.where(thr2 < d, thr2, d)
+        assert tr.tobytes() == exp.tobytes()
+        np.testing.assert_array_equal(fl.astype(bool), d < thr2)
+    # exact ties with the threshold: thr2 set to computed errors themselves
+    F = rng.normal(size=9) * 1e-4
+    c = rng.uniform(0, 1600, (2000, 4)).astype(np.float32)
+    d = np.empty(2000)
+    tr = np.empty(2000)
+    fl = np.empty(2000, np.uint8)
+    host_lib.host_sampson(F.ctypes.data, 2000, c.ctypes.data, 1.0, d.ctypes.data, tr.ctypes.data, fl.ctypes.data)
+    for thr2 in d[:200]:
+        host_lib.host_sampson(F.ctypes.data, 2000, c.ctypes.data, float(thr2), d.ctypes.data, tr.ctypes.data,
+                              fl.ctypes.data)
+        exp = np.where(thr2 < d, thr2, d)
+        assert tr.tobytes() == exp.tobytes()
+        np.testing.assert_array_equal(fl.astype(bool), d < thr2)
