@@ -104,3 +104,21 @@ def test_reference_pin_with_refinement(oracle_mod):
         assert refined["chosen"] >= 0 and plain["chosen"] >= 0
         assert np.linalg.norm(refined["model"][18:27].reshape(3, 3) - R[p]) < 0.05
         assert refined["model"][30] <= plain["model"][30] * 1.05
+
+
+def test_padding_with_the_last_sample_keeps_the_choice(oracle_mod):
+    """The reference loop on a short sample sequence and on the same sequence padded with repeats of
+    its last sample gives the same result (the padding the C++ wrapper and batched calls use)."""
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    off, corrs, K, R, t, inl = synth.two_view_pairs(13, n_pairs=4, n_min=8, n_max=40, inlier_min=0.4,
+                                                    inlier_max=0.9)
+    for p in range(4):
+        c = corrs[off[p]:off[p + 1]]
+        s = oracle_mod.ref_shuffle_samples(c.shape[0], 1000, 60 + p)
+        assert 0 < s.shape[0] < 1001  # short: few correspondences
+        padded = np.concatenate([s, np.repeat(s[-1:], 1001 - s.shape[0], axis=0)])
+        a = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, s)
+        b = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], 2.0, 1000, padded)
+        assert a["chosen"] == b["chosen"] and a["n_inliers"] == b["n_inliers"]
+        np.testing.assert_array_equal(a["model"], b["model"])
