@@ -604,5 +604,243 @@ V3DM_HD bool essential_pose(const double* E, int n, const double* x1, const doub
   return true;
 }
 
+
+// ---- refinement of a relative pose ----------------------------------------------------------
+// refineRelativePose (v3d_poseutilities.cpp:1063-1101) with its RelativePoseMinimizer (:812-1006)
+// on the reference's dense Levenberg-Marquardt loop (V3D/Math/v3d_optimization.h:25-277), restated:
+//   f_k = (q^T E p) / sqrt((Ep)_0^2 + (Ep)_1^2 + (E^T q)_0^2 + (E^T q)_1^2) on normalised points,
+//   E = [T]x R; weights w_k = 1 if |e_k| < thr, else sqrt(thr / |e_k|), with e_k the same quantity on
+//   pixel points under F = K2^-T E K1^-1; residual r = -w f; J = df/d(omega, T) (not weighted);
+//   delta = (J^T J + lambda I)^-1 J^T r (Cholesky); R <- R Rodrigues(omega), T <- (T + dT) / |T + dT|;
+//   lambda = 1e-3 max diag(J^T J) at the first iteration, x0.1 (at least 1e-10) after an improvement
+//   (rho > 0), x10 and the step undone otherwise; stop when |J^T r|_inf < 1e-8, when (from the 10th
+//   iteration) |delta| < 1e-8 (4 + 1e-8), or after 50 iterations.
+struct PoseCorr {  // one correspondence: normalised and pixel positions
+  double lx, ly, rx, ry;
+  double plx, ply, prx, pry;
+};
+
+V3DM_HD void pose_essential(const double* R, const double* T, double* E) {  // E = [T]x R
+  const double Tx[9] = {0.0, -T[2], T[1], T[2], 0.0, -T[0], -T[1], T[0], 0.0};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += Tx[3 * i + k] * R[3 * k + j];
+      E[3 * i + j] = v;
+    }
+}
+
+// (q^T M p) / sqrt(...) of one correspondence under M (E on normalised, F on pixel points), with the
+// intermediate products; M p and M^T q summed as multiply_A_v_affine (the last column first).
+V3DM_HD double pose_residual(const double* M, double px, double py, double qx, double qy, double* Mp, double* Mtq) {
+  Mp[0] = M[2] + M[0] * px + M[1] * py;
+  Mp[1] = M[5] + M[3] * px + M[4] * py;
+  Mp[2] = M[8] + M[6] * px + M[7] * py;
+  Mtq[0] = M[6] + M[0] * qx + M[3] * qy;
+  Mtq[1] = M[7] + M[1] * qx + M[4] * qy;
+  const double num = qx * Mp[0] + qy * Mp[1] + Mp[2];
+  const double denom = sqrt(Mp[0] * Mp[0] + Mp[1] * Mp[1] + Mtq[0] * Mtq[0] + Mtq[1] * Mtq[1]);
+  return num / denom;
+}
+
+V3DM_HD void pose_update(const double* Rold, const double* Told, const double* delta, double* R, double* T) {
+  // createRotationMatrixRodrigues(omega) (v3d_mathutilities.h:170-190), then R = Rold dR
+  const double w0 = delta[0], w1 = delta[1], w2 = delta[2];
+  const double theta = sqrt(w0 * w0 + w1 * w1 + w2 * w2);
+  double dR[9] = {1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+  if (fabs(theta) > 1e-6) {
+    const double J[9] = {0.0, -w2, w1, w2, 0.0, -w0, -w1, w0, 0.0};
+    double J2[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += J[3 * i + k] * J[3 * k + j];
+        J2[3 * i + j] = v;
+      }
+    const double c1 = sin(theta) / theta;
+    const double c2 = (1 - cos(theta)) / (theta * theta);
+    for (int k = 0; k < 9; ++k) dR[k] += c1 * J[k] + c2 * J2[k];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += Rold[3 * i + k] * dR[3 * k + j];
+      R[3 * i + j] = v;
+    }
+  double t[3] = {Told[0] + delta[3], Told[1] + delta[4], Told[2] + delta[5]};
+  const double nt = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  for (int k = 0; k < 3; ++k) T[k] = t[k] / nt;
+}
+
+// The weighted residual e = -w f under (R, T), with weights from the pixel positions; returns |e|^2.
+V3DM_HD double pose_weighted_residual(const PoseCorr* c, int n, const double* R, const double* T,
+                                      const double* invK1, const double* invK2t, double thr, double* w, double* e,
+                                      bool fillWeights) {
+  double E[9], tmp[9], F[9], a[3], b[2];
+  pose_essential(R, T, E);
+  if (fillWeights) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += invK2t[3 * i + k] * E[3 * k + j];
+        tmp[3 * i + j] = v;
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += tmp[3 * i + k] * invK1[3 * k + j];
+        F[3 * i + j] = v;
+      }
+    for (int k = 0; k < n; ++k) {
+      const double ek = pose_residual(F, c[k].plx, c[k].ply, c[k].prx, c[k].pry, a, b);
+      w[k] = (fabs(ek) < thr) ? 1.0 : sqrt(thr / fabs(ek));
+    }
+  }
+  double err = 0.0;
+  for (int k = 0; k < n; ++k) {
+    e[k] = w[k] * (0.0 - pose_residual(E, c[k].lx, c[k].ly, c[k].rx, c[k].ry, a, b));
+    err += e[k] * e[k];
+  }
+  return err;
+}
+
+// J^T J (6 x 6) and J^T e of f under (R, T).
+V3DM_HD void pose_normal_equations(const PoseCorr* c, int n, const double* R, const double* T, const double* e,
+                                   double* JtJ, double* Jte) {
+  double E[9];
+  pose_essential(R, T, E);
+  double inner[9][6];  // dE / d(omega_x, omega_y, omega_z, T_x, T_y, T_z)
+  for (int r = 0; r < 3; ++r) {
+    inner[3 * r + 0][0] = 0.0;
+    inner[3 * r + 1][0] = E[3 * r + 2];
+    inner[3 * r + 2][0] = -E[3 * r + 1];
+    inner[3 * r + 0][1] = -E[3 * r + 2];
+    inner[3 * r + 1][1] = 0.0;
+    inner[3 * r + 2][1] = E[3 * r + 0];
+    inner[3 * r + 0][2] = E[3 * r + 1];
+    inner[3 * r + 1][2] = -E[3 * r + 0];
+    inner[3 * r + 2][2] = 0.0;
+  }
+  for (int j = 0; j < 3; ++j) {
+    inner[j][3] = 0.0;
+    inner[3 + j][3] = -R[6 + j];
+    inner[6 + j][3] = R[3 + j];
+    inner[j][4] = R[6 + j];
+    inner[3 + j][4] = 0.0;
+    inner[6 + j][4] = -R[j];
+    inner[j][5] = -R[3 + j];
+    inner[3 + j][5] = R[j];
+    inner[6 + j][5] = 0.0;
+  }
+  for (int k = 0; k < 36; ++k) JtJ[k] = 0.0;
+  for (int k = 0; k < 6; ++k) Jte[k] = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double p[3] = {c[k].lx, c[k].ly, 1.0}, q[3] = {c[k].rx, c[k].ry, 1.0};
+    double Ep[3], Etq[2];
+    const double num0 = pose_residual(E, p[0], p[1], q[0], q[1], Ep, Etq);
+    (void)num0;
+    const double num = q[0] * Ep[0] + q[1] * Ep[1] + Ep[2];
+    const double sqrDenom = Ep[0] * Ep[0] + Ep[1] * Ep[1] + Etq[0] * Etq[0] + Etq[1] * Etq[1];
+    const double denom = sqrt(sqrDenom);
+    const double invDenom = 1.0 / denom;
+    const double invSqrDenom = 1.0 / sqrDenom;
+    double outer[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const double numDer = (i < 2 ? q[i] : 1.0) * (j < 2 ? p[j] : 1.0);
+        double sq = 0.0;  // d(sqrDenom)/dE_ij
+        if (i < 2 && j < 2) sq = 2 * Ep[i] * p[j] + 2 * Etq[j] * q[i];
+        else if (i < 2) sq = 2 * Ep[i];
+        else if (j < 2) sq = 2 * Etq[j];
+        outer[3 * i + j] = (numDer * denom - num * 0.5 * invDenom * sq) * invSqrDenom;
+      }
+    double J[6];
+    for (int col = 0; col < 6; ++col) {
+      double v = 0.0;
+      for (int j = 0; j < 9; ++j) v += outer[j] * inner[j][col];
+      J[col] = v;
+    }
+    for (int a = 0; a < 6; ++a) {
+      for (int b = 0; b < 6; ++b) JtJ[6 * a + b] += J[a] * J[b];
+      Jte[a] += J[a] * e[k];
+    }
+  }
+}
+
+// x = N^-1 b for a symmetric positive definite 6 x 6 N (Cholesky); false if not positive definite.
+V3DM_HD bool cholesky_solve6(const double* N, const double* b, double* x) {
+  double L[36];
+  for (int k = 0; k < 36; ++k) L[k] = 0.0;
+  for (int j = 0; j < 6; ++j) {
+    double d = N[6 * j + j];
+    for (int k = 0; k < j; ++k) d -= L[6 * j + k] * L[6 * j + k];
+    if (!(d > 0.0)) return false;
+    L[6 * j + j] = sqrt(d);
+    for (int i = j + 1; i < 6; ++i) {
+      double v = N[6 * i + j];
+      for (int k = 0; k < j; ++k) v -= L[6 * i + k] * L[6 * j + k];
+      L[6 * i + j] = v / L[6 * j + j];
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= L[6 * i + k] * y[k];
+    y[i] = v / L[6 * i + i];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double v = y[i];
+    for (int k = i + 1; k < 6; ++k) v -= L[6 * k + i] * x[k];
+    x[i] = v / L[6 * i + i];
+  }
+  return true;
+}
+
+// Refines (R, T) in place on n correspondences; w and e are scratch arrays of n doubles.
+V3DM_HD void refine_pose(const PoseCorr* c, int n, const double* invK1, const double* invK2t, double thr, double* R,
+                         double* T, double* w, double* e) {
+  double lambda = 1e-3, JtJ[36], Jte[6], N[36], delta[6], Rs[9], Ts[3];
+  bool computeDerivatives = true;
+  for (int it = 0; it < 50; ++it) {
+    const double err = pose_weighted_residual(c, n, R, T, invK1, invK2t, thr, w, e, true);
+    if (computeDerivatives) pose_normal_equations(c, n, R, T, e, JtJ, Jte);
+    double gmax = 0.0;
+    for (int k = 0; k < 6; ++k) gmax = fmax(gmax, fabs(Jte[k]));
+    if (gmax < 1e-8) return;
+    if (it == 0) {
+      double maxEl = -1e30;
+      for (int k = 0; k < 6; ++k) maxEl = fmax(maxEl, JtJ[7 * k]);
+      lambda = 1e-3 * maxEl;
+    }
+    for (int k = 0; k < 36; ++k) N[k] = JtJ[k];
+    for (int k = 0; k < 6; ++k) N[7 * k] += lambda;
+    if (!cholesky_solve6(N, Jte, delta)) return;
+    double dl = 0.0;
+    for (int k = 0; k < 6; ++k) dl += delta[k] * delta[k];
+    dl = sqrt(dl);
+    if (it >= 10 && dl < 1e-8 * (4.0 + 1e-8)) return;
+    for (int k = 0; k < 9; ++k) Rs[k] = R[k];
+    for (int k = 0; k < 3; ++k) Ts[k] = T[k];
+    pose_update(Rs, Ts, delta, R, T);
+    const double errNew = pose_weighted_residual(c, n, R, T, invK1, invK2t, thr, w, e, false);
+    double rho = err - errNew;
+    double d1 = 0.0, d2 = 0.0;
+    for (int k = 0; k < 6; ++k) {
+      d1 += delta[k] * delta[k];
+      d2 += delta[k] * Jte[k];
+    }
+    rho = rho / (lambda * d1 + d2);
+    if (rho > 0) {
+      lambda = fmax(1e-10, lambda * 0.1);
+      computeDerivatives = true;
+    } else {
+      for (int k = 0; k < 9; ++k) R[k] = Rs[k];
+      for (int k = 0; k < 3; ++k) T[k] = Ts[k];
+      lambda *= 10.0;
+      computeDerivatives = false;
+    }
+  }
+}
+
 }  // namespace ess
 }  // namespace v3dm

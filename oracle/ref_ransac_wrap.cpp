@@ -215,6 +215,26 @@ int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K
   return 0;
 }
 
+// refineRelativePose(left, right, K1, K2, R, T, inlierThreshold) (v3d_poseutilities.cpp:1063-1101)
+// on n pixel correspondences (left[2n], right[2n]); R (row-major) and T refined in place.
+int ref_refine_pose(int n, const double* left, const double* right, const double* K1, const double* K2,
+                    double inlierThreshold, double* R, double* T) {
+  std::vector<Vector2d> l(n), r(n);
+  for (int i = 0; i < n; ++i) {
+    l[i][0] = left[2 * i];
+    l[i][1] = left[2 * i + 1];
+    r[i][0] = right[2 * i];
+    r[i][1] = right[2 * i + 1];
+  }
+  Matrix3x3d Rm = mat(R);
+  Vector3d t;
+  for (int k = 0; k < 3; ++k) t[k] = T[k];
+  refineRelativePose(l, r, mat(K1), mat(K2), Rm, t, inlierThreshold);
+  put(Rm, R);
+  for (int k = 0; k < 3; ++k) T[k] = t[k];
+  return 0;
+}
+
 int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold, int nSamples,
                int nDraw, const int* samples, double* model, int* nInliers, unsigned char* flags, int* chosen) {
   return ref_ransac_mode(N, corrs, K1, K2, inlierThreshold, nSamples, nDraw, samples, 0, model, nInliers, flags,

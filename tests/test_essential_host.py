@@ -121,3 +121,51 @@ def test_truncated_sampson_is_exact(host_lib):
         exp = np.where(thr2 < d, thr2, d)
         assert tr.tobytes() == exp.tobytes()
         np.testing.assert_array_equal(fl.astype(bool), d < thr2)
+
+
+def test_pose_refinement_matches_the_reference(host_lib, oracle_mod):
+    """The restated refineRelativePose (Levenberg-Marquardt on Sampson residuals with the
+    reference's weights, damping and stopping rules; not yet on the RANSAC kernels' path) against
+    the reference's own on noisy inliers from a perturbed starting pose: R and T within 1e-8."""
+    if not oracle_mod.ref_ransac_available():
+        pytest.skip("reference relative-orientation code not built (oracle/_ref)")
+    host_lib.host_refine_pose.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 2
+    ref = oracle_mod._ref_ransac_lib()
+    ref.ref_refine_pose.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 2
+    rng = np.random.default_rng(3)
+    moved = 0
+    for t in range(30):
+        K = np.array([[rng.uniform(900, 1500), 0, 800], [0, rng.uniform(900, 1500), 600], [0, 0, 1.0]])
+        v = rng.normal(size=3) * 0.2
+        th = np.linalg.norm(v)
+        k = v / th
+        Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+        R = np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * Kx @ Kx
+        T = rng.normal(size=3)
+        T /= np.linalg.norm(T)
+        n = int(rng.integers(20, 400))
+        X = np.c_[rng.uniform(-2, 2, (n, 2)), rng.uniform(4, 10, n)]
+        Y = (R @ X.T).T + T
+        pl = (K @ X.T).T
+        pl = pl[:, :2] / pl[:, 2:] + rng.normal(0, 0.5, (n, 2))
+        pr = (K @ Y.T).T
+        pr = pr[:, :2] / pr[:, 2:] + rng.normal(0, 0.5, (n, 2))
+        w = rng.normal(size=3) * 0.01
+        R0 = R @ (np.eye(3) + np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]]))
+        u, _, vt = np.linalg.svd(R0)
+        R0 = u @ vt
+        T0 = T + rng.normal(size=3) * 0.02
+        T0 /= np.linalg.norm(T0)
+        left = np.ascontiguousarray(pl.reshape(-1))
+        right = np.ascontiguousarray(pr.reshape(-1))
+        iK = np.linalg.inv(K)
+        Rh, Th = R0.reshape(-1).copy(), T0.copy()
+        Rr, Tr = R0.reshape(-1).copy(), T0.copy()
+        host_lib.host_refine_pose(n, left.ctypes.data, right.ctypes.data, iK.ctypes.data, iK.ctypes.data, 2.0,
+                                  Rh.ctypes.data, Th.ctypes.data)
+        Kc = np.ascontiguousarray(K)
+        ref.ref_refine_pose(n, left.ctypes.data, right.ctypes.data, Kc.ctypes.data, Kc.ctypes.data, 2.0,
+                            Rr.ctypes.data, Tr.ctypes.data)
+        assert np.abs(Rh - Rr).max() < 1e-8 and np.abs(Th - Tr).max() < 1e-8, t
+        moved += np.abs(Rr - R0.reshape(-1)).max() > 1e-3
+    assert moved > 20  # the refinement does move the starting poses
