@@ -737,8 +737,7 @@ V3DM_HD void pose_normal_equations(const PoseCorr* c, int n, const double* R, co
   for (int k = 0; k < n; ++k) {
     const double p[3] = {c[k].lx, c[k].ly, 1.0}, q[3] = {c[k].rx, c[k].ry, 1.0};
     double Ep[3], Etq[2];
-    const double num0 = pose_residual(E, p[0], p[1], q[0], q[1], Ep, Etq);
-    (void)num0;
+    pose_residual(E, p[0], p[1], q[0], q[1], Ep, Etq);  // for E p and E^T q
     const double num = q[0] * Ep[0] + q[1] * Ep[1] + Ep[2];
     const double sqrDenom = Ep[0] * Ep[0] + Ep[1] * Ep[1] + Etq[0] * Etq[0] + Etq[1] * Etq[1];
     const double denom = sqrt(sqrDenom);
