@@ -43,3 +43,24 @@ def test_null_arguments_are_rejected(v3dm_mod):
     assert lib.v3dm_voctree_counts(0, 3, None, None) == v3dm_mod.ERR_ARG
     assert v3dm_mod.voctree_counts(10, 6) == (1111110, 1000000)
     assert v3dm_mod.voctree_counts(50, 3) == (127550, 125000)
+
+
+def test_header_is_plain_c_and_links(v3dm_mod, tmp_path):
+    """include/v3dm.h compiles as C99 (-Wall -Werror -pedantic) and every declared entry point links
+    against libv3dm.so from a C program, as a cgo / JNI / FFI binding would see it."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    names = _declared(v3dm_mod.HEADER_PATH)
+    src = tmp_path / "abi_check.c"
+    body = "\n".join(f"  p[{i}] = (void (*)(void))&{n};" for i, n in enumerate(names))
+    src.write_text('#include "v3dm.h"\n#include <stdio.h>\n\nint main(void) {\n'
+                   f"  void (*p[{len(names)}])(void);\n{body}\n"
+                   '  printf("%d\\n", (int)(sizeof(p) / sizeof(p[0])));\n  return 0;\n}\n')
+    out = tmp_path / "abi_check"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I",
+                    str(v3dm_mod.HEADER_PATH.parent), str(src), "-o", str(out), "-L", str(v3dm_mod.LIB_PATH.parent),
+                    "-lv3dm", f"-Wl,-rpath,{v3dm_mod.LIB_PATH.parent}"], check=True, capture_output=True, text=True)
+    r = subprocess.run([str(out)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and int(r.stdout) == len(names)
