@@ -33,6 +33,10 @@ def test_no_cpu_fallback_without_gpu(v3dm_mod):
     with pytest.raises(v3dm_mod.V3DMError) as e:
         v3dm_mod.VocabularyTreeTraversal(10, 3)
     assert e.value.status == v3dm_mod.ERR_NO_DEVICE
+    for make in (v3dm_mod.BatchMatching, v3dm_mod.Loader, v3dm_mod.Retrieval, v3dm_mod.Ransac):
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            make()
+        assert e.value.status == v3dm_mod.ERR_NO_DEVICE, make.__name__
 
 
 def test_null_arguments_are_rejected(v3dm_mod):
@@ -43,6 +47,12 @@ def test_null_arguments_are_rejected(v3dm_mod):
     assert lib.v3dm_voctree_counts(0, 3, None, None) == v3dm_mod.ERR_ARG
     assert v3dm_mod.voctree_counts(10, 6) == (1111110, 1000000)
     assert v3dm_mod.voctree_counts(50, 3) == (127550, 125000)
+    assert lib.v3dm_retrieval_create(None, 0) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_ransac_create(None, 0) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_retrieval_binomial(None, 10, 1, None, None, 0.1, 1, None, None) == v3dm_mod.ERR_ARG
+    assert lib.v3dm_ransac_essential(None, 1, None, None, None, 2.0, 10, 11, None, 0, None, None, None) == \
+        v3dm_mod.ERR_ARG
+    assert lib.v3dm_retrieval_wait(None) == v3dm_mod.ERR_ARG and lib.v3dm_ransac_wait(None) == v3dm_mod.ERR_ARG
 
 
 def test_header_is_plain_c_and_links(v3dm_mod, tmp_path):
