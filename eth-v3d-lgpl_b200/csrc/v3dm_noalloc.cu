@@ -62,11 +62,14 @@ __global__ void k_noalloc_status(const int32_t* info, long long cap, int32_t* co
   *count = bad ? -1 : info[kInfoPairs];
 }
 
+// Makes `dev` current for the call and restores the caller's device afterwards.  ok is false
+// when the device cannot be made current; the call must then queue nothing.
 struct NoAllocDeviceGuard {
   int prev = -1;
+  bool ok = false;
   explicit NoAllocDeviceGuard(int dev) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
+    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
   }
   ~NoAllocDeviceGuard() {
     int cur = -1;
@@ -87,7 +90,14 @@ extern "C" int v3dm_putative_u8_noalloc(int device, const uint8_t* d_left, int n
       (nLeft > 0 && nRight > 0 && !d_pairs) || device < 0 || device >= 128)
     return V3DM_ERR_ARG;
   if (nLeft > kNoAllocMaxFeatures || nRight > kNoAllocMaxFeatures) return V3DM_ERR_SIZE;
+  int nDev = 0;
+  if (cudaGetDeviceCount(&nDev) != cudaSuccess) return V3DM_ERR_NO_DEVICE;
+  if (device >= nDev) return V3DM_ERR_ARG;
+  // An error left pending by earlier, unrelated work would surface only after this call had
+  // queued kernels; refuse up front instead, and leave the error for its owner to read.
+  if (cudaPeekAtLastError() != cudaSuccess) return V3DM_ERR_CUDA;
   NoAllocDeviceGuard guard(device);
+  if (!guard.ok) return V3DM_ERR_CUDA;
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_scratchMutex);
