@@ -28,10 +28,16 @@ class Gate(C.Structure):
     _fields_ = [("type", C.c_int), ("m", C.c_double * 9), ("thr", C.c_float)]
 
 
+def ref_dir() -> Path:
+    """The reference's V3D source tree: V3D_REF_DIR, else the reference checkout beside this
+    repository."""
+    return Path(os.environ.get("V3D_REF_DIR", str(HERE.parent.parent / "reference" / "V3D")))
+
+
 def build() -> None:
     """Builds liboracle.so (and the _ref libraries when the reference sources exist)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if Path(os.environ.get("V3D_REF_DIR", "/root/reference/V3D")).exists():
+    if ref_dir().exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
 
 
@@ -46,6 +52,8 @@ def lib() -> C.CDLL:
         L.orc_match_u8.restype = i32
         L.orc_voctree_quantize_f32.argtypes = [i32, i32, vp, i32, vp, vp, i32, i32]
         L.orc_voctree_quantize_u8.argtypes = [i32, i32, vp, i32, vp, vp, i32, i32]
+        L.orc_match_u8_calls.argtypes = [i32, i32, vp, vp, f32, f32, i32, vp, vp, vp, vp, vp, vp, i32]
+        L.orc_match_u8_calls.restype = i32
         L.orc_scores_u8.argtypes = [i32, i32, vp, vp, vp]
         L.orc_ref_feature_count.argtypes = [i32, i32]
         L.orc_ref_feature_count.restype = i32
@@ -95,6 +103,34 @@ def match(L: np.ndarray, R: np.ndarray, min_score: float = 0.9, min_ratio: float
     if with_sides:
         return out, colmax[:nL].copy(), rowmax[:nR].copy()
     return out
+
+
+def match_calls(L: np.ndarray, R: np.ndarray, min_score: float, min_ratio: float, calls, lpos=None, rpos=None,
+                threads: int = 0):
+    """A putative call and guided calls on the same features from one score computation, as
+    the reference's guided calls mask the putative call's stored matrix.  calls: a list of
+    gate lists, one per call, each extending the previous one (gates compound); the first is
+    normally [] (putative).  Returns one (n, 2) pair array per call."""
+    L = np.ascontiguousarray(L, np.uint8)
+    R = np.ascontiguousarray(R, np.uint8)
+    nL, nR = L.shape[0], R.shape[0]
+    calls = [list(c) for c in calls]
+    for a, b in zip(calls, calls[1:]):
+        if b[:len(a)] != a:
+            raise ValueError("each call's gates must extend the previous call's")
+    g = _gates(calls[-1])
+    upto = np.array([len(c) for c in calls], np.int32)
+    lp = np.ascontiguousarray(lpos, np.float32) if lpos is not None else np.zeros((1, 2), np.float32)
+    rp = np.ascontiguousarray(rpos, np.float32) if rpos is not None else np.zeros((1, 2), np.float32)
+    cap = max(1, min(nL, nR))
+    pairs = np.empty((len(calls), cap, 2), np.int32)
+    n_out = np.zeros(len(calls), np.int32)
+    rc = lib().orc_match_u8_calls(nL, nR, L.ctypes.data, R.ctypes.data, min_score, min_ratio, len(calls),
+                                  upto.ctypes.data, C.addressof(g), lp.ctypes.data, rp.ctypes.data,
+                                  pairs.ctypes.data, n_out.ctypes.data, threads)
+    if rc != 0:
+        raise ValueError("oracle rejected the arguments")
+    return [pairs[c, :n_out[c]].copy() for c in range(len(calls))]
 
 
 def scores(L: np.ndarray, R: np.ndarray) -> np.ndarray:
@@ -216,6 +252,51 @@ def ref_cuda_match_f32(L_f32: np.ndarray, R_f32: np.ndarray, min_score: float, m
     if res.returncode != 0:
         raise RuntimeError(f"reference matcher failed ({res.returncode}): {res.stderr[-2000:]}")
     return np.load(wd / "out.npy")
+
+
+_REF_TIME_CHILD = r"""
+import ctypes as C, json, sys, numpy as np
+d = np.load(sys.argv[1])
+L = C.CDLL(sys.argv[2])
+L.v3dref_time_pairs.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+off = np.ascontiguousarray(d['off'], np.int32); desc = np.ascontiguousarray(d['desc'], np.float32)
+pos = np.ascontiguousarray(d['pos'], np.float32); pairs = np.ascontiguousarray(d['pairs'], np.int32)
+F = np.ascontiguousarray(d['F'], np.float64); reps = int(d['reps'])
+sec = np.zeros(reps, np.float64); nm = C.c_longlong(0)
+rc = L.v3dref_time_pairs(int(d['nmax']), off.size - 1, off.ctypes.data, desc.ctypes.data, pos.ctypes.data,
+                         pairs.shape[0], pairs.ctypes.data, int(d['guided']), F.ctypes.data, float(d['thr']),
+                         float(d['ms']), float(d['mr']), reps, sec.ctypes.data, C.byref(nm))
+print(json.dumps({"rc": rc, "seconds": sec.tolist(), "matches": nm.value}))
+sys.exit(0 if rc == 0 else 3)
+"""
+
+
+def ref_cuda_time_pairs(desc_u8: np.ndarray, offsets: np.ndarray, pairs: np.ndarray, min_score: float,
+                        min_ratio: float, reps: int, positions=None, F=None, thr: float = 2.0,
+                        n_max: int | None = None, timeout: float = 900.0) -> dict:
+    """Wall time of the reference's own SIFT_Matching (v3d_cudamatching.cu, built unmodified
+    for the B200) in the apps' per-pair loop over `pairs` of the images in desc_u8 (u/512
+    floats), with F-guided matching after each putative call when F (9 doubles per pair) is
+    given.  Runs in a child process because the reference exits on any CUDA error.
+    Returns {"seconds": [per repetition], "matches": pairs found in the last repetition}."""
+    import json
+    import tempfile
+    wd = Path(tempfile.mkdtemp(prefix="v3dref_time_"))
+    off = np.ascontiguousarray(offsets, np.int32)
+    counts = np.diff(off)
+    guided = F is not None
+    np.savez(wd / "in.npz", off=off, desc=np.asarray(desc_u8, np.float32) / 512.0,
+             pos=np.zeros((max(1, off[-1]), 2), np.float32) if positions is None else positions,
+             pairs=np.ascontiguousarray(pairs, np.int32).reshape(-1, 2),
+             F=np.zeros(9, np.float64) if F is None else np.asarray(F, np.float64).reshape(-1),
+             guided=int(guided), thr=thr, ms=min_score, mr=min_ratio, reps=reps,
+             nmax=int(n_max if n_max is not None else (int(counts.max()) & ~31)))
+    res = subprocess.run([sys.executable, "-c", _REF_TIME_CHILD, str(wd / "in.npz"), str(REF_CUDA)],
+                         capture_output=True, text=True, timeout=timeout)
+    if res.returncode != 0:
+        raise RuntimeError(f"reference matcher failed ({res.returncode}): {res.stderr[-2000:]}")
+    return json.loads(res.stdout.strip().splitlines()[-1])
 
 
 # ---- the reference's feature-file serializer -------------------------------------------------

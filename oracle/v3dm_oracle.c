@@ -263,6 +263,104 @@ int orc_match_u8(int nL, int nR, const uint8_t* L, const uint8_t* R, float minSc
     return n;
 }
 
+/* A findPutativeMatches call followed by guided calls on the same features, from ONE score
+ * computation, as the reference does: the putative call writes the score matrix
+ * (.cu:529-530) and each later runGuidedMatching / runGuidedHomographyMatching masks that
+ * stored matrix in place and re-runs the maxima (.cu:554-623, :625-694), so gates compound.
+ * Call c (0 <= c < nCalls) sees gates[0 .. gatesUpTo[c]-1]; gatesUpTo[0] is normally 0 (the
+ * putative call).  pairsOut holds nCalls blocks of min(nL, nR) pairs; nOut[c] gets call c's
+ * pair count.  Results equal nCalls separate orc_match_u8 calls.  Returns 0, or -1 on bad
+ * arguments.                                                                             */
+int orc_match_u8_calls(int nL, int nR, const uint8_t* L, const uint8_t* R, float minScore, float minRatio,
+                       int nCalls, const int* gatesUpTo, const orc_gate* gates, const float* lpos,
+                       const float* rpos, int* pairsOut, int* nOut, int nThreads) {
+    if (nL < 0 || nR < 0 || nCalls < 1 || !gatesUpTo || !nOut) return -1;
+    int nGates = 0;
+    for (int c = 0; c < nCalls; ++c) {
+        if (gatesUpTo[c] < 0 || (c > 0 && gatesUpTo[c] < gatesUpTo[c - 1])) return -1;
+        nGates = gatesUpTo[c];
+    }
+    if (nGates > 0 && (!lpos || !rpos || !gates)) return -1;
+    for (int c = 0; c < nCalls; ++c) nOut[c] = 0;
+    if (nL == 0 || nR == 0) return 0;
+#ifdef _OPENMP
+    if (nThreads <= 0) nThreads = omp_get_max_threads();
+#else
+    nThreads = 1;
+#endif
+    orc_gate_pre* pre = NULL;
+    if (nGates > 0) {
+        pre = (orc_gate_pre*)calloc((size_t)nGates, sizeof(orc_gate_pre));
+        for (int g = 0; g < nGates; ++g) gate_precompute(&gates[g], nL, nR, lpos, rpos, &pre[g]);
+    }
+    const size_t cap = (size_t)(nL < nR ? nL : nR);
+    int* rowMax = (int*)malloc(sizeof(int) * (size_t)nR * (size_t)nCalls);
+    orc_top2* colPart = (orc_top2*)malloc(sizeof(orc_top2) * (size_t)nL * (size_t)nThreads * (size_t)nCalls);
+    float* rowBuf = (float*)malloc(sizeof(float) * (size_t)nL * (size_t)nThreads * 2);
+
+#pragma omp parallel num_threads(nThreads)
+    {
+        int tid = 0, nt = 1;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+        nt = omp_get_num_threads();
+#endif
+        float* sc = rowBuf + (size_t)tid * nL * 2;
+        float* masked = sc + nL;
+        for (int c = 0; c < nCalls; ++c) {
+            orc_top2* cp = colPart + ((size_t)c * nThreads + tid) * nL;
+            for (int l = 0; l < nL; ++l) top2_init(&cp[l]);
+        }
+        int r0 = (int)((long long)nR * tid / nt), r1 = (int)((long long)nR * (tid + 1) / nt);
+        for (int r = r0; r < r1; ++r) {
+            const uint8_t* rr = R + (size_t)r * 128;
+            for (int l = 0; l < nL; ++l) sc[l] = (float)dot_u8(L + (size_t)l * 128, rr) * 0x1p-18f;
+            memcpy(masked, sc, sizeof(float) * (size_t)nL);
+            int applied = 0;
+            for (int c = 0; c < nCalls; ++c) {
+                for (; applied < gatesUpTo[c]; ++applied)
+                    for (int l = 0; l < nL; ++l)
+                        if (gate_rejects(&pre[applied], l, r)) masked[l] = ORC_MASKED;
+                orc_top2* cp = colPart + ((size_t)c * nThreads + tid) * nL;
+                orc_top2 rt;
+                top2_init(&rt);
+                for (int l = 0; l < nL; ++l) {
+                    top2_push(&rt, masked[l], l);
+                    top2_push(&cp[l], masked[l], r);
+                }
+                rowMax[(size_t)c * nR + r] = top2_decide(rt, minScore, minRatio);
+            }
+        }
+    }
+    for (int c = 0; c < nCalls; ++c) {
+        const int* rm = rowMax + (size_t)c * nR;
+        int* out = pairsOut ? pairsOut + 2 * cap * (size_t)c : NULL;
+        int n = 0;
+        for (int k = 0; k < nL; ++k) {
+            orc_top2 acc = colPart[((size_t)c * nThreads) * nL + k];
+            for (int t = 1; t < nThreads; ++t) acc = top2_concat(acc, colPart[((size_t)c * nThreads + t) * nL + k]);
+            int l = top2_decide(acc, minScore, minRatio);
+            if (l >= 0 && rm[l] == k) { /* mutual filter, .cu:546-551 */
+                if (out) {
+                    out[2 * n] = k;
+                    out[2 * n + 1] = l;
+                }
+                ++n;
+            }
+        }
+        nOut[c] = n;
+    }
+    for (int g = 0; g < nGates; ++g) {
+        free(pre[g].lv);
+        free(pre[g].rv);
+    }
+    free(pre);
+    free(rowMax);
+    free(colPart);
+    free(rowBuf);
+    return 0;
+}
+
 /* The reference's size handling in front of every call (.cu:444-460 allocate, .cu:493-519
  * setLeft/RightFeatures): round down to a multiple of 32, then clamp to nMax.             */
 int orc_ref_feature_count(int n, int nMaxRounded) {

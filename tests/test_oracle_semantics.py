@@ -86,3 +86,20 @@ def test_threads_do_not_change_result(oracle_mod):
     a = oracle_mod.match(L, R, 0.7, 0.8, threads=1)
     b = oracle_mod.match(L, R, 0.7, 0.8, threads=7)
     np.testing.assert_array_equal(a, b)
+
+
+def test_one_score_pass_equals_separate_calls():
+    """match_calls (putative and compounding guided calls from one score computation, as the
+    reference masks its stored matrix) equals separate oracle calls."""
+    import numpy as np
+    from oracle import oracle
+    from v3dm import synth
+    L, R, lp, rp, F, _ = synth.stereo(3, 900, 1000)
+    H = np.eye(3)
+    H[0, 2] = 5.0
+    calls = [[], [("F", F, 2.0)], [("F", F, 2.0), ("H", H, 400.0)]]
+    got = oracle.match_calls(L, R, 0.7, 0.8, calls, lpos=lp, rpos=rp, threads=3)
+    for g, c in zip(got, calls):
+        exp = oracle.match(L, R, 0.7, 0.8, gates=c, lpos=lp, rpos=rp)
+        assert np.array_equal(g, exp)
+    assert got[0].shape[0] > got[2].shape[0] > 0
