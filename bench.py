@@ -1,20 +1,22 @@
 #!/usr/bin/env python
 """Benchmark of the SIFT matching path on B200.
 
-Default workload (one step): putative matching followed by F-guided matching (2 px gate) of one
-16384 x 16384 pair of uint8 SIFT-like descriptors, minScore 0.7, ratio 0.8 -- the single large
-guided pair.  Metric: image pairs per second.  `value` times the steps with descriptors and
-positions resident in HBM (device-output C-ABI calls); `e2e` times the same step through the
-host C-ABI calls (pinned host buffers in, host pairs out, copies inside the timed region).
-Other workloads: --workload batch (all 19,900 pairs of 200 images in one batched call),
---workload voctree (2M descriptors through a BF 10, depth 6 tree), --workload retrieval (the
-voctree app's image-retrieval scoring of a 4096-image sequence), and others listed under
---workload; the default line is the stereo one.
+Default workload (one step): batched all-pairs matching of 200 synthetic images (1000..12000
+uint8 SIFT-like features each, 15% shared tracks): all 19,900 pairs in one call, minScore 0.7,
+ratio 0.8.  Metric: image pairs per second.  `value` times the steps with descriptors resident
+in HBM (the device-output C-ABI call, replayed as a CUDA graph); `e2e` times the same step
+through the host C-ABI calls (pinned host descriptors in, host (pair, left, right) triples out,
+copies inside the timed region).
+Other workloads (--workload): pair (one 4096 x 4096 pair, putative), stereo (one 16384 x 16384
+pair, putative + F-guided), voctree (2M descriptors through a BF 10, depth 6 tree), proposal
+(learned candidate proposal against exhaustive matching), float (float descriptors, BF16 hi/lo
+path), ingest (feature files to device descriptors), retrieval (the voctree app's image-retrieval
+scoring of a 4096-image sequence) and ransac (batched essential-matrix RANSAC).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
 
-Under torchrun each rank runs an independent replica on its own GPU (the path is one pair per
-GPU; pairs are independent), timed on the device, max over ranks.
+Under torchrun each rank runs an independent replica on its own GPU (pairs are independent; the
+path shards with no exchange), timed on the device, max over ranks.
 """
 from __future__ import annotations
 
@@ -46,9 +48,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["stereo", "batch", "voctree", "proposal", "float", "ingest", "retrieval",
-                                                   "ransac"],
-                    default="stereo")
+    ap.add_argument("--workload", choices=["batch", "pair", "stereo", "voctree", "proposal", "float", "ingest",
+                                           "retrieval", "ransac"],
+                    default="batch")
     ap.add_argument("--kernel", choices=["tcgen05", "simt"], default="tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
@@ -164,16 +166,37 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_stereo(L, R, lpos, rpos, F, n_left_sample: int, threads: int = 0):
-    """Oracle putative + F-guided matching of n_left_sample lefts against all rights; returns
-    (seconds, fraction of the full pair covered)."""
+def cpu_stereo(L, R, lpos, rpos, F, threads: int = 0):
+    """Oracle putative + F-guided matching of the whole pair from one score computation (the
+    reference's guided call masks the putative call's stored matrix); returns seconds."""
     from oracle import oracle
-    Ls, lp = L[:n_left_sample], lpos[:n_left_sample]
     t0 = time.perf_counter()
-    oracle.match(Ls, R, MIN_SCORE, MIN_RATIO, threads=threads)
-    oracle.match(Ls, R, MIN_SCORE, MIN_RATIO, gates=[("F", F, GATE_PX)], lpos=lp, rpos=rpos, threads=threads)
-    dt = time.perf_counter() - t0
-    return dt, n_left_sample / L.shape[0]
+    oracle.match_calls(L, R, MIN_SCORE, MIN_RATIO, [[], [("F", F, GATE_PX)]], lpos=lpos, rpos=rpos,
+                       threads=threads)
+    return time.perf_counter() - t0
+
+
+def ref_gpu_key(desc, offs, pairs, reps, positions=None, F=None, what=""):
+    """The reference's own CUDA matcher (v3d_cudamatching.cu built unmodified for sm_100a: cuBLAS
+    SGEMM of the full score matrix, its maxima kernels, blocking copies) in the apps' per-pair
+    loop on this GPU, wall time per repetition; None when that build is absent."""
+    from oracle import oracle
+    if not oracle.ref_cuda_available():
+        return None
+    try:
+        r = oracle.ref_cuda_time_pairs(desc, offs, pairs, MIN_SCORE, MIN_RATIO, reps + 1, positions=positions,
+                                       F=F, thr=GATE_PX)
+    except Exception as e:  # the reference exits on CUDA errors; report instead of failing the arm
+        return {"unavailable": f"reference matcher failed: {str(e)[-200:]}"}
+    sec = r["seconds"][1:]  # the first repetition warms cuBLAS and the allocator
+    t = statistics.mean(sec)
+    n = len(pairs)
+    return {"value": n / t, "unit": "pairs/s", "ms_per_step": 1000.0 * t, "reps": len(sec),
+            "pairs_per_rep": n, "matches_found": r["matches"],
+            "what": "the reference's CUDA SIFT_Matching (cublasSgemm + its maxima kernels, built unmodified for "
+                    "sm_100a) on this GPU in the apps' loop: setLeft/RightFeatures from pageable host memory, "
+                    "findPutativeMatches" + (", runGuidedMatching" if F is not None else "") +
+                    " per pair; counts rounded down to multiples of 32 as the apps do; wall time " + what}
 
 
 def run_reference_arm(args, ws, rank):
@@ -181,35 +204,48 @@ def run_reference_arm(args, ws, rank):
         return run_reference_retrieval(args, ws, rank)
     if args.workload == "ransac":
         return run_reference_ransac(args, ws, rank)
-    return run_reference_stereo(args, ws, rank)
+    if args.workload == "batch":
+        return run_reference_batch(args, ws, rank)
+    if args.workload == "pair":
+        return run_reference_pair(args, ws, rank)
+    if args.workload == "stereo":
+        return run_reference_stereo(args, ws, rank)
+    print(json.dumps({"impl": "reference", "unavailable": f"no reference arm for workload {args.workload}"}),
+          flush=True)
+
+
+def _reference_line(args, metric, v, ms, config, sample, dtype="u8"):
+    from oracle import oracle
+    return {
+        "impl": "reference", "metric": metric, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded generator)",
+        "config": config,
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
 
 
 def run_reference_stereo(args, ws, rank):
-    """The reference's CPU path (the oracle port: the reference has no CPU matcher of its own),
-    all host threads, on the same workload; each step is a bounded sample."""
-    from oracle import oracle
+    """The reference's path on the host cores: the oracle port (the reference has no CPU
+    matcher of its own), all host threads, the whole 16384 x 16384 pair per step: one score
+    computation, putative then F-guided decisions."""
     from v3dm import synth
     if rank != 0:
         return
     L, R, lpos, rpos, F, _ = synth.stereo(args.seed, N_SIDE, N_SIDE)
-    sample = 2048
     for _ in range(args.warmup):
-        cpu_stereo(L, R, lpos, rpos, F, sample)
-    times = []
-    for _ in range(args.steps):
-        dt, frac = cpu_stereo(L, R, lpos, rpos, F, sample)
-        times.append(dt / frac)
+        cpu_stereo(L, R, lpos, rpos, F)
+    times = [cpu_stereo(L, R, lpos, rpos, F) for _ in range(args.steps)]
     ms = 1000.0 * statistics.mean(times)
-    v = 1000.0 / ms
-    line = {
-        "impl": "reference", "metric": "image pairs/s (16384x16384 putative + F-guided)", "value": v,
-        "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": stereo_config(args, "cpu"),
-        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
-                         "sample": f"{sample} of 16384 lefts x all 16384 rights per step, extrapolated x8"},
-        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    line = _reference_line(args, "image pairs/s (16384x16384 putative + F-guided)", 1000.0 / ms, ms,
+                           stereo_config(args, "cpu"),
+                           "the whole pair per step (one score computation, putative and guided decisions)")
+    off = np.array([0, N_SIDE, 2 * N_SIDE], np.int32)
+    line["reference_gpu"] = ref_gpu_key(np.concatenate([L, R]), off, np.array([[0, 1]], np.int32), 5,
+                                        positions=np.concatenate([lpos, rpos]), F=np.asarray(F).reshape(1, 9),
+                                        what="of the pair's putative + guided calls")
     print(json.dumps(line), flush=True)
 
 
@@ -356,10 +392,159 @@ def run_stereo(args, ws, rank, local):
     }
     if not args.no_cpu_baseline and ws == 1:
         from oracle import oracle
-        dt, frac = cpu_stereo(L, R, lpos, rpos, F, 2048)
-        line["cpu_baseline"] = {"value": frac / dt, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
-                                "sample": "2048 of 16384 lefts x all 16384 rights, putative + guided, "
-                                          "extrapolated x8"}
+        dt = cpu_stereo(L, R, lpos, rpos, F)
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                                "sample": "the whole pair once: one score computation, putative and guided "
+                                          "decisions"}
+    print(json.dumps(line), flush=True)
+
+
+N_PAIR = 4096
+
+
+def pair_config(args, where):
+    return {"workload": "one pair 4096x4096 uint8 SIFT-like (30% planted noisy copies), putative, minScore 0.7, "
+                        "ratio 0.8", "n_left": N_PAIR, "n_right": N_PAIR, "seed": args.seed,
+            "kernel": args.kernel if where == "gpu" else "oracle",
+            "l2": "flushed between steps (512 MiB write on the matcher stream, outside the step events)"}
+
+
+def run_pair(args, ws, rank, local):
+    """One 4096 x 4096 pair, putative matching: a step is one findPutativeMatches call."""
+    import torch
+
+    import v3dm
+    from v3dm import synth
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L, R, _ = synth.pair(args.seed, N_PAIR, N_PAIR)
+    kern = v3dm.KERNEL_TCGEN05 if args.kernel == "tcgen05" else v3dm.KERNEL_SIMT
+    m = v3dm.SIFTMatching(local, kern)
+    m.allocate(N_PAIR, N_PAIR)
+    stream = torch.cuda.ExternalStream(m.stream(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    m.set_left_features(L)
+    m.set_right_features(R)
+    d_pairs = torch.empty((N_PAIR, 2), dtype=torch.int32, device=dev)
+    d_cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    if args.tile_config < 0:
+        m.autotune(MIN_SCORE, MIN_RATIO, 3)
+    else:
+        m.set_config(args.tile_config)
+    cfg_id, cfg_rows, cfg_cols = m.config()
+    for _ in range(max(args.warmup, 3)):
+        m.putative_device(MIN_SCORE, MIN_RATIO, d_pairs.data_ptr(), d_cnt.data_ptr())
+        try:
+            m.wait()
+        except v3dm.V3DMError as e:  # the candidate list grew: the next call repeats it
+            if e.status != v3dm.ERR_CANDIDATES:
+                raise
+    steps = max(args.steps, 200)  # a 4096^2 call is tens of microseconds: enough steps for the clock sampler
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches = 0
+    m.profile(True)
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[i][0].record(stream)
+        m.putative_device(MIN_SCORE, MIN_RATIO, d_pairs.data_ptr(), d_cnt.data_ptr())
+        launches += m.last_launches()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    m.wait()
+    ms = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in ev), dev)
+    kms, kl = m.profile_read(0)
+    m.profile(False)
+    k_avg_ms = max_over_ranks(ws, kms / max(kl, 1), dev)
+    n_found = int(d_cnt[0].item())
+
+    Lp = torch.from_numpy(L).pin_memory().numpy()
+    Rp = torch.from_numpy(R).pin_memory().numpy()
+
+    def step_host():
+        m.set_left_features(Lp)
+        m.set_right_features(Rp)
+        return m.find_putative_matches(MIN_SCORE, MIN_RATIO).shape[0]
+
+    for _ in range(max(args.warmup, 3)):
+        step_host()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    n_host = 0
+    barrier(ws)
+    torch.cuda.synchronize()
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev2[i][0].record(stream)
+        n_host = step_host()
+        ev2[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(b) for a, b in ev2), dev)
+    m.close()
+    if rank != 0:
+        return
+    peaks = load_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    ops = 2.0 * N_PAIR * N_PAIR * 128
+    achieved = ops / (k_avg_ms * 1e-3) / 1e12
+    line = {
+        "metric": "image pairs/s (4096x4096 putative)", "value": ws * 1000.0 / ms, "unit": "pairs/s",
+        "n_gpus": ws, "steps": steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": pair_config(args, "gpu"),
+        "tile": {"config": cfg_id, "left_rows": cfg_rows, "right_cols": cfg_cols,
+                 "chosen_by": "autotune" if args.tile_config < 0 else "flag"},
+        "pairs_found": n_found,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS(int8)",
+                     "frac": achieved / int8_peak, "traffic": traffic_from_profiles("k_side_pair4096"),
+                     "peak_src": f"2 x {peaks['src']} bf16 dense ({peaks['bf16_tflops']} TFLOP/s burst)",
+                     "kernel_ms": k_avg_ms, "ops_per_launch": ops,
+                     "kernel": "k_side pass A (every left x every right)"},
+        "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(L.nbytes + R.nbytes),
+                "d2h_bytes_per_step": int(n_host * 8 + 16)},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import oracle
+        reps = 0
+        t0 = time.perf_counter()
+        while reps < 3 or time.perf_counter() - t0 < 5.0:
+            oracle.match(L, R, MIN_SCORE, MIN_RATIO)
+            reps += 1
+        dt = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                                "sample": f"the whole pair, {reps} times"}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_pair(args, ws, rank):
+    """The reference's path on the host cores for the 4096 x 4096 pair: the oracle port, all host
+    threads, the whole pair per step."""
+    from oracle import oracle
+    from v3dm import synth
+    if rank != 0:
+        return
+    L, R, _ = synth.pair(args.seed, N_PAIR, N_PAIR)
+    for _ in range(args.warmup):
+        oracle.match(L, R, MIN_SCORE, MIN_RATIO)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.match(L, R, MIN_SCORE, MIN_RATIO)
+        times.append(time.perf_counter() - t0)
+    ms = 1000.0 * statistics.mean(times)
+    line = _reference_line(args, "image pairs/s (4096x4096 putative)", 1000.0 / ms, ms, pair_config(args, "cpu"),
+                           "the whole pair per step")
+    off = np.array([0, N_PAIR, 2 * N_PAIR], np.int32)
+    line["reference_gpu"] = ref_gpu_key(np.concatenate([L, R]), off, np.array([[0, 1]] * 20, np.int32), 5,
+                                        what="of 20 putative calls on the pair")
     print(json.dumps(line), flush=True)
 
 
@@ -442,10 +627,7 @@ def run_batch(args, ws, rank, local):
         "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{args.images} images, 1000..12000 uint8 SIFT-like features each, 15% shared "
-                               f"tracks, all {n_pairs} pairs, minScore 0.7, ratio 0.8", "pairs": n_pairs,
-                   "descriptors": int(counts.sum()), "seed": args.seed + 1,
-                   "l2": f"inputs larger than L2 ({desc.nbytes / 1e6:.0f} MB of descriptors and the per-pair state)"},
+        "config": batch_config(args, n_pairs, int(counts.sum()), desc.nbytes),
         "aggregate_int8_tops": ops / (ms * 1e-3) / 1e12,
         "tile": {"config": cfg, "schedule": sch, "chosen_by": "autotune" if args.tile_config < 0 else "flag"},
         "pairs_found": n_out,
@@ -461,19 +643,67 @@ def run_batch(args, ws, rank, local):
     }
     if not args.no_cpu_baseline and ws == 1:
         from oracle import oracle
-        pairs = synth.all_pairs(len(counts))
-        rng = np.random.default_rng(0)
-        sample = rng.choice(len(pairs), 12, replace=False)
-        t0 = time.perf_counter()
-        s_ops = 0
-        for k in sample:
-            i, j = pairs[k]
-            oracle.match(desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]], MIN_SCORE, MIN_RATIO)
-            s_ops += 2 * 128 * int(counts[i]) * int(counts[j])
-        dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": n_pairs / (dt * ops / s_ops), "unit": "pairs/s",
-                                "cores": oracle.num_threads(), "kind": "port",
-                                "sample": f"12 random pairs of the {n_pairs}, extrapolated by int8 operations"}
+        n_s, dt = cpu_batch_sample(desc, counts, offs, BATCH_CPU_SAMPLE, 0)
+        line["cpu_baseline"] = {"value": n_s / dt, "unit": "pairs/s", "cores": oracle.num_threads(), "kind": "port",
+                                "sample": f"{n_s} pairs drawn uniformly from the {n_pairs} (seed 0), each matched "
+                                          f"in full ({dt:.1f} s); value = pairs / time, not extrapolated"}
+    print(json.dumps(line), flush=True)
+
+
+BATCH_CPU_SAMPLE = 150   # pairs in the cpu_baseline leg (about 10 s of oracle work on 16 threads)
+BATCH_REF_STEP = 16      # pairs per step of the reference arm
+BATCH_REF_GPU = 400      # pairs per repetition of the reference's CUDA matcher
+
+
+def batch_config(args, n_pairs, n_desc, l2_bytes):
+    return {"workload": f"{args.images} images, 1000..12000 uint8 SIFT-like features each, 15% shared "
+                        f"tracks, all {n_pairs} pairs, minScore 0.7, ratio 0.8", "pairs": n_pairs,
+            "descriptors": n_desc, "seed": args.seed + 1,
+            "l2": f"inputs larger than L2 ({l2_bytes / 1e6:.0f} MB of descriptors and the per-pair state)"}
+
+
+def batch_sample(n_images, k, seed):
+    from v3dm import synth
+    pairs = synth.all_pairs(n_images)
+    rng = np.random.default_rng(seed)
+    return pairs[rng.choice(len(pairs), min(k, len(pairs)), replace=False)]
+
+
+def cpu_batch_sample(desc, counts, offs, k, seed, threads: int = 0):
+    """The oracle on k pairs drawn uniformly from all pairs, each matched in full; returns
+    (pairs matched, seconds)."""
+    from oracle import oracle
+    sample = batch_sample(len(counts), k, seed)
+    t0 = time.perf_counter()
+    for i, j in sample:
+        oracle.match(desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]], MIN_SCORE, MIN_RATIO, threads=threads)
+    return len(sample), time.perf_counter() - t0
+
+
+def run_reference_batch(args, ws, rank):
+    """The reference's path on the host cores for the all-pairs workload: the oracle port, all
+    host threads; each step matches BATCH_REF_STEP pairs drawn uniformly from the 19,900 (a new
+    draw per step), each in full.  value = pairs matched / time (a sample, not extrapolated)."""
+    from v3dm import synth
+    if rank != 0:
+        return
+    desc, counts, offs = synth.images(args.seed + 1, n_images=args.images)
+    n_pairs = args.images * (args.images - 1) // 2
+    for w in range(args.warmup):
+        cpu_batch_sample(desc, counts, offs, 2, 1000 + w)
+    times, done = [], 0
+    for k in range(args.steps):
+        n, dt = cpu_batch_sample(desc, counts, offs, BATCH_REF_STEP, 1 + k)
+        times.append(dt)
+        done += n
+    ms = 1000.0 * statistics.mean(times)
+    line = _reference_line(args, f"image pairs/s (all {n_pairs} pairs of {args.images} images)",
+                           done / sum(times), ms, batch_config(args, n_pairs, int(counts.sum()), desc.nbytes),
+                           f"{BATCH_REF_STEP} pairs per step drawn uniformly from the {n_pairs} (a new draw per "
+                           "step), each matched in full; value = pairs / time, not extrapolated")
+    sample = batch_sample(len(counts), BATCH_REF_GPU, 0)
+    line["reference_gpu"] = ref_gpu_key(desc, offs, sample, 3,
+                                        what=f"of {len(sample)} pairs drawn uniformly from the {n_pairs} (seed 0)")
     print(json.dumps(line), flush=True)
 
 
@@ -671,6 +901,7 @@ def run_proposal(args, ws, rank, local):
         b.match_proposal_device(net, args.probes, MIN_SCORE, MIN_RATIO, d_cnt.data_ptr(), args.probes_right)
         assert b.wait() == v3dm.OK
     ka, na = b.profile_read(0)
+    kv, nv = b.profile_read(1)
     b.profile(False)
     # ablation: the same cells fitted to the untrained network
     net0 = v3dm.Projection(local, seed=args.seed)
@@ -724,6 +955,7 @@ def run_proposal(args, ws, rank, local):
         "recall": rec, "precision": prec, "recall_inliers": rec_in,
         "matches_exhaustive": int(len(exh)), "inliers_exhaustive": int(inl.sum()), "matches_proposal": int(len(got)),
         "scored_fraction": scored / exhaustive,
+        "verification_ms": kv / max(nv, 1),
         "ablation_untrained": {"recall": rec0, "precision": prec0, "recall_inliers": rec0_in,
                                "scored_fraction": scored0 / exhaustive,
                                "ms_per_step": ms0},
@@ -1324,6 +1556,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, ws, rank)
+        elif args.workload == "pair":
+            run_pair(args, ws, rank, local)
         elif args.workload == "stereo":
             run_stereo(args, ws, rank, local)
         elif args.workload == "batch":
