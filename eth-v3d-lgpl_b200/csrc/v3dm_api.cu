@@ -540,7 +540,7 @@ int set_features_bf16x3(v3dm_matcher* h, bool left, int n, const float* desc) {
   return stage_to_float(h, left, n);
 }
 
-int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
+int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc, bool onDevice = false) {
   if (!h || n < 0 || (n > 0 && !desc)) return V3DM_ERR_ARG;
   if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
   if (n > (left ? h->nMaxL : h->nMaxR)) return V3DM_ERR_SIZE;
@@ -548,8 +548,8 @@ int set_features_f32(v3dm_matcher* h, bool left, int n, const float* desc) {
   uint8_t* dst = left ? h->dL : h->dR;
   if (n > 0) {
     V3DM_CUDA_TRY(cudaMemsetAsync(h->dInfo + kInfoErr, 0, sizeof(int32_t), h->stream));
-    V3DM_CUDA_TRY(cudaMemcpyAsync(h->dStage, desc, (size_t)n * kDescBytes * sizeof(float), cudaMemcpyHostToDevice,
-                                  h->stream));
+    V3DM_CUDA_TRY(cudaMemcpyAsync(h->dStage, desc, (size_t)n * kDescBytes * sizeof(float),
+                                  onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
     V3DM_CUDA_TRY(launch_f32_to_u8(h->dStage, dst, n, h->dInfo + kInfoErr, h->stream));
     V3DM_CUDA_TRY(cudaMemcpyAsync(h->hInfo + kInfoErr, h->dInfo + kInfoErr, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1007,6 +1007,10 @@ int v3dm_set_left_u8_device(v3dm_matcher* h, int n, const uint8_t* d) { return s
 int v3dm_set_right_u8_device(v3dm_matcher* h, int n, const uint8_t* d) { return set_features_u8(h, false, n, d, true); }
 int v3dm_set_left_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, true, n, d); }
 int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, false, n, d); }
+int v3dm_set_left_f32_device(v3dm_matcher* h, int n, const float* d) { return set_features_f32(h, true, n, d, true); }
+int v3dm_set_right_f32_device(v3dm_matcher* h, int n, const float* d) {
+  return set_features_f32(h, false, n, d, true);
+}
 int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, true, n, d); }
 int v3dm_set_right_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, false, n, d); }
 

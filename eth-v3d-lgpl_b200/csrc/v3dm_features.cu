@@ -10,9 +10,13 @@
 // 540 bytes per feature.  Here:
 //   - v3dm_features_read parses one file into caller arrays (the reference's deserializer);
 //   - a loader reads many files at once (one host thread per file at a time), keeps the
-//     positions on the host, copies all descriptors to the device in one transfer from pinned
-//     memory and re-quantises them there to u8 (u = round(512 x), clamped to 0..255), ready for
-//     the u8 matchers (v3dm_batch_set_images_u8_device, v3dm_set_left_u8_device).
+//     positions on the host and copies all descriptors to the device in one transfer from
+//     pinned memory.  There they become u8 (u = 512 x) for the u8 matchers
+//     (v3dm_batch_set_images_u8_device, v3dm_set_left_u8_device) when every value is exactly
+//     u/512; the extractors' unit-L2 floats (normalizeDescriptor, v3d_feature.h:19-39) are not,
+//     so those are kept as floats (V3DM_LOAD_KEEP_F32) for the float matcher
+//     (v3dm_set_left_f32_device: BF16 hi/lo scores), refused (V3DM_ERR_NOT_U8), or rounded
+//     only when the caller asks for it (V3DM_LOAD_LOSSY_U8).
 // The text archive ("V3DTXT") is not read: V3DM_ERR_UNSUPPORTED.
 #include <algorithm>
 #include <atomic>
@@ -103,28 +107,41 @@ int decode_features(FILE* f, long long n, int32_t* ids, float* pos, float* dir, 
 }
 
 // u8 re-quantisation: u = round(512 x) (half to even), clamped to 0..255; NaN gives 0.  For
-// descriptors of the form u/512 it returns u.  Four values per thread.
-__global__ void k_quantize_u8(const float4* __restrict__ x, long long n4, uchar4* __restrict__ out) {
+// descriptors of the form u/512 it returns u.  Four values per thread.  When inexact is not
+// null, it is set to 1 if any value is not exactly u/512 with u in 0..255 (one atomic per
+// warp that saw such a value).
+__global__ void k_quantize_u8(const float4* __restrict__ x, long long n4, uchar4* __restrict__ out,
+                              int* __restrict__ inexact) {
+  bool bad = false;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
     const float4 v = x[i];
-    auto q = [](float a) -> unsigned char {
-      if (!(a == a)) return 0;
-      const float r = rintf(a * 512.0f);
-      return (unsigned char)fminf(fmaxf(r, 0.0f), 255.0f);
+    auto q = [&bad](float a) -> unsigned char {
+      if (!(a == a)) {
+        bad = true;
+        return 0;
+      }
+      const float t = a * 512.0f;  // exact: a power-of-two scale
+      const float r = rintf(t);
+      const float c = fminf(fmaxf(r, 0.0f), 255.0f);
+      bad |= c != t;
+      return (unsigned char)c;
     };
     out[i] = make_uchar4(q(v.x), q(v.y), q(v.z), q(v.w));
   }
+  if (inexact && __any_sync(__activemask(), bad) && (threadIdx.x & 31) == (__ffs(__activemask()) - 1))
+    atomicOr(inexact, 1);
 }
 
 }  // namespace
 
-cudaError_t launch_quantize_u8(const float* d_x, long long nValues, uint8_t* d_out, cudaStream_t s) {
+cudaError_t launch_quantize_u8(const float* d_x, long long nValues, uint8_t* d_out, cudaStream_t s,
+                               int* d_inexact) {
   if (nValues <= 0) return cudaSuccess;
   if (nValues % 4 != 0) return cudaErrorInvalidValue;
   const long long n4 = nValues / 4;
   const long long blocks = std::min<long long>((n4 + 255) / 256, 148LL * 16);
   k_quantize_u8<<<(unsigned)blocks, 256, 0, s>>>(reinterpret_cast<const float4*>(d_x), n4,
-                                                  reinterpret_cast<uchar4*>(d_out));
+                                                  reinterpret_cast<uchar4*>(d_out), d_inexact);
   return cudaGetLastError();
 }
 
@@ -143,6 +160,11 @@ struct v3dm_loader {
   long long descCap = 0;    // bytes
   std::vector<float> positions;
   long long total = 0;      // features kept by the last load
+  int* dInexact = nullptr;  // device flag: a value of the last load was not u/512
+  int* hInexact = nullptr;  // pinned copy
+  bool keptF32 = false;     // dStage holds the last load's floats for the caller
+  bool u8Valid = false;     // dDesc holds the last load's descriptors as u8 (exact or lossy by request)
+  bool exact = false;       // every value of the last load was u/512, u in 0..255
 };
 
 namespace {
@@ -206,7 +228,11 @@ int v3dm_loader_create(int device, v3dm_loader** out) {
   if (!ld) return V3DM_ERR_ARG;
   ld->device = device;
   LoaderDeviceGuard g(device);
-  if (cudaStreamCreateWithFlags(&ld->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&ld->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&ld->dInexact), sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&ld->hInexact), sizeof(int)) != cudaSuccess) {
+    if (ld->dInexact) cudaFree(ld->dInexact);
+    if (ld->stream) cudaStreamDestroy(ld->stream);
     delete ld;
     return V3DM_ERR_CUDA;
   }
@@ -221,6 +247,8 @@ int v3dm_loader_destroy(v3dm_loader* ld) {
   if (ld->hStage) cudaFreeHost(ld->hStage);
   if (ld->dStage) cudaFree(ld->dStage);
   if (ld->dDesc) cudaFree(ld->dDesc);
+  if (ld->dInexact) cudaFree(ld->dInexact);
+  if (ld->hInexact) cudaFreeHost(ld->hInexact);
   if (ld->stream) cudaStreamDestroy(ld->stream);
   delete ld;
   return V3DM_OK;
@@ -229,7 +257,7 @@ int v3dm_loader_destroy(v3dm_loader* ld) {
 int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* paths, int maxPerImage, int flags,
                      int32_t* counts) {
   if (!ld || nFiles < 0 || (nFiles > 0 && (!paths || !counts))) return V3DM_ERR_ARG;
-  if ((flags & ~V3DM_LOAD_ROUND32) != 0) return V3DM_ERR_ARG;
+  if ((flags & ~(V3DM_LOAD_ROUND32 | V3DM_LOAD_KEEP_F32 | V3DM_LOAD_LOSSY_U8)) != 0) return V3DM_ERR_ARG;
   if (!host_little_endian()) return V3DM_ERR_UNSUPPORTED;
   LoaderDeviceGuard g(ld->device);
   // headers: how many features each file holds and how many are kept
@@ -274,6 +302,7 @@ int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* paths, int 
   }
   ld->positions.assign((size_t)total * 2, 0.0f);
   ld->total = 0;
+  ld->keptF32 = ld->u8Valid = ld->exact = false;
   // decode: files are handed out to the host threads one at a time
   std::atomic<int> next(0), err(V3DM_OK);
   auto work = [&]() {
@@ -297,15 +326,23 @@ int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* paths, int 
   work();
   for (auto& t : pool) t.join();
   if (err.load() != V3DM_OK) return err.load();
-  // one copy to the device, re-quantisation there
+  // one copy to the device, u8 conversion there with a flag for values that are not u/512
+  *ld->hInexact = 0;
+  V3DM_LTRY(cudaMemsetAsync(ld->dInexact, 0, sizeof(int), ld->stream));
   if (nValues > 0) {
     V3DM_LTRY(cudaMemcpyAsync(ld->dStage, ld->hStage, (size_t)nValues * sizeof(float), cudaMemcpyHostToDevice,
                               ld->stream));
-    V3DM_LTRY(launch_quantize_u8(ld->dStage, nValues, ld->dDesc, ld->stream));
+    V3DM_LTRY(launch_quantize_u8(ld->dStage, nValues, ld->dDesc, ld->stream, ld->dInexact));
+    V3DM_LTRY(cudaMemcpyAsync(ld->hInexact, ld->dInexact, sizeof(int), cudaMemcpyDeviceToHost, ld->stream));
   }
   V3DM_LTRY(cudaStreamSynchronize(ld->stream));
   for (int i = 0; i < nFiles; ++i) counts[i] = (int32_t)kept[i];
   ld->total = total;
+  ld->exact = *ld->hInexact == 0;
+  ld->keptF32 = (flags & V3DM_LOAD_KEEP_F32) != 0;
+  ld->u8Valid = ld->exact || (flags & V3DM_LOAD_LOSSY_U8) != 0;
+  // floats that are not u/512 with neither floats kept nor rounding asked for: refuse
+  if (!ld->u8Valid && !ld->keptF32) return V3DM_ERR_NOT_U8;
   return V3DM_OK;
 }
 
@@ -317,8 +354,25 @@ int v3dm_loader_positions(v3dm_loader* ld, float* positions) {
 
 int v3dm_loader_descriptors_device(v3dm_loader* ld, const uint8_t** d_desc, long long* total) {
   if (!ld || !d_desc || !total) return V3DM_ERR_ARG;
-  *d_desc = ld->dDesc;
+  *d_desc = nullptr;
   *total = ld->total;
+  if (ld->total > 0 && !ld->u8Valid) return V3DM_ERR_NOT_U8;
+  *d_desc = ld->dDesc;
+  return V3DM_OK;
+}
+
+int v3dm_loader_descriptors_f32_device(v3dm_loader* ld, const float** d_desc, long long* total) {
+  if (!ld || !d_desc || !total) return V3DM_ERR_ARG;
+  *d_desc = nullptr;
+  *total = ld->total;
+  if (!ld->keptF32) return V3DM_ERR_NOT_ALLOCATED;
+  *d_desc = ld->dStage;
+  return V3DM_OK;
+}
+
+int v3dm_loader_exact_u8(v3dm_loader* ld, int* exact) {
+  if (!ld || !exact) return V3DM_ERR_ARG;
+  *exact = ld->exact ? 1 : 0;
   return V3DM_OK;
 }
 

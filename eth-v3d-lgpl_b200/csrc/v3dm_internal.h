@@ -29,6 +29,7 @@ cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, 
 constexpr int kErrWaitTimeout = 1;  // a bounded mbarrier wait in the tcgen05 kernel gave up
 constexpr int kErrNotU8 = 2;        // a float descriptor was not u/512-valued
 constexpr int kErrTmem = 4;         // TMEM allocation returned an unexpected address
+constexpr int kErrBadTree = 8;      // a vocabulary-tree descent would have left the node array
 
 // Layout of the small info block every matching call writes (int32 words).
 constexpr int kInfoPairs = 0;     // number of mutual pairs
@@ -176,7 +177,8 @@ struct PostArgs {
 };
 cudaError_t launch_post(const PostArgs& a, cudaStream_t s);
 // u8 re-quantisation of nValues floats (a multiple of 4), v3dm_features.cu.
-cudaError_t launch_quantize_u8(const float* d_x, long long nValues, uint8_t* d_out, cudaStream_t s);
+cudaError_t launch_quantize_u8(const float* d_x, long long nValues, uint8_t* d_out, cudaStream_t s,
+                               int* d_inexact = nullptr);
 
 // ---- float descriptors: BF16 hi/lo scores (v3dm_match_f.cu) ------------------------------
 // Operand layouts: 6 planes of rowsCap x 128 bytes (64 BF16 values of a K slice per row).

@@ -65,10 +65,14 @@ def _files(tmp_path, counts, seed=2, real_floats=False):
 
 @pytest.mark.parametrize("max_per_image,flags", [(0, 0), (0, 1), (700, 0), (700, 1)])
 def test_loader_equals_reader_and_quantisation(v3dm_mod, tmp_path, max_per_image, flags):
+    """Unit-L2 float files rounded on request (LOAD_LOSSY_U8) equal the reader's floats
+    quantised by numpy; the positions equal the reader's."""
     counts = [1000, 0, 31, 33, 2500, 700, 64]
     paths, feats = _files(tmp_path, counts, real_floats=True)
+    flags |= v3dm_mod.LOAD_LOSSY_U8
     with v3dm_mod.Loader() as ld:
         kept = ld.load(paths, max_per_image, flags)
+        assert not ld.exact_u8()
         exp_kept = []
         for n in counts:
             k = n & ~31 if flags & v3dm_mod.LOAD_ROUND32 else n
@@ -133,3 +137,74 @@ def test_loader_errors(v3dm_mod, tmp_path):
         assert e.value.status == v3dm_mod.ERR_UNSUPPORTED
         # still usable after an error
         np.testing.assert_array_equal(ld.load(paths), [100, 50])
+
+
+def test_loader_refuses_to_round_unit_floats_silently(v3dm_mod, tmp_path):
+    """The extractors store unit-L2 floats; without LOAD_LOSSY_U8 or LOAD_KEEP_F32 the loader
+    reports them instead of rounding them.  u/512 files load as u8 with no flag."""
+    paths, _ = _files(tmp_path, [300, 200], real_floats=True)
+    (tmp_path / "u").mkdir()
+    upaths, ufeats = _files(tmp_path / "u", [300, 200])
+    with v3dm_mod.Loader() as ld:
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            ld.load(paths)
+        assert e.value.status == v3dm_mod.ERR_NOT_U8
+        np.testing.assert_array_equal(ld.load(upaths), [300, 200])
+        assert ld.exact_u8()
+        d_ptr, total = ld.descriptors_device()
+        got = _device_bytes(d_ptr, total * 128).reshape(total, 128)
+        np.testing.assert_array_equal(got, np.concatenate([_quantize(f["descriptors"]) for f in ufeats]))
+        # floats kept: the u8 view is refused, the float view is the file's floats
+        ld.load(paths, 0, v3dm_mod.LOAD_KEEP_F32)
+        with pytest.raises(v3dm_mod.V3DMError) as e:
+            ld.descriptors_device()
+        assert e.value.status == v3dm_mod.ERR_NOT_U8
+
+
+def _device_floats(ptr, n):
+    raw = _device_bytes(ptr, n * 4)
+    return raw.view(np.float32)
+
+
+def test_loader_keeps_floats_for_the_float_matcher(v3dm_mod, tmp_path):
+    """Feature files of unit-L2 float descriptors (what the extractors write): the loader keeps
+    the floats bit for bit (LOAD_KEEP_F32), and matching them from the loader's device buffer
+    gives the same pairs as matching the in-memory floats (the BF16 hi/lo path), for putative
+    and F-guided matching."""
+    L, R, lp, rp, F, _ = synth.stereo(17, 1800, 2100)
+    rng = np.random.default_rng(3)
+    # unit-L2 floats with the generator's directions (not u/512)
+    Lf = (L.astype(np.float32) + rng.uniform(-0.49, 0.49, L.shape).astype(np.float32))
+    Rf = (R.astype(np.float32) + rng.uniform(-0.49, 0.49, R.shape).astype(np.float32))
+    Lf = np.maximum(Lf, 0) / np.linalg.norm(np.maximum(Lf, 0), axis=1, keepdims=True)
+    Rf = np.maximum(Rf, 0) / np.linalg.norm(np.maximum(Rf, 0), axis=1, keepdims=True)
+    Lf, Rf = Lf.astype(np.float32), Rf.astype(np.float32)
+    paths = []
+    for i, (D, P) in enumerate(((Lf, lp), (Rf, rp))):
+        f = synth.feature_arrays(rng, D.shape[0])
+        f["descriptors"] = D
+        f["positions"] = P.astype(np.float32)
+        path = tmp_path / f"s{i}.features"
+        synth.write_features(path, f)
+        paths.append(str(path))
+    with v3dm_mod.Loader() as ld:
+        kept = ld.load(paths, 0, v3dm_mod.LOAD_KEEP_F32)
+        np.testing.assert_array_equal(kept, [1800, 2100])
+        assert not ld.exact_u8()
+        d_ptr, total = ld.descriptors_f32_device()
+        assert total == 3900
+        np.testing.assert_array_equal(_device_floats(d_ptr, total * 128).reshape(total, 128),
+                                      np.concatenate([Lf, Rf]))
+        pos = ld.positions()
+        np.testing.assert_array_equal(pos, np.concatenate([lp, rp]).astype(np.float32))
+        with v3dm_mod.SIFTMatching() as m:
+            m.allocate(2100, 2100, True)
+            m.set_left_features_f32_device(d_ptr, 1800)
+            m.set_right_features_f32_device(d_ptr + 1800 * 128 * 4, 2100)
+            put = m.find_putative_matches(0.7, 0.8)
+            gui = m.run_guided_matching(F, 2.0, pos[:1800], pos[1800:], 0.7, 0.8)
+            m.set_left_features(Lf)
+            m.set_right_features(Rf)
+            np.testing.assert_array_equal(put, m.find_putative_matches(0.7, 0.8))
+            np.testing.assert_array_equal(gui, m.run_guided_matching(F, 2.0, lp, rp, 0.7, 0.8))
+            assert put.shape[0] > 100 and 0 < gui.shape[0] <= put.shape[0]
