@@ -4,9 +4,27 @@
 // Tree layout as in the reference: nodeCount x 128 descriptors in breadth-first order
 // without the root; level-1 nodes are 0..BF-1 and the children of node i are
 // (i+1)*BF .. (i+1)*BF + BF-1 (.cu:784-785).  Each level picks the child with the largest
-// dot product, the first child on ties (strict '>', .cu:781).  Nodes and keys are uint8
-// (u/512 in the reference's float convention), so every dot product is an exact integer
-// and leaf ids match the reference whatever the summation order.
+// dot product, the first child on ties (strict '>', .cu:781).
+//
+// Two kernels:
+//   - k_voctree: uint8 nodes and keys (u/512 in the reference's float convention).  Every dot
+//     product is an exact integer, so leaf ids match the reference whatever the summation
+//     order.
+//   - k_voctree_f32: float nodes and keys of any values (the apps' trees are float k-means
+//     centres of unit-L2 descriptors, v3d_voctree.h:38-52).  The leaf ids equal those of the
+//     reference's CPU tree, VocabularyTree::findBestNodeIndex (v3d_voctree.h:82-99), which sums
+//     key[i] * node[i] sequentially for i = 0..127 in FP32 (one rounded product and one rounded
+//     add per term, no FMA: the reference builds for plain x86-64) and keeps the first child
+//     whose score is strictly above the running maximum (initially -1e30f, child -1).
+//     A fast pass scores every child with FMA partial sums (four threads per key, coalesced
+//     64-byte loads) and bounds its distance to the sequential FP32 sum: both are within
+//     gamma_128 * sum|k_i n_i| <= 7.63e-6 * |k| |n| of the exact dot product (the standard bound
+//     for recursive summation, n = 128 terms; the FMA pass has at most 34 roundings per term),
+//     so |fast - sequential| <= 1.53e-5 * |k| |n|; the kernel uses 2e-5 * |k| |n| + 1e-36 with
+//     precomputed node norms rounded up.  When one child's lower bound is above every other
+//     child's upper bound (and above -1e30f), it is the sequential rule's choice.  Otherwise
+//     (near ties, equal children, non-finite values) one thread of the key replays the
+//     reference's sequential FP32 loop over all children, with __fmul_rn / __fadd_rn.
 //
 // Kernel: four threads per key, each holding 32 bytes of the key in registers; a warp
 // descends eight keys.  At each level a thread loads its 32-byte slice of every child (each
@@ -15,6 +33,7 @@
 // instead runs one 32-thread block per key with a racy warp-synchronous shared-memory
 // reduction (.cu:770-779).  (Measured on the BF 10, depth 6 tree with 2M keys: 0.95 ms with
 // four threads per key, 1.18 ms with eight, 1.53 ms with two, 2.86 ms with one.)
+#include <algorithm>
 #include <new>
 
 #include "v3dm_internal.h"
@@ -89,6 +108,365 @@ __global__ void k_vt_f32_to_u8(const float4* __restrict__ src, uint32_t* __restr
   if (!ok) atomicOr(err, 1);
 }
 
+// ---- bucketed descent of uint8 trees ------------------------------------------------------
+// Levels 1..L (the top) are descended by k_vt_top, with the top rows staged in shared memory
+// when they fit; the keys are then sorted by the node they reached (a counting sort over the
+// bf^L nodes of level L), and k_vt_sub descends the remaining T = depth - L levels bucket by
+// bucket: a CTA stages the bucket node's whole subtree (bf + bf^2 + ... + bf^T rows, contiguous
+// per level) in shared memory once and descends every key of the bucket against it.  Each node
+// row then leaves DRAM about once per call, instead of once per key that reaches it (the
+// one-kernel descent re-read the leaf level per key: 4.5x the algorithmic bytes).  The dot
+// products are exact integers, so the order of evaluation does not matter; ties keep the
+// first child (strict '>').
+constexpr int kVtRowsMax = 1600;        // rows of a staged subtree / top (200 KB)
+constexpr int kVtBktThreads = 512;
+constexpr int kVtItemKeys = 2048;       // keys per work item of k_vt_sub
+constexpr int kVtMaxSubLevels = 10;     // levels of a staged subtree
+
+// 16-byte chunk c of staged row r lives at r * 128 + ((c ^ (r & 7)) << 4): rows read by the
+// lanes of one instruction spread over the banks.
+__device__ __forceinline__ uint32_t vt_swz(int r, int c) { return (uint32_t)r * 128u + ((uint32_t)(c ^ (r & 7)) << 4); }
+
+__device__ __forceinline__ void vt_stage(uint8_t* smem, const uint8_t* __restrict__ src, long long rows, int dstRow0) {
+  const int n16 = (int)rows * 8;
+  for (int i = threadIdx.x; i < n16; i += blockDim.x) {
+    const int r = i >> 3, c = i & 7;
+    *reinterpret_cast<uint4*>(smem + vt_swz(dstRow0 + r, c)) = __ldg(reinterpret_cast<const uint4*>(src) + i);
+  }
+}
+
+// Best child of the bf rows starting at staged row `row0` for the key slice kw (four threads
+// per key, thread `part` holding chunks 2 part, 2 part + 1).
+__device__ __forceinline__ int vt_best_staged(const uint8_t* smem, int row0, int bf, const uint4 (&kw)[kQ], int part,
+                                              bool valid) {
+  int best = 0, bestScore = -1;
+#pragma unroll 2
+  for (int c = 0; c < bf; ++c) {
+    const int r = row0 + c;
+    uint32_t acc = 0;
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < kQ; ++q) {
+        const uint4 w = *reinterpret_cast<const uint4*>(smem + vt_swz(r, part * kQ + q));
+        acc = __dp4a(kw[q].x, w.x, acc);
+        acc = __dp4a(kw[q].y, w.y, acc);
+        acc = __dp4a(kw[q].z, w.z, acc);
+        acc = __dp4a(kw[q].w, w.w, acc);
+      }
+    }
+    int sc = (int)acc;
+#pragma unroll
+    for (int o = 1; o < kTpk; o <<= 1) sc += __shfl_xor_sync(0xffffffffu, sc, o);
+    if (sc > bestScore) {
+      bestScore = sc;
+      best = c;
+    }
+  }
+  return best;
+}
+
+__device__ __forceinline__ void vt_load_key(const uint8_t* __restrict__ keys, int key, int part, bool valid,
+                                            uint4 (&kw)[kQ]) {
+#pragma unroll
+  for (int q = 0; q < kQ; ++q)
+    kw[q] = valid ? __ldg(reinterpret_cast<const uint4*>(keys + (size_t)key * kDescBytes) + part * kQ + q)
+                  : make_uint4(0u, 0u, 0u, 0u);
+}
+
+// Levels 1..L of every key: bucket[key] = its level-L node minus the level's first index, and
+// the bucket histogram.  kStaged: the top rows (nodes 0 .. topRows-1) in shared memory.
+template <bool kStaged>
+__global__ void __launch_bounds__(kVtBktThreads)
+k_vt_top(const uint8_t* __restrict__ nodes, int bf, int L, long long topRows, long long levelStartL,
+         const uint8_t* __restrict__ keys, int n, int32_t* __restrict__ bucket, int* __restrict__ hist) {
+  extern __shared__ __align__(128) uint8_t vsm[];
+  if constexpr (kStaged) {
+    vt_stage(vsm, nodes, topRows, 0);
+    __syncthreads();
+  }
+  const int part = threadIdx.x % kTpk;
+  const int perIter = (gridDim.x * kVtBktThreads) / kTpk;
+  for (int k0 = (blockIdx.x * kVtBktThreads + threadIdx.x) / kTpk; k0 - (int)(threadIdx.x / kTpk) < n; k0 += perIter) {
+    const bool valid = k0 < n;
+    uint4 kw[kQ];
+    vt_load_key(keys, valid ? k0 : 0, part, valid, kw);
+    long long nextId = 0, leafId = 0;
+    for (int d = 0; d < L; ++d) {
+      int best;
+      if constexpr (kStaged) {
+        best = vt_best_staged(vsm, (int)nextId, bf, kw, part, valid);
+      } else {
+        const uint4* base = reinterpret_cast<const uint4*>(nodes + (size_t)nextId * kDescBytes) + part * kQ;
+        int bestScore = -1;
+        best = 0;
+        for (int c = 0; c < bf; ++c) {
+          uint32_t acc = 0;
+          if (valid) {
+#pragma unroll
+            for (int q = 0; q < kQ; ++q) {
+              const uint4 w = __ldg(base + (size_t)c * (kDescBytes / 16) + q);
+              acc = __dp4a(kw[q].x, w.x, acc);
+              acc = __dp4a(kw[q].y, w.y, acc);
+              acc = __dp4a(kw[q].z, w.z, acc);
+              acc = __dp4a(kw[q].w, w.w, acc);
+            }
+          }
+          int sc = (int)acc;
+#pragma unroll
+          for (int o = 1; o < kTpk; o <<= 1) sc += __shfl_xor_sync(0xffffffffu, sc, o);
+          if (sc > bestScore) {
+            bestScore = sc;
+            best = c;
+          }
+        }
+      }
+      leafId = nextId + best;
+      nextId = (leafId + 1) * bf;
+    }
+    if (valid && part == 0) {
+      const int b = (int)(leafId - levelStartL);
+      bucket[k0] = b;
+      atomicAdd(&hist[b], 1);
+    }
+  }
+}
+
+// Bucket offsets and the work items of k_vt_sub: (bucket, first key in sorted order, count),
+// at most kVtItemKeys keys each.  One block.  With bins == 1 and single > 0, one bucket of
+// `single` keys (no top levels, no histogram).
+__global__ void __launch_bounds__(1024)
+k_vt_scan(const int* __restrict__ hist, int bins, int single, int* __restrict__ off, int4* __restrict__ items,
+          int* __restrict__ nItems) {
+  __shared__ long long sh[1024];
+  __shared__ long long shI[1024];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int per = (bins + T - 1) / T;
+  const int b0 = min(bins, tid * per), b1 = min(bins, b0 + per);
+  auto cnt = [&](int b) { return single > 0 ? single : hist[b]; };
+  long long sk = 0, si = 0;
+  for (int b = b0; b < b1; ++b) {
+    sk += cnt(b);
+    si += (cnt(b) + kVtItemKeys - 1) / kVtItemKeys;
+  }
+  sh[tid] = sk;
+  shI[tid] = si;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    const long long v = tid >= o ? sh[tid - o] : 0, w = tid >= o ? shI[tid - o] : 0;
+    __syncthreads();
+    sh[tid] += v;
+    shI[tid] += w;
+    __syncthreads();
+  }
+  long long k = sh[tid] - sk, it = shI[tid] - si;
+  for (int b = b0; b < b1; ++b) {
+    const int c = cnt(b);
+    off[b] = (int)k;
+    for (int j = 0; j < c; j += kVtItemKeys) items[it++] = make_int4(b, (int)k + j, min(kVtItemKeys, c - j), 0);
+    k += c;
+  }
+  if (tid == T - 1) {
+    off[bins] = (int)sh[T - 1];
+    *nItems = (int)shI[T - 1];
+  }
+}
+
+// Keys in bucket order.
+__global__ void k_vt_scatter(const int32_t* __restrict__ bucket, int n, const int* __restrict__ off,
+                             int* __restrict__ cursor, int32_t* __restrict__ perm) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int b = bucket[k];
+    perm[off[b] + atomicAdd(&cursor[b], 1)] = k;
+  }
+}
+
+// Levels L+1..depth, one work item at a time: the item's bucket node p (global index
+// levelStartL + bucket, or the root when L = 0) has its subtree staged (T levels, level t of
+// bf^(t+1) rows starting at global node g_t: g_0 = (p + 1) bf, g_(t+1) = (g_t + 1) bf), and
+// each key of the item descends it: at level t the local node idx has children idx * bf + c.
+__global__ void __launch_bounds__(kVtBktThreads)
+k_vt_sub(const uint8_t* __restrict__ nodes, int bf, int T, long long levelStartL, int haveTop,
+         const int4* __restrict__ items, const int* __restrict__ nItems, const int32_t* __restrict__ perm,
+         const uint8_t* __restrict__ keys, long long leafBase, int32_t* __restrict__ out, int idMode) {
+  extern __shared__ __align__(128) uint8_t vsm[];
+  const int part = threadIdx.x % kTpk;
+  const int nIt = *nItems;
+  int staged = -1;
+  for (int it = blockIdx.x; it < nIt; it += gridDim.x) {
+    const int4 item = items[it];
+    const long long p = haveTop ? levelStartL + item.x : -1;
+    long long g[kVtMaxSubLevels];
+    g[0] = (p + 1) * bf;
+    for (int t = 1; t < T; ++t) g[t] = (g[t - 1] + 1) * bf;
+    if (item.x != staged) {
+      __syncthreads();  // every key of the previous item is done with the staged rows
+      long long len = bf;
+      int row0 = 0;
+      for (int t = 0; t < T; ++t) {
+        vt_stage(vsm, nodes + (size_t)g[t] * kDescBytes, len, row0);
+        row0 += (int)len;
+        len *= bf;
+      }
+      __syncthreads();
+      staged = item.x;
+    }
+    for (int k = threadIdx.x / kTpk; k - (int)(threadIdx.x / kTpk) < item.z; k += kVtBktThreads / kTpk) {
+      const bool valid = k < item.z;
+      const int key = valid ? (perm ? perm[item.y + k] : item.y + k) : 0;
+      uint4 kw[kQ];
+      vt_load_key(keys, key, part, valid, kw);
+      long long idx = 0;
+      int lvlRow = 0;
+      long long lvlLen = bf;
+      for (int t = 0; t < T; ++t) {
+        const int best = vt_best_staged(vsm, lvlRow + (int)(t == 0 ? 0 : idx * bf), bf, kw, part, valid);
+        idx = t == 0 ? best : idx * bf + best;
+        lvlRow += (int)lvlLen;
+        lvlLen *= bf;
+      }
+      if (valid && part == 0) {
+        const long long leafId = g[T - 1] + idx;
+        out[key] = (int32_t)(idMode == V3DM_LEAF_LOCAL ? leafId - leafBase : leafId);
+      }
+    }
+  }
+}
+
+// Bound of |FMA-pass score - sequential FP32 score| relative to |key| |node| (2 gamma_128 =
+// 1.53e-5, with margin for the rounding of the norms), and an absolute term for underflow.
+constexpr float kSeqRel = 2.0e-5f;
+constexpr float kSeqAbs = 1.0e-36f;
+
+// The reference's sequential FP32 scan over the children of one node (v3d_voctree.h:82-99).
+__device__ __forceinline__ int seq_best_child(const float* __restrict__ key, const float* __restrict__ base, int bf) {
+  int bestNode = -1;
+  float maxScore = -1e30f;
+#pragma unroll 1
+  for (int k = 0; k < bf; ++k) {
+    const float* cur = base + (size_t)k * kDescBytes;
+    float score = 0.0f;
+#pragma unroll 4
+    for (int i = 0; i < kDescBytes; ++i) score = __fadd_rn(score, __fmul_rn(__ldg(key + i), __ldg(cur + i)));
+    if (score > maxScore) {
+      bestNode = k;
+      maxScore = score;
+    }
+  }
+  return bestNode;
+}
+
+// Float descent.  Four threads per key; thread `part` holds key floats q*16 + part*4 .. +3 for
+// q = 0..7, so the four threads of a key read 64 contiguous bytes of a node row per load.
+// nodeNorm[i] >= |node i| (L2).  exactCount (optional) counts the key-levels resolved by the
+// sequential replay.  err gets kErrBadTree when a child block would leave the tree.
+__global__ void __launch_bounds__(kVtThreads, 2)
+k_voctree_f32(const float* __restrict__ nodes, const float* __restrict__ nodeNorm, long long nodeCount, int bf,
+              int depth, long long leafBase, const float* __restrict__ keys, int n, int32_t* __restrict__ out,
+              int idMode, unsigned long long* __restrict__ exactCount, int32_t* __restrict__ err) {
+  const int gt = blockIdx.x * kVtThreads + threadIdx.x;
+  const int key = gt / kTpk;
+  const int part = gt % kTpk;
+  const int lane = threadIdx.x & 31;
+  const unsigned grp = 0xfu << (lane & ~3);
+  const bool valid = key < n;
+  const float* krow = keys + (size_t)(valid ? key : 0) * kDescBytes;
+  float4 kv[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    kv[q] = valid ? __ldg(reinterpret_cast<const float4*>(krow) + q * 4 + part) : make_float4(0.f, 0.f, 0.f, 0.f);
+  float ss = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    ss = fmaf(kv[q].x, kv[q].x, ss);
+    ss = fmaf(kv[q].y, kv[q].y, ss);
+    ss = fmaf(kv[q].z, kv[q].z, ss);
+    ss = fmaf(kv[q].w, kv[q].w, ss);
+  }
+  ss += __shfl_xor_sync(0xffffffffu, ss, 1);
+  ss += __shfl_xor_sync(0xffffffffu, ss, 2);
+  const float kn = __fmul_ru(__fsqrt_ru(ss), 1.000001f);
+  long long nextId = 0, leafId = 0;
+  unsigned long long replays = 0;
+  bool ok = true;
+  for (int d = 0; d < depth; ++d) {
+    if (nextId < 0 || nextId + bf > nodeCount) {  // cannot happen for a finite tree; leaves the loop safely
+      ok = false;
+      break;
+    }
+    const float* base = nodes + (size_t)nextId * kDescBytes;
+    float lo1 = -INFINITY, up1 = -INFINITY, up2 = -INFINITY;
+    int c1 = -1, cu1 = -1;
+    bool finite = true;
+#pragma unroll 2
+    for (int c = 0; c < bf; ++c) {
+      const float4* row = reinterpret_cast<const float4*>(base + (size_t)c * kDescBytes) + part;
+      float acc = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 w = __ldg(row + q * 4);
+        acc = fmaf(kv[q].x, w.x, acc);
+        acc = fmaf(kv[q].y, w.y, acc);
+        acc = fmaf(kv[q].z, w.z, acc);
+        acc = fmaf(kv[q].w, w.w, acc);
+      }
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);  // fadd commutes: the four lanes agree exactly
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      const float e = __fadd_ru(__fmul_ru(__fmul_ru(kSeqRel, kn), __ldg(nodeNorm + nextId + c)), kSeqAbs);
+      const float lo = __fsub_rd(acc, e), up = __fadd_ru(acc, e);
+      finite = finite && isfinite(lo) && isfinite(up);
+      if (lo > lo1) {
+        lo1 = lo;
+        c1 = c;
+      }
+      if (up > up1) {
+        up2 = up1;
+        up1 = up;
+        cu1 = c;
+      } else if (up > up2) {
+        up2 = up;
+      }
+    }
+    const float othersUp = cu1 == c1 ? up2 : up1;
+    int best = c1;
+    // the same on the four lanes of the key: their scores and bounds are bit-identical
+    if (!(finite && c1 >= 0 && othersUp < lo1 && lo1 > -1e30f)) {
+      int b = -1;
+      if (part == 0 && valid) {
+        b = seq_best_child(krow, base, bf);
+        ++replays;
+      }
+      best = __shfl_sync(grp, b, lane & ~3);
+    }
+    if (!valid) best = 0;
+    leafId = nextId + best;
+    nextId = (leafId + 1) * bf;
+  }
+  if (!ok && part == 0 && valid) atomicOr(err, kErrBadTree);
+  if (valid && part == 0) out[key] = (int32_t)(idMode == V3DM_LEAF_LOCAL ? leafId - leafBase : leafId);
+  if (exactCount && part == 0 && replays) atomicAdd(exactCount, replays);
+}
+
+// |node i| rounded up, for the bound above (double sum, then an upward margin).
+__global__ void k_node_norms(const float* __restrict__ nodes, long long nodeCount, float* __restrict__ norm) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nodeCount) return;
+  const float4* r = reinterpret_cast<const float4*>(nodes + (size_t)i * kDescBytes);
+  double s = 0.0;
+  for (int q = 0; q < kDescBytes / 4; ++q) {
+    const float4 v = r[q];
+    s += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+  }
+  norm[i] = __double2float_ru(sqrt(s) * (1.0 + 1e-12));
+}
+
+// u8 -> float (u/512), for float keys against a tree given as bytes.
+__global__ void k_u8_to_f32(const uchar4* __restrict__ src, float4* __restrict__ dst, long long n4) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const uchar4 u = src[i];
+  dst[i] = make_float4(u.x / 512.0f, u.y / 512.0f, u.z / 512.0f, u.w / 512.0f);
+}
+
 bool tree_counts(int bf, int depth, long long* nodes, long long* leaves, long long* leafBase) {
   if (bf < 1 || depth < 1) return false;
   long long total = 0, len = 1, base = 0;
@@ -123,43 +501,162 @@ struct v3dm_voctree {
   int bf = 0, depth = 0;
   long long nodeCount = 0, leafCount = 0, leafBase = 0;
   cudaStream_t stream = nullptr;
-  uint8_t* dNodes = nullptr;
+  uint8_t* dNodes = nullptr;    // u8 tree (valid when nodesU8)
+  float* dNodesF = nullptr;     // float tree (valid when nodesF)
+  float* dNorm = nullptr;       // |node i| rounded up (valid when nodesF)
+  bool nodesU8 = false;         // the tree's values are all u/512, u in 0..255
+  bool nodesF = false;
   int nMax = 0;
   uint8_t* dKeys = nullptr;
   float* dStage = nullptr;
   int32_t* dIds = nullptr;
   int32_t* dErr = nullptr;
   int32_t* hErr = nullptr;
+  unsigned long long* dReplays = nullptr;  // key-levels resolved by the sequential replay
+  // bucketed descent of u8 trees: L top levels, T subtree levels (T = 0: one-kernel descent)
+  int L = 0, T = 0;
+  long long topRows = 0, subRows = 0, bins = 1, levelStartL = 0;
+  int32_t* dBucket = nullptr;   // nMax
+  int32_t* dPerm = nullptr;     // nMax
+  int* dHist = nullptr;         // bins, then bins cursors
+  int* dOff = nullptr;          // bins + 1
+  int4* dItems = nullptr;       // nMax / kVtItemKeys + bins + 1
+  int* dNItems = nullptr;
+  int numSMs = 148;
 };
 
 namespace {
 
+// Split of a u8 tree for the bucketed descent: the deepest T levels whose subtree fits the
+// shared-memory budget, the L = depth - T levels above them.
+void vt_plan(v3dm_voctree* t) {
+  long long rows = 0, len = 1;
+  int T = 0;
+  while (T < t->depth && T < kVtMaxSubLevels) {
+    len *= t->bf;
+    if (rows + len > kVtRowsMax) break;
+    rows += len;
+    ++T;
+  }
+  t->T = T;
+  t->L = t->depth - T;
+  t->subRows = rows;
+  long long top = 0, l = 1, startL = 0;
+  for (int d = 0; d < t->L; ++d) {
+    startL = top;
+    l *= t->bf;
+    top += l;
+  }
+  t->topRows = top;
+  t->bins = t->L > 0 ? l : 1;
+  t->levelStartL = startL;
+}
+
 int vt_launch(v3dm_voctree* t, int n, const uint8_t* dKeys, int32_t* dIds, int idMode) {
   if (n == 0) return V3DM_OK;
-  long long threads = (long long)n * kTpk;
-  unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
-  k_voctree<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodes, t->bf, t->depth, t->leafBase, dKeys, n, dIds, idMode);
+  if (t->T == 0 || !t->dPerm || n > t->nMax) {  // one-kernel descent
+    long long threads = (long long)n * kTpk;
+    unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
+    k_voctree<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodes, t->bf, t->depth, t->leafBase, dKeys, n, dIds, idMode);
+    return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
+  }
+  const int bins = (int)t->bins;
+  if (t->L > 0) {
+    if (cudaMemsetAsync(t->dHist, 0, 2 * (size_t)bins * sizeof(int), t->stream) != cudaSuccess) return V3DM_ERR_CUDA;
+    const long long keyBlocks = ((long long)n * kTpk + kVtBktThreads - 1) / kVtBktThreads;
+    const unsigned topGrid = (unsigned)std::min<long long>(keyBlocks, (long long)t->numSMs * 2);
+    if (t->topRows <= kVtRowsMax) {
+      const size_t smem = (size_t)t->topRows * kDescBytes;
+      k_vt_top<true><<<topGrid, kVtBktThreads, smem, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
+                                                                 t->levelStartL, dKeys, n, t->dBucket, t->dHist);
+    } else {
+      k_vt_top<false><<<(unsigned)keyBlocks, kVtBktThreads, 0, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
+                                                                          t->levelStartL, dKeys, n, t->dBucket,
+                                                                          t->dHist);
+    }
+    if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+  }
+  k_vt_scan<<<1, 1024, 0, t->stream>>>(t->dHist, bins, t->L > 0 ? 0 : n, t->dOff, t->dItems, t->dNItems);
+  if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+  if (t->L > 0) {
+    k_vt_scatter<<<(unsigned)std::min<long long>(((long long)n + 255) / 256, (long long)t->numSMs * 8), 256, 0,
+                   t->stream>>>(t->dBucket, n, t->dOff, t->dHist + bins, t->dPerm);
+    if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+  }
+  const size_t smem = (size_t)t->subRows * kDescBytes;
+  const long long maxItems = (long long)n / kVtItemKeys + bins + 1;
+  const unsigned subGrid = (unsigned)std::min<long long>(maxItems, (long long)t->numSMs * (smem <= 100 * 1024 ? 2 : 1));
+  k_vt_sub<<<subGrid, kVtBktThreads, smem, t->stream>>>(t->dNodes, t->bf, t->T, t->levelStartL, t->L > 0, t->dItems,
+                                                        t->dNItems, t->L > 0 ? t->dPerm : nullptr, dKeys,
+                                                        t->leafBase, dIds, idMode);
   return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
 }
 
-int vt_convert(v3dm_voctree* t, const float* host, size_t count, uint8_t* dst) {
+int vt_launch_f32(v3dm_voctree* t, int n, const float* dKeys, int32_t* dIds, int idMode) {
+  if (n == 0) return V3DM_OK;
+  long long threads = (long long)n * kTpk;
+  unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
+  k_voctree_f32<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodesF, t->dNorm, t->nodeCount, t->bf, t->depth,
+                                                      t->leafBase, dKeys, n, dIds, idMode, t->dReplays, t->dErr);
+  return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
+}
+
+// floats on the device -> u8 (u = 512 x); *exact = every value was u/512 with u in 0..255.
+int vt_to_u8(v3dm_voctree* t, const float* dSrc, size_t count, uint8_t* dst, bool* exact) {
+  *exact = true;
   if (count == 0) return V3DM_OK;
   if (cudaMemsetAsync(t->dErr, 0, sizeof(int32_t), t->stream) != cudaSuccess) return V3DM_ERR_CUDA;
-  // stage through dStage in chunks of its capacity (nMax descriptors)
-  size_t cap = (size_t)(t->nMax > 0 ? t->nMax : 1) * kDescBytes;
-  for (size_t off = 0; off < count; off += cap) {
-    size_t c = count - off < cap ? count - off : cap;
-    if (cudaMemcpyAsync(t->dStage, host + off, c * sizeof(float), cudaMemcpyHostToDevice, t->stream) != cudaSuccess)
-      return V3DM_ERR_CUDA;
-    long long n4 = (long long)(c / 4);
-    k_vt_f32_to_u8<<<(unsigned)((n4 + 255) / 256), 256, 0, t->stream>>>(
-        reinterpret_cast<const float4*>(t->dStage), reinterpret_cast<uint32_t*>(dst + off), n4, t->dErr);
-    if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
-  }
+  long long n4 = (long long)(count / 4);
+  k_vt_f32_to_u8<<<(unsigned)((n4 + 255) / 256), 256, 0, t->stream>>>(reinterpret_cast<const float4*>(dSrc),
+                                                                      reinterpret_cast<uint32_t*>(dst), n4, t->dErr);
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(t->hErr, t->dErr, sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
+      cudaStreamSynchronize(t->stream) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  *exact = *t->hErr == 0;
+  return V3DM_OK;
+}
+
+// Node norms of the float tree.
+int vt_norms(v3dm_voctree* t) {
+  if (!t->dNorm && cudaMalloc(reinterpret_cast<void**>(&t->dNorm), (size_t)t->nodeCount * sizeof(float)) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  k_node_norms<<<(unsigned)((t->nodeCount + 255) / 256), 256, 0, t->stream>>>(t->dNodesF, t->nodeCount, t->dNorm);
+  return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
+}
+
+int vt_alloc_float_tree(v3dm_voctree* t) {
+  if (!t->dNodesF &&
+      cudaMalloc(reinterpret_cast<void**>(&t->dNodesF), (size_t)t->nodeCount * kDescBytes * sizeof(float)) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  return V3DM_OK;
+}
+
+// The float tree from the u8 one (u/512), when float keys meet a tree given as bytes.
+int vt_ensure_float_tree(v3dm_voctree* t) {
+  if (t->nodesF) return V3DM_OK;
+  if (!t->nodesU8) return V3DM_ERR_NOT_ALLOCATED;
+  int st = vt_alloc_float_tree(t);
+  if (st != V3DM_OK) return st;
+  const long long n4 = t->nodeCount * kDescBytes / 4;
+  k_u8_to_f32<<<(unsigned)((n4 + 255) / 256), 256, 0, t->stream>>>(reinterpret_cast<const uchar4*>(t->dNodes),
+                                                                  reinterpret_cast<float4*>(t->dNodesF), n4);
+  if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+  st = vt_norms(t);
+  if (st != V3DM_OK) return st;
+  t->nodesF = true;
+  return V3DM_OK;
+}
+
+int vt_check_err(v3dm_voctree* t) {
   if (cudaMemcpyAsync(t->hErr, t->dErr, sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
       cudaStreamSynchronize(t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  return *t->hErr ? V3DM_ERR_NOT_U8 : V3DM_OK;
+  if (*t->hErr & kErrBadTree) {
+    cudaMemsetAsync(t->dErr, 0, sizeof(int32_t), t->stream);
+    return V3DM_ERR_ARG;
+  }
+  return V3DM_OK;
 }
 
 }  // namespace
@@ -192,12 +689,30 @@ int v3dm_voctree_create(v3dm_voctree** out, int device, int bf, int depth) {
   t->nodeCount = nc;
   t->leafCount = lc;
   t->leafBase = lb;
+  t->numSMs = prop.multiProcessorCount;
+  vt_plan(t);
   DeviceGuardVt g(device);
   if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&t->dErr), sizeof(int32_t)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&t->hErr), sizeof(int32_t)) != cudaSuccess) {
+      cudaMallocHost(reinterpret_cast<void**>(&t->hErr), sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&t->dReplays), sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemsetAsync(t->dErr, 0, sizeof(int32_t), t->stream) != cudaSuccess ||
+      cudaMemsetAsync(t->dReplays, 0, sizeof(unsigned long long), t->stream) != cudaSuccess ||
+      (t->T > 0 && (cudaMalloc(reinterpret_cast<void**>(&t->dHist), 2 * (size_t)t->bins * sizeof(int)) != cudaSuccess ||
+                    cudaMalloc(reinterpret_cast<void**>(&t->dOff), ((size_t)t->bins + 1) * sizeof(int)) != cudaSuccess ||
+                    cudaMalloc(reinterpret_cast<void**>(&t->dNItems), sizeof(int)) != cudaSuccess ||
+                    cudaFuncSetAttribute(k_vt_top<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kVtRowsMax * kDescBytes) != cudaSuccess ||
+                    cudaFuncSetAttribute(k_vt_sub, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kVtRowsMax * kDescBytes) != cudaSuccess)) ||
+      cudaStreamSynchronize(t->stream) != cudaSuccess) {
     if (t->stream) cudaStreamDestroy(t->stream);
     if (t->dErr) cudaFree(t->dErr);
+    if (t->hErr) cudaFreeHost(t->hErr);
+    if (t->dReplays) cudaFree(t->dReplays);
+    if (t->dHist) cudaFree(t->dHist);
+    if (t->dOff) cudaFree(t->dOff);
+    if (t->dNItems) cudaFree(t->dNItems);
     delete t;
     return V3DM_ERR_CUDA;
   }
@@ -210,6 +725,15 @@ int v3dm_voctree_destroy(v3dm_voctree* t) {
   DeviceGuardVt g(t->device);
   cudaStreamSynchronize(t->stream);
   if (t->dNodes) cudaFree(t->dNodes);
+  if (t->dNodesF) cudaFree(t->dNodesF);
+  if (t->dNorm) cudaFree(t->dNorm);
+  if (t->dReplays) cudaFree(t->dReplays);
+  if (t->dHist) cudaFree(t->dHist);
+  if (t->dOff) cudaFree(t->dOff);
+  if (t->dNItems) cudaFree(t->dNItems);
+  if (t->dBucket) cudaFree(t->dBucket);
+  if (t->dPerm) cudaFree(t->dPerm);
+  if (t->dItems) cudaFree(t->dItems);
   if (t->dKeys) cudaFree(t->dKeys);
   if (t->dStage) cudaFree(t->dStage);
   if (t->dIds) cudaFree(t->dIds);
@@ -227,14 +751,24 @@ int v3dm_voctree_allocate(v3dm_voctree* t, int nMax) {
   if (t->dKeys) cudaFree(t->dKeys);
   if (t->dStage) cudaFree(t->dStage);
   if (t->dIds) cudaFree(t->dIds);
+  if (t->dBucket) cudaFree(t->dBucket);
+  if (t->dPerm) cudaFree(t->dPerm);
+  if (t->dItems) cudaFree(t->dItems);
   t->dKeys = nullptr;
   t->dStage = nullptr;
   t->dIds = nullptr;
+  t->dBucket = t->dPerm = nullptr;
+  t->dItems = nullptr;
   t->nMax = 0;
   size_t m = nMax > 0 ? (size_t)nMax : 1;
   if (cudaMalloc(reinterpret_cast<void**>(&t->dKeys), m * kDescBytes) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&t->dStage), m * kDescBytes * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&t->dIds), m * sizeof(int32_t)) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  if (t->T > 0 &&
+      (cudaMalloc(reinterpret_cast<void**>(&t->dBucket), m * sizeof(int32_t)) != cudaSuccess ||
+       cudaMalloc(reinterpret_cast<void**>(&t->dPerm), m * sizeof(int32_t)) != cudaSuccess ||
+       cudaMalloc(reinterpret_cast<void**>(&t->dItems), (m / kVtItemKeys + t->bins + 1) * sizeof(int4)) != cudaSuccess))
     return V3DM_ERR_CUDA;
   t->nMax = nMax;
   return V3DM_OK;
@@ -245,62 +779,115 @@ int v3dm_voctree_set_nodes_u8(v3dm_voctree* t, const uint8_t* nodes) {
   DeviceGuardVt g(t->device);
   if (!t->dNodes && cudaMalloc(reinterpret_cast<void**>(&t->dNodes), (size_t)t->nodeCount * kDescBytes) != cudaSuccess)
     return V3DM_ERR_CUDA;
+  t->nodesU8 = t->nodesF = false;
   if (cudaMemcpyAsync(t->dNodes, nodes, (size_t)t->nodeCount * kDescBytes, cudaMemcpyHostToDevice, t->stream) !=
           cudaSuccess ||
       cudaStreamSynchronize(t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
+  t->nodesU8 = true;
   return V3DM_OK;
 }
 
 int v3dm_voctree_set_nodes_f32(v3dm_voctree* t, const float* nodes) {
   if (!t || !nodes) return V3DM_ERR_ARG;
-  if (!t->dStage) return V3DM_ERR_NOT_ALLOCATED;
   DeviceGuardVt g(t->device);
+  t->nodesU8 = t->nodesF = false;
+  int st = vt_alloc_float_tree(t);
+  if (st != V3DM_OK) return st;
   if (!t->dNodes && cudaMalloc(reinterpret_cast<void**>(&t->dNodes), (size_t)t->nodeCount * kDescBytes) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  return vt_convert(t, nodes, (size_t)t->nodeCount * kDescBytes, t->dNodes);
+  const size_t count = (size_t)t->nodeCount * kDescBytes;
+  if (cudaMemcpyAsync(t->dNodesF, nodes, count * sizeof(float), cudaMemcpyHostToDevice, t->stream) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  st = vt_norms(t);
+  if (st != V3DM_OK) return st;
+  bool exact = false;
+  st = vt_to_u8(t, t->dNodesF, count, t->dNodes, &exact);  // synchronises
+  if (st != V3DM_OK) return st;
+  t->nodesF = true;
+  t->nodesU8 = exact;  // u/512 trees also keep the faster integer descent
+  return V3DM_OK;
 }
 
 int v3dm_voctree_quantize_u8(v3dm_voctree* t, int n, const uint8_t* keys, int32_t* ids, int idMode) {
   if (!t || n < 0 || (n > 0 && (!keys || !ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
     return V3DM_ERR_ARG;
-  if (!t->dNodes || !t->dKeys) return V3DM_ERR_NOT_ALLOCATED;
+  if (!(t->nodesU8 || t->nodesF) || !t->dKeys) return V3DM_ERR_NOT_ALLOCATED;
   if (n > t->nMax) return V3DM_ERR_SIZE;
   if (n == 0) return V3DM_OK;
   DeviceGuardVt g(t->device);
   if (cudaMemcpyAsync(t->dKeys, keys, (size_t)n * kDescBytes, cudaMemcpyHostToDevice, t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  int st = vt_launch(t, n, t->dKeys, t->dIds, idMode);
+  int st;
+  if (t->nodesU8) {
+    st = vt_launch(t, n, t->dKeys, t->dIds, idMode);
+  } else {  // float tree: the keys as u/512 floats through the float descent
+    const long long n4 = (long long)n * kDescBytes / 4;
+    k_u8_to_f32<<<(unsigned)((n4 + 255) / 256), 256, 0, t->stream>>>(reinterpret_cast<const uchar4*>(t->dKeys),
+                                                                    reinterpret_cast<float4*>(t->dStage), n4);
+    st = cudaGetLastError() == cudaSuccess ? vt_launch_f32(t, n, t->dStage, t->dIds, idMode) : V3DM_ERR_CUDA;
+  }
   if (st != V3DM_OK) return st;
-  if (cudaMemcpyAsync(ids, t->dIds, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
-      cudaStreamSynchronize(t->stream) != cudaSuccess)
+  if (cudaMemcpyAsync(ids, t->dIds, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  return V3DM_OK;
+  return vt_check_err(t);
 }
 
 int v3dm_voctree_quantize_f32(v3dm_voctree* t, int n, const float* keys, int32_t* ids, int idMode) {
   if (!t || n < 0 || (n > 0 && (!keys || !ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
     return V3DM_ERR_ARG;
-  if (!t->dNodes || !t->dKeys) return V3DM_ERR_NOT_ALLOCATED;
+  if (!(t->nodesU8 || t->nodesF) || !t->dKeys) return V3DM_ERR_NOT_ALLOCATED;
   if (n > t->nMax) return V3DM_ERR_SIZE;
   if (n == 0) return V3DM_OK;
   DeviceGuardVt g(t->device);
-  int st = vt_convert(t, keys, (size_t)n * kDescBytes, t->dKeys);
-  if (st != V3DM_OK) return st;
-  st = vt_launch(t, n, t->dKeys, t->dIds, idMode);
-  if (st != V3DM_OK) return st;
-  if (cudaMemcpyAsync(ids, t->dIds, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
-      cudaStreamSynchronize(t->stream) != cudaSuccess)
+  const size_t count = (size_t)n * kDescBytes;
+  if (cudaMemcpyAsync(t->dStage, keys, count * sizeof(float), cudaMemcpyHostToDevice, t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  return V3DM_OK;
+  bool exact = false;
+  int st = V3DM_OK;
+  if (t->nodesU8) {
+    st = vt_to_u8(t, t->dStage, count, t->dKeys, &exact);
+    if (st != V3DM_OK) return st;
+  }
+  if (exact) {  // u/512 keys on a u/512 tree: every dot product is exact, the integer descent gives the same ids
+    st = vt_launch(t, n, t->dKeys, t->dIds, idMode);
+  } else {
+    st = vt_ensure_float_tree(t);
+    if (st == V3DM_OK) st = vt_launch_f32(t, n, t->dStage, t->dIds, idMode);
+  }
+  if (st != V3DM_OK) return st;
+  if (cudaMemcpyAsync(ids, t->dIds, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  return vt_check_err(t);
 }
 
 int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode) {
   if (!t || n < 0 || (n > 0 && (!d_keys || !d_ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
     return V3DM_ERR_ARG;
-  if (!t->dNodes) return V3DM_ERR_NOT_ALLOCATED;
+  if (!t->nodesU8) return t->nodesF ? V3DM_ERR_NOT_U8 : V3DM_ERR_NOT_ALLOCATED;
   DeviceGuardVt g(t->device);
   return vt_launch(t, n, d_keys, d_ids, idMode);
+}
+
+int v3dm_voctree_quantize_f32_device(v3dm_voctree* t, int n, const float* d_keys, int32_t* d_ids, int idMode) {
+  if (!t || n < 0 || (n > 0 && (!d_keys || !d_ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
+    return V3DM_ERR_ARG;
+  if (!(t->nodesU8 || t->nodesF)) return V3DM_ERR_NOT_ALLOCATED;
+  DeviceGuardVt g(t->device);
+  int st = vt_ensure_float_tree(t);
+  if (st != V3DM_OK) return st;
+  return vt_launch_f32(t, n, d_keys, d_ids, idMode);
+}
+
+int v3dm_voctree_replays(v3dm_voctree* t, long long* n) {
+  if (!t || !n) return V3DM_ERR_ARG;
+  DeviceGuardVt g(t->device);
+  unsigned long long v = 0;
+  if (cudaMemcpyAsync(&v, t->dReplays, sizeof(v), cudaMemcpyDeviceToHost, t->stream) != cudaSuccess ||
+      cudaStreamSynchronize(t->stream) != cudaSuccess)
+    return V3DM_ERR_CUDA;
+  *n = (long long)v;
+  return V3DM_OK;
 }
 
 int v3dm_voctree_stream(v3dm_voctree* t, void** s) {

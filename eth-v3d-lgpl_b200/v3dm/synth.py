@@ -159,15 +159,33 @@ def all_pairs(n_images: int) -> np.ndarray:
     return np.stack([i, j], 1).astype(np.int32)
 
 
+def unit_sift(rng: np.random.Generator, n: int) -> np.ndarray:
+    """n x 128 float32 SIFT-like descriptors as the extractors store them: Gamma(0.6) values,
+    L2-normalised, clamped at 0.2 and normalised again (SIFT_Feature::normalizeDescriptor after
+    the extractor's clamp); not of the form u/512."""
+    out = np.empty((n, 128), np.float32)
+    step = 1 << 18
+    for s in range(0, n, step):
+        e = min(n, s + step)
+        x = rng.gamma(0.6, 1.0, size=(e - s, 128)).astype(np.float32)
+        x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+        np.minimum(x, 0.2, out=x)
+        x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+        out[s:e] = x
+    return out
+
+
 def hkm_tree(rng: np.random.Generator, data: np.ndarray, bf: int, depth: int, iters: int = 4,
              chunk: int = 1 << 16) -> np.ndarray:
-    """Hierarchical k-means vocabulary tree with uint8-valued centres.
+    """Hierarchical k-means vocabulary tree.
 
-    Returns nodeCount x 128 uint8 centres in breadth-first order without the root (the layout
-    of V3D/Base/v3d_voctree.h:22-34).  Points are assigned to the child with the largest dot
-    product, the rule the quantizer descends by.  Centres are rounded means; a cluster that
-    loses all its points keeps its previous centre; a node with fewer points than children
-    seeds the missing children from noisy copies of its points (or fresh descriptors)."""
+    Returns nodeCount x 128 centres in breadth-first order without the root (the layout of
+    V3D/Base/v3d_voctree.h:22-34): uint8 rounded means for uint8 data, float32 means for float
+    data (the apps' trees: k-means centres of unit-L2 descriptors).  Points are assigned to the
+    child with the largest dot product, the rule the quantizer descends by.  A cluster that
+    loses all its points keeps its previous centre; a node with fewer points than children seeds
+    the missing children from noisy copies of its points (or fresh descriptors)."""
+    floats = data.dtype != np.uint8
     n = data.shape[0]
     node_of = np.zeros(n, np.int64)  # node index (global, -1 = root) of each point's current node
     level_nodes = 1
@@ -185,10 +203,14 @@ def hkm_tree(rng: np.random.Generator, data: np.ndarray, bf: int, depth: int, it
         pick = starts[:, None] + (rng.random((n_parents, bf)) * np.maximum(cnt, 1)[:, None]).astype(np.int64)
         pick = np.minimum(pick, n - 1)
         cent = data[order[pick.reshape(-1)]].reshape(n_parents, bf, 128)
-        cent = noisy_copy(rng, cent, 4.0)
+        if floats:
+            cent = np.abs(cent + rng.normal(0.0, 4.0 / 512, size=cent.shape)).astype(np.float32)
+        else:
+            cent = noisy_copy(rng, cent, 4.0)
         empty = cnt == 0
         if empty.any():
-            cent[empty] = sift_like(rng, int(empty.sum()) * bf).reshape(-1, bf, 128)
+            fresh = unit_sift if floats else sift_like
+            cent[empty] = fresh(rng, int(empty.sum()) * bf).reshape(-1, bf, 128)
         centf = cent.astype(np.float32)
         for it in range(iters + 1):
             child = np.empty(n, np.int64)
@@ -205,9 +227,12 @@ def hkm_tree(rng: np.random.Generator, data: np.ndarray, bf: int, depth: int, it
             num = np.bincount(idx, minlength=n_parents * bf)
             has = num > 0
             newc = centf.reshape(-1, 128).copy()
-            newc[has] = np.clip(np.rint(sums[has] / num[has, None]), 0, 255)
+            if floats:
+                newc[has] = sums[has] / num[has, None]
+            else:
+                newc[has] = np.clip(np.rint(sums[has] / num[has, None]), 0, 255)
             centf = newc.reshape(n_parents, bf, 128).astype(np.float32)
-        out.append(centf.astype(np.uint8).reshape(-1, 128))
+        out.append((centf if floats else centf.astype(np.uint8)).reshape(-1, 128))
         level_start = sum(bf ** (k + 1) for k in range(d))
         node_of = level_start + local_parent * bf + child
         parent_base = level_start
@@ -223,12 +248,14 @@ def _segment_sum(sums: np.ndarray, idx: np.ndarray, data: np.ndarray) -> None:
 
 
 def voctree(seed: int = 3, bf: int = 10, depth: int = 6, n_train: int = 500_000,
-            n_query: int = 2_000_000, iters: int = 4):
-    """(nodes, queries): an HKM tree trained on n_train descriptors and n_query queries."""
+            n_query: int = 2_000_000, iters: int = 4, floats: bool = False):
+    """(nodes, queries): an HKM tree trained on n_train descriptors and n_query queries; uint8
+    (u/512) data, or with floats=True unit-L2 float descriptors and float k-means centres."""
     rng = rng_for(seed)
-    train = sift_like(rng, n_train)
+    gen = unit_sift if floats else sift_like
+    train = gen(rng, n_train)
     nodes = hkm_tree(rng, train, bf, depth, iters)
-    queries = sift_like(rng, n_query)
+    queries = gen(rng, n_query)
     return nodes, queries
 
 
