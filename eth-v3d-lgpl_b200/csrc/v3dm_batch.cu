@@ -312,7 +312,8 @@ k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, co
 constexpr int kCntRowsP = 8;      // counter words of the proposal (after the batch ones)
 constexpr int kCntOverP = 9;      // 1: the proposal row table was too small
 constexpr int kCntScored = 10;    // two words: scored (left, right) pairs, 64-bit
-constexpr int kCntRowsPB = 12;    // rows of the proposal's pass B
+constexpr int kCntRowsVL = 13;    // rows of the proposal's exact verification, left side
+constexpr int kCntRowsVR = 14;    // and right side
 
 // Per image and cell: rows whose probed cells include the cell (A) and rows whose best cell
 // it is (B).
@@ -527,95 +528,144 @@ k_pchoose(const BPair* __restrict__ pairs, int nPairs, const long long* __restri
   }
 }
 
-// Pass B of the proposal on the tensor cores.  Every pass-B state (an accepted left l of pair
-// (i, j) and the right r it names) becomes one entry per cell c that r probes and in which
-// image i has lefts; an entry is scored against the lefts of (i, c) in the A layout, the same
-// block pass A used, so the entries of a state together cover exactly r's candidates (a left
-// probing several of r's cells is seen once per such cell with the same key).  Entries are
-// grouped by unit u = i * C + c; a row of the pass-B table is a group of up to GM entries of
-// one unit against that unit's left block.  The side kernel gathers the entries' right
-// descriptors itself (no copy of them is made).
+// Exact verification of the proposal (two gathered side passes on the tensor cores).  Pass A
+// of the proposal scores each left only against its candidate rights, so its decisions (and
+// those of a candidate-restricted pass B) can accept a pair that the reference's rules on the
+// full score matrix reject: a missing second-best makes the ratio test more lenient.  Every
+// pass-B state (an accepted left l of pair (i, j)) is therefore decided again over the full
+// score matrix of its pair:
+//   V-left:  l against every right of image j -> l's exact decision r (the reference's column
+//            rule, v3d_cudamatching.cu:133-162);
+//   V-right: that r against every left of image i -> r's exact decision (the row rule,
+//            .cu:164-210).
+// The state is a match when r's exact decision is l (the mutual filter, .cu:546-551).  Every
+// output pair is then a pair of exhaustive matching; what the proposal can still miss are
+// lefts that pass A did not accept.  V-left entries are the states grouped by right image (a
+// counting sort); V-right entries are the states themselves, already grouped by left image.
 
-// Pass 1: entries per unit.
-__global__ void k_pbcount(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
-                          const uint8_t* __restrict__ cell, int probes, int probesR, int C,
-                          const int* __restrict__ cntA, const int* __restrict__ chosenRight,
-                          const int* __restrict__ chosenSorted, const int* __restrict__ counters,
-                          int* __restrict__ cntE) {
+// V-left, pass 1: states per right image.
+__global__ void k_vcount(const BPair* __restrict__ pairs, const int* __restrict__ chosenSorted,
+                         const int* __restrict__ counters, int* __restrict__ cntJ) {
   const int n = counters[kCntStates];  // 0 after a state overflow
-  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
-    const BPair q = pairs[chosenSorted[st]];
-    const int rRow = im[q.ri].rowOff + chosenRight[st];
-    for (int pr = 0; pr < probesR; ++pr) {
-      const int u = q.li * C + cell[(size_t)rRow * probes + pr];
-      if (cntA[u] > 0) atomicAdd(&cntE[u], 1);
-    }
-  }
+  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x)
+    atomicAdd(&cntJ[pairs[chosenSorted[st]].ri], 1);
 }
 
-// Entry offsets and row starts per unit (exclusive prefix sums; offE has nUnits + 1 entries).
-// One block.  A row table too small for the rows raises the overflow flag (the host grows
-// the pass-B buffers, and with them the table, and repeats the call); k_pbrows then writes
-// nothing.
+// Entry offsets per right image and row starts of both verification passes (exclusive prefix
+// sums).  One block.  Row counts go to kCntRowsVL / kCntRowsVR; a row table too small raises
+// the overflow flag.
 __global__ void __launch_bounds__(kScanThreads)
-k_pbscan(const int* __restrict__ cntE, int nUnits, int GM, long long capRows, int* __restrict__ offE,
-         int* __restrict__ rowStartE, int* __restrict__ counters) {
+k_vscan(const int* __restrict__ cntJ, const BImage* __restrict__ im, int nImages, const long long* __restrict__ prefC,
+        int GR, long long capRows, int* __restrict__ offJ, int* __restrict__ rowStartL, int* __restrict__ rowStartR,
+        int* __restrict__ counters) {
   __shared__ long long sh[kScanThreads];
   const long long total = block_scan(
-      nUnits, [&](int u) { return (long long)cntE[u]; }, [&](int u, long long x) { offE[u] = (int)x; }, sh);
+      nImages, [&](int j) { return (long long)cntJ[j]; }, [&](int j, long long x) { offJ[j] = (int)x; }, sh);
   __syncthreads();
-  const long long rows = block_scan(
-      nUnits, [&](int u) { return (long long)((cntE[u] + GM - 1) / GM); },
-      [&](int u, long long x) { rowStartE[u] = (int)x; }, sh);
+  const long long rowsL = block_scan(
+      nImages, [&](int j) { return (long long)((cntJ[j] + GR - 1) / GR); },
+      [&](int j, long long x) { rowStartL[j] = (int)x; }, sh);
+  __syncthreads();
+  const long long rowsR = block_scan(
+      nImages,
+      [&](int i) {
+        const long long c = prefC[im[i].pairEnd] - prefC[im[i].pairBeg];
+        return (c + GR - 1) / GR;
+      },
+      [&](int i, long long x) { rowStartR[i] = (int)x; }, sh);
   if (threadIdx.x == 0) {
-    offE[nUnits] = (int)total;
-    const bool over = rows > capRows;
-    counters[kCntRowsPB] = over ? 0 : (int)rows;
+    offJ[nImages] = (int)total;
+    // after a state overflow there are no states: no rows either (the call is repeated)
+    const bool over = counters[kCntOverflow] != 0 || rowsL > capRows || rowsR > capRows;
+    counters[kCntRowsVL] = over ? 0 : (int)rowsL;
+    counters[kCntRowsVR] = over ? 0 : (int)rowsR;
     if (over) counters[kCntOverflow] = 1;
   }
 }
 
-// Pass 2: every entry's source row (the right's descriptor row in the image buffer) and
-// state.  Counts down cntE, which ends at zero for the next call.
-__global__ void k_pbscatter(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
-                            const uint8_t* __restrict__ cell, int probes, int probesR, int C,
-                            const int* __restrict__ cntA, const int* __restrict__ chosenRight,
-                            const int* __restrict__ chosenSorted, const int* __restrict__ counters,
-                            const int* __restrict__ offE, int* __restrict__ cntE, int* __restrict__ srcRowE,
-                            int* __restrict__ stateE) {
-  const int n = counters[kCntStates];  // the states k_pbcount counted: cntE ends at zero
+// V-left, pass 2: every state's entry (its left's descriptor row in the image buffer), grouped
+// by right image.  Counts cntJ down to zero for the next call.
+__global__ void k_vscatter(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
+                           const int* __restrict__ chosenLeft, const int* __restrict__ chosenSorted,
+                           const int* __restrict__ counters, const int* __restrict__ offJ, int* __restrict__ cntJ,
+                           int* __restrict__ srcRow, int* __restrict__ stateOf) {
+  const int n = counters[kCntStates];
   for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
     const BPair q = pairs[chosenSorted[st]];
-    const int rRow = im[q.ri].rowOff + chosenRight[st];
-    for (int pr = 0; pr < probesR; ++pr) {
-      const int u = q.li * C + cell[(size_t)rRow * probes + pr];
-      if (cntA[u] == 0) continue;
-      const int pos = offE[u] + atomicSub(&cntE[u], 1) - 1;
-      srcRowE[pos] = rRow;
-      stateE[pos] = st;
+    const int pos = offJ[q.ri] + atomicSub(&cntJ[q.ri], 1) - 1;
+    srcRow[pos] = im[q.li].rowOff + chosenLeft[st];
+    stateOf[pos] = st;
+  }
+}
+
+// V-left, pass 3: rows of up to GR entries of one right image against that image (one thread
+// per image).
+__global__ void k_vrows_left(const BImage* __restrict__ im, int nImages, int GR, int BN, const int* __restrict__ offJ,
+                             const int* __restrict__ rowStartL, const int* __restrict__ counters,
+                             BatchRow* __restrict__ rows) {
+  if (counters[kCntOverflow]) return;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nImages; j += gridDim.x * blockDim.x) {
+    const int e0 = offJ[j], ne = offJ[j + 1] - e0;
+    int at = rowStartL[j];
+    for (int g = 0; g * GR < ne; ++g) {
+      BatchRow r;
+      r.aRow = e0 + g * GR;
+      r.validRows = min(GR, ne - g * GR);
+      r.bRow0 = im[j].rowOff;
+      r.nB = im[j].n;
+      r.nTiles = (im[j].n + BN - 1) / BN;
+      r.pad = 0;
+      r.state0 = 0;  // the state of an entry comes from stateOf
+      rows[at++] = r;
     }
   }
 }
 
-// Pass 3: the rows (one thread per unit).
-__global__ void k_pbrows(int nUnits, int GM, int BN, const int* __restrict__ cntA, const int* __restrict__ offA,
-                         const int* __restrict__ offE, const int* __restrict__ rowStartE,
-                         const int* __restrict__ counters, BatchRow* __restrict__ rows) {
+// V-right: the right each state's exact left decision named (row 0 of its image when there is
+// none: scored, then ignored), and rows of up to GR consecutive states of one left image
+// against that image; a row's states are its entries (state0 = aRow).
+__global__ void k_vsrc_right(const BPair* __restrict__ pairs, const BImage* __restrict__ im,
+                             const int* __restrict__ chosenSorted, const int32_t* __restrict__ decLeft,
+                             const int* __restrict__ counters, int* __restrict__ srcRow) {
+  const int n = counters[kCntStates];
+  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
+    const int r = decLeft[st];
+    srcRow[st] = im[pairs[chosenSorted[st]].ri].rowOff + (r >= 0 ? r : 0);
+  }
+}
+
+__global__ void k_vrows_right(const BImage* __restrict__ im, int nImages, const long long* __restrict__ prefC, int GR,
+                              int BN, const int* __restrict__ rowStartR, const int* __restrict__ counters,
+                              BatchRow* __restrict__ rows) {
   if (counters[kCntOverflow]) return;
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nUnits; u += gridDim.x * blockDim.x) {
-    const int e0 = offE[u], ne = offE[u + 1] - e0;
-    int at = rowStartE[u];
-    for (int g = 0; g * GM < ne; ++g) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nImages; i += gridDim.x * blockDim.x) {
+    const long long s0 = prefC[im[i].pairBeg], ns = prefC[im[i].pairEnd] - s0;
+    int at = rowStartR[i];
+    for (long long g = 0; g * GR < ns; ++g) {
       BatchRow r;
-      r.aRow = e0 + g * GM;
-      r.validRows = min(GM, ne - g * GM);
-      r.bRow0 = offA[u];
-      r.nB = cntA[u];
-      r.nTiles = (cntA[u] + BN - 1) / BN;
+      r.aRow = (int)(s0 + g * GR);
+      r.validRows = (int)min((long long)GR, ns - g * GR);
+      r.bRow0 = im[i].rowOff;
+      r.nB = im[i].n;
+      r.nTiles = (im[i].n + BN - 1) / BN;
       r.pad = 0;
-      r.state0 = 0;
+      r.state0 = r.aRow;
       rows[at++] = r;
     }
+  }
+}
+
+// A state is a match when its left's exact decision names a right whose exact decision names
+// the left back.  The right of the state becomes that exact right; decB holds the left for the
+// mutual kernels (k_bmutual_*) when it is a match, else -1.
+__global__ void k_vmerge(const int* __restrict__ counters, const int32_t* __restrict__ decLeft,
+                         const int* __restrict__ chosenLeft, int* __restrict__ chosenRight, int32_t* __restrict__ decB) {
+  const int n = counters[kCntStates];
+  for (int st = blockIdx.x * blockDim.x + threadIdx.x; st < n; st += gridDim.x * blockDim.x) {
+    const int r = decLeft[st], l = chosenLeft[st];
+    const bool ok = r >= 0 && decB[st] == l;
+    chosenRight[st] = r;
+    decB[st] = ok ? l : -1;
   }
 }
 
@@ -725,19 +775,22 @@ struct v3dm_batch {
   long long chosenSortedCap = 0;
   TcMaps mapsP;
   bool mapsPValid = false;
-  // proposal pass B (gathered entries)
-  int* dCntE = nullptr;             // per unit: entries (zero between calls)
-  int* dOffE = nullptr;             // per unit + 1: first entry
-  int* dRowStartE = nullptr;        // per unit: first pass-B row
+  // proposal: exact verification of its states (gathered entries against whole images)
+  int* dCntE = nullptr;             // per image: V-left entries (zero between calls)
+  int* dOffE = nullptr;             // per image + 1: first V-left entry
+  int* dRowStartE = nullptr;        // per image: first V-left row
+  int* dRowStartR = nullptr;        // per image: first V-right row
   long long unitTabCap = 0;
-  int* dSrcRowE = nullptr;          // per entry: descriptor row of its right in the image buffer
-  int* dStateE = nullptr;           // per entry: its pass-B state
+  int* dSrcRowE = nullptr;          // per V-left entry: its left's row in the image buffer
+  int* dStateE = nullptr;           // per V-left entry: its state
+  int* dSrcRowR = nullptr;          // per state: row of the right its exact left decision named
+  int32_t* dDecL = nullptr;         // per state: exact decision of its left
   long long entryCap = 0;
-  BatchRow* dRowsPB = nullptr;
+  BatchRow* dRowsPB = nullptr;      // row table of V-left, then of V-right
   long long rowsPBCap = 0;
-  CUtensorMap mapPB;                // B of pass B: the A layout, gather-configuration tiles
-  const uint8_t* mapPBla = nullptr;
-  long long mapPBrows = 0;
+  CUtensorMap mapImgG;              // B of the verification: the image buffer, gather-configuration tiles
+  const uint8_t* mapImgGimg = nullptr;
+  long long mapImgGrows = 0;
   const uint8_t* mapsPla = nullptr;
   const uint8_t* mapsPlb = nullptr;
   cudaGraphExec_t graphP = nullptr;
@@ -1152,31 +1205,38 @@ int prepare_proposal(v3dm_batch* b, int probesL, int probesR, int C) {
     b->pairTabCap = tab;
   }
   V3DM_BTRY(ensure(&b->dRowsP, &b->rowsPCap, rowsBound));
-  // pass B: entries <= states x probesR, rows <= entries / GM + units
-  if (tab + 1 > b->unitTabCap) {
-    long long c0 = 0, c1 = 0, c2 = 0;
+  // exact verification: one entry per state on each side, per-image tables
+  const long long imgTab = (long long)std::max(b->nImages, 1) + 1;
+  if (imgTab > b->unitTabCap) {
+    long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     bfree(b->dCntE);
     bfree(b->dOffE);
     bfree(b->dRowStartE);
+    bfree(b->dRowStartR);
     b->unitTabCap = 0;
-    V3DM_BTRY(ensure(&b->dCntE, &c0, tab + 1));
-    V3DM_BTRY(ensure(&b->dOffE, &c1, tab + 1));
-    V3DM_BTRY(ensure(&b->dRowStartE, &c2, tab + 1));
-    V3DM_BTRY(cudaMemsetAsync(b->dCntE, 0, (size_t)(tab + 1) * sizeof(int), b->stream));
-    b->unitTabCap = tab + 1;
+    V3DM_BTRY(ensure(&b->dCntE, &c0, imgTab));
+    V3DM_BTRY(ensure(&b->dOffE, &c1, imgTab));
+    V3DM_BTRY(ensure(&b->dRowStartE, &c2, imgTab));
+    V3DM_BTRY(ensure(&b->dRowStartR, &c3, imgTab));
+    V3DM_BTRY(cudaMemsetAsync(b->dCntE, 0, (size_t)imgTab * sizeof(int), b->stream));
+    b->unitTabCap = imgTab;
   }
-  const long long entries = std::max<long long>(b->capB * probesR, 1);
+  const long long entries = std::max<long long>(b->capB, 1);
   if (entries > 0x7fffffffLL) return V3DM_ERR_SIZE;
   if (entries > b->entryCap) {
-    long long c0 = 0, c1 = 0;
+    long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     bfree(b->dSrcRowE);
     bfree(b->dStateE);
+    bfree(b->dSrcRowR);
+    bfree(b->dDecL);
     b->entryCap = 0;
     V3DM_BTRY(ensure(&b->dSrcRowE, &c0, entries));
     V3DM_BTRY(ensure(&b->dStateE, &c1, entries));
+    V3DM_BTRY(ensure(&b->dSrcRowR, &c2, entries));
+    V3DM_BTRY(ensure(&b->dDecL, &c3, entries));
     b->entryCap = entries;
   }
-  V3DM_BTRY(ensure(&b->dRowsPB, &b->rowsPBCap, entries / tc_gather_rows() + tab + 1));
+  V3DM_BTRY(ensure(&b->dRowsPB, &b->rowsPBCap, entries / tc_gather_rows() + imgTab + 1));
   if (b->dLA != la0 || b->dLB != lb0 || b->dRowsP != rp0 || !b->mapsPValid || b->laRows != laRows ||
       b->lbRows != lbRows || b->mapsP.cfg != tc_get_config(b->tc)) {
     V3DM_BTRY(tc_side_maps(b->tc, &b->mapsP, b->dLA, (int)laRows, b->dLB, (int)lbRows));
@@ -1186,10 +1246,10 @@ int prepare_proposal(v3dm_batch* b, int probesL, int probesR, int C) {
     if (b->graphP) cudaGraphExecDestroy(b->graphP);
     b->graphP = nullptr;
   }
-  if (b->mapPBla != b->dLA || b->mapPBrows != laRows) {
-    V3DM_BTRY(tc_gather_map(&b->mapPB, b->dLA, (int)laRows));
-    b->mapPBla = b->dLA;
-    b->mapPBrows = laRows;
+  if (b->mapImgGimg != b->dImg || b->mapImgGrows != b->totalRows) {
+    V3DM_BTRY(tc_gather_map(&b->mapImgG, b->dImg, (int)std::max<long long>(b->totalRows, 1)));
+    b->mapImgGimg = b->dImg;
+    b->mapImgGrows = b->totalRows;
     if (b->graphP) cudaGraphExecDestroy(b->graphP);
     b->graphP = nullptr;
   }
@@ -1267,7 +1327,7 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
   pa.decision = b->dDecA;
   V3DM_BTRY(launch_post(pa, b->stream));
   launches += 3;
-  // pass B: each accepted left's right against the lefts that share a probed cell with it
+  // pass-B states: the accepted lefts of every pair, in pair order
   const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
   k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
   V3DM_BTRY(cudaGetLastError());
@@ -1277,62 +1337,80 @@ int enqueue_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL, in
                                                           b->dChosenRight, b->dChosenPair, b->dChosenSorted,
                                                           b->dCounters);
   V3DM_BTRY(cudaGetLastError());
-  const int GB = tc_gather_rows();
+  // exact verification of every state over the full score matrix of its pair
+  const int GR = tc_gather_rows(), BNG = tc_gather_cols();
   const int stateGrid = 4 * 148;
-  k_pbcount<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA,
-                                              b->dChosenRight, b->dChosenSorted, b->dCounters, b->dCntE);
+  const int imgBlocks = std::max(1, (nI + 255) / 256);
+  k_vcount<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dChosenSorted, b->dCounters, b->dCntE);
   V3DM_BTRY(cudaGetLastError());
-  k_pbscan<<<1, kScanThreads, 0, b->stream>>>(b->dCntE, nI * C, GB, b->rowsPBCap, b->dOffE, b->dRowStartE,
-                                              b->dCounters);
+  k_vscan<<<1, kScanThreads, 0, b->stream>>>(b->dCntE, b->dImages, nI, b->dPrefC, GR, b->rowsPBCap, b->dOffE,
+                                             b->dRowStartE, b->dRowStartR, b->dCounters);
   V3DM_BTRY(cudaGetLastError());
-  k_pbscatter<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dCell, probes, probesR, C, b->dCntA,
-                                                b->dChosenRight, b->dChosenSorted, b->dCounters, b->dOffE, b->dCntE,
-                                                b->dSrcRowE, b->dStateE);
+  k_vscatter<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dChosenLeft, b->dChosenSorted, b->dCounters,
+                                               b->dOffE, b->dCntE, b->dSrcRowE, b->dStateE);
   V3DM_BTRY(cudaGetLastError());
-  k_pbrows<<<std::max(1, (nI * C + 255) / 256), 256, 0, b->stream>>>(nI * C, GB, tc_gather_cols(), b->dCntA, b->dOffA, b->dOffE,
-                                                                     b->dRowStartE, b->dCounters, b->dRowsPB);
+  k_vrows_left<<<imgBlocks, 256, 0, b->stream>>>(b->dImages, nI, GR, BNG, b->dOffE, b->dRowStartE, b->dCounters,
+                                                 b->dRowsPB);
   V3DM_BTRY(cudaGetLastError());
-  SideArgs sb;
-  std::memset(&sb, 0, sizeof(sb));
-  sb.Smin = Smin;
-  if (host_candidate_threshold(minScore, minRatio, false, &sb.Tsec) != V3DM_OK) sb.Tsec = 0;
-  sb.records = b->dRecords;
-  sb.segCount = b->dSegCount;
-  sb.segCap = b->segCap;
-  sb.nSeg = b->nSeg;
-  sb.err = b->dInfo + kInfoErr;
-  sb.aIsLeft = 0;
-  sb.best = b->dBest;
-  sb.sec = b->dSec;
-  sb.amap = b->dStateE;
-  sb.rows = b->dRowsPB;
-  sb.nRowsPtr = b->dCounters + kCntRowsPB;
-  sb.nRows = (int)std::min<long long>(b->rowsPBCap, 0x7fffffff);
-  sb.schedule = 2;
-  sb.aSrc = b->dImg;
-  sb.aSrcRow = b->dSrcRowE;
+  SideArgs sv;
+  std::memset(&sv, 0, sizeof(sv));
+  sv.Smin = Smin;
+  if (host_candidate_threshold(minScore, minRatio, false, &sv.Tsec) != V3DM_OK) sv.Tsec = 0;
+  sv.records = b->dRecords;
+  sv.segCount = b->dSegCount;
+  sv.segCap = b->segCap;
+  sv.nSeg = b->nSeg;
+  sv.err = b->dInfo + kInfoErr;
+  sv.best = b->dBest;
+  sv.sec = b->dSec;
+  sv.schedule = 2;
+  sv.aSrc = b->dImg;
+  sv.nRows = (int)std::min<long long>(b->rowsPBCap, 0x7fffffff);
+  // V-left: each state's left against every right of its pair's right image
+  sv.aIsLeft = 1;
+  sv.amap = b->dStateE;
+  sv.aSrcRow = b->dSrcRowE;
+  sv.rows = b->dRowsPB;
+  sv.nRowsPtr = b->dCounters + kCntRowsVL;
   if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
-  V3DM_BTRY(launch_side_gather(b->tc, b->mapPB, sb, b->stream));
+  V3DM_BTRY(launch_side_gather(b->tc, b->mapImgG, sv, b->stream));
+  PostArgs pv;
+  std::memset(&pv, 0, sizeof(pv));
+  pv.records = b->dRecords;
+  pv.segCount = b->dSegCount;
+  pv.segCap = b->segCap;
+  pv.nSeg = b->nSeg;
+  pv.Smin = Smin;
+  pv.minScore = minScore;
+  pv.minRatio = minRatio;
+  pv.best = b->dBest;
+  pv.sec = b->dSec;
+  pv.err = b->dInfo + kInfoErr;
+  pv.nRows = (int)std::min<long long>(b->capB, 0x7fffffff);
+  pv.rowsPtr = b->dCounters + kCntStates;
+  pv.aIsLeft = 1;
+  pv.decision = b->dDecL;
+  V3DM_BTRY(launch_post(pv, b->stream));
+  // V-right: the right each exact left decision named, against every left of the pair's left image
+  k_vsrc_right<<<stateGrid, 256, 0, b->stream>>>(b->dPairs, b->dImages, b->dChosenSorted, b->dDecL, b->dCounters,
+                                                 b->dSrcRowR);
+  V3DM_BTRY(cudaGetLastError());
+  k_vrows_right<<<imgBlocks, 256, 0, b->stream>>>(b->dImages, nI, b->dPrefC, GR, BNG, b->dRowStartR, b->dCounters,
+                                                  b->dRowsPB);
+  V3DM_BTRY(cudaGetLastError());
+  sv.aIsLeft = 0;
+  sv.amap = nullptr;
+  sv.aSrcRow = b->dSrcRowR;
+  sv.nRowsPtr = b->dCounters + kCntRowsVR;
+  V3DM_BTRY(launch_side_gather(b->tc, b->mapImgG, sv, b->stream));
   if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[3], b->stream));
-  PostArgs pb;
-  std::memset(&pb, 0, sizeof(pb));
-  pb.records = b->dRecords;
-  pb.bmap = b->dMapA;
-  pb.segCount = b->dSegCount;
-  pb.segCap = b->segCap;
-  pb.nSeg = b->nSeg;
-  pb.Smin = Smin;
-  pb.minScore = minScore;
-  pb.minRatio = minRatio;
-  pb.best = b->dBest;
-  pb.sec = b->dSec;
-  pb.err = b->dInfo + kInfoErr;
-  pb.nRows = (int)std::min<long long>(b->capB, 0x7fffffff);
-  pb.rowsPtr = b->dCounters + kCntStates;
-  pb.aIsLeft = 0;
-  pb.decision = b->dDecB;
-  V3DM_BTRY(launch_post(pb, b->stream));
-  launches += 7;  // four layout kernels, side pass, records, decisions
+  pv.aIsLeft = 0;
+  pv.decision = b->dDecB;
+  V3DM_BTRY(launch_post(pv, b->stream));
+  k_vmerge<<<stateGrid, 256, 0, b->stream>>>(b->dCounters, b->dDecL, b->dChosenLeft, b->dChosenRight, b->dDecB);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 13;  // four V-left layout kernels, two gathered side passes with their records and decisions,
+                   // two V-right layout kernels, the merge
   const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
   k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
   V3DM_BTRY(cudaGetLastError());
@@ -1450,6 +1528,9 @@ void free_all(v3dm_batch* b) {
   bfree(b->dRowStartE);
   bfree(b->dSrcRowE);
   bfree(b->dStateE);
+  bfree(b->dSrcRowR);
+  bfree(b->dDecL);
+  bfree(b->dRowStartR);
   bfree(b->dRowsPB);
   bfree(b->dRowsP);
   bfree(b->dChosenSorted);

@@ -1,9 +1,12 @@
 """Candidate-proposal matching (v3dm_batch_match_proposal) on the GPU.
 
-The proposal result is, by definition, the reference's matching (v3d_cudamatching.cu:133-210,
-:546-551) on the score matrix in which every non-candidate entry is masked (-1e20, as the
-guided gates mask): a candidate is a (left, right) whose right's best cell is among the left's
-probed cells.  That restatement (numpy, float32 per operation) is the checker; with every cell
+Pass A of the proposal applies the reference's column rule (v3d_cudamatching.cu:133-162) to the
+score matrix in which every non-candidate entry is masked (-1e20, as the guided gates mask): a
+candidate is a (left, right) whose cells share a probed cell.  Each left it accepts is then
+decided again on the full score matrix of its pair, and so is the right that exact decision
+names (.cu:164-210); the pair is kept when the two name each other (.cu:546-551).  So the result
+is the set of exhaustive matches whose left the masked pass accepted: a subset of exhaustive
+matching.  That restatement (numpy, float32 per operation) is the checker; with every cell
 probed the proposal must reproduce exhaustive matching exactly."""
 import numpy as np
 import pytest
@@ -16,34 +19,40 @@ pytestmark = pytest.mark.gpu
 f32 = np.float32
 
 
-def _masked_match(L, R, mask, ms, mr):
-    """Reference decisions on scores[r, l] with non-candidates at -1e20 (vectorised; the same
-    float32 operations as tests/pyref.py)."""
-    S = (R.astype(np.int64) @ L.astype(np.int64).T).astype(np.float32) * f32(2.0 ** -18)
-    S = np.where(mask.T, S, f32(-1e20)).astype(np.float32)
+def _side(M, ms, mr):
+    """Reference decisions of the rows of M (rows = the side deciding, columns = the other
+    side; the same float32 operations as tests/pyref.py)."""
+    n, m = M.shape
+    if m == 0:
+        return np.full(n, -1)
+    arg = np.argmax(M, axis=1)  # first index on ties, as the strict '>' scan
+    mx = M[np.arange(n), arg]
+    if m > 1:
+        srt = -np.sort(-M, axis=1)
+        nxt = srt[:, 1]
+    else:
+        nxt = np.full(n, f32(-1e30), np.float32)
+    if mr < 0:
+        return np.where(mx > f32(ms), arg, -1)
+    nextDist = np.maximum(0.001, (f32(2.0) - f32(2.0) * nxt).astype(np.float64)).astype(np.float32)
+    bestDist = (f32(2.0) - f32(2.0) * mx).astype(np.float32)
+    ratio = (bestDist / nextDist).astype(np.float32)
+    return np.where((mx > f32(ms)) & (ratio < f32(mr)), arg, -1)
 
-    def side(M):  # rows = the side deciding, columns = the other side
-        n, m = M.shape
-        if m == 0:
-            return np.full(n, -1)
-        arg = np.argmax(M, axis=1)  # first index on ties, as the strict '>' scan
-        mx = M[np.arange(n), arg]
-        if m > 1:
-            srt = -np.sort(-M, axis=1)
-            nxt = srt[:, 1]
-        else:
-            nxt = np.full(n, f32(-1e30), np.float32)
-        if mr < 0:
-            return np.where(mx > f32(ms), arg, -1)
-        nextDist = np.maximum(0.001, (f32(2.0) - f32(2.0) * nxt).astype(np.float64)).astype(np.float32)
-        bestDist = (f32(2.0) - f32(2.0) * mx).astype(np.float32)
-        ratio = (bestDist / nextDist).astype(np.float32)
-        return np.where((mx > f32(ms)) & (ratio < f32(mr)), arg, -1)
 
-    col = side(S.T)  # per left
-    row = side(S)    # per right
-    out = [(k, col[k]) for k in range(L.shape[0]) if col[k] >= 0 and row[col[k]] == k]
+def _proposal_reference(L, R, mask, ms, mr):
+    """Exhaustive matches (l, r) whose left the masked column rule accepts."""
+    S = (R.astype(np.int64) @ L.astype(np.int64).T).astype(np.float32) * f32(2.0 ** -18)  # [r, l]
+    masked = np.where(mask.T, S, f32(-1e20)).astype(np.float32)
+    accepted = _side(masked.T, ms, mr) >= 0
+    col = _side(S.T, ms, mr)  # exact, per left
+    row = _side(S, ms, mr)    # exact, per right
+    out = [(k, col[k]) for k in range(L.shape[0]) if accepted[k] and col[k] >= 0 and row[col[k]] == k]
     return np.array(out, np.int32).reshape(-1, 2)
+
+
+def _exhaustive_reference(L, R, ms, mr):
+    return _proposal_reference(L, R, np.ones((L.shape[0], R.shape[0]), bool), ms, mr)
 
 
 def _images(seed, counts, track_frac=0.2):
@@ -91,8 +100,12 @@ def test_proposal_equals_masked_reference(v3dm_mod, small, probes, probes_right,
     for k, (i, j) in enumerate(pairs):
         ci, cj = cells[offs[i]:offs[i + 1], :probes], cells[offs[j]:offs[j + 1], :probes_right]
         mask = (ci[:, :, None, None] == cj[None, None, :, :]).any(axis=(1, 3))  # [left, right]
-        exp = _masked_match(desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]], mask, ms, mr)
+        Li, Rj = desc[offs[i]:offs[i + 1]], desc[offs[j]:offs[j + 1]]
+        exp = _proposal_reference(Li, Rj, mask, ms, mr)
         np.testing.assert_array_equal(per[k], exp, err_msg=f"pair {k} ({i}, {j})")
+        # precision 1: every pair it returns is a pair of exhaustive matching
+        full = {tuple(x) for x in _exhaustive_reference(Li, Rj, ms, mr)}
+        assert all(tuple(x) in full for x in per[k])
     scored, exhaustive = b.proposal_scored()
     assert 0 < scored <= exhaustive * min(probes, probes_right)  # once per shared cell
     b.close()
@@ -148,7 +161,8 @@ def test_trained_projection_gains_recall(v3dm_mod):
         results[trained] = proposal.recall(exh, got)
         net.close()
     assert results[True][0] > results[False][0], results
-    assert results[True][0] > 0.85 and results[True][1] > 0.8, results
+    assert results[True][0] > 0.85, results
+    assert results[True][1] == 1.0 and results[False][1] == 1.0, results  # a subset of exhaustive matching
     b.close()
 
 
