@@ -82,11 +82,12 @@ inline void retrieveSequence(int nLeaves, std::vector<std::vector<int> > const& 
 // corrs[p]: the putative correspondences of pair p; K1[p], K2[p]: its calibrations (indexable as
 // K[i][j]).  res[p] receives the result; pairs with fewer than 6 correspondences (for which the
 // reference draws no sample; it throws below 5) or without a consistent sample get error -1 and no
-// inliers.
+// inliers.  iterativeRefinement is RobustOrientationMode::iterativeRefinement (the apps set it).
 template <typename Corr, typename Mat3, typename Result>
 inline void computeRobustOrientationBatch(std::vector<std::vector<Corr> > const& corrs, std::vector<Mat3> const& K1,
                                           std::vector<Mat3> const& K2, double inlierThreshold, int nSamples,
-                                          std::vector<Result>& res, unsigned seed, int device = 0) {
+                                          std::vector<Result>& res, unsigned seed, int device = 0,
+                                          bool iterativeRefinement = false) {
   const int nPairs = (int)corrs.size();
   res.assign(nPairs, Result());
   if (nPairs == 0) return;
@@ -141,7 +142,9 @@ inline void computeRobustOrientationBatch(std::vector<std::vector<Corr> > const&
   std::vector<uint8_t> flags((size_t)offsets[nb] + 1);
   v3dm_ransac* r = nullptr;
   detail::check(v3dm_ransac_create(&r, device), "computeRobustOrientationBatch()");
-  const int st = v3dm_ransac_essential(r, nb, offsets.data(), c.data(), K.data(), inlierThreshold, nSamples, nDraw,
+  int st = v3dm_ransac_set_refinement(r, iterativeRefinement ? 1 : 0);
+  if (st == V3DM_OK)
+    st = v3dm_ransac_essential(r, nb, offsets.data(), c.data(), K.data(), inlierThreshold, nSamples, nDraw,
                                        samplesAll.data(), 0, models.data(), nIn.data(), flags.data());
   v3dm_ransac_destroy(r);
   detail::check(st, "computeRobustOrientationBatch()");

@@ -704,12 +704,8 @@ V3DM_HD double pose_weighted_residual(const PoseCorr* c, int n, const double* R,
   return err;
 }
 
-// J^T J (6 x 6) and J^T e of f under (R, T).
-V3DM_HD void pose_normal_equations(const PoseCorr* c, int n, const double* R, const double* T, const double* e,
-                                   double* JtJ, double* Jte) {
-  double E[9];
-  pose_essential(R, T, E);
-  double inner[9][6];  // dE / d(omega_x, omega_y, omega_z, T_x, T_y, T_z)
+// dE / d(omega_x, omega_y, omega_z, T_x, T_y, T_z) of E = [T]x R under the update of pose_update.
+V3DM_HD void pose_inner(const double* E, const double* R, double (*inner)[6]) {
   for (int r = 0; r < 3; ++r) {
     inner[3 * r + 0][0] = 0.0;
     inner[3 * r + 1][0] = E[3 * r + 2];
@@ -732,33 +728,49 @@ V3DM_HD void pose_normal_equations(const PoseCorr* c, int n, const double* R, co
     inner[3 + j][5] = R[j];
     inner[6 + j][5] = 0.0;
   }
+}
+
+// Jacobian row of f (the normalised Sampson residual) of one correspondence (p = (lx, ly),
+// q = (rx, ry)) under E, from pose_inner's dE/dx.
+V3DM_HD void pose_jacobian_row(const double* E, const double (*inner)[6], double lx, double ly, double rx, double ry,
+                               double* J) {
+  const double p[3] = {lx, ly, 1.0}, q[3] = {rx, ry, 1.0};
+  double Ep[3], Etq[2];
+  pose_residual(E, p[0], p[1], q[0], q[1], Ep, Etq);  // for E p and E^T q
+  const double num = q[0] * Ep[0] + q[1] * Ep[1] + Ep[2];
+  const double sqrDenom = Ep[0] * Ep[0] + Ep[1] * Ep[1] + Etq[0] * Etq[0] + Etq[1] * Etq[1];
+  const double denom = sqrt(sqrDenom);
+  const double invDenom = 1.0 / denom;
+  const double invSqrDenom = 1.0 / sqrDenom;
+  double outer[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double numDer = (i < 2 ? q[i] : 1.0) * (j < 2 ? p[j] : 1.0);
+      double sq = 0.0;  // d(sqrDenom)/dE_ij
+      if (i < 2 && j < 2) sq = 2 * Ep[i] * p[j] + 2 * Etq[j] * q[i];
+      else if (i < 2) sq = 2 * Ep[i];
+      else if (j < 2) sq = 2 * Etq[j];
+      outer[3 * i + j] = (numDer * denom - num * 0.5 * invDenom * sq) * invSqrDenom;
+    }
+  for (int col = 0; col < 6; ++col) {
+    double v = 0.0;
+    for (int j = 0; j < 9; ++j) v += outer[j] * inner[j][col];
+    J[col] = v;
+  }
+}
+
+// J^T J (6 x 6) and J^T e of f under (R, T).
+V3DM_HD void pose_normal_equations(const PoseCorr* c, int n, const double* R, const double* T, const double* e,
+                                   double* JtJ, double* Jte) {
+  double E[9];
+  pose_essential(R, T, E);
+  double inner[9][6];
+  pose_inner(E, R, inner);
   for (int k = 0; k < 36; ++k) JtJ[k] = 0.0;
   for (int k = 0; k < 6; ++k) Jte[k] = 0.0;
   for (int k = 0; k < n; ++k) {
-    const double p[3] = {c[k].lx, c[k].ly, 1.0}, q[3] = {c[k].rx, c[k].ry, 1.0};
-    double Ep[3], Etq[2];
-    pose_residual(E, p[0], p[1], q[0], q[1], Ep, Etq);  // for E p and E^T q
-    const double num = q[0] * Ep[0] + q[1] * Ep[1] + Ep[2];
-    const double sqrDenom = Ep[0] * Ep[0] + Ep[1] * Ep[1] + Etq[0] * Etq[0] + Etq[1] * Etq[1];
-    const double denom = sqrt(sqrDenom);
-    const double invDenom = 1.0 / denom;
-    const double invSqrDenom = 1.0 / sqrDenom;
-    double outer[9];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) {
-        const double numDer = (i < 2 ? q[i] : 1.0) * (j < 2 ? p[j] : 1.0);
-        double sq = 0.0;  // d(sqrDenom)/dE_ij
-        if (i < 2 && j < 2) sq = 2 * Ep[i] * p[j] + 2 * Etq[j] * q[i];
-        else if (i < 2) sq = 2 * Ep[i];
-        else if (j < 2) sq = 2 * Etq[j];
-        outer[3 * i + j] = (numDer * denom - num * 0.5 * invDenom * sq) * invSqrDenom;
-      }
     double J[6];
-    for (int col = 0; col < 6; ++col) {
-      double v = 0.0;
-      for (int j = 0; j < 9; ++j) v += outer[j] * inner[j][col];
-      J[col] = v;
-    }
+    pose_jacobian_row(E, inner, c[k].lx, c[k].ly, c[k].rx, c[k].ry, J);
     for (int a = 0; a < 6; ++a) {
       for (int b = 0; b < 6; ++b) JtJ[6 * a + b] += J[a] * J[b];
       Jte[a] += J[a] * e[k];

@@ -22,7 +22,13 @@
 //                   budget) over them in loop order, its state carried to the next round;
 // and at the end
 //   k_rs_finish     pose, error and inlier flags of the chosen candidate.
-// The loop's iterative refinement (mode.iterativeRefinement) is not run.
+// With the loop's iterative refinement (mode.iterativeRefinement, v3dm_ransac_set_refinement),
+// k_rs_select refines each accepted pose as reconstruction_common.cpp:255-314 does: the pose of the
+// accepted sample is refined by refineRelativePose (v3d_poseutilities.cpp:1063-1101: Levenberg-
+// Marquardt on the weighted Sampson residuals of the candidate's inliers; ess::refine_pose restates
+// it, here with its sums over the inliers split across the warp), the refined F is scored over all
+// correspondences in the loop's order, and the loop keeps min(cost, refined cost), the refined
+// model and the refined inlier count for its sample budget.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -289,15 +295,160 @@ __device__ __forceinline__ int rs_budget(double outlierRatio) {
   return (int)N;
 }
 
+// Warp-wide sum: every lane gets the same bits (xor butterfly; double addition commutes).
+__device__ __forceinline__ double rs_wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// F = (invK2^T E) invK1, the reference's product order (reconstruction_common.cpp:271).
+__device__ void rs_fund(const double* invK1, const double* invK2t, const double* E, double* F) {
+  double tmp[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += invK2t[3 * i + k] * E[3 * k + j];
+      tmp[3 * i + j] = v;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += tmp[3 * i + k] * invK1[3 * k + j];
+      F[3 * i + j] = v;
+    }
+}
+
+// One pass of the refinement over the inliers of F0 (Sampson distance below thr2, the set the
+// reference hands to refineRelativePose): RelativePoseMinimizer's weights at pose (Rw, Tw), the
+// weighted residuals at (R, T) and, with derivs, the normal equations (ess::pose_weighted_residual
+// and ess::pose_normal_equations per correspondence).  Returns |e|^2; every lane gets the sums.
+__device__ double rs_lm_pass(const float4* __restrict__ px, const double4* __restrict__ nm, int n, const double* F0,
+                             double thr2, const double* invK1, const double* invK2t, double thr, const double* Rw,
+                             const double* Tw, const double* R, const double* T, bool derivs, double* JtJ,
+                             double* Jte) {
+  double Ew[9], Fw[9], E[9], inner[9][6], a[3], b[2];
+  ess::pose_essential(Rw, Tw, Ew);
+  rs_fund(invK1, invK2t, Ew, Fw);
+  ess::pose_essential(R, T, E);
+  if (derivs) ess::pose_inner(E, R, inner);
+  double err = 0.0, jtj[21], jte[6];
+  for (int k = 0; k < 21; ++k) jtj[k] = 0.0;
+  for (int k = 0; k < 6; ++k) jte[k] = 0.0;
+  for (int k = threadIdx.x & 31; k < n; k += 32) {
+    const float4 c = px[k];
+    if (!(ess::sampson(F0, c.x, c.y, c.z, c.w) < thr2)) continue;
+    const double4 q = nm[k];
+    const double ew = ess::pose_residual(Fw, c.x, c.y, c.z, c.w, a, b);
+    const double w = (fabs(ew) < thr) ? 1.0 : sqrt(thr / fabs(ew));
+    const double ek = w * (0.0 - ess::pose_residual(E, q.x, q.y, q.z, q.w, a, b));
+    err += ek * ek;
+    if (derivs) {
+      double J[6];
+      ess::pose_jacobian_row(E, inner, q.x, q.y, q.z, q.w, J);
+      int t = 0;
+      for (int i = 0; i < 6; ++i) {
+        for (int j = i; j < 6; ++j) jtj[t++] += J[i] * J[j];
+        jte[i] += J[i] * ek;
+      }
+    }
+  }
+  if (derivs) {
+    int t = 0;
+    for (int i = 0; i < 6; ++i) {
+      for (int j = i; j < 6; ++j) {
+        const double v = rs_wsum(jtj[t++]);
+        JtJ[6 * i + j] = v;
+        JtJ[6 * j + i] = v;
+      }
+      Jte[i] = rs_wsum(jte[i]);
+    }
+  }
+  return rs_wsum(err);
+}
+
+// refineRelativePose on the inliers of F0: the Levenberg-Marquardt loop of ess::refine_pose
+// (SimpleLevenbergOptimizer's damping schedule and stopping rules), warp-uniform.
+__device__ void rs_refine_warp(const float4* __restrict__ px, const double4* __restrict__ nm, int n, const double* F0,
+                               double thr2, const double* invK1, const double* invK2t, double thr, double* R,
+                               double* T) {
+  double lambda = 1e-3, JtJ[36], Jte[6], N[36], delta[6], Rs[9], Ts[3];
+  bool computeDerivatives = true;
+  for (int it = 0; it < 50; ++it) {
+    const double err = rs_lm_pass(px, nm, n, F0, thr2, invK1, invK2t, thr, R, T, R, T, computeDerivatives, JtJ, Jte);
+    double gmax = 0.0;
+    for (int k = 0; k < 6; ++k) gmax = fmax(gmax, fabs(Jte[k]));
+    if (gmax < 1e-8) return;
+    if (it == 0) {
+      double maxEl = -1e30;
+      for (int k = 0; k < 6; ++k) maxEl = fmax(maxEl, JtJ[7 * k]);
+      lambda = 1e-3 * maxEl;
+    }
+    for (int k = 0; k < 36; ++k) N[k] = JtJ[k];
+    for (int k = 0; k < 6; ++k) N[7 * k] += lambda;
+    if (!ess::cholesky_solve6(N, Jte, delta)) return;
+    double dl = 0.0;
+    for (int k = 0; k < 6; ++k) dl += delta[k] * delta[k];
+    dl = sqrt(dl);
+    if (it >= 10 && dl < 1e-8 * (4.0 + 1e-8)) return;
+    for (int k = 0; k < 9; ++k) Rs[k] = R[k];
+    for (int k = 0; k < 3; ++k) Ts[k] = T[k];
+    ess::pose_update(Rs, Ts, delta, R, T);
+    const double errNew = rs_lm_pass(px, nm, n, F0, thr2, invK1, invK2t, thr, Rs, Ts, R, T, false, nullptr, nullptr);
+    double rho = err - errNew;
+    double d1 = 0.0, d2 = 0.0;
+    for (int k = 0; k < 6; ++k) {
+      d1 += delta[k] * delta[k];
+      d2 += delta[k] * Jte[k];
+    }
+    rho = rho / (lambda * d1 + d2);
+    if (rho > 0) {
+      lambda = fmax(1e-10, lambda * 0.1);
+      computeDerivatives = true;
+    } else {
+      for (int k = 0; k < 9; ++k) R[k] = Rs[k];
+      for (int k = 0; k < 3; ++k) T[k] = Ts[k];
+      lambda *= 10.0;
+      computeDerivatives = false;
+    }
+  }
+}
+
+// sum_i min(d_i, thr2) over all correspondences in index order (the loop's sum, as k_rs_score
+// forms it) and the count of d_i < thr2; every lane gets both.
+__device__ void rs_cost_in_order(const float4* __restrict__ px, int n, const double* F, double thr2, double* cost,
+                                 int* nIn) {
+  const int lane = threadIdx.x & 31;
+  double sum = 0.0;
+  int cnt = 0;
+  for (int k0 = 0; k0 < n; k0 += 32) {
+    double t = 0.0;
+    bool in = false;
+    if (k0 + lane < n) {
+      const float4 c = px[k0 + lane];
+      t = ess::sampson_truncated(F, (double)c.x, (double)c.y, (double)c.z, (double)c.w, thr2, in);
+    }
+    cnt += __popc(__ballot_sync(0xffffffffu, in));
+    const int m = min(32, n - k0);
+    for (int l = 0; l < m; ++l) sum = ess::dadd(sum, __shfl_sync(0xffffffffu, t, l));
+  }
+  *cost = sum;
+  *nIn = cnt;
+}
+
 // One warp per pair: the round's costs, pose flags and inlier counts staged in shared memory by
-// the warp (coalesced), then lane 0 walks the loop over the round's samples in order (the rule of
-// reconstruction_common.cpp:177-335 without refinement); the last accepted candidate's E and F are
-// kept (the warp copies them).
+// the warp (coalesced), then the loop over the round's samples in order (the rule of
+// reconstruction_common.cpp:177-335).  Without refinement lane 0 walks it and the warp copies the
+// last accepted candidate's E and F; with refinement every lane walks it (the same decisions) and
+// the warp refines each accepted pose, keeping the refined E, F, R and T.
+template <bool kRefine>
 __global__ void __launch_bounds__(32)
 k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
             const int8_t* __restrict__ counts, const uint8_t* __restrict__ slotOk, const double* __restrict__ cost,
             const int32_t* __restrict__ inl, const double* __restrict__ slots, RsState* __restrict__ st,
-            double* __restrict__ bestEF) {
+            double* __restrict__ bestEF, const float4* __restrict__ corrs, const double4* __restrict__ norm,
+            const int32_t* __restrict__ samples, const double* __restrict__ invK, double thr, double thr2,
+            double* __restrict__ bestRT) {
   const int p = blockIdx.x;
   const int lane = threadIdx.x;
   __shared__ double sCost[kRsRound * kRsMaxSol];
@@ -319,6 +470,59 @@ k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, 
     }
   }
   __syncwarp();
+  if constexpr (kRefine) {
+    const int b = offsets[p], n = offsets[p + 1] - b;
+    double invK1[9], invK2t[9];
+    for (int k = 0; k < 9; ++k) invK1[k] = invK[(size_t)p * 18 + k];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) invK2t[3 * i + j] = invK[(size_t)p * 18 + 9 + 3 * j + i];
+    for (int j = 0; j < len; ++j) {
+      if (s.drawn > s.budget) break;
+      ++s.drawn;
+      const int ns = sCnt[j];
+      for (int r = 0; r < ns; ++r) {
+        const int idx = j * kRsMaxSol + r;
+        if (!(sCost[idx] < s.minError)) continue;
+        if (!sOk[idx]) continue;
+        double EF[kRsSlotDoubles];
+        for (int k = 0; k < kRsSlotDoubles; ++k) EF[k] = slots[(base * kRsMaxSol + idx) * kRsSlotDoubles + k];
+        const int32_t* smp = samples + ((long long)p * nDraw + s0 + j) * 5;
+        double x1[5], y1[5], x2[5], y2[5];
+        for (int k = 0; k < 5; ++k) {
+          const double4 v = norm[b + smp[k]];
+          x1[k] = v.x;
+          y1[k] = v.y;
+          x2[k] = v.z;
+          y2[k] = v.w;
+        }
+        double R[9], T[3];
+        if (!ess::essential_pose(EF, 5, x1, y1, x2, y2, R, T)) continue;  // relativePoseFromEssential
+        rs_refine_warp(corrs + b, norm + b, n, EF + 9, thr2, invK1, invK2t, thr, R, T);
+        double Er[9], Fr[9], costR;
+        int nInR;
+        ess::pose_essential(R, T, Er);
+        rs_fund(invK1, invK2t, Er, Fr);
+        rs_cost_in_order(corrs + b, n, Fr, thr2, &costR, &nInR);
+        s.minError = fmin(sCost[idx], costR);
+        s.chosen = s0 + j;
+        const float frac = (float)(nInR - 5) / (float)(n - 5);
+        s.budget = min(s.budget, rs_budget(1.0 - (double)frac));
+        double* ef = bestEF + (size_t)p * kRsSlotDoubles;
+        double* rt = bestRT + (size_t)p * 12;
+        if (lane < 9) {
+          ef[lane] = Er[lane];
+          ef[9 + lane] = Fr[lane];
+          rt[lane] = R[lane];
+        } else if (lane < 12) {
+          rt[lane] = T[lane - 9];
+        }
+      }
+    }
+    if (lane == 0) {
+      if (s.drawn > s.budget || s0 + len >= nDraw) s.done = 1;
+      st[p] = s;
+    }
+  } else {
   if (lane == 0) {
     const int n = offsets[p + 1] - offsets[p];
     int accepted = -1;
@@ -345,13 +549,14 @@ k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, 
   const int accepted = sAccepted;
   if (accepted >= 0 && lane < kRsSlotDoubles)
     bestEF[(size_t)p * kRsSlotDoubles + lane] = slots[(base * kRsMaxSol + accepted) * kRsSlotDoubles + lane];
+  }
 }
 
 // One thread per pair: E, F, R, T and error of the choice.
 __global__ void k_rs_finish(const int32_t* __restrict__ offsets, int nPairs, int nDraw,
                             const int32_t* __restrict__ samples, const double4* __restrict__ norm,
                             const RsState* __restrict__ st, const double* __restrict__ bestEF,
-                            double* __restrict__ out) {
+                            double* __restrict__ out, int refine, const double* __restrict__ bestRT) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nPairs) return;
   double* o = out + (size_t)p * 31;  // E 9, F 9, R 9, T 3, error 1
@@ -373,7 +578,11 @@ __global__ void k_rs_finish(const int32_t* __restrict__ offsets, int nPairs, int
   }
   const double* ef = bestEF + (size_t)p * kRsSlotDoubles;
   for (int k = 0; k < 18; ++k) o[k] = ef[k];
-  ess::essential_pose(ef, 5, x1, y1, x2, y2, o + 18, o + 27);
+  if (refine) {  // the refined pose (reconstruction_common.cpp:321-322)
+    for (int k = 0; k < 12; ++k) o[18 + k] = bestRT[(size_t)p * 12 + k];
+  } else {
+    ess::essential_pose(ef, 5, x1, y1, x2, y2, o + 18, o + 27);
+  }
   o[30] = s.minError / n;
 }
 
@@ -470,6 +679,10 @@ struct v3dm_ransac {
   size_t stateCap = 0;
   double* dBestEF = nullptr;
   size_t bestEFCap = 0;
+  double* dBestRT = nullptr;   // refined R, T per pair (iterative refinement)
+  size_t bestRTCap = 0;
+  bool refine = false;         // RobustOrientationMode::iterativeRefinement
+  double thr = 0.0;            // inlier threshold of the call (pixels)
   unsigned long long* dWork = nullptr;  // candidates, Sampson evaluations of the last call
   size_t workCap = 0;
   double* dOut = nullptr;
@@ -516,6 +729,7 @@ int rs_enqueue(v3dm_ransac* r, int nPairs, int nCorrs, int nDraw, int nSamples, 
     r->dState = st;
   }
   V3DM_RS_TRY(rs_grow(r->dBestEF, r->bestEFCap, (size_t)nPairs * kRsSlotDoubles));
+  V3DM_RS_TRY(rs_grow(r->dBestRT, r->bestRTCap, (size_t)nPairs * 12));
   V3DM_RS_TRY(rs_grow(r->dWork, r->workCap, (size_t)2));
   RsState* state = static_cast<RsState*>(r->dState);
   int launches = 0;
@@ -546,12 +760,18 @@ int rs_enqueue(v3dm_ransac* r, int nPairs, int nCorrs, int nDraw, int nSamples, 
     k_rs_score<<<dim3(nPairs, chunks), kRsScoreThreads, 0, r->stream>>>(r->dOffsets, dCorrs, r->dList, r->dListN,
                                                                        r->dSlots, thr2, r->dCost, r->dInl);
     V3DM_RS_TRY(rs_mark(r, 1));
-    k_rs_select<<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
-                                               r->dCost, r->dInl, r->dSlots, state, r->dBestEF);
+    if (r->refine)
+      k_rs_select<true><<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
+                                                      r->dCost, r->dInl, r->dSlots, state, r->dBestEF, dCorrs,
+                                                      r->dNorm, dSamples, r->dInvK, r->thr, thr2, r->dBestRT);
+    else
+      k_rs_select<false><<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
+                                                       r->dCost, r->dInl, r->dSlots, state, r->dBestEF, dCorrs,
+                                                       r->dNorm, dSamples, r->dInvK, r->thr, thr2, r->dBestRT);
     launches += 4;
   }
   k_rs_finish<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm, state,
-                                                           r->dBestEF, dOut);
+                                                           r->dBestEF, dOut, r->refine ? 1 : 0, r->dBestRT);
   V3DM_RS_TRY(cudaMemsetAsync(dNIn, 0, (size_t)nPairs * sizeof(int32_t), r->stream));
   launches += 1;
   if (nCorrs > 0) {
@@ -596,7 +816,7 @@ int v3dm_ransac_destroy(v3dm_ransac* r) {
   cudaStreamSynchronize(r->stream);
   void* bufs[] = {r->dOffsets, r->dCorrs, r->dNorm, r->dInvK, r->dSamples, r->dSlots, r->dSlotOk, r->dCounts,
                   r->dList,    r->dListN, r->dCost, r->dInl,  r->dState,   r->dBestEF, r->dWork,  r->dOut,
-                  r->dFlags,   r->dNIn};
+                  r->dFlags,   r->dNIn,   r->dBestRT};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 2; ++k)
@@ -678,6 +898,7 @@ int v3dm_ransac_essential(v3dm_ransac* r, int nPairs, const int32_t* offsets, co
   if (samples)
     V3DM_RS_TRY(cudaMemcpyAsync(r->dSamples, samples, (size_t)nPairs * nDraw * 5 * sizeof(int32_t),
                                 cudaMemcpyHostToDevice, r->stream));
+  r->thr = inlierThreshold;
   st = rs_enqueue(r, nPairs, nCorrs, nDraw, nSamples, samples == nullptr, seed, inlierThreshold * inlierThreshold,
                   r->dCorrs, r->dSamples, r->dOut, r->dNIn, r->dFlags);
   if (st != V3DM_OK) return st;
@@ -706,8 +927,17 @@ int v3dm_ransac_essential_device(v3dm_ransac* r, int nPairs, const int32_t* offs
   st = rs_stage(r, nPairs, offsets, K, nDraw);
   if (st != V3DM_OK) return st;
   int32_t* dS = d_samples ? const_cast<int32_t*>(d_samples) : r->dSamples;
+  r->thr = inlierThreshold;
   return rs_enqueue(r, nPairs, nCorrs, nDraw, nSamples, d_samples == nullptr, seed, inlierThreshold * inlierThreshold,
                     reinterpret_cast<const float4*>(d_corrs), dS, d_models, d_nInliers, d_inlierFlags);
+}
+
+int v3dm_ransac_set_refinement(v3dm_ransac* r, int enable) {
+  if (!r) return V3DM_ERR_ARG;
+  RsDeviceGuard g(r->device);
+  V3DM_RS_TRY(cudaStreamSynchronize(r->stream));
+  r->refine = enable != 0;
+  return V3DM_OK;
 }
 
 int v3dm_ransac_candidates(v3dm_ransac* r, long long* nCandidates, long long* nEvaluations) {

@@ -111,6 +111,48 @@ def test_reference_sample_sequence_gives_the_reference_choice(v3dm_mod, oracle_m
         assert agree >= 0.97 * total, (agree, total)
 
 
+@pytest.mark.parametrize("n_pairs,n_min,n_max,thr,n_samples", [(30, 300, 1500, 2.0, 1000), (6, 2500, 4000, 1.0, 500)])
+def test_iterative_refinement_gives_the_reference_result(v3dm_mod, oracle_mod, n_pairs, n_min, n_max, thr,
+                                                         n_samples):
+    """mode.iterativeRefinement (set by the apps): each accepted pose refined on its inliers
+    (refineRelativePose), the loop continuing from the refined cost and inlier count.  With the
+    reference's own sample sequence, the same model (unit E within 1e-5) on >= 97% of the pairs
+    (as without refinement: the same candidate choice), and for those the refined error, R and T
+    to 1e-4 (the refinement's sums over the inliers are summed in another order) and the inlier
+    flags to 0.2% of the correspondences; all pairs, batched in one call, give the same models."""
+    _need_ref(oracle_mod)
+    off, corrs, K, R, t, inl = synth.two_view_pairs(n_pairs + 7 * n_min, n_pairs=n_pairs, n_min=n_min, n_max=n_max)
+    seqs = [v3dm_mod.ransac_shuffle_samples(int(off[p + 1] - off[p]), n_samples, 300 + p) for p in range(n_pairs)]
+    n_draw = max(s.shape[0] for s in seqs)
+    padded = np.stack([np.concatenate([s, np.repeat(s[-1:], n_draw - s.shape[0], 0)]) for s in seqs])
+    with v3dm_mod.Ransac() as r:
+        r.set_refinement(True)
+        allp = r.essential(off, corrs, K, thr, n_samples, samples=padded)
+        r.set_refinement(False)
+        plain = r.essential(off, corrs, K, thr, n_samples, samples=padded)
+    agree, moved = 0, 0
+    for p in range(n_pairs):
+        c = corrs[off[p]:off[p + 1]]
+        n = c.shape[0]
+        ref = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], thr, n_samples, seqs[p], refine=True)
+        if ref["chosen"] < 0 or allp["n_inliers"][p] < 0:
+            agree += ref["chosen"] < 0 and allp["n_inliers"][p] < 0
+            continue
+        moved += np.abs(allp["R"][p] - plain["R"][p]).max() > 1e-9
+        if np.linalg.norm(_unit(allp["E"][p]) - _unit(ref["model"][:9])) < 1e-5:
+            agree += 1
+            np.testing.assert_allclose(allp["error"][p], ref["model"][30], rtol=1e-4)
+            assert np.abs(allp["R"][p].reshape(-1) - ref["model"][18:27]).max() < 1e-4
+            assert np.abs(allp["T"][p] - ref["model"][27:30]).max() < 1e-4
+            slack = max(2, n // 500)
+            fl = allp["flags"][off[p]:off[p + 1]]
+            assert int((fl != ref["flags"]).sum()) <= slack
+            assert abs(int(allp["n_inliers"][p]) - ref["n_inliers"]) <= slack
+    print(f"refinement: {agree} of {n_pairs} pairs agree with the reference; {moved} poses moved by it")
+    assert agree >= 0.97 * n_pairs, (agree, n_pairs)
+    assert moved > 0  # the refinement does change the poses
+
+
 def test_batched_call_with_small_pairs(v3dm_mod):
     """A batch that mixes pairs with fewer than 5 correspondences (no model: -1, no inlier flags) with
     ordinary ones; single-pair calls of the same data run."""
