@@ -68,7 +68,7 @@ def lib() -> C.CDLL:
         L.v3dm_deallocate.argtypes = [vp]
         for n in ("v3dm_set_left_f32", "v3dm_set_right_f32", "v3dm_set_left_u8", "v3dm_set_right_u8",
                   "v3dm_set_left_f32_bf16x3", "v3dm_set_right_f32_bf16x3", "v3dm_set_left_u8_device",
-                  "v3dm_set_right_u8_device"):
+                  "v3dm_set_right_u8_device", "v3dm_set_left_f32_device", "v3dm_set_right_f32_device"):
             getattr(L, n).argtypes = [vp, i32, vp]
         L.v3dm_features_read.argtypes = [C.c_char_p, i32, C.POINTER(i32)] + [vp] * 6
         L.v3dm_quantize_u8_device.argtypes = [vp, C.c_longlong, vp, vp]
@@ -77,6 +77,8 @@ def lib() -> C.CDLL:
         L.v3dm_loader_load.argtypes = [vp, i32, C.POINTER(C.c_char_p), i32, i32, vp]
         L.v3dm_loader_positions.argtypes = [vp, vp]
         L.v3dm_loader_descriptors_device.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_longlong)]
+        L.v3dm_loader_descriptors_f32_device.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_longlong)]
+        L.v3dm_loader_exact_u8.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_scores_f32.argtypes = [vp, vp]
         L.v3dm_float_threshold.argtypes = [f32, f32, C.POINTER(C.c_float)]
         L.v3dm_putative.argtypes = [vp, f32, f32, vp, i32, C.POINTER(i32)]
@@ -104,6 +106,8 @@ def lib() -> C.CDLL:
         L.v3dm_voctree_quantize_f32.argtypes = [vp, i32, vp, vp, i32]
         L.v3dm_voctree_quantize_u8.argtypes = [vp, i32, vp, vp, i32]
         L.v3dm_voctree_quantize_u8_device.argtypes = [vp, i32, vp, vp, i32]
+        L.v3dm_voctree_quantize_f32_device.argtypes = [vp, i32, vp, vp, i32]
+        L.v3dm_voctree_replays.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.v3dm_voctree_stream.argtypes = [vp, C.POINTER(vp)]
         i64, i64p = C.c_longlong, C.POINTER(C.c_longlong)
         L.v3dm_batch_create.argtypes = [C.POINTER(vp), i32]
@@ -150,6 +154,7 @@ def lib() -> C.CDLL:
         L.v3dm_ransac_essential_device.argtypes = [vp, i32, vp, vp, vp, C.c_double, i32, i32, vp, C.c_uint64, vp,
                                                    vp, vp]
         L.v3dm_ransac_wait.argtypes = [vp]
+        L.v3dm_ransac_set_refinement.argtypes = [vp, i32]
         L.v3dm_ransac_profile.argtypes = [vp, i32]
         L.v3dm_ransac_candidates.argtypes = [vp, i64p, i64p]
         L.v3dm_ransac_profile_read.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
@@ -258,6 +263,16 @@ class SIFTMatching:
 
     def set_right_features_device(self, d_desc: int, n: int):
         _check(lib().v3dm_set_right_u8_device(self._h, n, C.c_void_p(d_desc)), "setRightFeatures")
+        self.n_right = n
+
+    def set_left_features_f32_device(self, d_desc: int, n: int):
+        """Float descriptors already in device memory (v3dm_set_left_f32_device): u/512 values
+        take the exact integer path, others the BF16 hi/lo path."""
+        _check(lib().v3dm_set_left_f32_device(self._h, n, C.c_void_p(d_desc)), "setLeftFeatures")
+        self.n_left = n
+
+    def set_right_features_f32_device(self, d_desc: int, n: int):
+        _check(lib().v3dm_set_right_f32_device(self._h, n, C.c_void_p(d_desc)), "setRightFeatures")
         self.n_right = n
 
     def set_left_features_bf16x3(self, desc: np.ndarray):
@@ -419,6 +434,17 @@ class VocabularyTreeTraversal:
     def quantize_device(self, n: int, d_keys: int, d_ids: int, id_mode: int = LEAF_GLOBAL):
         _check(lib().v3dm_voctree_quantize_u8_device(self._h, n, C.c_void_p(d_keys), C.c_void_p(d_ids), id_mode),
                "quantize_device")
+
+    def quantize_f32_device(self, n: int, d_keys: int, d_ids: int, id_mode: int = LEAF_GLOBAL):
+        """Float keys in device memory, the reference CPU tree's sequential FP32 order."""
+        _check(lib().v3dm_voctree_quantize_f32_device(self._h, n, C.c_void_p(d_keys), C.c_void_p(d_ids), id_mode),
+               "quantize_f32_device")
+
+    def replays(self) -> int:
+        """Key-levels decided by the sequential replay since the tree was created."""
+        n = C.c_longlong(0)
+        _check(lib().v3dm_voctree_replays(self._h, C.byref(n)), "replays")
+        return n.value
 
     def stream(self) -> int:
         s = C.c_void_p()
@@ -657,6 +683,8 @@ class Projection:
 # ---- feature files ----------------------------------------------------------------------------
 
 LOAD_ROUND32 = 1
+LOAD_KEEP_F32 = 2
+LOAD_LOSSY_U8 = 4
 ERR_IO = 11
 
 
@@ -684,8 +712,10 @@ def quantize_u8_device(d_values: int, n_values: int, d_out: int, stream: int = 0
 
 
 class Loader:
-    """Feature-file loader (v3dm_loader_*): many files at once, descriptors re-quantised to u8
-    on the device."""
+    """Feature-file loader (v3dm_loader_*): many files at once, descriptors copied to the device
+    in one transfer.  They become u8 there when every value is u/512; the extractors' unit-L2
+    floats are kept as floats with LOAD_KEEP_F32 (for the float matcher), refused by default
+    (V3DMError NOT_U8), or rounded with LOAD_LOSSY_U8."""
 
     def __init__(self, device: int = 0):
         h = C.c_void_p()
@@ -722,8 +752,22 @@ class Loader:
         _check(lib().v3dm_loader_descriptors_device(self._h, C.byref(p), C.byref(n)), "loader_descriptors_device")
         return p.value or 0, n.value
 
+    def descriptors_f32_device(self):
+        """(device pointer of the float descriptors, their count); after a LOAD_KEEP_F32 load."""
+        p, n = C.c_void_p(), C.c_longlong(0)
+        _check(lib().v3dm_loader_descriptors_f32_device(self._h, C.byref(p), C.byref(n)),
+               "loader_descriptors_f32_device")
+        return p.value or 0, n.value
+
+    def exact_u8(self) -> bool:
+        """True when every descriptor value of the last load was exactly u/512."""
+        e = C.c_int(0)
+        _check(lib().v3dm_loader_exact_u8(self._h, C.byref(e)), "loader_exact_u8")
+        return bool(e.value)
+
     def positions(self) -> np.ndarray:
-        _, n = self.descriptors_device()
+        p, n = C.c_void_p(), C.c_longlong(0)
+        lib().v3dm_loader_descriptors_device(self._h, C.byref(p), C.byref(n))
         out = np.empty((n, 2), np.float32)
         _check(lib().v3dm_loader_positions(self._h, _ptr(out)), "loader_positions")
         return out
@@ -891,6 +935,10 @@ class Ransac:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_refinement(self, enable: bool) -> None:
+        """RobustOrientationMode::iterativeRefinement (the apps switch it on)."""
+        _check(lib().v3dm_ransac_set_refinement(self._h, int(bool(enable))), "ransac_set_refinement")
 
     def essential(self, offsets, corrs, K, inlier_threshold: float, n_samples: int = 1000, samples=None,
                   n_draw: int | None = None, seed: int = 0, flags: bool = True):

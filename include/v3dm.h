@@ -95,6 +95,12 @@ V3DM_API int v3dm_set_right_f32(v3dm_matcher* h, int n, const float* desc);
  * it is exact).  Non-finite values: V3DM_ERR_ARG. */
 V3DM_API int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* desc);
 V3DM_API int v3dm_set_right_f32_bf16x3(v3dm_matcher* h, int n, const float* desc);
+/* setLeftFeatures / setRightFeatures (.cu:490-520) with the float descriptors already in
+ * device memory (for instance a loader's float descriptors, V3DM_LOAD_KEEP_F32 below); the
+ * same rules as v3dm_set_left_f32: u/512 values take the exact integer path, other finite
+ * values the BF16 hi/lo path on a tcgen05 handle. */
+V3DM_API int v3dm_set_left_f32_device(v3dm_matcher* h, int n, const float* d_desc);
+V3DM_API int v3dm_set_right_f32_device(v3dm_matcher* h, int n, const float* d_desc);
 /* Diagnostic: the BF16 hi/lo scores of the current descriptors, nLeft x nRight floats (row =
  * left), at most 2^26 of them. */
 V3DM_API int v3dm_scores_f32(v3dm_matcher* h, float* scores);
@@ -305,17 +311,31 @@ V3DM_API int v3dm_voctree_destroy(v3dm_voctree* t);
 V3DM_API int v3dm_voctree_counts(int branchFactor, int depth, int64_t* nodeCount, int64_t* leafCount);
 /* allocate(nMaxFeatures) / deallocate (v3d_cudamatching.h:73-74, .cu:803-829). */
 V3DM_API int v3dm_voctree_allocate(v3dm_voctree* t, int nMax);
-/* setNodes(nodes) (v3d_cudamatching.h:76, .cu:831-843): nodeCount x 128 descriptors in
- * breadth-first order without the root.  Float nodes and keys follow the matcher's
- * convention: u/512 with u in 0..255 (else V3DM_ERR_NOT_U8).  For such data every FP32 dot
- * product of the reference is exact, so leaf ids do not depend on summation order. */
+/* setNodes(nodes) (v3d_cudamatching.h:76, .cu:831-843) and VocabularyTree::loadTreeFromFile's
+ * node array (v3d_voctree.h:38-52): nodeCount x 128 descriptors in breadth-first order without
+ * the root.  Float nodes may hold any finite values (the apps' trees are k-means centres of
+ * unit-L2 descriptors); u8 nodes are u/512 values. */
 V3DM_API int v3dm_voctree_set_nodes_f32(v3dm_voctree* t, const float* nodes);
 V3DM_API int v3dm_voctree_set_nodes_u8(v3dm_voctree* t, const uint8_t* nodes);
-/* traverseTree(n, features, leaveIds) (v3d_cudamatching.h:78, .cu:845-863). */
+/* traverseTree(n, features, leaveIds) (v3d_cudamatching.h:78, .cu:845-863) and
+ * VocabularyTree::getVisualWord (v3d_voctree.h:56-79, with V3DM_LEAF_LOCAL).  The ids are those
+ * of the reference's CPU descent, VocabularyTree::findBestNodeIndex (v3d_voctree.h:82-99): each
+ * dot product is the sequential FP32 sum over i = 0..127 of the rounded products key[i] *
+ * node[i], and the first child whose score is strictly above the running maximum (initially
+ * -1e30f) wins.  For u/512 data every such sum is exact, and the integer descent is used.
+ * (The reference's GPU kernel, .cu:705-792, sums in a different order with fast-math and can
+ * differ from its CPU tree at near ties of float data; the CPU order is the one the apps use.)
+ * V3DM_ERR_ARG when the tree holds values that make a descent leave the node array. */
 V3DM_API int v3dm_voctree_quantize_f32(v3dm_voctree* t, int n, const float* keys, int32_t* ids, int idMode);
 V3DM_API int v3dm_voctree_quantize_u8(v3dm_voctree* t, int n, const uint8_t* keys, int32_t* ids, int idMode);
-/* Device-resident variant: keys and ids in device memory, asynchronous on the tree's stream. */
+/* Device-resident variants: keys and ids in device memory, asynchronous on the tree's stream.
+ * The u8 variant needs a u/512 tree (else V3DM_ERR_NOT_U8). */
 V3DM_API int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode);
+V3DM_API int v3dm_voctree_quantize_f32_device(v3dm_voctree* t, int n, const float* d_keys, int32_t* d_ids,
+                                              int idMode);
+/* Diagnostic: key-levels, since the tree was created, whose float scores were too close to
+ * decide from the fast pass and were replayed in the reference's sequential order. */
+V3DM_API int v3dm_voctree_replays(v3dm_voctree* t, long long* n);
 V3DM_API int v3dm_voctree_stream(v3dm_voctree* t, void** stream);
 
 /* ---- feature files ------------------------------------------------------------------ */
@@ -336,11 +356,23 @@ V3DM_API int v3dm_quantize_u8_device(const float* d_values, long long nValues, u
 /* Loader: the apps read one feature file per image and copy each pair's descriptors to the
  * matcher (match_sequence.cpp:124-146, 183-186, 214-231).  A loader reads many files at once
  * (host threads, one file each at a time), keeps the positions on the host, and copies all
- * descriptors to the device in one transfer from pinned memory, re-quantised there to u8 for the
- * u8 matchers (v3dm_batch_set_images_u8_device, v3dm_set_left_u8_device).  No counterpart in
- * the reference. */
+ * descriptors to the device in one transfer from pinned memory.  No counterpart in the
+ * reference.
+ * The extractors store unit-L2 floats (SIFT_Feature::normalizeDescriptor, v3d_feature.h:19-39,
+ * called by Apps/SfM/extract_sift_*.cpp), which are not of the form u/512 in general; the
+ * reference's matcher scores them in FP32.  So:
+ *   - by default the descriptors become u8 only when every value is exactly u/512 (u = 0..255);
+ *     otherwise the load returns V3DM_ERR_NOT_U8 (nothing is rounded silently);
+ *   - V3DM_LOAD_KEEP_F32 keeps the float descriptors on the device (v3dm_loader_descriptors_
+ *     f32_device) for v3dm_set_left_f32_device / v3dm_set_right_f32_device, which score
+ *     non-u/512 values with the BF16 hi/lo path; the load then succeeds whatever the values,
+ *     and u8 descriptors exist only when they are all u/512;
+ *   - V3DM_LOAD_LOSSY_U8 re-quantises any values to u = round(512 x) clamped to 0..255 (lossy
+ *     for unit-L2 floats: scores and pairs can differ from the reference's). */
 typedef struct v3dm_loader v3dm_loader;
-#define V3DM_LOAD_ROUND32 1 /* keep a multiple of 32 features per file, as the apps' '& 0xffe0' */
+#define V3DM_LOAD_ROUND32 1  /* keep a multiple of 32 features per file, as the apps' '& 0xffe0' */
+#define V3DM_LOAD_KEEP_F32 2 /* keep the float descriptors on the device                      */
+#define V3DM_LOAD_LOSSY_U8 4 /* round any values to u8 (lossy unless they are u/512)           */
 V3DM_API int v3dm_loader_create(int device, v3dm_loader** out);
 V3DM_API int v3dm_loader_destroy(v3dm_loader* ld);
 /* Reads nFiles files; counts[i] = features kept from file i (its first ones: at most
@@ -350,8 +382,14 @@ V3DM_API int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* pa
                               int32_t* counts);
 /* Positions of the kept features (2 floats each), files in order. */
 V3DM_API int v3dm_loader_positions(v3dm_loader* ld, float* positions);
-/* Device u8 descriptors of the kept features (128 bytes each), files in order, and their count. */
+/* Device u8 descriptors of the kept features (128 bytes each), files in order, and their count.
+ * V3DM_ERR_NOT_U8 when the last load kept floats that are not all u/512 (and was not lossy). */
 V3DM_API int v3dm_loader_descriptors_device(v3dm_loader* ld, const uint8_t** d_desc, long long* total);
+/* Device float descriptors of the kept features (128 floats each), files in order, as read from
+ * the files; only after a load with V3DM_LOAD_KEEP_F32 (else V3DM_ERR_NOT_ALLOCATED). */
+V3DM_API int v3dm_loader_descriptors_f32_device(v3dm_loader* ld, const float** d_desc, long long* total);
+/* *exact = 1 when every descriptor value of the last load was exactly u/512, u in 0..255. */
+V3DM_API int v3dm_loader_exact_u8(v3dm_loader* ld, int* exact);
 
 /* ---- retrieval scoring (V3D::LeafDocuments, v3d_voctree.h:105-289) ------------------- */
 /* The image loop of match_using_voctree.cpp:176-222 over visual words: image i is scored
@@ -441,6 +479,14 @@ V3DM_API int v3dm_ransac_essential_device(v3dm_ransac* r, int nPairs, const int3
                                           const int32_t* d_samples, uint64_t seed, double* d_models,
                                           int32_t* d_nInliers, uint8_t* d_inlierFlags);
 V3DM_API int v3dm_ransac_wait(v3dm_ransac* r);
+/* RobustOrientationMode::iterativeRefinement (reconstruction_common.h:631-640; the apps switch it
+ * on, match_sequence.cpp:267): each accepted candidate's pose is refined by refineRelativePose
+ * (v3d_poseutilities.cpp:1063-1101) on its inliers, the loop keeps min(cost, refined cost) and the
+ * refined model, and the refined inlier count sets the sample budget
+ * (reconstruction_common.cpp:255-314).  Off by default, as in the reference.  The refinement's
+ * sums over the inliers run in parallel, so the refined pose agrees with the reference's to
+ * rounding, not bit for bit. */
+V3DM_API int v3dm_ransac_set_refinement(v3dm_ransac* r, int enable);
 /* The sample sequence computeRobustOrientationMLE draws for a pair of N correspondences after
  * srand(seed): getShuffleCount(N, nSamples, 5) shuffles of 0..N-1 (random_shuffle over the C
  * library's rand()), each cut into consecutive 5-tuples while j < N - 5; at most cap tuples are
