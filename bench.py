@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--temperature", type=float, default=0.2, help="proposal workload: InfoNCE temperature")
     ap.add_argument("--rt-images", type=int, default=4096, help="retrieval workload: images in the sequence")
     ap.add_argument("--rs-pairs", type=int, default=256, help="ransac workload: image pairs per call")
+    ap.add_argument("--refine", action="store_true",
+                    help="ransac workload: the loop's iterative refinement (the apps' mode)")
     return ap.parse_args()
 
 
@@ -1375,15 +1377,16 @@ def ransac_data(args, n_pairs):
     return synth.two_view_pairs(args.seed + 7, n_pairs=n_pairs, n_min=500, n_max=3000)
 
 
-def ransac_config(n_pairs, n_corrs):
+def ransac_config(n_pairs, n_corrs, refine=False):
     return {"workload": f"essential-matrix RANSAC of {n_pairs} image pairs ({n_corrs} putative correspondences, "
                         f"500..3000 per pair, 30..80% inliers), nSamples {RS_SAMPLES}, threshold {RS_THR} px, "
-                        "no iterative refinement",
+                        + ("iterative refinement of each accepted pose (the apps' mode)" if refine
+                           else "no iterative refinement"),
             "pairs": n_pairs, "correspondences": n_corrs, "n_samples": RS_SAMPLES, "threshold_px": RS_THR,
-            "l2": "flushed between steps (512 MiB write)"}
+            "iterative_refinement": refine, "l2": "flushed between steps (512 MiB write)"}
 
 
-def ref_ransac_pairs(off, corrs, K, pairs):
+def ref_ransac_pairs(off, corrs, K, pairs, refine=False):
     """The reference loop (its five-point solver and pose recovery, the loop restated) on the given
     pairs with the app's own sample sequence; returns seconds."""
     from oracle import oracle
@@ -1392,7 +1395,7 @@ def ref_ransac_pairs(off, corrs, K, pairs):
         c = corrs[off[p]:off[p + 1]]
         smp = oracle.ref_shuffle_samples(c.shape[0], RS_SAMPLES, 1000 + p)  # the reference's own draws
         t0 = time.perf_counter()
-        oracle.ref_ransac(c, K[p, 0], K[p, 1], RS_THR, RS_SAMPLES, smp)
+        oracle.ref_ransac(c, K[p, 0], K[p, 1], RS_THR, RS_SAMPLES, smp, refine=refine)
         t += time.perf_counter() - t0
     return t
 
@@ -1412,18 +1415,18 @@ def run_reference_ransac(args, ws, rank):
     off, corrs, K, _, _, _ = ransac_data(args, n_pairs)
     k = min(8, n_pairs)
     for w in range(args.warmup):
-        ref_ransac_pairs(off, corrs, K, [(w * 37) % n_pairs])
+        ref_ransac_pairs(off, corrs, K, [(w * 37) % n_pairs], args.refine)
     per_pair = []
     for st in range(args.steps):
         sel = [(st * k + j) * 29 % n_pairs for j in range(k)]
-        per_pair.append(ref_ransac_pairs(off, corrs, K, sel) / k)
+        per_pair.append(ref_ransac_pairs(off, corrs, K, sel, args.refine) / k)
     ms = 1000.0 * statistics.mean(per_pair) * n_pairs
     v = n_pairs * 1000.0 / ms
     line = {
         "impl": "reference", "metric": "image pairs/s robust relative orientation (5-point RANSAC, Sampson costs)",
         "value": v, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, int(off[-1])),
+        "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, int(off[-1]), args.refine),
         "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": 1, "kind": "reference",
                          "sample": f"{k} of the {n_pairs} pairs per step with the app's own sample sequence; "
                                    "whole-call time = mean per pair x pairs"},
@@ -1449,6 +1452,7 @@ def run_ransac(args, ws, rank, local):
     n_corrs = int(off[-1])
     n_draw = RS_SAMPLES + 1
     r = v3dm.Ransac(local)
+    r.set_refinement(args.refine)
     stream = torch.cuda.ExternalStream(r.stream(), device=dev)
     dc = torch.from_numpy(corrs).to(dev)
     dm = torch.empty((n_pairs, 31), dtype=torch.float64, device=dev)
@@ -1520,7 +1524,7 @@ def run_ransac(args, ws, rank, local):
         "metric": "image pairs/s robust relative orientation (5-point RANSAC, Sampson costs)",
         "value": ws * n_pairs * 1000.0 / ms, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, n_corrs),
+        "dtype": "f64", "data": "synthetic (seeded two-view correspondences)", "config": ransac_config(n_pairs, n_corrs, args.refine),
         "pose_recovered": rot_ok,
         "candidates": n_cand, "sampson_evaluations": n_evals,
         "kernels_ms_per_call": {"k_rs_hyp (five-point solutions)": hyp_ms, "k_rs_score (costs of the candidates)": score_ms,
@@ -1542,7 +1546,7 @@ def run_ransac(args, ws, rank, local):
         from oracle import oracle
         if oracle.ref_ransac_available():
             sel = list(range(0, n_pairs, max(1, n_pairs // 16)))[:16]
-            sec = ref_ransac_pairs(off, corrs, K, sel)
+            sec = ref_ransac_pairs(off, corrs, K, sel, args.refine)
             line["cpu_baseline"] = {"value": len(sel) / sec, "unit": "pairs/s", "cores": 1, "kind": "reference",
                                     "sample": f"{len(sel)} of the {n_pairs} pairs, the reference's solver and pose "
                                               "recovery in the loop restated, the app's own sample sequence "

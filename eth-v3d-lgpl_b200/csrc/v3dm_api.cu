@@ -43,6 +43,8 @@ struct v3dm_matcher {
   uint4* dRecordsA = nullptr;            // pass-A chunk records: nSeg x segCap x kRecordQuads
   int32_t* dPassA = nullptr;             // nSeg record counts, then nMaxL + 1 per-left bounds
   bool passAValid = false;
+  long long testWaitLimit = 0;  // failure-path test hooks of pass A (v3dm_matcher_test_wait_fault)
+  int testSkipLoad = 0;
   int32_t passASmin = 0, passATsec = 0;
   int* dSegCount = nullptr;              // nSeg counts
   long long segCap = 0;
@@ -700,7 +702,11 @@ int enqueue_match_tc(v3dm_matcher* h, float minScore, float minRatio, int32_t* d
       if (e != V3DM_OK) return e;
       V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
     }
+    sa.waitLimit = h->testWaitLimit;
+    sa.skipLoad = h->testSkipLoad;
     V3DM_CUDA_TRY(launch_side(h->tc, h->mapsA, sa, h->stream));
+    sa.waitLimit = 0;
+    sa.skipLoad = 0;
     if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
     h->passAValid = true;
     h->passASmin = Smin;
@@ -926,7 +932,10 @@ int read_info(v3dm_matcher* h) {
   V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->pendingCheck = false;
   int err = h->hInfo[kInfoErr];
-  if (err & kErrWaitTimeout) return V3DM_ERR_TIMEOUT;
+  if (err & kErrWaitTimeout) {
+    h->passAValid = false;  // the pass stopped early: its records are incomplete
+    return V3DM_ERR_TIMEOUT;
+  }
   if (err) return V3DM_ERR_CUDA;
   long long need = h->hInfo[kInfoMaxSeg];
   if (need > h->segCap) {
@@ -1013,6 +1022,17 @@ int v3dm_set_right_f32_device(v3dm_matcher* h, int n, const float* d) {
 }
 int v3dm_set_left_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, true, n, d); }
 int v3dm_set_right_f32_bf16x3(v3dm_matcher* h, int n, const float* d) { return set_features_bf16x3(h, false, n, d); }
+
+int v3dm_matcher_test_wait_fault(v3dm_matcher* h, long long waitCycles, int skipLoad) {
+  if (!h || waitCycles < 0 || skipLoad < 0) return V3DM_ERR_ARG;
+  if (skipLoad > 0 && waitCycles == 0) return V3DM_ERR_ARG;  // a skipped load needs a short wait limit
+  DeviceGuard g(h->device);
+  V3DM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->testWaitLimit = waitCycles;
+  h->testSkipLoad = skipLoad;
+  h->passAValid = false;
+  return V3DM_OK;
+}
 
 int v3dm_float_threshold(float minScore, float minRatio, float* T) {
   if (!T) return V3DM_ERR_ARG;

@@ -106,6 +106,11 @@ struct SideArgs {
   // gathered A (launch_side_gather): A row e of the row table is descriptor aSrcRow[e] of aSrc
   const uint8_t* aSrc;
   const int* aSrcRow;
+  // failure-path test hooks (zero in production): the bounded waits give up after waitLimit
+  // cycles (0: the default), and CTA 0's producer does not issue its skipLoad-th B tile load
+  // (0: none), so that the consumer's bounded wait for it runs out
+  long long waitLimit;
+  int skipLoad;
 };
 // Chunk record: {A index (state), first B column, B count, first B row of the tile's image
 // block} then the chunk's 32 scores.

@@ -256,6 +256,7 @@ template <class C, bool kBatch, bool kGather = false>
 __global__ void __launch_bounds__(kThreads, 1)
 k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int nTiles, SideArgs a) {
   static_assert(!kGather || kBatch, "gathered A blocks only in the batched pass");
+  const long long lim = a.waitLimit > 0 ? a.waitLimit : kWaitCycles;
   pdl_wait();
   pdl_launch_dependents();
   extern __shared__ uint8_t smemRaw[];
@@ -353,7 +354,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         if (mbar_try(bar, par)) return true;
         arrive_all();
         int okl = 1;
-        if (lane == 0) okl = mbar_wait(bar, par, &s.abort, a.err) ? 1 : 0;
+        if (lane == 0) okl = mbar_wait(bar, par, &s.abort, a.err, lim) ? 1 : 0;
         return __shfl_sync(0xffffffffu, okl, 0) != 0;
       };
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
@@ -429,6 +430,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
       uint32_t phase = 0, aPhase = 1;
       uint32_t armedPhase[C::kStages], armedAPhase[C::kASlots];
       bool armed[C::kStages], armedA[C::kASlots];
+      int nIssued = 0;  // B tile loads issued (test hook)
       for (int i = 0; i < C::kStages; ++i) armed[i] = false;
       for (int i = 0; i < C::kASlots; ++i) armedA[i] = false;
       for (Cursor wc = make_cursor(); wc.more(); wc.next()) {
@@ -438,7 +440,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
             aBuf = 0;
             aPhase ^= 1;
           }
-          if (!mbar_wait(&s.emptyA[aBuf], aPhase ^ 1, &s.abort, a.err)) break;
+          if (!mbar_wait(&s.emptyA[aBuf], aPhase ^ 1, &s.abort, a.err, lim)) break;
           mbar_expect_tx(&s.fullA[aBuf], C::kABytes);
           int aRow;
           if constexpr (kBatch) aRow = wc.cur.aRow;
@@ -447,14 +449,18 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           armedA[aBuf] = true;
           armedAPhase[aBuf] = aPhase;
         }
-        if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
-        mbar_expect_tx(&s.fullB[stage], C::kBBytes);
-        int bRow;
-        if constexpr (kBatch) bRow = wc.cur.bRow0 + wc.t * C::BN;
-        else bRow = wc.t * C::BN;
-        tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, bRow);
-        armed[stage] = true;
-        armedPhase[stage] = phase;
+        if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err, lim)) break;
+        if (a.skipLoad > 0 && blockIdx.x == 0 && ++nIssued == a.skipLoad) {
+          armed[stage] = false;  // test hook: this tile never arrives; the MMA's bounded wait gives up
+        } else {
+          mbar_expect_tx(&s.fullB[stage], C::kBBytes);
+          int bRow;
+          if constexpr (kBatch) bRow = wc.cur.bRow0 + wc.t * C::BN;
+          else bRow = wc.t * C::BN;
+          tma_load_2d(s.b[stage], &tmB, &s.fullB[stage], 0, bRow);
+          armed[stage] = true;
+          armedPhase[stage] = phase;
+        }
         if (++stage == C::kStages) {
           stage = 0;
           phase ^= 1;
@@ -489,12 +495,12 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
             aBuf = 0;
             aPhase ^= 1;
           }
-          if (!mbar_wait(&s.fullA[aBuf], aPhase, &s.abort, a.err)) break;
+          if (!mbar_wait(&s.fullA[aBuf], aPhase, &s.abort, a.err, lim)) break;
           aAddr = smem_u32(s.a[aBuf]);
           anyA = true;
         }
-        if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
-        if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) break;
+        if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err, lim)) break;
+        if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err, lim)) break;
         tc_fence_after();
         const uint32_t bAddr = smem_u32(s.b[stage]);
 #pragma unroll
@@ -566,7 +572,7 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         lw = 0;
       }
       const int colBase = wc.t * C::BN + colOff;
-      ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
+      ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err, lim);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
       tc_fence_after();

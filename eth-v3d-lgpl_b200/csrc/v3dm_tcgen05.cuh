@@ -42,13 +42,14 @@ __device__ __forceinline__ bool mbar_try(unsigned long long* b, uint32_t parity)
 
 // Bounded wait for the phase with the given parity.  Returns false on timeout or when
 // another role of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, int* abortFlag, int* err) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, int* abortFlag, int* err,
+                                          long long limit = kWaitCycles) {
   if (mbar_try(b, parity)) return true;
   long long t0 = clock64();
   while (true) {
     if (mbar_try(b, parity)) return true;
     if (*reinterpret_cast<volatile int*>(abortFlag)) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       atomicOr(err, kErrWaitTimeout);
       *reinterpret_cast<volatile int*>(abortFlag) = 1;
       return false;

@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
         L.v3dm_matcher_num_configs.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_matcher_get_config.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
         L.v3dm_matcher_set_config.argtypes = [vp, i32]
+        L.v3dm_matcher_test_wait_fault.argtypes = [vp, C.c_longlong, i32]
         L.v3dm_matcher_autotune.argtypes = [vp, f32, f32, i32, C.POINTER(i32), C.POINTER(C.c_double)]
         L.v3dm_matcher_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i32)]
         L.v3dm_matcher_profile_read_pass.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(i32)]
@@ -376,6 +377,11 @@ class SIFTMatching:
         else:
             _check(lib().v3dm_matcher_profile_read_pass(self._h, pass_id, C.byref(ms), C.byref(n)), "profile_read")
         return ms.value, n.value
+
+    def test_wait_fault(self, wait_cycles: int, skip_load: int) -> None:
+        """Failure-path test hook (v3dm_matcher_test_wait_fault): bounded waits of pass A give up
+        after wait_cycles, and CTA 0 skips its skip_load-th tile load; (0, 0) turns it off."""
+        _check(lib().v3dm_matcher_test_wait_fault(self._h, int(wait_cycles), int(skip_load)), "test_wait_fault")
 
     def last_launches(self) -> int:
         n = C.c_int(0)
@@ -767,8 +773,8 @@ class Loader:
 
     def positions(self) -> np.ndarray:
         p, n = C.c_void_p(), C.c_longlong(0)
-        lib().v3dm_loader_descriptors_device(self._h, C.byref(p), C.byref(n))
-        out = np.empty((n, 2), np.float32)
+        lib().v3dm_loader_descriptors_device(self._h, C.byref(p), C.byref(n))  # the count, whatever the status
+        out = np.empty((n.value, 2), np.float32)
         _check(lib().v3dm_loader_positions(self._h, _ptr(out)), "loader_positions")
         return out
 

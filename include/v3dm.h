@@ -159,6 +159,15 @@ V3DM_API int v3dm_matcher_autotune(v3dm_matcher* h, float minScore, float minRat
                                    double* msBest);
 /* Number of kernels the last matching call launched. */
 V3DM_API int v3dm_matcher_last_launches(v3dm_matcher* h, int* n);
+/* Test of the failure path (no counterpart in the reference, which exits on any CUDA error,
+ * v3d_cudamatching.cu:12-27).  Every device wait of the tcgen05 side pass is bounded; when one
+ * runs out, the CTA raises an abort flag, its roles stop, wait (bounded) for their own copies and
+ * MMAs in flight, free TMEM and return, and the call reports V3DM_ERR_TIMEOUT; the handle stays
+ * usable.  This hook makes that happen on purpose: pass A's bounded waits give up after
+ * waitCycles SM cycles, and with skipLoad = k > 0 the producer of CTA 0 does not issue its k-th B
+ * tile load, so the MMA issuer's wait for that tile runs out.  waitCycles = skipLoad = 0 (the
+ * default) turns it off. */
+V3DM_API int v3dm_matcher_test_wait_fault(v3dm_matcher* h, long long waitCycles, int skipLoad);
 
 /* Candidate threshold of the fused selection: every score S >= T is examined exactly and
  * no score below T can change a decision.  Exposed for tests.  Host-only, no device. */
