@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--tile-config", type=int, default=-1, help="fused-kernel tile configuration (-1: autotune)")
     ap.add_argument("--images", type=int, default=200, help="batch workload: number of images")
     ap.add_argument("--cache-dir", default="", help="voctree workload: keep the generated tree and queries here")
+    ap.add_argument("--float-tree", action="store_true",
+                    help="voctree workload: a float k-means tree of unit-L2 descriptors and float queries (the "
+                         "apps' trees), quantised in the reference CPU tree's sequential FP32 order")
     ap.add_argument("--cells", type=int, default=128, help="proposal workload: cells of the projection")
     ap.add_argument("--probes", type=int, default=4, help="proposal workload: probed cells per left")
     ap.add_argument("--probes-right", type=int, default=4, help="proposal workload: cells each right is listed under")
@@ -721,12 +724,14 @@ def run_voctree(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     bf, depth, n = 10, 6, 2_000_000
-    cache = Path(args.cache_dir) / f"voctree_{args.seed + 2}.npz" if args.cache_dir else None
+    fl = args.float_tree
+    tag = "f32_" if fl else ""
+    cache = Path(args.cache_dir) / f"voctree_{tag}{args.seed + 2}.npz" if args.cache_dir else None
     if cache is not None and cache.exists():
         d = np.load(cache)
         nodes, keys = d["nodes"], d["keys"]
     else:
-        nodes, keys = synth.voctree(args.seed + 2, bf, depth, 500_000, n)
+        nodes, keys = synth.voctree(args.seed + 2, bf, depth, 500_000, n, floats=fl)
         if cache is not None:
             cache.parent.mkdir(parents=True, exist_ok=True)
             np.savez(cache, nodes=nodes, keys=keys)
@@ -737,15 +742,21 @@ def run_voctree(args, ws, rank, local):
     d_keys = torch.from_numpy(keys).to(dev)
     d_ids = torch.empty(n, dtype=torch.int32, device=dev)
 
+    def quantize(tree):
+        if fl:
+            tree.quantize_f32_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+        else:
+            tree.quantize_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+
     def timed(tree, steps):
         s = torch.cuda.ExternalStream(tree.stream(), device=dev)
         for _ in range(max(args.warmup, 3)):
-            tree.quantize_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+            quantize(tree)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         torch.cuda.synchronize()
         for a, c in evs:
             a.record(s)
-            tree.quantize_device(n, d_keys.data_ptr(), d_ids.data_ptr())
+            quantize(tree)
             c.record(s)
         torch.cuda.synchronize()
         return statistics.mean(a.elapsed_time(c) for a, c in evs)
@@ -781,28 +792,36 @@ def run_voctree(args, ws, rank, local):
         c.record(stream)
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(ws, statistics.mean(a.elapsed_time(c) for a, c in ev2), dev)
+    t_replays = t.replays()
     t.close()
     if rank != 0:
         return
     peaks = load_peaks()
-    node_bytes = nodes.shape[0] * 128
-    alg_bytes = n * 128 + n * 4 + node_bytes
+    esz = 4 if fl else 1
+    replays = t_replays if fl else None
+    node_bytes = nodes.shape[0] * 128 * esz
+    alg_bytes = n * 128 * esz + n * 4 + node_bytes
     achieved = alg_bytes / (ms * 1e-3) / 1e9
-    level_bytes = n * bf * 128
+    level_bytes = n * bf * 128 * esz
     line = {
         "metric": "descriptors/s (vocabulary-tree quantization, BF 10, depth 6)", "value": ws * n * 1000.0 / ms,
         "unit": "desc/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fl else "u8",
         "data": "synthetic (seeded generator)",
         "config": {"workload": "voctree BF 10 depth 6 (1,111,110 HKM nodes from 500k descriptors), 2,000,000 "
-                               "uint8 SIFT-like queries", "seed": args.seed + 2,
-                   "l2": "inputs larger than L2 (256 MB of keys, 142 MB of nodes)"},
+                               + ("unit-L2 float queries, float k-means centres (the reference CPU tree's sequential "
+                                  "FP32 order)" if fl else "uint8 SIFT-like queries"), "seed": args.seed + 2,
+                   "l2": "inputs larger than L2 (%d MB of keys, %d MB of nodes)" % (n * 128 * esz // 10**6,
+                                                                                  node_bytes // 10**6)},
+        "sequential_replays": replays,
         "per_level": [{"level": d + 1, "ms": level_ms[d], "gathered_GBps": level_bytes / (level_ms[d] * 1e-3) / 1e9
                        if level_ms[d] > 0 else None} for d in range(depth)],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profiles("k_voctree"),
                      "peak_src": f"{peaks['src']} copy bandwidth",
-                     "bytes_per_launch": alg_bytes, "kernel": "k_voctree (all levels, one launch)"},
+                     "bytes_per_launch": alg_bytes,
+                     "kernel": "k_voctree_f32 (all levels, one launch)" if fl else
+                               "k_vt_top + k_vt_scan + k_vt_scatter + k_vt_sub (bucketed descent, one call)"},
         "e2e": {"value": ws * n * 1000.0 / ms_e2e, "unit": "desc/s", "h2d_bytes_per_step": int(keys.nbytes),
                 "d2h_bytes_per_step": int(n * 4)},
         "gpu_launches": args.steps,
@@ -811,8 +830,8 @@ def run_voctree(args, ws, rank, local):
     if not args.no_cpu_baseline and ws == 1:
         from oracle import oracle
         sample = 200_000
-        kf = keys[:sample].astype(np.float32) / 512
-        nf = nodes.astype(np.float32) / 512
+        kf = keys[:sample].astype(np.float32) if fl else keys[:sample].astype(np.float32) / 512
+        nf = nodes.astype(np.float32) if fl else nodes.astype(np.float32) / 512
         if oracle.ref_voctree_available():
             t0 = time.perf_counter()
             ref = oracle.ref_voctree(bf, depth, nf, kf)

@@ -15,9 +15,13 @@
 //     std::runtime_error when V3DM_COMPAT_THROW is defined before this header.
 // Differences: enableReductionPath() is accepted and has no effect (the reference's reduction
 // kernels read past their shared arrays and race, .cu:87-130, :212-273; the non-reduction
-// semantics are used); descriptors passed as floats must be u/512-valued uint8 descriptors
-// (otherwise the call fails with "float descriptor is not u/512").  The guided calls take the
-// reference's V3D::Matrix3x3d / V3D::Vector2f (any type indexable as F[i][j] and p[k]).
+// semantics are used); float descriptors of the form u/512 are scored exactly on the integer
+// path, any other finite floats (the extractors' unit-L2 descriptors) with a BF16 hi/lo split
+// (score error <= 2e-5 of FP64, then the reference's decision rules; the reference scores them
+// with FP32 cuBLAS); VocabularyTreeTraversal returns the ids of the reference's CPU tree
+// (v3d_voctree.h:82-99: sequential FP32 dot products) for any float tree and features.  The guided
+// calls take the reference's V3D::Matrix3x3d / V3D::Vector2f (any type indexable as F[i][j] and
+// p[k]).
 #ifndef V3D_CUDA_MATCHING_H
 #define V3D_CUDA_MATCHING_H
 

@@ -52,23 +52,31 @@ constexpr int kEpiWarps = 16;    // four per TMEM lane quadrant
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr int kTmemCols = 512;
 
-template <int NB_, int BN_, int STAGES_, int ASLOTS_ = 2>
+template <int NB_, int BN_, int STAGES_, int ASLOTS_ = 2, int SPLIT_ = 1, int PIPE_ = 0>
 struct TcCfg {
   static constexpr int NB = NB_;                 // 128-row MMA blocks per left group
   static constexpr int BN = BN_;                 // rights per tile
   static constexpr int kStages = STAGES_;        // right-tile ring depth
   static constexpr int kASlots = ASLOTS_;        // left-group buffers (more: short rows prefetch further)
+  // kSplit = 2: each tile is scored as two BN/2-column MMAs into two accumulator stages, so the MMA
+  // can run further ahead of the epilogue (twice the stages of half the width)
+  static constexpr int kSplit = SPLIT_;
+  // kPipe = 1: the epilogue loads its second chunk while it filters the first
+  static constexpr int kPipe = PIPE_;
   static constexpr int GM = BM * NB;             // left rows per group
   static constexpr int kABytes = GM * kDescBytes;
   static constexpr int kBBytes = BN * kDescBytes;
-  static constexpr int kAccCols = NB * BN;       // TMEM columns per accumulator stage
+  static constexpr int kMmaN = BN / kSplit;      // columns of one MMA / accumulator block
+  static constexpr int kAccCols = NB * kMmaN;    // TMEM columns per accumulator stage
   static constexpr int kAcc = kTmemCols / kAccCols;  // accumulator stages
-  // Epilogue split: the four warps of a lane quadrant own (block, column quarter or half):
-  // with NB == 2 a warp owns one block and half of the BN columns, with NB == 1 a quarter.
-  static constexpr int kWarpCols = NB == 2 ? BN / 2 : BN / 4;
+  // Epilogue split: the four warps of a lane quadrant own (block, column quarter or half) of a
+  // stage: with NB == 2 a warp owns one block and half of the columns, with NB == 1 a quarter.
+  static constexpr int kWarpCols = NB == 2 ? kMmaN / 2 : kMmaN / 4;
   static constexpr int kChunks = kWarpCols / 32;
   static_assert(NB == 1 || NB == 2, "one or two blocks per group");
+  static_assert(kSplit == 1 || (kSplit == 2 && NB == 1), "split tiles with one block per group");
   static_assert(kWarpCols >= 32 && kWarpCols % 32 == 0 && kChunks <= 2 && BN <= 256, "1..2 chunks per warp");
+  static_assert(kPipe == 0 || kChunks == 2, "pipelined loads need two chunks");
   static_assert(kAcc >= 2, "at least two accumulator stages");
 };
 
@@ -499,27 +507,37 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           aAddr = smem_u32(s.a[aBuf]);
           anyA = true;
         }
-        if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err, lim)) break;
         if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err, lim)) break;
-        tc_fence_after();
         const uint32_t bAddr = smem_u32(s.b[stage]);
+        bool stop = false;
 #pragma unroll
-        for (int blk = 0; blk < C::NB; ++blk) {
-          const uint32_t d = tmem + (uint32_t)(acc * C::kAccCols + blk * C::BN);
-          const uint32_t ab = aAddr + (uint32_t)(blk * BM * kDescBytes);
+        for (int h = 0; h < C::kSplit; ++h) {
+          if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err, lim)) {
+            stop = true;
+            break;
+          }
+          tc_fence_after();
+          // columns h * kMmaN .. of the tile: B rows 128 bytes each, 1024-byte aligned halves
+          const uint32_t bh = bAddr + (uint32_t)(h * C::kMmaN * kDescBytes);
 #pragma unroll
-          for (int k = 0; k < kDescBytes / 32; ++k)
-            mma_i8<C::BN>(d, sdesc(ab + 32u * k), sdesc(bAddr + 32u * k), k > 0 ? 1u : 0u);
+          for (int blk = 0; blk < C::NB; ++blk) {
+            const uint32_t d = tmem + (uint32_t)(acc * C::kAccCols + blk * C::kMmaN);
+            const uint32_t ab = aAddr + (uint32_t)(blk * BM * kDescBytes);
+#pragma unroll
+            for (int k = 0; k < kDescBytes / 32; ++k)
+              mma_i8<C::kMmaN>(d, sdesc(ab + 32u * k), sdesc(bh + 32u * k), k > 0 ? 1u : 0u);
+          }
+          mma_commit(&s.accFull[acc]);
+          if (++acc == C::kAcc) {
+            acc = 0;
+            accPhase ^= 1;
+          }
         }
+        if (stop) break;
         mma_commit(&s.emptyB[stage]);
-        mma_commit(&s.accFull[acc]);
         if (++stage == C::kStages) {
           stage = 0;
           phase ^= 1;
-        }
-        if (++acc == C::kAcc) {
-          acc = 0;
-          accPhase ^= 1;
         }
       }
       if (anyA) mma_commit(&s.emptyA[aBuf]);
@@ -571,27 +589,43 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         }
         lw = 0;
       }
-      const int colBase = wc.t * C::BN + colOff;
+      for (int h = 0; h < C::kSplit; ++h) {
+      const int colBase = wc.t * C::BN + h * C::kMmaN + colOff;
       ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err, lim);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
       tc_fence_after();
       const uint32_t tbase =
-          tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * C::kAccCols + blk * C::BN + colOff);
+          tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * C::kAccCols + blk * C::kMmaN + colOff);
       // All of this warp's scores into registers, then hand the stage back at once so the
-      // MMA never waits for the filtering below.
+      // MMA never waits for the filtering below (kPipe: the second chunk is loaded while the
+      // first is filtered, and the stage handed back after it).
       uint32_t v[C::kChunks][32];
+      if constexpr (C::kPipe) {
+        tmem_ld32(tbase, v[0]);
+        tmem_wait(v[0]);
+        tmem_ld32(tbase + 32u, v[1]);
+      } else {
 #pragma unroll
-      for (int c = 0; c < C::kChunks; ++c) tmem_ld32(tbase + (uint32_t)(c * 32), v[c]);
+        for (int c = 0; c < C::kChunks; ++c) tmem_ld32(tbase + (uint32_t)(c * 32), v[c]);
 #pragma unroll
-      for (int c = 0; c < C::kChunks; ++c) tmem_wait(v[c]);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+        for (int c = 0; c < C::kChunks; ++c) tmem_wait(v[c]);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+      }
 #pragma unroll
       for (int c = 0; c < C::kChunks; ++c) {
+        if constexpr (C::kPipe) {
+          if (c == 1) {
+            tmem_wait(v[1]);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+          }
+        }
         const int col0 = colBase + 32 * c;
-        if (col0 >= nB) break;  // chunks past the last B descriptor (warp-uniform)
+        if (col0 >= nB) continue;  // chunks past the last B descriptor (warp-uniform)
         if (col0 + 32 > nB) {
           // The chunk holding the last B descriptor: the columns past it hold zero fill, zero
           // padding or the next block's descriptors; a 0 there is <= every real score, so the
@@ -623,6 +657,8 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
         acc = 0;
         accPhase ^= 1;
       }
+      }
+      if (!ok) break;
     }
     if (started && ok) flush();
     if (lane == 0) a.segCount[blockIdx.x * kEpiWarps + e] = segN;
@@ -672,6 +708,9 @@ using Cfg3 = TcCfg<2, 64, 16>;   // 256 x 64 tiles, 4 accumulator stages
 using Cfg4 = TcCfg<1, 256, 6>;   // 128 x 256 tiles, 2 accumulator stages, 6-deep ring
 using Cfg5 = TcCfg<1, 256, 4, 4>;   // as Cfg0 with 4 left-group buffers (rows of few tiles)
 using Cfg6 = TcCfg<1, 128, 6, 6>;   // 128 x 128 tiles, 6 left-group buffers
+using Cfg7 = TcCfg<1, 256, 4, 4, 2>;      // as Cfg5, each tile as two 128-column MMAs (4 accumulator stages)
+using Cfg8 = TcCfg<1, 256, 6, 2, 2>;      // as Cfg4, split the same way
+using Cfg9 = TcCfg<1, 256, 4, 4, 1, 1>;   // as Cfg5 with the epilogue's second chunk loaded while the first is filtered
 
 template <class C, bool kBatch, bool kGather = false>
 cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles, const SideArgs& a, int grid,
@@ -686,9 +725,11 @@ cudaError_t launch_cfg(const CUtensorMap& mA, const CUtensorMap& mB, int nTiles,
   return launch_pdl(k_side<C, kBatch, kGather>, dim3(grid), dim3(kThreads), smem, st, mA, mB, nTiles, a);
 }
 
-constexpr int kNumCfg = 7;
-constexpr int kCfgNB[kNumCfg] = {Cfg0::NB, Cfg1::NB, Cfg2::NB, Cfg3::NB, Cfg4::NB, Cfg5::NB, Cfg6::NB};
-constexpr int kCfgBN[kNumCfg] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN};
+constexpr int kNumCfg = 10;
+constexpr int kCfgNB[kNumCfg] = {Cfg0::NB, Cfg1::NB, Cfg2::NB, Cfg3::NB, Cfg4::NB,
+                                 Cfg5::NB, Cfg6::NB, Cfg7::NB, Cfg8::NB, Cfg9::NB};
+constexpr int kCfgBN[kNumCfg] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN,
+                                 Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN};
 constexpr int kDefaultCfg = 0;
 
 }  // namespace
@@ -759,7 +800,10 @@ cudaError_t launch_side(TcPlan* p, const TcMaps& m, const SideArgs& a, cudaStrea
     case 3: return launch_cfg<Cfg3, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[3]);
     case 4: return launch_cfg<Cfg4, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[4]);
     case 5: return launch_cfg<Cfg5, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[5]);
-    default: return launch_cfg<Cfg6, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[6]);
+    case 6: return launch_cfg<Cfg6, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[6]);
+    case 7: return launch_cfg<Cfg7, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[7]);
+    case 8: return launch_cfg<Cfg8, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[8]);
+    default: return launch_cfg<Cfg9, false>(m.a, m.b, nTiles, a, grid, st, p->attrSet[9]);
   }
 }
 
@@ -781,6 +825,9 @@ cudaError_t tc_prepare_batch(TcPlan* p, int cfg) {
     case 4: return set_batch_attr<Cfg4>(p->attrSetBatch[4]);
     case 5: return set_batch_attr<Cfg5>(p->attrSetBatch[5]);
     case 6: return set_batch_attr<Cfg6>(p->attrSetBatch[6]);
+    case 7: return set_batch_attr<Cfg7>(p->attrSetBatch[7]);
+    case 8: return set_batch_attr<Cfg8>(p->attrSetBatch[8]);
+    case 9: return set_batch_attr<Cfg9>(p->attrSetBatch[9]);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -801,7 +848,10 @@ cudaError_t launch_side_batch(TcPlan* p, const TcMaps& m, const SideArgs& a, cud
     case 3: return launch_cfg<Cfg3, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[3]);
     case 4: return launch_cfg<Cfg4, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[4]);
     case 5: return launch_cfg<Cfg5, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[5]);
-    default: return launch_cfg<Cfg6, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[6]);
+    case 6: return launch_cfg<Cfg6, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[6]);
+    case 7: return launch_cfg<Cfg7, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[7]);
+    case 8: return launch_cfg<Cfg8, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[8]);
+    default: return launch_cfg<Cfg9, true>(m.a, m.b, 0, a, grid, st, p->attrSetBatch[9]);
   }
 }
 

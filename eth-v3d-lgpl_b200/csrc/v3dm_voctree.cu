@@ -122,6 +122,7 @@ constexpr int kVtRowsMax = 1600;        // rows of a staged subtree / top (200 K
 constexpr int kVtBktThreads = 512;
 constexpr int kVtItemKeys = 2048;       // keys per work item of k_vt_sub
 constexpr int kVtMaxSubLevels = 10;     // levels of a staged subtree
+constexpr int kVtLocalBins = 4096;      // bucket counts kept in shared memory by k_vt_top / k_vt_scatter
 
 // 16-byte chunk c of staged row r lives at r * 128 + ((c ^ (r & 7)) << 4): rows read by the
 // lanes of one instruction spread over the banks.
@@ -136,31 +137,46 @@ __device__ __forceinline__ void vt_stage(uint8_t* smem, const uint8_t* __restric
 }
 
 // Best child of the bf rows starting at staged row `row0` for the key slice kw (four threads
-// per key, thread `part` holding chunks 2 part, 2 part + 1).
+// per key, thread `part` holding chunks 2 part, 2 part + 1).  Children are scored kVtGroup at a
+// time with independent accumulators and shuffles (instruction-level parallelism: a CTA that
+// stages a whole subtree runs only 16 warps per SM); the comparisons keep index order.
+constexpr int kVtGroup = 5;
 __device__ __forceinline__ int vt_best_staged(const uint8_t* smem, int row0, int bf, const uint4 (&kw)[kQ], int part,
                                               bool valid) {
   int best = 0, bestScore = -1;
-#pragma unroll 2
-  for (int c = 0; c < bf; ++c) {
-    const int r = row0 + c;
-    uint32_t acc = 0;
-    if (valid) {
+  for (int c0 = 0; c0 < bf; c0 += kVtGroup) {
+    uint32_t acc[kVtGroup];
+    uint4 w[kVtGroup][kQ];
 #pragma unroll
-      for (int q = 0; q < kQ; ++q) {
-        const uint4 w = *reinterpret_cast<const uint4*>(smem + vt_swz(r, part * kQ + q));
-        acc = __dp4a(kw[q].x, w.x, acc);
-        acc = __dp4a(kw[q].y, w.y, acc);
-        acc = __dp4a(kw[q].z, w.z, acc);
-        acc = __dp4a(kw[q].w, w.w, acc);
+    for (int g = 0; g < kVtGroup; ++g) {
+      const int r = row0 + min(c0 + g, bf - 1);  // past the last child: re-read it, the score is ignored
+#pragma unroll
+      for (int q = 0; q < kQ; ++q) w[g][q] = *reinterpret_cast<const uint4*>(smem + vt_swz(r, part * kQ + q));
+    }
+#pragma unroll
+    for (int g = 0; g < kVtGroup; ++g) {
+      uint32_t a0 = 0, a1 = 0;
+      if (valid) {
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) {
+          a0 = __dp4a(kw[q].x, w[g][q].x, a0);
+          a1 = __dp4a(kw[q].y, w[g][q].y, a1);
+          a0 = __dp4a(kw[q].z, w[g][q].z, a0);
+          a1 = __dp4a(kw[q].w, w[g][q].w, a1);
+        }
       }
+      acc[g] = a0 + a1;
     }
-    int sc = (int)acc;
 #pragma unroll
-    for (int o = 1; o < kTpk; o <<= 1) sc += __shfl_xor_sync(0xffffffffu, sc, o);
-    if (sc > bestScore) {
-      bestScore = sc;
-      best = c;
-    }
+    for (int o = 1; o < kTpk; o <<= 1)
+#pragma unroll
+      for (int g = 0; g < kVtGroup; ++g) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], o);
+#pragma unroll
+    for (int g = 0; g < kVtGroup; ++g)
+      if (c0 + g < bf && (int)acc[g] > bestScore) {  // strict '>': the first child wins ties (.cu:781)
+        bestScore = (int)acc[g];
+        best = c0 + g;
+      }
   }
   return best;
 }
@@ -178,12 +194,16 @@ __device__ __forceinline__ void vt_load_key(const uint8_t* __restrict__ keys, in
 template <bool kStaged>
 __global__ void __launch_bounds__(kVtBktThreads)
 k_vt_top(const uint8_t* __restrict__ nodes, int bf, int L, long long topRows, long long levelStartL,
-         const uint8_t* __restrict__ keys, int n, int32_t* __restrict__ bucket, int* __restrict__ hist) {
+         const uint8_t* __restrict__ keys, int n, int32_t* __restrict__ bucket, int* __restrict__ hist, int bins) {
   extern __shared__ __align__(128) uint8_t vsm[];
-  if constexpr (kStaged) {
-    vt_stage(vsm, nodes, topRows, 0);
-    __syncthreads();
-  }
+  // the bucket histogram is counted in shared memory (after the staged rows) and added to the
+  // global one once per CTA when it fits, else directly in global memory
+  int* shHist = reinterpret_cast<int*>(vsm + (kStaged ? topRows * kDescBytes : 0));
+  const bool local = bins <= kVtLocalBins;
+  if (local)
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) shHist[b] = 0;
+  if constexpr (kStaged) vt_stage(vsm, nodes, topRows, 0);
+  __syncthreads();
   const int part = threadIdx.x % kTpk;
   const int perIter = (gridDim.x * kVtBktThreads) / kTpk;
   for (int k0 = (blockIdx.x * kVtBktThreads + threadIdx.x) / kTpk; k0 - (int)(threadIdx.x / kTpk) < n; k0 += perIter) {
@@ -226,8 +246,13 @@ k_vt_top(const uint8_t* __restrict__ nodes, int bf, int L, long long topRows, lo
     if (valid && part == 0) {
       const int b = (int)(leafId - levelStartL);
       bucket[k0] = b;
-      atomicAdd(&hist[b], 1);
+      atomicAdd(local ? &shHist[b] : &hist[b], 1);
     }
+  }
+  if (local) {
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += blockDim.x)
+      if (shHist[b]) atomicAdd(&hist[b], shHist[b]);
   }
 }
 
@@ -271,12 +296,36 @@ k_vt_scan(const int* __restrict__ hist, int bins, int single, int* __restrict__ 
   }
 }
 
-// Keys in bucket order.
-__global__ void k_vt_scatter(const int32_t* __restrict__ bucket, int n, const int* __restrict__ off,
-                             int* __restrict__ cursor, int32_t* __restrict__ perm) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+// Keys in bucket order.  Each CTA takes a contiguous range of keys, counts them per bucket in
+// shared memory, reserves its slots of every bucket with one global atomic per bucket, and
+// places its keys with shared-memory ranks (the order within a bucket does not matter).
+constexpr int kVtScatterThreads = 1024;
+__global__ void __launch_bounds__(kVtScatterThreads)
+k_vt_scatter(const int32_t* __restrict__ bucket, int n, const int* __restrict__ off, int* __restrict__ cursor,
+             int32_t* __restrict__ perm, int bins) {
+  __shared__ int cnt[kVtLocalBins];
+  __shared__ int base[kVtLocalBins];
+  const long long per = ((long long)n + gridDim.x - 1) / gridDim.x;
+  const int k0 = (int)min((long long)n, per * blockIdx.x), k1 = (int)min((long long)n, per * (blockIdx.x + 1));
+  if (bins > kVtLocalBins) {  // too many buckets for shared memory: one global atomic per key
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+      const int b = bucket[k];
+      perm[off[b] + atomicAdd(&cursor[b], 1)] = k;
+    }
+    return;
+  }
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) cnt[b] = 0;
+  __syncthreads();
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) atomicAdd(&cnt[bucket[k]], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    base[b] = cnt[b] ? off[b] + atomicAdd(&cursor[b], cnt[b]) : 0;
+    cnt[b] = 0;
+  }
+  __syncthreads();
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     const int b = bucket[k];
-    perm[off[b] + atomicAdd(&cursor[b], 1)] = k;
+    perm[base[b] + atomicAdd(&cnt[b], 1)] = k;
   }
 }
 
@@ -565,22 +614,25 @@ int vt_launch(v3dm_voctree* t, int n, const uint8_t* dKeys, int32_t* dIds, int i
     if (cudaMemsetAsync(t->dHist, 0, 2 * (size_t)bins * sizeof(int), t->stream) != cudaSuccess) return V3DM_ERR_CUDA;
     const long long keyBlocks = ((long long)n * kTpk + kVtBktThreads - 1) / kVtBktThreads;
     const unsigned topGrid = (unsigned)std::min<long long>(keyBlocks, (long long)t->numSMs * 2);
+    const size_t histBytes = bins <= kVtLocalBins ? (size_t)bins * sizeof(int) : 0;
     if (t->topRows <= kVtRowsMax) {
-      const size_t smem = (size_t)t->topRows * kDescBytes;
+      const size_t smem = (size_t)t->topRows * kDescBytes + histBytes;
       k_vt_top<true><<<topGrid, kVtBktThreads, smem, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
-                                                                 t->levelStartL, dKeys, n, t->dBucket, t->dHist);
+                                                                 t->levelStartL, dKeys, n, t->dBucket, t->dHist,
+                                                                 bins);
     } else {
-      k_vt_top<false><<<(unsigned)keyBlocks, kVtBktThreads, 0, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
-                                                                          t->levelStartL, dKeys, n, t->dBucket,
-                                                                          t->dHist);
+      k_vt_top<false><<<topGrid, kVtBktThreads, histBytes, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
+                                                                       t->levelStartL, dKeys, n, t->dBucket,
+                                                                       t->dHist, bins);
     }
     if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
   }
   k_vt_scan<<<1, 1024, 0, t->stream>>>(t->dHist, bins, t->L > 0 ? 0 : n, t->dOff, t->dItems, t->dNItems);
   if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
   if (t->L > 0) {
-    k_vt_scatter<<<(unsigned)std::min<long long>(((long long)n + 255) / 256, (long long)t->numSMs * 8), 256, 0,
-                   t->stream>>>(t->dBucket, n, t->dOff, t->dHist + bins, t->dPerm);
+    k_vt_scatter<<<(unsigned)std::max<long long>(1, std::min<long long>(((long long)n + 4095) / 4096,
+                                                                         (long long)t->numSMs * 2)),
+                   kVtScatterThreads, 0, t->stream>>>(t->dBucket, n, t->dOff, t->dHist + bins, t->dPerm, bins);
     if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
   }
   const size_t smem = (size_t)t->subRows * kDescBytes;
@@ -702,7 +754,7 @@ int v3dm_voctree_create(v3dm_voctree** out, int device, int bf, int depth) {
                     cudaMalloc(reinterpret_cast<void**>(&t->dOff), ((size_t)t->bins + 1) * sizeof(int)) != cudaSuccess ||
                     cudaMalloc(reinterpret_cast<void**>(&t->dNItems), sizeof(int)) != cudaSuccess ||
                     cudaFuncSetAttribute(k_vt_top<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kVtRowsMax * kDescBytes) != cudaSuccess ||
+                                         kVtRowsMax * kDescBytes + kVtLocalBins * (int)sizeof(int)) != cudaSuccess ||
                     cudaFuncSetAttribute(k_vt_sub, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kVtRowsMax * kDescBytes) != cudaSuccess)) ||
       cudaStreamSynchronize(t->stream) != cudaSuccess) {
