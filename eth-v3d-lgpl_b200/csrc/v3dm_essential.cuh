@@ -643,6 +643,54 @@ V3DM_HD double pose_residual(const double* M, double px, double py, double qx, d
   return num / denom;
 }
 
+// sin and cos of |x| <= 1, correctly rounded (but for inputs whose exact value lies within
+// about 2^-100 relative of a rounding boundary): Taylor series evaluated in double-double
+// arithmetic (Dekker's exact product and Knuth's exact sum; Hida, Li and Bailey, "Library for
+// double-double and quad-double arithmetic", 2001), then rounded once.  The device path of
+// pose_update uses them so that the rotation update rounds as the host's C library does; the
+// host path calls std::sin / std::cos.
+struct DD {
+  double hi, lo;
+};
+V3DM_HD DD dd_two_sum(double a, double b) {
+  const double s = a + b, bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+V3DM_HD DD dd_add(DD x, DD y) {
+  DD s = dd_two_sum(x.hi, y.hi);
+  const double lo = s.lo + x.lo + y.lo;
+  return dd_two_sum(s.hi, lo);
+}
+V3DM_HD DD dd_mul(DD x, DD y) {
+  const double p = x.hi * y.hi;
+  const double e = fma(x.hi, y.hi, -p);
+  return dd_two_sum(p, e + (x.hi * y.lo + x.lo * y.hi));
+}
+V3DM_HD DD dd_div_int(DD x, double n) {  // x / n for an integer n below 2^53
+  const double q1 = x.hi / n;
+  const double p = q1 * n, pe = fma(q1, n, -p);  // q1 * n exactly
+  const double r = ((x.hi - p) - pe) + x.lo;
+  return dd_two_sum(q1, r / n);
+}
+V3DM_HD void sincos_dd(double x, double* sn, double* cs) {
+  const DD x2 = dd_mul({x, 0.0}, {x, 0.0});
+  DD ts = {x, 0.0}, s = ts;      // x^(2k+1) / (2k+1)!
+  DD tc = {1.0, 0.0}, c = tc;    // x^(2k) / (2k)!
+  for (int k = 1; k <= 16; ++k) {
+    tc = dd_div_int(dd_mul(tc, x2), (double)((2 * k - 1) * (2 * k)));
+    ts = dd_div_int(dd_mul(ts, x2), (double)((2 * k) * (2 * k + 1)));
+    if (k & 1) {
+      c = dd_add(c, {-tc.hi, -tc.lo});
+      s = dd_add(s, {-ts.hi, -ts.lo});
+    } else {
+      c = dd_add(c, tc);
+      s = dd_add(s, ts);
+    }
+  }
+  *sn = s.hi + s.lo;
+  *cs = c.hi + c.lo;
+}
+
 V3DM_HD void pose_update(const double* Rold, const double* Told, const double* delta, double* R, double* T) {
   // createRotationMatrixRodrigues(omega) (v3d_mathutilities.h:170-190), then R = Rold dR
   const double w0 = delta[0], w1 = delta[1], w2 = delta[2];
@@ -657,8 +705,19 @@ V3DM_HD void pose_update(const double* Rold, const double* Told, const double* d
         for (int k = 0; k < 3; ++k) v += J[3 * i + k] * J[3 * k + j];
         J2[3 * i + j] = v;
       }
-    const double c1 = sin(theta) / theta;
-    const double c2 = (1 - cos(theta)) / (theta * theta);
+#ifdef __CUDA_ARCH__
+    double sn, cs;
+    if (theta <= 1.0) {
+      sincos_dd(theta, &sn, &cs);
+    } else {
+      sn = sin(theta);
+      cs = cos(theta);
+    }
+#else
+    const double sn = std::sin(theta), cs = std::cos(theta);
+#endif
+    const double c1 = sn / theta;
+    const double c2 = (1 - cs) / (theta * theta);
     for (int k = 0; k < 9; ++k) dR[k] += c1 * J[k] + c2 * J2[k];
   }
   for (int i = 0; i < 3; ++i)

@@ -38,16 +38,14 @@
 
 #include "v3dm_essential.cuh"
 #include "v3dm_internal.h"
+#include "v3dm_ransac.cuh"
 
 using namespace v3dm;
 
 namespace {
 
-constexpr int kRsMaxSol = 10;        // solutions per sample
-constexpr int kRsSlotDoubles = 18;   // E, F
 constexpr int kRsScoreThreads = 128;
 constexpr int kRsStage = 1024;       // correspondences staged at a time in k_rs_score
-constexpr int kRsRound = 128;        // samples per pair per round
 
 struct RsDeviceGuard {
   int prev = -1;
@@ -125,15 +123,6 @@ __global__ void k_rs_draw(const int32_t* __restrict__ offsets, int nPairs, int n
   }
   for (int k = got; k < 5; ++k) s[k] = (s[k - 1] + 1) % n;  // unreachable in practice (n >= 5)
 }
-
-// The loop's state per pair, carried from round to round.
-struct RsState {
-  double minError;  // best cost so far (1e30: none)
-  int budget;       // nSamples, lowered by each accepted candidate
-  int drawn;        // samples consumed
-  int chosen;       // sample of the accepted candidate, -1: none
-  int done;         // the loop has ended for this pair
-};
 
 __global__ void k_rs_init(const int32_t* __restrict__ offsets, int nPairs, int nSamples, RsState* __restrict__ st) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -286,169 +275,16 @@ k_rs_score(const int32_t* __restrict__ offsets, const float4* __restrict__ corrs
   }
 }
 
-// ransacNSamples(5, outlierRatio, 1 - 1e-9) (reconstruction_common.h:627-635).
-__device__ __forceinline__ int rs_budget(double outlierRatio) {
-  const double maxN = 1e8;
-  if (outlierRatio >= 1.0) return (int)maxN;
-  double N = log(1.0 - (1.0 - 10e-10)) / log(1.0 - pow(1.0 - outlierRatio, 5));
-  N = fmax(0.0, fmin(maxN, N));
-  return (int)N;
-}
-
-// Warp-wide sum: every lane gets the same bits (xor butterfly; double addition commutes).
-__device__ __forceinline__ double rs_wsum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// F = (invK2^T E) invK1, the reference's product order (reconstruction_common.cpp:271).
-__device__ void rs_fund(const double* invK1, const double* invK2t, const double* E, double* F) {
-  double tmp[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double v = 0.0;
-      for (int k = 0; k < 3; ++k) v += invK2t[3 * i + k] * E[3 * k + j];
-      tmp[3 * i + j] = v;
-    }
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double v = 0.0;
-      for (int k = 0; k < 3; ++k) v += tmp[3 * i + k] * invK1[3 * k + j];
-      F[3 * i + j] = v;
-    }
-}
-
-// One pass of the refinement over the inliers of F0 (Sampson distance below thr2, the set the
-// reference hands to refineRelativePose): RelativePoseMinimizer's weights at pose (Rw, Tw), the
-// weighted residuals at (R, T) and, with derivs, the normal equations (ess::pose_weighted_residual
-// and ess::pose_normal_equations per correspondence).  Returns |e|^2; every lane gets the sums.
-__device__ double rs_lm_pass(const float4* __restrict__ px, const double4* __restrict__ nm, int n, const double* F0,
-                             double thr2, const double* invK1, const double* invK2t, double thr, const double* Rw,
-                             const double* Tw, const double* R, const double* T, bool derivs, double* JtJ,
-                             double* Jte) {
-  double Ew[9], Fw[9], E[9], inner[9][6], a[3], b[2];
-  ess::pose_essential(Rw, Tw, Ew);
-  rs_fund(invK1, invK2t, Ew, Fw);
-  ess::pose_essential(R, T, E);
-  if (derivs) ess::pose_inner(E, R, inner);
-  double err = 0.0, jtj[21], jte[6];
-  for (int k = 0; k < 21; ++k) jtj[k] = 0.0;
-  for (int k = 0; k < 6; ++k) jte[k] = 0.0;
-  for (int k = threadIdx.x & 31; k < n; k += 32) {
-    const float4 c = px[k];
-    if (!(ess::sampson(F0, c.x, c.y, c.z, c.w) < thr2)) continue;
-    const double4 q = nm[k];
-    const double ew = ess::pose_residual(Fw, c.x, c.y, c.z, c.w, a, b);
-    const double w = (fabs(ew) < thr) ? 1.0 : sqrt(thr / fabs(ew));
-    const double ek = w * (0.0 - ess::pose_residual(E, q.x, q.y, q.z, q.w, a, b));
-    err += ek * ek;
-    if (derivs) {
-      double J[6];
-      ess::pose_jacobian_row(E, inner, q.x, q.y, q.z, q.w, J);
-      int t = 0;
-      for (int i = 0; i < 6; ++i) {
-        for (int j = i; j < 6; ++j) jtj[t++] += J[i] * J[j];
-        jte[i] += J[i] * ek;
-      }
-    }
-  }
-  if (derivs) {
-    int t = 0;
-    for (int i = 0; i < 6; ++i) {
-      for (int j = i; j < 6; ++j) {
-        const double v = rs_wsum(jtj[t++]);
-        JtJ[6 * i + j] = v;
-        JtJ[6 * j + i] = v;
-      }
-      Jte[i] = rs_wsum(jte[i]);
-    }
-  }
-  return rs_wsum(err);
-}
-
-// refineRelativePose on the inliers of F0: the Levenberg-Marquardt loop of ess::refine_pose
-// (SimpleLevenbergOptimizer's damping schedule and stopping rules), warp-uniform.
-__device__ void rs_refine_warp(const float4* __restrict__ px, const double4* __restrict__ nm, int n, const double* F0,
-                               double thr2, const double* invK1, const double* invK2t, double thr, double* R,
-                               double* T) {
-  double lambda = 1e-3, JtJ[36], Jte[6], N[36], delta[6], Rs[9], Ts[3];
-  bool computeDerivatives = true;
-  for (int it = 0; it < 50; ++it) {
-    const double err = rs_lm_pass(px, nm, n, F0, thr2, invK1, invK2t, thr, R, T, R, T, computeDerivatives, JtJ, Jte);
-    double gmax = 0.0;
-    for (int k = 0; k < 6; ++k) gmax = fmax(gmax, fabs(Jte[k]));
-    if (gmax < 1e-8) return;
-    if (it == 0) {
-      double maxEl = -1e30;
-      for (int k = 0; k < 6; ++k) maxEl = fmax(maxEl, JtJ[7 * k]);
-      lambda = 1e-3 * maxEl;
-    }
-    for (int k = 0; k < 36; ++k) N[k] = JtJ[k];
-    for (int k = 0; k < 6; ++k) N[7 * k] += lambda;
-    if (!ess::cholesky_solve6(N, Jte, delta)) return;
-    double dl = 0.0;
-    for (int k = 0; k < 6; ++k) dl += delta[k] * delta[k];
-    dl = sqrt(dl);
-    if (it >= 10 && dl < 1e-8 * (4.0 + 1e-8)) return;
-    for (int k = 0; k < 9; ++k) Rs[k] = R[k];
-    for (int k = 0; k < 3; ++k) Ts[k] = T[k];
-    ess::pose_update(Rs, Ts, delta, R, T);
-    const double errNew = rs_lm_pass(px, nm, n, F0, thr2, invK1, invK2t, thr, Rs, Ts, R, T, false, nullptr, nullptr);
-    double rho = err - errNew;
-    double d1 = 0.0, d2 = 0.0;
-    for (int k = 0; k < 6; ++k) {
-      d1 += delta[k] * delta[k];
-      d2 += delta[k] * Jte[k];
-    }
-    rho = rho / (lambda * d1 + d2);
-    if (rho > 0) {
-      lambda = fmax(1e-10, lambda * 0.1);
-      computeDerivatives = true;
-    } else {
-      for (int k = 0; k < 9; ++k) R[k] = Rs[k];
-      for (int k = 0; k < 3; ++k) T[k] = Ts[k];
-      lambda *= 10.0;
-      computeDerivatives = false;
-    }
-  }
-}
-
-// sum_i min(d_i, thr2) over all correspondences in index order (the loop's sum, as k_rs_score
-// forms it) and the count of d_i < thr2; every lane gets both.
-__device__ void rs_cost_in_order(const float4* __restrict__ px, int n, const double* F, double thr2, double* cost,
-                                 int* nIn) {
-  const int lane = threadIdx.x & 31;
-  double sum = 0.0;
-  int cnt = 0;
-  for (int k0 = 0; k0 < n; k0 += 32) {
-    double t = 0.0;
-    bool in = false;
-    if (k0 + lane < n) {
-      const float4 c = px[k0 + lane];
-      t = ess::sampson_truncated(F, (double)c.x, (double)c.y, (double)c.z, (double)c.w, thr2, in);
-    }
-    cnt += __popc(__ballot_sync(0xffffffffu, in));
-    const int m = min(32, n - k0);
-    for (int l = 0; l < m; ++l) sum = ess::dadd(sum, __shfl_sync(0xffffffffu, t, l));
-  }
-  *cost = sum;
-  *nIn = cnt;
-}
-
 // One warp per pair: the round's costs, pose flags and inlier counts staged in shared memory by
-// the warp (coalesced), then the loop over the round's samples in order (the rule of
-// reconstruction_common.cpp:177-335).  Without refinement lane 0 walks it and the warp copies the
-// last accepted candidate's E and F; with refinement every lane walks it (the same decisions) and
-// the warp refines each accepted pose, keeping the refined E, F, R and T.
-template <bool kRefine>
+// the warp (coalesced), then lane 0 walks the loop over the round's samples in order (the rule of
+// reconstruction_common.cpp:177-335 without refinement); the last accepted candidate's E and F are
+// kept (the warp copies them).  With refinement the selection is k_rs_select_refine
+// (v3dm_ransac_refine.cu).
 __global__ void __launch_bounds__(32)
 k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, int len,
             const int8_t* __restrict__ counts, const uint8_t* __restrict__ slotOk, const double* __restrict__ cost,
             const int32_t* __restrict__ inl, const double* __restrict__ slots, RsState* __restrict__ st,
-            double* __restrict__ bestEF, const float4* __restrict__ corrs, const double4* __restrict__ norm,
-            const int32_t* __restrict__ samples, const double* __restrict__ invK, double thr, double thr2,
-            double* __restrict__ bestRT) {
+            double* __restrict__ bestEF) {
   const int p = blockIdx.x;
   const int lane = threadIdx.x;
   __shared__ double sCost[kRsRound * kRsMaxSol];
@@ -470,59 +306,6 @@ k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, 
     }
   }
   __syncwarp();
-  if constexpr (kRefine) {
-    const int b = offsets[p], n = offsets[p + 1] - b;
-    double invK1[9], invK2t[9];
-    for (int k = 0; k < 9; ++k) invK1[k] = invK[(size_t)p * 18 + k];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) invK2t[3 * i + j] = invK[(size_t)p * 18 + 9 + 3 * j + i];
-    for (int j = 0; j < len; ++j) {
-      if (s.drawn > s.budget) break;
-      ++s.drawn;
-      const int ns = sCnt[j];
-      for (int r = 0; r < ns; ++r) {
-        const int idx = j * kRsMaxSol + r;
-        if (!(sCost[idx] < s.minError)) continue;
-        if (!sOk[idx]) continue;
-        double EF[kRsSlotDoubles];
-        for (int k = 0; k < kRsSlotDoubles; ++k) EF[k] = slots[(base * kRsMaxSol + idx) * kRsSlotDoubles + k];
-        const int32_t* smp = samples + ((long long)p * nDraw + s0 + j) * 5;
-        double x1[5], y1[5], x2[5], y2[5];
-        for (int k = 0; k < 5; ++k) {
-          const double4 v = norm[b + smp[k]];
-          x1[k] = v.x;
-          y1[k] = v.y;
-          x2[k] = v.z;
-          y2[k] = v.w;
-        }
-        double R[9], T[3];
-        if (!ess::essential_pose(EF, 5, x1, y1, x2, y2, R, T)) continue;  // relativePoseFromEssential
-        rs_refine_warp(corrs + b, norm + b, n, EF + 9, thr2, invK1, invK2t, thr, R, T);
-        double Er[9], Fr[9], costR;
-        int nInR;
-        ess::pose_essential(R, T, Er);
-        rs_fund(invK1, invK2t, Er, Fr);
-        rs_cost_in_order(corrs + b, n, Fr, thr2, &costR, &nInR);
-        s.minError = fmin(sCost[idx], costR);
-        s.chosen = s0 + j;
-        const float frac = (float)(nInR - 5) / (float)(n - 5);
-        s.budget = min(s.budget, rs_budget(1.0 - (double)frac));
-        double* ef = bestEF + (size_t)p * kRsSlotDoubles;
-        double* rt = bestRT + (size_t)p * 12;
-        if (lane < 9) {
-          ef[lane] = Er[lane];
-          ef[9 + lane] = Fr[lane];
-          rt[lane] = R[lane];
-        } else if (lane < 12) {
-          rt[lane] = T[lane - 9];
-        }
-      }
-    }
-    if (lane == 0) {
-      if (s.drawn > s.budget || s0 + len >= nDraw) s.done = 1;
-      st[p] = s;
-    }
-  } else {
   if (lane == 0) {
     const int n = offsets[p + 1] - offsets[p];
     int accepted = -1;
@@ -549,7 +332,6 @@ k_rs_select(const int32_t* __restrict__ offsets, int nPairs, int nDraw, int s0, 
   const int accepted = sAccepted;
   if (accepted >= 0 && lane < kRsSlotDoubles)
     bestEF[(size_t)p * kRsSlotDoubles + lane] = slots[(base * kRsMaxSol + accepted) * kRsSlotDoubles + lane];
-  }
 }
 
 // One thread per pair: E, F, R, T and error of the choice.
@@ -761,13 +543,12 @@ int rs_enqueue(v3dm_ransac* r, int nPairs, int nCorrs, int nDraw, int nSamples, 
                                                                        r->dSlots, thr2, r->dCost, r->dInl);
     V3DM_RS_TRY(rs_mark(r, 1));
     if (r->refine)
-      k_rs_select<true><<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
-                                                      r->dCost, r->dInl, r->dSlots, state, r->dBestEF, dCorrs,
-                                                      r->dNorm, dSamples, r->dInvK, r->thr, thr2, r->dBestRT);
+      V3DM_RS_TRY(launch_rs_select_refine(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk, r->dCost,
+                                          r->dSlots, state, r->dBestEF, dCorrs, r->dNorm, dSamples, r->dInvK, r->thr,
+                                          thr2, r->dBestRT, r->stream));
     else
-      k_rs_select<false><<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
-                                                       r->dCost, r->dInl, r->dSlots, state, r->dBestEF, dCorrs,
-                                                       r->dNorm, dSamples, r->dInvK, r->thr, thr2, r->dBestRT);
+      k_rs_select<<<nPairs, 32, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, s0, len, r->dCounts, r->dSlotOk,
+                                                 r->dCost, r->dInl, r->dSlots, state, r->dBestEF);
     launches += 4;
   }
   k_rs_finish<<<(nPairs + 127) / 128, 128, 0, r->stream>>>(r->dOffsets, nPairs, nDraw, dSamples, r->dNorm, state,

@@ -60,3 +60,8 @@ extern "C" void host_refine_pose(int n, const double* left, const double* right,
   std::vector<double> w(n), e(n);
   v3dm::ess::refine_pose(c.data(), n, invK1, invK2t, thr, R, T, w.data(), e.data());
 }
+
+// The double-double sin and cos of the device rotation update, on the host.
+extern "C" void host_sincos_dd(int n, const double* x, double* s, double* c) {
+  for (int i = 0; i < n; ++i) v3dm::ess::sincos_dd(x[i], s + i, c + i);
+}

@@ -169,3 +169,29 @@ def test_pose_refinement_matches_the_reference(host_lib, oracle_mod):
         assert np.abs(Rh - Rr).max() < 1e-8 and np.abs(Th - Tr).max() < 1e-8, t
         moved += np.abs(Rr - R0.reshape(-1)).max() > 1e-3
     assert moved > 20  # the refinement does move the starting poses
+
+
+def test_double_double_sin_cos_are_correctly_rounded(host_lib):
+    """The device rotation update's sin and cos (double-double Taylor series, rounded once) are the
+    correctly rounded values over the range the refinement uses (|theta| <= 1), checked against
+    200-bit evaluations; the C library's (which the reference calls) agree with them except for
+    about 1e-3 of the inputs, by one unit in the last place."""
+    mpmath = pytest.importorskip("mpmath")
+    host_lib.host_sincos_dd.argtypes = [C.c_int] + [C.c_void_p] * 3
+    libm = C.CDLL("libm.so.6")
+    libm.sin.restype = libm.cos.restype = C.c_double
+    libm.sin.argtypes = libm.cos.argtypes = [C.c_double]
+    rng = np.random.default_rng(11)
+    x = np.concatenate([10.0 ** rng.uniform(-6, 0, 6000), rng.uniform(0, 1, 2000), [1e-6, 0.5, 1.0]])
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    host_lib.host_sincos_dd(x.size, x.ctypes.data, s.ctypes.data, c.ctypes.data)
+    mpmath.mp.prec = 200
+    exact_s = np.array([float(mpmath.sin(mpmath.mpf(float(v)))) for v in x])
+    exact_c = np.array([float(mpmath.cos(mpmath.mpf(float(v)))) for v in x])
+    assert s.tobytes() == exact_s.tobytes()
+    assert c.tobytes() == exact_c.tobytes()
+    lib_s = np.array([libm.sin(v) for v in x])
+    lib_c = np.array([libm.cos(v) for v in x])
+    assert np.abs(lib_s - s).max() <= np.spacing(1.0) and np.abs(lib_c - c).max() <= np.spacing(1.0)
+    assert (lib_s != s).mean() < 5e-3 and (lib_c != c).mean() < 5e-3
