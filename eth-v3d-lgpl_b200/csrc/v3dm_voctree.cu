@@ -206,10 +206,17 @@ k_vt_top(const uint8_t* __restrict__ nodes, int bf, int L, long long topRows, lo
   __syncthreads();
   const int part = threadIdx.x % kTpk;
   const int perIter = (gridDim.x * kVtBktThreads) / kTpk;
-  for (int k0 = (blockIdx.x * kVtBktThreads + threadIdx.x) / kTpk; k0 - (int)(threadIdx.x / kTpk) < n; k0 += perIter) {
+  // the next iteration's key is loaded before this one is descended (the loads are the latency)
+  int k0 = (blockIdx.x * kVtBktThreads + threadIdx.x) / kTpk;
+  uint4 nw[kQ];
+  vt_load_key(keys, k0 < n ? k0 : 0, part, k0 < n, nw);
+  for (; k0 - (int)(threadIdx.x / kTpk) < n; k0 += perIter) {
     const bool valid = k0 < n;
     uint4 kw[kQ];
-    vt_load_key(keys, valid ? k0 : 0, part, valid, kw);
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) kw[q] = nw[q];
+    const int kn = k0 + perIter;
+    vt_load_key(keys, kn < n ? kn : 0, part, kn < n, nw);
     long long nextId = 0, leafId = 0;
     for (int d = 0; d < L; ++d) {
       int best;
@@ -359,11 +366,22 @@ k_vt_sub(const uint8_t* __restrict__ nodes, int bf, int T, long long levelStartL
       __syncthreads();
       staged = item.x;
     }
-    for (int k = threadIdx.x / kTpk; k - (int)(threadIdx.x / kTpk) < item.z; k += kVtBktThreads / kTpk) {
+    constexpr int kStep = kVtBktThreads / kTpk;
+    auto key_at = [&](int kk) { return kk < item.z ? (perm ? __ldg(perm + item.y + kk) : item.y + kk) : 0; };
+    int k = threadIdx.x / kTpk;
+    int nkey = key_at(k), nnkey = key_at(k + kStep);
+    uint4 nw[kQ];
+    vt_load_key(keys, nkey, part, k < item.z, nw);
+    for (; k - (int)(threadIdx.x / kTpk) < item.z; k += kStep) {
+      // the next key and the index after it are loaded before this key is descended
       const bool valid = k < item.z;
-      const int key = valid ? (perm ? perm[item.y + k] : item.y + k) : 0;
+      const int key = nkey;
       uint4 kw[kQ];
-      vt_load_key(keys, key, part, valid, kw);
+#pragma unroll
+      for (int q = 0; q < kQ; ++q) kw[q] = nw[q];
+      nkey = nnkey;
+      vt_load_key(keys, nkey, part, k + kStep < item.z, nw);
+      nnkey = key_at(k + 2 * kStep);
       long long idx = 0;
       int lvlRow = 0;
       long long lvlLen = bf;

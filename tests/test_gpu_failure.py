@@ -15,11 +15,13 @@ pytestmark = pytest.mark.gpu
 
 
 def test_a_wait_that_runs_out_reports_timeout_and_the_handle_recovers(v3dm_mod, oracle_mod):
-    L, R, lp, rp, F, _ = synth.stereo(23, 3000, 2800)
+    # 6000 x 5600 with 128 x 256 tiles: 47 x 22 tiles over 148 CTAs, so CTA 0 loads six B tiles
+    L, R, lp, rp, F, _ = synth.stereo(23, 6000, 5600)
     exp = oracle_mod.match(L, R, 0.7, 0.8)
     exp_g = oracle_mod.match(L, R, 0.7, 0.8, gates=[("F", F, 2.0)], lpos=lp, rpos=rp)
     with v3dm_mod.SIFTMatching(0) as m:
-        m.allocate(3000, 2800, True)
+        m.allocate(6000, 5600, True)
+        m.set_config(0)
         m.set_left_features(L)
         m.set_right_features(R)
         np.testing.assert_array_equal(m.find_putative_matches(0.7, 0.8), exp)
