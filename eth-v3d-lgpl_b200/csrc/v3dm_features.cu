@@ -17,10 +17,20 @@
 //     so those are kept as floats (V3DM_LOAD_KEEP_F32) for the float matcher
 //     (v3dm_set_left_f32_device: BF16 hi/lo scores), refused (V3DM_ERR_NOT_U8), or rounded
 //     only when the caller asks for it (V3DM_LOAD_LOSSY_U8).
-// The text archive ("V3DTXT") is not read: V3DM_ERR_UNSUPPORTED.
+// The text archive ("V3DTXT", serializeDataToFile(..., writeBinary = false), :956-977) is read
+// too: "V3DTXT", then whitespace-separated tokens written by TextOStreamArchive (:177-265): the
+// count, "{", per feature the tag "SIFT_Feature", "{", the 135 values and "}", and a closing "}".
+// Values are parsed as TextIStreamArchive's `is >> value` parses them (:267-338: decimal digits,
+// sign, point and exponent only, strtof rounding for floats); a value it could not read (a
+// "nan" or "inf" the writer printed, an overflow, a stray character) or a wrong tag or bracket
+// gives V3DM_ERR_IO, where the reference throws.
 #include <algorithm>
 #include <atomic>
+#include <cctype>
 #include <cstdio>
+#include <cerrno>
+#include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <thread>
@@ -51,10 +61,58 @@ bool host_little_endian() {
 
 struct FileReader {
   FILE* f = nullptr;
+  bool text = false;        // a V3DTXT archive: the rest of the file is in txt
+  std::vector<char> txt;    // text after the tag, NUL-terminated
+  size_t at = 0;            // next unread character of txt
   ~FileReader() {
     if (f) std::fclose(f);
   }
+  // The next whitespace-delimited token of a text archive, or nullptr at its end.  The token is
+  // NUL-terminated in place.
+  char* token() {
+    char* p = txt.data();
+    const size_t n = txt.size() - 1;
+    while (at < n && std::isspace((unsigned char)p[at])) ++at;
+    if (at >= n) return nullptr;
+    char* t = p + at;
+    while (at < n && !std::isspace((unsigned char)p[at])) ++at;
+    p[at] = '\0';
+    if (at < n) ++at;
+    return t;
+  }
 };
+
+// A token of a number as the stream extraction accepts it: digits, signs, point and exponent.
+bool number_chars(const char* t, bool allowFloat) {
+  if (!*t) return false;
+  for (const char* c = t; *c; ++c) {
+    const bool ok = (*c >= '0' && *c <= '9') || *c == '+' || *c == '-' ||
+                    (allowFloat && (*c == '.' || *c == 'e' || *c == 'E'));
+    if (!ok) return false;
+  }
+  return true;
+}
+
+bool parse_float(const char* t, float* v) {
+  if (!t || !number_chars(t, true)) return false;
+  char* end = nullptr;
+  const float x = std::strtof(t, &end);
+  if (end == t || *end != '\0' || std::isinf(x)) return false;  // an overflow fails the extraction
+  *v = x;
+  return true;
+}
+
+bool parse_long(const char* t, long long lo, long long hi, long long* v) {
+  if (!t || !number_chars(t, false)) return false;
+  char* end = nullptr;
+  errno = 0;
+  const long long x = std::strtoll(t, &end, 10);
+  if (end == t || *end != '\0' || errno == ERANGE || x < lo || x > hi) return false;
+  *v = x;
+  return true;
+}
+
+bool is_tag(const char* t, const char* want) { return t && std::strcmp(t, want) == 0; }
 
 // Opens a feature file and checks its header; *count is the number of features it holds.
 int open_features(const char* path, FileReader& r, uint32_t* count) {
@@ -62,7 +120,19 @@ int open_features(const char* path, FileReader& r, uint32_t* count) {
   if (!r.f) return V3DM_ERR_IO;
   unsigned char head[kHeaderBytes];
   if (std::fread(head, 1, kTagLen, r.f) != (size_t)kTagLen) return V3DM_ERR_IO;
-  if (std::memcmp(head, "V3DTXT", kTagLen) == 0) return V3DM_ERR_UNSUPPORTED;
+  if (std::memcmp(head, "V3DTXT", kTagLen) == 0) {
+    r.text = true;
+    if (std::fseek(r.f, 0, SEEK_END) != 0) return V3DM_ERR_IO;
+    const long long size = std::ftell(r.f);
+    if (size < kTagLen || std::fseek(r.f, (long)kTagLen, SEEK_SET) != 0) return V3DM_ERR_IO;
+    r.txt.assign((size_t)(size - kTagLen) + 1, '\0');
+    if (std::fread(r.txt.data(), 1, (size_t)(size - kTagLen), r.f) != (size_t)(size - kTagLen)) return V3DM_ERR_IO;
+    long long c = 0;
+    // an unsigned int, then the vector's opening bracket (serializeVector, :852-859)
+    if (!parse_long(r.token(), 0, 0xffffffffLL, &c) || !is_tag(r.token(), "{")) return V3DM_ERR_IO;
+    *count = (uint32_t)c;
+    return V3DM_OK;
+  }
   if (std::memcmp(head, "V3DBIN", kTagLen) != 0) return V3DM_ERR_IO;
   if (std::fread(head + kTagLen, 1, 4, r.f) != 4) return V3DM_ERR_IO;
   *count = le32(head + kTagLen);
@@ -75,10 +145,41 @@ int open_features(const char* path, FileReader& r, uint32_t* count) {
   return V3DM_OK;
 }
 
+// Decodes the first n features of a text archive opened by open_features.  With n equal to the
+// file's count (whole) the closing bracket must follow, as the reference's reader requires.
+int decode_text(FileReader& r, long long n, bool whole, int32_t* ids, float* pos, float* dir, float* scale,
+                float* mag, float* desc) {
+  for (long long i = 0; i < n; ++i) {
+    if (!is_tag(r.token(), "SIFT_Feature") || !is_tag(r.token(), "{")) return V3DM_ERR_IO;
+    long long id = 0;
+    if (!parse_long(r.token(), -2147483648LL, 2147483647LL, &id)) return V3DM_ERR_IO;
+    float v[134];
+    for (int k = 0; k < 134; ++k)
+      if (!parse_float(r.token(), &v[k])) return V3DM_ERR_IO;
+    if (!is_tag(r.token(), "}")) return V3DM_ERR_IO;
+    if (ids) ids[i] = (int32_t)id;
+    if (pos) {
+      pos[2 * i] = v[0];
+      pos[2 * i + 1] = v[1];
+    }
+    if (dir) {
+      dir[2 * i] = v[2];
+      dir[2 * i + 1] = v[3];
+    }
+    if (scale) scale[i] = v[4];
+    if (mag) mag[i] = v[5];
+    if (desc) std::memcpy(desc + i * 128, v + 6, 128 * sizeof(float));
+  }
+  if (whole && !is_tag(r.token(), "}")) return V3DM_ERR_IO;
+  return V3DM_OK;
+}
+
 // Decodes the first n features of an open file (positioned after the header).  Null outputs
-// are skipped.  Reads in blocks of kBlock features.
-int decode_features(FILE* f, long long n, int32_t* ids, float* pos, float* dir, float* scale, float* mag,
-                    float* desc) {
+// are skipped.  Binary archives are read in blocks of kBlock features.
+int decode_features(FileReader& r, long long n, bool whole, int32_t* ids, float* pos, float* dir, float* scale,
+                    float* mag, float* desc) {
+  if (r.text) return decode_text(r, n, whole, ids, pos, dir, scale, mag, desc);
+  FILE* f = r.f;
   constexpr int kBlock = 2048;
   std::vector<unsigned char> buf((size_t)kBlock * kFeatureBytes);
   for (long long i0 = 0; i0 < n; i0 += kBlock) {
@@ -207,7 +308,7 @@ int v3dm_features_read(const char* path, int cap, int32_t* n, int32_t* ids, floa
   const bool any = ids || positions || directions || scales || magnitudes || descriptors;
   if (!any) return V3DM_OK;
   if ((long long)count > cap) return V3DM_ERR_CAPACITY;
-  return decode_features(r.f, count, ids, positions, directions, scales, magnitudes, descriptors);
+  return decode_features(r, count, true, ids, positions, directions, scales, magnitudes, descriptors);
 }
 
 int v3dm_quantize_u8_device(const float* d_values, long long nValues, uint8_t* d_out, void* stream) {
@@ -312,8 +413,8 @@ int v3dm_loader_load(v3dm_loader* ld, int nFiles, const char* const* paths, int 
       int st = open_features(paths[i], r, &c);
       if (st == V3DM_OK && (long long)c < kept[i]) st = V3DM_ERR_IO;  // the file changed since its header was read
       if (st == V3DM_OK)
-        st = decode_features(r.f, kept[i], nullptr, ld->positions.data() + 2 * off[i], nullptr, nullptr, nullptr,
-                             ld->hStage + off[i] * 128);
+        st = decode_features(r, kept[i], kept[i] == (long long)c, nullptr, ld->positions.data() + 2 * off[i],
+                             nullptr, nullptr, nullptr, ld->hStage + off[i] * 128);
       if (st != V3DM_OK) {
         int expect = V3DM_OK;
         err.compare_exchange_strong(expect, st);

@@ -695,8 +695,8 @@ ERR_IO = 11
 
 
 def features_read(path: str) -> dict:
-    """v3dm_features_read: the reference's binary feature archive (SerializableVector<SIFT_Feature>)
-    as arrays: ids (n), positions (n, 2), directions (n, 2), scales (n), magnitudes (n),
+    """v3dm_features_read: the reference's feature archive (SerializableVector<SIFT_Feature>,
+    binary "V3DBIN" or text "V3DTXT") as arrays: ids (n), positions (n, 2), directions (n, 2), scales (n), magnitudes (n),
     descriptors (n, 128) float32."""
     n = C.c_int32(0)
     p = str(path).encode()

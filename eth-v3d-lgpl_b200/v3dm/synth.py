@@ -289,6 +289,23 @@ def write_features(path, f: dict) -> None:
         fh.write(rec.tobytes())
 
 
+def write_features_text(path, f: dict) -> None:
+    """The reference's text feature archive of f (serializeDataToFile(..., writeBinary = false)):
+    "V3DTXT", then the tokens TextOStreamArchive writes, each followed by a blank: the count, "{",
+    per feature "SIFT_Feature", "{", the id and 134 values printed with 6 significant digits (the
+    stream's default precision) and "}" with a line break and the 2-blank indentation, then "}"
+    and a line break."""
+    n = f["ids"].shape[0]
+    six = np.concatenate([f["positions"], f["directions"], f["scales"][:, None], f["magnitudes"][:, None]], 1)
+    parts = [f"V3DTXT\n{n} {{ "]
+    for i in range(n):
+        vals = " ".join(f"{float(v):g}" for v in (*six[i], *f["descriptors"][i]))
+        parts.append(f"SIFT_Feature {{ {int(f['ids'][i])} {vals} }} \n  ")
+    parts.append("} \n")
+    with open(path, "w") as fh:
+        fh.write("".join(parts))
+
+
 def sequence_words(seed: int = 4, n_images: int = 2048, n_leaves: int = 125_000, n_min: int = 2000,
                    n_max: int = 6000, window: int = 8, keep: float = 0.6, zipf: float = 0.5):
     """Visual words of an image sequence: a scene of points, each with a word drawn from a Zipf

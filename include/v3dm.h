@@ -348,13 +348,17 @@ V3DM_API int v3dm_voctree_replays(v3dm_voctree* t, long long* n);
 V3DM_API int v3dm_voctree_stream(v3dm_voctree* t, void** stream);
 
 /* ---- feature files ------------------------------------------------------------------ */
-/* serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) for the binary archive
- * (v3d_serialization.h:983-1017; SIFT_Feature fields v3d_feature.h:12-47): "V3DBIN", uint32
- * count, then per feature int32 id, position[2], direction[2], scale, magnitude, descriptor[128].
+/* serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) (v3d_serialization.h:983-1017;
+ * SIFT_Feature fields v3d_feature.h:12-47).  Binary archive: "V3DBIN", uint32 count, then per
+ * feature int32 id, position[2], direction[2], scale, magnitude, descriptor[128].  Text archive
+ * (writeBinary = false): "V3DTXT" and the same fields as whitespace-separated tokens with the
+ * tags and brackets of TextOStreamArchive (:177-265), parsed as the stream extraction parses them
+ * (:267-338); a value it cannot read ("nan", "inf", an overflow), a wrong tag or bracket gives
+ * V3DM_ERR_IO, where the reference throws.  For a text archive with every array NULL only the
+ * head is read.
  * *n = number of features.  With every array NULL only *n is set; otherwise cap must be >= *n
  * (else V3DM_ERR_CAPACITY).  NULL arrays are skipped.  positions / directions: 2n floats,
- * descriptors: 128n floats.  A text archive ("V3DTXT") gives V3DM_ERR_UNSUPPORTED, an unknown
- * tag, a missing or a short file V3DM_ERR_IO. */
+ * descriptors: 128n floats.  An unknown tag, a missing or a short file gives V3DM_ERR_IO. */
 V3DM_API int v3dm_features_read(const char* path, int cap, int32_t* n, int32_t* ids, float* positions,
                                 float* directions, float* scales, float* magnitudes, float* descriptors);
 /* u8 re-quantisation on the device: out = round(512 * x) (half to even) clamped to 0..255,

@@ -311,16 +311,18 @@ def ref_features_available() -> bool:
 def _ref_features_lib():
     L = C.CDLL(str(REF_FEATURES))
     L.ref_features_write.argtypes = [C.c_char_p, C.c_int] + [C.c_void_p] * 6
+    L.ref_features_write_as.argtypes = [C.c_char_p, C.c_int, C.c_int] + [C.c_void_p] * 6
     L.ref_features_read.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int)] + [C.c_void_p] * 6
     return L
 
 
-def ref_features_write(path: str, f: dict) -> None:
-    """serializeDataToFile(path, SerializableVector<SIFT_Feature>) of the reference (binary)."""
+def ref_features_write(path: str, f: dict, binary: bool = True) -> None:
+    """serializeDataToFile(path, SerializableVector<SIFT_Feature>, binary) of the reference
+    (binary: "V3DBIN", else the text archive "V3DTXT")."""
     L = _ref_features_lib()
     n = f["ids"].shape[0]
     a = [np.ascontiguousarray(f[k], np.int32 if k == "ids" else np.float32) for k in FEATURE_FIELDS]
-    if L.ref_features_write(str(path).encode(), n, *[x.ctypes.data for x in a]) != 0:
+    if L.ref_features_write_as(str(path).encode(), int(binary), n, *[x.ctypes.data for x in a]) != 0:
         raise OSError(f"reference writer failed on {path}")
 
 
@@ -335,7 +337,9 @@ def ref_features_count(path: str) -> int:
 
 
 def ref_features_read(path: str) -> dict:
-    """serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) of the reference."""
+    """serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) of the reference.  Only for
+    well-formed files: on a malformed text archive the reference's reader throws from a
+    destructor, which ends the process."""
     L = _ref_features_lib()
     n = C.c_int(0)
     if L.ref_features_read(str(path).encode(), 0, C.byref(n), *([None] * 6)) != 0:

@@ -15,9 +15,10 @@ using V3D::SIFT_Feature;
 
 extern "C" {
 
-// Writes n features (binary archive).  Returns 0, or -1 on an exception.
-int ref_features_write(const char* path, int n, const int* ids, const float* pos, const float* dir,
-                       const float* scale, const float* mag, const float* desc) {
+// Writes n features, a binary archive when binary != 0, else a text archive.  Returns 0, or -1
+// on an exception.
+int ref_features_write_as(const char* path, int binary, int n, const int* ids, const float* pos, const float* dir,
+                          const float* scale, const float* mag, const float* desc) {
   try {
     SerializableVector<SIFT_Feature> v(n);
     for (int i = 0; i < n; ++i) {
@@ -31,11 +32,17 @@ int ref_features_write(const char* path, int n, const int* ids, const float* pos
       f.magnitude = mag[i];
       std::memcpy(f.descriptor, desc + (size_t)i * 128, 128 * sizeof(float));
     }
-    V3D::serializeDataToFile(path, v, true);
+    V3D::serializeDataToFile(path, v, binary != 0);
     return 0;
   } catch (...) {
     return -1;
   }
+}
+
+// Writes n features (binary archive).
+int ref_features_write(const char* path, int n, const int* ids, const float* pos, const float* dir,
+                       const float* scale, const float* mag, const float* desc) {
+  return ref_features_write_as(path, 1, n, ids, pos, dir, scale, mag, desc);
 }
 
 // Reads a feature file the reference's way.  With cap < count only *n is set.  Returns 0, or

@@ -16,7 +16,8 @@ test, guided F matching and compounding F + H gates, and a case with duplicated 
 features: a binary feature archive written by the reference's serializer (oracle/_ref/
 libv3dref_features.so, from V3D/Base/v3d_serialization.h and v3d_feature.h) and the arrays its
 reader returns for it.  The records hold edge values (negative ids, NaN, infinities, negative
-zero, denormals) so that the check is on the bytes.
+zero, denormals) so that the check is on the bytes.  Beside it, a text archive ("V3DTXT") written
+by the same serializer with writeBinary = false, and what its reader makes of it.
 
 retrieval: the image loop of match_using_voctree.cpp:176-222 (computeBinomialScores, then
 insertDocument) on the reference's LeafDocuments (oracle/_ref/libv3dref_retrieval.so, from
@@ -135,6 +136,18 @@ def make_features(out: Path) -> None:
         assert back[k].tobytes() == np.ascontiguousarray(f[k]).tobytes(), k
     np.savez_compressed(out / "features_ref.npz", **back)
     print("wrote", path, "and", out / "features_ref.npz")
+    # the text archive (writeBinary = false): values as the stream prints them (6 significant
+    # digits), so the fixture holds what the reference's reader makes of that text.  Finite
+    # values only: the reference cannot read back the "nan" / "inf" it prints.
+    t = synth.feature_arrays(synth.rng_for(4343), 23)
+    t["ids"][:3] = [-2147483648, 2147483647, 0]
+    t["descriptors"][0, :8] = np.array([-0.0, 1e-45, -3.5, 1e30, 0.5 / 512, 3.4028235e38, 1.17549435e-38, 7e-39],
+                                       np.float32)
+    tpath = out / "features_ref_text.features"
+    oracle.ref_features_write(tpath, t, binary=False)
+    tback = oracle.ref_features_read(tpath)
+    np.savez_compressed(out / "features_ref_text.npz", **tback)
+    print("wrote", tpath, "and", out / "features_ref_text.npz")
 
 
 def _retrieval_cases():

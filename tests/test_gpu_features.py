@@ -48,7 +48,9 @@ def _device_bytes(ptr, nbytes):
     return torch.as_tensor(_View(), device="cuda").cpu().numpy()
 
 
-def _files(tmp_path, counts, seed=2, real_floats=False):
+def _files(tmp_path, counts, seed=2, real_floats=False, text=()):
+    """Feature files; those whose index is in text are text archives (V3DTXT) laid out as the
+    reference's text serializer writes them."""
     rng = np.random.default_rng(seed)
     paths, feats = [], []
     for i, n in enumerate(counts):
@@ -57,7 +59,10 @@ def _files(tmp_path, counts, seed=2, real_floats=False):
             x = rng.gamma(0.6, 1.0, (n, 128)).astype(np.float32)
             f["descriptors"] = (x / np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)).astype(np.float32)
         p = tmp_path / f"img{i}.features"
-        synth.write_features(p, f)
+        if i in text:
+            synth.write_features_text(p, f)
+        else:
+            synth.write_features(p, f)
         paths.append(str(p))
         feats.append(f)
     return paths, feats
@@ -68,7 +73,7 @@ def test_loader_equals_reader_and_quantisation(v3dm_mod, tmp_path, max_per_image
     """Unit-L2 float files rounded on request (LOAD_LOSSY_U8) equal the reader's floats
     quantised by numpy; the positions equal the reader's."""
     counts = [1000, 0, 31, 33, 2500, 700, 64]
-    paths, feats = _files(tmp_path, counts, real_floats=True)
+    paths, feats = _files(tmp_path, counts, real_floats=True, text=(2, 4))
     flags |= v3dm_mod.LOAD_LOSSY_U8
     with v3dm_mod.Loader() as ld:
         kept = ld.load(paths, max_per_image, flags)
@@ -83,7 +88,7 @@ def test_loader_equals_reader_and_quantisation(v3dm_mod, tmp_path, max_per_image
         got = _device_bytes(d_ptr, total * 128).reshape(total, 128)
         pos = ld.positions()
     exp_desc = np.concatenate([v3dm_mod.features_read(p)["descriptors"][:k] for p, k in zip(paths, exp_kept)])
-    exp_pos = np.concatenate([f["positions"][:k] for f, k in zip(feats, exp_kept)])
+    exp_pos = np.concatenate([v3dm_mod.features_read(p)["positions"][:k] for p, k in zip(paths, exp_kept)])
     np.testing.assert_array_equal(got, _quantize(exp_desc))
     np.testing.assert_array_equal(pos, exp_pos)
 
