@@ -18,6 +18,11 @@
 //     (.cu:546-551);
 //   - mutual filter and an ordered compaction into (pair, left, right) triples, grouped by pair
 //     (pairs in order of their left image, then table order), ascending left within a pair.
+// A guided call (v3dm_batch_match_guided) is runGuidedMatching / runGuidedHomographyMatching
+// (.cu:554-694) of every pair after its findPutativeMatches, with one gate per pair: the same
+// passes, the pair's gate applied on the fly wherever a score can decide (the chunk records,
+// k_records), and an exact warp re-score (k_brescore) of the few descriptors whose gated
+// second value the side pass could only bound.
 // Every launch after the first reads its sizes from device memory, so the whole sequence is
 // captured once as a CUDA graph and replayed while the images, pairs and parameters stay the same.
 #include <algorithm>
@@ -62,6 +67,8 @@ constexpr int kCntOut = 3;        // triples written
 constexpr int kCntNeedStates = 4; // sizes the pass-B buffers need
 constexpr int kCntNeedRows = 5;
 constexpr int kCntNeedTable = 6;
+constexpr int kCntFlagA = 7;      // guided call: pass-A states flagged for an exact re-score
+constexpr int kCntFlagB = 12;     // and pass-B states
 constexpr int kCntAll = 16;      // batch and proposal counter words
 
 constexpr int kScanThreads = 1024;
@@ -299,6 +306,70 @@ k_bmutual_write(int* __restrict__ counters, const int32_t* __restrict__ decB, co
       const int s = beg + i;
       out[off++] = make_int3(chosenPair[s], chosenLeft[s], chosenRight[s]);
     }
+}
+
+// Exact second values of the flagged states of a guided pass (k_decide flagged the states whose
+// gated bound straddles the decision), then their decisions; clears their state.  One warp per
+// flagged state: every lane holds the state's descriptor, the lanes take the other image's
+// descriptors in turn.  Scores >= T (below it any second value decides like none) that are not
+// the best and that the pair's gate keeps give the exact second value, the reference's nextVal
+// over its masked matrix (.cu:146).
+constexpr int kBRescoreThreads = 256;
+
+__global__ void __launch_bounds__(kBRescoreThreads)
+k_brescore(BatchGateArgs g, int aIsLeft, const int* __restrict__ flagged, const int* __restrict__ flaggedCount,
+           const BImage* __restrict__ im, const uint8_t* __restrict__ img, int32_t T, float minScore, float minRatio,
+           unsigned long long* __restrict__ best, unsigned int* __restrict__ sec, int32_t* __restrict__ decision) {
+  const int lane = threadIdx.x & 31;
+  const int n = *flaggedCount;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < n; f += nWarps) {
+    const int idx = flagged[f];
+    int pair = 0, aIdx = 0;
+    bgate_resolve(g, aIsLeft, idx, &pair, &aIdx);
+    const int2 lr = g.pairLR[pair];
+    const int aImg = aIsLeft ? lr.x : lr.y, bImg = aIsLeft ? lr.y : lr.x;
+    const BImage ma = im[aImg], mb = im[bImg];
+    uint32_t av[32];
+    const uint4* ap = reinterpret_cast<const uint4*>(img + ((size_t)ma.rowOff + aIdx) * kDescBytes);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const uint4 x = __ldg(ap + w);
+      av[4 * w] = x.x;
+      av[4 * w + 1] = x.y;
+      av[4 * w + 2] = x.z;
+      av[4 * w + 3] = x.w;
+    }
+    const float* m = g.gm + (size_t)pair * kBGateFloats;
+    const float2 pa = g.pos[g.posOff[aImg] + aIdx];
+    const float4 aT = aIsLeft ? gate_left_terms(g.type, m, pa) : gate_right_terms(g.type, m, pa);
+    const unsigned long long bk = best[idx];
+    unsigned s2 = 0;
+    for (int j = lane; j < mb.n; j += 32) {
+      const uint4* bp = reinterpret_cast<const uint4*>(img + ((size_t)mb.rowOff + j) * kDescBytes);
+      uint32_t S = 0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        const uint4 x = __ldg(bp + w);
+        S = __dp4a(av[4 * w], x.x, S);
+        S = __dp4a(av[4 * w + 1], x.y, S);
+        S = __dp4a(av[4 * w + 2], x.z, S);
+        S = __dp4a(av[4 * w + 3], x.w, S);
+      }
+      if ((int32_t)S < T || best_key((int32_t)S, j) == bk) continue;
+      const float2 pb = g.pos[g.posOff[bImg] + j];
+      const bool masked = aIsLeft ? gate_rejects_terms(g.type, m[9], aT, gate_right_terms(g.type, m, pb))
+                                  : gate_rejects_terms(g.type, m[9], gate_left_terms(g.type, m, pb), aT);
+      if (!masked) s2 = max(s2, S + 1u);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s2 = max(s2, __shfl_xor_sync(0xffffffffu, s2, o));
+    if (lane == 0) {
+      decision[idx] = decide(bk, s2, minScore, minRatio);
+      best[idx] = 0;
+      sec[idx] = 0;
+    }
+  }
 }
 
 // ---- proposal matching (learned cells) --------------------------------------------------
@@ -798,6 +869,19 @@ struct v3dm_batch {
   int gpProbes = 0, gpCells = 0, gpLaunches = 0;
   const v3dm_projection* gpProj = nullptr;
   long long exhaustivePairs = 0;    // sum over pairs of nL * nR
+  // guided calls: positions of the images' descriptors and one gate per pair
+  float2* dPos = nullptr;
+  long long posCap = 0;
+  bool havePositions = false;
+  float* dGate = nullptr;           // kBGateFloats per pair (caller's order)
+  long long gateCap = 0;
+  int2* dPairLR = nullptr;          // per pair (caller's order): left, right image
+  long long pairLRCap = 0;
+  long long* dStateA0 = nullptr;    // per pair (batch order): first pass-A state
+  int* dOrigOf = nullptr;           // per pair (batch order): index in the caller's order
+  long long pairAuxCap = 0;
+  int* dFlag = nullptr;             // flagged states of one pass
+  long long flagCap = 0;
   // profiling
   bool profile = false;
   cudaEvent_t ev[4] = {};
@@ -954,17 +1038,25 @@ int ensure_maps(v3dm_batch* b) {
   return V3DM_OK;
 }
 
-// Enqueues one batch call (all launches read their sizes from device memory).
-int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents) {
+// Enqueues one batch call (all launches read their sizes from device memory).  With bg set, the
+// call is guided: every pair's gate applies, and flagged states are re-scored exactly.
+int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents,
+                  const BatchGateArgs* bg = nullptr) {
   int GM = 0, BN = 0;
   tc_config_shape(tc_get_config(b->tc), &GM, &BN);
   const int32_t Smin = host_smallest_passing_score(minScore);
+  const bool gated = bg != nullptr;
+  int32_t Tg = 0;
+  if (gated) {
+    const int st = host_candidate_threshold(minScore, minRatio, true, &Tg);
+    if (st != V3DM_OK) return st;
+  }
   int launches = 0;
   V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
   SideArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.Smin = Smin;
-  if (host_candidate_threshold(minScore, minRatio, false, &sa.Tsec) != V3DM_OK) sa.Tsec = 0;
+  if (host_candidate_threshold(minScore, minRatio, gated, &sa.Tsec) != V3DM_OK) sa.Tsec = 0;
   sa.records = b->dRecords;
   sa.segCount = b->dSegCount;
   sa.segCap = b->segCap;
@@ -982,6 +1074,13 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   pa.best = b->dBest;
   pa.sec = b->dSec;
   pa.err = b->dInfo + kInfoErr;
+  const int rescoreGrid = 4 * 148;
+  if (gated) {
+    pa.gated = 1;
+    pa.bg = *bg;
+    pa.flagged = b->dFlag;
+    pa.flaggedCount = b->dCounters + kCntFlagA;
+  }
   // ---- pass A: every (pair, left group) against the pair's right image
   sa.aIsLeft = 1;
   sa.best = b->dBest;
@@ -998,6 +1097,13 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   pa.decision = b->dDecA;
   V3DM_BTRY(launch_post(pa, b->stream));
   launches += 3;
+  if (gated) {
+    k_brescore<<<rescoreGrid, kBRescoreThreads, 0, b->stream>>>(*bg, 1, b->dFlag, b->dCounters + kCntFlagA,
+                                                                 b->dImages, b->dImg, Tg, minScore, minRatio,
+                                                                 b->dBest, b->dSec, b->dDecA);
+    V3DM_BTRY(cudaGetLastError());
+    launches += 1;
+  }
   // ---- pass-B layout
   const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
   k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
@@ -1023,8 +1129,16 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   pa.rowsPtr = b->dCounters + kCntStates;
   pa.aIsLeft = 0;
   pa.decision = b->dDecB;
+  if (gated) pa.flaggedCount = b->dCounters + kCntFlagB;
   V3DM_BTRY(launch_post(pa, b->stream));
   launches += 4;
+  if (gated) {
+    k_brescore<<<rescoreGrid, kBRescoreThreads, 0, b->stream>>>(*bg, 0, b->dFlag, b->dCounters + kCntFlagB,
+                                                                 b->dImages, b->dImg, Tg, minScore, minRatio,
+                                                                 b->dBest, b->dSec, b->dDecB);
+    V3DM_BTRY(cudaGetLastError());
+    launches += 1;
+  }
   // ---- mutual filter, ordered triples
   const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
   k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
@@ -1145,6 +1259,41 @@ int finish_call(v3dm_batch* b) {
     return V3DM_ERR_CANDIDATES;
   }
   return V3DM_OK;
+}
+
+// One guided call (no graph): the flagged-state buffer, the gate arguments, the launches.
+int launch_call_guided(v3dm_batch* b, int type, float minScore, float minRatio) {
+  int st = prepare(b);
+  if (st != V3DM_OK) return st;
+  b->pendingCheck = true;
+  if (b->totalRows == 0 || b->nPairs == 0) {
+    V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                              b->stream));
+    b->lastLaunches = 0;
+    return V3DM_OK;
+  }
+  V3DM_BTRY(ensure(&b->dFlag, &b->flagCap, std::max<long long>(std::max(b->SA, b->capB), 1)));
+  BatchGateArgs bg;
+  std::memset(&bg, 0, sizeof(bg));
+  bg.on = 1;
+  bg.type = type;
+  bg.gm = b->dGate;
+  bg.pairLR = b->dPairLR;
+  bg.pos = b->dPos;
+  bg.posOff = b->dSrcOff;
+  bg.stateA0 = b->dStateA0;
+  bg.origOf = b->dOrigOf;
+  bg.nPairs = b->nPairs;
+  bg.chosenPair = b->dChosenPair;
+  bg.chosenRight = b->dChosenRight;
+  if (b->profile) {
+    for (int i = 0; i < 4; ++i)
+      if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
+  }
+  st = enqueue_batch(b, minScore, minRatio, b->profile, &bg);
+  if (st == V3DM_OK && b->profile) b->profPending = true;
+  return st;
 }
 
 int run_host(v3dm_batch* b, float minScore, float minRatio) {
@@ -1534,6 +1683,12 @@ void free_all(v3dm_batch* b) {
   bfree(b->dRowsPB);
   bfree(b->dRowsP);
   bfree(b->dChosenSorted);
+  bfree(b->dPos);
+  bfree(b->dGate);
+  bfree(b->dPairLR);
+  bfree(b->dStateA0);
+  bfree(b->dOrigOf);
+  bfree(b->dFlag);
   b->dCounters = nullptr;  // points into dInfo
   bfree(b->dInfo);
   if (b->hInfo) cudaFreeHost(b->hInfo);
@@ -1555,6 +1710,7 @@ int set_images(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t*
   if (rows > 0x7fffff00LL) return V3DM_ERR_SIZE;
   BDeviceGuard g(b->device);
   V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  b->havePositions = false;  // positions belong to the images
   // Same image sizes as before: the padded layout, the pair table and the row tables stay
   // valid, only the descriptors change (the graph reads them from the same buffer).
   const bool sameLayout = b->haveImages && nImages == b->nImages && std::equal(counts, counts + nImages, b->counts.begin());
@@ -1791,6 +1947,84 @@ int v3dm_batch_match(v3dm_batch* b, float minScore, float minRatio, int32_t* tri
     V3DM_BTRY(cudaStreamSynchronize(b->stream));
   }
   return n > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
+}
+
+int v3dm_batch_set_positions(v3dm_batch* b, const float* positions) {
+  if (!b) return V3DM_ERR_ARG;
+  if (!b->haveImages) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->totalDesc > 0 && !positions) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  b->havePositions = false;
+  V3DM_BTRY(ensure(&b->dPos, &b->posCap, std::max<long long>(b->totalDesc, 1)));
+  if (b->totalDesc > 0)
+    V3DM_BTRY(cudaMemcpyAsync(b->dPos, positions, (size_t)b->totalDesc * sizeof(float2), cudaMemcpyDefault,
+                              b->stream));
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  b->havePositions = true;
+  return V3DM_OK;
+}
+
+int v3dm_batch_set_positions_device(v3dm_batch* b, const float* d_positions) {
+  return v3dm_batch_set_positions(b, d_positions);
+}
+
+int v3dm_batch_match_guided(v3dm_batch* b, int type, const double* M, const float* thr, float minScore,
+                            float minRatio, int32_t* triples, long long cap, long long* nOut) {
+  if (!b || !nOut || cap < 0 || (cap > 0 && !triples) || (type != 1 && type != 2)) return V3DM_ERR_ARG;
+  if (!b->haveImages || !b->havePairs || !b->havePositions) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->nPairs > 0 && (!M || !thr)) return V3DM_ERR_ARG;
+  BDeviceGuard g(b->device);
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  const int n = b->nPairs;
+  if (n > 0) {
+    // per pair: the matrix as the reference's float3 rows (.cu:592-595), then thr^2 in float
+    // (.cu:591); the pair's images; per batch-order pair its first state and caller index
+    std::vector<float> gm((size_t)n * kBGateFloats);
+    std::vector<int2> lr(n);
+    for (int p = 0; p < n; ++p) {
+      for (int i = 0; i < 9; ++i) gm[(size_t)p * kBGateFloats + i] = (float)M[9 * (size_t)p + i];
+      gm[(size_t)p * kBGateFloats + 9] = thr[p] * thr[p];
+      lr[p] = make_int2(b->pairLi[p], b->pairRi[p]);
+    }
+    std::vector<long long> s0(n);
+    std::vector<int> oo(n);
+    for (int k = 0; k < n; ++k) {
+      s0[k] = b->bp[k].stateA0;
+      oo[k] = b->bp[k].orig;
+    }
+    V3DM_BTRY(ensure(&b->dGate, &b->gateCap, (long long)n * kBGateFloats));
+    V3DM_BTRY(ensure(&b->dPairLR, &b->pairLRCap, (long long)n));
+    if ((long long)n > b->pairAuxCap) {
+      bfree(b->dStateA0);
+      bfree(b->dOrigOf);
+      b->pairAuxCap = 0;
+      V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dStateA0), (size_t)n * sizeof(long long)));
+      V3DM_BTRY(cudaMalloc(reinterpret_cast<void**>(&b->dOrigOf), (size_t)n * sizeof(int)));
+      b->pairAuxCap = n;
+    }
+    V3DM_BTRY(cudaMemcpyAsync(b->dGate, gm.data(), gm.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->dPairLR, lr.data(), lr.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->dStateA0, s0.data(), s0.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                              b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->dOrigOf, oo.data(), oo.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));  // pageable host vectors
+  }
+  int st = V3DM_ERR_CANDIDATES;
+  for (int attempt = 0; attempt < 6 && st == V3DM_ERR_CANDIDATES; ++attempt) {
+    st = launch_call_guided(b, type, minScore, minRatio);
+    if (st != V3DM_OK) return st;
+    st = finish_call(b);
+  }
+  if (st != V3DM_OK) return st;
+  const long long nT = b->hInfo[kInfoWords + kCntOut];
+  *nOut = nT;
+  const long long m = std::min(nT, cap);
+  if (m > 0) {
+    V3DM_BTRY(cudaMemcpyAsync(triples, b->dOut, (size_t)m * sizeof(int3), cudaMemcpyDeviceToHost, b->stream));
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  }
+  return nT > cap ? V3DM_ERR_CAPACITY : V3DM_OK;
 }
 
 int v3dm_batch_match_device(v3dm_batch* b, float minScore, float minRatio, int32_t* d_count) {

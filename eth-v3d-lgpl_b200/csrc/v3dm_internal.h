@@ -144,6 +144,23 @@ int tc_gather_cols();
 cudaError_t tc_gather_map(CUtensorMap* m, const uint8_t* dB, int rowsB);
 cudaError_t launch_side_gather(TcPlan* p, const CUtensorMap& mB, const SideArgs& a, cudaStream_t st);
 
+// Gates of a batched guided call (v3dm_batch.cu): one gate per pair, evaluated on the fly from
+// the positions.  gm: per pair (caller's order) the 3x3 matrix as floats, then thr^2.
+constexpr int kBGateFloats = 10;
+struct BatchGateArgs {
+  int on;                        // 0: no batched gates
+  int type;                      // 1 epipolar (F), 2 homography (H)
+  const float* gm;
+  const int2* pairLR;            // per pair (caller's order): left image, right image
+  const float2* pos;             // positions of all images' descriptors, concatenated
+  const long long* posOff;       // per image: its first descriptor in pos
+  const long long* stateA0;      // per pair in batch order: its first pass-A state
+  const int* origOf;             // per pair in batch order: its index in the caller's order
+  int nPairs;
+  const int* chosenPair;         // per pass-B state: its pair (caller's order) and right
+  const int* chosenRight;
+};
+
 // Decision and bookkeeping kernels around the side passes (v3dm_pair.cu).
 struct PostArgs {
   int nRows;                     // rows of the pass (A side); with rowsPtr the device count
@@ -163,6 +180,7 @@ struct PostArgs {
   int32_t Smin;
   int nGates;
   const GateParams* gatesDev;
+  BatchGateArgs bg;              // batched guided call: per-pair gates instead of gatesDev
   float minScore, minRatio;
   int gated;
   int32_t* decision;             // per index: accepted partner or -1

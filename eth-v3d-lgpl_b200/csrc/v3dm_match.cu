@@ -158,29 +158,9 @@ struct GateMat {
 __global__ void k_gate_precompute(int type, GateMat g, const float2* __restrict__ lpos, int nL,
                                   const float2* __restrict__ rpos, int nR, float4* __restrict__ lv,
                                   float4* __restrict__ rv) {
-  const float* m = g.m;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nL) {
-    float2 p = lpos[i];
-    float x = __fadd_rn(__fadd_rn(__fmul_rn(m[0], p.x), __fmul_rn(m[1], p.y)), m[2]);
-    float y = __fadd_rn(__fadd_rn(__fmul_rn(m[3], p.x), __fmul_rn(m[4], p.y)), m[5]);
-    float z = __fadd_rn(__fadd_rn(__fmul_rn(m[6], p.x), __fmul_rn(m[7], p.y)), m[8]);
-    if (type == 2) {
-      x = __fdiv_rn(x, z);
-      y = __fdiv_rn(y, z);
-    }
-    lv[i] = make_float4(x, y, z, 0.f);
-  }
-  if (i < nR) {
-    float2 q = rpos[i];
-    if (type == 1) {
-      float fx = __fadd_rn(__fadd_rn(__fmul_rn(m[0], q.x), __fmul_rn(m[3], q.y)), m[6]);
-      float fy = __fadd_rn(__fadd_rn(__fmul_rn(m[1], q.x), __fmul_rn(m[4], q.y)), m[7]);
-      rv[i] = make_float4(q.x, q.y, fx, fy);
-    } else {
-      rv[i] = make_float4(q.x, q.y, 0.f, 0.f);
-    }
-  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nL) lv[i] = gate_left_terms(type, g.m, lpos[i]);
+  if (i < nR) rv[i] = gate_right_terms(type, g.m, rpos[i]);
 }
 
 __device__ __forceinline__ uint32_t f32_to_u8_checked(float v, bool& ok) {

@@ -56,12 +56,16 @@ __global__ void k_records(PostArgs a) {
       unsigned long long key[4];
       bool valid[4];
       unsigned long long cb = 0;
+      int bPair = 0, bIdx = orig;  // batched gates: the record's pair and its A-side index
+      if (a.bg.on && have) bgate_resolve(a.bg, a.aIsLeft, orig, &bPair, &bIdx);
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int col = col0 + 4 * part + t;
         valid[t] = have && col < nB;
         const int32_t S = (int32_t)sv[t];
         bool strong = valid[t] && S >= a.Smin;
+        if (a.bg.on && strong)
+          strong = !bgate_rejects(a.bg, bPair, a.aIsLeft ? bIdx : col, a.aIsLeft ? col : bIdx);
         for (int gi = 0; gi < a.nGates && strong; ++gi)
           strong = !gate_rejects(a.gatesDev[gi], a.aIsLeft ? orig : col, a.aIsLeft ? col : orig);
         key[t] = strong ? best_key(S, a.bmap ? __ldg(a.bmap + bRow0 + col) : col) : 0ull;

@@ -118,6 +118,9 @@ def lib() -> C.CDLL:
         L.v3dm_batch_set_pairs.argtypes = [vp, i32, vp]
         L.v3dm_batch_match.argtypes = [vp, f32, f32, vp, i64, i64p]
         L.v3dm_batch_match_device.argtypes = [vp, f32, f32, vp]
+        L.v3dm_batch_set_positions.argtypes = [vp, vp]
+        L.v3dm_batch_set_positions_device.argtypes = [vp, vp]
+        L.v3dm_batch_match_guided.argtypes = [vp, i32, vp, vp, f32, f32, vp, i64, i64p]
         L.v3dm_batch_wait.argtypes = [vp]
         L.v3dm_batch_result_device.argtypes = [vp, C.POINTER(vp)]
         L.v3dm_batch_stream.argtypes = [vp, C.POINTER(vp)]
@@ -476,6 +479,12 @@ class BatchMatching:
 
     __del__ = close
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def set_images(self, desc: np.ndarray, counts) -> None:
         """desc: (sum(counts), 128) uint8, the images' descriptors concatenated."""
         d = np.ascontiguousarray(desc, dtype=np.uint8)
@@ -513,6 +522,30 @@ class BatchMatching:
                 cap = n.value
                 continue
             _check(st, "batch_match")
+            self._last_n = n.value
+            return out[: n.value].copy()
+
+    def set_positions(self, positions: np.ndarray) -> None:
+        """positions: (sum(counts), 2) float32, every descriptor's (x, y), in descriptor order."""
+        p = np.ascontiguousarray(positions, dtype=np.float32)
+        _check(lib().v3dm_batch_set_positions(self._h, _ptr(p)), "batch_set_positions")
+
+    def match_guided(self, M: np.ndarray, thr, min_score: float = 0.9, min_ratio: float = 0.8,
+                     homography: bool = False, cap: int | None = None) -> np.ndarray:
+        """Guided matching of every pair (v3dm_batch_match_guided): M (n_pairs, 3, 3) fundamental
+        matrices (or homographies), thr a threshold per pair (or one for all).  Triples like match()."""
+        m = np.ascontiguousarray(M, dtype=np.float64).reshape(-1, 9)
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(thr, np.float32), (m.shape[0],)), dtype=np.float32)
+        cap = cap if cap is not None else max(1 << 20, getattr(self, "_last_n", 0))
+        while True:
+            out = np.empty((max(1, cap), 3), np.int32)
+            n = C.c_longlong(0)
+            st = lib().v3dm_batch_match_guided(self._h, 2 if homography else 1, _ptr(m), _ptr(t), min_score,
+                                               min_ratio, _ptr(out), cap, C.byref(n))
+            if st == ERR_CAPACITY:
+                cap = n.value
+                continue
+            _check(st, "batch_match_guided")
             self._last_n = n.value
             return out[: n.value].copy()
 

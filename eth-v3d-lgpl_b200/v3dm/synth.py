@@ -146,6 +146,48 @@ def images(seed: int = 2, n_images: int = 200, n_min: int = 1000, n_max: int = 1
     return desc, counts.astype(np.int32), offsets
 
 
+def scene(seed: int = 6, n_images: int = 12, n_min: int = 500, n_max: int = 4000, track_frac: float = 0.3,
+          f: float = 1200.0, width: int = 1600, height: int = 1200, spacing: float = 0.3,
+          max_yaw_deg: float = 10.0, noise_px: float = 1.0):
+    """An image set with geometry for guided matching.  The descriptors and tracks are those of
+    images(seed, ...); image c is a camera at (spacing * c, 0, 0) with a random yaw, every track
+    is a 3-D point in front of the cameras, and a track observation sits at the point's
+    projection plus N(0, noise_px^2) noise; other features are uniform in the image.  Returns
+    (desc, counts, offsets, positions (n, 2) float32, cams) with cams = (K, rotations, centres)."""
+    desc, counts, offsets, track_id = images(seed, n_images, n_min, n_max, track_frac, tracks=True)
+    rng = rng_for(seed + 1000)
+    K = np.array([[f, 0, width / 2.0], [0, f, height / 2.0], [0, 0, 1.0]])
+    rots, centres = [], []
+    for c in range(n_images):
+        yaw = np.deg2rad(rng.uniform(-max_yaw_deg, max_yaw_deg))
+        co, si = np.cos(yaw), np.sin(yaw)
+        rots.append(np.array([[co, 0, si], [0, 1, 0], [-si, 0, co]]))
+        centres.append(np.array([spacing * c, 0.0, 0.0]))
+    n_tracks = int(track_id.max()) + 1 if track_id.size else 0
+    X = np.stack([rng.uniform(-6.0, 6.0 + spacing * n_images, n_tracks), rng.uniform(-4.0, 4.0, n_tracks),
+                  rng.uniform(4.0, 20.0, n_tracks)], 1)
+    pos = np.stack([rng.uniform(0, width, desc.shape[0]), rng.uniform(0, height, desc.shape[0])], 1)
+    for c in range(n_images):
+        sl = slice(int(offsets[c]), int(offsets[c + 1]))
+        tr = track_id[sl]
+        m = tr >= 0
+        Xc = (rots[c] @ (X[tr[m]] - centres[c]).T)
+        q = K @ Xc
+        p = pos[sl]
+        p[m] = (q[:2] / q[2]).T + rng.normal(0.0, noise_px, (int(m.sum()), 2))
+    return desc, counts, offsets, pos.astype(np.float32), (K, rots, centres)
+
+
+def fundamental(cams, i: int, j: int) -> np.ndarray:
+    """F with q^T F p = 0 for p in image i and q in image j of a scene()."""
+    K, rots, centres = cams
+    Rot = rots[j] @ rots[i].T
+    t = rots[j] @ (centres[i] - centres[j])
+    tx = np.array([[0, -t[2], t[1]], [t[2], 0, -t[0]], [-t[1], t[0], 0]])
+    Ki = np.linalg.inv(K)
+    return Ki.T @ tx @ Rot @ Ki
+
+
 def inlier_mask(triples: np.ndarray, pairs: np.ndarray, offsets: np.ndarray, track_id: np.ndarray) -> np.ndarray:
     """True for the match triples (pair, left, right) that join two views of one track."""
     tl = track_id[offsets[pairs[triples[:, 0], 0]] + triples[:, 1]]

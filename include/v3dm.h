@@ -223,6 +223,21 @@ V3DM_API int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pair
  * ascending left within a pair; the first 'cap' are written (V3DM_ERR_CAPACITY if more). */
 V3DM_API int v3dm_batch_match(v3dm_batch* b, float minScore, float minRatio, int32_t* triples, long long cap,
                               long long* nOut);
+/* Positions (x, y) of every image's descriptors, two floats each, concatenated in the order of
+ * the descriptors given to v3dm_batch_set_images_*; host or device memory (the _device name is
+ * an alias).  The guided call needs them; new images drop them. */
+V3DM_API int v3dm_batch_set_positions(v3dm_batch* b, const float* positions);
+V3DM_API int v3dm_batch_set_positions_device(v3dm_batch* b, const float* d_positions);
+/* runGuidedMatching (type 1: M = the pair's fundamental matrix, epipolar gate,
+ * v3d_cudamatching.cu:554-623) or runGuidedHomographyMatching (type 2: M = H, transfer-distance
+ * gate, .cu:625-694) of every pair of the table, each after its findPutativeMatches: the apps'
+ * per-pair sequence putative -> RANSAC -> guided (match_sequence.cpp:306-324) for a whole batch.
+ * M: 9 doubles per pair (row-major), thr: one distance threshold per pair, both in the caller's
+ * pair order.  Each pair's scores are masked by its own gate only (one guided call after a
+ * putative call).  Output and errors as v3dm_batch_match; V3DM_ERR_NOT_ALLOCATED without
+ * images, pairs or positions. */
+V3DM_API int v3dm_batch_match_guided(v3dm_batch* b, int type, const double* M, const float* thr, float minScore,
+                                     float minRatio, int32_t* triples, long long cap, long long* nOut);
 /* Device-resident variant: enqueues the call on the batch's stream (replayed as a CUDA graph
  * while images, pairs, parameters and configuration stay the same) and copies the triple
  * count to d_count (device int32, may be NULL).  v3dm_batch_wait checks the call; it returns
