@@ -338,7 +338,7 @@ const char* v3dm_status_string(int s) {
     case V3DM_ERR_TIMEOUT: return "device wait timed out";
     case V3DM_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case V3DM_ERR_CANDIDATES: return "candidate list overflow (list grown; repeat the call)";
-    case V3DM_ERR_IO: return "feature file missing, not a binary feature archive, or truncated";
+    case V3DM_ERR_IO: return "feature file missing, not a feature archive, malformed or truncated";
     default: return "unknown status";
   }
 }

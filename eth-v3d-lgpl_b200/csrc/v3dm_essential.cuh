@@ -705,7 +705,7 @@ V3DM_HD void pose_update(const double* Rold, const double* Told, const double* d
         for (int k = 0; k < 3; ++k) v += J[3 * i + k] * J[3 * k + j];
         J2[3 * i + j] = v;
       }
-#ifdef __CUDA_ARCH__
+#if defined(__CUDA_ARCH__) || defined(V3DM_HOST_SINCOS_DD)
     double sn, cs;
     if (theta <= 1.0) {
       sincos_dd(theta, &sn, &cs);

@@ -51,8 +51,8 @@ extern "C" {
 #define V3DM_ERR_NO_DEVICE 9       /* no sm_100 device (the library has no CPU path)   */
 #define V3DM_ERR_CANDIDATES 10     /* a device-only call overflowed the candidate list; the
                                       list has been grown, repeat the call             */
-#define V3DM_ERR_IO 11             /* a feature file cannot be opened, is not a binary
-                                      feature archive, or is shorter than its count    */
+#define V3DM_ERR_IO 11             /* a feature file cannot be opened, is not a feature
+                                      archive, is malformed or shorter than its count  */
 
 V3DM_API const char* v3dm_status_string(int status);
 /* Detail of the last V3DM_ERR_CUDA raised by a matcher call on this thread (the CUDA error

@@ -409,7 +409,13 @@ def _ref_ransac_lib():
                              C.POINTER(C.c_int)]
     L.ref_ransac_mode.argtypes = [C.c_int, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp, C.c_int, vp,
                                   C.POINTER(C.c_int), vp, C.POINTER(C.c_int)]
+    L.ref_ransac_swap.argtypes = [C.c_int, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp,
+                                  C.POINTER(C.c_int), vp, C.POINTER(C.c_int)]
     return L
+
+
+# ref_ransac(swap=...): the library's restatements in place of the reference's components.
+SWAP_SOLVER, SWAP_POSE, SWAP_REFINE = 1, 2, 4
 
 
 def ref_five_point(x1, y1, x2, y2):
@@ -431,10 +437,12 @@ def ref_shuffle_samples(n: int, n_samples: int, seed: int) -> np.ndarray:
 
 
 def ref_ransac(corrs: np.ndarray, K1: np.ndarray, K2: np.ndarray, inlier_threshold: float, n_samples: int,
-               samples: np.ndarray, refine: bool = False):
+               samples: np.ndarray, refine: bool = False, swap: int = 0):
     """The loop of computeRobustOrientationMLE on one pair with the given samples, without
     (default) or with mode.iterativeRefinement: dict(model (31), n_inliers, flags,
-    chosen = sample * 10 + solution index or -1)."""
+    chosen = sample * 10 + solution index or -1).  swap (SWAP_* bits) replaces the reference's
+    five-point solver, pose recovery or refinement by the library's restatement; all three give
+    the GPU's algorithm on the CPU."""
     L = _ref_ransac_lib()
     c = np.ascontiguousarray(corrs, np.float32).reshape(-1, 4)
     k1 = np.ascontiguousarray(K1, np.float64)
@@ -443,7 +451,7 @@ def ref_ransac(corrs: np.ndarray, K1: np.ndarray, K2: np.ndarray, inlier_thresho
     model = np.empty(31)
     nin, ch = C.c_int(0), C.c_int(0)
     flags = np.empty(c.shape[0], np.uint8)
-    L.ref_ransac_mode(c.shape[0], c.ctypes.data, k1.ctypes.data, k2.ctypes.data, float(inlier_threshold), n_samples,
-                      s.shape[0], s.ctypes.data, int(refine), model.ctypes.data, C.byref(nin), flags.ctypes.data,
-                      C.byref(ch))
+    L.ref_ransac_swap(c.shape[0], c.ctypes.data, k1.ctypes.data, k2.ctypes.data, float(inlier_threshold), n_samples,
+                      s.shape[0], s.ctypes.data, int(refine), int(swap), model.ctypes.data, C.byref(nin),
+                      flags.ctypes.data, C.byref(ch))
     return {"model": model, "n_inliers": nin.value, "flags": flags, "chosen": ch.value}

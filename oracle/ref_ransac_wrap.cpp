@@ -10,10 +10,17 @@
 // reference's own solver, pose recovery, matrix inverse and products, with the samples given rather
 // than drawn; ref_ransac is the default mode (no refinement); ref_shuffle_samples draws the samples
 // the way that loop does (srand(seed), std::random_shuffle, consecutive 5-tuples).
+// ref_ransac_swap runs the same loop with some of the reference's components replaced by the
+// library's restatements (v3dm_essential.cuh, with the device's sin/cos): the five-point solver,
+// the pose recovery, the refinement.  With all three it is the GPU's algorithm on the CPU; swapping
+// one at a time attributes a difference between the GPU and the reference to one component.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
+
+#define V3DM_HOST_SINCOS_DD 1  // the restated refinement with the device's sin/cos
+#include "v3dm_essential.cuh"
 
 #include "Geometry/v3d_poseutilities.h"
 #include "Math/v3d_linear.h"
@@ -111,8 +118,12 @@ int ref_shuffle_samples(int N, int nSamples, unsigned seed, int cap, int* sample
 // accepted pose refined by refineRelativePose on the inliers of its F, then E, F, cost and inlier
 // count from the refined pose).  model: E 9, F 9, R 9, T 3, error (-1 when nothing was accepted);
 // *nInliers and flags (N bytes) from the chosen F; *chosen = sample * 10 + solution index, or -1.
-int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold,
-                    int nSamples, int nDraw, const int* samples, int refine, double* model, int* nInliers,
+// swap: bit 0 the restated five-point solver, bit 1 the restated pose recovery, bit 2 the restated
+// refinement in place of the reference's.
+constexpr int kSwapSolver = 1, kSwapPose = 2, kSwapRefine = 4;
+
+int ref_ransac_swap(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold,
+                    int nSamples, int nDraw, const int* samples, int refine, int swap, double* model, int* nInliers,
                     unsigned char* flags, int* chosen) {
   int const minSize = 5;
   double const sqrInlierThreshold = inlierThreshold * inlierThreshold;
@@ -148,7 +159,14 @@ int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K
       y2[k] = nr[c][1];
     }
     std::vector<Matrix3x3d> Es;
-    computeEssentialsFromFiveCorrs(x1, y1, x2, y2, Es);
+    if (swap & kSwapSolver) {
+      double E10[10][9];
+      const int ns = v3dm::ess::five_point(x1, y1, x2, y2, E10);
+      Es.resize(ns);
+      for (int k = 0; k < ns; ++k) Es[k] = mat(E10[k]);
+    } else {
+      computeEssentialsFromFiveCorrs(x1, y1, x2, y2, Es);
+    }
     ++drawnSamples;
     for (size_t r = 0; r < Es.size(); ++r) {
       Matrix3x3d fund = invK2_t * Es[r] * invK1;
@@ -162,7 +180,16 @@ int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K
       if (curError < minError) {
         Matrix3x3d R;
         Vector3d t;
-        if (!relativePoseFromEssential(Es[r], 5, x1, y1, x2, y2, R, t)) continue;
+        if (swap & kSwapPose) {
+          double Ef[9], Rr[9], Tt[3];
+          put(Es[r], Ef);
+          if (!v3dm::ess::essential_pose(Ef, 5, x1, y1, x2, y2, Rr, Tt)) continue;
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) R[a][b] = Rr[3 * a + b];
+          for (int k = 0; k < 3; ++k) t[k] = Tt[k];
+        } else if (!relativePoseFromEssential(Es[r], 5, x1, y1, x2, y2, R, t)) {
+          continue;
+        }
         if (refine) {
           std::vector<Vector2d> left, right;
           for (int i = 0; i < N; ++i)
@@ -176,7 +203,36 @@ int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K
               left.push_back(l);
               right.push_back(q);
             }
-          refineRelativePose(left, right, mat(K1), mat(K2), R, t, inlierThreshold);
+          if (swap & kSwapRefine) {
+            std::vector<v3dm::ess::PoseCorr> c(left.size());
+            double iK1[9], iK2[9], iK2t[9], Rr[9], Tt[3];
+            put(invK1, iK1);
+            put(invK2, iK2);
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) iK2t[3 * a + b] = iK2[3 * b + a];
+            for (size_t i = 0; i < left.size(); ++i) {
+              Vector2d nl2, nr2;
+              multiply_A_v_projective(invK1, left[i], nl2);
+              multiply_A_v_projective(invK2, right[i], nr2);
+              c[i].lx = nl2[0];
+              c[i].ly = nl2[1];
+              c[i].rx = nr2[0];
+              c[i].ry = nr2[1];
+              c[i].plx = left[i][0];
+              c[i].ply = left[i][1];
+              c[i].prx = right[i][0];
+              c[i].pry = right[i][1];
+            }
+            put(R, Rr);
+            for (int k = 0; k < 3; ++k) Tt[k] = t[k];
+            std::vector<double> w(c.size()), e(c.size());
+            v3dm::ess::refine_pose(c.data(), (int)c.size(), iK1, iK2t, inlierThreshold, Rr, Tt, w.data(), e.data());
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) R[a][b] = Rr[3 * a + b];
+            for (int k = 0; k < 3; ++k) t[k] = Tt[k];
+          } else {
+            refineRelativePose(left, right, mat(K1), mat(K2), R, t, inlierThreshold);
+          }
           Matrix3x3d const E_refined = computeEssentialFromRelativePose(R, t);
           Matrix3x3d const F_refined = invK2_t * E_refined * invK1;
           double curError_refined = 0;
@@ -237,8 +293,16 @@ int ref_refine_pose(int n, const double* left, const double* right, const double
 
 int ref_ransac(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold, int nSamples,
                int nDraw, const int* samples, double* model, int* nInliers, unsigned char* flags, int* chosen) {
-  return ref_ransac_mode(N, corrs, K1, K2, inlierThreshold, nSamples, nDraw, samples, 0, model, nInliers, flags,
+  return ref_ransac_swap(N, corrs, K1, K2, inlierThreshold, nSamples, nDraw, samples, 0, 0, model, nInliers, flags,
                          chosen);
+}
+
+// The reference's own loop (no component replaced).
+int ref_ransac_mode(int N, const float* corrs, const double* K1, const double* K2, double inlierThreshold,
+                    int nSamples, int nDraw, const int* samples, int refine, double* model, int* nInliers,
+                    unsigned char* flags, int* chosen) {
+  return ref_ransac_swap(N, corrs, K1, K2, inlierThreshold, nSamples, nDraw, samples, refine, 0, model, nInliers,
+                         flags, chosen);
 }
 
 }  // extern "C"

@@ -137,9 +137,9 @@ def test_loader_errors(v3dm_mod, tmp_path):
         with pytest.raises(v3dm_mod.V3DMError) as e:
             ld.load(paths + [str(tmp_path / "missing.features")])
         assert e.value.status == v3dm_mod.ERR_IO
-        with pytest.raises(v3dm_mod.V3DMError) as e:
+        with pytest.raises(v3dm_mod.V3DMError) as e:  # a text archive without its brackets
             ld.load([str(tmp_path / "bad.features")])
-        assert e.value.status == v3dm_mod.ERR_UNSUPPORTED
+        assert e.value.status == v3dm_mod.ERR_IO
         # still usable after an error
         np.testing.assert_array_equal(ld.load(paths), [100, 50])
 

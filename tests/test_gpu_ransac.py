@@ -1,17 +1,22 @@
 """Essential-matrix RANSAC on the GPU (v3dm_ransac_*) against the reference pin (oracle/_ref: the
-reference's computeEssentialsFromFiveCorrs and relativePoseFromEssential in the loop of
-computeRobustOrientationMLE, V3D/Apps/SfM/reconstruction_common.cpp:139-340, refinement off).
+reference's computeEssentialsFromFiveCorrs, relativePoseFromEssential and refineRelativePose in the
+loop of computeRobustOrientationMLE, V3D/Apps/SfM/reconstruction_common.cpp:139-340).
 
-Tolerances: the five-point solutions are floating point (the reference's SVD null space and
-polynomial solver against a QR null space and derivative-bracketed roots here); they agree to
-about 1e-12, so the per-sample solution counts must agree on >= 99.5% of random samples and >= 99%
-of the reference's solutions must have a counterpart within 1e-6 (unit norm, sign-fixed).  The
-costs are evaluated in double in the reference's operation order, so with the reference's own
-sample sequence the chosen candidate must be the same (unit E within 1e-5) on >= 97% of the pairs
-(a different choice can only come from costs that tie to within the solutions' rounding); for those
-the error, R and T agree to 1e-4 and the inlier flags to 0.2% of the correspondences (ill-conditioned
-samples give solutions that differ by up to ~1.5e-6 between the two solvers, and pixel coordinates
-near 1000 amplify that in the Sampson costs to a few 1e-6 relative)."""
+The five-point solutions are floating point (the reference's SVD null space and polynomial solver
+against a QR null space and derivative-bracketed roots here); they agree to about 1e-12, so the
+per-sample solution counts must agree on >= 99.5% of random samples and >= 99% of the reference's
+solutions must have a counterpart within 1e-6 (unit norm, sign-fixed).
+
+The loop is checked two ways, with the reference's own sample sequence:
+  - exactly against the same loop with the library's solver, pose recovery and refinement in place
+    of the reference's (oracle ref_ransac swap=7, the GPU's algorithm on the CPU): the same choice on
+    every pair, the same inlier flags and counts, E, R, T and the error to 1e-5 (the GPU's double
+    arithmetic is the host's up to the last bits of a few operations);
+  - against the reference itself: the same choice on most pairs, and every pair where the choice
+    differs must differ in the same way when only the reference's five-point solver is replaced
+    (swap=1): the solvers' 1e-12 differences decide near-ties between candidates' costs.  The
+    restated pose recovery and refinement alone (swap=6) never change the reference's choice
+    (tests/test_ransac_restated.py)."""
 import numpy as np
 import pytest
 
@@ -29,6 +34,26 @@ def _unit(E):
     e = E.reshape(-1)
     e = e / np.linalg.norm(e)
     return e * np.sign(e[np.argmax(np.abs(e))])
+
+
+def _check_restated(oracle_mod, got, p, c, K, thr, n_samples, samples, refine, flags):
+    """The GPU's pair p equals the loop with the library's components on the CPU (swap=7)."""
+    o = oracle_mod.ref_ransac(c, K[0], K[1], thr, n_samples, samples, refine=refine, swap=7)
+    if o["chosen"] < 0:
+        assert got["n_inliers"][p] == -1, p
+        return
+    assert got["n_inliers"][p] == o["n_inliers"], p
+    assert np.linalg.norm(_unit(got["E"][p]) - _unit(o["model"][:9])) < 1e-5, p
+    np.testing.assert_allclose(got["error"][p], o["model"][30], rtol=1e-5)
+    assert np.abs(got["R"][p].reshape(-1) - o["model"][18:27]).max() < 1e-5
+    assert np.abs(got["T"][p] - o["model"][27:30]).max() < 1e-5
+    np.testing.assert_array_equal(flags, o["flags"])
+
+
+def _same_choice(a, b):
+    if a["chosen"] < 0 or b["chosen"] < 0:
+        return a["chosen"] < 0 and b["chosen"] < 0
+    return a["chosen"] // 10 == b["chosen"] // 10 and np.linalg.norm(_unit(a["model"][:9]) - _unit(b["model"][:9])) < 1e-5
 
 
 def _rot(rng):
@@ -95,12 +120,11 @@ def test_reference_sample_sequence_gives_the_reference_choice(v3dm_mod, oracle_m
                 continue
             got = r.essential(np.array([0, n]), c, K[p:p + 1], thr, n_samples, samples=s[None])
             total += 1
+            _check_restated(oracle_mod, got, 0, c, K[p], thr, n_samples, s, False, got["flags"])
             if ref["chosen"] < 0:
                 agree += got["n_inliers"][0] == -1
                 continue
-            if got["n_inliers"][0] < 0:
-                continue
-            if np.linalg.norm(_unit(got["E"][0]) - _unit(ref["model"][:9])) < 1e-5:
+            if got["n_inliers"][0] >= 0 and np.linalg.norm(_unit(got["E"][0]) - _unit(ref["model"][:9])) < 1e-5:
                 agree += 1
                 np.testing.assert_allclose(got["error"][0], ref["model"][30], rtol=1e-4)
                 assert np.abs(got["R"][0].reshape(-1) - ref["model"][18:27]).max() < 1e-4
@@ -108,7 +132,10 @@ def test_reference_sample_sequence_gives_the_reference_choice(v3dm_mod, oracle_m
                 slack = max(2, n // 500)
                 diff = int((got["flags"] != ref["flags"]).sum())
                 assert diff <= slack and abs(int(got["n_inliers"][0]) - ref["n_inliers"]) <= slack
-        assert agree >= 0.97 * total, (agree, total)
+            else:  # the reference's solver is the only difference that changes the choice
+                solver = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], thr, n_samples, s, swap=oracle_mod.SWAP_SOLVER)
+                assert not _same_choice(solver, ref), p
+        assert agree >= 0.95 * total, (agree, total)
 
 
 @pytest.mark.parametrize("n_pairs,n_min,n_max,thr,n_samples", [(30, 300, 1500, 2.0, 1000), (6, 2500, 4000, 1.0, 500)])
@@ -116,10 +143,10 @@ def test_iterative_refinement_gives_the_reference_result(v3dm_mod, oracle_mod, n
                                                          n_samples):
     """mode.iterativeRefinement (set by the apps): each accepted pose refined on its inliers
     (refineRelativePose), the loop continuing from the refined cost and inlier count.  With the
-    reference's own sample sequence, the same model (unit E within 1e-5) on >= 97% of the pairs
-    (as without refinement: the same candidate choice), and for those the refined error, R and T
-    to 1e-4 (the refinement's sums over the inliers are summed in another order) and the inlier
-    flags to 0.2% of the correspondences; all pairs, batched in one call, give the same models."""
+    reference's own sample sequence: exactly the loop with the library's components on every pair;
+    the reference's model (unit E within 1e-5, refined error, R and T to 1e-4, inlier flags to 0.2%
+    of the correspondences) on >= 90% of the pairs, and on the others a choice that the restated
+    five-point solver alone makes too.  All pairs run batched in one call."""
     _need_ref(oracle_mod)
     off, corrs, K, R, t, inl = synth.two_view_pairs(n_pairs + 7 * n_min, n_pairs=n_pairs, n_min=n_min, n_max=n_max)
     seqs = [v3dm_mod.ransac_shuffle_samples(int(off[p + 1] - off[p]), n_samples, 300 + p) for p in range(n_pairs)]
@@ -134,6 +161,7 @@ def test_iterative_refinement_gives_the_reference_result(v3dm_mod, oracle_mod, n
     for p in range(n_pairs):
         c = corrs[off[p]:off[p + 1]]
         n = c.shape[0]
+        _check_restated(oracle_mod, allp, p, c, K[p], thr, n_samples, seqs[p], True, allp["flags"][off[p]:off[p + 1]])
         ref = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], thr, n_samples, seqs[p], refine=True)
         if ref["chosen"] < 0 or allp["n_inliers"][p] < 0:
             agree += ref["chosen"] < 0 and allp["n_inliers"][p] < 0
@@ -148,8 +176,12 @@ def test_iterative_refinement_gives_the_reference_result(v3dm_mod, oracle_mod, n
             fl = allp["flags"][off[p]:off[p + 1]]
             assert int((fl != ref["flags"]).sum()) <= slack
             assert abs(int(allp["n_inliers"][p]) - ref["n_inliers"]) <= slack
+        else:  # the reference's solver is the only difference that changes the choice
+            solver = oracle_mod.ref_ransac(c, K[p, 0], K[p, 1], thr, n_samples, seqs[p], refine=True,
+                                           swap=oracle_mod.SWAP_SOLVER)
+            assert not _same_choice(solver, ref), p
     print(f"refinement: {agree} of {n_pairs} pairs agree with the reference; {moved} poses moved by it")
-    assert agree >= 0.97 * n_pairs, (agree, n_pairs)
+    assert agree >= 0.90 * n_pairs, (agree, n_pairs)
     assert moved > 0  # the refinement does change the poses
 
 
