@@ -879,6 +879,7 @@ def run_voctree(args, ws, rank, local):
     clocks = Clocks(local)
     ms = max_over_ranks(ws, timed(t, args.steps), dev)
     clk = clocks.stop()
+    launches_per_call = t.last_launches()
     ids = d_ids.cpu().numpy()
     # per level: the same kernel on the depth-d prefix trees
     level_ms, prev = [], 0.0
@@ -930,14 +931,15 @@ def run_voctree(args, ws, rank, local):
         "per_level": [{"level": d + 1, "ms": level_ms[d], "gathered_GBps": level_bytes / (level_ms[d] * 1e-3) / 1e9
                        if level_ms[d] > 0 else None} for d in range(depth)],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_from_profiles("k_voctree"),
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": traffic_from_profiles("k_voctree_f32" if fl else "k_vtc"),
                      "peak_src": f"{peaks['src']} copy bandwidth",
                      "bytes_per_launch": alg_bytes,
                      "kernel": "k_voctree_f32 (all levels, one launch)" if fl else
-                               "k_vt_top + k_vt_scan + k_vt_scatter + k_vt_sub (bucketed descent, one call)"},
+                               "k_vtc x 3 (two levels per phase, tcgen05) + k_vt_scan + k_vt_scatter (one call)"},
         "e2e": {"value": ws * n * 1000.0 / ms_e2e, "unit": "desc/s", "h2d_bytes_per_step": int(keys.nbytes),
                 "d2h_bytes_per_step": int(n * 4)},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * launches_per_call,
         "clocks": clk,
     }
     if not args.no_cpu_baseline and ws == 1:

@@ -144,6 +144,40 @@ int tc_gather_cols();
 cudaError_t tc_gather_map(CUtensorMap* m, const uint8_t* dB, int rowsB);
 cudaError_t launch_side_gather(TcPlan* p, const CUtensorMap& mB, const SideArgs& a, cudaStream_t st);
 
+// Tensor-core voctree phase (v3dm_voctree_tc.cu): every work item (bucket b, first position,
+// count) descends `levels` (1 or 2) levels below its bucket node (bucketBase + b; the root when
+// bucketBase < 0) for the keys perm[first .. first + count) (positions themselves when perm is
+// null).  final: out[key] = the node reached (minus leafBase with V3DM_LEAF_LOCAL); else
+// next[key] = node - nextBase and hist[node - nextBase] counts it (bins buckets).
+struct VtcArgs {
+  const uint8_t* nodes;
+  int bf, levels;
+  long long bucketBase;
+  const int4* items;
+  const int* nItems;
+  int singleN;                   // > 0: one bucket of singleN keys (items and nItems unused)
+  const int32_t* perm;
+  const uint8_t* keys;
+  int final;
+  int32_t* out;
+  int idMode;
+  long long leafBase;
+  int32_t* next;
+  long long nextBase;
+  int* hist;
+  int bins;
+  int* err;
+};
+bool vtc_supported(int bf);
+// Rows of the tree read by the phases: a tensor map over the node rows with boxes of kVtcBoxRows;
+// the keys of a phase with singleN > 0: a map over the key rows with boxes of kVtcKeyBox rows.
+constexpr int kVtcBoxRows = 16;
+constexpr int kVtcKeyBox = 128;
+cudaError_t launch_vtc(const VtcArgs& a, const CUtensorMap& nodeMap, const CUtensorMap& keyMap, int grid,
+                       cudaStream_t st);
+// 2-D map over rows x 128 bytes with a box of boxRows rows and the 128-byte swizzle (v3dm_match_tc.cu).
+cudaError_t tc_rows_map(CUtensorMap* m, const uint8_t* base, int rows, int boxRows);
+
 // Gates of a batched guided call (v3dm_batch.cu): one gate per pair, evaluated on the fly from
 // the positions.  gm: per pair (caller's order) the 3x3 matrix as floats, then thr^2.
 constexpr int kBGateFloats = 10;

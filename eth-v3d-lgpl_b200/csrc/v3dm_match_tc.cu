@@ -862,6 +862,11 @@ using CfgG = Cfg6;
 int tc_gather_rows() { return CfgG::GM; }
 int tc_gather_cols() { return CfgG::BN; }
 
+cudaError_t tc_rows_map(CUtensorMap* m, const uint8_t* base, int rows, int boxRows) {
+  if (rows <= 0 || boxRows <= 0 || boxRows > 256) return cudaErrorInvalidValue;
+  return encode_rows(m, base, rows, boxRows) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t tc_gather_map(CUtensorMap* m, const uint8_t* dB, int rowsB) {
   if (rowsB <= 0) return cudaErrorInvalidValue;
   return encode_rows(m, dB, rowsB, CfgG::BN) ? cudaSuccess : cudaErrorInvalidValue;

@@ -6,11 +6,14 @@
 // (i+1)*BF .. (i+1)*BF + BF-1 (.cu:784-785).  Each level picks the child with the largest
 // dot product, the first child on ties (strict '>', .cu:781).
 //
-// Two kernels:
-//   - k_voctree: uint8 nodes and keys (u/512 in the reference's float convention).  Every dot
-//     product is an exact integer, so leaf ids match the reference whatever the summation
-//     order.
-//   - k_voctree_f32: float nodes and keys of any values (the apps' trees are float k-means
+// uint8 nodes and keys (u/512 in the reference's float convention): every dot product is an
+// exact integer, so leaf ids match the reference whatever the summation order.
+//   - the tensor-core descent (v3dm_voctree_tc.cu) when the shape allows it (BF <= 15, enough
+//     keys per bucket): phases of two levels, keys sorted by bucket between phases, each bucket's
+//     keys scored against its children and grandchildren with tcgen05 int8 GEMMs;
+//   - k_voctree otherwise: one launch, four threads per key (below).
+// Float nodes and keys of any value:
+//   - k_voctree_f32: float nodes and keys (the apps' trees are float k-means
 //     centres of unit-L2 descriptors, v3d_voctree.h:38-52).  The leaf ids equal those of the
 //     reference's CPU tree, VocabularyTree::findBestNodeIndex (v3d_voctree.h:82-99), which sums
 //     key[i] * node[i] sequentially for i = 0..127 in FP32 (one rounded product and one rounded
@@ -26,7 +29,7 @@
 //     (near ties, equal children, non-finite values) one thread of the key replays the
 //     reference's sequential FP32 loop over all children, with __fmul_rn / __fadd_rn.
 //
-// Kernel: four threads per key, each holding 32 bytes of the key in registers; a warp
+// k_voctree: four threads per key, each holding 32 bytes of the key in registers; a warp
 // descends eight keys.  At each level a thread loads its 32-byte slice of every child (each
 // child row is one 128-byte line read by the four threads together), forms eight dp4a
 // partial sums, and the four partials are summed with two butterfly shuffles.  The reference
@@ -34,6 +37,7 @@
 // reduction (.cu:770-779).  (Measured on the BF 10, depth 6 tree with 2M keys: 0.95 ms with
 // four threads per key, 1.18 ms with eight, 1.53 ms with two, 2.86 ms with one.)
 #include <algorithm>
+#include <cstring>
 #include <new>
 
 #include "v3dm_internal.h"
@@ -108,164 +112,17 @@ __global__ void k_vt_f32_to_u8(const float4* __restrict__ src, uint32_t* __restr
   if (!ok) atomicOr(err, 1);
 }
 
-// ---- bucketed descent of uint8 trees ------------------------------------------------------
-// Levels 1..L (the top) are descended by k_vt_top, with the top rows staged in shared memory
-// when they fit; the keys are then sorted by the node they reached (a counting sort over the
-// bf^L nodes of level L), and k_vt_sub descends the remaining T = depth - L levels bucket by
-// bucket: a CTA stages the bucket node's whole subtree (bf + bf^2 + ... + bf^T rows, contiguous
-// per level) in shared memory once and descends every key of the bucket against it.  Each node
-// row then leaves DRAM about once per call, instead of once per key that reaches it (the
-// one-kernel descent re-read the leaf level per key: 4.5x the algorithmic bytes).  The dot
-// products are exact integers, so the order of evaluation does not matter; ties keep the
-// first child (strict '>').
-constexpr int kVtRowsMax = 1600;        // rows of a staged subtree / top (200 KB)
-constexpr int kVtBktThreads = 512;
-constexpr int kVtItemKeys = 2048;       // keys per work item of k_vt_sub
-constexpr int kVtMaxSubLevels = 10;     // levels of a staged subtree
-constexpr int kVtLocalBins = 4096;      // bucket counts kept in shared memory by k_vt_top / k_vt_scatter
+// ---- bucketed descent of uint8 trees --------------------------------------------------------
+// Phases of two levels (v3dm_voctree_tc.cu): the first phase descends every key from the root,
+// each later one the keys of one bucket node at a time, the buckets being the nodes the previous
+// phase reached.  Between phases the keys are sorted by bucket (a counting sort: k_vt_scan,
+// then k_vt_scatter), and k_vt_scan cuts every bucket into work items of at most kVtItemKeys keys.
+constexpr int kVtItemKeys = 2048;       // keys per work item
+constexpr int kVtLocalBins = 16384;     // bucket counts kept in shared memory by k_vt_scatter (2 x 64 KB)
 
-// 16-byte chunk c of staged row r lives at r * 128 + ((c ^ (r & 7)) << 4): rows read by the
-// lanes of one instruction spread over the banks.
-__device__ __forceinline__ uint32_t vt_swz(int r, int c) { return (uint32_t)r * 128u + ((uint32_t)(c ^ (r & 7)) << 4); }
-
-__device__ __forceinline__ void vt_stage(uint8_t* smem, const uint8_t* __restrict__ src, long long rows, int dstRow0) {
-  const int n16 = (int)rows * 8;
-  for (int i = threadIdx.x; i < n16; i += blockDim.x) {
-    const int r = i >> 3, c = i & 7;
-    *reinterpret_cast<uint4*>(smem + vt_swz(dstRow0 + r, c)) = __ldg(reinterpret_cast<const uint4*>(src) + i);
-  }
-}
-
-// Best child of the bf rows starting at staged row `row0` for the key slice kw (four threads
-// per key, thread `part` holding chunks 2 part, 2 part + 1).  Children are scored kVtGroup at a
-// time with independent accumulators and shuffles (instruction-level parallelism: a CTA that
-// stages a whole subtree runs only 16 warps per SM); the comparisons keep index order.
-constexpr int kVtGroup = 5;
-__device__ __forceinline__ int vt_best_staged(const uint8_t* smem, int row0, int bf, const uint4 (&kw)[kQ], int part,
-                                              bool valid) {
-  int best = 0, bestScore = -1;
-  for (int c0 = 0; c0 < bf; c0 += kVtGroup) {
-    uint32_t acc[kVtGroup];
-    uint4 w[kVtGroup][kQ];
-#pragma unroll
-    for (int g = 0; g < kVtGroup; ++g) {
-      const int r = row0 + min(c0 + g, bf - 1);  // past the last child: re-read it, the score is ignored
-#pragma unroll
-      for (int q = 0; q < kQ; ++q) w[g][q] = *reinterpret_cast<const uint4*>(smem + vt_swz(r, part * kQ + q));
-    }
-#pragma unroll
-    for (int g = 0; g < kVtGroup; ++g) {
-      uint32_t a0 = 0, a1 = 0;
-      if (valid) {
-#pragma unroll
-        for (int q = 0; q < kQ; ++q) {
-          a0 = __dp4a(kw[q].x, w[g][q].x, a0);
-          a1 = __dp4a(kw[q].y, w[g][q].y, a1);
-          a0 = __dp4a(kw[q].z, w[g][q].z, a0);
-          a1 = __dp4a(kw[q].w, w[g][q].w, a1);
-        }
-      }
-      acc[g] = a0 + a1;
-    }
-#pragma unroll
-    for (int o = 1; o < kTpk; o <<= 1)
-#pragma unroll
-      for (int g = 0; g < kVtGroup; ++g) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], o);
-#pragma unroll
-    for (int g = 0; g < kVtGroup; ++g)
-      if (c0 + g < bf && (int)acc[g] > bestScore) {  // strict '>': the first child wins ties (.cu:781)
-        bestScore = (int)acc[g];
-        best = c0 + g;
-      }
-  }
-  return best;
-}
-
-__device__ __forceinline__ void vt_load_key(const uint8_t* __restrict__ keys, int key, int part, bool valid,
-                                            uint4 (&kw)[kQ]) {
-#pragma unroll
-  for (int q = 0; q < kQ; ++q)
-    kw[q] = valid ? __ldg(reinterpret_cast<const uint4*>(keys + (size_t)key * kDescBytes) + part * kQ + q)
-                  : make_uint4(0u, 0u, 0u, 0u);
-}
-
-// Levels 1..L of every key: bucket[key] = its level-L node minus the level's first index, and
-// the bucket histogram.  kStaged: the top rows (nodes 0 .. topRows-1) in shared memory.
-template <bool kStaged>
-__global__ void __launch_bounds__(kVtBktThreads)
-k_vt_top(const uint8_t* __restrict__ nodes, int bf, int L, long long topRows, long long levelStartL,
-         const uint8_t* __restrict__ keys, int n, int32_t* __restrict__ bucket, int* __restrict__ hist, int bins) {
-  extern __shared__ __align__(128) uint8_t vsm[];
-  // the bucket histogram is counted in shared memory (after the staged rows) and added to the
-  // global one once per CTA when it fits, else directly in global memory
-  int* shHist = reinterpret_cast<int*>(vsm + (kStaged ? topRows * kDescBytes : 0));
-  const bool local = bins <= kVtLocalBins;
-  if (local)
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) shHist[b] = 0;
-  if constexpr (kStaged) vt_stage(vsm, nodes, topRows, 0);
-  __syncthreads();
-  const int part = threadIdx.x % kTpk;
-  const int perIter = (gridDim.x * kVtBktThreads) / kTpk;
-  // the next iteration's key is loaded before this one is descended (the loads are the latency)
-  int k0 = (blockIdx.x * kVtBktThreads + threadIdx.x) / kTpk;
-  uint4 nw[kQ];
-  vt_load_key(keys, k0 < n ? k0 : 0, part, k0 < n, nw);
-  for (; k0 - (int)(threadIdx.x / kTpk) < n; k0 += perIter) {
-    const bool valid = k0 < n;
-    uint4 kw[kQ];
-#pragma unroll
-    for (int q = 0; q < kQ; ++q) kw[q] = nw[q];
-    const int kn = k0 + perIter;
-    vt_load_key(keys, kn < n ? kn : 0, part, kn < n, nw);
-    long long nextId = 0, leafId = 0;
-    for (int d = 0; d < L; ++d) {
-      int best;
-      if constexpr (kStaged) {
-        best = vt_best_staged(vsm, (int)nextId, bf, kw, part, valid);
-      } else {
-        const uint4* base = reinterpret_cast<const uint4*>(nodes + (size_t)nextId * kDescBytes) + part * kQ;
-        int bestScore = -1;
-        best = 0;
-        for (int c = 0; c < bf; ++c) {
-          uint32_t acc = 0;
-          if (valid) {
-#pragma unroll
-            for (int q = 0; q < kQ; ++q) {
-              const uint4 w = __ldg(base + (size_t)c * (kDescBytes / 16) + q);
-              acc = __dp4a(kw[q].x, w.x, acc);
-              acc = __dp4a(kw[q].y, w.y, acc);
-              acc = __dp4a(kw[q].z, w.z, acc);
-              acc = __dp4a(kw[q].w, w.w, acc);
-            }
-          }
-          int sc = (int)acc;
-#pragma unroll
-          for (int o = 1; o < kTpk; o <<= 1) sc += __shfl_xor_sync(0xffffffffu, sc, o);
-          if (sc > bestScore) {
-            bestScore = sc;
-            best = c;
-          }
-        }
-      }
-      leafId = nextId + best;
-      nextId = (leafId + 1) * bf;
-    }
-    if (valid && part == 0) {
-      const int b = (int)(leafId - levelStartL);
-      bucket[k0] = b;
-      atomicAdd(local ? &shHist[b] : &hist[b], 1);
-    }
-  }
-  if (local) {
-    __syncthreads();
-    for (int b = threadIdx.x; b < bins; b += blockDim.x)
-      if (shHist[b]) atomicAdd(&hist[b], shHist[b]);
-  }
-}
-
-// Bucket offsets and the work items of k_vt_sub: (bucket, first key in sorted order, count),
-// at most kVtItemKeys keys each.  One block.  With bins == 1 and single > 0, one bucket of
-// `single` keys (no top levels, no histogram).
+// Bucket offsets and the work items of a phase: (bucket, first key in sorted order, count), at
+// most kVtItemKeys keys each.  One block.  With bins == 1 and single > 0, one bucket of `single`
+// keys (the first phase: no histogram).
 __global__ void __launch_bounds__(1024)
 k_vt_scan(const int* __restrict__ hist, int bins, int single, int* __restrict__ off, int4* __restrict__ items,
           int* __restrict__ nItems) {
@@ -310,8 +167,9 @@ constexpr int kVtScatterThreads = 1024;
 __global__ void __launch_bounds__(kVtScatterThreads)
 k_vt_scatter(const int32_t* __restrict__ bucket, int n, const int* __restrict__ off, int* __restrict__ cursor,
              int32_t* __restrict__ perm, int bins) {
-  __shared__ int cnt[kVtLocalBins];
-  __shared__ int base[kVtLocalBins];
+  extern __shared__ int vtScatterSmem[];  // 2 x bins when bins <= kVtLocalBins
+  int* cnt = vtScatterSmem;
+  int* base = vtScatterSmem + bins;
   const long long per = ((long long)n + gridDim.x - 1) / gridDim.x;
   const int k0 = (int)min((long long)n, per * blockIdx.x), k1 = (int)min((long long)n, per * (blockIdx.x + 1));
   if (bins > kVtLocalBins) {  // too many buckets for shared memory: one global atomic per key
@@ -333,69 +191,6 @@ k_vt_scatter(const int32_t* __restrict__ bucket, int n, const int* __restrict__ 
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     const int b = bucket[k];
     perm[base[b] + atomicAdd(&cnt[b], 1)] = k;
-  }
-}
-
-// Levels L+1..depth, one work item at a time: the item's bucket node p (global index
-// levelStartL + bucket, or the root when L = 0) has its subtree staged (T levels, level t of
-// bf^(t+1) rows starting at global node g_t: g_0 = (p + 1) bf, g_(t+1) = (g_t + 1) bf), and
-// each key of the item descends it: at level t the local node idx has children idx * bf + c.
-__global__ void __launch_bounds__(kVtBktThreads)
-k_vt_sub(const uint8_t* __restrict__ nodes, int bf, int T, long long levelStartL, int haveTop,
-         const int4* __restrict__ items, const int* __restrict__ nItems, const int32_t* __restrict__ perm,
-         const uint8_t* __restrict__ keys, long long leafBase, int32_t* __restrict__ out, int idMode) {
-  extern __shared__ __align__(128) uint8_t vsm[];
-  const int part = threadIdx.x % kTpk;
-  const int nIt = *nItems;
-  int staged = -1;
-  for (int it = blockIdx.x; it < nIt; it += gridDim.x) {
-    const int4 item = items[it];
-    const long long p = haveTop ? levelStartL + item.x : -1;
-    long long g[kVtMaxSubLevels];
-    g[0] = (p + 1) * bf;
-    for (int t = 1; t < T; ++t) g[t] = (g[t - 1] + 1) * bf;
-    if (item.x != staged) {
-      __syncthreads();  // every key of the previous item is done with the staged rows
-      long long len = bf;
-      int row0 = 0;
-      for (int t = 0; t < T; ++t) {
-        vt_stage(vsm, nodes + (size_t)g[t] * kDescBytes, len, row0);
-        row0 += (int)len;
-        len *= bf;
-      }
-      __syncthreads();
-      staged = item.x;
-    }
-    constexpr int kStep = kVtBktThreads / kTpk;
-    auto key_at = [&](int kk) { return kk < item.z ? (perm ? __ldg(perm + item.y + kk) : item.y + kk) : 0; };
-    int k = threadIdx.x / kTpk;
-    int nkey = key_at(k), nnkey = key_at(k + kStep);
-    uint4 nw[kQ];
-    vt_load_key(keys, nkey, part, k < item.z, nw);
-    for (; k - (int)(threadIdx.x / kTpk) < item.z; k += kStep) {
-      // the next key and the index after it are loaded before this key is descended
-      const bool valid = k < item.z;
-      const int key = nkey;
-      uint4 kw[kQ];
-#pragma unroll
-      for (int q = 0; q < kQ; ++q) kw[q] = nw[q];
-      nkey = nnkey;
-      vt_load_key(keys, nkey, part, k + kStep < item.z, nw);
-      nnkey = key_at(k + 2 * kStep);
-      long long idx = 0;
-      int lvlRow = 0;
-      long long lvlLen = bf;
-      for (int t = 0; t < T; ++t) {
-        const int best = vt_best_staged(vsm, lvlRow + (int)(t == 0 ? 0 : idx * bf), bf, kw, part, valid);
-        idx = t == 0 ? best : idx * bf + best;
-        lvlRow += (int)lvlLen;
-        lvlLen *= bf;
-      }
-      if (valid && part == 0) {
-        const long long leafId = g[T - 1] + idx;
-        out[key] = (int32_t)(idMode == V3DM_LEAF_LOCAL ? leafId - leafBase : leafId);
-      }
-    }
   }
 }
 
@@ -580,90 +375,128 @@ struct v3dm_voctree {
   int32_t* dErr = nullptr;
   int32_t* hErr = nullptr;
   unsigned long long* dReplays = nullptr;  // key-levels resolved by the sequential replay
-  // bucketed descent of u8 trees: L top levels, T subtree levels (T = 0: one-kernel descent)
-  int L = 0, T = 0;
-  long long topRows = 0, subRows = 0, bins = 1, levelStartL = 0;
-  int32_t* dBucket = nullptr;   // nMax
-  int32_t* dPerm = nullptr;     // nMax
-  int* dHist = nullptr;         // bins, then bins cursors
-  int* dOff = nullptr;          // bins + 1
-  int4* dItems = nullptr;       // nMax / kVtItemKeys + bins + 1
+  // tensor-core descent of u8 trees in phases of two levels (tcPath false: one-kernel descent)
+  bool tcPath = false;
+  int phases = 0;
+  long long maxBins = 1;        // buckets of the last phase
+  int32_t* dBucket = nullptr;   // nMax: per key, the bucket it reached
+  int32_t* dPerm = nullptr;     // nMax: keys in bucket order
+  int* dHist = nullptr;         // maxBins counts, then maxBins cursors
+  int* dOff = nullptr;          // maxBins + 1
+  int4* dItems = nullptr;       // nMax / kVtItemKeys + maxBins + 1
   int* dNItems = nullptr;
   int numSMs = 148;
+  int lastLaunches = 0;         // kernels launched by the last quantization
+  CUtensorMap tmNodes;          // the u8 node rows for the tensor path's TMA loads
+  bool tmValid = false;
+  CUtensorMap tmKeys;           // the keys of the last call (first phase), for TMA tiles
+  const uint8_t* tmKeysPtr = nullptr;
+  int tmKeysRows = 0;
 };
 
 namespace {
 
-// Split of a u8 tree for the bucketed descent: the deepest T levels whose subtree fits the
-// shared-memory budget, the L = depth - T levels above them.
+// First global index of the nodes at depth d (1-based; the root has none).
+long long level_start(int bf, int d) {
+  long long start = 0, len = 1;
+  for (int k = 1; k < d; ++k) {
+    len *= bf;
+    start += len;
+  }
+  return start;
+}
+
+// Phases of the tensor-core descent: ceil(depth / 2), the last one's buckets are the nodes at
+// depth 2 (phases - 1).
 void vt_plan(v3dm_voctree* t) {
-  long long rows = 0, len = 1;
-  int T = 0;
-  while (T < t->depth && T < kVtMaxSubLevels) {
-    len *= t->bf;
-    if (rows + len > kVtRowsMax) break;
-    rows += len;
-    ++T;
-  }
-  t->T = T;
-  t->L = t->depth - T;
-  t->subRows = rows;
-  long long top = 0, l = 1, startL = 0;
-  for (int d = 0; d < t->L; ++d) {
-    startL = top;
-    l *= t->bf;
-    top += l;
-  }
-  t->topRows = top;
-  t->bins = t->L > 0 ? l : 1;
-  t->levelStartL = startL;
+  t->phases = (t->depth + 1) / 2;
+  long long bins = 1;
+  for (int k = 0; k < 2 * (t->phases - 1); ++k) bins *= t->bf;
+  t->maxBins = bins;
+  t->tcPath = vtc_supported(t->bf) && bins <= (1LL << 22);
 }
 
 int vt_launch(v3dm_voctree* t, int n, const uint8_t* dKeys, int32_t* dIds, int idMode) {
+  t->lastLaunches = 0;
   if (n == 0) return V3DM_OK;
-  if (t->T == 0 || !t->dPerm || n > t->nMax) {  // one-kernel descent
+  // the tensor path needs its buffers and enough keys per bucket of the last phase to fill
+  // 128-key tiles; otherwise the one-kernel descent
+  if (t->tcPath && !t->tmValid && t->dNodes &&
+      tc_rows_map(&t->tmNodes, t->dNodes, (int)t->nodeCount, kVtcBoxRows) == cudaSuccess)
+    t->tmValid = true;
+  if (!t->tcPath || !t->tmValid || !t->dPerm || n > t->nMax || (long long)n < 16 * t->maxBins) {
     long long threads = (long long)n * kTpk;
     unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
     k_voctree<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodes, t->bf, t->depth, t->leafBase, dKeys, n, dIds, idMode);
+    t->lastLaunches = 1;
     return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
   }
-  const int bins = (int)t->bins;
-  if (t->L > 0) {
-    if (cudaMemsetAsync(t->dHist, 0, 2 * (size_t)bins * sizeof(int), t->stream) != cudaSuccess) return V3DM_ERR_CUDA;
-    const long long keyBlocks = ((long long)n * kTpk + kVtBktThreads - 1) / kVtBktThreads;
-    const unsigned topGrid = (unsigned)std::min<long long>(keyBlocks, (long long)t->numSMs * 2);
-    const size_t histBytes = bins <= kVtLocalBins ? (size_t)bins * sizeof(int) : 0;
-    if (t->topRows <= kVtRowsMax) {
-      const size_t smem = (size_t)t->topRows * kDescBytes + histBytes;
-      k_vt_top<true><<<topGrid, kVtBktThreads, smem, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
-                                                                 t->levelStartL, dKeys, n, t->dBucket, t->dHist,
-                                                                 bins);
-    } else {
-      k_vt_top<false><<<topGrid, kVtBktThreads, histBytes, t->stream>>>(t->dNodes, t->bf, t->L, t->topRows,
-                                                                       t->levelStartL, dKeys, n, t->dBucket,
-                                                                       t->dHist, bins);
+  if (t->tmKeysPtr != dKeys || t->tmKeysRows != n) {
+    t->tmKeysPtr = nullptr;
+    if (tc_rows_map(&t->tmKeys, dKeys, n, kVtcKeyBox) == cudaSuccess) {
+      t->tmKeysPtr = dKeys;
+      t->tmKeysRows = n;
     }
-    if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
   }
-  k_vt_scan<<<1, 1024, 0, t->stream>>>(t->dHist, bins, t->L > 0 ? 0 : n, t->dOff, t->dItems, t->dNItems);
-  if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
-  if (t->L > 0) {
-    k_vt_scatter<<<(unsigned)std::max<long long>(1, std::min<long long>(((long long)n + 4095) / 4096,
-                                                                         (long long)t->numSMs * 2)),
-                   kVtScatterThreads, 0, t->stream>>>(t->dBucket, n, t->dOff, t->dHist + bins, t->dPerm, bins);
-    if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+  if (t->tmKeysPtr != dKeys) {  // keys a tensor map cannot describe (not 16-byte aligned)
+    long long threads = (long long)n * kTpk;
+    unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
+    k_voctree<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodes, t->bf, t->depth, t->leafBase, dKeys, n, dIds, idMode);
+    t->lastLaunches = 1;
+    return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
   }
-  const size_t smem = (size_t)t->subRows * kDescBytes;
-  const long long maxItems = (long long)n / kVtItemKeys + bins + 1;
-  const unsigned subGrid = (unsigned)std::min<long long>(maxItems, (long long)t->numSMs * (smem <= 100 * 1024 ? 2 : 1));
-  k_vt_sub<<<subGrid, kVtBktThreads, smem, t->stream>>>(t->dNodes, t->bf, t->T, t->levelStartL, t->L > 0, t->dItems,
-                                                        t->dNItems, t->L > 0 ? t->dPerm : nullptr, dKeys,
-                                                        t->leafBase, dIds, idMode);
-  return cudaGetLastError() == cudaSuccess ? V3DM_OK : V3DM_ERR_CUDA;
+  const int bf = t->bf;
+  VtcArgs va;
+  std::memset(&va, 0, sizeof(va));
+  va.nodes = t->dNodes;
+  va.bf = bf;
+  va.items = t->dItems;
+  va.nItems = t->dNItems;
+  va.keys = dKeys;
+  va.out = dIds;
+  va.idMode = idMode;
+  va.leafBase = t->leafBase;
+  va.next = t->dBucket;
+  va.hist = t->dHist;
+  va.err = t->dErr;
+  long long bins = 1;
+  for (int p = 0; p < t->phases; ++p) {
+    const int levels = std::min(2, t->depth - 2 * p);
+    const bool last = p == t->phases - 1;
+    const long long nextBins = bins * bf * bf;
+    if (p > 0) {
+      // keys sorted by the bucket the previous phase reached
+      k_vt_scan<<<1, 1024, 0, t->stream>>>(t->dHist, (int)bins, 0, t->dOff, t->dItems, t->dNItems);
+      if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+      if (cudaMemsetAsync(t->dHist + t->maxBins, 0, (size_t)bins * sizeof(int), t->stream) != cudaSuccess)
+        return V3DM_ERR_CUDA;
+      const unsigned sg = (unsigned)std::max<long long>(
+          1, std::min<long long>(((long long)n + 4095) / 4096, (long long)t->numSMs * 2));
+      const size_t ssm = bins <= kVtLocalBins ? 2 * (size_t)bins * sizeof(int) : 0;
+      k_vt_scatter<<<sg, kVtScatterThreads, ssm, t->stream>>>(t->dBucket, n, t->dOff, t->dHist + t->maxBins, t->dPerm,
+                                                              (int)bins);
+      if (cudaGetLastError() != cudaSuccess) return V3DM_ERR_CUDA;
+    }
+    if (!last && cudaMemsetAsync(t->dHist, 0, (size_t)nextBins * sizeof(int), t->stream) != cudaSuccess)
+      return V3DM_ERR_CUDA;
+    va.levels = levels;
+    va.singleN = p == 0 ? n : 0;  // the first phase: one bucket (the root), items implied
+    va.bucketBase = p == 0 ? -1 : level_start(bf, 2 * p);
+    va.perm = p == 0 ? nullptr : t->dPerm;
+    va.final = last ? 1 : 0;
+    va.nextBase = last ? 0 : level_start(bf, 2 * p + 2);
+    va.bins = last ? 0 : (int)nextBins;
+    if (launch_vtc(va, t->tmNodes, t->tmKeys, t->numSMs, t->stream) != cudaSuccess) return V3DM_ERR_CUDA;
+    t->lastLaunches += p == 0 ? 1 : 3;  // scan and scatter (after the first phase), the phase
+    bins = nextBins;
+  }
+  return V3DM_OK;
 }
 
 int vt_launch_f32(v3dm_voctree* t, int n, const float* dKeys, int32_t* dIds, int idMode) {
+  t->lastLaunches = 0;
   if (n == 0) return V3DM_OK;
+  t->lastLaunches = 1;
   long long threads = (long long)n * kTpk;
   unsigned blocks = (unsigned)((threads + kVtThreads - 1) / kVtThreads);
   k_voctree_f32<<<blocks, kVtThreads, 0, t->stream>>>(t->dNodesF, t->dNorm, t->nodeCount, t->bf, t->depth,
@@ -768,13 +601,12 @@ int v3dm_voctree_create(v3dm_voctree** out, int device, int bf, int depth) {
       cudaMalloc(reinterpret_cast<void**>(&t->dReplays), sizeof(unsigned long long)) != cudaSuccess ||
       cudaMemsetAsync(t->dErr, 0, sizeof(int32_t), t->stream) != cudaSuccess ||
       cudaMemsetAsync(t->dReplays, 0, sizeof(unsigned long long), t->stream) != cudaSuccess ||
-      (t->T > 0 && (cudaMalloc(reinterpret_cast<void**>(&t->dHist), 2 * (size_t)t->bins * sizeof(int)) != cudaSuccess ||
-                    cudaMalloc(reinterpret_cast<void**>(&t->dOff), ((size_t)t->bins + 1) * sizeof(int)) != cudaSuccess ||
-                    cudaMalloc(reinterpret_cast<void**>(&t->dNItems), sizeof(int)) != cudaSuccess ||
-                    cudaFuncSetAttribute(k_vt_top<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kVtRowsMax * kDescBytes + kVtLocalBins * (int)sizeof(int)) != cudaSuccess ||
-                    cudaFuncSetAttribute(k_vt_sub, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kVtRowsMax * kDescBytes) != cudaSuccess)) ||
+      (t->tcPath &&
+       (cudaMalloc(reinterpret_cast<void**>(&t->dHist), 2 * (size_t)t->maxBins * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&t->dOff), ((size_t)t->maxBins + 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&t->dNItems), sizeof(int)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_vt_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kVtLocalBins * (int)sizeof(int)) != cudaSuccess)) ||
       cudaStreamSynchronize(t->stream) != cudaSuccess) {
     if (t->stream) cudaStreamDestroy(t->stream);
     if (t->dErr) cudaFree(t->dErr);
@@ -835,10 +667,11 @@ int v3dm_voctree_allocate(v3dm_voctree* t, int nMax) {
       cudaMalloc(reinterpret_cast<void**>(&t->dStage), m * kDescBytes * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&t->dIds), m * sizeof(int32_t)) != cudaSuccess)
     return V3DM_ERR_CUDA;
-  if (t->T > 0 &&
+  if (t->tcPath &&
       (cudaMalloc(reinterpret_cast<void**>(&t->dBucket), m * sizeof(int32_t)) != cudaSuccess ||
        cudaMalloc(reinterpret_cast<void**>(&t->dPerm), m * sizeof(int32_t)) != cudaSuccess ||
-       cudaMalloc(reinterpret_cast<void**>(&t->dItems), (m / kVtItemKeys + t->bins + 1) * sizeof(int4)) != cudaSuccess))
+       cudaMalloc(reinterpret_cast<void**>(&t->dItems), (m / kVtItemKeys + t->maxBins + 1) * sizeof(int4)) !=
+           cudaSuccess))
     return V3DM_ERR_CUDA;
   t->nMax = nMax;
   return V3DM_OK;
@@ -957,6 +790,12 @@ int v3dm_voctree_replays(v3dm_voctree* t, long long* n) {
       cudaStreamSynchronize(t->stream) != cudaSuccess)
     return V3DM_ERR_CUDA;
   *n = (long long)v;
+  return V3DM_OK;
+}
+
+int v3dm_voctree_last_launches(v3dm_voctree* t, int* n) {
+  if (!t || !n) return V3DM_ERR_ARG;
+  *n = t->lastLaunches;
   return V3DM_OK;
 }
 

@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         L.v3dm_voctree_quantize_f32_device.argtypes = [vp, i32, vp, vp, i32]
         L.v3dm_voctree_replays.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.v3dm_voctree_stream.argtypes = [vp, C.POINTER(vp)]
+        L.v3dm_voctree_last_launches.argtypes = [vp, C.POINTER(i32)]
         i64, i64p = C.c_longlong, C.POINTER(C.c_longlong)
         L.v3dm_batch_create.argtypes = [C.POINTER(vp), i32]
         L.v3dm_batch_destroy.argtypes = [vp]
@@ -414,6 +415,12 @@ class VocabularyTreeTraversal:
 
     __del__ = close
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def get_node_count(self) -> int:
         return voctree_counts(self.branch_factor, self.depth)[0]
 
@@ -459,6 +466,12 @@ class VocabularyTreeTraversal:
         s = C.c_void_p()
         _check(lib().v3dm_voctree_stream(self._h, C.byref(s)), "stream")
         return s.value or 0
+
+    def last_launches(self) -> int:
+        """Kernels launched by the last quantization call."""
+        n = C.c_int32(0)
+        _check(lib().v3dm_voctree_last_launches(self._h, C.byref(n)), "last_launches")
+        return n.value
 
 
 class BatchMatching:

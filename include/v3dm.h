@@ -361,6 +361,8 @@ V3DM_API int v3dm_voctree_quantize_f32_device(v3dm_voctree* t, int n, const floa
  * decide from the fast pass and were replayed in the reference's sequential order. */
 V3DM_API int v3dm_voctree_replays(v3dm_voctree* t, long long* n);
 V3DM_API int v3dm_voctree_stream(v3dm_voctree* t, void** stream);
+/* Kernels launched by the last quantization call (the float conversion of float keys excluded). */
+V3DM_API int v3dm_voctree_last_launches(v3dm_voctree* t, int* n);
 
 /* ---- feature files ------------------------------------------------------------------ */
 /* serializeDataFromFile(path, SerializableVector<SIFT_Feature>&) (v3d_serialization.h:983-1017;

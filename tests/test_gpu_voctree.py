@@ -28,6 +28,25 @@ def test_quantize_matches_oracle(v3dm_mod, oracle_mod, bf, depth, n):
     t2.close()
 
 
+@pytest.mark.parametrize("bf,depth,n,vmax", [(2, 6, 5000, 3), (5, 4, 20000, 2), (11, 4, 30000, 255), (15, 2, 5000, 1),
+                                             (10, 5, 200000, 4), (3, 1, 100, 255), (13, 3, 12000, 255)])
+def test_tensor_descent_shapes_and_ties(v3dm_mod, oracle_mod, bf, depth, n, vmax):
+    """Shapes the tensor-core descent takes (two levels per phase, 128-key tiles, the chosen
+    child's grandchildren selected out of all BF^2 scores) with values drawn from 0..vmax: small
+    vmax makes equal scores common, so the first-child rule is exercised at every level; 255 gives
+    the largest scores."""
+    rng = synth.rng_for(7000 + bf * 10 + depth)
+    nodes = rng.integers(0, vmax + 1, (v3dm_mod.voctree_counts(bf, depth)[0], 128)).astype(np.uint8)
+    keys = rng.integers(0, vmax + 1, (n, 128)).astype(np.uint8)
+    keys[0] = 0  # a zero key ties everywhere
+    keys[1] = vmax
+    with v3dm_mod.VocabularyTreeTraversal(bf, depth) as t:
+        t.allocate(n)
+        t.set_nodes(nodes)
+        for mode, glob in ((v3dm_mod.LEAF_GLOBAL, True), (v3dm_mod.LEAF_LOCAL, False)):
+            np.testing.assert_array_equal(t.traverse_tree(keys, mode), oracle_mod.voctree(bf, depth, nodes, keys, glob))
+
+
 def test_ties_take_first_child(v3dm_mod, oracle_mod):
     bf, depth = 4, 2
     nodes = np.zeros((20, 128), np.uint8)
