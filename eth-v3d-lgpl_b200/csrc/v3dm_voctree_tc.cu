@@ -498,7 +498,9 @@ __global__ void __launch_bounds__(kVtcThreads, 1)
       } else {
         const int bkt = (int)(node - a.nextBase);
         a.next[key] = bkt;
-        atomicAdd(localHist ? &s.hist[bkt] : &a.hist[bkt], 1);
+        // one update per distinct bucket of the warp (keys of a tile often share buckets)
+        const unsigned peers = __match_any_sync(__activemask(), bkt);
+        if (lane == __ffs(peers) - 1) atomicAdd(localHist ? &s.hist[bkt] : &a.hist[bkt], __popc(peers));
       }
     }
   }
