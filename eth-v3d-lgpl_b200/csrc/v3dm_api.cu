@@ -1101,6 +1101,7 @@ int v3dm_guided_H(v3dm_matcher* h, const double* H, float thr, const float* lpos
 
 int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count) {
   if (!h || !d_pairs || !d_count) return V3DM_ERR_ARG;
+  if (!dev_aligned(d_pairs, 8) || !dev_aligned(d_count, 4)) return V3DM_ERR_ARG;  // pairs are written as int2
   if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
   DeviceGuard g(h->device);
   h->nGates = 0;
@@ -1116,6 +1117,9 @@ int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_
 int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, const float* d_lpos, const float* d_rpos,
                          float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count) {
   if (!h || !F || !d_pairs || !d_count) return V3DM_ERR_ARG;
+  // pairs are written as int2, positions read as float2
+  if (!dev_aligned(d_pairs, 8) || !dev_aligned(d_count, 4) || !dev_aligned(d_lpos, 8) || !dev_aligned(d_rpos, 8))
+    return V3DM_ERR_ARG;
   if (!h->allocated) return V3DM_ERR_NOT_ALLOCATED;
   DeviceGuard g(h->device);
   int st = add_gate(h, 1, F, thr, d_lpos, d_rpos, true);

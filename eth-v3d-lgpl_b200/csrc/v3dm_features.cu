@@ -313,6 +313,7 @@ int v3dm_features_read(const char* path, int cap, int32_t* n, int32_t* ids, floa
 
 int v3dm_quantize_u8_device(const float* d_values, long long nValues, uint8_t* d_out, void* stream) {
   if (nValues < 0 || (nValues > 0 && (!d_values || !d_out))) return V3DM_ERR_ARG;
+  if (!dev_aligned(d_values, 16) || !dev_aligned(d_out, 4)) return V3DM_ERR_ARG;  // float4 in, uchar4 out
   if (nValues % 4 != 0) return V3DM_ERR_ARG;
   V3DM_LTRY(launch_quantize_u8(d_values, nValues, d_out, static_cast<cudaStream_t>(stream)));
   return V3DM_OK;

@@ -282,6 +282,9 @@ cudaError_t proj_assign(const v3dm_projection* p, const uint8_t* dDesc, long lon
 int proj_cells(const v3dm_projection* p);
 cudaStream_t proj_stream(const v3dm_projection* p);
 
+// Whether a caller's device buffer meets the alignment its kernels access it with (a power of two).
+inline bool dev_aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+
 // Records the detail v3dm_last_error() reports for this thread (v3dm_api.cu).
 void record_cuda_error(cudaError_t e, const char* file, int line, const char* what);
 // Smallest integer score S whose float score S * 2^-18 passes 's > minScore' (v3dm_api.cu).

@@ -89,6 +89,9 @@ extern "C" int v3dm_putative_u8_noalloc(int device, const uint8_t* d_left, int n
   if (nLeft < 0 || nRight < 0 || !d_count || (nLeft > 0 && !d_left) || (nRight > 0 && !d_right) ||
       (nLeft > 0 && nRight > 0 && !d_pairs) || device < 0 || device >= 128)
     return V3DM_ERR_ARG;
+  // descriptors are read as 32-bit words, pairs written as int2
+  if (!dev_aligned(d_left, 4) || !dev_aligned(d_right, 4) || !dev_aligned(d_pairs, 8) || !dev_aligned(d_count, 4))
+    return V3DM_ERR_ARG;
   if (nLeft > kNoAllocMaxFeatures || nRight > kNoAllocMaxFeatures) return V3DM_ERR_SIZE;
   int nDev = 0;
   if (cudaGetDeviceCount(&nDev) != cudaSuccess) return V3DM_ERR_NO_DEVICE;

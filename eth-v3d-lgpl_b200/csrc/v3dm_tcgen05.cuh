@@ -40,6 +40,22 @@ __device__ __forceinline__ bool mbar_try(unsigned long long* b, uint32_t parity)
   return ok != 0;
 }
 
+// As mbar_try, but a thread whose phase is not complete is suspended by the hardware until the
+// phase completes or about kSuspendNs pass, instead of returning at once: a waiting thread then
+// takes no issue slots from the warps it shares its sub-partition with.
+constexpr uint32_t kSuspendNs = 1000000;  // 1 ms: the bounded waits still notice an abort or a timeout
+__device__ __forceinline__ bool mbar_try_sleep(unsigned long long* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(kSuspendNs)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait for the phase with the given parity.  Returns false on timeout or when
 // another role of the CTA has aborted.
 __device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity, int* abortFlag, int* err,
@@ -47,7 +63,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity
   if (mbar_try(b, parity)) return true;
   long long t0 = clock64();
   while (true) {
-    if (mbar_try(b, parity)) return true;
+    if (mbar_try_sleep(b, parity)) return true;
     if (*reinterpret_cast<volatile int*>(abortFlag)) return false;
     if (clock64() - t0 > limit) {
       atomicOr(err, kErrWaitTimeout);

@@ -764,9 +764,13 @@ int v3dm_voctree_quantize_f32(v3dm_voctree* t, int n, const float* keys, int32_t
   return vt_check_err(t);
 }
 
+// Device buffers of the quantize calls: keys read as 16-byte vectors, ids written as int32.
+bool vt_aligned(const void* keys, const void* ids) { return dev_aligned(keys, 16) && dev_aligned(ids, 4); }
+
 int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode) {
   if (!t || n < 0 || (n > 0 && (!d_keys || !d_ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
     return V3DM_ERR_ARG;
+  if (n > 0 && !vt_aligned(d_keys, d_ids)) return V3DM_ERR_ARG;
   if (!t->nodesU8) return t->nodesF ? V3DM_ERR_NOT_U8 : V3DM_ERR_NOT_ALLOCATED;
   DeviceGuardVt g(t->device);
   return vt_launch(t, n, d_keys, d_ids, idMode);
@@ -775,6 +779,7 @@ int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_key
 int v3dm_voctree_quantize_f32_device(v3dm_voctree* t, int n, const float* d_keys, int32_t* d_ids, int idMode) {
   if (!t || n < 0 || (n > 0 && (!d_keys || !d_ids)) || (idMode != V3DM_LEAF_GLOBAL && idMode != V3DM_LEAF_LOCAL))
     return V3DM_ERR_ARG;
+  if (n > 0 && !vt_aligned(d_keys, d_ids)) return V3DM_ERR_ARG;
   if (!(t->nodesU8 || t->nodesF)) return V3DM_ERR_NOT_ALLOCATED;
   DeviceGuardVt g(t->device);
   int st = vt_ensure_float_tree(t);

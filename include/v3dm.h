@@ -131,8 +131,9 @@ V3DM_API int v3dm_guided_H(v3dm_matcher* h, const double* H, float thr, const fl
                   float minScore, float minRatio, int32_t* pairs, int cap, int* nOut);
 
 /* Device-resident variants (no host copies, no synchronisation): the result is written to
- * device memory on the handle's stream.  d_pairs holds 2*min(nLeft, nRight) int32,
- * d_count one int32.  Used to time the kernels with inputs resident in HBM. */
+ * device memory on the handle's stream.  d_pairs holds 2*min(nLeft, nRight) int32 (8-byte
+ * aligned), d_count one int32, positions 2 floats per feature (8-byte aligned); misaligned
+ * buffers give V3DM_ERR_ARG.  Used to time the kernels with inputs resident in HBM. */
 V3DM_API int v3dm_putative_device(v3dm_matcher* h, float minScore, float minRatio, int32_t* d_pairs, int32_t* d_count);
 V3DM_API int v3dm_guided_F_device(v3dm_matcher* h, const double* F, float thr, const float* d_leftPos,
                          const float* d_rightPos, float minScore, float minRatio, int32_t* d_pairs,
@@ -191,7 +192,8 @@ V3DM_API int v3dm_candidate_threshold(float minScore, float minRatio, int gated,
  * V3DM_NOALLOC_MAX_CANDIDATES scores at or above the candidate threshold per call.
  * All calls share the one array: calls that overlap on the GPU race, so serialise them.
  * The first call on a device looks up the array's address (cudaGetSymbolAddress with that
- * device current); make it before any stream capture begins. */
+ * device current); make it before any stream capture begins.  Descriptors 4-byte aligned,
+ * d_pairs 8-byte aligned (else V3DM_ERR_ARG). */
 #define V3DM_NOALLOC_MAX_FEATURES 8192
 #define V3DM_NOALLOC_MAX_CANDIDATES 524288
 V3DM_API int v3dm_putative_u8_noalloc(int device, const uint8_t* d_left, int nLeft, const uint8_t* d_right, int nRight,
@@ -352,8 +354,9 @@ V3DM_API int v3dm_voctree_set_nodes_u8(v3dm_voctree* t, const uint8_t* nodes);
  * V3DM_ERR_ARG when the tree holds values that make a descent leave the node array. */
 V3DM_API int v3dm_voctree_quantize_f32(v3dm_voctree* t, int n, const float* keys, int32_t* ids, int idMode);
 V3DM_API int v3dm_voctree_quantize_u8(v3dm_voctree* t, int n, const uint8_t* keys, int32_t* ids, int idMode);
-/* Device-resident variants: keys and ids in device memory, asynchronous on the tree's stream.
- * The u8 variant needs a u/512 tree (else V3DM_ERR_NOT_U8). */
+/* Device-resident variants: keys and ids in device memory, asynchronous on the tree's stream;
+ * keys 16-byte aligned and ids 4-byte aligned (else V3DM_ERR_ARG).  The u8 variant needs a u/512
+ * tree (else V3DM_ERR_NOT_U8). */
 V3DM_API int v3dm_voctree_quantize_u8_device(v3dm_voctree* t, int n, const uint8_t* d_keys, int32_t* d_ids, int idMode);
 V3DM_API int v3dm_voctree_quantize_f32_device(v3dm_voctree* t, int n, const float* d_keys, int32_t* d_ids,
                                               int idMode);
@@ -379,8 +382,9 @@ V3DM_API int v3dm_voctree_last_launches(v3dm_voctree* t, int* n);
 V3DM_API int v3dm_features_read(const char* path, int cap, int32_t* n, int32_t* ids, float* positions,
                                 float* directions, float* scales, float* magnitudes, float* descriptors);
 /* u8 re-quantisation on the device: out = round(512 * x) (half to even) clamped to 0..255,
- * NaN -> 0; the identity for descriptors of the form u/512.  nValues a multiple of 4.  No
- * counterpart in the reference (its matcher takes the floats). */
+ * NaN -> 0; the identity for descriptors of the form u/512.  nValues a multiple of 4; d_values
+ * 16-byte and d_out 4-byte aligned (else V3DM_ERR_ARG).  No counterpart in the reference (its
+ * matcher takes the floats). */
 V3DM_API int v3dm_quantize_u8_device(const float* d_values, long long nValues, uint8_t* d_out, void* stream);
 
 /* Loader: the apps read one feature file per image and copy each pair's descriptors to the

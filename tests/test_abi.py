@@ -74,3 +74,22 @@ def test_header_is_plain_c_and_links(v3dm_mod, tmp_path):
                     "-lv3dm", f"-Wl,-rpath,{v3dm_mod.LIB_PATH.parent}"], check=True, capture_output=True, text=True)
     r = subprocess.run([str(out)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and int(r.stdout) == len(names)
+
+
+def test_misaligned_device_buffers_are_rejected(v3dm_mod):
+    """Device buffers that the kernels access as vectors must be aligned for them; a misaligned
+    one is an argument error before any device work (checked here without a GPU; the tree's
+    device calls are checked in tests/test_gpu_voctree.py)."""
+    import ctypes as C
+    lib = v3dm_mod.lib()
+    fn = lib.v3dm_putative_u8_noalloc
+    fn.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                   C.c_void_p, C.c_void_p]
+    ok, odd4, odd8 = 4096, 4096 + 2, 4096 + 4  # fake device addresses: aligned, off by 2, 4-aligned only
+    for left, right, pairs, count in ((odd4, ok, ok, ok), (ok, odd4, ok, ok), (ok, ok, odd8, ok), (ok, ok, ok, odd4)):
+        st = fn(0, C.c_void_p(left), 10, C.c_void_p(right), 10, 0.7, 0.8, C.c_void_p(pairs), C.c_void_p(count), None)
+        assert st == v3dm_mod.ERR_ARG, (left, right, pairs, count)
+    q = lib.v3dm_quantize_u8_device
+    q.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
+    assert q(C.c_void_p(odd8), 8, C.c_void_p(ok), None) == v3dm_mod.ERR_ARG      # floats read as float4
+    assert q(C.c_void_p(ok), 8, C.c_void_p(odd4), None) == v3dm_mod.ERR_ARG      # bytes written as uchar4

@@ -157,3 +157,28 @@ def test_config_tree_all_queries(v3dm_mod, oracle_mod):
     else:
         exp = oracle_mod.voctree(10, 6, nodes, keys, False)
     np.testing.assert_array_equal(got, exp)
+
+
+def test_device_calls_reject_misaligned_buffers(v3dm_mod):
+    """The device entry points read keys as 16-byte vectors and write int32 ids: misaligned
+    buffers are an argument error, not a device fault."""
+    import ctypes as C
+    import torch
+    dev = torch.device("cuda", 0)
+    bf, depth, n = 4, 3, 100
+    nodes = synth.sift_like(synth.rng_for(9), v3dm_mod.voctree_counts(bf, depth)[0])
+    keys = torch.from_numpy(synth.sift_like(synth.rng_for(10), n + 1)).to(dev)
+    ids = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+    with v3dm_mod.VocabularyTreeTraversal(bf, depth) as t:
+        t.allocate(n)
+        t.set_nodes(nodes)
+        L = v3dm_mod.lib()
+        base_k, base_i = keys.data_ptr(), ids.data_ptr()
+        assert L.v3dm_voctree_quantize_u8_device(t._h, n, C.c_void_p(base_k), C.c_void_p(base_i), 0) == v3dm_mod.OK
+        for dk, di in ((base_k + 8, base_i), (base_k + 1, base_i), (base_k, base_i + 2)):
+            st = L.v3dm_voctree_quantize_u8_device(t._h, n, C.c_void_p(dk), C.c_void_p(di), 0)
+            assert st == v3dm_mod.ERR_ARG, (dk - base_k, di - base_i)
+        fk = torch.zeros((n + 1) * 128 + 4, dtype=torch.float32, device=dev)
+        st = L.v3dm_voctree_quantize_f32_device(t._h, n, C.c_void_p(fk.data_ptr() + 4), C.c_void_p(base_i), 0)
+        assert st == v3dm_mod.ERR_ARG
+        torch.cuda.synchronize()
