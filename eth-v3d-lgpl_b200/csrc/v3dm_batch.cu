@@ -23,6 +23,11 @@
 // passes, the pair's gate applied on the fly wherever a score can decide (the chunk records,
 // k_records), and an exact warp re-score (k_brescore) of the few descriptors whose gated
 // second value the side pass could only bound.
+// Float descriptors that are not all of the form u/512 (v3dm_batch_set_images_f32) take the same
+// passes on the BF16 hi/lo layouts of the single-pair float matcher (v3dm_match_f.cu): groups of
+// 128 lefts against tiles of 64 columns, each descriptor's exact best and second over the other
+// image kept in registers and decided with the float rules, so each pair's result equals that
+// matcher's.
 // Every launch after the first reads its sizes from device memory, so the whole sequence is
 // captured once as a CUDA graph and replayed while the images, pairs and parameters stay the same.
 #include <algorithm>
@@ -188,12 +193,15 @@ k_bscan(const int* __restrict__ cnt, int nPairs, const BImage* __restrict__ im, 
 }
 
 // Gathers, per pair and in ascending left order, the right named by every accepted left into
-// the pass-B operand buffer, with its (pair, left, right) identity.
+// the pass-B operand buffer, with its (pair, left, right) identity.  A row is 'planes' blocks of
+// 128 bytes, block p of row r at (p * planeRows + r) * 128 (one block: uint8 descriptors; six:
+// the planar BF16 hi/lo layout).
 __global__ void __launch_bounds__(kChooseThreads)
 k_bchoose(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict__ im,
           const BImageB* __restrict__ imgB, const long long* __restrict__ prefC, const int32_t* __restrict__ decA,
           const uint8_t* __restrict__ img, uint8_t* __restrict__ dAB, int* __restrict__ chosenLeft,
-          int* __restrict__ chosenRight, int* __restrict__ chosenPair, const int* __restrict__ counters) {
+          int* __restrict__ chosenRight, int* __restrict__ chosenPair, const int* __restrict__ counters, int planes,
+          long long srcPlaneRows, long long dstPlaneRows) {
   __shared__ int wsum[kChooseThreads / 32];
   if (counters[kCntOverflow]) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -224,10 +232,13 @@ k_bchoose(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict_
         chosenLeft[st] = l;
         chosenRight[st] = d;
         chosenPair[st] = q.orig;
-        const uint4* src = reinterpret_cast<const uint4*>(img + ((size_t)rRowOff + d) * kDescBytes);
-        uint4* dst = reinterpret_cast<uint4*>(dAB + (size_t)(rowBase + k) * kDescBytes);
+        for (int p = 0; p < planes; ++p) {
+          const uint4* src =
+              reinterpret_cast<const uint4*>(img + ((size_t)p * srcPlaneRows + rRowOff + d) * kDescBytes);
+          uint4* dst = reinterpret_cast<uint4*>(dAB + ((size_t)p * dstPlaneRows + rowBase + k) * kDescBytes);
 #pragma unroll
-        for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = src[x];
+          for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = src[x];
+        }
       }
       run += tot;
       __syncthreads();
@@ -882,6 +893,21 @@ struct v3dm_batch {
   long long pairAuxCap = 0;
   int* dFlag = nullptr;             // flagged states of one pass
   long long flagCap = 0;
+  // float descriptors not all of the form u/512: BF16 hi/lo layouts (6 planes of fRows x 128 B)
+  bool floatMode = false;
+  int numSMs = 0;
+  float* dStageF = nullptr;         // the caller's floats, staged
+  long long stageFCap = 0;          // floats
+  int* dRowOffI = nullptr;          // per image: first row (device copy of rowOff)
+  long long rowOffCap = 0;
+  uint8_t* dFA = nullptr;           // A layout of every image: [hi | lo | hi]
+  uint8_t* dFB = nullptr;           // B layout of every image: [hi | hi | lo]
+  long long fImgCapA = 0, fImgCapB = 0;  // bytes
+  int fRows = 0;                    // rows per plane of dFA / dFB
+  uint8_t* dFAB = nullptr;          // pass-B A operand: the chosen rights' A rows, capRowsB rows per plane
+  long long fabCap = 0;             // bytes
+  CUtensorMap fmA_A, fmA_B, fmB_A, fmB_B;
+  bool fMapsValid = false;
   // profiling
   bool profile = false;
   cudaEvent_t ev[4] = {};
@@ -993,14 +1019,15 @@ cudaError_t alloc_passB(v3dm_batch* b, long long capStates) {
   b->capRowsB = capRows;
   b->capTableB = capTable;
   b->mapsValid = false;
+  b->fMapsValid = false;
   return cudaSuccess;
 }
 
-// Pass-A rows for the current configuration.
-int build_rows(v3dm_batch* b) {
-  int GM = 0, BN = 0;
-  const int cfg = tc_get_config(b->tc);
-  tc_config_shape(cfg, &GM, &BN);
+// Row-table key of the float passes (the integer ones use the tile configuration).
+constexpr int kFloatRowsCfg = -2;
+
+// Pass-A rows for groups of GM lefts and tiles of BN columns; cfg names the shape.
+int build_rows(v3dm_batch* b, int GM, int BN, int cfg) {
   std::vector<BatchRow> rows;
   for (const BPair& q : b->bp) {
     const int nR = b->counts[q.ri];
@@ -1114,7 +1141,7 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   V3DM_BTRY(cudaGetLastError());
   k_bchoose<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, b->dImgB, b->dPrefC,
                                                           b->dDecA, b->dImg, b->dAB, b->dChosenLeft, b->dChosenRight,
-                                                          b->dChosenPair, b->dCounters);
+                                                          b->dChosenPair, b->dCounters, 1, 0, 0);
   V3DM_BTRY(cudaGetLastError());
   launches += 3;
   // ---- pass B: the rights the accepted lefts named, against their left image
@@ -1154,10 +1181,96 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
   return V3DM_OK;
 }
 
+// Enqueues one batch call on the float layouts: the passes of enqueue_batch with the float side
+// kernel, which writes every state's decision itself (one CTA scores a whole row, so the exact
+// best and second of each descriptor stay in registers): no chunk records, no re-score.
+int enqueue_batch_f(v3dm_batch* b, float minScore, float minRatio, bool withEvents) {
+  const int GM = f_group_rows(), BN = f_tile_cols();
+  const float Tf = host_float_threshold(minScore, minRatio);
+  int launches = 0;
+  V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
+  // pairs whose right image is empty have no rows: their lefts decide 'none'
+  V3DM_BTRY(cudaMemsetAsync(b->dDecA, 0xff, (size_t)std::max<long long>(b->SA, 1) * sizeof(int32_t), b->stream));
+  SideArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.err = b->dInfo + kInfoErr;
+  sa.minScore = minScore;
+  sa.minRatio = minRatio;
+  // ---- pass A: every (pair, group of 128 lefts) against the pair's right image
+  sa.aIsLeft = 1;
+  sa.rows = b->dRowsA;
+  sa.nRows = b->nRowsA;
+  sa.decision = b->dDecA;
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[0], b->stream));
+  V3DM_BTRY(launch_side_f_batch(b->fmA_A, b->fmA_B, sa, Tf, b->numSMs, b->stream));
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[1], b->stream));
+  launches += b->nRowsA > 0;
+  // ---- pass-B layout: the chosen rights' A rows (six planes)
+  const int chooseGrid = std::max(1, std::min(b->nPairs, 4 * 148));
+  k_bcount<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dDecA, b->dCnt);
+  V3DM_BTRY(cudaGetLastError());
+  k_bscan<<<1, kScanThreads, 0, b->stream>>>(b->dCnt, b->nPairs, b->dImages, b->nImages, GM, BN, b->capB,
+                                             b->capRowsB, b->capTableB, b->dPrefC, b->dImgB, b->dRowsB,
+                                             b->dCounters);
+  V3DM_BTRY(cudaGetLastError());
+  k_bchoose<<<chooseGrid, kChooseThreads, 0, b->stream>>>(b->dPairs, b->nPairs, b->dImages, b->dImgB, b->dPrefC,
+                                                          b->dDecA, b->dFA, b->dFAB, b->dChosenLeft, b->dChosenRight,
+                                                          b->dChosenPair, b->dCounters, kFloatRowBytes / kDescBytes,
+                                                          b->fRows, b->capRowsB);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 3;
+  // ---- pass B: the rights the accepted lefts named, against their left image
+  sa.aIsLeft = 0;
+  sa.rows = b->dRowsB;
+  sa.nRowsPtr = b->dCounters + kCntRowsB;
+  sa.nRows = (int)std::min<long long>(b->capTableB, 0x7fffffff);
+  sa.decision = b->dDecB;
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[2], b->stream));
+  V3DM_BTRY(launch_side_f_batch(b->fmB_A, b->fmB_B, sa, Tf, b->numSMs, b->stream));
+  if (withEvents) V3DM_BTRY(cudaEventRecord(b->ev[3], b->stream));
+  launches += 1;
+  // ---- mutual filter, ordered triples
+  const int mutBlocks = (int)((b->capB + kBMutPerBlock - 1) / kBMutPerBlock);
+  k_bmutual_count<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft, b->dBlockCount);
+  V3DM_BTRY(cudaGetLastError());
+  k_bmutual_write<<<mutBlocks, kBMutThreads, 0, b->stream>>>(b->dCounters, b->dDecB, b->dChosenLeft,
+                                                             b->dChosenRight, b->dChosenPair, b->dBlockCount,
+                                                             mutBlocks, b->dOut, b->dInfo);
+  V3DM_BTRY(cudaGetLastError());
+  launches += 2;
+  V3DM_BTRY(cudaMemcpyAsync(b->hInfo, b->dInfo, (kInfoWords + kCntAll) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            b->stream));
+  b->lastLaunches = launches;
+  return V3DM_OK;
+}
+
+// The float passes' rows, pass-B operand and tensor maps.
+int prepare_float(v3dm_batch* b) {
+  if (b->rowsDirty || b->rowsCfg != kFloatRowsCfg) {
+    int st = build_rows(b, f_group_rows(), f_tile_cols(), kFloatRowsCfg);
+    if (st != V3DM_OK) return st;
+  }
+  if (b->totalRows == 0) return V3DM_OK;
+  const long long need = (long long)kFloatRowBytes * b->capRowsB;
+  if (b->fabCap < need || !b->dFAB) {
+    V3DM_BTRY(ensure(&b->dFAB, &b->fabCap, need));
+    b->fMapsValid = false;
+  }
+  if (!b->fMapsValid) {
+    V3DM_BTRY(f_maps(&b->fmA_A, b->dFA, b->fRows, &b->fmA_B, b->dFB, b->fRows));
+    V3DM_BTRY(f_maps(&b->fmB_A, b->dFAB, (int)b->capRowsB, &b->fmB_B, b->dFB, b->fRows));
+    b->fMapsValid = true;
+  }
+  return V3DM_OK;
+}
+
 int prepare(v3dm_batch* b) {
   if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->floatMode) return prepare_float(b);
   if (b->rowsDirty || b->rowsCfg != tc_get_config(b->tc)) {
-    int st = build_rows(b);
+    int GM = 0, BN = 0;
+    tc_config_shape(tc_get_config(b->tc), &GM, &BN);
+    int st = build_rows(b, GM, BN, tc_get_config(b->tc));
     if (st != V3DM_OK) return st;
   }
   if (b->totalRows > 0) {
@@ -1166,6 +1279,11 @@ int prepare(v3dm_batch* b) {
   }
   V3DM_BTRY(tc_prepare_batch(b->tc, tc_get_config(b->tc)));
   return V3DM_OK;
+}
+
+int enqueue_call(v3dm_batch* b, float minScore, float minRatio, bool withEvents) {
+  return b->floatMode ? enqueue_batch_f(b, minScore, minRatio, withEvents)
+                      : enqueue_batch(b, minScore, minRatio, withEvents);
 }
 
 // One call: graph replay (or direct launches), then nothing else; the info block lands in
@@ -1187,16 +1305,16 @@ int launch_call(v3dm_batch* b, float minScore, float minRatio) {
   if (b->profile) {
     for (int i = 0; i < 4; ++i)
       if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
-    st = enqueue_batch(b, minScore, minRatio, true);
+    st = enqueue_call(b, minScore, minRatio, true);
     if (st == V3DM_OK) b->profPending = true;
     return st;
   }
-  if (!b->useGraph) return enqueue_batch(b, minScore, minRatio, false);
+  if (!b->useGraph) return enqueue_call(b, minScore, minRatio, false);
   if (!b->graph || b->graphMs != ms || b->graphMr != mr) {
     drop_graph(b);
     cudaGraph_t g = nullptr;
     V3DM_BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    st = enqueue_batch(b, minScore, minRatio, false);
+    st = enqueue_call(b, minScore, minRatio, false);
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (st != V3DM_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1583,6 +1701,7 @@ int launch_call_proposal(v3dm_batch* b, const v3dm_projection* proj, int probesL
   if (probesL > C || probesR > C) return V3DM_ERR_ARG;
   const int probes = probesL * 16 + probesR;  // graph key
   if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->floatMode) return V3DM_ERR_UNSUPPORTED;
   b->pendingCheck = true;
   if (b->totalRows == 0 || b->nPairs == 0) {
     V3DM_BTRY(cudaMemsetAsync(b->dInfo, 0, (kInfoWords + kCntAll) * sizeof(int32_t), b->stream));
@@ -1689,10 +1808,25 @@ void free_all(v3dm_batch* b) {
   bfree(b->dStateA0);
   bfree(b->dOrigOf);
   bfree(b->dFlag);
+  bfree(b->dStageF);
+  bfree(b->dRowOffI);
+  bfree(b->dFA);
+  bfree(b->dFB);
+  bfree(b->dFAB);
   b->dCounters = nullptr;  // points into dInfo
   bfree(b->dInfo);
   if (b->hInfo) cudaFreeHost(b->hInfo);
   b->hInfo = nullptr;
+}
+
+// Switches between the uint8 and the float layouts; the graph and the row tables of the other
+// mode are dropped.
+void set_float_mode(v3dm_batch* b, bool on) {
+  if (b->floatMode == on) return;
+  drop_graph(b);
+  b->floatMode = on;
+  b->rowsDirty = true;
+  b->fMapsValid = false;
 }
 
 // Layout of the images: padded row offsets, per-image table.
@@ -1781,6 +1915,72 @@ int set_images(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t*
   return V3DM_OK;
 }
 
+// Float descriptors.  All of the form u/512: the uint8 layout (the integer path, whose scores
+// are the float ones exactly).  Otherwise the BF16 hi/lo layouts of every image, at the rows of
+// the uint8 layout, scored as the single-pair float matcher scores them.
+int set_images_f32(v3dm_batch* b, int nImages, const int32_t* counts, const float* desc, bool onDevice) {
+  if (!b || nImages < 0 || (nImages > 0 && !counts)) return V3DM_ERR_ARG;
+  long long total = 0;
+  for (int i = 0; i < nImages; ++i) {
+    if (counts[i] < 0) return V3DM_ERR_ARG;
+    if (counts[i] > V3DM_MAX_FEATURES) return V3DM_ERR_SIZE;
+    total += counts[i];
+  }
+  if (total > 0 && !desc) return V3DM_ERR_ARG;
+  if (onDevice && (reinterpret_cast<uintptr_t>(desc) & 15)) return V3DM_ERR_ARG;
+  if (total > 0x7fffffffLL / kDescBytes) return V3DM_ERR_SIZE;  // value indices of the conversion are int32
+  BDeviceGuard g(b->device);
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  int32_t* err = b->dInfo + kInfoErr;
+  bool exact = true;
+  const float* src = desc;
+  if (total > 0) {
+    if (!onDevice) {
+      V3DM_BTRY(ensure(&b->dStageF, &b->stageFCap, total * kDescBytes));
+      V3DM_BTRY(cudaMemcpyAsync(b->dStageF, desc, (size_t)total * kDescBytes * sizeof(float), cudaMemcpyHostToDevice,
+                                b->stream));
+      src = b->dStageF;
+    }
+    V3DM_BTRY(ensure(&b->dStage, &b->stageCap, total * kDescBytes));
+    V3DM_BTRY(cudaMemsetAsync(err, 0, sizeof(int32_t), b->stream));
+    V3DM_BTRY(launch_f32_to_u8(src, b->dStage, (int)total, err, b->stream));
+    V3DM_BTRY(cudaMemcpyAsync(b->hInfo + kInfoErr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream));
+    V3DM_BTRY(cudaStreamSynchronize(b->stream));
+    exact = (b->hInfo[kInfoErr] & kErrNotU8) == 0;
+    V3DM_BTRY(cudaMemsetAsync(err, 0, sizeof(int32_t), b->stream));
+  }
+  // the layout (and, for exact descriptors, the integer operand) from the uint8 staging buffer
+  int st = set_images(b, nImages, counts, total > 0 ? b->dStage : nullptr, true);
+  if (st != V3DM_OK) return st;
+  if (exact) {
+    set_float_mode(b, false);
+    return V3DM_OK;
+  }
+  b->haveImages = false;
+  set_float_mode(b, true);
+  b->fMapsValid = false;  // re-encoded before the next call (same buffers: same maps)
+  const int fRows = (int)std::max<long long>(b->totalRows, 256);
+  const uint8_t* oldA = b->dFA;
+  const uint8_t* oldB = b->dFB;
+  V3DM_BTRY(ensure(&b->dFA, &b->fImgCapA, (long long)fRows * kFloatRowBytes));
+  V3DM_BTRY(ensure(&b->dFB, &b->fImgCapB, (long long)fRows * kFloatRowBytes));
+  if (b->dFA != oldA || b->dFB != oldB || b->fRows != fRows) drop_graph(b);  // the graph's maps name the buffers
+  b->fRows = fRows;
+  V3DM_BTRY(ensure(&b->dRowOffI, &b->rowOffCap, std::max(nImages, 1)));
+  V3DM_BTRY(cudaMemcpyAsync(b->dRowOffI, b->rowOff.data(), (size_t)nImages * sizeof(int), cudaMemcpyHostToDevice,
+                            b->stream));
+  V3DM_BTRY(launch_hilo_images(src, total, b->dSrcOff, b->dRowOffI, nImages, fRows, b->dFA, b->dFB, err, b->stream));
+  V3DM_BTRY(cudaMemcpyAsync(b->hInfo + kInfoErr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream));
+  V3DM_BTRY(cudaStreamSynchronize(b->stream));
+  if (b->hInfo[kInfoErr]) {  // a value that is not finite
+    cudaMemsetAsync(err, 0, sizeof(int32_t), b->stream);
+    cudaStreamSynchronize(b->stream);
+    return V3DM_ERR_ARG;
+  }
+  b->haveImages = true;
+  return V3DM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1796,6 +1996,7 @@ int v3dm_batch_create(v3dm_batch** out, int device) {
   v3dm_batch* b = new (std::nothrow) v3dm_batch();
   if (!b) return V3DM_ERR_ARG;
   b->device = device;
+  b->numSMs = prop.multiProcessorCount;
   BDeviceGuard g(device);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             tc_plan_create(&b->tc, device) == cudaSuccess &&
@@ -1830,11 +2031,29 @@ int v3dm_batch_destroy(v3dm_batch* b) {
 }
 
 int v3dm_batch_set_images_u8(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* desc) {
-  return set_images(b, nImages, counts, desc, false);
+  const int st = set_images(b, nImages, counts, desc, false);
+  if (st == V3DM_OK) set_float_mode(b, false);
+  return st;
 }
 
 int v3dm_batch_set_images_u8_device(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* d_desc) {
-  return set_images(b, nImages, counts, d_desc, true);
+  const int st = set_images(b, nImages, counts, d_desc, true);
+  if (st == V3DM_OK) set_float_mode(b, false);
+  return st;
+}
+
+int v3dm_batch_set_images_f32(v3dm_batch* b, int nImages, const int32_t* counts, const float* desc) {
+  return set_images_f32(b, nImages, counts, desc, false);
+}
+
+int v3dm_batch_set_images_f32_device(v3dm_batch* b, int nImages, const int32_t* counts, const float* d_desc) {
+  return set_images_f32(b, nImages, counts, d_desc, true);
+}
+
+int v3dm_batch_float_mode(v3dm_batch* b, int* isFloat) {
+  if (!b || !isFloat) return V3DM_ERR_ARG;
+  *isFloat = b->floatMode ? 1 : 0;
+  return V3DM_OK;
 }
 
 int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs) {
@@ -1974,6 +2193,7 @@ int v3dm_batch_match_guided(v3dm_batch* b, int type, const double* M, const floa
   if (!b || !nOut || cap < 0 || (cap > 0 && !triples) || (type != 1 && type != 2)) return V3DM_ERR_ARG;
   if (!b->haveImages || !b->havePairs || !b->havePositions) return V3DM_ERR_NOT_ALLOCATED;
   if (b->nPairs > 0 && (!M || !thr)) return V3DM_ERR_ARG;
+  if (b->floatMode) return V3DM_ERR_UNSUPPORTED;
   BDeviceGuard g(b->device);
   V3DM_BTRY(cudaStreamSynchronize(b->stream));
   const int n = b->nPairs;
@@ -2132,6 +2352,7 @@ int v3dm_batch_autotune(v3dm_batch* b, float minScore, float minRatio, int reps,
                         float* msOut) {
   if (!b || reps < 1) return V3DM_ERR_ARG;
   if (!b->haveImages || !b->havePairs) return V3DM_ERR_NOT_ALLOCATED;
+  if (b->floatMode) return V3DM_ERR_UNSUPPORTED;  // one tile shape on the float layouts
   BDeviceGuard g(b->device);
   const int nCfg = tc_num_configs();
   const bool graphWas = b->useGraph;

@@ -106,6 +106,9 @@ struct SideArgs {
   // gathered A (launch_side_gather): A row e of the row table is descriptor aSrcRow[e] of aSrc
   const uint8_t* aSrc;
   const int* aSrcRow;
+  // batched float pass (launch_side_f_batch): decisions written per state, the float rules
+  int32_t* decision;
+  float minScore, minRatio;
   // failure-path test hooks (zero in production): the bounded waits give up after waitLimit
   // cycles (0: the default), and CTA 0's producer does not issue its skipLoad-th B tile load
   // (0: none), so that the consumer's bounded wait for it runs out
@@ -244,9 +247,21 @@ int f_segments(int numSMs);
 cudaError_t f_maps(CUtensorMap* mA, const void* dA, int rowsA, CUtensorMap* mB, const void* dB, int rowsB);
 cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf, float* dump,
                           int numSMs, cudaStream_t st);
+// Batched float side pass over a.rows (a.nRows, or *a.nRowsPtr rows), rows interleaved over the
+// persistent CTAs; A groups of f_group_rows() rows, B tiles of f_tile_cols() columns.  Writes
+// the decision of every state of the rows to a.decision (the float rules with a.minScore,
+// a.minRatio and the candidate threshold Tf); no chunk records.
+cudaError_t launch_side_f_batch(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf,
+                                int numSMs, cudaStream_t st);
+int f_group_rows();
+int f_tile_cols();
 cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s);
 cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, void* la, void* lb, int* err,
                         cudaStream_t s);
+// The same layouts for the n concatenated descriptors of nImages images: image i (first
+// descriptor srcOff[i], ascending) goes to rows rowOff[i] onwards of the rowsCap-row planes.
+cudaError_t launch_hilo_images(const float* f, long long n, const long long* srcOff, const int* rowOff, int nImages,
+                               int rowsCap, void* la, void* lb, int* err, cudaStream_t s);
 float host_float_threshold(float minScore, float minRatio);
 // Exact re-score of the flagged descriptors of side A against side B.
 struct RescoreArgs {

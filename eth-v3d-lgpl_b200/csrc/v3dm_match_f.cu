@@ -74,9 +74,105 @@ __device__ __forceinline__ float fmax32(const float* v) {
   return fmaxf(fmaxf(m[0], m[2]), fmaxf(m[1], m[3]));
 }
 
-// One pair: side A (nA rows, amap as in k_side) against side B (nB rows).  Same roles and
-// bounded waits as k_side; the A group is single-buffered (96 KB).  With 'dump' set (small
-// diagnostic calls) every score is also written to dump[index * nB + column].
+// The work of one CTA, in the order every role walks it.  One pair (kBatch false): the flat range
+// of (A group of 128 rows, B tile of 64 columns) this CTA owns.  A batch (kBatch true): the rows of
+// the row table interleaved over the CTAs (row r, r + gridDim.x, ...), each an A group of one image
+// against every 64-column tile of its B image; a row's state indices are state0 + its rows.
+template <bool kBatch>
+struct FWalk {
+  // one pair
+  long long w, w1;
+  int nTiles, nA, nB0;
+  const int* amap;
+  // batch
+  const BatchRow* rows;
+  int r, nRows;
+  BatchRow cur;
+  // the current item
+  int t;          // B tile of the A group
+  bool newA;      // the A group changes here
+  __device__ void init_pair(const SideArgs& a, int nA_) {
+    nA = nA_;
+    nB0 = a.nB;
+    amap = a.amap;
+    nTiles = (a.nB + kFN - 1) / kFN;
+    const long long nWork = (long long)((nA + kFM - 1) / kFM) * nTiles;
+    w = nWork * blockIdx.x / gridDim.x;
+    w1 = nWork * (blockIdx.x + 1) / gridDim.x;
+    t = nTiles > 0 ? (int)(w % nTiles) : 0;
+    newA = true;
+  }
+  __device__ void init_batch(const SideArgs& a) {
+    rows = a.rows;
+    nRows = a.nRowsPtr ? *a.nRowsPtr : a.nRows;
+    r = blockIdx.x;
+    t = 0;
+    newA = true;
+    if (r < nRows) cur = rows[r];
+  }
+  __device__ bool more() const {
+    if constexpr (kBatch) return r < nRows;
+    else return w < w1;
+  }
+  __device__ void next() {
+    if constexpr (kBatch) {
+      if (++t < cur.nTiles) {
+        newA = false;
+        return;
+      }
+      r += gridDim.x;
+      t = 0;
+      newA = true;
+      if (r < nRows) cur = rows[r];
+    } else {
+      ++w;
+      t = (int)(w % nTiles);
+      newA = t == 0;
+    }
+  }
+  __device__ int aRow() const {
+    if constexpr (kBatch) return cur.aRow;
+    else return (int)(w / nTiles) * kFM;
+  }
+  __device__ int bRow() const {
+    if constexpr (kBatch) return cur.bRow0 + t * kFN;
+    else return t * kFN;
+  }
+  __device__ int nB() const {
+    if constexpr (kBatch) return cur.nB;
+    else return nB0;
+  }
+  // the current tile is the last of its A group's row (batch walk only)
+  __device__ bool lastOfA() const { return t + 1 == cur.nTiles; }
+  // the state of row i (0..127) of the current A group, or -1 past its valid rows
+  __device__ long long state(int i) const {
+    if constexpr (kBatch) return i < cur.validRows ? cur.state0 + i : -1;
+    else {
+      const int row = (int)(w / nTiles) * kFM + i;
+      return row < nA ? (amap ? amap[row] : row) : -1;
+    }
+  }
+};
+
+// Running top two of one A row over the columns of a batch row, as ordered keys (f32_order; 0:
+// none): b1 the largest, c1 its first column, b2 the largest of the other columns.
+__device__ __forceinline__ void top2_push(uint32_t key, int col, uint32_t& b1, uint32_t& b2, int& c1) {
+  b2 = max(b2, min(key, b1));
+  c1 = key > b1 ? col : c1;
+  b1 = max(b1, key);
+}
+
+// Side A against side B.  One pair (kBatch false): nA rows (amap as in k_side) against nB rows;
+// the epilogue hands every 32-score chunk whose maximum reaches Tf to k_records_f.  A batch
+// (kBatch true): the row table; one CTA scores a row's A group against every tile of its B
+// image, so each epilogue thread keeps its A row's exact best and second over the whole image in
+// registers and writes the row's decision (a.decision[state]) after the last tile.  That is
+// what k_records_f and k_decide_f make of the chunk records: the best is the largest key (first
+// column on ties), the second the largest other key, both kept only when their score reaches Tf
+// (a non-best candidate reaches Tf only if the second does).  Same roles and bounded waits as
+// k_side; the A group is single-buffered (96 KB).  With 'dump' set (small one-pair diagnostic
+// calls) every score is also written to dump[index * nB + column].
+template <bool kBatch>
 __global__ void __launch_bounds__(kFThreads, 1)
 k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, SideArgs a, float Tf,
          float* dump) {
@@ -85,14 +181,16 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
   extern __shared__ uint8_t smemRaw[];
   SmemF& s = *reinterpret_cast<SmemF*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nA = a.nAptr ? *a.nAptr : a.nA;
-  const int nTiles = (a.nB + kFN - 1) / kFN;
-  const long long nWork = (long long)((nA + kFM - 1) / kFM) * nTiles;
-  if (nWork == 0) {
-    if (warp >= 2 && lane == 0) a.segCount[blockIdx.x * kFEpiWarps + (warp - 2)] = 0;
+  FWalk<kBatch> start;
+  if constexpr (kBatch) {
+    start.init_batch(a);
+  } else {
+    start.init_pair(a, a.nAptr ? *a.nAptr : a.nA);
+  }
+  if (!start.more()) {
+    if (!kBatch && warp >= 2 && lane == 0) a.segCount[blockIdx.x * kFEpiWarps + (warp - 2)] = 0;
     return;
   }
-  const long long w0 = nWork * blockIdx.x / gridDim.x, w1 = nWork * (blockIdx.x + 1) / gridDim.x;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kFStages; ++i) {
       mbar_init(&s.fullB[i], 1);
@@ -127,18 +225,17 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       uint32_t phase = 0;
       uint32_t armedPhase[kFStages] = {};
       bool armed[kFStages] = {};
-      for (long long w = w0; w < w1; ++w) {
-        const int g = (int)(w / nTiles), t = (int)(w - (long long)g * nTiles);
-        if (w == w0 || t == 0) {
+      for (FWalk<kBatch> wk = start; wk.more(); wk.next()) {
+        if (wk.newA) {
           // the previous group's MMAs must be done with the single A buffer
           if (groups > 0 && !mbar_wait(&s.emptyA, (groups - 1) & 1, &s.abort, a.err)) break;
           mbar_expect_tx(&s.fullA, (uint32_t)sizeof(s.a));
-          tma_load_3d(&s.a[0][0][0], &tmA, &s.fullA, 0, g * kFM, 0);
+          tma_load_3d(&s.a[0][0][0], &tmA, &s.fullA, 0, wk.aRow(), 0);
           ++groups;
         }
         if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
         mbar_expect_tx(&s.fullB[stage], (uint32_t)sizeof(s.b[0]));
-        tma_load_3d(&s.b[stage][0][0][0], &tmB, &s.fullB[stage], 0, t * kFN, 0);
+        tma_load_3d(&s.b[stage][0][0][0], &tmB, &s.fullB[stage], 0, wk.bRow(), 0);
         armed[stage] = true;
         armedPhase[stage] = phase;
         if (++stage == kFStages) {
@@ -165,9 +262,8 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       int stage = 0, acc = 0, groups = 0;
       uint32_t phase = 0, accPhase = 0;
       const uint32_t aBase = smem_u32(&s.a[0][0][0]);
-      for (long long w = w0; w < w1; ++w) {
-        const int t = (int)(w % nTiles);
-        if (w == w0 || t == 0) {
+      for (FWalk<kBatch> wk = start; wk.more(); wk.next()) {
+        if (wk.newA) {
           if (groups > 0) mma_commit(&s.emptyA);  // A buffer free once the previous group's MMAs end
           if (!mbar_wait(&s.fullA, groups & 1, &s.abort, a.err)) break;
           ++groups;
@@ -200,6 +296,61 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       while (!mbar_try(&s.mmaDone, 0) && clock64() - t0c < kWaitCycles) {
       }
     }
+  } else if constexpr (kBatch) {
+    // ---------------- epilogue (batch rows: decisions) ----------------
+    const int q = warp & 3;
+    int acc = 0;
+    uint32_t accPhase = 0;
+    bool ok = !s.abort;
+    long long st = -1;
+    uint32_t b1 = 0, b2 = 0;
+    int c1 = 0;
+    for (FWalk<kBatch> wk = start; wk.more() && ok; wk.next()) {
+      if (wk.newA) {
+        st = wk.state(q * 32 + lane);
+        b1 = b2 = 0u;
+        c1 = 0;
+      }
+      const int nB = wk.nB();
+      ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kFN);
+      uint32_t v[2][32];
+      tmem_ld32(tbase, v[0]);
+      tmem_ld32(tbase + 32u, v[1]);
+      tmem_wait(v[0]);
+      tmem_wait(v[1]);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
+      const int col0 = wk.t * kFN;
+      if (col0 + kFN <= nB) {  // warp-uniform: a full tile
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+          for (int k = 0; k < 32; ++k) top2_push(f32_order(__uint_as_float(v[c][k])), col0 + 32 * c + k, b1, b2, c1);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int col = col0 + 32 * c + k;
+            top2_push(col < nB ? f32_order(__uint_as_float(v[c][k])) : 0u, col, b1, b2, c1);
+          }
+      }
+      if (wk.lastOfA() && st >= 0) {
+        const float s1 = f32_unorder(b1), s2 = f32_unorder(b2);
+        const unsigned long long bk = (b1 != 0u && s1 >= Tf) ? best_key_f(s1, c1) : 0ull;
+        const uint32_t so = (b2 != 0u && s2 >= Tf) ? b2 : 0u;
+        a.decision[st] = decide_f(bk, so, a.minScore, a.minRatio);
+      }
+      if (++acc == kFAcc) {
+        acc = 0;
+        accPhase ^= 1;
+      }
+    }
   } else {
     // ---------------- epilogue ----------------
     const int e = warp - 2;
@@ -209,11 +360,12 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     int acc = 0;
     uint32_t accPhase = 0;
     bool ok = !s.abort;
-    for (long long w = w0; w < w1 && ok; ++w) {
-      const int g = (int)(w / nTiles), t = (int)(w - (long long)g * nTiles);
-      const int row = g * kFM + q * 32 + lane;
-      const bool rowValid = row < nA;
-      const int orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
+    long long st = -1;
+    for (FWalk<kBatch> wk = start; wk.more() && ok; wk.next()) {
+      if (wk.newA) st = wk.state(q * 32 + lane);
+      const bool rowValid = st >= 0;
+      const int orig = rowValid ? (int)st : 0;
+      const int nB = wk.nB();
       ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
@@ -229,13 +381,13 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
-        const int col0 = t * kFN + 32 * c;
-        if (col0 >= a.nB) break;  // warp-uniform
+        const int col0 = wk.t * kFN + 32 * c;
+        if (col0 >= nB) break;  // warp-uniform
         float f[32];
 #pragma unroll
-        for (int k = 0; k < 32; ++k) f[k] = (col0 + k < a.nB) ? __uint_as_float(v[c][k]) : -INFINITY;
-        if (dump && rowValid)
-          for (int k = 0; k < 32 && col0 + k < a.nB; ++k) dump[(size_t)orig * a.nB + col0 + k] = f[k];
+        for (int k = 0; k < 32; ++k) f[k] = (col0 + k < nB) ? __uint_as_float(v[c][k]) : -INFINITY;
+        if (!kBatch && dump && rowValid)
+          for (int k = 0; k < 32 && col0 + k < nB; ++k) dump[(size_t)orig * nB + col0 + k] = f[k];
         const float mx = fmax32(f);
         const bool trig = rowValid && mx >= Tf;
         if (__any_sync(0xffffffffu, trig)) {
@@ -244,7 +396,7 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             const int idx = segN + __popc(m & ((1u << lane) - 1u));
             if (idx < a.segCap) {
               uint4* rec = segBase + (long long)idx * kRecordQuads;
-              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)a.nB, 0u);
+              rec[0] = make_uint4((uint32_t)orig, (uint32_t)col0, (uint32_t)nB, 0u);
 #pragma unroll
               for (int k = 0; k < 8; ++k)
                 rec[1 + k] = make_uint4(v[c][4 * k], v[c][4 * k + 1], v[c][4 * k + 2], v[c][4 * k + 3]);
@@ -376,12 +528,25 @@ __global__ void k_decide_f(PostArgs a) {
 // A and B layouts of n descriptors: float values (or uint8 values u, read as u / 512) split
 // into BF16 hi and lo.  A row = [hi | lo | hi], B row = [hi | hi | lo] (384 values along K),
 // stored planar: plane p holds K positions 64p .. 64p + 63 of every row, rowsCap rows of 128 B
-// per plane.  Sets *err when a value is not finite.
-__global__ void k_hilo(const float* __restrict__ f, const uint8_t* __restrict__ u, int n, int rowsCap,
-                       __nv_bfloat16* __restrict__ la, __nv_bfloat16* __restrict__ lb, int* err) {
+// per plane.  Sets *err when a value is not finite.  With srcOff set, the n descriptors are the
+// concatenation of nImages images (image i starts at descriptor srcOff[i], ascending) and image
+// i's descriptors go to rows rowOff[i] onwards; otherwise descriptor d goes to row d.
+__global__ void k_hilo(const float* __restrict__ f, const uint8_t* __restrict__ u, long long n, int rowsCap,
+                       __nv_bfloat16* __restrict__ la, __nv_bfloat16* __restrict__ lb, int* err,
+                       const long long* __restrict__ srcOff, const int* __restrict__ rowOff, int nImages) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)n * kDescBytes) return;
-  const long long d = i / kDescBytes;
+  if (i >= n * kDescBytes) return;
+  const long long src = i / kDescBytes;
+  long long d = src;
+  if (srcOff) {
+    int lo = 0, hi = nImages - 1;  // last image whose first descriptor is <= src
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (srcOff[mid] <= src) lo = mid;
+      else hi = mid - 1;
+    }
+    d = rowOff[lo] + (src - srcOff[lo]);
+  }
   const int k = (int)(i % kDescBytes);
   const float x = f ? f[i] : (float)u[i] * (1.0f / 512.0f);
   if (!isfinite(x)) atomicOr(err, kErrNotU8);
@@ -445,7 +610,7 @@ cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const Si
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
   if (!attrSet[dev]) {
-    e = cudaFuncSetAttribute(k_side_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_side_f<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attrSet[dev] = true;
   }
@@ -454,8 +619,33 @@ cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const Si
   const long long maxWork = (long long)((a.nA + kFM - 1) / kFM) * nTiles;
   const int grid = (int)std::min<long long>(numSMs, std::max<long long>(1, maxWork));
   if (grid * kFEpiWarps > a.nSeg) return cudaErrorInvalidValue;
-  return launch_pdl(k_side_f, dim3(grid), dim3(kFThreads), smem, st, mA, mB, a, Tf, dump);
+  return launch_pdl(k_side_f<false>, dim3(grid), dim3(kFThreads), smem, st, mA, mB, a, Tf, dump);
 }
+
+cudaError_t launch_side_f_batch(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf,
+                                int numSMs, cudaStream_t st) {
+  const size_t smem = sizeof(SmemF) + 1024;
+  static bool attrSet[128] = {};  // per device ordinal
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  if (!attrSet[dev]) {
+    e = cudaFuncSetAttribute(k_side_f<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attrSet[dev] = true;
+  }
+  int grid = numSMs;
+  if (!a.nRowsPtr) {
+    if (a.nRows <= 0) return cudaSuccess;
+    grid = std::min(grid, a.nRows);
+  }
+  if (!a.rows || !a.decision) return cudaErrorInvalidValue;
+  return launch_pdl(k_side_f<true>, dim3(grid), dim3(kFThreads), smem, st, mA, mB, a, Tf, (float*)nullptr);
+}
+
+int f_group_rows() { return kFM; }
+int f_tile_cols() { return kFN; }
 
 cudaError_t launch_post_f(const PostArgs& a, float Tf, cudaStream_t s) {
   const int listBlocks = (a.nSeg * 32 + 255) / 256;
@@ -472,7 +662,18 @@ cudaError_t launch_hilo(const float* f, const uint8_t* u, int n, int rowsCap, vo
   if (n > rowsCap) return cudaErrorInvalidValue;
   const long long total = (long long)n * kDescBytes;
   k_hilo<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(f, u, n, rowsCap, static_cast<__nv_bfloat16*>(la),
-                                                         static_cast<__nv_bfloat16*>(lb), err);
+                                                         static_cast<__nv_bfloat16*>(lb), err, nullptr, nullptr, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hilo_images(const float* f, long long n, const long long* srcOff, const int* rowOff, int nImages,
+                               int rowsCap, void* la, void* lb, int* err, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (nImages <= 0 || !srcOff || !rowOff) return cudaErrorInvalidValue;
+  const long long total = n * kDescBytes;
+  k_hilo<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(f, nullptr, n, rowsCap, static_cast<__nv_bfloat16*>(la),
+                                                         static_cast<__nv_bfloat16*>(lb), err, srcOff, rowOff,
+                                                         nImages);
   return cudaGetLastError();
 }
 

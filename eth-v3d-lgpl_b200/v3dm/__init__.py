@@ -116,6 +116,9 @@ def lib() -> C.CDLL:
         L.v3dm_batch_destroy.argtypes = [vp]
         L.v3dm_batch_set_images_u8.argtypes = [vp, i32, vp, vp]
         L.v3dm_batch_set_images_u8_device.argtypes = [vp, i32, vp, vp]
+        L.v3dm_batch_set_images_f32.argtypes = [vp, i32, vp, vp]
+        L.v3dm_batch_set_images_f32_device.argtypes = [vp, i32, vp, vp]
+        L.v3dm_batch_float_mode.argtypes = [vp, C.POINTER(i32)]
         L.v3dm_batch_set_pairs.argtypes = [vp, i32, vp]
         L.v3dm_batch_match.argtypes = [vp, f32, f32, vp, i64, i64p]
         L.v3dm_batch_match_device.argtypes = [vp, f32, f32, vp]
@@ -499,17 +502,28 @@ class BatchMatching:
         self.close()
 
     def set_images(self, desc: np.ndarray, counts) -> None:
-        """desc: (sum(counts), 128) uint8, the images' descriptors concatenated."""
-        d = np.ascontiguousarray(desc, dtype=np.uint8)
+        """desc: (sum(counts), 128) uint8 or float32, the images' descriptors concatenated.
+        Float descriptors that are not all u/512 are matched as SIFTMatching matches them (the
+        BF16 hi/lo scores); `float_mode` tells which layout was chosen."""
         c = np.ascontiguousarray(counts, dtype=np.int32)
+        is_f = np.asarray(desc).dtype == np.float32
+        d = np.ascontiguousarray(desc, dtype=np.float32 if is_f else np.uint8)
         if d.ndim != 2 or d.shape[1] != 128 or int(c.sum()) != d.shape[0]:
-            raise ValueError("desc must be (sum(counts), 128) uint8")
-        _check(lib().v3dm_batch_set_images_u8(self._h, c.shape[0], _ptr(c), _ptr(d)), "batch_set_images")
+            raise ValueError("desc must be (sum(counts), 128) uint8 or float32")
+        fn = lib().v3dm_batch_set_images_f32 if is_f else lib().v3dm_batch_set_images_u8
+        _check(fn(self._h, c.shape[0], _ptr(c), _ptr(d)), "batch_set_images")
 
-    def set_images_device(self, d_desc: int, counts) -> None:
+    def set_images_device(self, d_desc: int, counts, dtype=np.uint8) -> None:
         c = np.ascontiguousarray(counts, dtype=np.int32)
-        _check(lib().v3dm_batch_set_images_u8_device(self._h, c.shape[0], _ptr(c), C.c_void_p(d_desc)),
-               "batch_set_images_device")
+        fn = lib().v3dm_batch_set_images_f32_device if np.dtype(dtype) == np.float32 else \
+            lib().v3dm_batch_set_images_u8_device
+        _check(fn(self._h, c.shape[0], _ptr(c), C.c_void_p(d_desc)), "batch_set_images_device")
+
+    @property
+    def float_mode(self) -> bool:
+        v = C.c_int(0)
+        _check(lib().v3dm_batch_float_mode(self._h, C.byref(v)), "batch_float_mode")
+        return bool(v.value)
 
     def set_pairs(self, pairs=None) -> None:
         """pairs: (n, 2) int32 (left image, right image); None = every (i, j), i < j."""

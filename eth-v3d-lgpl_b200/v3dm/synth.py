@@ -178,6 +178,16 @@ def scene(seed: int = 6, n_images: int = 12, n_min: int = 500, n_max: int = 4000
     return desc, counts, offsets, pos.astype(np.float32), (K, rots, centres)
 
 
+def float_from_u8(desc: np.ndarray, seed: int, sigma: float = 0.004) -> np.ndarray:
+    """Float descriptors that are not u/512: desc / 512 perturbed by |N(0, sigma^2)| noise and
+    renormalised to unit length (the values SIFT pipelines that keep floats hand over)."""
+    rng = rng_for(2000 + seed)
+    x = desc.astype(np.float64) / 512.0
+    y = np.abs(x + rng.normal(0.0, sigma, x.shape))
+    y /= np.maximum(np.linalg.norm(y, axis=1, keepdims=True), 1e-12)
+    return y.astype(np.float32)
+
+
 def fundamental(cams, i: int, j: int) -> np.ndarray:
     """F with q^T F p = 0 for p in image i and q in image j of a scene()."""
     K, rots, centres = cams

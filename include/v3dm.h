@@ -217,6 +217,17 @@ V3DM_API int v3dm_batch_destroy(v3dm_batch* b);
 V3DM_API int v3dm_batch_set_images_u8(v3dm_batch* b, int nImages, const int32_t* counts, const uint8_t* desc);
 V3DM_API int v3dm_batch_set_images_u8_device(v3dm_batch* b, int nImages, const int32_t* counts,
                                              const uint8_t* d_desc);
+/* The same for float descriptors (128 floats each; the reference's float setLeftFeatures /
+ * setRightFeatures, v3d_cudamatching.cu:490-520).  When every value is of the form u/512 the
+ * integer layout is used; otherwise every image is held in the BF16 hi/lo layouts of the
+ * single-pair float matcher and each pair's result equals SIFTMatching's float
+ * findPutativeMatches on the two images.  Guided and proposal calls need the integer layout
+ * (V3DM_ERR_UNSUPPORTED on float images).  Non-finite values: V3DM_ERR_ARG.  *isFloat reports
+ * which layout the last upload chose. */
+V3DM_API int v3dm_batch_set_images_f32(v3dm_batch* b, int nImages, const int32_t* counts, const float* desc);
+V3DM_API int v3dm_batch_set_images_f32_device(v3dm_batch* b, int nImages, const int32_t* counts,
+                                              const float* d_desc);
+V3DM_API int v3dm_batch_float_mode(v3dm_batch* b, int* isFloat);
 /* nPairs (left image, right image) int32 pairs; nPairs == -1 (pairs NULL) means every
  * (i, j) with i < j, left = i, in row-major order. */
 V3DM_API int v3dm_batch_set_pairs(v3dm_batch* b, int nPairs, const int32_t* pairs);

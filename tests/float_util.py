@@ -51,3 +51,14 @@ def reference_pairs(S_lr, ms, mr):
     row = _side(S.T, ms, mr)    # per right, over lefts
     out = [(k, col[k]) for k in range(S.shape[0]) if col[k] >= 0 and row[col[k]] == k]
     return np.array(out, np.int32).reshape(-1, 2)
+
+
+def float_images(seed, n_images, n_min, n_max, exact=()):
+    """An image set of float descriptors with shared tracks: synth.images' uint8 descriptors
+    through synth.float_from_u8 (not u/512), except the images listed in 'exact', which keep
+    u/512.  Returns (desc float32, counts, offsets)."""
+    desc, counts, offs = synth.images(seed, n_images, n_min, n_max)
+    out = synth.float_from_u8(desc, seed)
+    for i in exact:
+        out[offs[i]:offs[i + 1]] = desc[offs[i]:offs[i + 1]].astype(np.float32) / 512
+    return out, counts, offs
