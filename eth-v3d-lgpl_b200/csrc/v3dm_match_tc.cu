@@ -13,14 +13,17 @@
 //               'row' and reads its scores with tcgen05.ld (32 columns per chunk), hands the
 //               stage back, and per chunk does one of two things:
 //                 - all scores below Smin (the smallest score that can pass the min-score
-//                   test): W = max(W, chunk maximum + 1)                     (one op);
+//                   test): W = max(W, chunk maximum);
 //                 - some score >= Smin (true matches, ~1e-6 of unrelated pairs): the lane
 //                   writes a record (descriptor, first column, its 32 scores) to its warp's
 //                   segment; k_records (v3dm_pair.cu) does the exact work on it: guided
 //                   gates for every score >= Smin, chunk best (largest score, first index on
 //                   ties, the reference's argMax rule, v3d_cudamatching.cu:145), maximum of
 //                   the other scores.
-//               At the end of a work unit the lane's W goes to sec[] (atomicMax).
+//               At the end of a work unit the lane's W + 1 goes to sec[] (atomicMax).  W starts
+//               as a negative float's bits (below every score) and takes the spare input of the
+//               chunk's maximum tree: C = max(W, chunk); C >= Smin exactly when the chunk
+//               reaches Smin (W < Smin always), else W = C.
 // Resulting per-descriptor values (after the list pass in v3dm_pair.cu): best = the exact
 // best over scores >= Smin that pass the gates; sec = the exact second-best score without
 // gates, an upper bound of it with gates (masked scores are counted).  The decision
@@ -113,17 +116,30 @@ __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t ad, uint64_t bd,
       : "memory");
 }
 
-// Maximum of 32 scores: a balanced tree of two-input integer maxima (ALU pipe, short
-// latency, 16-way parallel at the first level).
-__device__ __forceinline__ uint32_t max32_bits(const uint32_t* v) {
-  uint32_t m[16];
+static_assert(kMaxScore < (1 << 23), "scores are zero or subnormal as floats");
+
+// Maximum of three scores in one instruction: the three-input max.f32 of sm_100 applied to the
+// scores' bit patterns.  Scores are integers in [0, 255^2 * 128] < 2^23, i.e. zero or subnormal
+// floats, whose float order is their integer order; max.f32 without .ftz keeps subnormals.
+__device__ __forceinline__ uint32_t max3_bits(uint32_t a, uint32_t b, uint32_t c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(__uint_as_float(a)), "f"(__uint_as_float(b)), "f"(__uint_as_float(c)));
+  return __float_as_uint(r);
+}
+
+// max(x, the 32 scores of v): a tree of three-input maxima, 16 instructions (a two-input tree
+// takes 31 for the scores alone; the epilogue's filtering is what limits the side kernel).  x
+// takes the spare input of the last one.
+__device__ __forceinline__ uint32_t max32_bits(const uint32_t* v, uint32_t x) {
+  uint32_t m[12];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) m[i] = max(v[i], v[i + 16]);
+  for (int i = 0; i < 10; ++i) m[i] = max3_bits(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+  m[10] = v[30];
+  m[11] = v[31];
+  uint32_t n[4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) m[i] = max(m[i], m[i + 8]);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) m[i] = max(m[i], m[i + 4]);
-  return max(max(m[0], m[2]), max(m[1], m[3]));
+  for (int i = 0; i < 4; ++i) n[i] = max3_bits(m[3 * i], m[3 * i + 1], m[3 * i + 2]);
+  return max3_bits(max3_bits(n[0], n[1], n[2]), n[3], x);
 }
 
 // Work range of this CTA in the flattened (group, tile) sequence.
@@ -566,10 +582,15 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
     int aLocal = 0;  // batched pass: index of this lane's A row within its image
     int nB = a.nB;
     int bRow0 = 0;
-    uint32_t lw = 0;  // max + 1 of this lane's scores in the current unit, chunks with a record excluded
+    // maximum of this lane's scores in the current unit, chunks with a record excluded; kNoScore
+    // (a negative float, below every score in the max.f32 order) while there is none
+    constexpr uint32_t kNoScore = 0xbf800000u;
+    uint32_t lw = kNoScore;
+    int32_t sminRow = 0x7fffffff;  // Smin for a valid row, above every score otherwise
     // a bound below Tsec cannot change the decision: no atomic for it
     auto flush = [&]() {
-      if (rowValid && lw > (uint32_t)a.Tsec) atomicMax(&a.sec[orig], lw);
+      const uint32_t w = lw == kNoScore ? 0u : lw + 1u;  // sec[] holds second + 1
+      if (rowValid && w > (uint32_t)a.Tsec) atomicMax(&a.sec[orig], w);
     };
     for (Cursor wc = make_cursor(); wc.more() && ok; wc.next()) {
       if (wc.fresh) {
@@ -587,7 +608,8 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           rowValid = row < nA;
           orig = rowValid ? (a.amap ? a.amap[row] : row) : 0;
         }
-        lw = 0;
+        lw = kNoScore;
+        sminRow = rowValid ? a.Smin : 0x7fffffff;
       }
       for (int h = 0; h < C::kSplit; ++h) {
       const int colBase = wc.t * C::BN + h * C::kMmaN + colOff;
@@ -634,9 +656,9 @@ k_side(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensor
           for (int k = 0; k < 32; ++k)
             if (col0 + k >= nB) v[c][k] = 0u;
         }
-        const uint32_t mx = max32_bits(v[c]);
-        const bool trig = rowValid && (int32_t)mx >= a.Smin;
-        if (rowValid && !trig) lw = max(lw, mx + 1u);
+        const uint32_t cm = max32_bits(v[c], lw);  // max(lw, chunk maximum)
+        const bool trig = (int32_t)cm >= sminRow;   // kNoScore is negative as an int32
+        if (!trig) lw = cm;                          // an invalid row's lw is never flushed
         if (__any_sync(0xffffffffu, trig)) {
           // rare: hand the chunk to k_records (its exact best, gates and other scores)
           const unsigned m = __ballot_sync(0xffffffffu, trig);
