@@ -34,7 +34,13 @@ constexpr int kFStages = 2;         // B tile ring
 constexpr int kFPlanes = 6;         // 128-byte K planes per row (384 BF16 values)
 constexpr int kFSteps = 24;         // K = 16 per MMA
 constexpr int kFAcc = 4;            // TMEM accumulator stages of kFN columns
-constexpr int kFTmemCols = 256;
+// The A group lives in TMEM during its tiles: copied once (tcgen05.cp) from its shared-memory
+// landing buffer, so that shared memory serves only the B tiles (the MMA then reads 2 KB of B
+// per 128x64x16 step instead of 6 KB of A and B).
+constexpr int kFACols = kFPlanes * 32;     // 128-byte K planes, 4 bytes per column: 192 columns
+constexpr int kFABase = kFAcc * kFN;       // A after the accumulators
+constexpr int kFTmemCols = 512;
+static_assert(kFABase + kFACols <= kFTmemCols, "accumulators and the A group fit in TMEM");
 constexpr int kFEpiWarps = 4;       // one per TMEM lane quadrant
 constexpr int kFThreads = (2 + kFEpiWarps) * 32;
 
@@ -54,13 +60,20 @@ __device__ __forceinline__ constexpr uint32_t idesc_f16() {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kFN >> 3) << 17) | ((uint32_t)(kFM >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+// A from TMEM (lane = row, K values packed two per column), B from shared memory.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t dtmem, uint32_t atmem, uint64_t bd, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
-      "l"(ad), "l"(bd), "r"(idesc_f16()), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
+      "r"(atmem), "l"(bd), "r"(idesc_f16()), "r"(accumulate)
       : "memory");
+}
+
+// A 128-row x 32-byte slice, described as the MMA would read it from shared memory, into TMEM
+// (row i to lane i, 8 columns); executes in issue order with the MMAs of the same thread.
+__device__ __forceinline__ void tmem_cp_slice(uint32_t taddr, uint64_t sd) {
+  asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(taddr), "l"(sd) : "memory");
 }
 
 __device__ __forceinline__ float fmax32(const float* v) {
@@ -262,10 +275,17 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       int stage = 0, acc = 0, groups = 0;
       uint32_t phase = 0, accPhase = 0;
       const uint32_t aBase = smem_u32(&s.a[0][0][0]);
+      const uint32_t aT = tmem + (uint32_t)kFABase;
       for (FWalk<kBatch> wk = start; wk.more(); wk.next()) {
         if (wk.newA) {
-          if (groups > 0) mma_commit(&s.emptyA);  // A buffer free once the previous group's MMAs end
           if (!mbar_wait(&s.fullA, groups & 1, &s.abort, a.err)) break;
+          // the group into TMEM (after the previous group's MMAs, which were issued first); the
+          // landing buffer is free once the copies are done
+#pragma unroll
+          for (int k = 0; k < kFSteps; ++k)
+            tmem_cp_slice(aT + (uint32_t)(8 * k),
+                          sdesc(aBase + (uint32_t)(k >> 2) * (kFM * 128) + (uint32_t)((k & 3) * 32)));
+          mma_commit(&s.emptyA);
           ++groups;
         }
         if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
@@ -277,7 +297,7 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
         for (int k = 0; k < kFSteps; ++k) {
           const uint32_t off = (uint32_t)((k & 3) * 32);
           const uint32_t pl = (uint32_t)(k >> 2);
-          mma_bf16(d, sdesc(aBase + pl * (kFM * 128) + off), sdesc(bBase + pl * (kFN * 128) + off), k > 0 ? 1u : 0u);
+          mma_bf16_ts(d, aT + (uint32_t)(8 * k), sdesc(bBase + pl * (kFN * 128) + off), k > 0 ? 1u : 0u);
         }
         mma_commit(&s.emptyB[stage]);
         mma_commit(&s.accFull[acc]);
