@@ -25,7 +25,7 @@
 // second value the side pass could only bound.
 // Float descriptors that are not all of the form u/512 (v3dm_batch_set_images_f32) take the same
 // passes on the BF16 hi/lo layouts of the single-pair float matcher (v3dm_match_f.cu): groups of
-// 128 lefts against tiles of 64 columns, each descriptor's exact best and second over the other
+// 128 lefts against tiles of 128 columns, each descriptor's exact best and second over the other
 // image kept in registers and decided with the float rules, so each pair's result equals that
 // matcher's.
 // Every launch after the first reads its sizes from device memory, so the whole sequence is

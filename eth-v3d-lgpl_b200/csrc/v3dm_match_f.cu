@@ -29,14 +29,17 @@ namespace v3dm {
 namespace {
 
 constexpr int kFM = 128;            // rows per MMA (TMEM lanes)
-constexpr int kFN = 64;             // B rows per tile
-constexpr int kFStages = 2;         // B tile ring
+constexpr int kFN = 128;            // B rows per tile (one MMA is 128 x 128 x 16: narrower MMAs ran 30% slower)
+constexpr int kFChunks = kFN / 32;  // 32-column TMEM loads per tile and lane quadrant
+constexpr int kFStages = 2;         // ring of 96 KB stages: a B tile or a whole A group
 constexpr int kFPlanes = 6;         // 128-byte K planes per row (384 BF16 values)
 constexpr int kFSteps = 24;         // K = 16 per MMA
-constexpr int kFAcc = 4;            // TMEM accumulator stages of kFN columns
-// The A group lives in TMEM during its tiles: copied once (tcgen05.cp) from its shared-memory
-// landing buffer, so that shared memory serves only the B tiles (the MMA then reads 2 KB of B
-// per 128x64x16 step instead of 6 KB of A and B).
+constexpr int kFAcc = 2;            // TMEM accumulator stages of kFN columns
+// The A group lives in TMEM during its tiles: it lands in a stage of the ring and is copied once
+// (tcgen05.cp) into TMEM, so that shared memory serves the B tiles (the MMA reads 4 KB of B per
+// 128x128x16 step instead of 8 KB of A and B) and the two stages hold B tiles between groups.
+constexpr int kFAPlanes = 6;        // planes of an A group per ring stage
+static_assert(kFAPlanes * kFM == kFPlanes * kFN && kFPlanes % kFAPlanes == 0, "A planes fill whole stages");
 constexpr int kFACols = kFPlanes * 32;     // 128-byte K planes, 4 bytes per column: 192 columns
 constexpr int kFABase = kFAcc * kFN;       // A after the accumulators
 constexpr int kFTmemCols = 512;
@@ -45,15 +48,14 @@ constexpr int kFEpiWarps = 4;       // one per TMEM lane quadrant
 constexpr int kFThreads = (2 + kFEpiWarps) * 32;
 
 struct SmemF {
-  uint8_t a[kFPlanes][kFM][128];              // 96 KB, one A group
-  uint8_t b[kFStages][kFPlanes][kFN][128];    // 2 x 48 KB
+  uint8_t b[kFStages][kFPlanes][kFN][128];    // 2 x 96 KB: a B tile, or an A group
   unsigned long long fullB[kFStages], emptyB[kFStages];
-  unsigned long long fullA, emptyA;
   unsigned long long accFull[kFAcc], accEmpty[kFAcc];
   unsigned long long mmaDone;
   uint32_t tmemBase;
   int abort;
 };
+static_assert(sizeof(SmemF) + 1024 <= 227 * 1024, "shared memory of one CTA");
 
 // kind::f16, D = F32, A = B = BF16, both K-major, M = 128, N = kFN.
 __device__ __forceinline__ constexpr uint32_t idesc_f16() {
@@ -88,9 +90,9 @@ __device__ __forceinline__ float fmax32(const float* v) {
 }
 
 // The work of one CTA, in the order every role walks it.  One pair (kBatch false): the flat range
-// of (A group of 128 rows, B tile of 64 columns) this CTA owns.  A batch (kBatch true): the rows of
+// of (A group of 128 rows, B tile of 128 columns) this CTA owns.  A batch (kBatch true): the rows of
 // the row table interleaved over the CTAs (row r, r + gridDim.x, ...), each an A group of one image
-// against every 64-column tile of its B image; a row's state indices are state0 + its rows.
+// against every 128-column tile of its B image; a row's state indices are state0 + its rows.
 template <bool kBatch>
 struct FWalk {
   // one pair
@@ -209,8 +211,6 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       mbar_init(&s.fullB[i], 1);
       mbar_init(&s.emptyB[i], 1);
     }
-    mbar_init(&s.fullA, 1);
-    mbar_init(&s.emptyA, 1);
     for (int i = 0; i < kFAcc; ++i) {
       mbar_init(&s.accFull[i], 1);
       mbar_init(&s.accEmpty[i], kFEpiWarps);
@@ -234,17 +234,30 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, groups = 0;
+      int stage = 0;
       uint32_t phase = 0;
       uint32_t armedPhase[kFStages] = {};
       bool armed[kFStages] = {};
       for (FWalk<kBatch> wk = start; wk.more(); wk.next()) {
         if (wk.newA) {
-          // the previous group's MMAs must be done with the single A buffer
-          if (groups > 0 && !mbar_wait(&s.emptyA, (groups - 1) & 1, &s.abort, a.err)) break;
-          mbar_expect_tx(&s.fullA, (uint32_t)sizeof(s.a));
-          tma_load_3d(&s.a[0][0][0], &tmA, &s.fullA, 0, wk.aRow(), 0);
-          ++groups;
+          // the A group through the ring (kFAPlanes planes per stage)
+          bool stop = false;
+#pragma unroll
+          for (int h = 0; h < kFPlanes / kFAPlanes; ++h) {
+            if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) {
+              stop = true;
+              break;
+            }
+            mbar_expect_tx(&s.fullB[stage], (uint32_t)sizeof(s.b[0]));
+            tma_load_3d(&s.b[stage][0][0][0], &tmA, &s.fullB[stage], 0, wk.aRow(), h * kFAPlanes);
+            armed[stage] = true;
+            armedPhase[stage] = phase;
+            if (++stage == kFStages) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+          if (stop) break;
         }
         if (!mbar_wait(&s.emptyB[stage], phase ^ 1, &s.abort, a.err)) break;
         mbar_expect_tx(&s.fullB[stage], (uint32_t)sizeof(s.b[0]));
@@ -263,30 +276,37 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
           while (!mbar_try(&s.fullB[i], armedPhase[i]) && clock64() - t0c < kWaitCycles) {
           }
         }
-      if (groups > 0) {
-        long long t0c = clock64();
-        while (!mbar_try(&s.fullA, (groups - 1) & 1) && clock64() - t0c < kWaitCycles) {
-        }
-      }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && !s.abort) {
-      int stage = 0, acc = 0, groups = 0;
+      int stage = 0, acc = 0;
       uint32_t phase = 0, accPhase = 0;
-      const uint32_t aBase = smem_u32(&s.a[0][0][0]);
       const uint32_t aT = tmem + (uint32_t)kFABase;
       for (FWalk<kBatch> wk = start; wk.more(); wk.next()) {
         if (wk.newA) {
-          if (!mbar_wait(&s.fullA, groups & 1, &s.abort, a.err)) break;
-          // the group into TMEM (after the previous group's MMAs, which were issued first); the
-          // landing buffer is free once the copies are done
+          // the group into TMEM (after the previous group's MMAs, which were issued first); its
+          // stage is free once the copies are done
+          bool stop = false;
 #pragma unroll
-          for (int k = 0; k < kFSteps; ++k)
-            tmem_cp_slice(aT + (uint32_t)(8 * k),
-                          sdesc(aBase + (uint32_t)(k >> 2) * (kFM * 128) + (uint32_t)((k & 3) * 32)));
-          mma_commit(&s.emptyA);
-          ++groups;
+          for (int h = 0; h < kFPlanes / kFAPlanes; ++h) {
+            if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) {
+              stop = true;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sb = smem_u32(&s.b[stage][0][0][0]);
+#pragma unroll
+            for (int kk = 0; kk < 4 * kFAPlanes; ++kk)
+              tmem_cp_slice(aT + (uint32_t)(8 * (h * 4 * kFAPlanes + kk)),
+                            sdesc(sb + (uint32_t)(kk >> 2) * (kFM * 128) + (uint32_t)((kk & 3) * 32)));
+            mma_commit(&s.emptyB[stage]);
+            if (++stage == kFStages) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+          if (stop) break;
         }
         if (!mbar_wait(&s.accEmpty[acc], accPhase ^ 1, &s.abort, a.err)) break;
         if (!mbar_wait(&s.fullB[stage], phase, &s.abort, a.err)) break;
@@ -337,23 +357,23 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       if (!ok) break;
       tc_fence_after();
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kFN);
-      uint32_t v[2][32];
-      tmem_ld32(tbase, v[0]);
-      tmem_ld32(tbase + 32u, v[1]);
-      tmem_wait(v[0]);
-      tmem_wait(v[1]);
+      uint32_t v[kFChunks][32];
+#pragma unroll
+      for (int c = 0; c < kFChunks; ++c) tmem_ld32(tbase + (uint32_t)(32 * c), v[c]);
+#pragma unroll
+      for (int c = 0; c < kFChunks; ++c) tmem_wait(v[c]);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
       const int col0 = wk.t * kFN;
       if (col0 + kFN <= nB) {  // warp-uniform: a full tile
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < kFChunks; ++c)
 #pragma unroll
           for (int k = 0; k < 32; ++k) top2_push(f32_order(__uint_as_float(v[c][k])), col0 + 32 * c + k, b1, b2, c1);
       } else {
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < kFChunks; ++c)
 #pragma unroll
           for (int k = 0; k < 32; ++k) {
             const int col = col0 + 32 * c + k;
@@ -391,16 +411,16 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       if (!ok) break;
       tc_fence_after();
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kFN);
-      uint32_t v[2][32];
-      tmem_ld32(tbase, v[0]);
-      tmem_ld32(tbase + 32u, v[1]);
-      tmem_wait(v[0]);
-      tmem_wait(v[1]);
+      uint32_t v[kFChunks][32];
+#pragma unroll
+      for (int c = 0; c < kFChunks; ++c) tmem_ld32(tbase + (uint32_t)(32 * c), v[c]);
+#pragma unroll
+      for (int c = 0; c < kFChunks; ++c) tmem_wait(v[c]);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
 #pragma unroll
-      for (int c = 0; c < 2; ++c) {
+      for (int c = 0; c < kFChunks; ++c) {
         const int col0 = wk.t * kFN + 32 * c;
         if (col0 >= nB) break;  // warp-uniform
         float f[32];
@@ -596,14 +616,14 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_f() {
   return fn;
 }
 
-// 3-D BF16 map over a planar layout (64 values of a K slice, row, plane), box (64, boxRows, 6),
-// 128-byte swizzle: one load fills 6 swizzled [boxRows][128 B] blocks.
-bool encode_f(CUtensorMap* map, const void* base, int rows, int boxRows) {
+// 3-D BF16 map over a planar layout (64 values of a K slice, row, plane), box (64, boxRows,
+// boxPlanes), 128-byte swizzle: one load fills boxPlanes swizzled [boxRows][128 B] blocks.
+bool encode_f(CUtensorMap* map, const void* base, int rows, int boxRows, int boxPlanes) {
   auto fn = get_encode_f();
   if (!fn) return false;
   cuuint64_t dims[3] = {64, (cuuint64_t)rows, (cuuint64_t)kFPlanes};
   cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
-  cuuint32_t box[3] = {64, (cuuint32_t)boxRows, (cuuint32_t)kFPlanes};
+  cuuint32_t box[3] = {64, (cuuint32_t)boxRows, (cuuint32_t)boxPlanes};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -617,7 +637,8 @@ int f_segments(int numSMs) { return numSMs * kFEpiWarps; }
 
 cudaError_t f_maps(CUtensorMap* mA, const void* dA, int rowsA, CUtensorMap* mB, const void* dB, int rowsB) {
   if (rowsA < kFM || rowsB < kFN) return cudaErrorInvalidValue;
-  if (!encode_f(mA, dA, rowsA, kFM) || !encode_f(mB, dB, rowsB, kFN)) return cudaErrorInvalidValue;
+  if (!encode_f(mA, dA, rowsA, kFM, kFAPlanes) || !encode_f(mB, dB, rowsB, kFN, kFPlanes))
+    return cudaErrorInvalidValue;
   return cudaSuccess;
 }
 
