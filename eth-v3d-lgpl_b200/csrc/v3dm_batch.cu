@@ -26,8 +26,8 @@
 // Float descriptors that are not all of the form u/512 (v3dm_batch_set_images_f32) take the same
 // passes on the BF16 hi/lo layouts of the single-pair float matcher (v3dm_match_f.cu): groups of
 // 128 lefts against tiles of 128 columns, each descriptor's exact best and second over the other
-// image kept in registers and decided with the float rules, so each pair's result equals that
-// matcher's.
+// image kept in registers (a guided call masks them with the pair's gate) and decided with the
+// float rules, so each pair's result equals that matcher's.
 // Every launch after the first reads its sizes from device memory, so the whole sequence is
 // captured once as a CUDA graph and replayed while the images, pairs and parameters stay the same.
 #include <algorithm>
@@ -1183,8 +1183,10 @@ int enqueue_batch(v3dm_batch* b, float minScore, float minRatio, bool withEvents
 
 // Enqueues one batch call on the float layouts: the passes of enqueue_batch with the float side
 // kernel, which writes every state's decision itself (one CTA scores a whole row, so the exact
-// best and second of each descriptor stay in registers): no chunk records, no re-score.
-int enqueue_batch_f(v3dm_batch* b, float minScore, float minRatio, bool withEvents) {
+// best and second of each descriptor stay in registers): no chunk records, no re-score.  With bg
+// set, the call is guided: each pair's gate masks its scores in both passes.
+int enqueue_batch_f(v3dm_batch* b, float minScore, float minRatio, bool withEvents,
+                    const BatchGateArgs* bg = nullptr) {
   const int GM = f_group_rows(), BN = f_tile_cols();
   const float Tf = host_float_threshold(minScore, minRatio);
   int launches = 0;
@@ -1196,6 +1198,7 @@ int enqueue_batch_f(v3dm_batch* b, float minScore, float minRatio, bool withEven
   sa.err = b->dInfo + kInfoErr;
   sa.minScore = minScore;
   sa.minRatio = minRatio;
+  if (bg) sa.bg = *bg;
   // ---- pass A: every (pair, group of 128 lefts) against the pair's right image
   sa.aIsLeft = 1;
   sa.rows = b->dRowsA;
@@ -1409,7 +1412,8 @@ int launch_call_guided(v3dm_batch* b, int type, float minScore, float minRatio) 
     for (int i = 0; i < 4; ++i)
       if (!b->ev[i]) V3DM_BTRY(cudaEventCreate(&b->ev[i]));
   }
-  st = enqueue_batch(b, minScore, minRatio, b->profile, &bg);
+  st = b->floatMode ? enqueue_batch_f(b, minScore, minRatio, b->profile, &bg)
+                    : enqueue_batch(b, minScore, minRatio, b->profile, &bg);
   if (st == V3DM_OK && b->profile) b->profPending = true;
   return st;
 }
@@ -2193,7 +2197,6 @@ int v3dm_batch_match_guided(v3dm_batch* b, int type, const double* M, const floa
   if (!b || !nOut || cap < 0 || (cap > 0 && !triples) || (type != 1 && type != 2)) return V3DM_ERR_ARG;
   if (!b->haveImages || !b->havePairs || !b->havePositions) return V3DM_ERR_NOT_ALLOCATED;
   if (b->nPairs > 0 && (!M || !thr)) return V3DM_ERR_ARG;
-  if (b->floatMode) return V3DM_ERR_UNSUPPORTED;
   BDeviceGuard g(b->device);
   V3DM_BTRY(cudaStreamSynchronize(b->stream));
   const int n = b->nPairs;

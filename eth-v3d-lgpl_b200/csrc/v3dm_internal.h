@@ -76,6 +76,23 @@ struct BatchRow {
   long long state0;  // state index of the group's first descriptor
 };
 
+// Gates of a batched guided call (v3dm_batch.cu): one gate per pair, evaluated on the fly from
+// the positions.  gm: per pair (caller's order) the 3x3 matrix as floats, then thr^2.
+constexpr int kBGateFloats = 10;
+struct BatchGateArgs {
+  int on;                        // 0: no batched gates
+  int type;                      // 1 epipolar (F), 2 homography (H)
+  const float* gm;
+  const int2* pairLR;            // per pair (caller's order): left image, right image
+  const float2* pos;             // positions of all images' descriptors, concatenated
+  const long long* posOff;       // per image: its first descriptor in pos
+  const long long* stateA0;      // per pair in batch order: its first pass-A state
+  const int* origOf;             // per pair in batch order: its index in the caller's order
+  int nPairs;
+  const int* chosenPair;         // per pass-B state: its pair (caller's order) and right
+  const int* chosenRight;
+};
+
 // One side pass scores the nA descriptors of side A against the nB descriptors of side B
 // (single pair), or walks a table of BatchRows (batched pass).
 struct SideArgs {
@@ -109,6 +126,7 @@ struct SideArgs {
   // batched float pass (launch_side_f_batch): decisions written per state, the float rules
   int32_t* decision;
   float minScore, minRatio;
+  BatchGateArgs bg;              // batched float pass of a guided call: each pair's gate (on = 0: none)
   // failure-path test hooks (zero in production): the bounded waits give up after waitLimit
   // cycles (0: the default), and CTA 0's producer does not issue its skipLoad-th B tile load
   // (0: none), so that the consumer's bounded wait for it runs out
@@ -181,22 +199,6 @@ cudaError_t launch_vtc(const VtcArgs& a, const CUtensorMap& nodeMap, const CUten
 // 2-D map over rows x 128 bytes with a box of boxRows rows and the 128-byte swizzle (v3dm_match_tc.cu).
 cudaError_t tc_rows_map(CUtensorMap* m, const uint8_t* base, int rows, int boxRows);
 
-// Gates of a batched guided call (v3dm_batch.cu): one gate per pair, evaluated on the fly from
-// the positions.  gm: per pair (caller's order) the 3x3 matrix as floats, then thr^2.
-constexpr int kBGateFloats = 10;
-struct BatchGateArgs {
-  int on;                        // 0: no batched gates
-  int type;                      // 1 epipolar (F), 2 homography (H)
-  const float* gm;
-  const int2* pairLR;            // per pair (caller's order): left image, right image
-  const float2* pos;             // positions of all images' descriptors, concatenated
-  const long long* posOff;       // per image: its first descriptor in pos
-  const long long* stateA0;      // per pair in batch order: its first pass-A state
-  const int* origOf;             // per pair in batch order: its index in the caller's order
-  int nPairs;
-  const int* chosenPair;         // per pass-B state: its pair (caller's order) and right
-  const int* chosenRight;
-};
 
 // Decision and bookkeeping kernels around the side passes (v3dm_pair.cu).
 struct PostArgs {

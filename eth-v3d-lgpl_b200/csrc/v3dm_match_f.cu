@@ -177,6 +177,24 @@ __device__ __forceinline__ void top2_push(uint32_t key, int col, uint32_t& b1, u
   b1 = max(b1, key);
 }
 
+// The gate of one lane's row in a guided batch (one gate per pair, the reference's expressions):
+// its pair's matrix and thr^2, the positions of the B image's descriptors, the A descriptor's
+// terms.
+struct GateLane {
+  const float* m;
+  const float2* bPos;
+  float4 aT;
+  int type, aIsLeft;
+};
+
+// Whether the gate masks (A descriptor of the lane, column col of the B image).  Called only for
+// scores that could enter the lane's top two, so it stays out of line.
+__device__ __noinline__ bool gate_rejects_col(GateLane gl, int col) {
+  const float2 pb = gl.bPos[col];
+  if (gl.aIsLeft) return gate_rejects_terms(gl.type, gl.m[9], gl.aT, gate_right_terms(gl.type, gl.m, pb));
+  return gate_rejects_terms(gl.type, gl.m[9], gate_left_terms(gl.type, gl.m, pb), gl.aT);
+}
+
 // Side A against side B.  One pair (kBatch false): nA rows (amap as in k_side) against nB rows;
 // the epilogue hands every 32-score chunk whose maximum reaches Tf to k_records_f.  A batch
 // (kBatch true): the row table; one CTA scores a row's A group against every tile of its B
@@ -345,11 +363,25 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     long long st = -1;
     uint32_t b1 = 0, b2 = 0;
     int c1 = 0;
+    const bool gated = a.bg.on != 0;
+    GateLane gl{};
     for (FWalk<kBatch> wk = start; wk.more() && ok; wk.next()) {
       if (wk.newA) {
         st = wk.state(q * 32 + lane);
         b1 = b2 = 0u;
         c1 = 0;
+        if (gated && st >= 0) {
+          int pair = 0, aIdx = 0;
+          bgate_resolve(a.bg, a.aIsLeft, st, &pair, &aIdx);
+          const int2 lr = a.bg.pairLR[pair];
+          const int aImg = a.aIsLeft ? lr.x : lr.y, bImg = a.aIsLeft ? lr.y : lr.x;
+          gl.m = a.bg.gm + (size_t)pair * kBGateFloats;
+          gl.type = a.bg.type;
+          gl.aIsLeft = a.aIsLeft;
+          const float2 pa = a.bg.pos[a.bg.posOff[aImg] + aIdx];
+          gl.aT = a.aIsLeft ? gate_left_terms(gl.type, gl.m, pa) : gate_right_terms(gl.type, gl.m, pa);
+          gl.bPos = a.bg.pos + a.bg.posOff[bImg];
+        }
       }
       const int nB = wk.nB();
       ok = mbar_wait(&s.accFull[acc], accPhase, &s.abort, a.err);
@@ -366,7 +398,22 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
       __syncwarp();
       if (lane == 0) mbar_arrive(&s.accEmpty[acc]);
       const int col0 = wk.t * kFN;
-      if (col0 + kFN <= nB) {  // warp-uniform: a full tile
+      if (gated) {
+        // a masked score counts as none (the reference's -1e20 is below Tf); the gate is tested
+        // only where a score could enter the top two (a key <= b2 leaves them unchanged)
+        const bool full = col0 + kFN <= nB;
+#pragma unroll
+        for (int c = 0; c < kFChunks; ++c)
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int col = col0 + 32 * c + k;
+            uint32_t key = (full || col < nB) ? f32_order(__uint_as_float(v[c][k])) : 0u;
+            if (key > b2) {
+              if (st >= 0 && gate_rejects_col(gl, col)) key = 0u;
+              top2_push(key, col, b1, b2, c1);
+            }
+          }
+      } else if (col0 + kFN <= nB) {  // warp-uniform: a full tile
 #pragma unroll
         for (int c = 0; c < kFChunks; ++c)
 #pragma unroll

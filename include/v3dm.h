@@ -221,9 +221,10 @@ V3DM_API int v3dm_batch_set_images_u8_device(v3dm_batch* b, int nImages, const i
  * setRightFeatures, v3d_cudamatching.cu:490-520).  When every value is of the form u/512 the
  * integer layout is used; otherwise every image is held in the BF16 hi/lo layouts of the
  * single-pair float matcher and each pair's result equals SIFTMatching's float
- * findPutativeMatches on the two images.  Guided and proposal calls need the integer layout
- * (V3DM_ERR_UNSUPPORTED on float images).  Non-finite values: V3DM_ERR_ARG.  *isFloat reports
- * which layout the last upload chose. */
+ * findPutativeMatches on the two images, and each pair's v3dm_batch_match_guided result equals
+ * that putative call followed by one runGuidedMatching / runGuidedHomographyMatching with the
+ * pair's gate.  Proposal calls need the integer layout (V3DM_ERR_UNSUPPORTED on float images).
+ * Non-finite values: V3DM_ERR_ARG.  *isFloat reports which layout the last upload chose. */
 V3DM_API int v3dm_batch_set_images_f32(v3dm_batch* b, int nImages, const int32_t* counts, const float* desc);
 V3DM_API int v3dm_batch_set_images_f32_device(v3dm_batch* b, int nImages, const int32_t* counts,
                                               const float* d_desc);
