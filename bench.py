@@ -1317,7 +1317,7 @@ def run_float(args, ws, rank, local):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s(bf16)",
                      "frac": achieved / peaks["bf16_tflops"], "traffic": traffic_from_profiles("k_side_f"),
                      "peak_src": f"{peaks['src']} bf16 dense burst", "kernel_ms": k_ms,
-                     "flops_per_launch": flops, "kernel": "k_side_f pass A (K = 384 BF16)"},
+                     "flops_per_launch": flops, "kernel": "k_side_f row walk, pass A (K = 384 BF16)"},
         "e2e": {"value": ws * 1000.0 / ms_e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(L.nbytes + R.nbytes),
                 "d2h_bytes_per_step": int(got.shape[0] * 8 + 16)},
         "gpu_launches": launches,

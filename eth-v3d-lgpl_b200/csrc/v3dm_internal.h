@@ -252,7 +252,8 @@ cudaError_t launch_side_f(const CUtensorMap& mA, const CUtensorMap& mB, const Si
 // Batched float side pass over a.rows (a.nRows, or *a.nRowsPtr rows), rows interleaved over the
 // persistent CTAs; A groups of f_group_rows() rows, B tiles of f_tile_cols() columns.  Writes
 // the decision of every state of the rows to a.decision (the float rules with a.minScore,
-// a.minRatio and the candidate threshold Tf); no chunk records.
+// a.minRatio and the candidate threshold Tf); no chunk records.  With a.rows null: one pair,
+// a.nA A rows against a.nB B rows, decisions indexed by A row.
 cudaError_t launch_side_f_batch(const CUtensorMap& mA, const CUtensorMap& mB, const SideArgs& a, float Tf,
                                 int numSMs, cudaStream_t st);
 int f_group_rows();
@@ -285,6 +286,10 @@ cudaError_t launch_rescore(const RescoreArgs& a, int grid, cudaStream_t s);
 // Rights accepted by some left: de-duplicated list, their descriptors gathered into dRc.
 cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
                           const uint8_t* dR, uint8_t* dRc, cudaStream_t s);
+// The same for rows of 'planes' 128-byte blocks (block p of row r at (p * cap + r) * 128).
+cudaError_t launch_choose_planes(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                                 const uint8_t* src, uint8_t* dst, int planes, int capSrc, int capDst,
+                                 cudaStream_t s);
 // Mutual filter and ordered compaction (blockCount: nL/2048 + 1 ints of scratch); clears chosenFlag.
 // The pair count goes to info[kInfoPairs] and, when countOut is set, to *countOut.
 cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,

@@ -92,7 +92,9 @@ __device__ __forceinline__ float fmax32(const float* v) {
 // The work of one CTA, in the order every role walks it.  One pair (kBatch false): the flat range
 // of (A group of 128 rows, B tile of 128 columns) this CTA owns.  A batch (kBatch true): the rows of
 // the row table interleaved over the CTAs (row r, r + gridDim.x, ...), each an A group of one image
-// against every 128-column tile of its B image; a row's state indices are state0 + its rows.
+// against every 128-column tile of its B image; a row's state indices are state0 + its rows.  With
+// no row table (a.rows null) the rows are those of one pair: row r is A rows 128r .. against all
+// a.nB B rows, its states the A row indices.
 template <bool kBatch>
 struct FWalk {
   // one pair
@@ -101,7 +103,7 @@ struct FWalk {
   const int* amap;
   // batch
   const BatchRow* rows;
-  int r, nRows;
+  int r, nRows, pairA, pairB;
   BatchRow cur;
   // the current item
   int t;          // B tile of the A group
@@ -117,13 +119,27 @@ struct FWalk {
     t = nTiles > 0 ? (int)(w % nTiles) : 0;
     newA = true;
   }
+  __device__ BatchRow row_at(int rr) const {
+    if (rows) return rows[rr];
+    BatchRow b;
+    b.aRow = rr * kFM;
+    b.validRows = min(kFM, pairA - rr * kFM);
+    b.bRow0 = 0;
+    b.nB = pairB;
+    b.nTiles = (pairB + kFN - 1) / kFN;
+    b.pad = 0;
+    b.state0 = (long long)rr * kFM;
+    return b;
+  }
   __device__ void init_batch(const SideArgs& a) {
     rows = a.rows;
-    nRows = a.nRowsPtr ? *a.nRowsPtr : a.nRows;
+    pairA = a.nA;
+    pairB = a.nB;
+    nRows = rows ? (a.nRowsPtr ? *a.nRowsPtr : a.nRows) : (pairB > 0 ? (pairA + kFM - 1) / kFM : 0);
     r = blockIdx.x;
     t = 0;
     newA = true;
-    if (r < nRows) cur = rows[r];
+    if (r < nRows) cur = row_at(r);
   }
   __device__ bool more() const {
     if constexpr (kBatch) return r < nRows;
@@ -138,7 +154,7 @@ struct FWalk {
       r += gridDim.x;
       t = 0;
       newA = true;
-      if (r < nRows) cur = rows[r];
+      if (r < nRows) cur = row_at(r);
     } else {
       ++w;
       t = (int)(w % nTiles);
@@ -724,11 +740,14 @@ cudaError_t launch_side_f_batch(const CUtensorMap& mA, const CUtensorMap& mB, co
     attrSet[dev] = true;
   }
   int grid = numSMs;
-  if (!a.nRowsPtr) {
+  if (!a.rows) {  // one pair: its rows are implicit
+    if (a.nA <= 0 || a.nB <= 0) return cudaSuccess;
+    grid = std::min(grid, (a.nA + kFM - 1) / kFM);
+  } else if (!a.nRowsPtr) {
     if (a.nRows <= 0) return cudaSuccess;
     grid = std::min(grid, a.nRows);
   }
-  if (!a.rows || !a.decision) return cudaErrorInvalidValue;
+  if (!a.decision) return cudaErrorInvalidValue;
   return launch_pdl(k_side_f<true>, dim3(grid), dim3(kFThreads), smem, st, mA, mB, a, Tf, (float*)nullptr);
 }
 

@@ -234,8 +234,11 @@ __global__ void k_rescore_decide(RescoreArgs a) {
   }
 }
 
+// A row is 'planes' blocks of 128 bytes, block p of row r at (p * cap + r) * 128 (one block:
+// uint8 descriptors; six: the planar BF16 hi/lo layout).
 __global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chosenFlag, int* chosenList,
-                         int* chosenCount, const uint8_t* __restrict__ dR, uint8_t* __restrict__ dRc) {
+                         int* chosenCount, const uint8_t* __restrict__ dR, uint8_t* __restrict__ dRc, int planes,
+                         int capSrc, int capDst) {
   pdl_wait();
   pdl_launch_dependents();
   const int lane = threadIdx.x & 31;
@@ -254,10 +257,12 @@ __global__ void k_choose(const int32_t* __restrict__ leftDec, int nL, int* chose
     if (!claim) continue;
     const int k = base + __popc(m & ((1u << lane) - 1u));
     chosenList[k] = r;
-    const uint4* src = reinterpret_cast<const uint4*>(dR + (size_t)r * kDescBytes);
-    uint4* dst = reinterpret_cast<uint4*>(dRc + (size_t)k * kDescBytes);
+    for (int p = 0; p < planes; ++p) {
+      const uint4* src = reinterpret_cast<const uint4*>(dR + ((size_t)p * capSrc + r) * kDescBytes);
+      uint4* dst = reinterpret_cast<uint4*>(dRc + ((size_t)p * capDst + k) * kDescBytes);
 #pragma unroll
-    for (int w = 0; w < kDescBytes / 16; ++w) dst[w] = src[w];
+      for (int w = 0; w < kDescBytes / 16; ++w) dst[w] = src[w];
+    }
   }
 }
 
@@ -353,7 +358,18 @@ cudaError_t launch_choose(const int32_t* leftDec, int nL, int* chosenFlag, int* 
   if (nL == 0) return cudaSuccess;
   int blocks = (nL + 255) / 256;
   if (blocks > 148) blocks = 148;
-  return launch_pdl(k_choose, dim3(blocks), dim3(256), 0, s, leftDec, nL, chosenFlag, chosenList, chosenCount, dR, dRc);
+  return launch_pdl(k_choose, dim3(blocks), dim3(256), 0, s, leftDec, nL, chosenFlag, chosenList, chosenCount, dR, dRc,
+                    1, 0, 0);
+}
+
+cudaError_t launch_choose_planes(const int32_t* leftDec, int nL, int* chosenFlag, int* chosenList, int* chosenCount,
+                                 const uint8_t* src, uint8_t* dst, int planes, int capSrc, int capDst,
+                                 cudaStream_t s) {
+  if (nL == 0) return cudaSuccess;
+  int blocks = (nL + 255) / 256;
+  if (blocks > 148) blocks = 148;
+  return launch_pdl(k_choose, dim3(blocks), dim3(256), 0, s, leftDec, nL, chosenFlag, chosenList, chosenCount, src,
+                    dst, planes, capSrc, capDst);
 }
 
 cudaError_t launch_mutual(const int32_t* leftDec, int nL, const int32_t* rightDec, int* chosenFlag, int* blockCount,
