@@ -853,40 +853,21 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
     if (e != V3DM_OK) return e;
     V3DM_CUDA_TRY(cudaEventRecord(evA[0], h->stream));
   }
-  const bool rowWalk = h->nGates == 0;
-  if (rowWalk) {
-    // Ungated: each CTA scores whole rows (128 lefts against every right) and decides them from
-    // the exact best and second it keeps in registers; no chunk records for pass A.
-    sa.rows = nullptr;
-    sa.decision = h->dLeftDec;
-    sa.minScore = minScore;
-    sa.minRatio = minRatio;
-    V3DM_CUDA_TRY(launch_side_f_batch(h->fmA_A, h->fmA_B, sa, Tf, h->numSMs, h->stream));
-    sa.decision = nullptr;
-  } else {
-    V3DM_CUDA_TRY(launch_side_f(h->fmA_A, h->fmA_B, sa, Tf, nullptr, h->numSMs, h->stream));
-  }
+  // Each CTA scores whole rows (128 lefts against every right) and decides them from the exact
+  // best and second it keeps in registers, the call's gates applied where a score could enter
+  // them; no chunk records for pass A.
+  sa.rows = nullptr;
+  sa.nGates = h->nGates;
+  sa.gatesDev = h->dGates;
+  sa.decision = h->dLeftDec;
+  sa.minScore = minScore;
+  sa.minRatio = minRatio;
+  V3DM_CUDA_TRY(launch_side_f_batch(h->fmA_A, h->fmA_B, sa, Tf, h->numSMs, h->stream));
+  sa.decision = nullptr;
   if (h->profile) V3DM_CUDA_TRY(cudaEventRecord(evA[1], h->stream));
-  if (rowWalk) {
-    V3DM_CUDA_TRY(launch_choose_planes(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dRfA,
-                                       h->dRcf, kFloatRowBytes / kDescBytes, h->capFR, h->capFR, h->stream));
-  } else {
-    pa.nRows = h->nL;
-    pa.aIsLeft = 1;
-    pa.best = h->dLBest;
-    pa.sec = h->dLSec;
-    pa.decision = h->dLeftDec;
-    pa.chooseFlag = h->dChosenFlag;  // accepted rights chosen while deciding
-    pa.chooseList = h->dChosenList;
-    pa.chooseCount = h->dCounters;
-    pa.chooseSrc = h->dRfA;
-    pa.chooseDst = h->dRcf;
-    pa.chooseCapSrc = h->capFR;
-    pa.chooseCapDst = h->capFR;
-    pa.choosePlanes = 6;
-    V3DM_CUDA_TRY(launch_post_f(pa, Tf, h->stream));
-    pa.chooseFlag = nullptr;
-  }
+  // the accepted rights, once each, gathered (six planes) for pass B
+  V3DM_CUDA_TRY(launch_choose_planes(h->dLeftDec, h->nL, h->dChosenFlag, h->dChosenList, h->dCounters, h->dRfA,
+                                     h->dRcf, kFloatRowBytes / kDescBytes, h->capFR, h->capFR, h->stream));
   // pass B: the chosen rights against every left
   sa.nAptr = h->dCounters;
   sa.nA = h->nR;
@@ -913,7 +894,7 @@ int enqueue_match_f(v3dm_matcher* h, float minScore, float minRatio, int32_t* dP
   V3DM_CUDA_TRY(launch_mutual(h->dLeftDec, h->nL, h->dRightDec, h->dChosenFlag, h->dScratch,
                               reinterpret_cast<int2*>(dPairs), h->dInfo, h->countOut, h->stream));
   h->countWritten = h->countOut != nullptr;
-  h->lastLaunches = (h->floatL ? 0 : 1) + (h->floatR ? 0 : 1) + (rowWalk ? 7 : 8);
+  h->lastLaunches = (h->floatL ? 0 : 1) + (h->floatR ? 0 : 1) + 7;
   return V3DM_OK;
 }
 

@@ -211,6 +211,14 @@ __device__ __noinline__ bool gate_rejects_col(GateLane gl, int col) {
   return gate_rejects_terms(gl.type, gl.m[9], gate_left_terms(gl.type, gl.m, pb), gl.aT);
 }
 
+// Whether any of the single-pair matcher's gates (compounding since the last putative call) masks
+// (left l, right r); out of line for the same reason.
+__device__ __noinline__ bool gates_reject(const GateParams* gates, int n, int l, int r) {
+  for (int g = 0; g < n; ++g)
+    if (gate_rejects(gates[g], l, r)) return true;
+  return false;
+}
+
 // Side A against side B.  One pair (kBatch false): nA rows (amap as in k_side) against nB rows;
 // the epilogue hands every 32-score chunk whose maximum reaches Tf to k_records_f.  A batch
 // (kBatch true): the row table; one CTA scores a row's A group against every tile of its B
@@ -379,14 +387,14 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     long long st = -1;
     uint32_t b1 = 0, b2 = 0;
     int c1 = 0;
-    const bool gated = a.bg.on != 0;
+    const bool gated = a.bg.on != 0 || a.nGates > 0;
     GateLane gl{};
     for (FWalk<kBatch> wk = start; wk.more() && ok; wk.next()) {
       if (wk.newA) {
         st = wk.state(q * 32 + lane);
         b1 = b2 = 0u;
         c1 = 0;
-        if (gated && st >= 0) {
+        if (a.bg.on && st >= 0) {
           int pair = 0, aIdx = 0;
           bgate_resolve(a.bg, a.aIsLeft, st, &pair, &aIdx);
           const int2 lr = a.bg.pairLR[pair];
@@ -425,7 +433,12 @@ k_side_f(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             const int col = col0 + 32 * c + k;
             uint32_t key = (full || col < nB) ? f32_order(__uint_as_float(v[c][k])) : 0u;
             if (key > b2) {
-              if (st >= 0 && gate_rejects_col(gl, col)) key = 0u;
+              if (st >= 0) {
+                const bool masked = a.bg.on ? gate_rejects_col(gl, col)
+                                            : gates_reject(a.gatesDev, a.nGates, a.aIsLeft ? (int)st : col,
+                                                           a.aIsLeft ? col : (int)st);
+                if (masked) key = 0u;
+              }
               top2_push(key, col, b1, b2, c1);
             }
           }
