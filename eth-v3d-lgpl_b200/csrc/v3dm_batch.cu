@@ -78,6 +78,7 @@ constexpr int kCntAll = 16;      // batch and proposal counter words
 
 constexpr int kScanThreads = 1024;
 constexpr int kChooseThreads = 256;
+constexpr int kChoosePer = 4;     // lefts per thread and step in k_bchoose
 constexpr int kBMutThreads = 256;
 constexpr int kBMutPerBlock = 2048;
 
@@ -213,12 +214,22 @@ k_bchoose(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict_
     const long long rowBase = ib.padBase + (s0 - ib.stateB0);
     const int rRowOff = im[q.ri].rowOff;
     int run = 0;
-    for (int l0 = 0; l0 < q.nL; l0 += kChooseThreads) {
-      const int l = l0 + threadIdx.x;
-      const int d = l < q.nL ? decA[q.stateA0 + l] : -1;
-      const bool acc = d >= 0;
-      const unsigned m = __ballot_sync(0xffffffffu, acc);
-      if (lane == 0) wsum[w] = __popc(m);
+    // each thread takes kChoosePer consecutive lefts per step (their loads in flight together)
+    for (int l0 = 0; l0 < q.nL; l0 += kChooseThreads * kChoosePer) {
+      const int lb = l0 + threadIdx.x * kChoosePer;
+      int d[kChoosePer];
+#pragma unroll
+      for (int i = 0; i < kChoosePer; ++i) d[i] = lb + i < q.nL ? decA[q.stateA0 + lb + i] : -1;
+      int c = 0;
+#pragma unroll
+      for (int i = 0; i < kChoosePer; ++i) c += d[i] >= 0;
+      int inc = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+      }
+      if (lane == 31) wsum[w] = inc;
       __syncthreads();
       int before = 0, tot = 0;
 #pragma unroll
@@ -226,19 +237,22 @@ k_bchoose(const BPair* __restrict__ pairs, int nPairs, const BImage* __restrict_
         before += k < w ? wsum[k] : 0;
         tot += wsum[k];
       }
-      if (acc) {
-        const int k = run + before + __popc(m & ((1u << lane) - 1u));
+      int k = run + before + inc - c;  // slot of this thread's first accepted left, ascending left order
+#pragma unroll
+      for (int i = 0; i < kChoosePer; ++i) {
+        if (d[i] < 0) continue;
         const long long st = s0 + k;
-        chosenLeft[st] = l;
-        chosenRight[st] = d;
+        chosenLeft[st] = lb + i;
+        chosenRight[st] = d[i];
         chosenPair[st] = q.orig;
-        for (int p = 0; p < planes; ++p) {
+        for (int pl = 0; pl < planes; ++pl) {
           const uint4* src =
-              reinterpret_cast<const uint4*>(img + ((size_t)p * srcPlaneRows + rRowOff + d) * kDescBytes);
-          uint4* dst = reinterpret_cast<uint4*>(dAB + ((size_t)p * dstPlaneRows + rowBase + k) * kDescBytes);
+              reinterpret_cast<const uint4*>(img + ((size_t)pl * srcPlaneRows + rRowOff + d[i]) * kDescBytes);
+          uint4* dst = reinterpret_cast<uint4*>(dAB + ((size_t)pl * dstPlaneRows + rowBase + k) * kDescBytes);
 #pragma unroll
           for (int x = 0; x < kDescBytes / 16; ++x) dst[x] = src[x];
         }
+        ++k;
       }
       run += tot;
       __syncthreads();
