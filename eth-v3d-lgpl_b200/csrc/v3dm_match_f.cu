@@ -8,11 +8,17 @@
 // (tcgen05.mma.kind::f16, BF16 x BF16 -> F32 in TMEM).  For u/512 inputs hi is exact and lo = 0,
 // so the scores equal the integer path's exactly.
 //
-// Selection differs from the integer path in one point: the side kernel hands over every
-// 32-score chunk whose maximum reaches Tf, the float candidate threshold -- the smallest score a
-// second value must reach to change any decision (scores below it never matter, see
-// host_float_threshold).  k_records_f then sees every score that matters, so the best and the
-// second value are exact for the float scores and no re-score pass exists.
+// Selection is exact for the float scores, in one of two ways.  Tf, the float candidate
+// threshold, is the smallest score a second value must reach to change any decision (scores
+// below it never matter, see host_float_threshold).
+//   - Flat walk (k_side_f<false>: a CTA owns a range of (A group, B tile) items, so a row's
+//     scores are spread over CTAs): the side kernel hands over every 32-score chunk whose maximum
+//     reaches Tf, and k_records_f / k_decide_f select from those records.
+//   - Row walk (k_side_f<true>: a CTA scores a whole row, an A group against every tile of its B
+//     side): each epilogue lane keeps its row's best and second in registers and writes the
+//     decision itself; gates are tested only where a score could enter those two.
+// Batches and pass A of a single pair take the row walk; pass B of a single pair (few chosen
+// rights, too few rows to fill the CTAs) takes the flat walk.  No re-score pass exists.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
