@@ -1,6 +1,10 @@
 // -*- C++ -*-
-// compat/V3DM/v3dm_sfm_stages.h -- two SfM-app stages around the matcher, batched on libv3dm.so,
-// with the apps' own containers:
+// compat/V3DM/v3dm_sfm_stages.h -- SfM-app stages around the matcher, batched on libv3dm.so, with
+// the apps' own containers:
+//   - findPutativeMatchesBatch() / runGuidedMatchingBatch(): match_sequence's per-pair loop
+//     (V3D/Apps/SfM/match_sequence.cpp:165-234: setLeftFeatures, then setRightFeatures and
+//     findPutativeMatches for every right view; runGuidedMatching after RANSAC, :306-324) for a
+//     whole list of view pairs in one batched call, each pair's matches as that loop gets them;
 //   - retrieveSequence(): the voctree app's retrieval loop (V3D/Apps/SfM/match_using_voctree.cpp:
 //     176-222: LeafDocuments::computeBinomialScores, then insertDocument, for every image) in one
 //     call, filling the same per-image score lists (nBestDocuments entries, best first) and the same
@@ -17,6 +21,7 @@
 #ifndef V3DM_SFM_STAGES_H
 #define V3DM_SFM_STAGES_H
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -45,7 +50,115 @@ inline void check(int status, const char* what) {
 #endif
 }
 
+// Concatenated float descriptors of the views, each view cut to the count the apps pass to
+// setLeftFeatures / setRightFeatures: min(nMaxFeatures, size & 0xffe0) (match_sequence.cpp:183,
+// :215), its first descriptors in order.
+template <typename Views>
+inline void viewDescriptors(Views const& views, int nMaxFeatures, std::vector<int32_t>& counts,
+                            std::vector<float>& desc) {
+  const int n = (int)views.size();
+  counts.assign(n, 0);
+  size_t total = 0;
+  for (int v = 0; v < n; ++v) {
+    counts[v] = std::min(nMaxFeatures, int(views[v].size() & 0xffe0));
+    if (counts[v] < 0) counts[v] = 0;
+    total += (size_t)counts[v];
+  }
+  desc.resize(total * 128);
+  size_t at = 0;
+  for (int v = 0; v < n; ++v)
+    for (int k = 0; k < counts[v]; ++k, ++at)
+      for (int i = 0; i < 128; ++i) desc[at * 128 + i] = views[v][k].descriptor[i];
+}
+
+// Runs one batched call (putative, or guided with M/thr) and splits the (pair, left, right)
+// triples into one (left, right) list per pair, ascending left.
+inline void batchMatches(v3dm_batch* b, std::vector<std::pair<int, int> > const& pairs, const double* M,
+                         const float* thr, float minScore, float minRatio,
+                         std::vector<std::vector<std::pair<int, int> > >& matches, const char* who) {
+  std::vector<int32_t> tab(2 * pairs.size());
+  for (size_t p = 0; p < pairs.size(); ++p) {
+    tab[2 * p] = pairs[p].first;
+    tab[2 * p + 1] = pairs[p].second;
+  }
+  check(v3dm_batch_set_pairs(b, (int)pairs.size(), tab.data()), who);
+  long long cap = 1 << 20, n = 0;
+  std::vector<int32_t> t;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    t.resize((size_t)3 * (size_t)(cap > 0 ? cap : 1));
+    const int st = M ? v3dm_batch_match_guided(b, 1, M, thr, minScore, minRatio, t.data(), cap, &n)
+                     : v3dm_batch_match(b, minScore, minRatio, t.data(), cap, &n);
+    if (st == V3DM_ERR_CAPACITY && attempt == 0) {
+      cap = n;
+      continue;
+    }
+    check(st, who);
+    break;
+  }
+  matches.assign(pairs.size(), std::vector<std::pair<int, int> >());
+  for (long long k = 0; k < n; ++k) matches[t[3 * k]].push_back(std::make_pair(t[3 * k + 1], t[3 * k + 2]));
+}
+
 }  // namespace detail
+
+// views[v]: view v's features (any container of elements with descriptor[128] floats, e.g.
+// SerializableVector<SIFT_Feature>); pairs[p] = (view1, view2), view1 the left.  matches[p]
+// receives what findPutativeMatches(matches, minScore, minRatio) returns for that pair in the
+// app's loop, with each view cut to min(nMaxFeatures, size & 0xffe0) features.  Descriptors that
+// are not u/512 take the BF16 hi/lo path of the float matcher, as setLeftFeatures(float*) does.
+template <typename Views>
+inline void findPutativeMatchesBatch(Views const& views, int nMaxFeatures,
+                                     std::vector<std::pair<int, int> > const& pairs, float minScore, float minRatio,
+                                     std::vector<std::vector<std::pair<int, int> > >& matches, int device = 0) {
+  const char* who = "findPutativeMatchesBatch()";
+  std::vector<int32_t> counts;
+  std::vector<float> desc;
+  detail::viewDescriptors(views, nMaxFeatures, counts, desc);
+  v3dm_batch* b = nullptr;
+  detail::check(v3dm_batch_create(&b, device), who);
+  const int st = v3dm_batch_set_images_f32(b, (int)counts.size(), counts.data(), desc.data());
+  if (st != V3DM_OK) {
+    v3dm_batch_destroy(b);
+    detail::check(st, who);
+  }
+  detail::batchMatches(b, pairs, nullptr, nullptr, minScore, minRatio, matches, who);
+  v3dm_batch_destroy(b);
+}
+
+// The same pairs after RANSAC: matches[p] receives runGuidedMatching(F[p], thr[p], leftPos,
+// rightPos, matches, minScore, minRatio) of pair p after its findPutativeMatches, the positions
+// being the features' position[0], position[1].  F[p] indexable as F[i][j] (e.g. Matrix3x3d).
+template <typename Views, typename Mat3>
+inline void runGuidedMatchingBatch(Views const& views, int nMaxFeatures, std::vector<std::pair<int, int> > const& pairs,
+                                   std::vector<Mat3> const& F, std::vector<float> const& thr, float minScore,
+                                   float minRatio, std::vector<std::vector<std::pair<int, int> > >& matches,
+                                   int device = 0) {
+  const char* who = "runGuidedMatchingBatch()";
+  if (F.size() != pairs.size() || thr.size() != pairs.size()) detail::check(V3DM_ERR_ARG, who);
+  std::vector<int32_t> counts;
+  std::vector<float> desc;
+  detail::viewDescriptors(views, nMaxFeatures, counts, desc);
+  std::vector<float> pos;
+  for (size_t v = 0; v < views.size(); ++v)
+    for (int k = 0; k < counts[v]; ++k) {
+      pos.push_back(views[v][k].position[0]);
+      pos.push_back(views[v][k].position[1]);
+    }
+  std::vector<double> M(9 * pairs.size());
+  for (size_t p = 0; p < pairs.size(); ++p)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) M[9 * p + 3 * i + j] = F[p][i][j];
+  v3dm_batch* b = nullptr;
+  detail::check(v3dm_batch_create(&b, device), who);
+  int st = v3dm_batch_set_images_f32(b, (int)counts.size(), counts.data(), desc.data());
+  if (st == V3DM_OK) st = v3dm_batch_set_positions(b, pos.empty() ? nullptr : pos.data());
+  if (st != V3DM_OK) {
+    v3dm_batch_destroy(b);
+    detail::check(st, who);
+  }
+  detail::batchMatches(b, pairs, M.data(), thr.data(), minScore, minRatio, matches, who);
+  v3dm_batch_destroy(b);
+}
 
 // visualWords[i]: the leaf-local words of image i (VocabularyTree::getVisualWord, or
 // v3dm_voctree_quantize_* with V3DM_LEAF_LOCAL); nLeaves = the tree's visualWordCount().

@@ -1,6 +1,9 @@
 // Builds against compat/V3DM/v3dm_sfm_stages.h with stand-ins for the apps' types (the same member
-// names as V3D's PointCorrespondence, Matrix3x3d and RobustOrientationResult) and runs both stages
-// on a tiny input.  Without a GPU it must fail loudly (exit 1 with the header's message).
+// names as V3D's PointCorrespondence, Matrix3x3d, RobustOrientationResult and SIFT_Feature) and runs
+// one stage on a tiny input.  Without a GPU it must fail loudly (exit 1 with the header's message).
+// Mode 'm' / 'g' with an input and an output file: the batched putative / guided matching stage on
+// the views and pairs of the input, its per-pair matches written to the output.
+#include <cstdint>
 #include <cstdio>
 #include <vector>
 
@@ -33,7 +36,59 @@ struct Result {
   double error;
 };
 
+struct Feature {
+  Vec2 position;
+  float descriptor[128];
+};
+
+// Input: int32 nViews, nPairs, nMaxFeatures; float minScore, minRatio; per view int32 n then n
+// features (2 floats position, 128 floats descriptor); per pair int32 view1, view2, 9 doubles F,
+// float thr.  Output: per pair int32 count then count (left, right) int32 pairs.
+static int run_matching(bool guided, const char* in, const char* out) {
+  FILE* f = std::fopen(in, "rb");
+  if (!f) return 2;
+  int32_t head[3];
+  float params[2];
+  if (std::fread(head, 4, 3, f) != 3 || std::fread(params, 4, 2, f) != 2) return 2;
+  std::vector<std::vector<Feature> > views(head[0]);
+  for (auto& v : views) {
+    int32_t n = 0;
+    if (std::fread(&n, 4, 1, f) != 1) return 2;
+    v.resize(n);
+    for (auto& x : v)
+      if (std::fread(x.position.v, 4, 2, f) != 2 || std::fread(x.descriptor, 4, 128, f) != 128) return 2;
+  }
+  std::vector<std::pair<int, int> > pairs(head[1]);
+  std::vector<Mat3> F(head[1]);
+  std::vector<float> thr(head[1]);
+  for (int p = 0; p < head[1]; ++p) {
+    int32_t vv[2];
+    if (std::fread(vv, 4, 2, f) != 2 || std::fread(F[p].m, 8, 9, f) != 9 || std::fread(&thr[p], 4, 1, f) != 1)
+      return 2;
+    pairs[p] = std::make_pair(vv[0], vv[1]);
+  }
+  std::fclose(f);
+  std::vector<std::vector<std::pair<int, int> > > matches;
+  if (guided)
+    V3D_B200::runGuidedMatchingBatch(views, head[2], pairs, F, thr, params[0], params[1], matches);
+  else
+    V3D_B200::findPutativeMatchesBatch(views, head[2], pairs, params[0], params[1], matches);
+  FILE* o = std::fopen(out, "wb");
+  if (!o) return 2;
+  for (auto const& m : matches) {
+    const int32_t n = (int32_t)m.size();
+    std::fwrite(&n, 4, 1, o);
+    for (auto const& pr : m) {
+      const int32_t lr[2] = {pr.first, pr.second};
+      std::fwrite(lr, 4, 2, o);
+    }
+  }
+  std::fclose(o);
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc > 3 && (argv[1][0] == 'm' || argv[1][0] == 'g')) return run_matching(argv[1][0] == 'g', argv[2], argv[3]);
   const bool ransacFirst = argc > 1 && argv[1][0] == 'r';
   std::vector<std::vector<Corr> > corrs(2, std::vector<Corr>(40));
   for (int p = 0; p < 2; ++p)

@@ -117,3 +117,83 @@ def test_stages_fail_loudly_without_gpu(stages_bin, mode, who):
     p = subprocess.run([str(stages_bin), mode], capture_output=True, text=True, timeout=120)
     assert p.returncode == 1
     assert f"V3D_B200 {who}: no sm_100" in p.stderr
+
+
+def _views_payload(views, pairs, F, thr, n_max, min_score, min_ratio):
+    """views: list of (positions (n, 2), float descriptors (n, 128)); pairs (view1, view2)."""
+    parts = [struct.pack("<iiiff", len(views), len(pairs), n_max, min_score, min_ratio)]
+    for pos, desc in views:
+        parts.append(struct.pack("<i", desc.shape[0]))
+        rec = np.concatenate([np.asarray(pos, np.float32), np.asarray(desc, np.float32)], axis=1)
+        parts.append(np.ascontiguousarray(rec, np.float32).tobytes())
+    for k, (a, b) in enumerate(pairs):
+        parts.append(struct.pack("<ii", int(a), int(b)))
+        parts.append(np.asarray(F[k], np.float64).tobytes())
+        parts.append(struct.pack("<f", float(thr[k])))
+    return b"".join(parts)
+
+
+def _read_matches(buf, n_pairs):
+    out, off = [], 0
+    for _ in range(n_pairs):
+        pr, off = _read_pairs(buf, off)
+        out.append(pr)
+    assert off == len(buf)
+    return out
+
+
+@pytest.mark.parametrize("mode,who", [("m", "findPutativeMatchesBatch()"), ("g", "runGuidedMatchingBatch()")])
+def test_matching_stages_fail_loudly_without_gpu(stages_bin, mode, who, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    rng = np.random.default_rng(0)
+    views = [(rng.uniform(0, 100, (40, 2)), rng.uniform(0, 1, (40, 128))) for _ in range(2)]
+    fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
+    fin.write_bytes(_views_payload(views, [(0, 1)], [np.eye(3)], [2.0], 4096, 0.7, 0.8))
+    p = subprocess.run([str(stages_bin), mode, str(fin), str(fout)], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 1
+    assert f"V3D_B200 {who}: no sm_100" in p.stderr
+
+
+@pytest.mark.gpu
+def test_matching_stages_equal_the_app_loop(stages_bin, oracle_mod, v3dm_mod, tmp_path):
+    """The app's per-pair loop (match_sequence.cpp:165-234, :306-324) with its count rounding
+    (min(nMaxFeatures, size & 0xffe0)): u/512 views against the oracle (putative and F-guided),
+    float views against the single-pair float matcher."""
+    desc8, counts, offs, pos, cams = synth.scene(24, 5, 300, 1500)
+    n_max = 1200
+    cut = [min(n_max, int(c) & 0xffe0) for c in counts]
+    pairs = [(0, 1), (1, 2), (0, 2), (3, 4), (2, 4), (4, 0)]
+    F = [synth.fundamental(cams, a, b) for a, b in pairs]
+    thr = [2.0, 8.0, 2.0, 2.0, 8.0, 2.0]
+    views8 = [(pos[offs[v]:offs[v + 1]], desc8[offs[v]:offs[v + 1]].astype(np.float32) / 512) for v in range(5)]
+    for mode in ("m", "g"):
+        fin, fout = tmp_path / f"in_{mode}.bin", tmp_path / f"out_{mode}.bin"
+        fin.write_bytes(_views_payload(views8, pairs, F, thr, n_max, 0.7, 0.8))
+        p = subprocess.run([str(stages_bin), mode, str(fin), str(fout)], capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stderr
+        got = _read_matches(fout.read_bytes(), len(pairs))
+        for k, (a, b) in enumerate(pairs):
+            L = desc8[offs[a]:offs[a] + cut[a]]
+            R = desc8[offs[b]:offs[b] + cut[b]]
+            if mode == "m":
+                exp = oracle_mod.match(L, R, 0.7, 0.8)
+            else:
+                exp = oracle_mod.match(L, R, 0.7, 0.8, gates=[("F", F[k], thr[k])], lpos=pos[offs[a]:offs[a] + cut[a]],
+                                       rpos=pos[offs[b]:offs[b] + cut[b]])
+            np.testing.assert_array_equal(got[k], exp, err_msg=f"{mode} pair {k}")
+    # float descriptors (not u/512): the single-pair float matcher's putative result
+    descf = synth.float_from_u8(desc8, 24)
+    viewsf = [(pos[offs[v]:offs[v + 1]], descf[offs[v]:offs[v + 1]]) for v in range(5)]
+    fin, fout = tmp_path / "in_f.bin", tmp_path / "out_f.bin"
+    fin.write_bytes(_views_payload(viewsf, pairs, F, thr, n_max, 0.7, 0.8))
+    p = subprocess.run([str(stages_bin), "m", str(fin), str(fout)], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    got = _read_matches(fout.read_bytes(), len(pairs))
+    for k, (a, b) in enumerate(pairs):
+        with v3dm_mod.SIFTMatching(0) as m:
+            m.allocate(cut[a], cut[b], False)
+            m.set_left_features(descf[offs[a]:offs[a] + cut[a]])
+            m.set_right_features(descf[offs[b]:offs[b] + cut[b]])
+            np.testing.assert_array_equal(got[k], m.find_putative_matches(0.7, 0.8), err_msg=f"float pair {k}")
